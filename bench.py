@@ -1,0 +1,397 @@
+"""Throughput of the particle-mesh step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3] [--impl ours|reference]
+
+One step = gather-kick + drift + rebin of every particle (updateVel +
+moveParticles of the reference) followed by the scalar CIC deposit of the new
+positions (scalarProjectionCIC_project + _comm): one fused lf2_step call.
+Metric: particle updates per second, whole job (sum over ranks).
+
+Workloads (seeded synthetic inputs; no dataset is involved):
+  c3  512^3 lattice, 134,217,728 particles, log-normal clustering
+      (rho ~ exp(2 delta_G - 2), delta_G Gaussian with P(k) ~ k^-2),
+      int64 fixed-point deposit  [default: the size the throughput target is
+      quoted on]
+  c2  256^3, 16,777,216 particles, half uniform, half in 64 Gaussian clumps
+      (sigma 0.01 box), FP32 deposit
+  c5  768^3, 452,984,832 particles, 90% uniform + 10% in 1,000 halos
+      (sigma 0.002 box), fixed-point deposit
+Velocities N(0, 0.01^2) box units per time; drift dtau = 0.1 * 64/N so the
+rms displacement per step (0.064 cells) matches the 64^3 reference case; the
+kick uses the central-difference gradient of a Gaussian random field.
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload
+(weak scaling, no collective on the data path); time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c3": dict(n=512, npart=512 ** 3, dist="lognormal", mode="fixed"),
+    "c2": dict(n=256, npart=256 ** 3, dist="clumps", mode="fp32"),
+    "c5": dict(n=768, npart=768 ** 3, dist="halos", mode="fixed"),
+    "c1": dict(n=64, npart=64 ** 3, dist="uniform", mode="fp32"),
+}
+METRIC = "particle updates/s (CIC deposit+gather+move)"
+UNIT = "particle-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (read-only query)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                mx = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------- workloads
+def make_workload(name, device):
+    import torch
+    import latfield2_b200.workloads as W
+    w = WORKLOADS[name]
+    n = (w["n"],) * 3
+    npart = w["npart"]
+    if w["dist"] == "lognormal":
+        cell, off = W.lognormal(n, npart, seed=3, device=device)
+    elif w["dist"] == "clumps":
+        cell, off = W.clumps(n, npart, 64, 0.01, seed=3, device=device)
+    elif w["dist"] == "halos":
+        cell, off = W.halos(n, npart, 1000, 0.002, seed=3, device=device)
+    else:
+        cell, off = W.uniform(n, npart, seed=3, device=device)
+    vel = W.velocities(npart, 0.01, seed=4, device=device)
+    F = W.grf_gradient(n, seed=2, device=device, amplitude=0.01)
+    torch.cuda.synchronize() if device != "cpu" else None
+    return n, cell, off, vel, F
+
+
+def alg_bytes_move(npart, nsites):
+    # particle state (int32 cell + 3 f32 offsets + 3 f32 velocities) read and
+    # written once, 3-component field read once
+    return npart * 56 + nsites * 12
+
+
+def alg_bytes_deposit(npart, nsites):
+    # cell + offsets read once, scalar density written once
+    return npart * 16 + nsites * 4
+
+
+def alg_bytes_step(npart, nsites):
+    return npart * 56 + nsites * 4 * (1 + 3)
+
+
+def traffic_from_profiles(kernel, workload):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(workload, {}).get(kernel)
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_baseline_port(seconds, n_sample=64, npart_sample=64 ** 3, procs=1):
+    """The oracle (reference restatement, double) on a bounded sample: a 64^3
+    lattice with 262,144 particles (same one-particle-per-cell density),
+    deposit + comm, updateVel with the CIC gather-kick, move; repeated until
+    `seconds` of CPU work; `procs` independent processes."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.starmap(_cpu_worker, [(seconds, n_sample, npart_sample, 100 + i)
+                                         for i in range(procs)])
+    ups = sum(r[0] for r in res)
+    steps = sum(r[1] for r in res)
+    return ups, steps
+
+
+def _cpu_worker(seconds, n, npart, seed):
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    nn = (n, n, n)
+    res = 1.0 / n
+    pos = rng.random((npart, 3))
+    vel = 0.01 * rng.standard_normal((npart, 3))
+    u = np.floor(pos * n).astype(np.int64)
+    cell = (u[:, 0] + n * (u[:, 1] + n * u[:, 2])).astype(np.int32)
+    F = O.projection_init(nn, 1, 3)
+    F[1:-1, 1:-1, 1:-1] = 0.01 * rng.standard_normal((n, n, n, 3))
+    O.update_halo(F, nn, 1)
+    dtau = 0.1
+    steps = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds or steps == 0:
+        cs, order = O.lists_from_insertion(nn, cell)
+        pos, vel, cell = pos[order], vel[order], cell[order]
+        O.scalar_cic(nn, 1, res, cs, pos, None, 1.0 / npart)
+        O.update_vel_cic(nn, 1, cs, pos, vel, F, dtau)
+        cell = O.move_simple(nn, 1.0, pos, vel, dtau)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return npart * steps / dt, steps
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ups, steps = cpu_baseline_port(args.cpu_seconds, procs=procs)
+    wall = time.perf_counter() - t0
+    w = WORKLOADS[args.workload]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ups, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * w["npart"] / ups, "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": args.workload, "lattice": w["n"],
+                                        "particles": w["npart"]},
+        "cpu_baseline": {"value": ups, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{procs} processes x 64^3 lattice, 262,144 uniform particles, "
+                                   f"{steps} steps of deposit+comm, updateVel CIC kick, move "
+                                   f"(CPU restatement of the reference, double)"},
+        "e2e": {"value": ups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- ours
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import numpy as np
+    import torch
+    import latfield2_b200 as L
+
+    torch.cuda.set_device(local)
+    device = f"cuda:{local}"
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    w = WORKLOADS[args.workload]
+    mode = L.DEPOSIT_FIXED64 if w["mode"] == "fixed" else L.DEPOSIT_FP32
+    n, cell, off, vel, F = make_workload(args.workload, device)
+    npart = int(cell.shape[0])
+    nsites = n[0] * n[1] * n[2]
+    ctx = L.Context(n, box=1.0, mode=mode, device=local)
+    ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
+    del cell, off, vel
+    Fh = ctx.field(3, F)
+    rho = ctx.field(1)
+    torch.cuda.empty_cache()
+    dtau = 0.1 * 64.0 / n[0]
+
+    ctx.deposit_scalar(rho)
+    for _ in range(args.warmup):
+        ctx.step(Fh, dtau, dtau, rho)
+    ctx.synchronize()
+    ctx.profile_read()
+    ctx.profile(True)
+    l0 = ctx.kernel_launches()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            ctx.step(Fh, dtau, dtau, rho)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+    launches = ctx.kernel_launches() - l0
+    ctx.synchronize()  # raises if a kernel flagged an error
+    ms = e0.elapsed_time(e1)
+    phases = ctx.profile_read()
+    ctx.profile(False)
+    if pg is not None:
+        t = torch.tensor([ms], device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = npart * world * args.steps / (ms / 1e3)
+
+    # dominant kernel and its roofline (algorithmic bytes per launch / mean launch time)
+    peak, peak_kind = peaks()
+    dom = max(("move", "deposit_tile"), key=lambda p: phases[p][0])
+    per_launch_ms = phases[dom][0] / max(1, phases[dom][1])
+    if dom == "move":
+        ab = alg_bytes_move(npart, nsites)
+        kname = "k_move<kick,drift>"
+    else:
+        ab = alg_bytes_deposit(npart, nsites)
+        kname = "k_deposit<scalar>"
+    achieved = ab / (per_launch_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "alg_bytes_per_launch": ab, "ms_per_launch": per_launch_ms,
+                "traffic": traffic_from_profiles(kname, args.workload)}
+    step_ab = alg_bytes_step(npart, nsites)
+    step_roofline = {"alg_bytes": step_ab, "achieved": step_ab / (ms_step / 1e3) / 1e9,
+                     "frac": step_ab / (ms_step / 1e3) / 1e9 / peak}
+    phase_ms = {k: v[0] / args.steps for k, v in phases.items()}
+
+    # end to end through the C ABI with host buffers: the force field comes
+    # from pinned host memory, the density and max |v| go back to the host
+    Fhost = F.cpu().pin_memory()
+    rho_host = torch.empty(nsites, dtype=torch.float32).pin_memory()
+    Fnp = Fhost.numpy().reshape(3, n[2], n[1], n[0]).transpose(1, 2, 3, 0)
+    Fref = np.ascontiguousarray(Fnp)  # reference layout (z, y, x, c), halo 0
+    Fpin = torch.from_numpy(Fref).pin_memory()
+    Fpin_np = Fpin.numpy()
+    rho_np = rho_host.numpy().reshape(n[2], n[1], n[0], 1)
+    ctx.step(Fh, dtau, dtau, rho)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        Fh.import_(Fpin_np, halo=0)
+        ctx.step(Fh, dtau, dtau, rho)
+        _export_into(rho, rho_np)
+        ctx.gather_kick(Fh, 0.0, want_max_v=True)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if pg is not None:
+        t = torch.tensor([t_e2e], device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": npart * world * args.e2e_steps / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": 3 * nsites * 4, "d2h_bytes_per_step": nsites * 4 + 8,
+           "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
+           "path": "lf2_field_import(F, host) + lf2_step + lf2_field_export(rho, host) + "
+                   "lf2_gather_kick(max_v)"}
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            ups, steps = cpu_baseline_port(args.cpu_seconds, procs=1)
+            cpu = {"value": ups, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"64^3 lattice, 262,144 uniform particles, {steps} steps of "
+                             "deposit+comm, updateVel CIC kick, move (CPU restatement of the "
+                             "reference, double, 1 thread)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (int64 fixed-point deposit)" if mode == L.DEPOSIT_FIXED64 else "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "lattice": n[0], "particles": npart,
+                       "distribution": w["dist"], "deposit": w["mode"],
+                       "step": "kick+drift+rebin+scalar deposit (lf2_step)",
+                       "l2": f"inputs larger than L2 ({step_ab / 1e9:.1f} GB per step)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": roofline, "step_roofline": step_roofline, "phase_ms": phase_ms,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
+            "gpu_launches": launches, "adjoint_forward_ratio": None,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def _export_into(field, out):
+    """lf2_field_export straight into a pinned host array."""
+    from latfield2_b200 import _lib
+    from latfield2_b200.core import _ptr
+    p, kind = _ptr(out)
+    _lib.check(field.ctx.h, _lib.load().lf2_field_export(field.ctx.h, field.h, p, 0, 4, 0, kind),
+               "export")
+
+
+if __name__ == "__main__":
+    main()

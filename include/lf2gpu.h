@@ -1,0 +1,198 @@
+/*
+ * lf2gpu.h -- C ABI of the B200 particle-mesh library (liblf2gpu.so).
+ *
+ * This is the boundary that replaces the reference's header-only particle
+ * path (particles/LATfield2_Particles.hpp, particles/projections.hpp,
+ * LATfield2_Field_decl.hpp).  Plain C types only: pointers, sizes, status
+ * codes.  The C++ compatibility layer (include/LATfield2.hpp) and the Python
+ * package (latfield2_b200) are both written on top of these functions.
+ *
+ * Conventions
+ *  - Every function returns an lf2_status: 0 on success, < 0 on failure;
+ *    lf2_last_error() gives the message.  Nothing exits or throws across the
+ *    boundary (the reference exit()s, throws 1 or calls MPI_Abort).
+ *  - The context owns all device memory it allocates.  Host pointers passed
+ *    in are only borrowed for the duration of the call.
+ *  - Work is stream-ordered on the context's stream.  Calls that return a
+ *    host value (counts, max |v|, conservation sums, flags) synchronise it.
+ *  - ptr_kind tells whether an array argument lives on the host
+ *    (LF2_PTR_HOST) or on the context's device (LF2_PTR_DEVICE).
+ *  - Lattice geometry: n[3] sites per dim, periodic, lattice resolution
+ *    res = box[i] / n[i] equal in every dim (particles_tools.hpp:6-19).
+ *    Cell index c = x + n0*(y + n1*z) (site order, LATfield2_Site.hpp:55-76).
+ *  - Particle state on the device: cell (int), in-cell offset in cell units
+ *    (FP32, [0,1)), velocity in box units per time (FP32), optional FP32
+ *    mass, optional int64 ID.  Positions in box units are
+ *    pos = (coord + off) * res.
+ *  - Fields on the device: FP32, component-major, no halo, periodic:
+ *    data[c * n0*n1*n2 + cell].  lf2_field_export/import convert to and from
+ *    the reference layout (halo'd, components interleaved, float or double).
+ */
+#ifndef LF2GPU_H
+#define LF2GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lf2_ctx lf2_ctx;
+typedef struct lf2_field_s* lf2_field;
+typedef int lf2_status;
+
+#define LF2_OK 0
+#define LF2_ERR_ARG (-1)         /* invalid argument */
+#define LF2_ERR_CUDA (-2)        /* CUDA runtime error */
+#define LF2_ERR_STATE (-3)       /* a kernel raised an error flag */
+#define LF2_ERR_NOMEM (-4)       /* device allocation failed */
+#define LF2_ERR_UNSUPPORTED (-5) /* combination not provided */
+
+#define LF2_DEPOSIT_FP32 0    /* FP32 shared-memory accumulation */
+#define LF2_DEPOSIT_FIXED64 1 /* int64 fixed point, 2^-32 of a unit mass */
+
+#define LF2_PTR_HOST 0
+#define LF2_PTR_DEVICE 1
+
+/* Device error bits returned by lf2_get_flags. */
+#define LF2_FLAG_NONFINITE 0x1u      /* NaN/Inf offset or velocity met */
+#define LF2_FLAG_BAD_CELL 0x2u       /* cell/offset out of range on load */
+#define LF2_FLAG_MASS_RANGE 0x4u     /* relative mass outside [0,64) (fixed) */
+#define LF2_FLAG_REPACK 0x8u         /* informational: store was repacked */
+#define LF2_FLAG_CAPACITY 0x10u      /* repack did not fit: state lost */
+#define LF2_FLAG_FIXED_OVERFLOW 0x20u /* fixed-point vertex sum overflowed */
+
+/* ------------------------------------------------------------------ context
+ * Replaces Lattice(3, n, halo) + Particles::initialize(info, type, &lat_part,
+ * boxSize) (LATfield2_Lattice.hpp:27-223, LATfield2_Particles.hpp:358-428):
+ * geometry, resolution check (get_lattice_resolution, particles_tools.hpp:6-19)
+ * and the deposit mode.  stream may be NULL (default stream) or a
+ * cudaStream_t. */
+lf2_status lf2_create(lf2_ctx** out, int device, const int n[3],
+                      const double box[3], int deposit_mode, void* stream);
+lf2_status lf2_destroy(lf2_ctx* ctx);
+const char* lf2_last_error(const lf2_ctx* ctx);
+lf2_status lf2_set_stream(lf2_ctx* ctx, void* stream);
+/* Waits for the context's stream and turns raised device flags into
+ * LF2_ERR_STATE. */
+lf2_status lf2_synchronize(lf2_ctx* ctx);
+/* Reads (and with clear != 0, clears) the device error bits. */
+lf2_status lf2_get_flags(lf2_ctx* ctx, uint32_t* flags, int clear);
+
+/* --------------------------------------------------------------- particles
+ * Replaces the addParticle_global loop (LATfield2_Particles.hpp:500-540):
+ * bulk upload of n particles in any order, binned on the device.  cell[i] in
+ * [0, n0*n1*n2); off3/vel3 are AoS (3 per particle).  mass may be NULL
+ * (global mass `global_mass`, the part_info mass, GLOBAL_MASS) or hold one
+ * FP32 mass per particle (INDIVIDUAL_MASS, :400-425).  id may be NULL (no
+ * IDs carried). */
+lf2_status lf2_particles_set(lf2_ctx* ctx, int64_t n, const int32_t* cell,
+                             const float* off3, const float* vel3,
+                             const float* mass, double global_mass,
+                             const int64_t* id, int ptr_kind);
+/* Same from positions in box units (part.pos, LATfield2_particle_simple.hpp:
+ * 40-45), as float (real_bytes 4) or double (8); the cell is
+ * floor(pos/res) mod n (getPartCoord, LATfield2_Particles.hpp:463-467).
+ * Host pointers only. */
+lf2_status lf2_particles_set_pos(lf2_ctx* ctx, int64_t n, const void* pos3,
+                                 const void* vel3, int real_bytes,
+                                 const float* mass, double global_mass,
+                                 const int64_t* id);
+/* Particles::numParticles (LATfield2_Particles.hpp:316-320). */
+lf2_status lf2_particles_count(lf2_ctx* ctx, int64_t* n);
+/* Downloads the particles in storage order (brick by brick).  Any output
+ * pointer may be NULL; mass and id must be NULL when not carried. */
+lf2_status lf2_particles_get(lf2_ctx* ctx, int32_t* cell, float* off3,
+                             float* vel3, float* mass, int64_t* id,
+                             int ptr_kind);
+/* Positions in box units as float or double (host pointers). */
+lf2_status lf2_particles_get_pos(lf2_ctx* ctx, void* pos3, void* vel3,
+                                 int real_bytes, int64_t* id);
+/* Number of particles in every cell (the size of each per-cell list). */
+lf2_status lf2_cell_counts(lf2_ctx* ctx, int32_t* counts, int ptr_kind);
+
+/* ------------------------------------------------------------------ fields
+ * Replaces Field<Real>(lattice, comps) / Field<Real>(lattice, 3, 3,
+ * symmetric) and alloc() (LATfield2_Field_decl.hpp:620-712).  A symmetric
+ * 3x3 field has 6 components in the order 00,01,02,11,12,22 (:772-788). */
+lf2_status lf2_field_create(lf2_ctx* ctx, int comps, lf2_field* out);
+/* A field over caller-owned device memory (comps * n0*n1*n2 FP32 values in
+ * the internal layout); lf2_field_destroy then releases only the handle. */
+lf2_status lf2_field_wrap(lf2_ctx* ctx, int comps, float* device_data,
+                          lf2_field* out);
+lf2_status lf2_field_destroy(lf2_ctx* ctx, lf2_field f);
+/* Device pointer of the field data (FP32, comps * n0*n1*n2 values). */
+lf2_status lf2_field_device_ptr(lf2_ctx* ctx, lf2_field f, float** data);
+lf2_status lf2_field_components(lf2_ctx* ctx, lf2_field f, int* comps);
+/* projection_init (projections.hpp:31-34). */
+lf2_status lf2_field_zero(lf2_ctx* ctx, lf2_field f);
+/* Writes the field in the reference layout: halo `halo`, components
+ * interleaved, float (real_bytes 4) or double (8).  fill_halo != 0 fills the
+ * halo periodically (Field::updateHalo, LATfield2_Field_decl.hpp:889-935);
+ * otherwise the halo is zero. */
+lf2_status lf2_field_export(lf2_ctx* ctx, lf2_field f, void* dst, int halo,
+                            int real_bytes, int fill_halo, int ptr_kind);
+/* Reads a field given in the reference layout (halo values are ignored). */
+lf2_status lf2_field_import(lf2_ctx* ctx, lf2_field f, const void* src,
+                            int halo, int real_bytes, int ptr_kind);
+/* Field::updateHalo for a device array already in the reference layout. */
+lf2_status lf2_halo_fill(lf2_ctx* ctx, void* data, int comps, int halo,
+                         int real_bytes);
+
+/* -------------------------------------------------------------- projections
+ * Each call is projection_init + *_project + *_comm of the reference: the
+ * field is overwritten with the periodic deposit of the current particles
+ * (the upper-halo fold of *_comm is done inside the deposit).
+ *   scalar : scalarProjectionCIC_project/_comm (projections.hpp:75-300),
+ *            rho = sum m W / res^3, deposit mode of the context.
+ *   vector : vectorProjectionCICNGP_project/_comm (:421-681), momentum
+ *            m v / res^3, component i on the link x + e_i/2 (NGP along i,
+ *            CIC across).  FP32 mode.
+ *   tensor : symtensorProjectionCICNGP_project/_comm (:708-976),
+ *            T_ii = m v_i^2 at vertices (CIC), T_ij = m v_i v_j on the (i,j)
+ *            plaquette (CIC along the third dim).  FP32 mode. */
+lf2_status lf2_deposit_scalar(lf2_ctx* ctx, lf2_field rho);
+lf2_status lf2_deposit_vector_cicngp(lf2_ctx* ctx, lf2_field v);
+lf2_status lf2_deposit_symtensor_cicngp(lf2_ctx* ctx, lf2_field t);
+
+/* ---------------------------------------------------------- particle moves
+ * Particles::updateVel(cic_kick, dtau, &F, 1) (LATfield2_Particles.hpp:
+ * 752-893) with the library's CIC gather-kick: vel_c += dtau * sum_k w_k
+ * F_c(corner_k), F a 3-component field.  max_v (may be NULL; synchronises)
+ * receives the return value of updateVel, sqrt(max |v|^2). */
+lf2_status lf2_gather_kick(lf2_ctx* ctx, lf2_field F, double dtau,
+                           double* max_v);
+/* Particles::moveParticles(move_particles_simple, dtau)
+ * (LATfield2_Particles.hpp:1810-2803, move_function.hpp:15-32): drift
+ * pos += dtau * vel, periodic wrap and rebin into cells. */
+lf2_status lf2_drift_rebin(lf2_ctx* ctx, double dtau);
+/* One fused kick-drift-rebin pass (updateVel then moveParticles) followed,
+ * when rho is not NULL, by the scalar deposit of the new positions. */
+lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
+                    double dtau_drift, lf2_field rho);
+/* FP64 conservation sums over all particles: total mass, momentum sum m v
+ * and max |v| (cout_particle_velocity_stats, LATfield2_Particles.hpp:
+ * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */
+lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
+                            double* max_v);
+
+/* ------------------------------------------------------------- measurement
+ * Per-phase device time, measured with CUDA events recorded on the context's
+ * stream around each kernel (no extra synchronisation while running).
+ * Phases: 0 gather-kick/drift/rebin pass, 1 mover insertion and repack,
+ * 2 deposit tile pass, 3 deposit face fix-up, 4 other kernels.  The
+ * launch counter counts every kernel this library launched. */
+#define LF2_NPHASE 5
+lf2_status lf2_profile_enable(lf2_ctx* ctx, int on);
+/* Synchronises; adds the milliseconds and launches of each phase since the
+ * previous read into ms[LF2_NPHASE] / launches[LF2_NPHASE] (either may be
+ * NULL) and resets the accumulators. */
+lf2_status lf2_profile_read(lf2_ctx* ctx, double* ms, int64_t* launches);
+/* Total kernel launches since the context was created. */
+lf2_status lf2_kernel_launches(lf2_ctx* ctx, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,9 @@
+"""latfield2_b200 -- B200 (sm_100a) particle-mesh path of LATfield2.
+
+CIC deposit (scalar, vector CIC-NGP, symmetric-tensor CIC-NGP), CIC gather
+with kick, drift and rebin of brick-binned particles, written as CUDA kernels
+behind the C ABI in include/lf2gpu.h.  `latfield2_b200.particles` mirrors the
+reference's Particles / Field / projection interface on top of that ABI.
+"""
+from ._lib import (DEPOSIT_FIXED64, DEPOSIT_FP32, LF2Error, library_path, load)  # noqa: F401
+from .core import Context, FieldHandle  # noqa: F401

@@ -1,0 +1,110 @@
+"""ctypes binding of liblf2gpu.so (the C ABI in include/lf2gpu.h).
+
+The library is loaded from this package directory.  If it is missing it is
+built with nvcc (latfield2_b200/build.py); if that is impossible the import
+fails loudly.  There is no CPU fallback: every call runs the CUDA kernels.
+"""
+import ctypes
+import os
+
+from . import build as _build
+
+LF2_OK = 0
+LF2_ERR_ARG = -1
+LF2_ERR_CUDA = -2
+LF2_ERR_STATE = -3
+LF2_ERR_NOMEM = -4
+LF2_ERR_UNSUPPORTED = -5
+
+DEPOSIT_FP32 = 0
+DEPOSIT_FIXED64 = 1
+PTR_HOST = 0
+PTR_DEVICE = 1
+
+FLAG_NONFINITE = 0x1
+FLAG_BAD_CELL = 0x2
+FLAG_MASS_RANGE = 0x4
+FLAG_REPACK = 0x8
+FLAG_CAPACITY = 0x10
+FLAG_FIXED_OVERFLOW = 0x20
+
+c_void_p = ctypes.c_void_p
+c_int = ctypes.c_int
+c_i64 = ctypes.c_int64
+c_double = ctypes.c_double
+P = ctypes.POINTER
+
+# name -> argtypes (restype is always lf2_status / int unless listed below)
+SIGNATURES = {
+    "lf2_create": [P(c_void_p), c_int, P(c_int), P(c_double), c_int, c_void_p],
+    "lf2_destroy": [c_void_p],
+    "lf2_last_error": [c_void_p],
+    "lf2_set_stream": [c_void_p, c_void_p],
+    "lf2_synchronize": [c_void_p],
+    "lf2_get_flags": [c_void_p, P(ctypes.c_uint32), c_int],
+    "lf2_particles_set": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                          c_void_p, c_int],
+    "lf2_particles_set_pos": [c_void_p, c_i64, c_void_p, c_void_p, c_int, c_void_p, c_double,
+                              c_void_p],
+    "lf2_particles_count": [c_void_p, P(c_i64)],
+    "lf2_particles_get": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int],
+    "lf2_particles_get_pos": [c_void_p, c_void_p, c_void_p, c_int, c_void_p],
+    "lf2_cell_counts": [c_void_p, c_void_p, c_int],
+    "lf2_field_create": [c_void_p, c_int, P(c_void_p)],
+    "lf2_field_wrap": [c_void_p, c_int, c_void_p, P(c_void_p)],
+    "lf2_field_destroy": [c_void_p, c_void_p],
+    "lf2_field_device_ptr": [c_void_p, c_void_p, P(c_void_p)],
+    "lf2_field_components": [c_void_p, c_void_p, P(c_int)],
+    "lf2_field_zero": [c_void_p, c_void_p],
+    "lf2_field_export": [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int],
+    "lf2_field_import": [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int],
+    "lf2_halo_fill": [c_void_p, c_void_p, c_int, c_int, c_int],
+    "lf2_deposit_scalar": [c_void_p, c_void_p],
+    "lf2_deposit_vector_cicngp": [c_void_p, c_void_p],
+    "lf2_deposit_symtensor_cicngp": [c_void_p, c_void_p],
+    "lf2_gather_kick": [c_void_p, c_void_p, c_double, P(c_double)],
+    "lf2_drift_rebin": [c_void_p, c_double],
+    "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],
+    "lf2_conservation": [c_void_p, P(c_double), P(c_double), P(c_double)],
+    "lf2_profile_enable": [c_void_p, c_int],
+    "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
+    "lf2_kernel_launches": [c_void_p, P(c_i64)],
+}
+NPHASE = 5
+PHASES = ("move", "insert_repack", "deposit_tile", "deposit_fixup", "other")
+RESTYPES = {"lf2_last_error": ctypes.c_char_p}
+
+_LIB = None
+
+
+def library_path():
+    return _build.LIB
+
+
+def load():
+    """Returns the loaded CDLL, building it first when it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = _build.LIB
+    if not os.path.exists(path):
+        _build.build()
+    lib = ctypes.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = RESTYPES.get(name, c_int)
+    _LIB = lib
+    return lib
+
+
+class LF2Error(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"lf2 status {status}: {message}")
+        self.status = status
+
+
+def check(ctx, status, what=""):
+    if status != LF2_OK:
+        msg = load().lf2_last_error(ctx) if ctx else b""
+        raise LF2Error(status, (what + ": " if what else "") + (msg or b"").decode())

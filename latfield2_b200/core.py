@@ -1,0 +1,245 @@
+"""Thin object wrapper over the C ABI (include/lf2gpu.h).
+
+`Context` owns one lf2_ctx: the lattice geometry, the device particle store
+and the deposit mode.  Arrays are numpy (host) or torch CUDA tensors
+(device); the pointer kind is chosen from the argument type.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+_c = ctypes
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    if x is None:
+        return None, _lib.PTR_HOST
+    if _is_torch(x):
+        if not x.is_cuda:
+            raise ValueError("torch tensors passed to lf2 must be CUDA tensors")
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return _c.c_void_p(x.data_ptr()), _lib.PTR_DEVICE
+    if not x.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return _c.c_void_p(x.ctypes.data), _lib.PTR_HOST
+
+
+def _same_kind(*arrs):
+    kinds = {(_is_torch(a)) for a in arrs if a is not None}
+    if len(kinds) > 1:
+        raise ValueError("mix of host and device arrays in one call")
+    return _lib.PTR_DEVICE if kinds == {True} else _lib.PTR_HOST
+
+
+class FieldHandle:
+    """A device field (FP32, component-major, no halo) owned by the context or
+    wrapping a caller's CUDA tensor."""
+
+    def __init__(self, ctx, comps, tensor=None):
+        self.ctx = ctx
+        self.comps = comps
+        self.tensor = tensor
+        h = _c.c_void_p()
+        lib = _lib.load()
+        if tensor is None:
+            _lib.check(ctx.h, lib.lf2_field_create(ctx.h, comps, _c.byref(h)), "field_create")
+        else:
+            if tensor.dtype.itemsize != 4 or tensor.numel() != comps * ctx.nsites:
+                raise ValueError("tensor must hold comps * nsites float32 values")
+            _lib.check(ctx.h, lib.lf2_field_wrap(ctx.h, comps, _c.c_void_p(tensor.data_ptr()),
+                                                 _c.byref(h)), "field_wrap")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            _lib.load().lf2_field_destroy(self.ctx.h, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def export(self, halo=0, dtype=np.float32, fill_halo=False):
+        """Reference layout: shape (n2+2h, n1+2h, n0+2h, comps)."""
+        n = self.ctx.n
+        out = np.empty((n[2] + 2 * halo, n[1] + 2 * halo, n[0] + 2 * halo, self.comps), dtype=dtype)
+        p, kind = _ptr(out)
+        _lib.check(self.ctx.h, _lib.load().lf2_field_export(
+            self.ctx.h, self.h, p, halo, out.itemsize, 1 if fill_halo else 0, kind), "export")
+        return out
+
+    def export_internal(self):
+        """Internal layout copy: shape (comps, n2, n1, n0), float32."""
+        return self.export(0, np.float32).transpose(3, 0, 1, 2).copy()
+
+    def import_(self, arr, halo=0):
+        p, kind = _ptr(arr)
+        _lib.check(self.ctx.h, _lib.load().lf2_field_import(
+            self.ctx.h, self.h, p, halo, arr.dtype.itemsize, kind), "import")
+
+    def zero(self):
+        _lib.check(self.ctx.h, _lib.load().lf2_field_zero(self.ctx.h, self.h), "zero")
+
+
+class Context:
+    def __init__(self, n, box=1.0, mode=_lib.DEPOSIT_FP32, device=0, stream=None):
+        if np.isscalar(n):
+            n = (int(n),) * 3
+        if np.isscalar(box):
+            box = tuple(float(box) * ni / n[0] for ni in n)
+        self.n = tuple(int(v) for v in n)
+        self.box = tuple(float(b) for b in box)
+        self.nsites = self.n[0] * self.n[1] * self.n[2]
+        self.res = self.box[0] / self.n[0]
+        self.mode = mode
+        lib = _lib.load()
+        h = _c.c_void_p()
+        na = (_c.c_int * 3)(*self.n)
+        ba = (_c.c_double * 3)(*self.box)
+        st = _c.c_void_p(stream) if stream is not None else None
+        s = lib.lf2_create(_c.byref(h), device, na, ba, mode, st)
+        if s != _lib.LF2_OK:
+            raise _lib.LF2Error(s, f"lf2_create(n={self.n}, box={self.box}, mode={mode})")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().lf2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status, what):
+        _lib.check(self.h, status, what)
+
+    def set_stream(self, stream):
+        self._check(_lib.load().lf2_set_stream(self.h, _c.c_void_p(stream)), "set_stream")
+
+    # ---------------------------------------------------------------- particles
+    def set_particles(self, cell, off, vel, mass=None, global_mass=0.0, ids=None):
+        kind = _same_kind(cell, off, vel, mass, ids)
+        n = int(cell.shape[0])
+        args = [_ptr(a)[0] for a in (cell, off, vel, mass)]
+        self._check(_lib.load().lf2_particles_set(
+            self.h, n, args[0], args[1], args[2], args[3], float(global_mass),
+            _ptr(ids)[0], kind), "particles_set")
+
+    def set_positions(self, pos, vel, mass=None, global_mass=0.0, ids=None):
+        pos = np.ascontiguousarray(pos)
+        vel = np.ascontiguousarray(vel, dtype=pos.dtype)
+        self._check(_lib.load().lf2_particles_set_pos(
+            self.h, int(pos.shape[0]), _ptr(pos)[0], _ptr(vel)[0], pos.itemsize,
+            _ptr(mass)[0], float(global_mass), _ptr(ids)[0]), "particles_set_pos")
+
+    def count(self):
+        n = _c.c_int64()
+        self._check(_lib.load().lf2_particles_count(self.h, _c.byref(n)), "count")
+        return n.value
+
+    def get_particles(self, mass=False, ids=False):
+        n = self.count()
+        cell = np.empty(n, np.int32)
+        off = np.empty((n, 3), np.float32)
+        vel = np.empty((n, 3), np.float32)
+        m = np.empty(n, np.float32) if mass else None
+        i = np.empty(n, np.int64) if ids else None
+        self._check(_lib.load().lf2_particles_get(
+            self.h, _ptr(cell)[0], _ptr(off)[0], _ptr(vel)[0], _ptr(m)[0], _ptr(i)[0],
+            _lib.PTR_HOST), "particles_get")
+        out = {"cell": cell, "off": off, "vel": vel}
+        if mass:
+            out["mass"] = m
+        if ids:
+            out["id"] = i
+        return out
+
+    def get_positions(self, dtype=np.float64, ids=False):
+        n = self.count()
+        pos = np.empty((n, 3), dtype)
+        vel = np.empty((n, 3), dtype)
+        i = np.empty(n, np.int64) if ids else None
+        self._check(_lib.load().lf2_particles_get_pos(
+            self.h, _ptr(pos)[0], _ptr(vel)[0], pos.itemsize, _ptr(i)[0]), "particles_get_pos")
+        return (pos, vel, i) if ids else (pos, vel)
+
+    def cell_counts(self):
+        out = np.empty(self.nsites, np.int32)
+        self._check(_lib.load().lf2_cell_counts(self.h, _ptr(out)[0], _lib.PTR_HOST), "cell_counts")
+        return out
+
+    # ------------------------------------------------------------------- fields
+    def field(self, comps, tensor=None):
+        return FieldHandle(self, comps, tensor)
+
+    def halo_fill(self, tensor, comps, halo):
+        self._check(_lib.load().lf2_halo_fill(self.h, _c.c_void_p(tensor.data_ptr()), comps, halo,
+                                              tensor.element_size()), "halo_fill")
+
+    # --------------------------------------------------------------- operations
+    def deposit_scalar(self, f):
+        self._check(_lib.load().lf2_deposit_scalar(self.h, f.h), "deposit_scalar")
+
+    def deposit_vector(self, f):
+        self._check(_lib.load().lf2_deposit_vector_cicngp(self.h, f.h), "deposit_vector")
+
+    def deposit_symtensor(self, f):
+        self._check(_lib.load().lf2_deposit_symtensor_cicngp(self.h, f.h), "deposit_symtensor")
+
+    def gather_kick(self, F, dtau, want_max_v=False):
+        mv = _c.c_double()
+        self._check(_lib.load().lf2_gather_kick(self.h, F.h, float(dtau),
+                                                _c.byref(mv) if want_max_v else None),
+                    "gather_kick")
+        return mv.value if want_max_v else None
+
+    def drift_rebin(self, dtau):
+        self._check(_lib.load().lf2_drift_rebin(self.h, float(dtau)), "drift_rebin")
+
+    def step(self, F, dtau_kick, dtau_drift, rho=None):
+        self._check(_lib.load().lf2_step(self.h, F.h, float(dtau_kick), float(dtau_drift),
+                                         rho.h if rho is not None else None), "step")
+
+    def conservation(self):
+        m = _c.c_double()
+        mom = (_c.c_double * 3)()
+        mv = _c.c_double()
+        self._check(_lib.load().lf2_conservation(self.h, _c.byref(m), mom, _c.byref(mv)),
+                    "conservation")
+        return m.value, np.array(list(mom)), mv.value
+
+    def flags(self, clear=False):
+        f = _c.c_uint32()
+        self._check(_lib.load().lf2_get_flags(self.h, _c.byref(f), 1 if clear else 0), "flags")
+        return f.value
+
+    def synchronize(self):
+        self._check(_lib.load().lf2_synchronize(self.h), "synchronize")
+
+    # ------------------------------------------------------------- measurement
+    def profile(self, on=True):
+        self._check(_lib.load().lf2_profile_enable(self.h, 1 if on else 0), "profile_enable")
+
+    def profile_read(self):
+        """{phase: (milliseconds, launches)} since the previous read."""
+        ms = (_c.c_double * _lib.NPHASE)()
+        ln = (_c.c_int64 * _lib.NPHASE)()
+        self._check(_lib.load().lf2_profile_read(self.h, ms, ln), "profile_read")
+        return {p: (ms[i], ln[i]) for i, p in enumerate(_lib.PHASES)}
+
+    def kernel_launches(self):
+        n = _c.c_int64()
+        self._check(_lib.load().lf2_kernel_launches(self.h, _c.byref(n)), "kernel_launches")
+        return n.value

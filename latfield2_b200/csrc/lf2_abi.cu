@@ -1,0 +1,767 @@
+// lf2_abi.cu -- implementation of the C ABI declared in include/lf2gpu.h.
+//
+// Host-side orchestration only: argument checks, device allocation owned by
+// the context, host<->device staging of borrowed host arrays, and the kernel
+// sequences of each call.  All kernels live in lf2_store.cu, lf2_move.cu,
+// lf2_deposit.cu and lf2_field.cu.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lf2_internal.h"
+
+namespace lf2 {
+size_t deposit_spill_slots(const lf2_ctx* c, int comps);
+}
+
+using namespace lf2;
+
+namespace {
+
+lf2_status fail(lf2_ctx* c, lf2_status code, const std::string& msg)
+{
+  if (c) c->err = msg;
+  return code;
+}
+
+#define LF2_CUDA(c, expr)                                                              \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail((c), LF2_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LF2_TRY(expr)                    \
+  do {                                   \
+    lf2_status s_ = (expr);              \
+    if (s_ != LF2_OK) return s_;         \
+  } while (0)
+
+// Stream-ordered device scratch, released on the context's stream.
+struct Scratch {
+  lf2_ctx* c;
+  void* p = nullptr;
+  Scratch(lf2_ctx* ctx) : c(ctx) {}
+  cudaError_t alloc(size_t bytes)
+  {
+    return cudaMallocAsync(&p, bytes > 0 ? bytes : 16, c->stream);
+  }
+  ~Scratch()
+  {
+    if (p) cudaFreeAsync(p, c->stream);
+  }
+};
+
+// Brackets one phase of a call with CUDA events on the context's stream when
+// profiling is on, and attributes the kernels launched inside it.
+cudaEvent_t take_event(lf2_ctx* c)
+{
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct PhaseScope {
+  lf2_ctx* c;
+  int phase;
+  int64_t l0;
+  cudaEvent_t e0 = nullptr;
+  PhaseScope(lf2_ctx* ctx, int ph) : c(ctx), phase(ph), l0(ctx->launches)
+  {
+    if (c->profiling) {
+      e0 = take_event(c);
+      if (e0) cudaEventRecord(e0, c->stream);
+    }
+  }
+  ~PhaseScope()
+  {
+    c->phase_launches[phase] += c->launches - l0;
+    if (e0) {
+      cudaEvent_t e1 = take_event(c);
+      if (e1) {
+        cudaEventRecord(e1, c->stream);
+        c->pending[phase].push_back({e0, e1});
+      }
+    }
+  }
+};
+
+enum { PH_MOVE = 0, PH_INSERT = 1, PH_DEPOSIT = 2, PH_FIXUP = 3, PH_OTHER = 4 };
+
+int bits_for(int n)
+{
+  int b = 0;
+  while ((1ll << b) < n) b++;
+  return b;
+}
+
+void free_parts(PartArrays& a)
+{
+  cudaFree(a.key);
+  cudaFree(a.ox);
+  cudaFree(a.oy);
+  cudaFree(a.oz);
+  cudaFree(a.vx);
+  cudaFree(a.vy);
+  cudaFree(a.vz);
+  cudaFree(a.mass);
+  cudaFree(a.id);
+  a = PartArrays();
+}
+
+cudaError_t alloc_parts(PartArrays& a, int64_t slots, bool mass, bool id)
+{
+  const size_t n = (size_t)(slots > 0 ? slots : 1);
+  cudaError_t e;
+  if ((e = cudaMalloc(&a.key, n * sizeof(uint32_t))) != cudaSuccess) return e;
+  float** fs[6] = {&a.ox, &a.oy, &a.oz, &a.vx, &a.vy, &a.vz};
+  for (auto f : fs)
+    if ((e = cudaMalloc(f, n * sizeof(float))) != cudaSuccess) return e;
+  if (mass && (e = cudaMalloc(&a.mass, n * sizeof(float))) != cudaSuccess) return e;
+  if (id && (e = cudaMalloc(&a.id, n * sizeof(int64_t))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+lf2_status check_flags(lf2_ctx* c)
+{
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_flags, c->flags, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  const uint32_t f = *c->h_flags & ~(uint32_t)ERR_REPACK;
+  if (f) {
+    char buf[160];
+    snprintf(buf, sizeof buf,
+             "device error flags 0x%x (1 non-finite state, 2 bad cell/offset, 4 mass range, "
+             "16 capacity, 32 fixed overflow)",
+             f);
+    return fail(c, LF2_ERR_STATE, buf);
+  }
+  return LF2_OK;
+}
+
+lf2_status ensure_spill(lf2_ctx* c, int comps)
+{
+  const size_t need = deposit_spill_slots(c, comps);
+  if (need <= c->spill_slots) return LF2_OK;
+  if (c->spill) {
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(c->spill);
+    c->spill = nullptr;
+    c->spill_slots = 0;
+  }
+  if (cudaMalloc(&c->spill, need * sizeof(uint64_t)) != cudaSuccess)
+    return fail(c, LF2_ERR_NOMEM, "cannot allocate the deposit shell store");
+  c->spill_slots = need;
+  return LF2_OK;
+}
+
+bool valid_field(lf2_ctx* c, lf2_field f) { return c && f && f->data; }
+
+// Common load path: inputs already on the device.
+lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                       const float* vel3, const float* mass, double gmass, const int64_t* id)
+{
+  const bool has_mass = mass != nullptr, has_id = id != nullptr;
+  const int64_t nb = c->g.nbricks;
+  const int64_t need = n + (n >> 3) + 32 * nb + 1024;
+  if (need > c->capacity || has_mass != c->has_mass || has_id != c->has_id ||
+      n > c->mov_capacity) {
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_parts(c->cur);
+    free_parts(c->alt);
+    free_parts(c->mov);
+    cudaFree(c->mov_placed);
+    c->mov_placed = nullptr;
+    c->capacity = c->mov_capacity = 0;
+    if (alloc_parts(c->cur, need, has_mass, has_id) != cudaSuccess ||
+        alloc_parts(c->alt, need, has_mass, has_id) != cudaSuccess ||
+        alloc_parts(c->mov, n, has_mass, has_id) != cudaSuccess ||
+        cudaMalloc(&c->mov_placed, sizeof(int32_t) * (size_t)(n > 0 ? n : 1)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(c, LF2_ERR_NOMEM, "cannot allocate the particle store");
+    }
+    c->capacity = need;
+    c->mov_capacity = n;
+  }
+  c->has_mass = has_mass;
+  c->has_id = has_id;
+  c->gmass = gmass;
+  LF2_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream));
+  LF2_CUDA(c, cudaMemsetAsync(c->count, 0, sizeof(int32_t) * nb, c->stream));
+  LF2_CUDA(c, cudaMemsetAsync(c->fill, 0, sizeof(int32_t) * nb, c->stream));
+  LF2_CUDA(c, launch_load_count(c, n, cell, off3));
+  LF2_CUDA(c, launch_caps_and_scan(c, c->count, c->cap, c->seg_start, nullptr));
+  LF2_CUDA(c, launch_load_scatter(c, n, cell, off3, vel3, mass, id));
+  LF2_CUDA(c, cudaMemcpyAsync(c->count, c->fill, sizeof(int32_t) * nb, cudaMemcpyDeviceToDevice,
+                              c->stream));
+  c->np = n;
+  if (check_flags(c) != LF2_OK) {
+    c->np = 0;
+    LF2_CUDA(c, cudaMemsetAsync(c->count, 0, sizeof(int32_t) * nb, c->stream));
+    return fail(c, LF2_ERR_ARG, "particles_set: a cell index or offset is out of range");
+  }
+  c->m_unit = gmass > 0 ? gmass : 1.0;
+  if (has_mass) {
+    LF2_CUDA(c, launch_conservation(c));
+    LF2_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats, sizeof(double) * 8, cudaMemcpyDeviceToHost,
+                                c->stream));
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->m_unit = (n > 0 && c->h_stats[1] > 0) ? c->h_stats[1] / (double)n : 1.0;
+  }
+  return LF2_OK;
+}
+
+template <typename T>
+lf2_status stage_in(lf2_ctx* c, Scratch& s, const T* src, size_t count, int ptr_kind, const T** out)
+{
+  if (!src) {
+    *out = nullptr;
+    return LF2_OK;
+  }
+  if (ptr_kind == LF2_PTR_DEVICE) {
+    *out = src;
+    return LF2_OK;
+  }
+  LF2_CUDA(c, s.alloc(count * sizeof(T)));
+  LF2_CUDA(c, cudaMemcpyAsync(s.p, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  *out = (const T*)s.p;
+  return LF2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double box[3],
+                      int deposit_mode, void* stream)
+{
+  if (!out || !n || !box) return LF2_ERR_ARG;
+  *out = nullptr;
+  for (int d = 0; d < 3; d++)
+    if (n[d] < 1 || !(box[d] > 0)) return LF2_ERR_ARG;
+  if (deposit_mode != LF2_DEPOSIT_FP32 && deposit_mode != LF2_DEPOSIT_FIXED64) return LF2_ERR_ARG;
+  // get_lattice_resolution (particles_tools.hpp:6-19) demands equal
+  // resolutions; equal here means to 1e-12 relative, so that box = res * n
+  // computed in floating point is accepted for any n.
+  const double res = box[0] / n[0];
+  if (std::fabs(box[1] / n[1] - res) > 1e-12 * res || std::fabs(box[2] / n[2] - res) > 1e-12 * res)
+    return LF2_ERR_ARG;
+  const int bits = bits_for(n[0]) + bits_for(n[1]) + bits_for(n[2]);
+  const int64_t nsites = (int64_t)n[0] * n[1] * n[2];
+  if (bits > 32 || nsites >= (1ll << 31)) return LF2_ERR_UNSUPPORTED;
+
+  lf2_ctx* c = new (std::nothrow) lf2_ctx();
+  if (!c) return LF2_ERR_NOMEM;
+  c->device = device;
+  c->stream = (cudaStream_t)stream;
+  c->mode = deposit_mode;
+  c->res = res;
+  for (int d = 0; d < 3; d++) c->box[d] = box[d];
+  Geom& g = c->g;
+  int shift = 0;
+  for (int d = 0; d < 3; d++) {
+    g.n[d] = n[d];
+    g.nb[d] = (n[d] + BRICK - 1) / BRICK;
+    g.shift[d] = shift;
+    const int b = bits_for(n[d]);
+    g.mask[d] = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+    shift += b;
+  }
+  g.nsites = nsites;
+  g.nbricks = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+  const int64_t nb = g.nbricks;
+
+  bool ok = cudaSetDevice(device) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->seg_start, sizeof(int64_t) * (nb + 1)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->seg_start_alt, sizeof(int64_t) * (nb + 1)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->count, sizeof(int32_t) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->cap, sizeof(int32_t) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->cap_alt, sizeof(int32_t) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->fill, sizeof(int32_t) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->brick_maxv2, sizeof(float) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->brick_sums, sizeof(double) * 5 * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->stats, sizeof(double) * 8) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->repack, sizeof(int32_t)) == cudaSuccess;
+  ok = ok && cudaMallocHost(&c->h_stats, sizeof(double) * 8) == cudaSuccess;
+  ok = ok && cudaMallocHost(&c->h_flags, sizeof(uint32_t)) == cudaSuccess;
+  ok = ok && cudaMallocHost(&c->h_i64, sizeof(int64_t) * 4) == cudaSuccess;
+  if (ok) {
+    ok = cudaMemsetAsync(c->count, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->cap, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->seg_start, 0, sizeof(int64_t) * (nb + 1), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->repack, 0, sizeof(int32_t), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
+         cudaStreamSynchronize(c->stream) == cudaSuccess;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    lf2_destroy(c);
+    return LF2_ERR_CUDA;
+  }
+  *out = c;
+  return LF2_OK;
+}
+
+lf2_status lf2_destroy(lf2_ctx* c)
+{
+  if (!c) return LF2_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  free_parts(c->cur);
+  free_parts(c->alt);
+  free_parts(c->mov);
+  cudaFree(c->mov_placed);
+  cudaFree(c->seg_start);
+  cudaFree(c->seg_start_alt);
+  cudaFree(c->count);
+  cudaFree(c->cap);
+  cudaFree(c->cap_alt);
+  cudaFree(c->fill);
+  cudaFree(c->brick_maxv2);
+  cudaFree(c->brick_sums);
+  cudaFree(c->stats);
+  cudaFree(c->mov_count);
+  cudaFree(c->flags);
+  cudaFree(c->repack);
+  cudaFree(c->spill);
+  cudaFreeHost(c->h_stats);
+  cudaFreeHost(c->h_flags);
+  cudaFreeHost(c->h_i64);
+  for (auto& v : c->pending)
+    for (auto& pr : v) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (auto e : c->event_pool) cudaEventDestroy(e);
+  delete c;
+  return LF2_OK;
+}
+
+const char* lf2_last_error(const lf2_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+lf2_status lf2_set_stream(lf2_ctx* c, void* stream)
+{
+  if (!c) return LF2_ERR_ARG;
+  c->stream = (cudaStream_t)stream;
+  return LF2_OK;
+}
+
+lf2_status lf2_synchronize(lf2_ctx* c)
+{
+  if (!c) return LF2_ERR_ARG;
+  return check_flags(c);
+}
+
+lf2_status lf2_get_flags(lf2_ctx* c, uint32_t* flags, int clear)
+{
+  if (!c || !flags) return LF2_ERR_ARG;
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_flags, c->flags, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  *flags = *c->h_flags;
+  if (clear) LF2_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream));
+  return LF2_OK;
+}
+
+lf2_status lf2_particles_set(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                             const float* vel3, const float* mass, double global_mass,
+                             const int64_t* id, int ptr_kind)
+{
+  if (!c || n < 0 || (n > 0 && (!cell || !off3 || !vel3))) return LF2_ERR_ARG;
+  if (n >= (1ll << 31)) return fail(c, LF2_ERR_UNSUPPORTED, "more than 2^31-1 particles");
+  if (!mass && !(global_mass > 0))
+    return fail(c, LF2_ERR_ARG, "particles need a mass (global or per particle)");
+  Scratch s1(c), s2(c), s3(c), s4(c), s5(c);
+  const int32_t* dc;
+  const float *doff, *dvel, *dmass;
+  const int64_t* did;
+  LF2_TRY(stage_in(c, s1, cell, (size_t)n, ptr_kind, &dc));
+  LF2_TRY(stage_in(c, s2, off3, (size_t)n * 3, ptr_kind, &doff));
+  LF2_TRY(stage_in(c, s3, vel3, (size_t)n * 3, ptr_kind, &dvel));
+  LF2_TRY(stage_in(c, s4, mass, (size_t)n, ptr_kind, &dmass));
+  LF2_TRY(stage_in(c, s5, id, (size_t)n, ptr_kind, &did));
+  return load_device(c, n, dc, doff, dvel, dmass, global_mass, did);
+}
+
+lf2_status lf2_particles_set_pos(lf2_ctx* c, int64_t n, const void* pos3, const void* vel3,
+                                 int real_bytes, const float* mass, double global_mass,
+                                 const int64_t* id)
+{
+  if (!c || n < 0 || (n > 0 && (!pos3 || !vel3)) || (real_bytes != 4 && real_bytes != 8))
+    return LF2_ERR_ARG;
+  if (n >= (1ll << 31)) return fail(c, LF2_ERR_UNSUPPORTED, "more than 2^31-1 particles");
+  if (!mass && !(global_mass > 0))
+    return fail(c, LF2_ERR_ARG, "particles need a mass (global or per particle)");
+  std::vector<float> vel((size_t)n * 3);
+  for (size_t i = 0; i < vel.size(); i++)
+    vel[i] = real_bytes == 8 ? (float)((const double*)vel3)[i] : ((const float*)vel3)[i];
+  Scratch sp(c), sc(c), so(c), sv(c), sm(c), si(c);
+  LF2_CUDA(c, sp.alloc((size_t)n * 3 * real_bytes));
+  LF2_CUDA(c, sc.alloc((size_t)n * sizeof(int32_t)));
+  LF2_CUDA(c, so.alloc((size_t)n * 3 * sizeof(float)));
+  LF2_CUDA(c, cudaMemcpyAsync(sp.p, pos3, (size_t)n * 3 * real_bytes, cudaMemcpyHostToDevice,
+                              c->stream));
+  LF2_CUDA(c, launch_pos_to_state(c, n, sp.p, real_bytes, (int32_t*)sc.p, (float*)so.p));
+  const float* dvel;
+  const float* dmass;
+  const int64_t* did;
+  LF2_TRY(stage_in(c, sv, vel.data(), vel.size(), LF2_PTR_HOST, &dvel));
+  LF2_TRY(stage_in(c, sm, mass, (size_t)n, LF2_PTR_HOST, &dmass));
+  LF2_TRY(stage_in(c, si, id, (size_t)n, LF2_PTR_HOST, &did));
+  return load_device(c, n, (const int32_t*)sc.p, (const float*)so.p, dvel, dmass, global_mass,
+                     did);
+}
+
+lf2_status lf2_particles_count(lf2_ctx* c, int64_t* n)
+{
+  if (!c || !n) return LF2_ERR_ARG;
+  *n = c->np;
+  return LF2_OK;
+}
+
+lf2_status lf2_particles_get(lf2_ctx* c, int32_t* cell, float* off3, float* vel3, float* mass,
+                             int64_t* id, int ptr_kind)
+{
+  if (!c) return LF2_ERR_ARG;
+  if ((mass && !c->has_mass) || (id && !c->has_id))
+    return fail(c, LF2_ERR_ARG, "mass/id requested but not carried");
+  const int64_t n = c->np;
+  Scratch st(c), sc(c), so(c), sv(c), sm(c), si(c);
+  LF2_CUDA(c, st.alloc(sizeof(int64_t) * (c->g.nbricks + 1)));
+  LF2_CUDA(c, launch_scan_counts(c, (int64_t*)st.p));
+  int32_t* dc = cell;
+  float *doff = off3, *dvel = vel3, *dmass = mass;
+  int64_t* did = id;
+  if (ptr_kind == LF2_PTR_HOST) {
+    if (cell) {
+      LF2_CUDA(c, sc.alloc(sizeof(int32_t) * n));
+      dc = (int32_t*)sc.p;
+    }
+    if (off3) {
+      LF2_CUDA(c, so.alloc(sizeof(float) * 3 * n));
+      doff = (float*)so.p;
+    }
+    if (vel3) {
+      LF2_CUDA(c, sv.alloc(sizeof(float) * 3 * n));
+      dvel = (float*)sv.p;
+    }
+    if (mass) {
+      LF2_CUDA(c, sm.alloc(sizeof(float) * n));
+      dmass = (float*)sm.p;
+    }
+    if (id) {
+      LF2_CUDA(c, si.alloc(sizeof(int64_t) * n));
+      did = (int64_t*)si.p;
+    }
+  }
+  LF2_CUDA(c, launch_get(c, (int64_t*)st.p, dc, doff, dvel, dmass, did));
+  if (ptr_kind == LF2_PTR_HOST) {
+    const cudaMemcpyKind k = cudaMemcpyDeviceToHost;
+    if (cell) LF2_CUDA(c, cudaMemcpyAsync(cell, dc, sizeof(int32_t) * n, k, c->stream));
+    if (off3) LF2_CUDA(c, cudaMemcpyAsync(off3, doff, sizeof(float) * 3 * n, k, c->stream));
+    if (vel3) LF2_CUDA(c, cudaMemcpyAsync(vel3, dvel, sizeof(float) * 3 * n, k, c->stream));
+    if (mass) LF2_CUDA(c, cudaMemcpyAsync(mass, dmass, sizeof(float) * n, k, c->stream));
+    if (id) LF2_CUDA(c, cudaMemcpyAsync(id, did, sizeof(int64_t) * n, k, c->stream));
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_particles_get_pos(lf2_ctx* c, void* pos3, void* vel3, int real_bytes, int64_t* id)
+{
+  if (!c || (real_bytes != 4 && real_bytes != 8)) return LF2_ERR_ARG;
+  if (id && !c->has_id) return fail(c, LF2_ERR_ARG, "id requested but not carried");
+  const int64_t n = c->np;
+  Scratch st(c), sc(c), so(c), sv(c), sp(c), si(c);
+  LF2_CUDA(c, st.alloc(sizeof(int64_t) * (c->g.nbricks + 1)));
+  LF2_CUDA(c, sc.alloc(sizeof(int32_t) * n));
+  LF2_CUDA(c, so.alloc(sizeof(float) * 3 * n));
+  LF2_CUDA(c, sv.alloc(sizeof(float) * 3 * n));
+  LF2_CUDA(c, sp.alloc((size_t)real_bytes * 3 * n));
+  if (id) LF2_CUDA(c, si.alloc(sizeof(int64_t) * n));
+  LF2_CUDA(c, launch_scan_counts(c, (int64_t*)st.p));
+  LF2_CUDA(c, launch_get(c, (int64_t*)st.p, (int32_t*)sc.p, (float*)so.p, (float*)sv.p, nullptr,
+                         (int64_t*)si.p));
+  LF2_CUDA(c, launch_state_to_pos(c, n, (const int32_t*)sc.p, (const float*)so.p, sp.p, real_bytes));
+  std::vector<float> vel((size_t)n * 3);
+  if (pos3)
+    LF2_CUDA(c, cudaMemcpyAsync(pos3, sp.p, (size_t)real_bytes * 3 * n, cudaMemcpyDeviceToHost,
+                                c->stream));
+  LF2_CUDA(c, cudaMemcpyAsync(vel.data(), sv.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost,
+                              c->stream));
+  if (id) LF2_CUDA(c, cudaMemcpyAsync(id, si.p, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (vel3)
+    for (size_t i = 0; i < vel.size(); i++) {
+      if (real_bytes == 8) ((double*)vel3)[i] = vel[i];
+      else ((float*)vel3)[i] = vel[i];
+    }
+  return LF2_OK;
+}
+
+lf2_status lf2_cell_counts(lf2_ctx* c, int32_t* counts, int ptr_kind)
+{
+  if (!c || !counts) return LF2_ERR_ARG;
+  Scratch s(c);
+  int32_t* d = counts;
+  if (ptr_kind == LF2_PTR_HOST) {
+    LF2_CUDA(c, s.alloc(sizeof(int32_t) * c->g.nsites));
+    d = (int32_t*)s.p;
+  }
+  LF2_CUDA(c, launch_cell_counts(c, d));
+  if (ptr_kind == LF2_PTR_HOST) {
+    LF2_CUDA(c, cudaMemcpyAsync(counts, d, sizeof(int32_t) * c->g.nsites, cudaMemcpyDeviceToHost,
+                                c->stream));
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_field_create(lf2_ctx* c, int comps, lf2_field* out)
+{
+  if (!c || !out || comps < 1 || comps > 64) return LF2_ERR_ARG;
+  *out = nullptr;
+  lf2_field f = new (std::nothrow) lf2_field_s();
+  if (!f) return LF2_ERR_NOMEM;
+  f->comps = comps;
+  if (cudaMalloc(&f->data, sizeof(float) * comps * c->g.nsites) != cudaSuccess) {
+    cudaGetLastError();
+    delete f;
+    return fail(c, LF2_ERR_NOMEM, "cannot allocate field");
+  }
+  LF2_CUDA(c, cudaMemsetAsync(f->data, 0, sizeof(float) * comps * c->g.nsites, c->stream));
+  *out = f;
+  return LF2_OK;
+}
+
+lf2_status lf2_field_wrap(lf2_ctx* c, int comps, float* device_data, lf2_field* out)
+{
+  if (!c || !out || !device_data || comps < 1 || comps > 64) return LF2_ERR_ARG;
+  lf2_field f = new (std::nothrow) lf2_field_s();
+  if (!f) return LF2_ERR_NOMEM;
+  f->comps = comps;
+  f->data = device_data;
+  f->owned = false;
+  *out = f;
+  return LF2_OK;
+}
+
+lf2_status lf2_field_destroy(lf2_ctx* c, lf2_field f)
+{
+  if (!f) return LF2_OK;
+  if (f->owned) {
+    if (c) cudaStreamSynchronize(c->stream);
+    cudaFree(f->data);
+  }
+  delete f;
+  return LF2_OK;
+}
+
+lf2_status lf2_field_device_ptr(lf2_ctx* c, lf2_field f, float** data)
+{
+  if (!valid_field(c, f) || !data) return LF2_ERR_ARG;
+  *data = f->data;
+  return LF2_OK;
+}
+
+lf2_status lf2_field_components(lf2_ctx* c, lf2_field f, int* comps)
+{
+  if (!valid_field(c, f) || !comps) return LF2_ERR_ARG;
+  *comps = f->comps;
+  return LF2_OK;
+}
+
+lf2_status lf2_field_zero(lf2_ctx* c, lf2_field f)
+{
+  if (!valid_field(c, f)) return LF2_ERR_ARG;
+  LF2_CUDA(c, cudaMemsetAsync(f->data, 0, sizeof(float) * f->comps * c->g.nsites, c->stream));
+  return LF2_OK;
+}
+
+lf2_status lf2_field_export(lf2_ctx* c, lf2_field f, void* dst, int halo, int real_bytes,
+                            int fill_halo, int ptr_kind)
+{
+  if (!valid_field(c, f) || !dst || halo < 0 || (real_bytes != 4 && real_bytes != 8))
+    return LF2_ERR_ARG;
+  const size_t gross = (size_t)(c->g.n[0] + 2 * halo) * (c->g.n[1] + 2 * halo) *
+                       (c->g.n[2] + 2 * halo);
+  const size_t bytes = gross * f->comps * real_bytes;
+  Scratch s(c);
+  void* d = dst;
+  if (ptr_kind == LF2_PTR_HOST) {
+    LF2_CUDA(c, s.alloc(bytes));
+    d = s.p;
+  }
+  LF2_CUDA(c, launch_export(c, f->comps, f->data, d, halo, real_bytes, fill_halo));
+  if (ptr_kind == LF2_PTR_HOST) {
+    LF2_CUDA(c, cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_field_import(lf2_ctx* c, lf2_field f, const void* src, int halo, int real_bytes,
+                            int ptr_kind)
+{
+  if (!valid_field(c, f) || !src || halo < 0 || (real_bytes != 4 && real_bytes != 8))
+    return LF2_ERR_ARG;
+  const size_t gross = (size_t)(c->g.n[0] + 2 * halo) * (c->g.n[1] + 2 * halo) *
+                       (c->g.n[2] + 2 * halo);
+  const size_t bytes = gross * f->comps * real_bytes;
+  Scratch s(c);
+  const void* d = src;
+  if (ptr_kind == LF2_PTR_HOST) {
+    LF2_CUDA(c, s.alloc(bytes));
+    LF2_CUDA(c, cudaMemcpyAsync(s.p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    d = s.p;
+  }
+  LF2_CUDA(c, launch_import(c, f->comps, f->data, d, halo, real_bytes));
+  return LF2_OK;
+}
+
+lf2_status lf2_halo_fill(lf2_ctx* c, void* data, int comps, int halo, int real_bytes)
+{
+  if (!c || !data || comps < 1 || halo < 0 || (real_bytes != 4 && real_bytes != 8))
+    return LF2_ERR_ARG;
+  for (int d = 0; d < 3; d++)
+    if (halo > c->g.n[d]) return fail(c, LF2_ERR_ARG, "halo wider than the lattice");
+  LF2_CUDA(c, launch_halo_fill(c, data, comps, halo, real_bytes));
+  return LF2_OK;
+}
+
+static lf2_status deposit(lf2_ctx* c, lf2_field f, int kind, int comps)
+{
+  if (!valid_field(c, f)) return LF2_ERR_ARG;
+  if (f->comps != comps) return fail(c, LF2_ERR_ARG, "field has the wrong number of components");
+  LF2_TRY(ensure_spill(c, comps));
+  {
+    PhaseScope ps(c, PH_DEPOSIT);
+    LF2_CUDA(c, launch_deposit(c, kind, f->data, 0));
+  }
+  {
+    PhaseScope ps(c, PH_FIXUP);
+    LF2_CUDA(c, launch_deposit(c, kind, f->data, 1));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_deposit_scalar(lf2_ctx* c, lf2_field rho) { return deposit(c, rho, 0, 1); }
+lf2_status lf2_deposit_vector_cicngp(lf2_ctx* c, lf2_field v) { return deposit(c, v, 1, 3); }
+lf2_status lf2_deposit_symtensor_cicngp(lf2_ctx* c, lf2_field t) { return deposit(c, t, 2, 6); }
+
+static lf2_status rebin_tail(lf2_ctx* c)
+{
+  PhaseScope ps(c, PH_INSERT);
+  LF2_CUDA(c, launch_insert(c));
+  LF2_CUDA(c, launch_repack(c));
+  return LF2_OK;
+}
+
+lf2_status lf2_gather_kick(lf2_ctx* c, lf2_field F, double dtau, double* max_v)
+{
+  if (!valid_field(c, F)) return LF2_ERR_ARG;
+  if (F->comps != 3) return fail(c, LF2_ERR_ARG, "the kick field needs 3 components");
+  MoveParams mp{(float)dtau, 0.0f};
+  {
+    PhaseScope ps(c, PH_MOVE);
+    LF2_CUDA(c, launch_move(c, F->data, true, false, mp));
+  }
+  if (max_v) {
+    LF2_CUDA(c, launch_reduce_maxv(c));
+    LF2_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats, sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+    *max_v = std::sqrt(c->h_stats[0]);
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_drift_rebin(lf2_ctx* c, double dtau)
+{
+  if (!c) return LF2_ERR_ARG;
+  MoveParams mp{0.0f, (float)(dtau / c->res)};
+  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  {
+    PhaseScope ps(c, PH_MOVE);
+    LF2_CUDA(c, launch_move(c, nullptr, false, true, mp));
+  }
+  return rebin_tail(c);
+}
+
+lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift, lf2_field rho)
+{
+  if (!valid_field(c, F)) return LF2_ERR_ARG;
+  if (F->comps != 3) return fail(c, LF2_ERR_ARG, "the kick field needs 3 components");
+  MoveParams mp{(float)dtau_kick, (float)(dtau_drift / c->res)};
+  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  {
+    PhaseScope ps(c, PH_MOVE);
+    LF2_CUDA(c, launch_move(c, F->data, true, true, mp));
+  }
+  LF2_TRY(rebin_tail(c));
+  if (rho) LF2_TRY(deposit(c, rho, 0, 1));
+  return LF2_OK;
+}
+
+lf2_status lf2_conservation(lf2_ctx* c, double* mass, double mom[3], double* max_v)
+{
+  if (!c) return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_conservation(c));
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats, sizeof(double) * 8, cudaMemcpyDeviceToHost,
+                              c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (mass) *mass = c->h_stats[1];
+  if (mom)
+    for (int d = 0; d < 3; d++) mom[d] = c->h_stats[2 + d];
+  if (max_v) *max_v = std::sqrt(c->h_stats[5]);
+  return LF2_OK;
+}
+
+lf2_status lf2_profile_enable(lf2_ctx* c, int on)
+{
+  if (!c) return LF2_ERR_ARG;
+  c->profiling = on != 0;
+  return LF2_OK;
+}
+
+lf2_status lf2_profile_read(lf2_ctx* c, double* ms, int64_t* launches)
+{
+  if (!c) return LF2_ERR_ARG;
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int p = 0; p < LF2_NPHASE; p++) {
+    double t = 0.0;
+    for (auto& pr : c->pending[p]) {
+      float x = 0.0f;
+      if (cudaEventElapsedTime(&x, pr.first, pr.second) == cudaSuccess) t += x;
+      c->event_pool.push_back(pr.first);
+      c->event_pool.push_back(pr.second);
+    }
+    c->pending[p].clear();
+    if (ms) ms[p] = t;
+    if (launches) launches[p] = c->phase_launches[p];
+    c->phase_launches[p] = 0;
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_kernel_launches(lf2_ctx* c, int64_t* n)
+{
+  if (!c || !n) return LF2_ERR_ARG;
+  *n = c->launches;
+  return LF2_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+// lf2_internal.h -- context layout and kernel launchers shared by the .cu
+// files of liblf2gpu.so.  Not part of the public ABI (include/lf2gpu.h).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "lf2_common.cuh"
+#include "lf2gpu.h"
+
+namespace lf2 {
+
+// Structure-of-arrays particle store (see lf2_common.cuh).
+struct PartArrays {
+  uint32_t* key = nullptr;
+  float* ox = nullptr;
+  float* oy = nullptr;
+  float* oz = nullptr;
+  float* vx = nullptr;
+  float* vy = nullptr;
+  float* vz = nullptr;
+  float* mass = nullptr;  // only with per-particle masses
+  int64_t* id = nullptr;  // only when IDs are carried
+};
+
+// Arguments shared by the per-brick kernels.
+struct StoreView {
+  Geom g;
+  PartArrays a;
+  const int64_t* seg_start;  // [nbricks + 1]
+  int32_t* count;            // [nbricks]
+  const int32_t* cap;        // [nbricks]
+};
+
+struct DepositParams {
+  float mf;          // FP32 mode: mass / res^3 for a global mass
+  float inv_vol;     // 1 / res^3
+  float fixed_scale; // fixed mode: 2^-32 * unit mass / res^3
+  float inv_unit;    // fixed mode: 1 / unit mass (per-particle masses)
+  int has_mass;
+};
+
+struct MoveParams {
+  float dtk;   // kick: dtau
+  float dtn;   // drift: dtau / res (cell units per velocity unit)
+};
+
+}  // namespace lf2
+
+struct lf2_field_s {
+  int comps = 0;
+  float* data = nullptr;
+  bool owned = true;
+};
+
+struct lf2_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  lf2::Geom g{};
+  double res = 0.0;
+  double box[3] = {0, 0, 0};
+  int mode = LF2_DEPOSIT_FP32;
+  std::string err;
+
+  // particle store
+  int64_t np = 0;
+  bool has_mass = false;
+  bool has_id = false;
+  double gmass = 0.0;   // global particle mass (GLOBAL_MASS types)
+  double m_unit = 1.0;  // unit mass of the fixed-point deposit
+  int64_t capacity = 0; // slots allocated in cur/alt
+  lf2::PartArrays cur, alt, mov;
+  int64_t mov_capacity = 0;
+  int32_t* mov_placed = nullptr;
+  int64_t* seg_start = nullptr;      // [nbricks + 1]
+  int64_t* seg_start_alt = nullptr;  // [nbricks + 1]
+  int32_t* count = nullptr;          // [nbricks]
+  int32_t* cap = nullptr;            // [nbricks]
+  int32_t* cap_alt = nullptr;        // [nbricks]
+  int32_t* fill = nullptr;           // [nbricks] scratch
+  unsigned long long* mov_count = nullptr;
+  uint32_t* flags = nullptr;         // device error bits
+  int32_t* repack = nullptr;         // device: 1 when a brick overflowed
+  float* brick_maxv2 = nullptr;      // [nbricks]
+  double* brick_sums = nullptr;      // [nbricks * 5]
+  double* stats = nullptr;           // [8] device
+  uint64_t* spill = nullptr;         // deposit shell store (8-byte slots)
+  size_t spill_slots = 0;
+  double* h_stats = nullptr;         // pinned [8]
+  uint32_t* h_flags = nullptr;       // pinned
+  int64_t* h_i64 = nullptr;          // pinned [4]
+
+  // measurement (lf2_profile_*)
+  int64_t launches = 0;              // kernels launched, all phases
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[LF2_NPHASE];
+  std::vector<cudaEvent_t> event_pool;
+  int64_t phase_launches[LF2_NPHASE] = {0, 0, 0, 0, 0};
+};
+
+// ---------------------------------------------------------------- launchers
+namespace lf2 {
+
+inline StoreView view(lf2_ctx* c)
+{
+  StoreView v;
+  v.g = c->g;
+  v.a = c->cur;
+  v.seg_start = c->seg_start;
+  v.count = c->count;
+  v.cap = c->cap;
+  return v;
+}
+
+// lf2_store.cu
+cudaError_t launch_load_count(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3);
+cudaError_t launch_caps_and_scan(lf2_ctx* c, const int32_t* counts, int32_t* caps, int64_t* starts,
+                                 int64_t* total_dev);
+cudaError_t launch_load_scatter(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                                const float* vel3, const float* mass, const int64_t* id);
+cudaError_t launch_pos_to_state(lf2_ctx* c, int64_t n, const void* pos3, int real_bytes,
+                                int32_t* cell, float* off3);
+cudaError_t launch_get(lf2_ctx* c, int64_t* out_start, int32_t* cell, float* off3, float* vel3,
+                       float* mass, int64_t* id);
+cudaError_t launch_state_to_pos(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                                void* pos3, int real_bytes);
+cudaError_t launch_cell_counts(lf2_ctx* c, int32_t* counts);
+cudaError_t launch_scan_counts(lf2_ctx* c, int64_t* out_start);
+cudaError_t launch_repack(lf2_ctx* c);
+
+// lf2_move.cu
+cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp);
+cudaError_t launch_insert(lf2_ctx* c);
+cudaError_t launch_reduce_maxv(lf2_ctx* c);
+
+// lf2_deposit.cu
+// stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
+cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
+
+// lf2_field.cu
+cudaError_t launch_export(lf2_ctx* c, int comps, const float* src, void* dst, int halo,
+                          int real_bytes, int fill_halo);
+cudaError_t launch_import(lf2_ctx* c, int comps, float* dst, const void* src, int halo,
+                          int real_bytes);
+cudaError_t launch_halo_fill(lf2_ctx* c, void* data, int comps, int halo, int real_bytes);
+cudaError_t launch_conservation(lf2_ctx* c);
+
+}  // namespace lf2

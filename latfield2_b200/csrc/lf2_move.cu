@@ -1,0 +1,285 @@
+// lf2_move.cu -- gather-kick, drift and rebin of the brick-binned particles.
+//
+// One CTA per brick.  The kick gathers the 3-component field at the 8 cell
+// corners from a shared-memory copy of the brick's (BRICK+1)^3 vertex tile
+// (the CIC gather the reference leaves to the updateVel callback,
+// LATfield2_Particles.hpp:752-893).  The drift is move_particles_simple
+// (move_function.hpp:15-32) in cell units: off += dtau/res * vel, then the
+// integer part is carried into the cell coordinates with a periodic wrap
+// (the wrap and rebin of moveParticles, LATfield2_Particles.hpp:2028-2056).
+//
+// Rebin: particles that stay in their brick are compacted in place at the
+// front of the brick's segment; particles that leave are appended to a mover
+// buffer and inserted into their new brick's free slots by k_insert.  A brick
+// that runs out of free slots sets the repack flag (lf2_store.cu).
+#include <cuda_runtime.h>
+
+#include "lf2_internal.h"
+
+namespace lf2 {
+
+namespace {
+
+constexpr int MOVE_THREADS = 256;
+
+__device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
+
+template <bool KICK, bool DRIFT>
+__global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float* __restrict__ F,
+                                                       MoveParams mp, PartArrays mov,
+                                                       unsigned long long* mov_count,
+                                                       float* brick_maxv2, uint32_t* flags)
+{
+  extern __shared__ float ftile[];  // [3][TILE3] when KICK
+  __shared__ int s_scan[32];
+  __shared__ float s_max[MOVE_THREADS / 32];
+
+  const Geom& g = v.g;
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+
+  if (KICK) {
+    const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+              ez = brick_extent(g.n[2], bz);
+    for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
+      const int i = t % TILE, j = (t / TILE) % TILE, k = t / (TILE * TILE);
+      if (i > ex || j > ey || k > ez) continue;
+      const int gx = x0 + i < g.n[0] ? x0 + i : 0;
+      const int gy = y0 + j < g.n[1] ? y0 + j : 0;
+      const int gz = z0 + k < g.n[2] ? z0 + k : 0;
+      const int64_t s = site_index(g, gx, gy, gz);
+      ftile[t] = __ldg(F + s);
+      ftile[TILE3 + t] = __ldg(F + g.nsites + s);
+      ftile[2 * TILE3 + t] = __ldg(F + 2 * g.nsites + s);
+    }
+    __syncthreads();
+  }
+
+  const int64_t base = v.seg_start[b];
+  const int cnt = LF2_BRICK_COUNT(v, b);
+  int write = 0;
+  float maxv2 = 0.0f;
+  const int lane = threadIdx.x & 31;
+
+  for (int c0 = 0; c0 < cnt; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    const bool active = i < cnt;
+    const int64_t p = base + i;
+    uint32_t key = 0;
+    float ox = 0.f, oy = 0.f, oz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, m = 0.f;
+    int64_t id = 0;
+    bool stay = true;
+    if (active) {
+      key = v.a.key[p];
+      ox = v.a.ox[p];
+      oy = v.a.oy[p];
+      oz = v.a.oz[p];
+      vx = v.a.vx[p];
+      vy = v.a.vy[p];
+      vz = v.a.vz[p];
+      if (DRIFT && v.a.mass) m = v.a.mass[p];
+      if (DRIFT && v.a.id) id = v.a.id[p];
+      int x, y, z;
+      unpack_key(g, key, x, y, z);
+      if (KICK) {
+        const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
+        const float gx = __fsub_rn(1.0f, ox), gy = __fsub_rn(1.0f, oy), gz = __fsub_rn(1.0f, oz);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+          const float w = __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz));
+          const int t = t0 + cx + cy * TILE + cz * TILE * TILE;
+          a0 = __fmaf_rn(w, ftile[t], a0);
+          a1 = __fmaf_rn(w, ftile[TILE3 + t], a1);
+          a2 = __fmaf_rn(w, ftile[2 * TILE3 + t], a2);
+        }
+        vx = __fmaf_rn(mp.dtk, a0, vx);
+        vy = __fmaf_rn(mp.dtk, a1, vy);
+        vz = __fmaf_rn(mp.dtk, a2, vz);
+      }
+      maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                     __fmul_rn(vz, vz)));
+      if (DRIFT) {
+        float o[3] = {ox, oy, oz};
+        const float vv[3] = {vx, vy, vz};
+        int xyz[3] = {x, y, z};
+        bool finite = true;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          float od = __fmaf_rn(mp.dtn, vv[d], o[d]);
+          if (!isfinite(od)) {
+            finite = false;
+            break;
+          }
+          const float fl = floorf(od);
+          od = __fsub_rn(od, fl);
+          int carry = (int)fl;
+          if (od >= 1.0f) {
+            od = 0.0f;
+            carry += 1;
+          }
+          o[d] = od;
+          xyz[d] = wrap_add(xyz[d], carry, g.n[d]);
+        }
+        if (finite) {
+          ox = o[0];
+          oy = o[1];
+          oz = o[2];
+          key = pack_key(g, xyz[0], xyz[1], xyz[2]);
+          stay = brick_of(g, xyz[0], xyz[1], xyz[2]) == b;
+        } else {
+          set_flag(flags, ERR_NONFINITE);
+        }
+      }
+    }
+
+    if (!DRIFT) {
+      if (active) {
+        v.a.vx[p] = vx;
+        v.a.vy[p] = vy;
+        v.a.vz[p] = vz;
+      }
+      continue;
+    }
+
+    // All loads of this chunk are complete before any slot is overwritten.
+    int total;
+    const int rank = block_exclusive_scan(active && stay ? 1 : 0, s_scan, &total);
+    if (active && stay) {
+      const int64_t q = base + write + rank;
+      v.a.key[q] = key;
+      v.a.ox[q] = ox;
+      v.a.oy[q] = oy;
+      v.a.oz[q] = oz;
+      v.a.vx[q] = vx;
+      v.a.vy[q] = vy;
+      v.a.vz[q] = vz;
+      if (v.a.mass) v.a.mass[q] = m;
+      if (v.a.id) v.a.id[q] = id;
+    }
+    const bool leave = active && !stay;
+    const unsigned bal = __ballot_sync(0xffffffffu, leave);
+    if (bal) {
+      const int leader = __ffs(bal) - 1;
+      unsigned long long s0 = 0;
+      if (lane == leader) s0 = atomicAdd(mov_count, (unsigned long long)__popc(bal));
+      s0 = __shfl_sync(0xffffffffu, s0, leader);
+      if (leave) {
+        const int64_t q = (int64_t)s0 + __popc(bal & ((1u << lane) - 1u));
+        mov.key[q] = key;
+        mov.ox[q] = ox;
+        mov.oy[q] = oy;
+        mov.oz[q] = oz;
+        mov.vx[q] = vx;
+        mov.vy[q] = vy;
+        mov.vz[q] = vz;
+        if (mov.mass) mov.mass[q] = m;
+        if (mov.id) mov.id[q] = id;
+      }
+    }
+    write += total;
+  }
+  if (DRIFT && threadIdx.x == 0) v.count[b] = write;
+
+  // max |v|^2 of the brick
+  for (int o = 16; o > 0; o >>= 1) maxv2 = fmaxf(maxv2, __shfl_xor_sync(0xffffffffu, maxv2, o));
+  if (lane == 0) s_max[threadIdx.x >> 5] = maxv2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float mm = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) mm = fmaxf(mm, s_max[w]);
+    brick_maxv2[b] = mm;
+  }
+}
+
+// Movers into the free slots of their new brick.
+__global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* __restrict__ mov_count,
+                         int32_t* placed, int32_t* repack)
+{
+  const int64_t nm = (int64_t)*mov_count;
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    unpack_key(v.g, mov.key[m], x, y, z);
+    const int64_t b = brick_of(v.g, x, y, z);
+    const int slot = atomicAdd(&v.count[b], 1);
+    if (slot < v.cap[b]) {
+      const int64_t q = v.seg_start[b] + slot;
+      v.a.key[q] = mov.key[m];
+      v.a.ox[q] = mov.ox[m];
+      v.a.oy[q] = mov.oy[m];
+      v.a.oz[q] = mov.oz[m];
+      v.a.vx[q] = mov.vx[m];
+      v.a.vy[q] = mov.vy[m];
+      v.a.vz[q] = mov.vz[m];
+      if (v.a.mass) v.a.mass[q] = mov.mass[m];
+      if (v.a.id) v.a.id[q] = mov.id[m];
+      placed[m] = 1;
+    } else {
+      placed[m] = 0;
+      *repack = 1;
+    }
+  }
+}
+
+// max over bricks of max |v|^2 -> stats[0] (one CTA, fixed order).
+__global__ void __launch_bounds__(1024) k_reduce_maxv(int64_t nb, const float* __restrict__ bm,
+                                                      double* stats)
+{
+  __shared__ float sh[1024];
+  float m = 0.0f;
+  for (int64_t b = threadIdx.x; b < nb; b += blockDim.x) m = fmaxf(m, bm[b]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) stats[0] = (double)sh[0];
+}
+
+}  // namespace
+
+// The caller zeroes c->mov_count before a drift.
+cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp)
+{
+  c->launches += 1;
+  const size_t smem = kick ? sizeof(float) * 3 * TILE3 : 0;
+  const unsigned nb = (unsigned)c->g.nbricks;
+  if (kick && drift) {
+    cudaFuncSetAttribute(k_move<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_move<true, true><<<nb, MOVE_THREADS, smem, c->stream>>>(view(c), F, mp, c->mov, c->mov_count,
+                                                             c->brick_maxv2, c->flags);
+  } else if (kick) {
+    cudaFuncSetAttribute(k_move<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    k_move<true, false><<<nb, MOVE_THREADS, smem, c->stream>>>(view(c), F, mp, c->mov, c->mov_count,
+                                                              c->brick_maxv2, c->flags);
+  } else if (drift) {
+    k_move<false, true><<<nb, MOVE_THREADS, 0, c->stream>>>(view(c), F, mp, c->mov, c->mov_count,
+                                                           c->brick_maxv2, c->flags);
+  } else {
+    k_move<false, false><<<nb, MOVE_THREADS, 0, c->stream>>>(view(c), F, mp, c->mov, c->mov_count,
+                                                            c->brick_maxv2, c->flags);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_insert(lf2_ctx* c)
+{
+  c->launches += 1;
+  k_insert<<<148 * 4, 256, 0, c->stream>>>(view(c), c->mov, c->mov_count, c->mov_placed, c->repack);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_maxv(lf2_ctx* c)
+{
+  c->launches += 1;
+  k_reduce_maxv<<<1, 1024, 0, c->stream>>>(c->g.nbricks, c->brick_maxv2, c->stats);
+  return cudaGetLastError();
+}
+
+}  // namespace lf2

@@ -1,0 +1,224 @@
+/*
+ * lf2_oracle.c -- CPU oracle for the LATfield2 particle-mesh path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker of the CUDA path, never linked into
+ * the product library.  See lf2_oracle.h for the two layers.
+ *
+ * Must be compiled with -ffp-contract=off so that no multiply-add is fused
+ * behind the back of the restated arithmetic.
+ */
+#include "lf2_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------ layer (A) */
+#define R double
+#define LF2O_FN(name) name##_d
+#include "lf2_oracle_ref.inc"
+#undef R
+#undef LF2O_FN
+
+#define R float
+#define LF2O_FN(name) name##_f
+#include "lf2_oracle_ref.inc"
+#undef R
+#undef LF2O_FN
+
+/* addParticle_global pushes each particle onto the front of its cell's
+ * forward_list (LATfield2_Particles.hpp:500-519), so a list holds its
+ * particles in reverse insertion order. */
+void lf2o_lists_from_insertion(int64_t ncells, int64_t np, const int32_t* cell,
+                               int64_t* cs, int64_t* order)
+{
+  memset(cs, 0, sizeof(int64_t) * (size_t)(ncells + 1));
+  for (int64_t p = 0; p < np; p++) cs[cell[p] + 1]++;
+  for (int64_t c = 0; c < ncells; c++) cs[c + 1] += cs[c];
+  int64_t* fill = (int64_t*)malloc(sizeof(int64_t) * (size_t)ncells);
+  for (int64_t c = 0; c < ncells; c++) fill[c] = cs[c + 1];
+  for (int64_t p = 0; p < np; p++) order[--fill[cell[p]]] = p;
+  free(fill);
+}
+
+/* ------------------------------------------------------------ layer (B) */
+
+static inline long wrapi(long v, long n)
+{
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+static inline void cell_coords(const int n[3], int32_t c, long xyz[3])
+{
+  xyz[0] = c % n[0];
+  xyz[1] = (c / n[0]) % n[1];
+  xyz[2] = c / ((long)n[0] * n[1]);
+}
+
+void lf2o_state_kick(const int n[3], int64_t np, const int32_t* cell,
+                     const float* off, float* vel, const float* F, float dtk)
+{
+  const long ns = (long)n[0] * n[1] * n[2];
+  for (int64_t p = 0; p < np; p++) {
+    long xyz[3];
+    cell_coords(n, cell[p], xyz);
+    const float fx = off[3 * p + 0], fy = off[3 * p + 1], fz = off[3 * p + 2];
+    const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+    const long xs[2] = {xyz[0], wrapi(xyz[0] + 1, n[0])};
+    const long ys[2] = {xyz[1], wrapi(xyz[1] + 1, n[1])};
+    const long zs[2] = {xyz[2], wrapi(xyz[2] + 1, n[2])};
+    float acc[3] = {0.0f, 0.0f, 0.0f};
+    for (int k = 0; k < 8; k++) {
+      const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+      const float w = ((bx ? fx : gx) * (by ? fy : gy)) * (bz ? fz : gz);
+      const long site = xs[bx] + (long)n[0] * (ys[by] + (long)n[1] * zs[bz]);
+      for (int c = 0; c < 3; c++) acc[c] = fmaf(w, F[c * ns + site], acc[c]);
+    }
+    for (int c = 0; c < 3; c++) vel[3 * p + c] = fmaf(dtk, acc[c], vel[3 * p + c]);
+  }
+}
+
+int64_t lf2o_state_drift(const int n[3], int64_t np, int32_t* cell, float* off,
+                         const float* vel, float dtn)
+{
+  int64_t bad = 0;
+  for (int64_t p = 0; p < np; p++) {
+    long xyz[3];
+    cell_coords(n, cell[p], xyz);
+    int ok = 1;
+    for (int l = 0; l < 3; l++) {
+      float o = fmaf(dtn, vel[3 * p + l], off[3 * p + l]);
+      if (!isfinite(o)) {
+        ok = 0;
+        break;
+      }
+      float fl = floorf(o);
+      o = o - fl;
+      long carry = (long)fl;
+      if (o >= 1.0f) {
+        o = 0.0f;
+        carry += 1;
+      }
+      off[3 * p + l] = o;
+      xyz[l] = wrapi(xyz[l] + carry, n[l]);
+    }
+    if (!ok) {
+      bad++;
+      continue;
+    }
+    cell[p] = (int32_t)(xyz[0] + n[0] * (xyz[1] + (long)n[1] * xyz[2]));
+  }
+  return bad;
+}
+
+uint64_t lf2o_fixed_weight(float wx, float wy, float wz, int bx, int by, int bz)
+{
+  const uint64_t one = 1ull << 31;
+  const uint64_t ux = (uint64_t)lrintf(wx * 2147483648.0f);
+  const uint64_t uy = (uint64_t)lrintf(wy * 2147483648.0f);
+  const uint64_t uz = (uint64_t)lrintf(wz * 2147483648.0f);
+  const uint64_t qx = bx ? ux : one - ux;
+  const uint64_t qy = by ? uy : one - uy;
+  const uint64_t qz = bz ? uz : one - uz;
+  const unsigned __int128 prod = (unsigned __int128)(qx * qy) * qz;
+  return (uint64_t)((prod + ((unsigned __int128)1 << 60)) >> 61);
+}
+
+void lf2o_state_deposit_fixed(const int n[3], int64_t np, const int32_t* cell,
+                              const float* off, const float* mrel, int64_t* acc)
+{
+  for (int64_t p = 0; p < np; p++) {
+    long xyz[3];
+    cell_coords(n, cell[p], xyz);
+    const long xs[2] = {xyz[0], wrapi(xyz[0] + 1, n[0])};
+    const long ys[2] = {xyz[1], wrapi(xyz[1] + 1, n[1])};
+    const long zs[2] = {xyz[2], wrapi(xyz[2] + 1, n[2])};
+    uint64_t mq = 0;
+    if (mrel) mq = (uint64_t)lrintf(mrel[p] * 16777216.0f);
+    for (int k = 0; k < 8; k++) {
+      const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+      uint64_t q = lf2o_fixed_weight(off[3 * p], off[3 * p + 1], off[3 * p + 2],
+                                     bx, by, bz);
+      if (mrel) q = (q * mq + (1ull << 23)) >> 24;
+      const long site = xs[bx] + (long)n[0] * (ys[by] + (long)n[1] * zs[bz]);
+      acc[site] += (int64_t)q;
+    }
+  }
+}
+
+void lf2o_state_fixed_to_f32(int64_t nsites, const int64_t* acc, float scale,
+                             float* rho)
+{
+  for (int64_t i = 0; i < nsites; i++) rho[i] = (float)acc[i] * scale;
+}
+
+void lf2o_state_deposit_f64(const int n[3], int64_t np, const int32_t* cell,
+                            const float* off, const float* mass, double gmass,
+                            double res, double* rho)
+{
+  const double vol = res * res * res;
+  for (int64_t p = 0; p < np; p++) {
+    long xyz[3];
+    cell_coords(n, cell[p], xyz);
+    const long xs[2] = {xyz[0], wrapi(xyz[0] + 1, n[0])};
+    const long ys[2] = {xyz[1], wrapi(xyz[1] + 1, n[1])};
+    const long zs[2] = {xyz[2], wrapi(xyz[2] + 1, n[2])};
+    const double m = (mass ? (double)mass[p] : gmass) / vol;
+    const double f[3] = {off[3 * p], off[3 * p + 1], off[3 * p + 2]};
+    for (int k = 0; k < 8; k++) {
+      const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+      const double w = (bx ? f[0] : 1.0 - f[0]) * (by ? f[1] : 1.0 - f[1]) *
+                       (bz ? f[2] : 1.0 - f[2]);
+      const long site = xs[bx] + (long)n[0] * (ys[by] + (long)n[1] * zs[bz]);
+      rho[site] += w * m;
+    }
+  }
+}
+
+/* List order after the rebin loop of moveParticles on one rank
+ * (LATfield2_Particles.hpp:1960-2056): cells are visited in site order; a
+ * particle whose cell changed is spliced to the front of its new cell's list
+ * (splice_after(before_begin, ...), :2049) and the walk resumes after its
+ * predecessor (:2052); a particle spliced into a later cell is visited again
+ * there and stays.  Input lists (cs_old, order_old) and the new cell of every
+ * particle; output lists in CSR form. */
+void lf2o_rebin_lists(int64_t ncells, int64_t np, const int64_t* cs_old,
+                      const int64_t* order_old, const int32_t* new_cell,
+                      int64_t* cs_new, int64_t* order_new)
+{
+  int64_t* head = (int64_t*)malloc(sizeof(int64_t) * (size_t)ncells);
+  int64_t* next = (int64_t*)malloc(sizeof(int64_t) * (size_t)(np > 0 ? np : 1));
+  for (int64_t c = 0; c < ncells; c++) {
+    head[c] = -1;
+    for (int64_t i = cs_old[c + 1] - 1; i >= cs_old[c]; i--) {
+      next[order_old[i]] = head[c];
+      head[c] = order_old[i];
+    }
+  }
+  for (int64_t c = 0; c < ncells; c++) {
+    int64_t prev = -1; /* -1 stands for before_begin */
+    int64_t it = head[c];
+    while (it >= 0) {
+      const int64_t nc = new_cell[it];
+      if (nc != c) {
+        if (prev < 0) head[c] = next[it];
+        else next[prev] = next[it];
+        next[it] = head[nc];
+        head[nc] = it;
+        it = (prev < 0) ? head[c] : next[prev];
+      } else {
+        prev = it;
+        it = next[it];
+      }
+    }
+  }
+  int64_t k = 0;
+  for (int64_t c = 0; c < ncells; c++) {
+    cs_new[c] = k;
+    for (int64_t it = head[c]; it >= 0; it = next[it]) order_new[k++] = it;
+  }
+  cs_new[ncells] = k;
+  free(head);
+  free(next);
+}

@@ -1,0 +1,65 @@
+"""Shared helpers of the test suite: seeded small cases and error measures."""
+import numpy as np
+
+
+def small_case(n, npart, seed, vel_sigma=0.01, clustered=False):
+    """Particles in the device representation (cell, off, vel) as numpy."""
+    rng = np.random.default_rng(seed)
+    n = tuple(int(v) for v in n)
+    if clustered:
+        centre = rng.random(3)
+        pos = np.mod(centre + 0.6 / max(n) * rng.standard_normal((npart, 3)), 1.0)
+    else:
+        pos = rng.random((npart, 3))
+    u = pos * np.array(n, np.float64)
+    fl = np.floor(u)
+    off = (u - fl).astype(np.float32)
+    carry = off >= 1.0
+    off[carry] = 0.0
+    fl = fl + carry
+    ci = np.mod(fl.astype(np.int64), np.array(n))
+    cell = (ci[:, 0] + n[0] * (ci[:, 1] + n[1] * ci[:, 2])).astype(np.int32)
+    vel = (vel_sigma * rng.standard_normal((npart, 3))).astype(np.float32)
+    return cell, off, vel
+
+
+def cell_xyz(n, cell):
+    c = np.asarray(cell, np.int64)
+    return np.stack([c % n[0], (c // n[0]) % n[1], c // (n[0] * n[1])], axis=1)
+
+
+def positions(n, res, cell, off):
+    return (cell_xyz(n, cell).astype(np.float64) + off.astype(np.float64)) * res
+
+
+def normalized_error(got, ref):
+    """max |got - ref| / max(max |ref|, tiny): the error relative to the
+    field's scale (per-vertex relative error is undefined where ref ~ 0)."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    scale = max(np.max(np.abs(ref)), 1e-300)
+    return float(np.max(np.abs(got - ref)) / scale)
+
+
+def mean_relative_error(got, ref, floor_frac=1e-3):
+    """Per-vertex relative error where |ref| exceeds floor_frac of its mean |ref|."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    m = np.abs(ref) > floor_frac * np.mean(np.abs(ref))
+    if not np.any(m):
+        return 0.0
+    return float(np.max(np.abs(got[m] - ref[m]) / np.abs(ref[m])))
+
+
+def by_id(d, ids_key="id"):
+    order = np.argsort(d[ids_key], kind="stable")
+    return {k: v[order] for k, v in d.items()}
+
+
+def internal_to_reference(F, halo):
+    """(c, z, y, x) internal -> (z+2h, y+2h, x+2h, c) reference layout, halo filled
+    periodically."""
+    a = np.ascontiguousarray(np.asarray(F).transpose(1, 2, 3, 0))
+    if halo:
+        a = np.pad(a, ((halo, halo), (halo, halo), (halo, halo), (0, 0)), mode="wrap")
+    return np.ascontiguousarray(a)

@@ -1,0 +1,67 @@
+"""CPU checks of the C ABI boundary: the built library loads without a GPU and
+exports every function that include/*.h declares; argument validation that
+happens before any device work."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(lf2_\w+)\s*\(", text, re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ("lf2_create", "lf2_particles_set", "lf2_deposit_scalar", "lf2_gather_kick",
+                 "lf2_drift_rebin", "lf2_step", "lf2_field_export", "lf2_conservation"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from latfield2_b200 import _lib
+    lib = _lib.load()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    for name in _lib.SIGNATURES:
+        assert name in declared_functions(), f"binding for undeclared {name}"
+
+
+def test_create_rejects_bad_geometry_without_touching_the_device():
+    from latfield2_b200 import _lib
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    n = (ctypes.c_int * 3)(8, 8, 8)
+    bad_box = (ctypes.c_double * 3)(1.0, 2.0, 1.0)  # unequal resolution
+    assert lib.lf2_create(ctypes.byref(h), 0, n, bad_box, 0, None) == _lib.LF2_ERR_ARG
+    box = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    assert lib.lf2_create(ctypes.byref(h), 0, n, box, 7, None) == _lib.LF2_ERR_ARG
+    zero = (ctypes.c_int * 3)(0, 8, 8)
+    assert lib.lf2_create(ctypes.byref(h), 0, zero, box, 0, None) == _lib.LF2_ERR_ARG
+    big = (ctypes.c_int * 3)(2048, 2048, 2048)
+    assert lib.lf2_create(ctypes.byref(h), 0, big, (ctypes.c_double * 3)(1, 1, 1), 0,
+                          None) == _lib.LF2_ERR_UNSUPPORTED
+
+
+def test_null_context_is_an_argument_error():
+    from latfield2_b200 import _lib
+    lib = _lib.load()
+    assert lib.lf2_deposit_scalar(None, None) == _lib.LF2_ERR_ARG
+    assert lib.lf2_drift_rebin(None, ctypes.c_double(0.1)) == _lib.LF2_ERR_ARG
+    assert lib.lf2_particles_count(None, None) == _lib.LF2_ERR_ARG
+    assert lib.lf2_last_error(None) == b"null context"
+
+
+def test_sources_target_sm100a_only():
+    from latfield2_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
