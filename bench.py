@@ -39,6 +39,8 @@ WORKLOADS = {
     "c2": dict(n=256, npart=256 ** 3, dist="clumps", mode="fp32"),
     "c5": dict(n=768, npart=768 ** 3, dist="halos", mode="fixed"),
     "c1": dict(n=64, npart=64 ** 3, dist="uniform", mode="fp32"),
+    # c3 statistics at 256^3 (16.8M particles): the size used for ncu captures
+    "c3s": dict(n=256, npart=256 ** 3, dist="lognormal", mode="fixed"),
 }
 METRIC = "particle updates/s (CIC deposit+gather+move)"
 UNIT = "particle-updates/s"

@@ -69,6 +69,7 @@ SIGNATURES = {
     "lf2_profile_enable": [c_void_p, c_int],
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
     "lf2_kernel_launches": [c_void_p, P(c_i64)],
+    "lf2_rebin_stats": [c_void_p, P(c_i64), P(c_i64)],
 }
 NPHASE = 5
 PHASES = ("move", "insert_repack", "deposit_tile", "deposit_fixup", "other")

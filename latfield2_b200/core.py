@@ -239,6 +239,12 @@ class Context:
         self._check(_lib.load().lf2_profile_read(self.h, ms, ln), "profile_read")
         return {p: (ms[i], ln[i]) for i, p in enumerate(_lib.PHASES)}
 
+    def rebin_stats(self):
+        """(repacks since creation, particles that changed brick in the last drift)."""
+        r, m = _c.c_int64(), _c.c_int64()
+        self._check(_lib.load().lf2_rebin_stats(self.h, _c.byref(r), _c.byref(m)), "rebin_stats")
+        return r.value, m.value
+
     def kernel_launches(self):
         n = _c.c_int64()
         self._check(_lib.load().lf2_kernel_launches(self.h, _c.byref(n)), "kernel_launches")

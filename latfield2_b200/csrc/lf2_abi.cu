@@ -294,6 +294,7 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->repack, sizeof(int32_t)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->diag, sizeof(unsigned long long) * 2) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_i64, sizeof(int64_t) * 4) == cudaSuccess;
@@ -303,6 +304,7 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
          cudaMemsetAsync(c->seg_start, 0, sizeof(int64_t) * (nb + 1), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->repack, 0, sizeof(int32_t), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->diag, 0, 2 * sizeof(unsigned long long), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
          cudaStreamSynchronize(c->stream) == cudaSuccess;
   }
@@ -336,6 +338,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->mov_count);
   cudaFree(c->flags);
   cudaFree(c->repack);
+  cudaFree(c->diag);
   cudaFree(c->spill);
   cudaFreeHost(c->h_stats);
   cudaFreeHost(c->h_flags);
@@ -754,6 +757,17 @@ lf2_status lf2_profile_read(lf2_ctx* c, double* ms, int64_t* launches)
     if (launches) launches[p] = c->phase_launches[p];
     c->phase_launches[p] = 0;
   }
+  return LF2_OK;
+}
+
+lf2_status lf2_rebin_stats(lf2_ctx* c, int64_t* repacks, int64_t* movers)
+{
+  if (!c) return LF2_ERR_ARG;
+  unsigned long long d[2] = {0, 0};
+  LF2_CUDA(c, cudaMemcpyAsync(d, c->diag, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (repacks) *repacks = (int64_t)d[0];
+  if (movers) *movers = (int64_t)d[1];
   return LF2_OK;
 }
 

@@ -122,17 +122,20 @@ __device__ inline void set_flag(uint32_t* flags, uint32_t bit)
   atomicOr(flags, bit);
 }
 
-// Fixed-point CIC weight of one corner: 1-D weights rounded to 2^-31, exact
-// 96-bit product, rounded to 2^-32 of a unit mass.  Same arithmetic as the
-// oracle's lf2o_fixed_weight.
+// Fixed-point CIC weight of one corner: 1-D weights rounded to 2^-31,
+// exact 96-bit product, rounded to 2^-32 of a unit mass:
+//   q = (qx*qy*qz + 2^60) >> 61.
+// With qx*qy = ph*2^32 + pl:  qx*qy*qz = ph*qz*2^32 + pl*qz, and because the
+// rounding term 2^60 has no bits below 2^32,
+//   q = (ph*qz + umulhi(pl, qz) + 2^28) >> 29
+// exactly (the dropped low 32 bits of pl*qz cannot carry across 2^61).
+// Same value as the oracle's 128-bit lf2o_fixed_weight.
 __device__ __forceinline__ uint64_t fixed_corner(uint32_t qx, uint32_t qy, uint32_t qz)
 {
-  const uint64_t p = (uint64_t)qx * (uint64_t)qy;          // <= 2^62
-  const uint64_t lo = p * (uint64_t)qz;
-  uint64_t hi = __umul64hi(p, (uint64_t)qz);
-  const uint64_t lo2 = lo + (1ull << 60);
-  hi += (lo2 < lo);
-  return (hi << 3) | (lo2 >> 61);
+  const uint64_t p = (uint64_t)qx * (uint64_t)qy;  // <= 2^62
+  const uint32_t ph = (uint32_t)(p >> 32), pl = (uint32_t)p;
+  const uint64_t hi = (uint64_t)ph * (uint64_t)qz + (uint64_t)__umulhi(pl, qz) + (1ull << 28);
+  return hi >> 29;
 }
 
 // Block-wide exclusive scan of one int per thread (blockDim.x <= 1024,

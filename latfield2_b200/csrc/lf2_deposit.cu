@@ -40,6 +40,49 @@ struct Comps<2> { static constexpr int value = 6; };
 
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
 
+// Fixed-point accumulation in shared memory.  Each 64-bit vertex sum is kept
+// as two 32-bit partial sums, lo = sum(q & 0xffff) and hi = sum(q >> 16), so
+// that every update is a native 32-bit shared-memory reduction; the sum is
+// lo + (hi << 16).  With q <= 2^32 per particle and corner, neither partial
+// sum can wrap while a brick holds at most 65535 particles (DEP_SPLIT_MAX);
+// larger bricks fall back to 64-bit shared atomics.
+constexpr int DEP_SPLIT_MAX = 65535;
+constexpr int DEP_ITEMS = 4;  // particles in flight per thread
+
+template <bool SPLIT>
+__device__ __forceinline__ void add_fixed(unsigned char* smem, int t, uint64_t q)
+{
+  if (SPLIT) {
+    uint32_t* lo = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* hi = lo + TILE3;
+    atomicAdd(&lo[t], (uint32_t)(q & 0xffffu));
+    atomicAdd(&hi[t], (uint32_t)(q >> 16));
+  } else {
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem) + t, (unsigned long long)q);
+  }
+}
+
+template <bool SPLIT>
+__device__ __forceinline__ void deposit_fixed_particle(unsigned char* smem, int t0, float fx,
+                                                       float fy, float fz, bool has_mass,
+                                                       uint64_t mq)
+{
+  // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle).
+  const uint32_t ux = __float2uint_rn(fx * 2147483648.0f);
+  const uint32_t uy = __float2uint_rn(fy * 2147483648.0f);
+  const uint32_t uz = __float2uint_rn(fz * 2147483648.0f);
+  const uint32_t qx[2] = {(1u << 31) - ux, ux};
+  const uint32_t qy[2] = {(1u << 31) - uy, uy};
+  const uint32_t qz[2] = {(1u << 31) - uz, uz};
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+    uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
+    if (has_mass) q = (q * mq + (1ull << 23)) >> 24;
+    add_fixed<SPLIT>(smem, t0 + cx + cy * TILE + cz * TILE * TILE, q);
+  }
+}
+
 template <int KIND, bool FIXED>
 __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositParams dp,
                                                          float* __restrict__ out,
@@ -47,9 +90,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
                                                          uint32_t* flags)
 {
   constexpr int C = Comps<KIND>::value;
-  using Acc = typename std::conditional<FIXED, unsigned long long, float>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Acc* acc = reinterpret_cast<Acc*>(smem_raw);  // [C][TILE3]
 
   const Geom& g = v.g;
   const int64_t b = blockIdx.x;
@@ -58,76 +99,95 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
   const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
             ez = brick_extent(g.n[2], bz);
   const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-
-  for (int t = threadIdx.x; t < C * TILE3; t += blockDim.x) acc[t] = 0;
-  __syncthreads();
-
   const int64_t base = v.seg_start[b];
   const int cnt = LF2_BRICK_COUNT(v, b);
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const int64_t p = base + i;
-    int x, y, z;
-    unpack_key(g, v.a.key[p], x, y, z);
-    const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
-    const float fx = v.a.ox[p], fy = v.a.oy[p], fz = v.a.oz[p];
-    if (KIND == 0 && FIXED) {
-      // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle).
-      const uint32_t ux = __float2uint_rn(fx * 2147483648.0f);
-      const uint32_t uy = __float2uint_rn(fy * 2147483648.0f);
-      const uint32_t uz = __float2uint_rn(fz * 2147483648.0f);
-      const uint32_t qx[2] = {(1u << 31) - ux, ux};
-      const uint32_t qy[2] = {(1u << 31) - uy, uy};
-      const uint32_t qz[2] = {(1u << 31) - uz, uz};
-      uint64_t mq = 0;
-      if (dp.has_mass) {
-        const float mr = __fmul_rn(v.a.mass[p], dp.inv_unit);
-        if (!(mr >= 0.0f && mr < 64.0f)) set_flag(flags, ERR_MASS_RANGE);
-        mq = (uint64_t)__float2uint_rn(fminf(fmaxf(mr, 0.0f), 63.0f) * 16777216.0f);
-      }
+  const bool split = FIXED && cnt <= DEP_SPLIT_MAX;
+
+  {
+    uint32_t* z = reinterpret_cast<uint32_t*>(smem_raw);
+    const int words = FIXED ? 2 * TILE3 : C * TILE3;
+    for (int t = threadIdx.x; t < words; t += blockDim.x) z[t] = 0u;
+  }
+  __syncthreads();
+
+  float* facc = reinterpret_cast<float*>(smem_raw);
+  for (int c0 = 0; c0 < cnt; c0 += DEP_ITEMS * DEP_THREADS) {
+    uint32_t key[DEP_ITEMS];
+    float fx[DEP_ITEMS], fy[DEP_ITEMS], fz[DEP_ITEMS], m[DEP_ITEMS];
+    float vx[DEP_ITEMS], vy[DEP_ITEMS], vz[DEP_ITEMS];
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-        uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
-        if (dp.has_mass) q = (q * mq + (1ull << 23)) >> 24;
-        atomicAdd(reinterpret_cast<unsigned long long*>(&acc[t0 + cx + cy * TILE + cz * TILE * TILE]),
-                  (unsigned long long)q);
+    for (int j = 0; j < DEP_ITEMS; j++) {
+      const int i = c0 + j * DEP_THREADS + threadIdx.x;
+      if (i < cnt) {
+        const int64_t p = base + i;
+        key[j] = v.a.key[p];
+        fx[j] = v.a.ox[p];
+        fy[j] = v.a.oy[p];
+        fz[j] = v.a.oz[p];
+        m[j] = dp.has_mass ? v.a.mass[p] : 0.0f;
+        if (KIND != 0) {
+          vx[j] = v.a.vx[p];
+          vy[j] = v.a.vy[p];
+          vz[j] = v.a.vz[p];
+        }
       }
-    } else {
-      float* facc = reinterpret_cast<float*>(acc);
-      const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy), gz = __fsub_rn(1.0f, fz);
-      const float mf = dp.has_mass ? __fmul_rn(v.a.mass[p], dp.inv_vol) : dp.mf;
+    }
+#pragma unroll
+    for (int j = 0; j < DEP_ITEMS; j++) {
+      const int i = c0 + j * DEP_THREADS + threadIdx.x;
+      if (i >= cnt) continue;
+      int x, y, z;
+      unpack_key(g, key[j], x, y, z);
+      const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
+      if (KIND == 0 && FIXED) {
+        uint64_t mq = 0;
+        if (dp.has_mass) {
+          const float mr = __fmul_rn(m[j], dp.inv_unit);
+          if (!(mr >= 0.0f && mr < 64.0f)) set_flag(flags, ERR_MASS_RANGE);
+          mq = (uint64_t)__float2uint_rn(fminf(fmaxf(mr, 0.0f), 63.0f) * 16777216.0f);
+        }
+        if (split)
+          deposit_fixed_particle<true>(smem_raw, t0, fx[j], fy[j], fz[j], dp.has_mass, mq);
+        else
+          deposit_fixed_particle<false>(smem_raw, t0, fx[j], fy[j], fz[j], dp.has_mass, mq);
+        continue;
+      }
+      const float gx = __fsub_rn(1.0f, fx[j]), gy = __fsub_rn(1.0f, fy[j]),
+                  gz = __fsub_rn(1.0f, fz[j]);
+      const float ox = fx[j], oy = fy[j], oz = fz[j];
+      const float mf = dp.has_mass ? __fmul_rn(m[j], dp.inv_vol) : dp.mf;
       if (KIND == 0) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
           const float w = __fmul_rn(
-              __fmul_rn(__fmul_rn(sel(cx, fx, gx), sel(cy, fy, gy)), sel(cz, fz, gz)), mf);
+              __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz)), mf);
           atomicAdd(&facc[t0 + cx + cy * TILE + cz * TILE * TILE], w);
         }
       } else if (KIND == 1) {
         // projections.hpp:501-544: component i is NGP along i, CIC across.
-        const float vxm = __fmul_rn(mf, v.a.vx[p]);
-        const float vym = __fmul_rn(mf, v.a.vy[p]);
-        const float vzm = __fmul_rn(mf, v.a.vz[p]);
+        const float vxm = __fmul_rn(mf, vx[j]);
+        const float vym = __fmul_rn(mf, vy[j]);
+        const float vzm = __fmul_rn(mf, vz[j]);
         constexpr int TY = TILE, TZ = TILE * TILE;
         float* a0 = facc;
         float* a1 = facc + TILE3;
         float* a2 = facc + 2 * TILE3;
         atomicAdd(&a0[t0], __fmul_rn(__fmul_rn(vxm, gy), gz));
-        atomicAdd(&a0[t0 + TY], __fmul_rn(__fmul_rn(vxm, fy), gz));
-        atomicAdd(&a0[t0 + TZ], __fmul_rn(__fmul_rn(vxm, gy), fz));
-        atomicAdd(&a0[t0 + TY + TZ], __fmul_rn(__fmul_rn(vxm, fy), fz));
+        atomicAdd(&a0[t0 + TY], __fmul_rn(__fmul_rn(vxm, oy), gz));
+        atomicAdd(&a0[t0 + TZ], __fmul_rn(__fmul_rn(vxm, gy), oz));
+        atomicAdd(&a0[t0 + TY + TZ], __fmul_rn(__fmul_rn(vxm, oy), oz));
         atomicAdd(&a1[t0], __fmul_rn(__fmul_rn(vym, gx), gz));
-        atomicAdd(&a1[t0 + 1], __fmul_rn(__fmul_rn(vym, fx), gz));
-        atomicAdd(&a1[t0 + TZ], __fmul_rn(__fmul_rn(vym, gx), fz));
-        atomicAdd(&a1[t0 + 1 + TZ], __fmul_rn(__fmul_rn(vym, fx), fz));
+        atomicAdd(&a1[t0 + 1], __fmul_rn(__fmul_rn(vym, ox), gz));
+        atomicAdd(&a1[t0 + TZ], __fmul_rn(__fmul_rn(vym, gx), oz));
+        atomicAdd(&a1[t0 + 1 + TZ], __fmul_rn(__fmul_rn(vym, ox), oz));
         atomicAdd(&a2[t0], __fmul_rn(__fmul_rn(vzm, gx), gy));
-        atomicAdd(&a2[t0 + 1], __fmul_rn(__fmul_rn(vzm, fx), gy));
-        atomicAdd(&a2[t0 + TY], __fmul_rn(__fmul_rn(vzm, gx), fy));
-        atomicAdd(&a2[t0 + 1 + TY], __fmul_rn(__fmul_rn(vzm, fx), fy));
+        atomicAdd(&a2[t0 + 1], __fmul_rn(__fmul_rn(vzm, ox), gy));
+        atomicAdd(&a2[t0 + TY], __fmul_rn(__fmul_rn(vzm, gx), oy));
+        atomicAdd(&a2[t0 + 1 + TY], __fmul_rn(__fmul_rn(vzm, ox), oy));
       } else {
         // projections.hpp:786-843: T_ii at the 8 vertices, T_ij on plaquettes.
-        const float vv[3] = {v.a.vx[p], v.a.vy[p], v.a.vz[p]};
+        const float vv[3] = {vx[j], vy[j], vz[j]};
         constexpr int diag[3] = {0, 3, 5};
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -137,7 +197,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
           for (int k = 0; k < 8; k++) {
             const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
             const float w = __fmul_rn(
-                __fmul_rn(__fmul_rn(mv2, sel(cx, fx, gx)), sel(cy, fy, gy)), sel(cz, fz, gz));
+                __fmul_rn(__fmul_rn(mv2, sel(cx, ox, gx)), sel(cy, oy, gy)), sel(cz, oz, gz));
             atomicAdd(&a[t0 + cx + cy * TILE + cz * TILE * TILE], w);
           }
         }
@@ -145,11 +205,11 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
         const float m02 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[2]);
         const float m12 = __fmul_rn(__fmul_rn(mf, vv[1]), vv[2]);
         atomicAdd(&facc[1 * TILE3 + t0], __fmul_rn(m01, gz));
-        atomicAdd(&facc[1 * TILE3 + t0 + TILE * TILE], __fmul_rn(m01, fz));
+        atomicAdd(&facc[1 * TILE3 + t0 + TILE * TILE], __fmul_rn(m01, oz));
         atomicAdd(&facc[2 * TILE3 + t0], __fmul_rn(m02, gy));
-        atomicAdd(&facc[2 * TILE3 + t0 + TILE], __fmul_rn(m02, fy));
+        atomicAdd(&facc[2 * TILE3 + t0 + TILE], __fmul_rn(m02, oy));
         atomicAdd(&facc[4 * TILE3 + t0], __fmul_rn(m12, gx));
-        atomicAdd(&facc[4 * TILE3 + t0 + 1], __fmul_rn(m12, fx));
+        atomicAdd(&facc[4 * TILE3 + t0 + 1], __fmul_rn(m12, ox));
       }
     }
   }
@@ -157,32 +217,31 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
 
   // Flush: interior vertices to the field, shell vertices to the shell store.
   uint64_t* sp = spill + (size_t)b * C * SHELL;
+  const uint32_t* lo = reinterpret_cast<const uint32_t*>(smem_raw);
+  const unsigned long long* a64 = reinterpret_cast<const unsigned long long*>(smem_raw);
   for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
     const int i = t % TILE, j = (t / TILE) % TILE, k = t / (TILE * TILE);
     if (i > ex || j > ey || k > ez) continue;
     const bool shell = i == 0 || i == ex || j == 0 || j == ey || k == 0 || k == ez;
+    if (FIXED) {
+      const uint64_t q = split ? (uint64_t)lo[t] + ((uint64_t)lo[TILE3 + t] << 16) : a64[t];
+      if (shell) {
+        sp[shell_index(i == ex ? BRICK : i, j == ey ? BRICK : j, k == ez ? BRICK : k)] = q;
+      } else {
+        if ((long long)q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+        out[site_index(g, x0 + i, y0 + j, z0 + k)] = __fmul_rn(__ll2float_rn((long long)q),
+                                                               dp.fixed_scale);
+      }
+      continue;
+    }
     if (shell) {
       const int si = shell_index(i == ex ? BRICK : i, j == ey ? BRICK : j, k == ez ? BRICK : k);
 #pragma unroll
-      for (int c = 0; c < C; c++) {
-        if (FIXED)
-          sp[c * SHELL + si] = (uint64_t)acc[c * TILE3 + t];
-        else
-          reinterpret_cast<float*>(sp)[c * SHELL + si] =
-              reinterpret_cast<const float*>(acc)[c * TILE3 + t];
-      }
+      for (int c = 0; c < C; c++) reinterpret_cast<float*>(sp)[c * SHELL + si] = facc[c * TILE3 + t];
     } else {
       const int64_t s = site_index(g, x0 + i, y0 + j, z0 + k);
 #pragma unroll
-      for (int c = 0; c < C; c++) {
-        if (FIXED) {
-          const long long q = (long long)acc[c * TILE3 + t];
-          if (q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-          out[c * g.nsites + s] = __fmul_rn(__ll2float_rn(q), dp.fixed_scale);
-        } else {
-          out[c * g.nsites + s] = reinterpret_cast<const float*>(acc)[c * TILE3 + t];
-        }
-      }
+      for (int c = 0; c < C; c++) out[c * g.nsites + s] = facc[c * TILE3 + t];
     }
   }
 }

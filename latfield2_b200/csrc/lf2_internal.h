@@ -83,6 +83,7 @@ struct lf2_ctx {
   unsigned long long* mov_count = nullptr;
   uint32_t* flags = nullptr;         // device error bits
   int32_t* repack = nullptr;         // device: 1 when a brick overflowed
+  unsigned long long* diag = nullptr; // device [2]: repacks, movers of the last drift
   float* brick_maxv2 = nullptr;      // [nbricks]
   double* brick_sums = nullptr;      // [nbricks * 5]
   double* stats = nullptr;           // [8] device

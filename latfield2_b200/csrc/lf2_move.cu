@@ -24,6 +24,8 @@ constexpr int MOVE_THREADS = 256;
 
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
 
+constexpr int MOVE_ITEMS = 4;  // particles in flight per thread
+
 template <bool KICK, bool DRIFT>
 __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float* __restrict__ F,
                                                        MoveParams mp, PartArrays mov,
@@ -39,72 +41,86 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
   int bx, by, bz;
   brick_coords(g, b, bx, by, bz);
   const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-
-  if (KICK) {
-    const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
-              ez = brick_extent(g.n[2], bz);
-    for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
-      const int i = t % TILE, j = (t / TILE) % TILE, k = t / (TILE * TILE);
-      if (i > ex || j > ey || k > ez) continue;
-      const int gx = x0 + i < g.n[0] ? x0 + i : 0;
-      const int gy = y0 + j < g.n[1] ? y0 + j : 0;
-      const int gz = z0 + k < g.n[2] ? z0 + k : 0;
-      const int64_t s = site_index(g, gx, gy, gz);
-      ftile[t] = __ldg(F + s);
-      ftile[TILE3 + t] = __ldg(F + g.nsites + s);
-      ftile[2 * TILE3 + t] = __ldg(F + 2 * g.nsites + s);
-    }
-    __syncthreads();
-  }
-
   const int64_t base = v.seg_start[b];
   const int cnt = LF2_BRICK_COUNT(v, b);
+
   int write = 0;
   float maxv2 = 0.0f;
   const int lane = threadIdx.x & 31;
 
-  for (int c0 = 0; c0 < cnt; c0 += blockDim.x) {
-    const int i = c0 + threadIdx.x;
-    const bool active = i < cnt;
-    const int64_t p = base + i;
-    uint32_t key = 0;
-    float ox = 0.f, oy = 0.f, oz = 0.f, vx = 0.f, vy = 0.f, vz = 0.f, m = 0.f;
-    int64_t id = 0;
-    bool stay = true;
-    if (active) {
-      key = v.a.key[p];
-      ox = v.a.ox[p];
-      oy = v.a.oy[p];
-      oz = v.a.oz[p];
-      vx = v.a.vx[p];
-      vy = v.a.vy[p];
-      vz = v.a.vz[p];
-      if (DRIFT && v.a.mass) m = v.a.mass[p];
-      if (DRIFT && v.a.id) id = v.a.id[p];
+  for (int c0 = 0; c0 < cnt; c0 += MOVE_ITEMS * MOVE_THREADS) {
+    uint32_t key[MOVE_ITEMS];
+    float ox[MOVE_ITEMS], oy[MOVE_ITEMS], oz[MOVE_ITEMS];
+    float vx[MOVE_ITEMS], vy[MOVE_ITEMS], vz[MOVE_ITEMS], m[MOVE_ITEMS];
+    int64_t id[MOVE_ITEMS];
+    bool act[MOVE_ITEMS], stay[MOVE_ITEMS];
+#pragma unroll
+    for (int j = 0; j < MOVE_ITEMS; j++) {
+      const int i = c0 + j * MOVE_THREADS + threadIdx.x;
+      act[j] = i < cnt;
+      stay[j] = true;
+      m[j] = 0.0f;
+      id[j] = 0;
+      if (act[j]) {
+        const int64_t p = base + i;
+        key[j] = v.a.key[p];
+        ox[j] = v.a.ox[p];
+        oy[j] = v.a.oy[p];
+        oz[j] = v.a.oz[p];
+        vx[j] = v.a.vx[p];
+        vy[j] = v.a.vy[p];
+        vz[j] = v.a.vz[p];
+        if (DRIFT && v.a.mass) m[j] = v.a.mass[p];
+        if (DRIFT && v.a.id) id[j] = v.a.id[p];
+      }
+    }
+    if (KICK && c0 == 0) {
+      // The brick's vertex tile of F, loaded while the first chunk's particle
+      // loads are in flight; empty bricks never load it.
+      const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+                ez = brick_extent(g.n[2], bz);
+      for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
+        const int i = t % TILE, jj = (t / TILE) % TILE, k = t / (TILE * TILE);
+        if (i > ex || jj > ey || k > ez) continue;
+        const int gx = x0 + i < g.n[0] ? x0 + i : 0;
+        const int gy = y0 + jj < g.n[1] ? y0 + jj : 0;
+        const int gz = z0 + k < g.n[2] ? z0 + k : 0;
+        const int64_t s = site_index(g, gx, gy, gz);
+        ftile[t] = __ldg(F + s);
+        ftile[TILE3 + t] = __ldg(F + g.nsites + s);
+        ftile[2 * TILE3 + t] = __ldg(F + 2 * g.nsites + s);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < MOVE_ITEMS; j++) {
+      if (!act[j]) continue;
       int x, y, z;
-      unpack_key(g, key, x, y, z);
+      unpack_key(g, key[j], x, y, z);
       if (KICK) {
         const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
-        const float gx = __fsub_rn(1.0f, ox), gy = __fsub_rn(1.0f, oy), gz = __fsub_rn(1.0f, oz);
+        const float gx = __fsub_rn(1.0f, ox[j]), gy = __fsub_rn(1.0f, oy[j]),
+                    gz = __fsub_rn(1.0f, oz[j]);
         float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-          const float w = __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz));
+          const float w = __fmul_rn(__fmul_rn(sel(cx, ox[j], gx), sel(cy, oy[j], gy)),
+                                    sel(cz, oz[j], gz));
           const int t = t0 + cx + cy * TILE + cz * TILE * TILE;
           a0 = __fmaf_rn(w, ftile[t], a0);
           a1 = __fmaf_rn(w, ftile[TILE3 + t], a1);
           a2 = __fmaf_rn(w, ftile[2 * TILE3 + t], a2);
         }
-        vx = __fmaf_rn(mp.dtk, a0, vx);
-        vy = __fmaf_rn(mp.dtk, a1, vy);
-        vz = __fmaf_rn(mp.dtk, a2, vz);
+        vx[j] = __fmaf_rn(mp.dtk, a0, vx[j]);
+        vy[j] = __fmaf_rn(mp.dtk, a1, vy[j]);
+        vz[j] = __fmaf_rn(mp.dtk, a2, vz[j]);
       }
-      maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
-                                     __fmul_rn(vz, vz)));
+      maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx[j], vx[j]), __fmul_rn(vy[j], vy[j])),
+                                     __fmul_rn(vz[j], vz[j])));
       if (DRIFT) {
-        float o[3] = {ox, oy, oz};
-        const float vv[3] = {vx, vy, vz};
+        float o[3] = {ox[j], oy[j], oz[j]};
+        const float vv[3] = {vx[j], vy[j], vz[j]};
         int xyz[3] = {x, y, z};
         bool finite = true;
 #pragma unroll
@@ -125,11 +141,11 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
           xyz[d] = wrap_add(xyz[d], carry, g.n[d]);
         }
         if (finite) {
-          ox = o[0];
-          oy = o[1];
-          oz = o[2];
-          key = pack_key(g, xyz[0], xyz[1], xyz[2]);
-          stay = brick_of(g, xyz[0], xyz[1], xyz[2]) == b;
+          ox[j] = o[0];
+          oy[j] = o[1];
+          oz[j] = o[2];
+          key[j] = pack_key(g, xyz[0], xyz[1], xyz[2]);
+          stay[j] = brick_of(g, xyz[0], xyz[1], xyz[2]) == b;
         } else {
           set_flag(flags, ERR_NONFINITE);
         }
@@ -137,47 +153,58 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
     }
 
     if (!DRIFT) {
-      if (active) {
-        v.a.vx[p] = vx;
-        v.a.vy[p] = vy;
-        v.a.vz[p] = vz;
+#pragma unroll
+      for (int j = 0; j < MOVE_ITEMS; j++) {
+        if (!act[j]) continue;
+        const int64_t p = base + c0 + j * MOVE_THREADS + threadIdx.x;
+        v.a.vx[p] = vx[j];
+        v.a.vy[p] = vy[j];
+        v.a.vz[p] = vz[j];
       }
       continue;
     }
 
-    // All loads of this chunk are complete before any slot is overwritten.
+    // All loads of this chunk are complete before any slot is overwritten:
+    // stayers of this chunk land below the start of the next chunk.
+    int mine = 0;
+#pragma unroll
+    for (int j = 0; j < MOVE_ITEMS; j++) mine += (act[j] && stay[j]) ? 1 : 0;
     int total;
-    const int rank = block_exclusive_scan(active && stay ? 1 : 0, s_scan, &total);
-    if (active && stay) {
-      const int64_t q = base + write + rank;
-      v.a.key[q] = key;
-      v.a.ox[q] = ox;
-      v.a.oy[q] = oy;
-      v.a.oz[q] = oz;
-      v.a.vx[q] = vx;
-      v.a.vy[q] = vy;
-      v.a.vz[q] = vz;
-      if (v.a.mass) v.a.mass[q] = m;
-      if (v.a.id) v.a.id[q] = id;
-    }
-    const bool leave = active && !stay;
-    const unsigned bal = __ballot_sync(0xffffffffu, leave);
-    if (bal) {
-      const int leader = __ffs(bal) - 1;
-      unsigned long long s0 = 0;
-      if (lane == leader) s0 = atomicAdd(mov_count, (unsigned long long)__popc(bal));
-      s0 = __shfl_sync(0xffffffffu, s0, leader);
-      if (leave) {
-        const int64_t q = (int64_t)s0 + __popc(bal & ((1u << lane) - 1u));
-        mov.key[q] = key;
-        mov.ox[q] = ox;
-        mov.oy[q] = oy;
-        mov.oz[q] = oz;
-        mov.vx[q] = vx;
-        mov.vy[q] = vy;
-        mov.vz[q] = vz;
-        if (mov.mass) mov.mass[q] = m;
-        if (mov.id) mov.id[q] = id;
+    int q0 = block_exclusive_scan(mine, s_scan, &total);
+#pragma unroll
+    for (int j = 0; j < MOVE_ITEMS; j++) {
+      if (act[j] && stay[j]) {
+        const int64_t q = base + write + q0;
+        q0++;
+        v.a.key[q] = key[j];
+        v.a.ox[q] = ox[j];
+        v.a.oy[q] = oy[j];
+        v.a.oz[q] = oz[j];
+        v.a.vx[q] = vx[j];
+        v.a.vy[q] = vy[j];
+        v.a.vz[q] = vz[j];
+        if (v.a.mass) v.a.mass[q] = m[j];
+        if (v.a.id) v.a.id[q] = id[j];
+      }
+      const bool leave = act[j] && !stay[j];
+      const unsigned bal = __ballot_sync(0xffffffffu, leave);
+      if (bal) {
+        const int leader = __ffs(bal) - 1;
+        unsigned long long s0 = 0;
+        if (lane == leader) s0 = atomicAdd(mov_count, (unsigned long long)__popc(bal));
+        s0 = __shfl_sync(0xffffffffu, s0, leader);
+        if (leave) {
+          const int64_t q = (int64_t)s0 + __popc(bal & ((1u << lane) - 1u));
+          mov.key[q] = key[j];
+          mov.ox[q] = ox[j];
+          mov.oy[q] = oy[j];
+          mov.oz[q] = oz[j];
+          mov.vx[q] = vx[j];
+          mov.vy[q] = vy[j];
+          mov.vz[q] = vz[j];
+          if (mov.mass) mov.mass[q] = m[j];
+          if (mov.id) mov.id[q] = id[j];
+        }
       }
     }
     write += total;

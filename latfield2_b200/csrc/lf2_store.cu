@@ -238,15 +238,18 @@ __device__ inline void copy_particle(const PartArrays& s, int64_t ps, const Part
   if (d.id) d.id[pd] = s.id[ps];
 }
 
+// The per-brick repack kernels run on a small grid (grid-stride over bricks)
+// so that returning early costs a few microseconds, not one CTA per brick.
 __global__ void k_repack_copy_out(StoreView v, PartArrays alt, const int64_t* __restrict__ start_alt,
                                   int32_t* fill, const int32_t* repack)
 {
   if (*repack == 0) return;
-  const int64_t b = blockIdx.x;
-  const int placed = min(v.count[b], v.cap[b]);
-  const int64_t s0 = v.seg_start[b], d0 = start_alt[b];
-  for (int i = threadIdx.x; i < placed; i += blockDim.x) copy_particle(v.a, s0 + i, alt, d0 + i);
-  if (threadIdx.x == 0) fill[b] = placed;
+  for (int64_t b = blockIdx.x; b < v.g.nbricks; b += gridDim.x) {
+    const int placed = min(v.count[b], v.cap[b]);
+    const int64_t s0 = v.seg_start[b], d0 = start_alt[b];
+    for (int i = threadIdx.x; i < placed; i += blockDim.x) copy_particle(v.a, s0 + i, alt, d0 + i);
+    if (threadIdx.x == 0) fill[b] = placed;
+  }
 }
 
 __global__ void k_repack_movers(Geom g, PartArrays mov, const int32_t* __restrict__ placed,
@@ -270,11 +273,12 @@ __global__ void k_repack_copy_back(StoreView v, PartArrays alt, const int64_t* _
                                    const int32_t* __restrict__ fill, const int32_t* repack)
 {
   if (*repack == 0) return;
-  const int64_t b = blockIdx.x;
-  const int n = fill[b];
-  const int64_t d0 = start_alt[b];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) copy_particle(alt, d0 + i, v.a, d0 + i);
-  if (threadIdx.x == 0) v.count[b] = n;
+  for (int64_t b = blockIdx.x; b < v.g.nbricks; b += gridDim.x) {
+    const int n = fill[b];
+    const int64_t d0 = start_alt[b];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) copy_particle(alt, d0 + i, v.a, d0 + i);
+    if (threadIdx.x == 0) v.count[b] = n;
+  }
 }
 
 __global__ void k_repack_finish(int64_t nb, const int64_t* __restrict__ start_alt,
@@ -289,12 +293,15 @@ __global__ void k_repack_finish(int64_t nb, const int64_t* __restrict__ start_al
   }
 }
 
-__global__ void k_repack_clear(int32_t* repack, uint32_t* flags)
+__global__ void k_repack_clear(int32_t* repack, uint32_t* flags, unsigned long long* diag,
+                               const unsigned long long* mov_count)
 {
   if (*repack) {
     set_flag(flags, ERR_REPACK);
+    diag[0] += 1;
     *repack = 0;
   }
+  diag[1] = *mov_count;
 }
 
 inline int grid_for(int64_t n, int threads)
@@ -388,16 +395,17 @@ cudaError_t launch_repack(lf2_ctx* c)
   const int64_t nb = c->g.nbricks;
   k_repack_caps<<<1, 1024, 0, c->stream>>>(nb, c->count, c->cap_alt, c->seg_start_alt, c->capacity,
                                            c->repack, c->flags);
-  k_repack_copy_out<<<(unsigned)nb, 256, 0, c->stream>>>(view(c), c->alt, c->seg_start_alt, c->fill,
-                                                         c->repack);
+  const unsigned small = (unsigned)(nb < 148 * 8 ? nb : 148 * 8);
+  k_repack_copy_out<<<small, 256, 0, c->stream>>>(view(c), c->alt, c->seg_start_alt, c->fill,
+                                                  c->repack);
   k_repack_movers<<<148 * 4, 256, 0, c->stream>>>(c->g, c->mov, c->mov_placed, c->mov_count, c->alt,
                                                   c->seg_start_alt, c->fill, c->repack);
-  k_repack_copy_back<<<(unsigned)nb, 256, 0, c->stream>>>(view(c), c->alt, c->seg_start_alt,
-                                                          c->fill, c->repack);
-  k_repack_finish<<<grid_for(nb + 1, 256), 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt,
+  k_repack_copy_back<<<small, 256, 0, c->stream>>>(view(c), c->alt, c->seg_start_alt, c->fill,
+                                                   c->repack);
+  k_repack_finish<<<small, 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt,
                                                                 c->seg_start, c->cap, c->repack,
                                                                 c->flags);
-  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags);
+  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag, c->mov_count);
   return cudaGetLastError();
 }
 
