@@ -177,6 +177,39 @@ lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
 lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
                             double* max_v);
 
+/* ---------------------------------------------------------- no allocation
+ * Scalar CIC deposit that allocates no device memory.  It has no
+ * counterpart in the reference; it exists for callers that may not allocate
+ * device memory while running (an application whose device memory comes
+ * from its own pool, a plugin allowed to allocate only at load time, a
+ * time-critical loop that cannot pay for cudaMalloc's synchronisation).
+ * No context is needed: the caller passes device inputs and the output.
+ *   cell[np], off3[3*np]  particles grouped by brick: brick b (BRICK^3 = 16^3
+ *                         cells; bricks numbered bx + nbx*(by + nby*bz),
+ *                         nbi = ceil(n[i]/16)) owns entries
+ *                         [brick_start[b], brick_start[b+1]); cells and
+ *                         offsets as in lf2_particles_set
+ *   brick_start[nb+1]     int64, device
+ *   rho[n0*n1*n2]         FP32 output, internal layout, overwritten
+ * Mass is global (particle_mass); deposit_mode as for lf2_create.  The
+ * scratch (the per-brick shell store) is a fixed 16 MiB device array inside
+ * the library, present on every GPU that loads it until the process exits,
+ * so lattices with more than LF2_NOALLOC_MAX_BRICKS bricks are rejected with
+ * LF2_ERR_UNSUPPORTED.  The first call on a device looks the array's device
+ * address up (once per device, with that device current); make that first
+ * call before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU race and must be serialised.  The work is queued on `stream`
+ * (NULL: default stream); with flags != NULL the call waits for it and
+ * returns the device error bits (LF2_FLAG_BAD_CELL for a particle outside
+ * its brick or with an offset outside [0,1)), with LF2_ERR_STATE if any. */
+#define LF2_NOALLOC_MAX_BRICKS 1363
+lf2_status lf2_deposit_scalar_noalloc(const int n[3], const double box[3],
+                                      int deposit_mode, double particle_mass,
+                                      int64_t np, const int32_t* cell,
+                                      const float* off3,
+                                      const int64_t* brick_start, float* rho,
+                                      void* stream, uint32_t* flags);
+
 /* ------------------------------------------------------------- measurement
  * Per-phase device time, measured with CUDA events recorded on the context's
  * stream around each kernel (no extra synchronisation while running).

@@ -27,6 +27,7 @@ FLAG_MASS_RANGE = 0x4
 FLAG_REPACK = 0x8
 FLAG_CAPACITY = 0x10
 FLAG_FIXED_OVERFLOW = 0x20
+NOALLOC_MAX_BRICKS = 1363
 
 c_void_p = ctypes.c_void_p
 c_int = ctypes.c_int
@@ -70,6 +71,8 @@ SIGNATURES = {
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
     "lf2_kernel_launches": [c_void_p, P(c_i64)],
     "lf2_rebin_stats": [c_void_p, P(c_i64), P(c_i64)],
+    "lf2_deposit_scalar_noalloc": [P(c_int), P(c_double), c_int, c_double, c_i64, c_void_p,
+                                   c_void_p, c_void_p, c_void_p, c_void_p, P(ctypes.c_uint32)],
 }
 NPHASE = 5
 PHASES = ("move", "insert_repack", "deposit_tile", "deposit_fixup", "other")
