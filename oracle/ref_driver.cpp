@@ -1,0 +1,250 @@
+// ref_driver.cpp -- runs the reference's own particle path on given inputs and
+// writes its results, to pin the oracle and the golden fixtures.
+// TEST INFRASTRUCTURE ONLY (built by oracle/build_ref.sh into oracle/_ref/).
+//
+// It includes the reference headers unmodified (LATfield2.hpp) with the
+// builder-written MPI stand-in (mpi_shim/mpi.h).  Two things are added around
+// them, both outside the reference sources:
+//  - a partList<part_simple> specialisation that also answers `.size != 0`:
+//    vectorProjectionCICNGP_project and symtensorProjectionCICNGP_project
+//    test `parts->field()(xPart).size != 0` (projections.hpp:473, :761), a
+//    member the shipped partList no longer has (LATfield2_Particles.hpp:
+//    97-103); here it means "the list is not empty", the intent of the test;
+//  - the CIC gather-kick callback for updateVel (the reference ships only the
+//    no-op updateVel_simple), the same arithmetic as the oracle's
+//    lf2o_update_vel_cic.
+//
+// Input  (little endian): "LF2G", int32 version=1, int32 n, int32 halo,
+//        int32 grid0, int32 grid1, double box, double gmass, int32 ops,
+//        double dtau_kick, double dtau_move, int64 np,
+//        np x {int64 id; double pos[3]; double vel[3]},
+//        if ops & OP_KICK: n^3 x 3 doubles, the force field F[z][y][x][c].
+// Output (one file per rank, <prefix>.<rank>): int32 rank, int32 coordSkip0
+//        (z offset), int32 coordSkip1 (y offset), int32 sizeLocal[3], int32 halo,
+//        then per op in bit order: the local gross field (double) for each
+//        deposit and for the halo-filled F; for the kick: double max_v,
+//        int64 nloc, nloc x {id, pos[3], vel[3]}; for the move: int64 nloc,
+//        nloc x {id, pos[3], vel[3]}.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "LATfield2.hpp"
+
+using namespace LATfield2;
+
+struct part_simple_dataType {};
+
+namespace LATfield2 {
+template <>
+struct partList<part_simple> {
+  struct NonEmpty {
+    bool operator!=(int v) const
+    {
+      const partList* self = reinterpret_cast<const partList*>(this);
+      return v == 0 ? !self->parts.empty() : true;
+    }
+  } size;  // first member: its address is the list's address
+  std::forward_list<part_simple> parts;
+  partList() : size(), parts() {}
+};
+}  // namespace LATfield2
+
+enum { OP_SCALAR = 1, OP_VECTOR = 2, OP_TENSOR = 4, OP_HALO = 8, OP_KICK = 16, OP_MOVE = 32 };
+
+// CIC gather of the 3-component field at the cell corners and kick, in the
+// callback signature of Particles::updateVel (LATfield2_Particles.hpp:753).
+Real cic_kick(double dtau, double lat_resolution, part_simple* part, double* frac,
+              part_simple_info info, Field<Real>** fields, Site* sites, int nfield,
+              double* params, double* outputs, int noutputs)
+{
+  Field<Real>& F = *fields[0];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < 8; k++) {
+    const int b[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+    double w = 1.0;
+    Site c = sites[0];
+    for (int l = 0; l < 3; l++) {
+      w *= b[l] ? frac[l] : 1.0 - frac[l];
+      if (b[l]) c = c + l;
+    }
+    for (int cc = 0; cc < 3; cc++) acc[cc] += w * F(c, cc);
+  }
+  double v2 = 0.0;
+  for (int cc = 0; cc < 3; cc++) {
+    part->vel[cc] += dtau * acc[cc];
+    v2 += (double)part->vel[cc] * (double)part->vel[cc];
+  }
+  if (noutputs > 0) outputs[0] = v2;
+  return v2;
+}
+
+template <typename T>
+static void rd(FILE* f, T* p, size_t n)
+{
+  if (fread(p, sizeof(T), n, f) != n) {
+    fprintf(stderr, "ref_driver: short input\n");
+    exit(2);
+  }
+}
+
+template <typename T>
+static void wr(FILE* f, const T* p, size_t n)
+{
+  fwrite(p, sizeof(T), n, f);
+}
+
+static void write_field(FILE* o, Field<Real>& f)
+{
+  const long gross = f.lattice().sitesLocalGross() * (long)f.components();
+  std::vector<double> buf(gross);
+  for (long i = 0; i < gross; i++) buf[i] = (double)f(i);
+  wr(o, buf.data(), buf.size());
+}
+
+static void write_particles(FILE* o, Particles<part_simple, part_simple_info, part_simple_dataType>& parts)
+{
+  std::vector<double> rec;
+  std::vector<int64_t> ids;
+  Site x(parts.lattice());
+  for (x.first(); x.test(); x.next())
+    for (auto it = parts.field()(x).parts.begin(); it != parts.field()(x).parts.end(); ++it) {
+      ids.push_back(it->ID);
+      for (int l = 0; l < 3; l++) rec.push_back((double)it->pos[l]);
+      for (int l = 0; l < 3; l++) rec.push_back((double)it->vel[l]);
+    }
+  const int64_t n = (int64_t)ids.size();
+  wr(o, &n, 1);
+  for (int64_t i = 0; i < n; i++) {
+    wr(o, &ids[i], 1);
+    wr(o, &rec[6 * i], 6);
+  }
+}
+
+int main(int argc, char** argv)
+{
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s input.bin output_prefix\n", argv[0]);
+    return 2;
+  }
+  FILE* in = fopen(argv[1], "rb");
+  if (!in) {
+    perror("input");
+    return 2;
+  }
+  char magic[4];
+  rd(in, magic, 4);
+  int32_t version, n, halo, g0, g1, ops;
+  double box, gmass, dtk, dtm;
+  int64_t np;
+  rd(in, &version, 1);
+  rd(in, &n, 1);
+  rd(in, &halo, 1);
+  rd(in, &g0, 1);
+  rd(in, &g1, 1);
+  rd(in, &box, 1);
+  rd(in, &gmass, 1);
+  rd(in, &ops, 1);
+  rd(in, &dtk, 1);
+  rd(in, &dtm, 1);
+  rd(in, &np, 1);
+  if (memcmp(magic, "LF2G", 4) != 0 || version != 1) {
+    fprintf(stderr, "ref_driver: bad input header\n");
+    return 2;
+  }
+
+  parallel.initialize(g0, g1);
+
+  Lattice lat_part(3, n, 0);
+  Lattice lat(3, n, halo);
+  Real boxSize[3] = {(Real)box, (Real)box, (Real)box};
+  part_simple_info info;
+  info.mass = gmass;
+  info.relativistic = 0;
+  set_parts_typename(&info, "part_simple");
+  part_simple_dataType dtype;
+  Particles<part_simple, part_simple_info, part_simple_dataType> parts;
+  parts.initialize(info, dtype, &lat_part, boxSize);
+
+  for (int64_t i = 0; i < np; i++) {
+    int64_t id;
+    double pv[6];
+    rd(in, &id, 1);
+    rd(in, pv, 6);
+    part_simple p;
+    p.ID = id;
+    for (int l = 0; l < 3; l++) {
+      p.pos[l] = (Real)pv[l];
+      p.vel[l] = (Real)pv[3 + l];
+    }
+    parts.addParticle_global(p);
+  }
+
+  Field<Real> F(lat, 3);
+  if (ops & (OP_HALO | OP_KICK)) {
+    std::vector<double> Fg((size_t)n * n * n * 3);
+    rd(in, Fg.data(), Fg.size());
+    Site x(lat);
+    for (x.first(); x.test(); x.next()) {
+      const long gx = x.coord(0), gy = x.coord(1), gz = x.coord(2);
+      for (int c = 0; c < 3; c++) F(x, c) = (Real)Fg[((gz * n + gy) * (size_t)n + gx) * 3 + c];
+    }
+    F.updateHalo();
+  }
+  fclose(in);
+
+  const std::string out_name = std::string(argv[2]) + "." + std::to_string(parallel.rank());
+  FILE* o = fopen(out_name.c_str(), "wb");
+  if (!o) {
+    perror("output");
+    return 3;
+  }
+  const int32_t rank = parallel.rank();
+  const int32_t skip0 = (int32_t)lat.coordSkip()[0], skip1 = (int32_t)lat.coordSkip()[1];
+  const int32_t sl[3] = {lat.sizeLocal(0), lat.sizeLocal(1), lat.sizeLocal(2)};
+  wr(o, &rank, 1);
+  wr(o, &skip0, 1);
+  wr(o, &skip1, 1);
+  wr(o, sl, 3);
+  wr(o, &halo, 1);
+
+  if (ops & OP_SCALAR) {
+    Field<Real> rho(lat, 1);
+    projection_init(&rho);
+    scalarProjectionCIC_project(&parts, &rho);
+    scalarProjectionCIC_comm(&rho);
+    write_field(o, rho);
+  }
+  if (ops & OP_VECTOR) {
+    Field<Real> B(lat, 3);
+    projection_init(&B);
+    vectorProjectionCICNGP_project(&parts, &B);
+    vectorProjectionCICNGP_comm(&B);
+    write_field(o, B);
+  }
+  if (ops & OP_TENSOR) {
+    Field<Real> T(lat, 3, 3, symmetric);
+    projection_init(&T);
+    symtensorProjectionCICNGP_project(&parts, &T);
+    symtensorProjectionCICNGP_comm(&T);
+    write_field(o, T);
+  }
+  if (ops & OP_HALO) write_field(o, F);
+  if (ops & OP_KICK) {
+    Field<Real>* fl[1] = {&F};
+    double out1[1];
+    int red[1] = {SUM};
+    const double maxv = parts.updateVel(&cic_kick, dtk, fl, 1, NULL, out1, red, 1);
+    wr(o, &maxv, 1);
+    write_particles(o, parts);
+  }
+  if (ops & OP_MOVE) {
+    parts.moveParticles(&move_particles_simple, dtm);
+    write_particles(o, parts);
+  }
+  fclose(o);
+  return 0;
+}

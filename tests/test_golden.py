@@ -1,0 +1,112 @@
+"""Pins the oracle (layer A) against the reference itself: the fixtures in
+tests/golden/ hold outputs of the reference's own particle path compiled
+from its sources (see tests/golden/make_golden.py).
+
+Single-rank cases must match bit for bit: the oracle restates the reference's
+arithmetic statement by statement and rebuilds its per-cell list order.  The
+2x2-rank case folds the halos through messages in a different order, so its
+deposits are compared to a tight tolerance; its moves are bit-exact.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(glob.glob(os.path.join(HERE, "*.npz")))
+
+
+def load(path):
+    return dict(np.load(path))
+
+
+def real_of(path):
+    return (np.float32, "f") if path.endswith("_single.npz") else (np.float64, "d")
+
+
+def ref_cells(n, posR, R):
+    """getPartCoord: (int)floor(pos * N) % N in the build's Real
+    (LATfield2_Particles.hpp:463-467)."""
+    u = np.floor(posR * R(n)).astype(np.int64) % n
+    return (u[:, 0] + n * (u[:, 1] + n * u[:, 2])).astype(np.int32)
+
+
+def test_fixtures_present():
+    names = {os.path.basename(p) for p in CASES}
+    for case in ("uniform8", "clustered12", "ranks16"):
+        for b in ("double", "single"):
+            assert f"{case}_{b}.npz" in names
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
+def test_oracle_matches_reference(path):
+    g = load(path)
+    R, prec = real_of(path)
+    n = int(g["n"])
+    halo = int(g["halo"])
+    nn = (n, n, n)
+    single_rank = int(np.prod(g["grid"])) == 1
+    res = R(1.0) / R(n)  # get_lattice_resolution in Real (particles_tools.hpp:6-19)
+    posR = g["pos"].astype(R)
+    velR = g["vel"].astype(R)
+    ids = g["ids"]
+    cell = ref_cells(n, posR, R)
+    cs, order = O.lists_from_insertion(nn, cell)
+    pos_l, vel_l, ids_l = posR[order], velR[order].copy(), ids[order]
+
+    tol = 0.0 if single_rank else (1e-13 if prec == "d" else 1e-6)
+    for key, fn in (("rho", O.scalar_cic), ("vec", O.vector_cicngp), ("ten", O.symtensor_cicngp)):
+        if key not in g:
+            continue
+        if key == "rho":
+            f = fn(nn, halo, res, cs, pos_l.astype(np.float64 if prec == "d" else np.float32),
+                   None, float(g["gmass"]), prec=prec)
+        else:
+            f = fn(nn, halo, res, cs, pos_l, vel_l, None, float(g["gmass"]), prec=prec)
+        got = f[halo:halo + n, halo:halo + n, halo:halo + n, :]
+        want = g[key]
+        if tol == 0.0:
+            np.testing.assert_array_equal(got.astype(np.float64), want, err_msg=key)
+        else:
+            scale = np.abs(want).max()
+            assert np.abs(got - want).max() <= tol * scale, key
+
+    if "F_halo" in g:
+        F = O.projection_init(nn, halo, 3, prec)
+        F[halo:halo + n, halo:halo + n, halo:halo + n, :] = g["F"].astype(R)
+        O.update_halo(F, nn, halo, prec)
+        np.testing.assert_array_equal(F.astype(np.float64), g["F_halo"])
+
+    if "kick_vel" in g:
+        Fh = O.projection_init(nn, halo, 3, prec)
+        Fh[halo:halo + n, halo:halo + n, halo:halo + n, :] = g["F"].astype(R)
+        O.update_halo(Fh, nn, halo, prec)
+        maxv, _ = O.update_vel_cic(nn, halo, cs, pos_l, vel_l, Fh, float(g["dtau_kick"]), prec)
+        k = np.argsort(ids_l)
+        np.testing.assert_array_equal(ids_l[k], g["kick_id"])
+        np.testing.assert_array_equal(vel_l[k].astype(np.float64), g["kick_vel"])
+        np.testing.assert_array_equal(pos_l[k].astype(np.float64), g["kick_pos"])
+        assert maxv == g["maxv"]
+
+    if "move_pos" in g:
+        # moveParticles(move_particles_simple) after the kick, on the 2x2 grid
+        k = np.argsort(ids_l)
+        p = pos_l[k].copy()
+        v = vel_l[k]
+        O.move_simple(nn, R(1.0), p, v, float(g["dtau_move"]), prec)
+        np.testing.assert_array_equal(g["move_id"], np.sort(ids))
+        np.testing.assert_array_equal(p.astype(np.float64), g["move_pos"])
+        np.testing.assert_array_equal(v.astype(np.float64), g["move_vel"])
+
+
+def test_reference_conserves_mass_in_every_fixture():
+    for path in CASES:
+        g = load(path)
+        n = int(g["n"])
+        if "rho" in g:
+            R, prec = real_of(path)
+            tol = 1e-12 if prec == "d" else 1e-5
+            assert g["rho"].sum() / n ** 3 == pytest.approx(1.0, rel=tol), path
