@@ -224,10 +224,11 @@ lf2_status lf2_profile_enable(lf2_ctx* ctx, int on);
 lf2_status lf2_profile_read(lf2_ctx* ctx, double* ms, int64_t* launches);
 /* Total kernel launches since the context was created. */
 lf2_status lf2_kernel_launches(lf2_ctx* ctx, int64_t* n);
-/* Rebin diagnostics (synchronises): number of store repacks since the
- * context was created and the number of particles that changed brick in the
- * last drift. */
-lf2_status lf2_rebin_stats(lf2_ctx* ctx, int64_t* repacks, int64_t* movers);
+/* Rebin diagnostics (synchronises): full store repacks and single-brick
+ * relocations since the context was created, and the number of particles
+ * that changed brick in the last drift.  Any pointer may be NULL. */
+lf2_status lf2_rebin_stats(lf2_ctx* ctx, int64_t* repacks, int64_t* relocations,
+                           int64_t* movers);
 
 #ifdef __cplusplus
 }

@@ -70,7 +70,7 @@ SIGNATURES = {
     "lf2_profile_enable": [c_void_p, c_int],
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
     "lf2_kernel_launches": [c_void_p, P(c_i64)],
-    "lf2_rebin_stats": [c_void_p, P(c_i64), P(c_i64)],
+    "lf2_rebin_stats": [c_void_p, P(c_i64), P(c_i64), P(c_i64)],
     "lf2_deposit_scalar_noalloc": [P(c_int), P(c_double), c_int, c_double, c_i64, c_void_p,
                                    c_void_p, c_void_p, c_void_p, c_void_p, P(ctypes.c_uint32)],
 }

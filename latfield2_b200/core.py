@@ -240,10 +240,12 @@ class Context:
         return {p: (ms[i], ln[i]) for i, p in enumerate(_lib.PHASES)}
 
     def rebin_stats(self):
-        """(repacks since creation, particles that changed brick in the last drift)."""
-        r, m = _c.c_int64(), _c.c_int64()
-        self._check(_lib.load().lf2_rebin_stats(self.h, _c.byref(r), _c.byref(m)), "rebin_stats")
-        return r.value, m.value
+        """(full repacks, single-brick relocations, particles that changed brick
+        in the last drift)."""
+        r, q, m = _c.c_int64(), _c.c_int64(), _c.c_int64()
+        self._check(_lib.load().lf2_rebin_stats(self.h, _c.byref(r), _c.byref(q), _c.byref(m)),
+                    "rebin_stats")
+        return r.value, q.value, m.value
 
     def kernel_launches(self):
         n = _c.c_int64()

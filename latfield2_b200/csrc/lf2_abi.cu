@@ -173,7 +173,9 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
 {
   const bool has_mass = mass != nullptr, has_id = id != nullptr;
   const int64_t nb = c->g.nbricks;
-  const int64_t need = n + (n >> 3) + 32 * nb + 1024;
+  // segments (count + slack, rounded to 4) plus a relocation region of about
+  // the same size as the slack
+  const int64_t need = n + (n >> 2) + 100 * nb + 1024;
   if (need > c->capacity || has_mass != c->has_mass || has_id != c->has_id ||
       n > c->mov_capacity) {
     LF2_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -204,6 +206,7 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
   LF2_CUDA(c, launch_load_scatter(c, n, cell, off3, vel3, mass, id));
   LF2_CUDA(c, cudaMemcpyAsync(c->count, c->fill, sizeof(int32_t) * nb, cudaMemcpyDeviceToDevice,
                               c->stream));
+  LF2_CUDA(c, launch_heap_reset(c));
   c->np = n;
   if (check_flags(c) != LF2_OK) {
     c->np = 0;
@@ -294,7 +297,11 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->repack, sizeof(int32_t)) == cudaSuccess;
-  ok = ok && cudaMalloc(&c->diag, sizeof(unsigned long long) * 2) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->diag, sizeof(unsigned long long) * 3) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->heap_top, sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->ovf_list, sizeof(int32_t) * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->ovf_count, sizeof(int32_t)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->ovf_state, sizeof(int32_t) * nb) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_i64, sizeof(int64_t) * 4) == cudaSuccess;
@@ -304,7 +311,10 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
          cudaMemsetAsync(c->seg_start, 0, sizeof(int64_t) * (nb + 1), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->repack, 0, sizeof(int32_t), c->stream) == cudaSuccess &&
-         cudaMemsetAsync(c->diag, 0, 2 * sizeof(unsigned long long), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->diag, 0, 3 * sizeof(unsigned long long), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->ovf_count, 0, sizeof(int32_t), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->ovf_state, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->heap_top, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
          cudaStreamSynchronize(c->stream) == cudaSuccess;
   }
@@ -339,6 +349,10 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->flags);
   cudaFree(c->repack);
   cudaFree(c->diag);
+  cudaFree(c->heap_top);
+  cudaFree(c->ovf_list);
+  cudaFree(c->ovf_count);
+  cudaFree(c->ovf_state);
   cudaFree(c->spill);
   cudaFreeHost(c->h_stats);
   cudaFreeHost(c->h_flags);
@@ -760,14 +774,15 @@ lf2_status lf2_profile_read(lf2_ctx* c, double* ms, int64_t* launches)
   return LF2_OK;
 }
 
-lf2_status lf2_rebin_stats(lf2_ctx* c, int64_t* repacks, int64_t* movers)
+lf2_status lf2_rebin_stats(lf2_ctx* c, int64_t* repacks, int64_t* relocations, int64_t* movers)
 {
   if (!c) return LF2_ERR_ARG;
-  unsigned long long d[2] = {0, 0};
+  unsigned long long d[3] = {0, 0, 0};  // repacks, movers of the last drift, relocations
   LF2_CUDA(c, cudaMemcpyAsync(d, c->diag, sizeof d, cudaMemcpyDeviceToHost, c->stream));
   LF2_CUDA(c, cudaStreamSynchronize(c->stream));
   if (repacks) *repacks = (int64_t)d[0];
   if (movers) *movers = (int64_t)d[1];
+  if (relocations) *relocations = (int64_t)d[2];
   return LF2_OK;
 }
 

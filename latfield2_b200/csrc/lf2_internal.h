@@ -82,8 +82,12 @@ struct lf2_ctx {
   int32_t* fill = nullptr;           // [nbricks] scratch
   unsigned long long* mov_count = nullptr;
   uint32_t* flags = nullptr;         // device error bits
-  int32_t* repack = nullptr;         // device: 1 when a brick overflowed
-  unsigned long long* diag = nullptr; // device [2]: repacks, movers of the last drift
+  int32_t* repack = nullptr;         // device: 1 when the whole store must be repacked
+  unsigned long long* diag = nullptr; // device [3]: repacks, movers of the last drift, relocations
+  unsigned long long* heap_top = nullptr;  // device: next free slot of the relocation region
+  int32_t* ovf_list = nullptr;       // [nbricks] bricks that ran out of slots in the last insert
+  int32_t* ovf_count = nullptr;      // device: entries of ovf_list
+  int32_t* ovf_state = nullptr;      // [nbricks] 0 none, 1 listed, 2 relocated
   float* brick_maxv2 = nullptr;      // [nbricks]
   double* brick_sums = nullptr;      // [nbricks * 5]
   double* stats = nullptr;           // [8] device
@@ -130,6 +134,7 @@ cudaError_t launch_state_to_pos(lf2_ctx* c, int64_t n, const int32_t* cell, cons
 cudaError_t launch_cell_counts(lf2_ctx* c, int32_t* counts);
 cudaError_t launch_scan_counts(lf2_ctx* c, int64_t* out_start);
 cudaError_t launch_repack(lf2_ctx* c);
+cudaError_t launch_heap_reset(lf2_ctx* c);
 
 // lf2_move.cu
 cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp);

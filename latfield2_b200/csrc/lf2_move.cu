@@ -20,11 +20,49 @@ namespace lf2 {
 
 namespace {
 
-constexpr int MOVE_THREADS = 256;
+// Launch shape and access pattern of k_move (chosen by measurement):
+//   MOVE_THREADS  threads per CTA (one CTA per brick)
+//   MOVE_ITEMS    particles per thread per chunk; with MOVE_BLOCKED a thread
+//                 owns MOVE_ITEMS consecutive slots and reads them with one
+//                 16-byte vector load per array (brick segments start on a
+//                 multiple of 4 slots and hold a multiple of 4 slots, so the
+//                 vector never leaves the segment)
+//   MOVE_F4       the brick's vertex tile of F kept as float4 (x, y, z, 0):
+//                 one 16-byte shared load per corner instead of three
+#ifndef LF2_MOVE_THREADS
+#define LF2_MOVE_THREADS 256
+#endif
+#ifndef LF2_MOVE_ITEMS
+#define LF2_MOVE_ITEMS 4
+#endif
+#ifndef LF2_MOVE_BLOCKED
+#define LF2_MOVE_BLOCKED 1
+#endif
+#ifndef LF2_MOVE_F4
+#define LF2_MOVE_F4 0
+#endif
+constexpr int MOVE_THREADS = LF2_MOVE_THREADS;
+constexpr int MOVE_ITEMS = LF2_MOVE_ITEMS;
+constexpr bool MOVE_BLOCKED = LF2_MOVE_BLOCKED != 0;
+constexpr bool MOVE_F4 = LF2_MOVE_F4 != 0;
+static_assert(!MOVE_BLOCKED || MOVE_ITEMS == 4, "blocked access reads 4 slots per vector");
 
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
 
-constexpr int MOVE_ITEMS = 4;  // particles in flight per thread
+template <typename T>
+__device__ __forceinline__ void load4(const T* __restrict__ a, int64_t p, T (&r)[4])
+{
+  static_assert(sizeof(T) == 4, "32-bit lanes");
+  const uint4 q = __ldcs(reinterpret_cast<const uint4*>(a + p));
+  r[0] = __uint_as_float(q.x), r[1] = __uint_as_float(q.y);
+  r[2] = __uint_as_float(q.z), r[3] = __uint_as_float(q.w);
+}
+
+__device__ __forceinline__ void load4u(const uint32_t* __restrict__ a, int64_t p, uint32_t (&r)[4])
+{
+  const uint4 q = __ldcs(reinterpret_cast<const uint4*>(a + p));
+  r[0] = q.x, r[1] = q.y, r[2] = q.z, r[3] = q.w;
+}
 
 template <bool KICK, bool DRIFT>
 __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float* __restrict__ F,
@@ -32,7 +70,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
                                                        unsigned long long* mov_count,
                                                        float* brick_maxv2, uint32_t* flags)
 {
-  extern __shared__ float ftile[];  // [3][TILE3] when KICK
+  extern __shared__ __align__(16) float ftile[];  // KICK: [3][TILE3] or float4[TILE3]
   __shared__ int s_scan[32];
   __shared__ float s_max[MOVE_THREADS / 32];
 
@@ -54,24 +92,55 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
     float vx[MOVE_ITEMS], vy[MOVE_ITEMS], vz[MOVE_ITEMS], m[MOVE_ITEMS];
     int64_t id[MOVE_ITEMS];
     bool act[MOVE_ITEMS], stay[MOVE_ITEMS];
+    // slot of item j: blocked = c0 + 4*tid + j, strided = c0 + j*THREADS + tid
+    auto slot = [&](int j) {
+      return MOVE_BLOCKED ? c0 + MOVE_ITEMS * (int)threadIdx.x + j
+                          : c0 + j * MOVE_THREADS + (int)threadIdx.x;
+    };
+    if constexpr (MOVE_BLOCKED) {
+      const int i0 = slot(0);
+      if (i0 < cnt) {
+        const int64_t p = base + i0;
+        {
+          load4u(v.a.key, p, key);
+          load4(v.a.ox, p, ox);
+          load4(v.a.oy, p, oy);
+          load4(v.a.oz, p, oz);
+          load4(v.a.vx, p, vx);
+          load4(v.a.vy, p, vy);
+          load4(v.a.vz, p, vz);
+        }
+      }
 #pragma unroll
-    for (int j = 0; j < MOVE_ITEMS; j++) {
-      const int i = c0 + j * MOVE_THREADS + threadIdx.x;
-      act[j] = i < cnt;
-      stay[j] = true;
-      m[j] = 0.0f;
-      id[j] = 0;
-      if (act[j]) {
-        const int64_t p = base + i;
-        key[j] = v.a.key[p];
-        ox[j] = v.a.ox[p];
-        oy[j] = v.a.oy[p];
-        oz[j] = v.a.oz[p];
-        vx[j] = v.a.vx[p];
-        vy[j] = v.a.vy[p];
-        vz[j] = v.a.vz[p];
-        if (DRIFT && v.a.mass) m[j] = v.a.mass[p];
-        if (DRIFT && v.a.id) id[j] = v.a.id[p];
+      for (int j = 0; j < MOVE_ITEMS; j++) {
+        act[j] = slot(j) < cnt;
+        stay[j] = true;
+        m[j] = 0.0f;
+        id[j] = 0;
+        if (act[j]) {
+          if (DRIFT && v.a.mass) m[j] = v.a.mass[base + slot(j)];
+          if (DRIFT && v.a.id) id[j] = v.a.id[base + slot(j)];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < MOVE_ITEMS; j++) {
+        act[j] = slot(j) < cnt;
+        stay[j] = true;
+        m[j] = 0.0f;
+        id[j] = 0;
+        if (act[j]) {
+          const int64_t p = base + slot(j);
+          key[j] = v.a.key[p];
+          ox[j] = v.a.ox[p];
+          oy[j] = v.a.oy[p];
+          oz[j] = v.a.oz[p];
+          vx[j] = v.a.vx[p];
+          vy[j] = v.a.vy[p];
+          vz[j] = v.a.vz[p];
+          if (DRIFT && v.a.mass) m[j] = v.a.mass[p];
+          if (DRIFT && v.a.id) id[j] = v.a.id[p];
+        }
       }
     }
     if (KICK && c0 == 0) {
@@ -86,9 +155,14 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
         const int gy = y0 + jj < g.n[1] ? y0 + jj : 0;
         const int gz = z0 + k < g.n[2] ? z0 + k : 0;
         const int64_t s = site_index(g, gx, gy, gz);
-        ftile[t] = __ldg(F + s);
-        ftile[TILE3 + t] = __ldg(F + g.nsites + s);
-        ftile[2 * TILE3 + t] = __ldg(F + 2 * g.nsites + s);
+        const float f0 = __ldg(F + s), f1 = __ldg(F + g.nsites + s), f2 = __ldg(F + 2 * g.nsites + s);
+        if (MOVE_F4) {
+          reinterpret_cast<float4*>(ftile)[t] = make_float4(f0, f1, f2, 0.0f);
+        } else {
+          ftile[t] = f0;
+          ftile[TILE3 + t] = f1;
+          ftile[2 * TILE3 + t] = f2;
+        }
       }
       __syncthreads();
     }
@@ -108,9 +182,16 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
           const float w = __fmul_rn(__fmul_rn(sel(cx, ox[j], gx), sel(cy, oy[j], gy)),
                                     sel(cz, oz[j], gz));
           const int t = t0 + cx + cy * TILE + cz * TILE * TILE;
-          a0 = __fmaf_rn(w, ftile[t], a0);
-          a1 = __fmaf_rn(w, ftile[TILE3 + t], a1);
-          a2 = __fmaf_rn(w, ftile[2 * TILE3 + t], a2);
+          float f0, f1, f2;
+          if (MOVE_F4) {
+            const float4 q = reinterpret_cast<const float4*>(ftile)[t];
+            f0 = q.x, f1 = q.y, f2 = q.z;
+          } else {
+            f0 = ftile[t], f1 = ftile[TILE3 + t], f2 = ftile[2 * TILE3 + t];
+          }
+          a0 = __fmaf_rn(w, f0, a0);
+          a1 = __fmaf_rn(w, f1, a1);
+          a2 = __fmaf_rn(w, f2, a2);
         }
         vx[j] = __fmaf_rn(mp.dtk, a0, vx[j]);
         vy[j] = __fmaf_rn(mp.dtk, a1, vy[j]);
@@ -153,13 +234,23 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
     }
 
     if (!DRIFT) {
+      if constexpr (MOVE_BLOCKED) {
+        const int i0 = slot(0);
+        if (i0 < cnt) {  // the whole vector stays inside the segment
+          const int64_t p = base + i0;
+          *reinterpret_cast<float4*>(v.a.vx + p) = make_float4(vx[0], vx[1], vx[2], vx[3]);
+          *reinterpret_cast<float4*>(v.a.vy + p) = make_float4(vy[0], vy[1], vy[2], vy[3]);
+          *reinterpret_cast<float4*>(v.a.vz + p) = make_float4(vz[0], vz[1], vz[2], vz[3]);
+        }
+      } else {
 #pragma unroll
-      for (int j = 0; j < MOVE_ITEMS; j++) {
-        if (!act[j]) continue;
-        const int64_t p = base + c0 + j * MOVE_THREADS + threadIdx.x;
-        v.a.vx[p] = vx[j];
-        v.a.vy[p] = vy[j];
-        v.a.vz[p] = vz[j];
+        for (int j = 0; j < MOVE_ITEMS; j++) {
+          if (!act[j]) continue;
+          const int64_t p = base + slot(j);
+          v.a.vx[p] = vx[j];
+          v.a.vy[p] = vy[j];
+          v.a.vz[p] = vz[j];
+        }
       }
       continue;
     }
@@ -224,7 +315,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
 
 // Movers into the free slots of their new brick.
 __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* __restrict__ mov_count,
-                         int32_t* placed, int32_t* repack)
+                         int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state)
 {
   const int64_t nm = (int64_t)*mov_count;
   for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
@@ -246,8 +337,8 @@ __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* 
       if (v.a.id) v.a.id[q] = mov.id[m];
       placed[m] = 1;
     } else {
-      placed[m] = 0;
-      *repack = 1;
+      placed[m] = 0;  // the brick is full: it gets relocated (lf2_store.cu)
+      if (atomicExch(&ovf_state[b], 1) == 0) ovf_list[atomicAdd(ovf_count, 1)] = (int32_t)b;
     }
   }
 }
@@ -274,7 +365,7 @@ __global__ void __launch_bounds__(1024) k_reduce_maxv(int64_t nb, const float* _
 cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp)
 {
   c->launches += 1;
-  const size_t smem = kick ? sizeof(float) * 3 * TILE3 : 0;
+  const size_t smem = kick ? (MOVE_F4 ? sizeof(float4) : 3 * sizeof(float)) * TILE3 : 0;
   const unsigned nb = (unsigned)c->g.nbricks;
   if (kick && drift) {
     cudaFuncSetAttribute(k_move<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -298,7 +389,8 @@ cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveP
 cudaError_t launch_insert(lf2_ctx* c)
 {
   c->launches += 1;
-  k_insert<<<148 * 4, 256, 0, c->stream>>>(view(c), c->mov, c->mov_count, c->mov_placed, c->repack);
+  k_insert<<<148 * 4, 256, 0, c->stream>>>(view(c), c->mov, c->mov_count, c->mov_placed,
+                                           c->ovf_list, c->ovf_count, c->ovf_state);
   return cudaGetLastError();
 }
 

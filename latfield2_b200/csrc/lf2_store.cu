@@ -21,6 +21,13 @@ __host__ __device__ inline int32_t slack_of(int32_t count)
   return s > SLACK_MIN ? s : SLACK_MIN;
 }
 
+// Slots of a brick segment: the particles plus slack, rounded up to a
+// multiple of 4 so that every segment starts on a 16-byte boundary.
+__host__ __device__ inline int32_t cap_of(int32_t count)
+{
+  return (count + slack_of(count) + 3) & ~3;
+}
+
 __device__ inline bool decode_cell(const Geom& g, int32_t c, int& x, int& y, int& z)
 {
   if (c < 0 || (int64_t)c >= g.nsites) return false;
@@ -59,7 +66,7 @@ __global__ void __launch_bounds__(1024) k_caps_scan(int64_t nb, const int32_t* _
   const int64_t lo = t * per, hi = min(nb, lo + per);
   int64_t s = 0;
   for (int64_t b = lo; b < hi; b++) {
-    const int32_t v = caps ? counts[b] + slack_of(counts[b]) : counts[b];
+    const int32_t v = caps ? cap_of(counts[b]) : counts[b];
     if (caps) caps[b] = v;
     s += v;
   }
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(1024) k_repack_caps(int64_t nb, const int32_t*
   const int64_t lo = t * per, hi = min(nb, lo + per);
   int64_t s = 0;
   for (int64_t b = lo; b < hi; b++) {
-    const int32_t c = cap_alt[b] = count[b] + slack_of(count[b]);
+    const int32_t c = cap_alt[b] = cap_of(count[b]);
     s += c;
   }
   sh[t] = s;
@@ -283,13 +290,14 @@ __global__ void k_repack_copy_back(StoreView v, PartArrays alt, const int64_t* _
 
 __global__ void k_repack_finish(int64_t nb, const int64_t* __restrict__ start_alt,
                                 const int32_t* __restrict__ cap_alt, int64_t* seg_start,
-                                int32_t* cap, int32_t* repack, uint32_t* flags)
+                                int32_t* cap, int32_t* repack, unsigned long long* heap_top)
 {
   if (*repack == 0) return;
   for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= nb;
        b += (int64_t)gridDim.x * blockDim.x) {
     seg_start[b] = start_alt[b];
     if (b < nb) cap[b] = cap_alt[b];
+    else *heap_top = (unsigned long long)start_alt[nb];  // relocation region starts after the segments
   }
 }
 
@@ -302,6 +310,75 @@ __global__ void k_repack_clear(int32_t* repack, uint32_t* flags, unsigned long l
     *repack = 0;
   }
   diag[1] = *mov_count;
+}
+
+// ----------------------------------------------------------- relocation
+// A brick that ran out of free slots in k_insert is moved on its own to a
+// fresh, larger segment carved from the relocation region (bump allocation
+// past the contiguous segments).  Its old slots are abandoned until the next
+// full repack.  Only when the region is exhausted does the whole store get
+// repacked (k_repack_*).
+
+__global__ void k_reloc(StoreView v, int64_t* seg_start, int32_t* cap, const int32_t* __restrict__ list,
+                        const int32_t* __restrict__ nlist, int32_t* state, int32_t* fill,
+                        unsigned long long* heap_top, int64_t capacity, int32_t* repack,
+                        unsigned long long* diag)
+{
+  __shared__ long long s_new;
+  const int n = *nlist;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int64_t b = list[i];
+    const int32_t need = v.count[b];  // stays + every arrival that tried
+    const int32_t placed = min(need, cap[b]);
+    const int32_t ncap = cap_of(need);
+    if (threadIdx.x == 0) {
+      const unsigned long long s0 = atomicAdd(heap_top, (unsigned long long)ncap);
+      s_new = (s0 + (unsigned long long)ncap <= (unsigned long long)capacity) ? (long long)s0 : -1;
+      if (s_new < 0) *repack = 1;  // region exhausted: repack everything
+    }
+    __syncthreads();
+    const long long d0 = s_new;
+    if (d0 >= 0) {
+      const int64_t s0 = seg_start[b];
+      for (int k = threadIdx.x; k < placed; k += blockDim.x) copy_particle(v.a, s0 + k, v.a, d0 + k);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        seg_start[b] = d0;
+        cap[b] = ncap;
+        fill[b] = placed;
+        state[b] = 2;
+        atomicAdd(&diag[2], 1ull);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_reloc_movers(Geom g, PartArrays mov, int32_t* placed,
+                               const unsigned long long* __restrict__ mov_count, PartArrays dst,
+                               const int64_t* __restrict__ seg_start, const int32_t* __restrict__ state,
+                               int32_t* fill, const int32_t* __restrict__ nlist)
+{
+  if (*nlist == 0) return;
+  const int64_t nm = (int64_t)*mov_count;
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    if (placed[m]) continue;
+    int x, y, z;
+    unpack_key(g, mov.key[m], x, y, z);
+    const int64_t b = brick_of(g, x, y, z);
+    if (state[b] != 2) continue;  // not relocated: left to the full repack
+    copy_particle(mov, m, dst, seg_start[b] + atomicAdd(&fill[b], 1));
+    placed[m] = 1;
+  }
+}
+
+__global__ void k_ovf_reset(int32_t* list, int32_t* nlist, int32_t* state)
+{
+  const int n = *nlist;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) state[list[i]] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) *nlist = 0;
 }
 
 inline int grid_for(int64_t n, int threads)
@@ -389,10 +466,21 @@ cudaError_t launch_cell_counts(lf2_ctx* c, int32_t* counts)
   return cudaGetLastError();
 }
 
+cudaError_t launch_heap_reset(lf2_ctx* c)
+{
+  return cudaMemcpyAsync(c->heap_top, c->seg_start + c->g.nbricks, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToDevice, c->stream);
+}
+
 cudaError_t launch_repack(lf2_ctx* c)
 {
-  c->launches += 6;
+  c->launches += 9;
   const int64_t nb = c->g.nbricks;
+  k_reloc<<<148, 256, 0, c->stream>>>(view(c), c->seg_start, c->cap, c->ovf_list, c->ovf_count,
+                                      c->ovf_state, c->fill, c->heap_top, c->capacity, c->repack,
+                                      c->diag);
+  k_reloc_movers<<<148 * 2, 256, 0, c->stream>>>(c->g, c->mov, c->mov_placed, c->mov_count, c->cur,
+                                                 c->seg_start, c->ovf_state, c->fill, c->ovf_count);
   k_repack_caps<<<1, 1024, 0, c->stream>>>(nb, c->count, c->cap_alt, c->seg_start_alt, c->capacity,
                                            c->repack, c->flags);
   const unsigned small = (unsigned)(nb < 148 * 8 ? nb : 148 * 8);
@@ -402,10 +490,10 @@ cudaError_t launch_repack(lf2_ctx* c)
                                                   c->seg_start_alt, c->fill, c->repack);
   k_repack_copy_back<<<small, 256, 0, c->stream>>>(view(c), c->alt, c->seg_start_alt, c->fill,
                                                    c->repack);
-  k_repack_finish<<<small, 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt,
-                                                                c->seg_start, c->cap, c->repack,
-                                                                c->flags);
+  k_repack_finish<<<small, 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt, c->seg_start,
+                                                 c->cap, c->repack, c->heap_top);
   k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag, c->mov_count);
+  k_ovf_reset<<<1, 256, 0, c->stream>>>(c->ovf_list, c->ovf_count, c->ovf_state);
   return cudaGetLastError();
 }
 

@@ -257,7 +257,8 @@ def test_repack_when_bricks_overflow(cuda):
     ctx = _ctx(n, 1)
     _load(ctx, cell, off, vel, 1.0 / npart)
     ctx.drift_rebin(dtau)
-    assert ctx.flags() & 0x8  # repacked
+    repacks, relocations, movers = ctx.rebin_stats()
+    assert repacks + relocations > 0 and movers > 0
     assert ctx.flags() & ~0x8 == 0
     got = by_id(ctx.get_particles(ids=True))
     np.testing.assert_array_equal(got["id"], np.arange(npart))
@@ -272,6 +273,43 @@ def test_repack_when_bricks_overflow(cuda):
     ctx.drift_rebin(-dtau)
     back = by_id(ctx.get_particles(ids=True))
     c3, o3, _ = O.state_drift(n, c2, o2, vel, np.float32(-dtau * 64))
+    np.testing.assert_array_equal(back["cell"], c3)
+    np.testing.assert_array_equal(back["off"], o3)
+
+
+def test_single_brick_relocation(cuda):
+    """A modest flux into one brick overflows only that brick: it is moved
+    to the relocation region on its own, without a full repack."""
+    n = (64, 64, 64)
+    rng = np.random.default_rng(8)
+    npart = 30000
+    pos = rng.random((npart, 3))
+    vel = np.zeros((npart, 3), np.float32)
+    # 300 particles of the brick above brick 0 (in z) fall into brick 0
+    above = np.where((pos[:, 0] < 0.25) & (pos[:, 1] < 0.25) & (pos[:, 2] >= 0.25) &
+                     (pos[:, 2] < 0.5))[0][:300]
+    vel[above, 2] = -0.25 / 1.0
+    u = pos * 64
+    cell = (np.floor(u[:, 0]) + 64 * (np.floor(u[:, 1]) + 64 * np.floor(u[:, 2]))).astype(np.int32)
+    off = (u - np.floor(u)).astype(np.float32)
+    ctx = _ctx(n, 1)
+    _load(ctx, cell, off, vel, 1.0 / npart)
+    ctx.drift_rebin(1.0)
+    repacks, relocations, movers = ctx.rebin_stats()
+    assert repacks == 0 and relocations >= 1 and movers >= 300
+    got = by_id(ctx.get_particles(ids=True))
+    c2, o2, _ = O.state_drift(n, cell, off, vel, np.float32(64.0))
+    np.testing.assert_array_equal(got["cell"], c2)
+    np.testing.assert_array_equal(got["off"], o2)
+    np.testing.assert_array_equal(ctx.cell_counts(), np.bincount(c2, minlength=64 ** 3))
+    rho = ctx.field(1)
+    ctx.deposit_scalar(rho)
+    exact = O.fixed_to_f32(O.state_deposit_fixed(n, c2, o2), fixed_scale(1.0 / npart, 1.0 / 64))
+    np.testing.assert_array_equal(rho.export_internal().reshape(-1), exact)
+    # and again: the relocated brick keeps working and can move back out
+    ctx.drift_rebin(-1.0)
+    back = by_id(ctx.get_particles(ids=True))
+    c3, o3, _ = O.state_drift(n, c2, o2, vel, np.float32(-64.0))
     np.testing.assert_array_equal(back["cell"], c3)
     np.testing.assert_array_equal(back["off"], o3)
 
