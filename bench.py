@@ -42,7 +42,7 @@ WORKLOADS = {
     # c3 statistics at 256^3 (16.8M particles): the size used for ncu captures
     "c3s": dict(n=256, npart=256 ** 3, dist="lognormal", mode="fixed"),
 }
-METRIC = "particle updates/s (CIC deposit+gather+move)"
+METRIC = "particle updates/s (CIC deposit+gather+move) & adjoint/forward time"
 UNIT = "particle-updates/s"
 
 
@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -216,6 +217,45 @@ def _cpu_worker(seconds, n, npart, seed):
     return npart * steps / dt, steps
 
 
+def adjoint_ratio(device, steps=8, reps=3):
+    """Differentiable chain at 128^3 with 2,097,152 uniform particles and
+    per-particle masses (1/Np)(1 + 0.1 U(-1,1)): 8 kick-drift steps of
+    deposit -> periodic 27-point stencil (81 seeded weights) -> CIC gather ->
+    kick -> drift, loss = sum w_g rho_g(final), particle checkpoints every 2
+    steps.  Returns device times of the forward alone and of forward +
+    adjoint (CUDA events, median of `reps`)."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import pm_chain_loss
+    n, npart = 128, 1 << 21
+    g = torch.Generator(device=device).manual_seed(41)
+    pos = torch.rand(npart, 3, generator=g, device=device, dtype=torch.float64)
+    vel = 0.01 * torch.randn(npart, 3, generator=g, device=device, dtype=torch.float64)
+    m = (1.0 + 0.1 * (2 * torch.rand(npart, generator=g, device=device, dtype=torch.float64) - 1)) / npart
+    S = 0.02 * torch.randn(81, generator=g, device=device, dtype=torch.float64)
+    w = torch.randn(n ** 3, generator=g, device=device, dtype=torch.float64)
+    ctx = L.Context((n, n, n), box=1.0)
+    dt = 0.1 * 64.0 / n
+
+    def timed(grad):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        leaves = [t.clone().requires_grad_(grad) for t in (pos, vel, m, S, w)]
+        torch.cuda.synchronize()
+        e0.record()
+        loss = pm_chain_loss(ctx, *leaves, steps=steps, dt=dt, checkpoint_every=2)
+        if grad:
+            loss.backward()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    timed(True)
+    fwd = sorted(timed(False) for _ in range(reps))[reps // 2]
+    both = sorted(timed(True) for _ in range(reps))[reps // 2]
+    return {"workload": "128^3, 2,097,152 particles, 8 steps, checkpoint every 2",
+            "forward_ms": fwd, "forward_adjoint_ms": both, "ratio": both / fwd}
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return
@@ -357,6 +397,8 @@ def main():
            "path": "lf2_field_import(F, host) + lf2_step + lf2_field_export(rho, host) + "
                    "lf2_gather_kick(max_v)"}
 
+    adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -378,7 +420,8 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": roofline, "step_roofline": step_roofline, "phase_ms": phase_ms,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
-            "gpu_launches": launches, "adjoint_forward_ratio": None,
+            "gpu_launches": launches,
+            "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

@@ -177,6 +177,48 @@ lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
 lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
                             double* max_v);
 
+/* ------------------------------------------------- differentiable PM chain
+ * Particle kernels on arrays kept in the caller's order (no rebinning, so
+ * gradients stay attached to their particles), for the adjoint of a
+ * multi-step particle-mesh chain.  They have no reference counterpart beyond
+ * the forward operations they differentiate: the CIC deposit
+ * (scalarProjectionCIC_project, projections.hpp:75-184), the CIC gather-kick
+ * of updateVel (LATfield2_Particles.hpp:752-893) and the drift of
+ * move_particles_simple (move_function.hpp:15-32).  All pointers are device
+ * pointers; offsets and offset gradients are in cell units; outputs marked
+ * (+=) are accumulated.  mass may be NULL (global mass gmass).
+ *   deposit          rho (+=) m/res^3 W                (FP32 atomics)
+ *   gather           out3[p] = sum_k W_k F(corner_k)
+ *   kick_drift       vel += dt_kick * G3 (G3 may be NULL); off += dt_drift/res
+ *                    * vel with the carry into cell
+ *   deposit_adjoint  g_off3 (+=), g_mass (+=) from g_rho
+ *   gather_adjoint   g_F (+=) CIC deposit of g_out3; g_off3 (+=)
+ *   stencil27        F3_c(g) = sum_o S[c*27 + (dz+1)*9 + (dy+1)*3 + (dx+1)]
+ *                    rho(g + o), periodic, S81 on the device
+ *   stencil27_adjoint g_rho (+=) and g_S81 (+=) from g_F3 */
+lf2_status lf2_pm_deposit(lf2_ctx* ctx, int64_t np, const int32_t* cell,
+                          const float* off3, const float* mass, double gmass,
+                          float* rho);
+lf2_status lf2_pm_gather(lf2_ctx* ctx, int64_t np, const int32_t* cell,
+                         const float* off3, const float* F, float* out3);
+lf2_status lf2_pm_kick_drift(lf2_ctx* ctx, int64_t np, int32_t* cell,
+                             float* off3, float* vel3, const float* G3,
+                             double dt_kick, double dt_drift);
+lf2_status lf2_pm_deposit_adjoint(lf2_ctx* ctx, int64_t np,
+                                  const int32_t* cell, const float* off3,
+                                  const float* mass, double gmass,
+                                  const float* g_rho, float* g_off3,
+                                  float* g_mass);
+lf2_status lf2_pm_gather_adjoint(lf2_ctx* ctx, int64_t np,
+                                 const int32_t* cell, const float* off3,
+                                 const float* F, const float* g_out3,
+                                 float* g_F, float* g_off3);
+lf2_status lf2_stencil27(lf2_ctx* ctx, const float* rho, const float* S81,
+                         float* F3);
+lf2_status lf2_stencil27_adjoint(lf2_ctx* ctx, const float* rho,
+                                 const float* S81, const float* g_F3,
+                                 float* g_rho, float* g_S81);
+
 /* ---------------------------------------------------------- no allocation
  * Scalar CIC deposit that allocates no device memory.  It has no
  * counterpart in the reference; it exists for callers that may not allocate

@@ -67,6 +67,16 @@ SIGNATURES = {
     "lf2_drift_rebin": [c_void_p, c_double],
     "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],
     "lf2_conservation": [c_void_p, P(c_double), P(c_double), P(c_double)],
+    "lf2_pm_deposit": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p],
+    "lf2_pm_gather": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p],
+    "lf2_pm_kick_drift": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                          c_double],
+    "lf2_pm_deposit_adjoint": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p,
+                               c_void_p, c_void_p],
+    "lf2_pm_gather_adjoint": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                              c_void_p],
+    "lf2_stencil27": [c_void_p, c_void_p, c_void_p, c_void_p],
+    "lf2_stencil27_adjoint": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_profile_enable": [c_void_p, c_int],
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
     "lf2_kernel_launches": [c_void_p, P(c_i64)],

@@ -1,0 +1,169 @@
+"""Differentiable multi-step particle-mesh chain on the CUDA kernels.
+
+Per step k (particles in the caller's order, no rebinning):
+    rho_k   = deposit(x_k, m)                    lf2_pm_deposit      (CIC, projections.hpp:75-184)
+    F_k     = stencil27(rho_k, S)                lf2_stencil27       (the grid operator)
+    G_k     = gather(x_k, F_k)                   lf2_pm_gather       (CIC gather of updateVel)
+    v_{k+1} = v_k + dt G_k ;  x_{k+1} = x_k + dt v_{k+1}             lf2_pm_kick_drift
+and finally rho_K = deposit(x_K, m), loss = sum_g w_g rho_K(g).
+
+`PMChain` is a torch.autograd.Function whose backward runs the hand-written
+adjoint kernels (lf2_pm_*_adjoint, lf2_stencil27_adjoint) in reverse.
+Particle states are checkpointed every `checkpoint_every` steps and the
+states in between are recomputed during the backward pass; the grid fields
+rho_k and F_k of every step are kept (4 floats per lattice site per step).
+Gradients are returned for the initial positions (box units), velocities,
+masses, the 81 stencil weights and the loss weights.
+"""
+import ctypes
+
+import torch
+
+from . import _lib
+from .core import Context
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _check(ctx, status, what):
+    _lib.check(ctx.h, status, what)
+
+
+def positions_to_state(pos, n, res):
+    """Box-unit positions (float64) -> int32 cell, FP32 in-cell offset."""
+    u = pos / res
+    fl = torch.floor(u)
+    off = (u - fl).to(torch.float32)
+    carry = off >= 1.0
+    off = torch.where(carry, torch.zeros_like(off), off)
+    fl = fl + carry.to(fl.dtype)
+    nn = torch.tensor(n, dtype=torch.int64, device=pos.device)
+    ci = torch.remainder(fl.to(torch.int64), nn)
+    cell = ci[:, 0] + n[0] * (ci[:, 1] + n[1] * ci[:, 2])
+    return cell.to(torch.int32).contiguous(), off.contiguous()
+
+
+class _Ops:
+    """The kernel calls of one chain, bound to a Context."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.lib = _lib.load()
+        self.ns = ctx.nsites
+
+    def deposit(self, cell, off, m, rho):
+        _check(self.ctx, self.lib.lf2_pm_deposit(self.ctx.h, cell.numel(), _p(cell), _p(off), _p(m),
+                                                 0.0, _p(rho)), "pm_deposit")
+
+    def stencil(self, rho, S, F):
+        _check(self.ctx, self.lib.lf2_stencil27(self.ctx.h, _p(rho), _p(S), _p(F)), "stencil27")
+
+    def gather(self, cell, off, F, G):
+        _check(self.ctx, self.lib.lf2_pm_gather(self.ctx.h, cell.numel(), _p(cell), _p(off), _p(F),
+                                                _p(G)), "pm_gather")
+
+    def kick_drift(self, cell, off, vel, G, dt):
+        _check(self.ctx, self.lib.lf2_pm_kick_drift(self.ctx.h, cell.numel(), _p(cell), _p(off),
+                                                    _p(vel), _p(G), dt, dt), "pm_kick_drift")
+
+    def deposit_adj(self, cell, off, m, g_rho, g_off, g_m):
+        _check(self.ctx, self.lib.lf2_pm_deposit_adjoint(self.ctx.h, cell.numel(), _p(cell), _p(off),
+                                                         _p(m), 0.0, _p(g_rho), _p(g_off),
+                                                         _p(g_m)), "pm_deposit_adjoint")
+
+    def gather_adj(self, cell, off, F, g_G, g_F, g_off):
+        _check(self.ctx, self.lib.lf2_pm_gather_adjoint(self.ctx.h, cell.numel(), _p(cell), _p(off),
+                                                        _p(F), _p(g_G), _p(g_F), _p(g_off)),
+               "pm_gather_adjoint")
+
+    def stencil_adj(self, rho, S, g_F, g_rho, g_S):
+        _check(self.ctx, self.lib.lf2_stencil27_adjoint(self.ctx.h, _p(rho), _p(S), _p(g_F),
+                                                        _p(g_rho), _p(g_S)), "stencil27_adjoint")
+
+    def fields(self, cell, off, m, S):
+        dev = cell.device
+        rho = torch.zeros(self.ns, dtype=torch.float32, device=dev)
+        self.deposit(cell, off, m, rho)
+        F = torch.empty(3 * self.ns, dtype=torch.float32, device=dev)
+        self.stencil(rho, S, F)
+        return rho, F
+
+    def step(self, cell, off, vel, F, dt):
+        G = torch.empty_like(vel)
+        self.gather(cell, off, F, G)
+        self.kick_drift(cell, off, vel, G, dt)
+
+
+class PMChain(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, pos0, vel0, mass, S, w, lf2ctx, steps, dt, checkpoint_every):
+        ops = _Ops(lf2ctx)
+        n, res = lf2ctx.n, lf2ctx.res
+        cell, off = positions_to_state(pos0.detach().to(torch.float64), n, res)
+        vel = vel0.detach().to(torch.float32).contiguous().clone()
+        m = mass.detach().to(torch.float32).contiguous()
+        S32 = S.detach().to(torch.float32).contiguous()
+        w32 = w.detach().to(torch.float32).contiguous().reshape(-1)
+        ckpts, rhos, Fs = {}, [], []
+        for k in range(steps):
+            if k % checkpoint_every == 0:
+                ckpts[k] = (cell.clone(), off.clone(), vel.clone())
+            rho, F = ops.fields(cell, off, m, S32)
+            rhos.append(rho)
+            Fs.append(F)
+            ops.step(cell, off, vel, F, dt)
+        rhoK = torch.zeros(lf2ctx.nsites, dtype=torch.float32, device=cell.device)
+        ops.deposit(cell, off, m, rhoK)
+        loss = torch.dot(w32.to(torch.float64), rhoK.to(torch.float64))
+        fctx.lf2 = (lf2ctx, steps, dt, checkpoint_every, ckpts, rhos, Fs)
+        fctx.save_for_backward(cell, off, m, S32, w32, rhoK)
+        fctx.pos_dtype = pos0.dtype
+        fctx.vel_dtype = vel0.dtype
+        return loss
+
+    @staticmethod
+    def backward(fctx, gloss):
+        lf2ctx, steps, dt, every, ckpts, rhos, Fs = fctx.lf2
+        cellK, offK, m, S32, w32, rhoK = fctx.saved_tensors
+        ops = _Ops(lf2ctx)
+        dev = cellK.device
+        res = lf2ctx.res
+        npart = cellK.numel()
+        g = float(gloss)
+        g_off = torch.zeros(npart, 3, dtype=torch.float32, device=dev)
+        g_v = torch.zeros(npart, 3, dtype=torch.float32, device=dev)
+        g_m = torch.zeros(npart, dtype=torch.float32, device=dev)
+        g_S = torch.zeros(81, dtype=torch.float32, device=dev)
+        ops.deposit_adj(cellK, offK, m, (w32 * g).contiguous(), g_off, g_m)
+        seg = {}
+        for k in range(steps - 1, -1, -1):
+            k0 = (k // every) * every
+            if k not in seg:
+                # replay the segment from its checkpoint, keeping each state
+                seg = {}
+                c, o, v = (t.clone() for t in ckpts[k0])
+                for j in range(k0, min(k0 + every, steps)):
+                    seg[j] = (c.clone(), o.clone())
+                    if j < k:
+                        ops.step(c, o, v, Fs[j], dt)
+            cell_k, off_k = seg[k]
+            # drift x_{k+1} = x_k + dt v_{k+1} (cell units: off += dt/res v)
+            g_v += (dt / res) * g_off
+            # kick v_{k+1} = v_k + dt G_k
+            g_G = (dt * g_v).contiguous()
+            g_F = torch.zeros(3 * lf2ctx.nsites, dtype=torch.float32, device=dev)
+            ops.gather_adj(cell_k, off_k, Fs[k], g_G, g_F, g_off)
+            g_rho = torch.zeros(lf2ctx.nsites, dtype=torch.float32, device=dev)
+            ops.stencil_adj(rhos[k], S32, g_F, g_rho, g_S)
+            ops.deposit_adj(cell_k, off_k, m, g_rho, g_off, g_m)
+        g_pos = (g_off.to(torch.float64) / res).to(fctx.pos_dtype)
+        g_w = (rhoK * g).to(torch.float64)
+        return (g_pos, g_v.to(fctx.vel_dtype), g_m.to(torch.float64), g_S.to(torch.float64), g_w,
+                None, None, None, None)
+
+
+def pm_chain_loss(ctx: Context, pos0, vel0, mass, S, w, steps=8, dt=0.1, checkpoint_every=2):
+    """Loss of the multi-step chain; differentiable in pos0, vel0, mass, S, w."""
+    return PMChain.apply(pos0, vel0, mass, S, w, ctx, steps, dt, checkpoint_every)

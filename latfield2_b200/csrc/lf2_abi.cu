@@ -354,6 +354,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->ovf_count);
   cudaFree(c->ovf_state);
   cudaFree(c->spill);
+  cudaFree(c->stencil_partial);
   cudaFreeHost(c->h_stats);
   cudaFreeHost(c->h_flags);
   cudaFreeHost(c->h_i64);
@@ -744,6 +745,83 @@ lf2_status lf2_conservation(lf2_ctx* c, double* mass, double mom[3], double* max
   if (mom)
     for (int d = 0; d < 3; d++) mom[d] = c->h_stats[2 + d];
   if (max_v) *max_v = std::sqrt(c->h_stats[5]);
+  return LF2_OK;
+}
+
+static lf2_status pm_call(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
+                          const float* mass, double gmass, const float* in_a, const float* in_b,
+                          float* out_a, float* out_b, double dta, double dtb, int32_t* cell_rw,
+                          float* off_rw, float* vel_rw)
+{
+  if (!c || np < 0) return LF2_ERR_ARG;
+  if (np == 0) return LF2_OK;
+  PhaseScope ps(c, PH_OTHER);
+  LF2_CUDA(c, launch_pm(c, op, np, cell, off3, mass, (float)gmass, in_a, in_b, out_a, out_b,
+                        (float)dta, (float)dtb, cell_rw, off_rw, vel_rw));
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_deposit(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
+                          const float* mass, double gmass, float* rho)
+{
+  if (!cell || !off3 || !rho) return LF2_ERR_ARG;
+  return pm_call(c, 0, np, cell, off3, mass, gmass, nullptr, nullptr, rho, nullptr, 0, 0, nullptr,
+                 nullptr, nullptr);
+}
+
+lf2_status lf2_pm_gather(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
+                         const float* F, float* out3)
+{
+  if (!cell || !off3 || !F || !out3) return LF2_ERR_ARG;
+  return pm_call(c, 1, np, cell, off3, nullptr, 0, F, nullptr, out3, nullptr, 0, 0, nullptr,
+                 nullptr, nullptr);
+}
+
+lf2_status lf2_pm_kick_drift(lf2_ctx* c, int64_t np, int32_t* cell, float* off3, float* vel3,
+                             const float* G3, double dt_kick, double dt_drift)
+{
+  if (!c || !cell || !off3 || !vel3) return LF2_ERR_ARG;
+  return pm_call(c, 2, np, nullptr, nullptr, nullptr, 0, G3, nullptr, nullptr, nullptr, dt_kick,
+                 dt_drift / c->res, cell, off3, vel3);
+}
+
+lf2_status lf2_pm_deposit_adjoint(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
+                                  const float* mass, double gmass, const float* g_rho,
+                                  float* g_off3, float* g_mass)
+{
+  if (!cell || !off3 || !g_rho) return LF2_ERR_ARG;
+  return pm_call(c, 3, np, cell, off3, mass, gmass, g_rho, nullptr, g_off3, g_mass, 0, 0, nullptr,
+                 nullptr, nullptr);
+}
+
+lf2_status lf2_pm_gather_adjoint(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
+                                 const float* F, const float* g_out3, float* g_F, float* g_off3)
+{
+  if (!cell || !off3 || !g_out3 || (g_off3 && !F)) return LF2_ERR_ARG;
+  return pm_call(c, 4, np, cell, off3, nullptr, 0, F, g_out3, g_F, g_off3, 0, 0, nullptr, nullptr,
+                 nullptr);
+}
+
+lf2_status lf2_stencil27(lf2_ctx* c, const float* rho, const float* S81, float* F3)
+{
+  if (!c || !rho || !S81 || !F3) return LF2_ERR_ARG;
+  PhaseScope ps(c, PH_OTHER);
+  LF2_CUDA(c, launch_stencil(c, 0, rho, S81, F3, nullptr));
+  return LF2_OK;
+}
+
+lf2_status lf2_stencil27_adjoint(lf2_ctx* c, const float* rho, const float* S81, const float* g_F3,
+                                 float* g_rho, float* g_S81)
+{
+  if (!c || !g_F3 || (g_rho && !S81) || (g_S81 && !rho)) return LF2_ERR_ARG;
+  PhaseScope ps(c, PH_OTHER);
+  if (g_rho) LF2_CUDA(c, launch_stencil(c, 1, g_F3, S81, g_rho, nullptr));
+  if (g_S81) {
+    if (!c->stencil_partial &&
+        cudaMalloc(&c->stencil_partial, sizeof(float) * stencil_partial_floats()) != cudaSuccess)
+      return fail(c, LF2_ERR_NOMEM, "cannot allocate stencil partial sums");
+    LF2_CUDA(c, launch_stencil(c, 2, g_F3, rho, g_S81, c->stencil_partial));
+  }
   return LF2_OK;
 }
 

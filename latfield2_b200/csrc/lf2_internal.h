@@ -92,6 +92,7 @@ struct lf2_ctx {
   double* brick_sums = nullptr;      // [nbricks * 5]
   double* stats = nullptr;           // [8] device
   uint64_t* spill = nullptr;         // deposit shell store (8-byte slots)
+  float* stencil_partial = nullptr;  // per-CTA partial sums of the stencil weight gradient
   size_t spill_slots = 0;
   double* h_stats = nullptr;         // pinned [8]
   uint32_t* h_flags = nullptr;       // pinned
@@ -144,6 +145,15 @@ cudaError_t launch_reduce_maxv(lf2_ctx* c);
 // lf2_deposit.cu
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
 cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
+
+// lf2_pm.cu (differentiable chain; op codes documented there)
+cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
+                      const float* mass, float gmass, const float* in_a, const float* in_b,
+                      float* out_a, float* out_b, float dta, float dtb, int32_t* cell_rw,
+                      float* off_rw, float* vel_rw);
+cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, float* out,
+                           float* partial);
+size_t stencil_partial_floats();
 
 // lf2_field.cu
 cudaError_t launch_export(lf2_ctx* c, int comps, const float* src, void* dst, int halo,

@@ -1,0 +1,141 @@
+"""GPU checks of the hand-written adjoint kernels and of the differentiable
+multi-step chain (latfield2_b200.autodiff.PMChain) against the FP64
+restatement in oracle/pm_chain.py (torch autograd in float64) and against
+FP64 central finite differences along random directions.
+
+Tolerances: single adjoint kernels 2e-5 of the gradient's norm; the 8-step
+chain 2e-3 of each gradient's norm (FP32 particle state through 8 steps);
+directional derivatives within 5e-3 of the rms directional derivative."""
+import numpy as np
+import pytest
+
+from oracle import pm_chain as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = a.double().reshape(-1)
+    b = b.double().reshape(-1)
+    return float((a - b).norm() / max(float(b.norm()), 1e-300))
+
+
+def _case(n, npart, seed, device):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    pos = torch.rand(npart, 3, generator=g, dtype=torch.float64)
+    vel = 0.02 * torch.randn(npart, 3, generator=g, dtype=torch.float64)
+    m = (1.0 + 0.1 * (2 * torch.rand(npart, generator=g, dtype=torch.float64) - 1)) / npart
+    S = 0.02 * torch.randn(81, generator=g, dtype=torch.float64)
+    w = torch.randn(n ** 3, generator=g, dtype=torch.float64)
+    return [t.to(device) for t in (pos, vel, m, S, w)]
+
+
+def _state(pos, n):
+    from latfield2_b200.autodiff import positions_to_state
+    return positions_to_state(pos, (n, n, n), 1.0 / n)
+
+
+def test_single_adjoint_kernels(cuda):
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops
+    n, npart = 24, 5000
+    pos, vel, m, S, w = _case(n, npart, 1, "cuda")
+    ctx = L.Context((n, n, n), box=1.0)
+    ops = _Ops(ctx)
+    cell, off = _state(pos, n)
+    # the FP64 positions the device sees
+    posd = ((torch.stack([cell.long() % n, (cell.long() // n) % n, cell.long() // (n * n)], 1)
+             .double() + off.double()) / n)
+    m32 = m.float().contiguous()
+    nn = (n, n, n)
+    # deposit adjoint
+    g_rho = torch.randn(n ** 3, dtype=torch.float64, device="cuda")
+    x = posd.clone().requires_grad_(True)
+    mm = m32.double().clone().requires_grad_(True)
+    (P.deposit(x, mm, nn) * g_rho).sum().backward()
+    g_off = torch.zeros(npart, 3, device="cuda")
+    g_m = torch.zeros(npart, device="cuda")
+    ops.deposit_adj(cell, off, m32, g_rho.float().contiguous(), g_off, g_m)
+    assert _rel(g_off * n, x.grad) < 2e-5
+    assert _rel(g_m, mm.grad) < 2e-5
+    # gather adjoint
+    F = torch.randn(3, n ** 3, dtype=torch.float64, device="cuda")
+    gG = torch.randn(npart, 3, dtype=torch.float64, device="cuda")
+    x = posd.clone().requires_grad_(True)
+    Fr = F.clone().requires_grad_(True)
+    (P.gather(x, Fr, nn) * gG).sum().backward()
+    g_F = torch.zeros(3 * n ** 3, device="cuda")
+    g_off = torch.zeros(npart, 3, device="cuda")
+    ops.gather_adj(cell, off, F.float().reshape(-1).contiguous(), gG.float().contiguous(), g_F, g_off)
+    assert _rel(g_off * n, x.grad) < 2e-5
+    assert _rel(g_F, Fr.grad) < 2e-5
+    # gather and deposit forward
+    G = torch.empty(npart, 3, device="cuda")
+    ops.gather(cell, off, F.float().reshape(-1).contiguous(), G)
+    assert _rel(G, P.gather(posd, F, nn)) < 2e-6
+    rho = torch.zeros(n ** 3, device="cuda")
+    ops.deposit(cell, off, m32, rho)
+    assert _rel(rho, P.deposit(posd, m32.double(), nn)) < 2e-6
+    # stencil and its adjoint
+    r = torch.randn(n ** 3, dtype=torch.float64, device="cuda")
+    F32 = torch.empty(3 * n ** 3, device="cuda")
+    ops.stencil(r.float().contiguous(), S.float().contiguous(), F32)
+    assert _rel(F32, P.stencil(r, S, nn)) < 2e-6
+    gF = torch.randn(3, n ** 3, dtype=torch.float64, device="cuda")
+    rr = r.clone().requires_grad_(True)
+    Sr = S.clone().requires_grad_(True)
+    (P.stencil(rr, Sr, nn) * gF).sum().backward()
+    g_r = torch.zeros(n ** 3, device="cuda")
+    g_S = torch.zeros(81, device="cuda")
+    ops.stencil_adj(r.float().contiguous(), S.float().contiguous(), gF.float().reshape(-1).contiguous(),
+                    g_r, g_S)
+    assert _rel(g_r, rr.grad) < 2e-5
+    assert _rel(g_S, Sr.grad) < 2e-5
+
+
+@pytest.mark.parametrize("n,npart,ndir", [(32, 20000, 1000)])
+def test_chain_gradients_against_fp64(cuda, n, npart, ndir):
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import pm_chain_loss
+    steps, dt = 8, 0.1
+    pos, vel, m, S, w = _case(n, npart, 7, "cuda")
+    # FP64 chain on the positions the device represents (FP32 offsets)
+    cell, off = _state(pos, n)
+    posd = ((torch.stack([cell.long() % n, (cell.long() // n) % n, cell.long() // (n * n)], 1)
+             .double() + off.double()) / n)
+    vel = vel.float().double()
+    m = m.float().double()
+    S = S.float().double()
+    w = w.float().double()
+    ctx = L.Context((n, n, n), box=1.0)
+    leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, S, w)]
+    loss = pm_chain_loss(ctx, *leaves, steps=steps, dt=dt, checkpoint_every=2)
+    loss.backward()
+    got = [t.grad for t in leaves]
+    ref_leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, S, w)]
+    ref_loss = P.chain_loss(*ref_leaves, (n, n, n), steps, dt)
+    ref = torch.autograd.grad(ref_loss, ref_leaves)
+    assert float(loss.detach()) == pytest.approx(float(ref_loss.detach()), rel=2e-4)
+    for name, a, b in zip(("pos", "vel", "mass", "stencil", "weights"), got, ref):
+        assert _rel(a, b) < 2e-3, name
+    # FP64 central differences of the FP64 chain along random directions
+    rng = np.random.default_rng(11)
+    base = [posd, vel, m, S]
+    fd, an_dev, an_ref = [], [], []
+    for _ in range(ndir):
+        us = [torch.from_numpy(rng.standard_normal(tuple(t.shape))).to("cuda") for t in base]
+        nrm = float(torch.sqrt(sum((u ** 2).sum() for u in us)))
+        us = [u / nrm for u in us]
+        with torch.no_grad():
+            d, _ = P.directional_fd(base, us, w, (n, n, n), steps, dt, eps=1e-7)
+        assert d is not None  # an eps without face crossings exists
+        fd.append(d)
+        an_dev.append(float(sum((g * u).sum() for g, u in zip(got[:4], us))))
+        an_ref.append(float(sum((g * u).sum() for g, u in zip(ref[:4], us))))
+    fd, an_dev, an_ref = map(np.array, (fd, an_dev, an_ref))
+    scale = np.sqrt(np.mean(fd ** 2))
+    assert np.max(np.abs(an_ref - fd)) < 1e-5 * scale  # the FP64 reference gradient
+    assert np.max(np.abs(an_dev - fd)) < 5e-3 * scale  # the CUDA adjoint
