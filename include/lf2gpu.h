@@ -187,20 +187,22 @@ lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
  * move_particles_simple (move_function.hpp:15-32).  All pointers are device
  * pointers; offsets and offset gradients are in cell units; outputs marked
  * (+=) are accumulated.  mass may be NULL (global mass gmass).
+ * The force field F4 and its gradient g_F4 hold one float4 (x, y, z, unused)
+ * per site, in site order, 16-byte aligned (LF2_ERR_ARG otherwise).
  *   deposit          rho (+=) m/res^3 W                (FP32 atomics)
- *   gather           out3[p] = sum_k W_k F(corner_k)
+ *   gather           out3[p] = sum_k W_k F4(corner_k)
  *   kick_drift       vel += dt_kick * G3 (G3 may be NULL); off += dt_drift/res
  *                    * vel with the carry into cell
  *   deposit_adjoint  g_off3 (+=), g_mass (+=) from g_rho
- *   gather_adjoint   g_F (+=) CIC deposit of g_out3; g_off3 (+=)
- *   stencil27        F3_c(g) = sum_o S[c*27 + (dz+1)*9 + (dy+1)*3 + (dx+1)]
+ *   gather_adjoint   g_F4 (+=) CIC deposit of g_out3; g_off3 (+=)
+ *   stencil27        F4_c(g) = sum_o S[c*27 + (dz+1)*9 + (dy+1)*3 + (dx+1)]
  *                    rho(g + o), periodic, S81 on the device
- *   stencil27_adjoint g_rho (+=) and g_S81 (+=) from g_F3 */
+ *   stencil27_adjoint g_rho (+=) and g_S81 (+=) from g_F4 */
 lf2_status lf2_pm_deposit(lf2_ctx* ctx, int64_t np, const int32_t* cell,
                           const float* off3, const float* mass, double gmass,
                           float* rho);
 lf2_status lf2_pm_gather(lf2_ctx* ctx, int64_t np, const int32_t* cell,
-                         const float* off3, const float* F, float* out3);
+                         const float* off3, const float* F4, float* out3);
 lf2_status lf2_pm_kick_drift(lf2_ctx* ctx, int64_t np, int32_t* cell,
                              float* off3, float* vel3, const float* G3,
                              double dt_kick, double dt_drift);
@@ -211,12 +213,12 @@ lf2_status lf2_pm_deposit_adjoint(lf2_ctx* ctx, int64_t np,
                                   float* g_mass);
 lf2_status lf2_pm_gather_adjoint(lf2_ctx* ctx, int64_t np,
                                  const int32_t* cell, const float* off3,
-                                 const float* F, const float* g_out3,
-                                 float* g_F, float* g_off3);
+                                 const float* F4, const float* g_out3,
+                                 float* g_F4, float* g_off3);
 lf2_status lf2_stencil27(lf2_ctx* ctx, const float* rho, const float* S81,
-                         float* F3);
+                         float* F4);
 lf2_status lf2_stencil27_adjoint(lf2_ctx* ctx, const float* rho,
-                                 const float* S81, const float* g_F3,
+                                 const float* S81, const float* g_F4,
                                  float* g_rho, float* g_S81);
 
 /* ---------------------------------------------------------- no allocation

@@ -86,7 +86,7 @@ class _Ops:
         dev = cell.device
         rho = torch.zeros(self.ns, dtype=torch.float32, device=dev)
         self.deposit(cell, off, m, rho)
-        F = torch.empty(3 * self.ns, dtype=torch.float32, device=dev)
+        F = torch.empty(4 * self.ns, dtype=torch.float32, device=dev)  # float4 per site
         self.stencil(rho, S, F)
         return rho, F
 
@@ -153,7 +153,7 @@ class PMChain(torch.autograd.Function):
             g_v += (dt / res) * g_off
             # kick v_{k+1} = v_k + dt G_k
             g_G = (dt * g_v).contiguous()
-            g_F = torch.zeros(3 * lf2ctx.nsites, dtype=torch.float32, device=dev)
+            g_F = torch.zeros(4 * lf2ctx.nsites, dtype=torch.float32, device=dev)
             ops.gather_adj(cell_k, off_k, Fs[k], g_G, g_F, g_off)
             g_rho = torch.zeros(lf2ctx.nsites, dtype=torch.float32, device=dev)
             ops.stencil_adj(rhos[k], S32, g_F, g_rho, g_S)

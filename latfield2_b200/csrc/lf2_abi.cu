@@ -748,6 +748,9 @@ lf2_status lf2_conservation(lf2_ctx* c, double* mass, double mom[3], double* max
   return LF2_OK;
 }
 
+// F4 fields hold one float4 per site and must start on a 16-byte boundary.
+static bool f4_ok(const float* p) { return !p || ((uintptr_t)p & 15) == 0; }
+
 static lf2_status pm_call(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
                           const float* mass, double gmass, const float* in_a, const float* in_b,
                           float* out_a, float* out_b, double dta, double dtb, int32_t* cell_rw,
@@ -770,10 +773,10 @@ lf2_status lf2_pm_deposit(lf2_ctx* c, int64_t np, const int32_t* cell, const flo
 }
 
 lf2_status lf2_pm_gather(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
-                         const float* F, float* out3)
+                         const float* F4, float* out3)
 {
-  if (!cell || !off3 || !F || !out3) return LF2_ERR_ARG;
-  return pm_call(c, 1, np, cell, off3, nullptr, 0, F, nullptr, out3, nullptr, 0, 0, nullptr,
+  if (!cell || !off3 || !F4 || !out3 || !f4_ok(F4)) return LF2_ERR_ARG;
+  return pm_call(c, 1, np, cell, off3, nullptr, 0, F4, nullptr, out3, nullptr, 0, 0, nullptr,
                  nullptr, nullptr);
 }
 
@@ -795,32 +798,33 @@ lf2_status lf2_pm_deposit_adjoint(lf2_ctx* c, int64_t np, const int32_t* cell, c
 }
 
 lf2_status lf2_pm_gather_adjoint(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
-                                 const float* F, const float* g_out3, float* g_F, float* g_off3)
+                                 const float* F4, const float* g_out3, float* g_F4, float* g_off3)
 {
-  if (!cell || !off3 || !g_out3 || (g_off3 && !F)) return LF2_ERR_ARG;
-  return pm_call(c, 4, np, cell, off3, nullptr, 0, F, g_out3, g_F, g_off3, 0, 0, nullptr, nullptr,
+  if (!cell || !off3 || !g_out3 || (g_off3 && !F4) || !f4_ok(F4) || !f4_ok(g_F4))
+    return LF2_ERR_ARG;
+  return pm_call(c, 4, np, cell, off3, nullptr, 0, F4, g_out3, g_F4, g_off3, 0, 0, nullptr, nullptr,
                  nullptr);
 }
 
-lf2_status lf2_stencil27(lf2_ctx* c, const float* rho, const float* S81, float* F3)
+lf2_status lf2_stencil27(lf2_ctx* c, const float* rho, const float* S81, float* F4)
 {
-  if (!c || !rho || !S81 || !F3) return LF2_ERR_ARG;
+  if (!c || !rho || !S81 || !F4 || !f4_ok(F4)) return LF2_ERR_ARG;
   PhaseScope ps(c, PH_OTHER);
-  LF2_CUDA(c, launch_stencil(c, 0, rho, S81, F3, nullptr));
+  LF2_CUDA(c, launch_stencil(c, 0, rho, S81, F4, nullptr));
   return LF2_OK;
 }
 
-lf2_status lf2_stencil27_adjoint(lf2_ctx* c, const float* rho, const float* S81, const float* g_F3,
+lf2_status lf2_stencil27_adjoint(lf2_ctx* c, const float* rho, const float* S81, const float* g_F4,
                                  float* g_rho, float* g_S81)
 {
-  if (!c || !g_F3 || (g_rho && !S81) || (g_S81 && !rho)) return LF2_ERR_ARG;
+  if (!c || !g_F4 || !f4_ok(g_F4) || (g_rho && !S81) || (g_S81 && !rho)) return LF2_ERR_ARG;
   PhaseScope ps(c, PH_OTHER);
-  if (g_rho) LF2_CUDA(c, launch_stencil(c, 1, g_F3, S81, g_rho, nullptr));
+  if (g_rho) LF2_CUDA(c, launch_stencil(c, 1, g_F4, S81, g_rho, nullptr));
   if (g_S81) {
     if (!c->stencil_partial &&
-        cudaMalloc(&c->stencil_partial, sizeof(float) * stencil_partial_floats()) != cudaSuccess)
+        cudaMalloc(&c->stencil_partial, sizeof(float) * stencil_partial_floats(c)) != cudaSuccess)
       return fail(c, LF2_ERR_NOMEM, "cannot allocate stencil partial sums");
-    LF2_CUDA(c, launch_stencil(c, 2, g_F3, rho, g_S81, c->stencil_partial));
+    LF2_CUDA(c, launch_stencil(c, 2, g_F4, rho, g_S81, c->stencil_partial));
   }
   return LF2_OK;
 }

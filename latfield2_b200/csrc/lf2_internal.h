@@ -153,7 +153,7 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
                       float* off_rw, float* vel_rw);
 cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, float* out,
                            float* partial);
-size_t stencil_partial_floats();
+size_t stencil_partial_floats(const lf2_ctx* c);
 
 // lf2_field.cu
 cudaError_t launch_export(lf2_ctx* c, int comps, const float* src, void* dst, int halo,

@@ -18,7 +18,9 @@
 //   stencil   gR(h)     = sum_c sum_o S[c][o] gF_c(h - o)
 //             dL/dS[c][o] = sum_g gF_c(g) rho(g + o)
 // dW/dfx = (bx ? 1 : -1) * wy * wz, etc.  Offsets and their gradients are in
-// cell units; positions in box units are (cell + off) * res.
+// cell units; positions in box units are (cell + off) * res.  The force field
+// F and its gradient are stored as one float4 (x, y, z, unused) per site, so
+// that a corner is one 16-byte load and one vector atomic.
 #include <cuda_runtime.h>
 
 #include "lf2_internal.h"
@@ -78,7 +80,7 @@ __global__ void k_pm_deposit(Geom g, int64_t np, const int32_t* __restrict__ cel
 }
 
 __global__ void k_pm_gather(Geom g, int64_t np, const int32_t* __restrict__ cell,
-                            const float* __restrict__ off3, const float* __restrict__ F,
+                            const float* __restrict__ off3, const float4* __restrict__ F4,
                             float* __restrict__ out3)
 {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
@@ -87,9 +89,12 @@ __global__ void k_pm_gather(Geom g, int64_t np, const int32_t* __restrict__ cell
     corners(g, cell[p], off3, p, k);
     float a[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-    for (int q = 0; q < 8; q++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) a[c] = fmaf(k.w[q], __ldg(F + c * g.nsites + k.site[q]), a[c]);
+    for (int q = 0; q < 8; q++) {
+      const float4 f = __ldg(F4 + k.site[q]);
+      a[0] = fmaf(k.w[q], f.x, a[0]);
+      a[1] = fmaf(k.w[q], f.y, a[1]);
+      a[2] = fmaf(k.w[q], f.z, a[2]);
+    }
     for (int c = 0; c < 3; c++) out3[3 * p + c] = a[c];
   }
 }
@@ -151,8 +156,8 @@ __global__ void k_pm_deposit_adj(Geom g, int64_t np, const int32_t* __restrict__
 }
 
 __global__ void k_pm_gather_adj(Geom g, int64_t np, const int32_t* __restrict__ cell,
-                                const float* __restrict__ off3, const float* __restrict__ F,
-                                const float* __restrict__ gG3, float* __restrict__ gF,
+                                const float* __restrict__ off3, const float4* __restrict__ F4,
+                                const float* __restrict__ gG3, float4* __restrict__ gF4,
                                 float* __restrict__ g_off3)
 {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
@@ -163,123 +168,178 @@ __global__ void k_pm_gather_adj(Geom g, int64_t np, const int32_t* __restrict__ 
     float d[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      float dot = 0.f;
-      for (int c = 0; c < 3; c++) {
-        if (gF) atomicAdd(&gF[c * g.nsites + k.site[q]], k.w[q] * gg[c]);
-        if (g_off3) dot = fmaf(gg[c], __ldg(F + c * g.nsites + k.site[q]), dot);
-      }
-      if (g_off3)
+      if (gF4) atomicAdd(&gF4[k.site[q]], make_float4(k.w[q] * gg[0], k.w[q] * gg[1], k.w[q] * gg[2], 0.f));
+      if (g_off3) {
+        const float4 f = __ldg(F4 + k.site[q]);
+        const float dot = fmaf(gg[0], f.x, fmaf(gg[1], f.y, gg[2] * f.z));
         for (int c = 0; c < 3; c++) d[c] = fmaf(k.dw[q][c], dot, d[c]);
+      }
     }
     if (g_off3)
       for (int c = 0; c < 3; c++) g_off3[3 * p + c] += d[c];
   }
 }
 
+// The three stencil kernels work on tiles of SX x SY x SZ sites, one CTA of
+// SX x SY threads per tile; each thread walks one z-column of the tile.  The
+// tile's input with a 1-site periodic halo is staged in shared memory, so
+// every input value is read from global memory about 1.5 times.
+constexpr int SX = 32, SY = 8, SZ = 8;
+constexpr int HX = SX + 2, HY = SY + 2, HZ = SZ + 2;
+constexpr int STENCIL_THREADS = SX * SY;
+
+struct Tile {
+  int x0, y0, z0, tx, ty;
+};
+
+__device__ inline Tile tile_of()
+{
+  return {(int)blockIdx.x * SX, (int)blockIdx.y * SY, (int)blockIdx.z * SZ, (int)threadIdx.x % SX,
+          (int)threadIdx.x / SX};
+}
+
+// halo site t of the tile (t < HX*HY*HZ) -> periodic global site index
+__device__ inline int64_t halo_site(const Geom& g, const Tile& T, int t)
+{
+  const int i = t % HX, j = (t / HX) % HY, k = t / (HX * HY);
+  return site_index(g, wrap_add(T.x0, i - 1, g.n[0]), wrap_add(T.y0, j - 1, g.n[1]),
+                    wrap_add(T.z0, k - 1, g.n[2]));
+}
+
 // F_c(g) = sum_o S[c][o] rho(g + o); o = (dz, dy, dx) in {-1,0,1}^3,
 // S index c*27 + (dz+1)*9 + (dy+1)*3 + (dx+1).
-__global__ void k_stencil(Geom g, const float* __restrict__ rho, const float* __restrict__ S,
-                          float* __restrict__ F)
+__global__ void __launch_bounds__(STENCIL_THREADS) k_stencil(Geom g, const float* __restrict__ rho,
+                                                             const float* __restrict__ S,
+                                                             float4* __restrict__ F4)
 {
   __shared__ float s[81];
+  __shared__ float r[HZ][HY][HX];
+  const Tile T = tile_of();
   if (threadIdx.x < 81) s[threadIdx.x] = S[threadIdx.x];
+  for (int t = threadIdx.x; t < HX * HY * HZ; t += STENCIL_THREADS)
+    (&r[0][0][0])[t] = __ldg(rho + halo_site(g, T, t));
   __syncthreads();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.nsites;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % g.n[0]), y = (int)((i / g.n[0]) % g.n[1]),
-              z = (int)(i / ((int64_t)g.n[0] * g.n[1]));
+  const int x = T.x0 + T.tx, y = T.y0 + T.ty;
+  if (x >= g.n[0] || y >= g.n[1]) return;
+  for (int kz = 0; kz < SZ && T.z0 + kz < g.n[2]; kz++) {
     float a[3] = {0.f, 0.f, 0.f};
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          const float r = __ldg(rho + site_index(g, wrap_add(x, dx, g.n[0]), wrap_add(y, dy, g.n[1]),
-                                                 wrap_add(z, dz, g.n[2])));
-          const int o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-          for (int c = 0; c < 3; c++) a[c] = fmaf(s[c * 27 + o], r, a[c]);
-        }
-    for (int c = 0; c < 3; c++) F[c * g.nsites + i] = a[c];
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      const float v = r[kz + o / 9][T.ty + (o / 3) % 3][T.tx + o % 3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) a[c] = fmaf(s[c * 27 + o], v, a[c]);
+    }
+    F4[site_index(g, x, y, T.z0 + kz)] = make_float4(a[0], a[1], a[2], 0.f);
   }
 }
 
 // gR(h) = sum_c sum_o S[c][o] gF_c(h - o)
-__global__ void k_stencil_adj_rho(Geom g, const float* __restrict__ gF, const float* __restrict__ S,
-                                  float* __restrict__ g_rho)
+__global__ void __launch_bounds__(STENCIL_THREADS) k_stencil_adj_rho(Geom g,
+                                                                     const float4* __restrict__ gF4,
+                                                                     const float* __restrict__ S,
+                                                                     float* __restrict__ g_rho)
 {
   __shared__ float s[81];
+  __shared__ float f[3][HZ][HY][HX];
+  const Tile T = tile_of();
   if (threadIdx.x < 81) s[threadIdx.x] = S[threadIdx.x];
+  for (int t = threadIdx.x; t < HX * HY * HZ; t += STENCIL_THREADS) {
+    const float4 v = __ldg(gF4 + halo_site(g, T, t));
+    (&f[0][0][0][0])[t] = v.x;
+    (&f[1][0][0][0])[t] = v.y;
+    (&f[2][0][0][0])[t] = v.z;
+  }
   __syncthreads();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.nsites;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % g.n[0]), y = (int)((i / g.n[0]) % g.n[1]),
-              z = (int)(i / ((int64_t)g.n[0] * g.n[1]));
+  const int x = T.x0 + T.tx, y = T.y0 + T.ty;
+  if (x >= g.n[0] || y >= g.n[1]) return;
+  for (int kz = 0; kz < SZ && T.z0 + kz < g.n[2]; kz++) {
     float a = 0.f;
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          const int64_t src = site_index(g, wrap_add(x, -dx, g.n[0]), wrap_add(y, -dy, g.n[1]),
-                                         wrap_add(z, -dz, g.n[2]));
-          const int o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-          for (int c = 0; c < 3; c++) a = fmaf(s[c * 27 + o], __ldg(gF + c * g.nsites + src), a);
-        }
-    g_rho[i] += a;
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      // h - o for o = (dz, dy, dx): halo offset (1 - d) per axis
+      const int k = kz + 2 - o / 9, j = T.ty + 2 - (o / 3) % 3, i = T.tx + 2 - o % 3;
+#pragma unroll
+      for (int c = 0; c < 3; c++) a = fmaf(s[c * 27 + o], f[c][k][j][i], a);
+    }
+    g_rho[site_index(g, x, y, T.z0 + kz)] += a;
   }
 }
 
-// Per-CTA partial sums of gS[c][o] = sum_g gF_c(g) rho(g + o); blockIdx.y is
-// the component c (27 values per thread).  k_stencil_adj_S_sum adds the CTA
-// partials in a fixed order.
-__global__ void __launch_bounds__(PM_THREADS) k_stencil_adj_S(Geom g, const float* __restrict__ gF,
-                                                              const float* __restrict__ rho,
-                                                              float* __restrict__ partial)
+// gS[c][o] = sum_g gF_c(g) rho(g + o).  Every thread keeps the 81 sums of
+// its z-column in registers; the warps reduce them with shuffles, the CTA
+// adds its 8 warps in order and writes one row of `partial` per tile;
+// k_stencil_adj_S_sum adds the rows in a fixed order.
+__global__ void __launch_bounds__(STENCIL_THREADS) k_stencil_adj_S(Geom g,
+                                                                   const float4* __restrict__ gF4,
+                                                                   const float* __restrict__ rho,
+                                                                   float* __restrict__ partial)
 {
-  __shared__ float red[PM_THREADS / 32][27];
-  const int c = blockIdx.y;
-  float acc[27];
-  for (int j = 0; j < 27; j++) acc[j] = 0.f;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.nsites;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % g.n[0]), y = (int)((i / g.n[0]) % g.n[1]),
-              z = (int)(i / ((int64_t)g.n[0] * g.n[1]));
-    const float f = __ldg(gF + c * g.nsites + i);
+  __shared__ float r[HZ][HY][HX];
+  __shared__ float red[STENCIL_THREADS / 32][81];
+  const Tile T = tile_of();
+  for (int t = threadIdx.x; t < HX * HY * HZ; t += STENCIL_THREADS)
+    (&r[0][0][0])[t] = __ldg(rho + halo_site(g, T, t));
+  __syncthreads();
+  float acc[81];
 #pragma unroll
-    for (int dz = -1; dz <= 1; dz++)
+  for (int q = 0; q < 81; q++) acc[q] = 0.f;
+  const int x = T.x0 + T.tx, y = T.y0 + T.ty;
+  if (x < g.n[0] && y < g.n[1]) {
+    for (int kz = 0; kz < SZ && T.z0 + kz < g.n[2]; kz++) {
+      const float4 q = __ldg(gF4 + site_index(g, x, y, T.z0 + kz));
 #pragma unroll
-      for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-        for (int dx = -1; dx <= 1; dx++) {
-          const float r = __ldg(rho + site_index(g, wrap_add(x, dx, g.n[0]), wrap_add(y, dy, g.n[1]),
-                                                 wrap_add(z, dz, g.n[2])));
-          const int o = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-          acc[o] = fmaf(f, r, acc[o]);
-        }
+      for (int o = 0; o < 27; o++) {
+        const float v = r[kz + o / 9][T.ty + (o / 3) % 3][T.tx + o % 3];
+        acc[o] = fmaf(q.x, v, acc[o]);
+        acc[27 + o] = fmaf(q.y, v, acc[27 + o]);
+        acc[54 + o] = fmaf(q.z, v, acc[54 + o]);
+      }
+    }
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int j = 0; j < 27; j++) {
-    float v = acc[j];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[w][j] = v;
+  for (int q = 0; q < 81; q++) {
+    float v = acc[q];
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    if (lane == 0) red[warp][q] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 27) {
+  if (threadIdx.x < 81) {
+    const int64_t tile = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
     float v = 0.f;
-    for (int k = 0; k < PM_THREADS / 32; k++) v += red[k][threadIdx.x];
-    partial[blockIdx.x * 81 + c * 27 + threadIdx.x] = v;
+    for (int w = 0; w < STENCIL_THREADS / 32; w++) v += red[w][threadIdx.x];
+    partial[tile * 81 + threadIdx.x] = v;
   }
 }
 
-__global__ void k_stencil_adj_S_sum(int nblocks, const float* __restrict__ partial, float* gS)
+__global__ void k_stencil_adj_S_sum(int ntiles, const float* __restrict__ partial, float* gS)
 {
-  if (threadIdx.x < 81) {
+  __shared__ float red[4][81];
+  // 4 x 81 threads: each sums a quarter of the tiles, then the quarters
+  const int out = threadIdx.x % 81, q = threadIdx.x / 81;
+  if (threadIdx.x < 324) {
     float v = 0.f;
-    for (int b = 0; b < nblocks; b++) v += partial[b * 81 + threadIdx.x];
-    gS[threadIdx.x] += v;
+    for (int t = q; t < ntiles; t += 4) v += partial[(size_t)t * 81 + out];
+    red[q][out] = v;
   }
+  __syncthreads();
+  if (threadIdx.x < 81) gS[threadIdx.x] += (red[0][threadIdx.x] + red[1][threadIdx.x]) +
+                                           (red[2][threadIdx.x] + red[3][threadIdx.x]);
 }
 
 }  // namespace
 
-constexpr int STENCIL_S_BLOCKS = 148 * 2;
+inline dim3 stencil_grid(const Geom& g)
+{
+  return dim3((g.n[0] + SX - 1) / SX, (g.n[1] + SY - 1) / SY, (g.n[2] + SZ - 1) / SZ);
+}
+
+inline int64_t stencil_tiles(const Geom& g)
+{
+  const dim3 d = stencil_grid(g);
+  return (int64_t)d.x * d.y * d.z;
+}
 
 cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
                       const float* mass, float gmass, const float* in_a, const float* in_b,
@@ -295,10 +355,10 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
       k_pm_deposit<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3, mass,
                                                                             gmass, inv_vol, out_a);
       break;
-    case 1:  // gather in_a (F) -> out_a (np x 3)
+    case 1:  // gather in_a (F4) -> out_a (np x 3)
       c->launches += 1;
-      k_pm_gather<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3, in_a,
-                                                                           out_a);
+      k_pm_gather<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+          g, np, cell, off3, reinterpret_cast<const float4*>(in_a), out_a);
       break;
     case 2:  // kick (in_a = G, may be NULL) + drift
       c->launches += 1;
@@ -310,10 +370,11 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
       k_pm_deposit_adj<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
           g, np, cell, off3, mass, gmass, inv_vol, in_a, out_a, out_b);
       break;
-    case 4:  // gather adjoint: in_a = F, in_b = gG; out_a = gF (+=), out_b = g_off (+=)
+    case 4:  // gather adjoint: in_a = F4, in_b = gG; out_a = gF4 (+=), out_b = g_off (+=)
       c->launches += 1;
       k_pm_gather_adj<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
-          g, np, cell, off3, in_a, in_b, out_a, out_b);
+          g, np, cell, off3, reinterpret_cast<const float4*>(in_a), in_b,
+          reinterpret_cast<float4*>(out_a), out_b);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -325,20 +386,23 @@ cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, f
                            float* partial)
 {
   const Geom g = c->g;
-  if (op == 0) {
+  const dim3 grid = stencil_grid(g);
+  if (op == 0) {  // a = rho -> out = F4
     c->launches += 1;
-    k_stencil<<<grid_for(g.nsites, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, a, S, out);
-  } else if (op == 1) {  // a = gF -> out = g_rho (+=)
+    k_stencil<<<grid, STENCIL_THREADS, 0, c->stream>>>(g, a, S, reinterpret_cast<float4*>(out));
+  } else if (op == 1) {  // a = gF4 -> out = g_rho (+=)
     c->launches += 1;
-    k_stencil_adj_rho<<<grid_for(g.nsites, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, a, S, out);
-  } else {  // a = gF, S = rho -> out = gS (+=)
+    k_stencil_adj_rho<<<grid, STENCIL_THREADS, 0, c->stream>>>(
+        g, reinterpret_cast<const float4*>(a), S, out);
+  } else {  // a = gF4, S = rho -> out = gS (+=)
     c->launches += 2;
-    k_stencil_adj_S<<<dim3(STENCIL_S_BLOCKS, 3), PM_THREADS, 0, c->stream>>>(g, a, S, partial);
-    k_stencil_adj_S_sum<<<1, 128, 0, c->stream>>>(STENCIL_S_BLOCKS, partial, out);
+    k_stencil_adj_S<<<grid, STENCIL_THREADS, 0, c->stream>>>(
+        g, reinterpret_cast<const float4*>(a), S, partial);
+    k_stencil_adj_S_sum<<<1, 352, 0, c->stream>>>((int)stencil_tiles(g), partial, out);
   }
   return cudaGetLastError();
 }
 
-size_t stencil_partial_floats() { return (size_t)STENCIL_S_BLOCKS * 81; }
+size_t stencil_partial_floats(const lf2_ctx* c) { return (size_t)stencil_tiles(c->g) * 81; }
 
 }  // namespace lf2

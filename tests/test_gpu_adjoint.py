@@ -66,31 +66,35 @@ def test_single_adjoint_kernels(cuda):
     x = posd.clone().requires_grad_(True)
     Fr = F.clone().requires_grad_(True)
     (P.gather(x, Fr, nn) * gG).sum().backward()
-    g_F = torch.zeros(3 * n ** 3, device="cuda")
+    F4 = torch.zeros(n ** 3, 4, device="cuda")
+    F4[:, :3] = F.float().t()
+    g_F4 = torch.zeros(n ** 3, 4, device="cuda")
     g_off = torch.zeros(npart, 3, device="cuda")
-    ops.gather_adj(cell, off, F.float().reshape(-1).contiguous(), gG.float().contiguous(), g_F, g_off)
+    ops.gather_adj(cell, off, F4, gG.float().contiguous(), g_F4, g_off)
     assert _rel(g_off * n, x.grad) < 2e-5
-    assert _rel(g_F, Fr.grad) < 2e-5
+    assert _rel(g_F4[:, :3].t(), Fr.grad) < 2e-5
+    assert float(g_F4[:, 3].abs().max()) == 0.0
     # gather and deposit forward
     G = torch.empty(npart, 3, device="cuda")
-    ops.gather(cell, off, F.float().reshape(-1).contiguous(), G)
+    ops.gather(cell, off, F4, G)
     assert _rel(G, P.gather(posd, F, nn)) < 2e-6
     rho = torch.zeros(n ** 3, device="cuda")
     ops.deposit(cell, off, m32, rho)
     assert _rel(rho, P.deposit(posd, m32.double(), nn)) < 2e-6
     # stencil and its adjoint
     r = torch.randn(n ** 3, dtype=torch.float64, device="cuda")
-    F32 = torch.empty(3 * n ** 3, device="cuda")
+    F32 = torch.empty(n ** 3, 4, device="cuda")
     ops.stencil(r.float().contiguous(), S.float().contiguous(), F32)
-    assert _rel(F32, P.stencil(r, S, nn)) < 2e-6
+    assert _rel(F32[:, :3].t(), P.stencil(r, S, nn)) < 2e-6
     gF = torch.randn(3, n ** 3, dtype=torch.float64, device="cuda")
     rr = r.clone().requires_grad_(True)
     Sr = S.clone().requires_grad_(True)
     (P.stencil(rr, Sr, nn) * gF).sum().backward()
     g_r = torch.zeros(n ** 3, device="cuda")
     g_S = torch.zeros(81, device="cuda")
-    ops.stencil_adj(r.float().contiguous(), S.float().contiguous(), gF.float().reshape(-1).contiguous(),
-                    g_r, g_S)
+    gF4 = torch.zeros(n ** 3, 4, device="cuda")
+    gF4[:, :3] = gF.float().t()
+    ops.stencil_adj(r.float().contiguous(), S.float().contiguous(), gF4, g_r, g_S)
     assert _rel(g_r, rr.grad) < 2e-5
     assert _rel(g_S, Sr.grad) < 2e-5
 
