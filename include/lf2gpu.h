@@ -62,6 +62,7 @@ typedef int lf2_status;
 #define LF2_FLAG_REPACK 0x8u         /* informational: store was repacked */
 #define LF2_FLAG_CAPACITY 0x10u      /* repack did not fit: state lost */
 #define LF2_FLAG_FIXED_OVERFLOW 0x20u /* fixed-point vertex sum overflowed */
+#define LF2_FLAG_TIMEOUT 0x40u       /* a bounded in-kernel wait gave up */
 
 /* ------------------------------------------------------------------ context
  * Replaces Lattice(3, n, halo) + Particles::initialize(info, type, &lat_part,
@@ -171,6 +172,12 @@ lf2_status lf2_drift_rebin(lf2_ctx* ctx, double dtau);
  * when rho is not NULL, by the scalar deposit of the new positions. */
 lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
                     double dtau_drift, lf2_field rho);
+/* Kernel of lf2_step's kick-drift-rebin pass: 0 automatic (currently the
+ * per-brick kernel), 1 the per-brick kernel, 2 the persistent TMA-pipelined
+ * kernel (needs n0 % 4 == 0, every n >= 32 and F 16-byte aligned, else
+ * LF2_ERR_UNSUPPORTED).  Both give the same particles (the order of the
+ * particles inside a brick may differ); no reference counterpart. */
+lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
 /* FP64 conservation sums over all particles: total mass, momentum sum m v
  * and max |v| (cout_particle_velocity_stats, LATfield2_Particles.hpp:
  * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */

@@ -212,6 +212,11 @@ class Context:
         self._check(_lib.load().lf2_step(self.h, F.h, float(dtau_kick), float(dtau_drift),
                                          rho.h if rho is not None else None), "step")
 
+    def set_move_kernel(self, which):
+        """Kernel of step()'s kick-drift-rebin pass: 0 automatic, 1 per-brick,
+        2 persistent TMA-pipelined."""
+        self._check(_lib.load().lf2_set_move_kernel(self.h, int(which)), "set_move_kernel")
+
     def conservation(self):
         m = _c.c_double()
         mom = (_c.c_double * 3)()

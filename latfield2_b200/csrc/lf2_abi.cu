@@ -176,8 +176,11 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
   // segments (count + slack, rounded to 4) plus a relocation region of about
   // the same size as the slack
   const int64_t need = n + (n >> 2) + 100 * nb + 1024;
+  // movers: one slot per particle plus the unfilled tail of each SM's last
+  // mover block (pipelined move)
+  const int64_t mov_need = n + (int64_t)c->num_sms * MOV_BLOCK;
   if (need > c->capacity || has_mass != c->has_mass || has_id != c->has_id ||
-      n > c->mov_capacity) {
+      mov_need > c->mov_capacity) {
     LF2_CUDA(c, cudaStreamSynchronize(c->stream));
     free_parts(c->cur);
     free_parts(c->alt);
@@ -187,13 +190,13 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
     c->capacity = c->mov_capacity = 0;
     if (alloc_parts(c->cur, need, has_mass, has_id) != cudaSuccess ||
         alloc_parts(c->alt, need, has_mass, has_id) != cudaSuccess ||
-        alloc_parts(c->mov, n, has_mass, has_id) != cudaSuccess ||
-        cudaMalloc(&c->mov_placed, sizeof(int32_t) * (size_t)(n > 0 ? n : 1)) != cudaSuccess) {
+        alloc_parts(c->mov, mov_need, has_mass, has_id) != cudaSuccess ||
+        cudaMalloc(&c->mov_placed, sizeof(int32_t) * (size_t)mov_need) != cudaSuccess) {
       cudaGetLastError();
       return fail(c, LF2_ERR_NOMEM, "cannot allocate the particle store");
     }
     c->capacity = need;
-    c->mov_capacity = n;
+    c->mov_capacity = mov_need;
   }
   c->has_mass = has_mass;
   c->has_id = has_id;
@@ -305,6 +308,9 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMallocHost(&c->h_stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_i64, sizeof(int64_t) * 4) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->work, sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->mov_real, sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
   if (ok) {
     ok = cudaMemsetAsync(c->count, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->cap, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
@@ -346,6 +352,8 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->brick_sums);
   cudaFree(c->stats);
   cudaFree(c->mov_count);
+  cudaFree(c->work);
+  cudaFree(c->mov_real);
   cudaFree(c->flags);
   cudaFree(c->repack);
   cudaFree(c->diag);
@@ -714,6 +722,7 @@ lf2_status lf2_drift_rebin(lf2_ctx* c, double dtau)
   LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
   {
     PhaseScope ps(c, PH_MOVE);
+    c->last_move_pipe = false;
     LF2_CUDA(c, launch_move(c, nullptr, false, true, mp));
   }
   return rebin_tail(c);
@@ -725,12 +734,26 @@ lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift
   if (F->comps != 3) return fail(c, LF2_ERR_ARG, "the kick field needs 3 components");
   MoveParams mp{(float)dtau_kick, (float)(dtau_drift / c->res)};
   LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  // automatic selection keeps the per-brick kernel until the pipelined one
+  // measures faster on the clustered workloads
+  const bool pipe = c->move_kernel == 2;
+  if (c->move_kernel == 2 && !move_pipe_eligible(c, F->data))
+    return fail(c, LF2_ERR_UNSUPPORTED, "pipelined move needs n0 % 4 == 0, n >= 32, aligned F");
+  if (pipe) LF2_CUDA(c, cudaMemsetAsync(c->mov_real, 0, sizeof(unsigned long long), c->stream));
+  c->last_move_pipe = pipe;
   {
     PhaseScope ps(c, PH_MOVE);
-    LF2_CUDA(c, launch_move(c, F->data, true, true, mp));
+    LF2_CUDA(c, pipe ? launch_move_pipe(c, F->data, mp) : launch_move(c, F->data, true, true, mp));
   }
   LF2_TRY(rebin_tail(c));
   if (rho) LF2_TRY(deposit(c, rho, 0, 1));
+  return LF2_OK;
+}
+
+lf2_status lf2_set_move_kernel(lf2_ctx* c, int which)
+{
+  if (!c || which < 0 || which > 2) return LF2_ERR_ARG;
+  c->move_kernel = which;
   return LF2_OK;
 }
 

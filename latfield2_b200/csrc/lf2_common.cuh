@@ -38,6 +38,7 @@ enum : uint32_t {
   ERR_REPACK = 1u << 3,         // a brick ran out of slots; store was repacked
   ERR_CAPACITY = 1u << 4,       // repack did not fit the allocation (lost state)
   ERR_FIXED_OVERFLOW = 1u << 5, // fixed-point vertex sum reached 2^63
+  ERR_TIMEOUT = 1u << 6,        // a bounded wait inside a kernel gave up
 };
 
 struct Geom {

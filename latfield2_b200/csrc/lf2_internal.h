@@ -42,6 +42,10 @@ struct DepositParams {
   int has_mass;
 };
 
+// Mover slots a CTA of the pipelined move reserves at a time; the mover
+// buffer holds this many slots per SM beyond one per particle.
+constexpr int MOV_BLOCK = 4096;
+
 struct MoveParams {
   float dtk;   // kick: dtau
   float dtn;   // drift: dtau / res (cell units per velocity unit)
@@ -98,6 +102,15 @@ struct lf2_ctx {
   uint32_t* h_flags = nullptr;       // pinned
   int64_t* h_i64 = nullptr;          // pinned [4]
 
+  // pipelined fused move (lf2_move_pipe.cu)
+  int num_sms = 0;
+  int move_kernel = 0;               // 0 auto, 1 per-brick k_move, 2 pipelined
+  int* work = nullptr;               // device brick counter
+  unsigned long long* mov_real = nullptr;  // device: movers of the last pipelined drift
+  bool last_move_pipe = false;       // the last drift used the pipelined kernel
+  const float* tmap_src = nullptr;   // field the cached tensor map describes
+  alignas(64) unsigned char tmap_bytes[128];
+
   // measurement (lf2_profile_*)
   int64_t launches = 0;              // kernels launched, all phases
   bool profiling = false;
@@ -141,6 +154,10 @@ cudaError_t launch_heap_reset(lf2_ctx* c);
 cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp);
 cudaError_t launch_insert(lf2_ctx* c);
 cudaError_t launch_reduce_maxv(lf2_ctx* c);
+
+// lf2_move_pipe.cu
+bool move_pipe_eligible(const lf2_ctx* c, const float* F);
+cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
 
 // lf2_deposit.cu
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)

@@ -313,15 +313,26 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
   }
 }
 
-// Movers into the free slots of their new brick.
+// Movers into the free slots of their new brick.  Slots with a negative
+// offset are unused tails of the pipelined move's mover blocks.
 __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* __restrict__ mov_count,
-                         int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state)
+                         int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state,
+                         uint32_t* flags)
 {
   const int64_t nm = (int64_t)*mov_count;
   for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
        m += (int64_t)gridDim.x * blockDim.x) {
+    if (mov.ox[m] < 0.0f) {  // unused slot of a mover block (offsets are >= 0)
+      placed[m] = 1;
+      continue;
+    }
     int x, y, z;
     unpack_key(v.g, mov.key[m], x, y, z);
+    if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move
+      set_flag(flags, ERR_BAD_CELL);
+      placed[m] = 1;
+      continue;
+    }
     const int64_t b = brick_of(v.g, x, y, z);
     const int slot = atomicAdd(&v.count[b], 1);
     if (slot < v.cap[b]) {
@@ -390,7 +401,7 @@ cudaError_t launch_insert(lf2_ctx* c)
 {
   c->launches += 1;
   k_insert<<<148 * 4, 256, 0, c->stream>>>(view(c), c->mov, c->mov_count, c->mov_placed,
-                                           c->ovf_list, c->ovf_count, c->ovf_state);
+                                           c->ovf_list, c->ovf_count, c->ovf_state, c->flags);
   return cudaGetLastError();
 }
 

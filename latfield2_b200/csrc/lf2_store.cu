@@ -302,14 +302,14 @@ __global__ void k_repack_finish(int64_t nb, const int64_t* __restrict__ start_al
 }
 
 __global__ void k_repack_clear(int32_t* repack, uint32_t* flags, unsigned long long* diag,
-                               const unsigned long long* mov_count)
+                               const unsigned long long* movers)
 {
   if (*repack) {
     set_flag(flags, ERR_REPACK);
     diag[0] += 1;
     *repack = 0;
   }
-  diag[1] = *mov_count;
+  diag[1] = *movers;
 }
 
 // ----------------------------------------------------------- relocation
@@ -492,7 +492,8 @@ cudaError_t launch_repack(lf2_ctx* c)
                                                    c->repack);
   k_repack_finish<<<small, 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt, c->seg_start,
                                                  c->cap, c->repack, c->heap_top);
-  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag, c->mov_count);
+  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag,
+                                         c->last_move_pipe ? c->mov_real : c->mov_count);
   k_ovf_reset<<<1, 256, 0, c->stream>>>(c->ovf_list, c->ovf_count, c->ovf_state);
   return cudaGetLastError();
 }
