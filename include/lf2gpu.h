@@ -172,9 +172,10 @@ lf2_status lf2_drift_rebin(lf2_ctx* ctx, double dtau);
  * when rho is not NULL, by the scalar deposit of the new positions. */
 lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
                     double dtau_drift, lf2_field rho);
-/* Kernel of lf2_step's kick-drift-rebin pass: 0 automatic (currently the
- * per-brick kernel), 1 the per-brick kernel, 2 the persistent TMA-pipelined
- * kernel (needs n0 % 4 == 0, every n >= 32 and F 16-byte aligned, else
+/* Kernel of lf2_step's kick-drift-rebin pass: 0 automatic (the persistent
+ * TMA-pipelined kernel where the lattice allows it, else the per-brick
+ * kernel), 1 the per-brick kernel, 2 the pipelined kernel (needs
+ * n0 % 4 == 0, every n >= 32 and F 16-byte aligned, else
  * LF2_ERR_UNSUPPORTED).  Both give the same particles (the order of the
  * particles inside a brick may differ); no reference counterpart. */
 lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);

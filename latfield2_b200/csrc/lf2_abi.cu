@@ -176,9 +176,7 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
   // segments (count + slack, rounded to 4) plus a relocation region of about
   // the same size as the slack
   const int64_t need = n + (n >> 2) + 100 * nb + 1024;
-  // movers: one slot per particle plus the unfilled tail of each SM's last
-  // mover block (pipelined move)
-  const int64_t mov_need = n + (int64_t)c->num_sms * MOV_BLOCK;
+  const int64_t mov_need = n > 0 ? n : 1;  // every particle may change brick
   if (need > c->capacity || has_mass != c->has_mass || has_id != c->has_id ||
       mov_need > c->mov_capacity) {
     LF2_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -309,7 +307,6 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMallocHost(&c->h_flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMallocHost(&c->h_i64, sizeof(int64_t) * 4) == cudaSuccess;
   ok = ok && cudaMalloc(&c->work, sizeof(int)) == cudaSuccess;
-  ok = ok && cudaMalloc(&c->mov_real, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
   if (ok) {
     ok = cudaMemsetAsync(c->count, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
@@ -353,7 +350,6 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->stats);
   cudaFree(c->mov_count);
   cudaFree(c->work);
-  cudaFree(c->mov_real);
   cudaFree(c->flags);
   cudaFree(c->repack);
   cudaFree(c->diag);
@@ -722,7 +718,6 @@ lf2_status lf2_drift_rebin(lf2_ctx* c, double dtau)
   LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
   {
     PhaseScope ps(c, PH_MOVE);
-    c->last_move_pipe = false;
     LF2_CUDA(c, launch_move(c, nullptr, false, true, mp));
   }
   return rebin_tail(c);
@@ -734,13 +729,9 @@ lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift
   if (F->comps != 3) return fail(c, LF2_ERR_ARG, "the kick field needs 3 components");
   MoveParams mp{(float)dtau_kick, (float)(dtau_drift / c->res)};
   LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
-  // automatic selection keeps the per-brick kernel until the pipelined one
-  // measures faster on the clustered workloads
-  const bool pipe = c->move_kernel == 2;
+  const bool pipe = c->move_kernel == 2 || (c->move_kernel == 0 && move_pipe_eligible(c, F->data));
   if (c->move_kernel == 2 && !move_pipe_eligible(c, F->data))
     return fail(c, LF2_ERR_UNSUPPORTED, "pipelined move needs n0 % 4 == 0, n >= 32, aligned F");
-  if (pipe) LF2_CUDA(c, cudaMemsetAsync(c->mov_real, 0, sizeof(unsigned long long), c->stream));
-  c->last_move_pipe = pipe;
   {
     PhaseScope ps(c, PH_MOVE);
     LF2_CUDA(c, pipe ? launch_move_pipe(c, F->data, mp) : launch_move(c, F->data, true, true, mp));

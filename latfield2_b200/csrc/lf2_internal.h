@@ -42,10 +42,6 @@ struct DepositParams {
   int has_mass;
 };
 
-// Mover slots a CTA of the pipelined move reserves at a time; the mover
-// buffer holds this many slots per SM beyond one per particle.
-constexpr int MOV_BLOCK = 4096;
-
 struct MoveParams {
   float dtk;   // kick: dtau
   float dtn;   // drift: dtau / res (cell units per velocity unit)
@@ -106,8 +102,6 @@ struct lf2_ctx {
   int num_sms = 0;
   int move_kernel = 0;               // 0 auto, 1 per-brick k_move, 2 pipelined
   int* work = nullptr;               // device brick counter
-  unsigned long long* mov_real = nullptr;  // device: movers of the last pipelined drift
-  bool last_move_pipe = false;       // the last drift used the pipelined kernel
   const float* tmap_src = nullptr;   // field the cached tensor map describes
   alignas(64) unsigned char tmap_bytes[128];
 

@@ -313,8 +313,7 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
   }
 }
 
-// Movers into the free slots of their new brick.  Slots with a negative
-// offset are unused tails of the pipelined move's mover blocks.
+// Movers into the free slots of their new brick.
 __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* __restrict__ mov_count,
                          int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state,
                          uint32_t* flags)
@@ -322,10 +321,6 @@ __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* 
   const int64_t nm = (int64_t)*mov_count;
   for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
        m += (int64_t)gridDim.x * blockDim.x) {
-    if (mov.ox[m] < 0.0f) {  // unused slot of a mover block (offsets are >= 0)
-      placed[m] = 1;
-      continue;
-    }
     int x, y, z;
     unpack_key(v.g, mov.key[m], x, y, z);
     if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move

@@ -1,11 +1,12 @@
 // lf2_move_pipe.cu -- fused gather-kick, drift and rebin (lf2_step) as a
 // persistent, warp-specialised kernel.
 //
-// Same arithmetic and the same rebin as k_move<kick, drift> (lf2_move.cu):
-// CIC gather of the 3-component field with the fixed corner order, kick,
-// drift in cell units with the periodic carry, in-place compaction of the
-// particles that stay in their brick (in slot order) and the mover buffer for
-// the others.  What differs is how the data reaches the SM:
+// Same arithmetic as k_move<kick, drift> (lf2_move.cu): CIC gather of the
+// 3-component field with the fixed corner order, kick, drift in cell units
+// with the periodic carry; particles that stay in their brick are written
+// back in place at the front of its segment, the others go to the mover
+// buffer.  What differs is how the data reaches the SM and how the work is
+// shared:
 //
 //   * one CTA per SM; warp 16 is the producer, warps 0-15 the consumers;
 //   * bricks are taken from a global counter (load balance for clustered
@@ -18,9 +19,13 @@
 //     signalled on mbarriers, so the next brick's tile and the next chunks
 //     stream in while the consumers work on the current ones;
 //   * vertices that wrap around the periodic boundary lie outside the tensor
-//     and arrive as zeros; the consumers patch those planes with plain loads.
+//     and arrive as zeros; the producer patches those planes with plain loads
+//     before it releases the tile;
+//   * consumer warps never wait for one another: each takes its own slice of
+//     every chunk and reserves its output slots with atomics.  The order of
+//     the stayers inside a brick therefore follows the warps' timing.
 //
-// Every mbarrier wait is bounded (LF2_FLAG_TIMEOUT and an early return).
+// Every mbarrier wait is bounded (LF2_FLAG_TIMEOUT, then the warp returns).
 // No cluster multicast is used.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -36,8 +41,9 @@ namespace {
 constexpr int PC_WARPS = 16;                     // consumer warps
 constexpr int PC_THREADS = PC_WARPS * 32;        // consumer threads
 constexpr int P_THREADS = PC_THREADS + 32;       // + one producer warp
-constexpr int P_ITEMS = 2;                       // consecutive slots per consumer thread
-constexpr int CHUNK = PC_THREADS * P_ITEMS;      // particles per chunk buffer
+constexpr int W_ITEMS = 2;                       // consecutive slots per lane
+constexpr int WSUB = 32 * W_ITEMS;               // slots per warp per chunk
+constexpr int CHUNK = PC_WARPS * WSUB;           // particles per chunk buffer
 constexpr int FX = 20;                           // padded tile row (floats)
 constexpr int FCOMP = FX * TILE * TILE;          // floats per component of a tile buffer
 constexpr uint32_t FBYTES = 3u * FCOMP * 4u;     // bytes one tile copy delivers
@@ -119,48 +125,10 @@ __device__ __forceinline__ void tma_tile4(void* dst, const CUtensorMap* map, int
       : "memory");
 }
 
-// named barrier of the consumer warps (the producer warp never joins it)
-__device__ __forceinline__ void cbar()
-{
-  asm volatile("bar.sync 1, %0;" ::"n"(PC_THREADS) : "memory");
-}
-
-// Exclusive scan over the consumer threads; `buf` is 32 ints of shared
-// memory that alternates between consecutive calls.
-__device__ __forceinline__ int cscan(int v, int* buf, int* total)
-{
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) buf[warp] = x;
-  cbar();
-  if (warp == 0) {
-    int t = lane < PC_WARPS ? buf[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < PC_WARPS; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, t, o);
-      if (lane >= o) t += y;
-    }
-    if (lane < PC_WARPS) buf[lane] = t;
-  }
-  cbar();
-  *total = buf[PC_WARPS - 1];
-  return (warp ? buf[warp - 1] : 0) + x - v;
-}
-
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
 
-// Chunk buffer layout: key, ox, oy, oz, vx, vy, vz [, mass] [, id], PITCH
-// entries each.  A chunk arrives at entry 0 of every array; the particles
-// that stay are written back to entry a + q (q their rank among the chunk's
-// stayers, a the 16-byte misalignment of their destination slot), so that
-// entry 4k lines up with an aligned 4-slot group of the destination.
-constexpr int PITCH = CHUNK + 32;
-
+// Chunk buffer layout: key, ox, oy, oz, vx, vy, vz [, mass] [, id], CHUNK
+// entries each.
 struct ChunkView {
   uint32_t* key;
   float *ox, *oy, *oz, *vx, *vy, *vz, *m;
@@ -171,65 +139,43 @@ __device__ __forceinline__ ChunkView chunk_view(unsigned char* p, bool has_m)
 {
   ChunkView c;
   c.key = reinterpret_cast<uint32_t*>(p);
-  c.ox = reinterpret_cast<float*>(p + 1 * PITCH * 4);
-  c.oy = reinterpret_cast<float*>(p + 2 * PITCH * 4);
-  c.oz = reinterpret_cast<float*>(p + 3 * PITCH * 4);
-  c.vx = reinterpret_cast<float*>(p + 4 * PITCH * 4);
-  c.vy = reinterpret_cast<float*>(p + 5 * PITCH * 4);
-  c.vz = reinterpret_cast<float*>(p + 6 * PITCH * 4);
-  c.m = reinterpret_cast<float*>(p + 7 * PITCH * 4);
-  c.id = reinterpret_cast<int64_t*>(p + (has_m ? 8 : 7) * PITCH * 4);
+  c.ox = reinterpret_cast<float*>(p + 1 * CHUNK * 4);
+  c.oy = reinterpret_cast<float*>(p + 2 * CHUNK * 4);
+  c.oz = reinterpret_cast<float*>(p + 3 * CHUNK * 4);
+  c.vx = reinterpret_cast<float*>(p + 4 * CHUNK * 4);
+  c.vy = reinterpret_cast<float*>(p + 5 * CHUNK * 4);
+  c.vz = reinterpret_cast<float*>(p + 6 * CHUNK * 4);
+  c.m = reinterpret_cast<float*>(p + 7 * CHUNK * 4);
+  c.id = reinterpret_cast<int64_t*>(p + (has_m ? 8 : 7) * CHUNK * 4);
   return c;
 }
 
-// Copy entries [a, a + total) of a staged 32-bit array to dst[d0 + a ...):
-// whole aligned 4-entry groups as 16-byte vectors, the partial first and
-// last groups entry by entry.  d0 is a multiple of 4 slots.
-__device__ __forceinline__ void copy_out32(const uint32_t* __restrict__ src, uint32_t* dst,
-                                           int64_t d0, int a, int total, int ct)
+// Bounded wait by lane 0 of the calling warp; the outcome is broadcast so the
+// warp stays together, and every lane then acquires the completed phase.
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, uint32_t* flags, int lane)
 {
-  const int end = a + total, ng = (end + 3) >> 2;
-  for (int k = ct; k < ng; k += PC_THREADS) {
-    const int e0 = 4 * k;
-    if (e0 >= a && e0 + 4 <= end) {
-      *reinterpret_cast<uint4*>(dst + d0 + e0) = *reinterpret_cast<const uint4*>(src + e0);
-    } else {
-      for (int e = max(e0, a); e < min(e0 + 4, end); e++) dst[d0 + e] = src[e];
-    }
-  }
-}
-
-__device__ __forceinline__ void copy_out64(const int64_t* __restrict__ src, int64_t* dst,
-                                           int64_t d0, int a, int total, int ct)
-{
-  const int end = a + total, ng = (end + 1) >> 1;
-  for (int k = ct; k < ng; k += PC_THREADS) {
-    const int e0 = 2 * k;
-    if (e0 >= a && e0 + 2 <= end) {
-      *reinterpret_cast<longlong2*>(dst + d0 + e0) = *reinterpret_cast<const longlong2*>(src + e0);
-    } else {
-      for (int e = max(e0, a); e < min(e0 + 2, end); e++) dst[d0 + e] = src[e];
-    }
-  }
+  int ok = 1;
+  if (lane == 0) ok = mbar_wait(bar, parity, flags);
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (ok) mbar_try(bar, parity);
+  return ok != 0;
 }
 
 __global__ void __launch_bounds__(P_THREADS, 1)
     k_move_pipe(const __grid_constant__ CUtensorMap tmF, StoreView v, const float* __restrict__ F,
                 MoveParams mp, PartArrays mov, unsigned long long* mov_count,
-                unsigned long long* mov_real, float* __restrict__ brick_maxv2, uint32_t* flags,
-                int* work, int nst, int stage_bytes)
+                float* __restrict__ brick_maxv2, uint32_t* flags, int* work, int nst,
+                int stage_bytes)
 {
   extern __shared__ unsigned char dyn[];
-  __shared__ uint64_t full_f[2], empty_f[2], full_p[MAX_STAGES], empty_p[MAX_STAGES];
+  // full_f: tile ready for the consumers; tma_f: tile copy landed (edge
+  // bricks, before the producer patches the wrapped planes); empty_f: all
+  // consumer warps are done with the brick; full_p / empty_p: chunk ring.
+  __shared__ uint64_t full_f[2], tma_f[2], empty_f[2], full_p[MAX_STAGES], empty_p[MAX_STAGES];
   __shared__ Job job[2];
-  __shared__ int s_scan[2][32];
-  __shared__ float s_max[PC_WARPS];
-  __shared__ int s_ok_f, s_ok_p;  // outcome of thread 0's last tile / chunk wait
-  // mover block of this CTA: slots [mv_base, mv_base + MOV_BLOCK) of the mover
-  // buffer, mv_used of them filled; mv_next a fresh block when a chunk's
-  // movers do not fit (double-buffered by chunk parity)
-  __shared__ long long s_mv_base[2], s_mv_next[2];
-  __shared__ int s_mv_used[2];
+  __shared__ int s_cursor[2];     // stayers written back so far (per tile buffer)
+  __shared__ int s_done[2];       // consumer warps finished with the brick
+  __shared__ unsigned s_maxv2[2]; // max |v|^2 of the brick (bits of a non-negative float)
 
   unsigned char* sm = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -237,189 +183,206 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
   const Geom& g = v.g;
   const bool has_m = v.a.mass != nullptr, has_id = v.a.id != nullptr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < 2; s++) mbar_init(&full_f[s], 1), mbar_init(&empty_f[s], 1);
-    for (int s = 0; s < nst; s++) mbar_init(&full_p[s], 1), mbar_init(&empty_p[s], 1);
+    for (int s = 0; s < 2; s++) {
+      mbar_init(&full_f[s], 1);
+      mbar_init(&tma_f[s], 1);
+      mbar_init(&empty_f[s], 1);
+    }
+    for (int s = 0; s < nst; s++) mbar_init(&full_p[s], 1), mbar_init(&empty_p[s], PC_WARPS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (threadIdx.x >= PC_THREADS) {
+  if (warp == PC_WARPS) {
     // ------------------------------------------------------------ producer
-    if (threadIdx.x != PC_THREADS) return;
     long long fk = 0, pk = 0;  // tile buffers and chunk buffers handed out so far
+    unsigned te = 0;           // bit s: parity of the next tma_f[s] phase
     for (;;) {
-      const long long b = atomicAdd(work, 1);
+      int state = 0;           // 0 brick posted, 1 empty brick, 2 finished, 3 timed out
+      int edge = 0, cnt = 0;
+      long long b = 0, base = 0;
       const int fs = (int)(fk & 1);
-      if (b >= g.nbricks) {
-        if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
-        job[fs].b = -1;
-        mbar_arrive(&full_f[fs]);
-        return;
+      if (lane == 0) {
+        b = atomicAdd(work, 1);
+        if (b >= g.nbricks) {
+          if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) {
+            state = 3;
+          } else {
+            job[fs].b = -1;
+            mbar_arrive(&full_f[fs]);
+            state = 2;
+          }
+        } else if ((cnt = LF2_BRICK_COUNT(v, b)) == 0) {
+          brick_maxv2[b] = 0.0f;
+          state = 1;
+        } else if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) {
+          state = 3;
+        } else {
+          base = v.seg_start[b];
+          job[fs].b = b;
+          job[fs].base = base;
+          job[fs].cnt = cnt;
+          s_cursor[fs] = 0;
+          s_done[fs] = 0;
+          s_maxv2[fs] = 0u;
+          int bx, by, bz;
+          brick_coords(g, b, bx, by, bz);
+          edge = bx * BRICK + brick_extent(g.n[0], bx) == g.n[0] ||
+                 by * BRICK + brick_extent(g.n[1], by) == g.n[1] ||
+                 bz * BRICK + brick_extent(g.n[2], bz) == g.n[2];
+          uint64_t* bar = edge ? &tma_f[fs] : &full_f[fs];
+          mbar_arrive_tx(bar, FBYTES);
+          tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, bar);
+        }
       }
-      const int cnt = LF2_BRICK_COUNT(v, b);
-      if (cnt == 0) {
-        brick_maxv2[b] = 0.0f;
-        continue;
+      state = __shfl_sync(0xffffffffu, state, 0);
+      if (state >= 2) return;
+      if (state == 1) continue;
+      edge = __shfl_sync(0xffffffffu, edge, 0);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      if (edge) {
+        // Vertex planes on the upper periodic boundary lie outside the
+        // tensor and arrive as zeros: plane i = ex holds x = 0 (likewise y, z).
+        if (!warp_wait(&tma_f[fs], (te >> fs) & 1u, flags, lane)) return;
+        te ^= 1u << fs;
+        float* ft = reinterpret_cast<float*>(sm + fs * FSTRIDE);
+        int bx, by, bz;
+        brick_coords(g, b, bx, by, bz);
+        const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+        const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+                  ez = brick_extent(g.n[2], bz);
+        const bool wx = x0 + ex == g.n[0], wy = y0 + ey == g.n[1], wz = z0 + ez == g.n[2];
+        const int np_ = TILE * TILE;
+        for (int t = lane; t < 3 * np_; t += 32) {
+          const int pl = t / np_, r = t % np_, u = r % TILE, w = r / TILE;
+          int i, j, k;
+          if (pl == 0) {
+            if (!wx) continue;
+            i = ex, j = u, k = w;
+          } else if (pl == 1) {
+            if (!wy) continue;
+            i = u, j = ey, k = w;
+          } else {
+            if (!wz) continue;
+            i = u, j = w, k = ez;
+          }
+          if (i > ex || j > ey || k > ez) continue;
+          const int gx = x0 + i < g.n[0] ? x0 + i : 0;
+          const int gy = y0 + j < g.n[1] ? y0 + j : 0;
+          const int gz = z0 + k < g.n[2] ? z0 + k : 0;
+          const int64_t s = site_index(g, gx, gy, gz);
+          const int o = i + FX * (j + TILE * k);
+          ft[o] = __ldg(F + s);
+          ft[FCOMP + o] = __ldg(F + g.nsites + s);
+          ft[2 * FCOMP + o] = __ldg(F + 2 * g.nsites + s);
+        }
+        // the buffer is later overwritten by a tile copy (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&full_f[fs]);
       }
-      if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
-      const long long base = v.seg_start[b];
-      job[fs].b = b;
-      job[fs].base = base;
-      job[fs].cnt = cnt;
-      int bx, by, bz;
-      brick_coords(g, b, bx, by, bz);
-      mbar_arrive_tx(&full_f[fs], FBYTES);
-      tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &full_f[fs]);
       fk++;
-      for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
-        const int ps = (int)(pk % nst);
-        const long long use = pk / nst;
-        if (use > 0 && !mbar_wait(&empty_p[ps], (uint32_t)((use - 1) & 1), flags)) return;
-        const int n = min(CHUNK, cnt - c0);
-        const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
-        const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
-        const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
-        const long long p = base + c0;
-        mbar_arrive_tx(&full_p[ps], bytes);
-        bulk_g2s(cv.key, v.a.key + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.ox, v.a.ox + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.oy, v.a.oy + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.oz, v.a.oz + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.vx, v.a.vx + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.vy, v.a.vy + p, n4 * 4u, &full_p[ps]);
-        bulk_g2s(cv.vz, v.a.vz + p, n4 * 4u, &full_p[ps]);
-        if (has_m) bulk_g2s(cv.m, v.a.mass + p, n4 * 4u, &full_p[ps]);
-        if (has_id) bulk_g2s(cv.id, v.a.id + p, n4 * 8u, &full_p[ps]);
-        pk++;
+      int ok = 1;
+      if (lane == 0) {
+        for (int c0 = 0; c0 < cnt && ok; c0 += CHUNK) {
+          const int ps = (int)(pk % nst);
+          const long long use = pk / nst;
+          if (use > 0 && !mbar_wait(&empty_p[ps], (uint32_t)((use - 1) & 1), flags)) {
+            ok = 0;
+            break;
+          }
+          const int n = min(CHUNK, cnt - c0);
+          const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
+          const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
+          const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
+          const long long p = base + c0;
+          mbar_arrive_tx(&full_p[ps], bytes);
+          bulk_g2s(cv.key, v.a.key + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.ox, v.a.ox + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.oy, v.a.oy + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.oz, v.a.oz + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.vx, v.a.vx + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.vy, v.a.vy + p, n4 * 4u, &full_p[ps]);
+          bulk_g2s(cv.vz, v.a.vz + p, n4 * 4u, &full_p[ps]);
+          if (has_m) bulk_g2s(cv.m, v.a.mass + p, n4 * 4u, &full_p[ps]);
+          if (has_id) bulk_g2s(cv.id, v.a.id + p, n4 * 8u, &full_p[ps]);
+          pk++;
+        }
       }
+      if (!__shfl_sync(0xffffffffu, ok, 0)) return;
     }
   }
 
   // -------------------------------------------------------------- consumers
-  // Thread 0 does the bounded mbarrier waits and hands the outcome to the
-  // other consumers through the named barrier, so that on a timeout all of
-  // them leave together and none is left waiting at a barrier.
-  const int ct = threadIdx.x, lane = ct & 31;
+  // Each warp takes slots [warp * WSUB, (warp + 1) * WSUB) of every chunk of
+  // the brick and works on its own: stayers are written back in place at
+  // slots taken from the brick's shared cursor, movers at slots taken from
+  // the global mover counter.  The last warp to finish a brick publishes its
+  // count and max |v|^2 and hands the tile buffer back.  In-place writes
+  // never reach a slot whose chunk has not been copied in: the cursor never
+  // exceeds the number of particles of the chunks already in the ring.
   long long fk = 0, pk = 0;
-  int sc = 0;             // parity of the per-chunk shared scratch
-  int pending = -1;       // chunk buffer to hand back at the next barrier
-  // mover block state, kept by thread 0
-  long long mv_base = -1, mv_real = 0;
-  int mv_used = MOV_BLOCK;
   for (;;) {
     const int fs = (int)(fk & 1);
-    const uint32_t fpar = (uint32_t)((fk >> 1) & 1);
-    if (ct == 0) s_ok_f = mbar_wait(&full_f[fs], fpar, flags);
-    cbar();
-    if (ct == 0 && pending >= 0) mbar_arrive(&empty_p[pending]);
-    pending = -1;
-    if (!s_ok_f) return;
-    mbar_try(&full_f[fs], fpar);  // completed: acquire for this thread
+    if (!warp_wait(&full_f[fs], (uint32_t)((fk >> 1) & 1), flags, lane)) return;
     const Job jb = job[fs];
-    if (jb.b < 0) {
-      // Unused slots of the last mover block get an invalid offset (-1),
-      // which k_insert skips.
-      if (ct == 0) {
-        s_mv_base[0] = mv_base;
-        s_mv_used[0] = mv_used;
-        if (mv_real) atomicAdd(mov_real, (unsigned long long)mv_real);
-      }
-      cbar();
-      if (s_mv_base[0] >= 0)
-        for (int i = s_mv_used[0] + ct; i < MOV_BLOCK; i += PC_THREADS) mov.ox[s_mv_base[0] + i] = -1.0f;
-      return;
-    }
+    if (jb.b < 0) return;
     const int64_t b = jb.b;
     const int cnt = jb.cnt;
-    float* ft = reinterpret_cast<float*>(sm + fs * FSTRIDE);
+    const float* ft = reinterpret_cast<const float*>(sm + fs * FSTRIDE);
     int bx, by, bz;
     brick_coords(g, b, bx, by, bz);
     const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-    const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
-              ez = brick_extent(g.n[2], bz);
-    const bool wx = x0 + ex == g.n[0], wy = y0 + ey == g.n[1], wz = z0 + ez == g.n[2];
-    if (wx || wy || wz) {
-      // Vertex planes on the upper periodic boundary lie outside the tensor:
-      // plane i = ex maps to x = 0 (likewise y, z).
-      const int np_ = TILE * TILE;
-      for (int t = ct; t < 3 * np_; t += PC_THREADS) {
-        const int pl = t / np_, r = t % np_, u = r % TILE, w = r / TILE;
-        int i, j, k;
-        if (pl == 0) {
-          if (!wx) continue;
-          i = ex, j = u, k = w;
-        } else if (pl == 1) {
-          if (!wy) continue;
-          i = u, j = ey, k = w;
-        } else {
-          if (!wz) continue;
-          i = u, j = w, k = ez;
-        }
-        if (i > ex || j > ey || k > ez) continue;
-        const int gx = x0 + i < g.n[0] ? x0 + i : 0;
-        const int gy = y0 + j < g.n[1] ? y0 + j : 0;
-        const int gz = z0 + k < g.n[2] ? z0 + k : 0;
-        const int64_t s = site_index(g, gx, gy, gz);
-        const int o = i + FX * (j + TILE * k);
-        ft[o] = __ldg(F + s);
-        ft[FCOMP + o] = __ldg(F + g.nsites + s);
-        ft[2 * FCOMP + o] = __ldg(F + 2 * g.nsites + s);
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      cbar();
-    }
+    const uint32_t key0 = pack_key(g, x0, y0, z0);  // a harmless key for empty lanes
 
-    int write = 0;
     float maxv2 = 0.0f;
     for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
       const int ps = (int)(pk % nst);
-      const uint32_t ppar = (uint32_t)((pk / nst) & 1);
-      if (ct == 0) {
-        s_ok_p = mbar_wait(&full_p[ps], ppar, flags);
-        s_mv_base[sc] = mv_base;
-        s_mv_used[sc] = mv_used;
-      }
-      cbar();
-      if (ct == 0 && pending >= 0) mbar_arrive(&empty_p[pending]);
-      pending = -1;
-      if (!s_ok_p) return;
-      mbar_try(&full_p[ps], ppar);
+      if (!warp_wait(&full_p[ps], (uint32_t)((pk / nst) & 1), flags, lane)) return;
+      pk++;
       const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
       const int n = min(CHUNK, cnt - c0);
-      const int i0 = P_ITEMS * ct;
-      uint32_t key[P_ITEMS];
-      float ox[P_ITEMS], oy[P_ITEMS], oz[P_ITEMS], vx[P_ITEMS], vy[P_ITEMS], vz[P_ITEMS];
-      float m[P_ITEMS];
-      int64_t id[P_ITEMS];
-      bool act[P_ITEMS], stay[P_ITEMS];
-      if (i0 < n) {
-        const uint2 k2 = *reinterpret_cast<const uint2*>(cv.key + i0);
-        const float2 a = *reinterpret_cast<const float2*>(cv.ox + i0);
-        const float2 bb = *reinterpret_cast<const float2*>(cv.oy + i0);
-        const float2 cc = *reinterpret_cast<const float2*>(cv.oz + i0);
-        const float2 d = *reinterpret_cast<const float2*>(cv.vx + i0);
-        const float2 e = *reinterpret_cast<const float2*>(cv.vy + i0);
-        const float2 f = *reinterpret_cast<const float2*>(cv.vz + i0);
-        key[0] = k2.x, key[1] = k2.y;
-        ox[0] = a.x, ox[1] = a.y, oy[0] = bb.x, oy[1] = bb.y, oz[0] = cc.x, oz[1] = cc.y;
-        vx[0] = d.x, vx[1] = d.y, vy[0] = e.x, vy[1] = e.y, vz[0] = f.x, vz[1] = f.y;
-      }
+      const int i0 = warp * WSUB + W_ITEMS * lane;
+      uint32_t key[W_ITEMS] = {key0, key0};
+      float ox[W_ITEMS] = {0.f, 0.f}, oy[W_ITEMS] = {0.f, 0.f}, oz[W_ITEMS] = {0.f, 0.f};
+      float vx[W_ITEMS] = {0.f, 0.f}, vy[W_ITEMS] = {0.f, 0.f}, vz[W_ITEMS] = {0.f, 0.f};
+      float m[W_ITEMS] = {0.f, 0.f};
+      int64_t id[W_ITEMS] = {0, 0};
+      bool act[W_ITEMS];
 #pragma unroll
-      for (int j = 0; j < P_ITEMS; j++) {
-        act[j] = i0 + j < n;
-        stay[j] = true;
-        m[j] = 0.0f;
-        id[j] = 0;
-        if (act[j]) {
-          if (has_m) m[j] = cv.m[i0 + j];
-          if (has_id) id[j] = cv.id[i0 + j];
+      for (int j = 0; j < W_ITEMS; j++) act[j] = i0 + j < n;
+      if (act[0]) {
+        if (act[1]) {
+          const uint2 k2 = *reinterpret_cast<const uint2*>(cv.key + i0);
+          const float2 a = *reinterpret_cast<const float2*>(cv.ox + i0);
+          const float2 bb = *reinterpret_cast<const float2*>(cv.oy + i0);
+          const float2 cc = *reinterpret_cast<const float2*>(cv.oz + i0);
+          const float2 d = *reinterpret_cast<const float2*>(cv.vx + i0);
+          const float2 e = *reinterpret_cast<const float2*>(cv.vy + i0);
+          const float2 f = *reinterpret_cast<const float2*>(cv.vz + i0);
+          key[0] = k2.x, key[1] = k2.y;
+          ox[0] = a.x, ox[1] = a.y, oy[0] = bb.x, oy[1] = bb.y, oz[0] = cc.x, oz[1] = cc.y;
+          vx[0] = d.x, vx[1] = d.y, vy[0] = e.x, vy[1] = e.y, vz[0] = f.x, vz[1] = f.y;
+        } else {
+          key[0] = cv.key[i0];
+          ox[0] = cv.ox[i0], oy[0] = cv.oy[i0], oz[0] = cv.oz[i0];
+          vx[0] = cv.vx[i0], vy[0] = cv.vy[i0], vz[0] = cv.vz[i0];
+        }
+#pragma unroll
+        for (int j = 0; j < W_ITEMS; j++) {
+          if (act[j] && has_m) m[j] = cv.m[i0 + j];
+          if (act[j] && has_id) id[j] = cv.id[i0 + j];
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty_p[ps]);  // this warp's slots are read
+
+      bool stay[W_ITEMS];
 #pragma unroll
-      for (int j = 0; j < P_ITEMS; j++) {
-        if (!act[j]) continue;
+      for (int j = 0; j < W_ITEMS; j++) {
         int x, y, z;
         unpack_key(g, key[j], x, y, z);
         const int t0 = (x - x0) + FX * ((y - y0) + TILE * (z - z0));
@@ -439,8 +402,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         vx[j] = __fmaf_rn(mp.dtk, a0, vx[j]);
         vy[j] = __fmaf_rn(mp.dtk, a1, vy[j]);
         vz[j] = __fmaf_rn(mp.dtk, a2, vz[j]);
-        maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx[j], vx[j]), __fmul_rn(vy[j], vy[j])),
-                                       __fmul_rn(vz[j], vz[j])));
+        if (act[j])
+          maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx[j], vx[j]), __fmul_rn(vy[j], vy[j])),
+                                         __fmul_rn(vz[j], vz[j])));
         float o[3] = {ox[j], oy[j], oz[j]};
         const float vv[3] = {vx[j], vy[j], vz[j]};
         int xyz[3] = {x, y, z};
@@ -448,10 +412,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           float od = __fmaf_rn(mp.dtn, vv[d], o[d]);
-          if (!isfinite(od)) {
-            finite = false;
-            break;
-          }
+          finite = finite && isfinite(od);
           const float fl = floorf(od);
           od = __fsub_rn(od, fl);
           int carry = (int)fl;
@@ -460,114 +421,79 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             carry += 1;
           }
           o[d] = od;
-          xyz[d] = wrap_add(xyz[d], carry, g.n[d]);
+          xyz[d] = finite ? wrap_add(xyz[d], carry, g.n[d]) : xyz[d];
         }
+        stay[j] = true;
         if (finite) {
           ox[j] = o[0];
           oy[j] = o[1];
           oz[j] = o[2];
           key[j] = pack_key(g, xyz[0], xyz[1], xyz[2]);
           stay[j] = brick_of(g, xyz[0], xyz[1], xyz[2]) == b;
-        } else {
+        } else if (act[j]) {
           set_flag(flags, ERR_NONFINITE);
         }
       }
 
-      // One scan ranks both groups: stayers in the low 16 bits, movers in the
-      // high 16 bits (at most CHUNK of each).
-      int ns = 0, nm = 0;
-#pragma unroll
-      for (int j = 0; j < P_ITEMS; j++) {
-        ns += (act[j] && stay[j]) ? 1 : 0;
-        nm += (act[j] && !stay[j]) ? 1 : 0;
+      // stayers: lane-major order inside the warp, slots from the brick cursor
+      const unsigned lt = (1u << lane) - 1u;
+      const unsigned s0 = __ballot_sync(0xffffffffu, act[0] && stay[0]);
+      const unsigned s1 = __ballot_sync(0xffffffffu, act[1] && stay[1]);
+      const int ns = __popc(s0) + __popc(s1);
+      const unsigned m0 = __ballot_sync(0xffffffffu, act[0] && !stay[0]);
+      const unsigned m1 = __ballot_sync(0xffffffffu, act[1] && !stay[1]);
+      const int nmv = __popc(m0) + __popc(m1);
+      int sbase = 0;
+      unsigned long long mbase = 0;
+      if (lane == 0) {
+        if (ns) sbase = atomicAdd(&s_cursor[fs], ns);
+        if (nmv) mbase = atomicAdd(mov_count, (unsigned long long)nmv);
       }
-      int tot;
-      const int pre = cscan(ns | (nm << 16), s_scan[sc], &tot);
-      const int total = tot & 0xffff, mtot = tot >> 16;
-      int q = pre & 0xffff, mq = pre >> 16;
-
-      // Movers: the chunk's movers take the next mtot slots of the CTA's
-      // mover block, spilling into a fresh block when the block is full.
-      const long long mb = s_mv_base[sc];
-      const int mu = s_mv_used[sc];
-      if (mtot > MOV_BLOCK - mu) {  // uniform: every consumer sees the same values
-        if (ct == 0) s_mv_next[sc] = (long long)atomicAdd(mov_count, (unsigned long long)MOV_BLOCK);
-        cbar();
-      }
-      const long long mn = mtot > MOV_BLOCK - mu ? s_mv_next[sc] : -1;
-
-      // Stayers are staged in the chunk buffer (all of it has been read:
-      // the scan's barriers are behind every consumer), movers go out now.
-      const int64_t dst = jb.base + write;
-      const int a = (int)(dst & 3);
+      sbase = __shfl_sync(0xffffffffu, sbase, 0);
+      mbase = __shfl_sync(0xffffffffu, mbase, 0);
+      int sq = sbase + __popc(s0 & lt) + __popc(s1 & lt);
+      long long mq = (long long)mbase + __popc(m0 & lt) + __popc(m1 & lt);
 #pragma unroll
-      for (int j = 0; j < P_ITEMS; j++) {
+      for (int j = 0; j < W_ITEMS; j++) {
         if (!act[j]) continue;
         if (stay[j]) {
-          const int e = a + q++;
-          cv.key[e] = key[j];
-          cv.ox[e] = ox[j];
-          cv.oy[e] = oy[j];
-          cv.oz[e] = oz[j];
-          cv.vx[e] = vx[j];
-          cv.vy[e] = vy[j];
-          cv.vz[e] = vz[j];
-          if (has_m) cv.m[e] = m[j];
-          if (has_id) cv.id[e] = id[j];
+          const int64_t q = jb.base + sq++;
+          v.a.key[q] = key[j];
+          v.a.ox[q] = ox[j];
+          v.a.oy[q] = oy[j];
+          v.a.oz[q] = oz[j];
+          v.a.vx[q] = vx[j];
+          v.a.vy[q] = vy[j];
+          v.a.vz[q] = vz[j];
+          if (has_m) v.a.mass[q] = m[j];
+          if (has_id) v.a.id[q] = id[j];
         } else {
-          const int idx = mu + mq++;
-          const int64_t s = idx < MOV_BLOCK ? mb + idx : mn + (idx - MOV_BLOCK);
-          mov.key[s] = key[j];
-          mov.ox[s] = ox[j];
-          mov.oy[s] = oy[j];
-          mov.oz[s] = oz[j];
-          mov.vx[s] = vx[j];
-          mov.vy[s] = vy[j];
-          mov.vz[s] = vz[j];
-          if (mov.mass) mov.mass[s] = m[j];
-          if (mov.id) mov.id[s] = id[j];
+          const int64_t q = mq++;
+          mov.key[q] = key[j];
+          mov.ox[q] = ox[j];
+          mov.oy[q] = oy[j];
+          mov.oz[q] = oz[j];
+          mov.vx[q] = vx[j];
+          mov.vy[q] = vy[j];
+          mov.vz[q] = vz[j];
+          if (mov.mass) mov.mass[q] = m[j];
+          if (mov.id) mov.id[q] = id[j];
         }
       }
-      if (ct == 0) {
-        mv_used = mu + mtot;
-        if (mn >= 0) {
-          mv_base = mn;
-          mv_used -= MOV_BLOCK;
-        }
-        mv_real += mtot;
-      }
-      cbar();
-      const int64_t d0 = dst - a;
-      copy_out32(cv.key, v.a.key, d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.ox), reinterpret_cast<uint32_t*>(v.a.ox), d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.oy), reinterpret_cast<uint32_t*>(v.a.oy), d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.oz), reinterpret_cast<uint32_t*>(v.a.oz), d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.vx), reinterpret_cast<uint32_t*>(v.a.vx), d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.vy), reinterpret_cast<uint32_t*>(v.a.vy), d0, a, total, ct);
-      copy_out32(reinterpret_cast<const uint32_t*>(cv.vz), reinterpret_cast<uint32_t*>(v.a.vz), d0, a, total, ct);
-      if (has_m)
-        copy_out32(reinterpret_cast<const uint32_t*>(cv.m), reinterpret_cast<uint32_t*>(v.a.mass), d0, a, total, ct);
-      if (has_id) copy_out64(cv.id, v.a.id, d0, a, total, ct);
-      // the buffer is handed back after the next barrier, when every
-      // consumer has copied its part out
-      pending = ps;
-      pk++;
-      sc ^= 1;
-      write += total;
     }
 
     for (int o = 16; o > 0; o >>= 1) maxv2 = fmaxf(maxv2, __shfl_xor_sync(0xffffffffu, maxv2, o));
-    if (lane == 0) s_max[ct >> 5] = maxv2;
-    cbar();
-    if (ct == 0) {
-      if (pending >= 0) mbar_arrive(&empty_p[pending]);
-      float mm = 0.0f;
-      for (int w = 0; w < PC_WARPS; w++) mm = fmaxf(mm, s_max[w]);
-      brick_maxv2[b] = mm;
-      v.count[b] = write;
-      mbar_arrive(&empty_f[fs]);  // all gathers of this brick are done
+    if (lane == 0) {
+      atomicMax(&s_maxv2[fs], __float_as_uint(maxv2));  // non-negative floats order as integers
+      __threadfence_block();
+      if (atomicAdd(&s_done[fs], 1) == PC_WARPS - 1) {
+        __threadfence_block();
+        brick_maxv2[b] = __uint_as_float(atomicAdd(&s_maxv2[fs], 0u));
+        v.count[b] = atomicAdd(&s_cursor[fs], 0);
+        mbar_arrive(&empty_f[fs]);  // every warp is done with this brick
+      }
     }
-    pending = -1;
+    __syncwarp();
     fk++;
   }
 }
@@ -594,7 +520,7 @@ EncodeTiledFn encode_fn()
 
 size_t stage_bytes_for(const lf2_ctx* c)
 {
-  return (size_t)PITCH * (28 + (c->has_mass ? 4 : 0) + (c->has_id ? 8 : 0));
+  return (size_t)CHUNK * (28 + (c->has_mass ? 4 : 0) + (c->has_id ? 8 : 0));
 }
 
 }  // namespace
@@ -647,8 +573,8 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp)
   if (e != cudaSuccess) return e;
   c->launches += 1;
   k_move_pipe<<<c->num_sms, P_THREADS, smem, c->stream>>>(*map, view(c), F, mp, c->mov, c->mov_count,
-                                                          c->mov_real, c->brick_maxv2, c->flags,
-                                                          c->work, nst, (int)sb);
+                                                          c->brick_maxv2, c->flags, c->work, nst,
+                                                          (int)sb);
   return cudaGetLastError();
 }
 

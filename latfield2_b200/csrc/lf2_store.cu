@@ -492,8 +492,7 @@ cudaError_t launch_repack(lf2_ctx* c)
                                                    c->repack);
   k_repack_finish<<<small, 256, 0, c->stream>>>(nb, c->seg_start_alt, c->cap_alt, c->seg_start,
                                                  c->cap, c->repack, c->heap_top);
-  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag,
-                                         c->last_move_pipe ? c->mov_real : c->mov_count);
+  k_repack_clear<<<1, 1, 0, c->stream>>>(c->repack, c->flags, c->diag, c->mov_count);
   k_ovf_reset<<<1, 256, 0, c->stream>>>(c->ovf_list, c->ovf_count, c->ovf_state);
   return cudaGetLastError();
 }
