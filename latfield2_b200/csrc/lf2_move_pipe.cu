@@ -8,7 +8,7 @@
 // buffer.  What differs is how the data reaches the SM and how the work is
 // shared:
 //
-//   * one CTA per SM; warp 16 is the producer, warps 0-15 the consumers;
+//   * one CTA per SM; the last warp is the producer, the others consumers;
 //   * bricks are taken from a global counter (load balance for clustered
 //     particle distributions); empty bricks cost one atomic;
 //   * the producer loads each brick's (BRICK+1)^3 vertex tile of F with one
@@ -38,17 +38,29 @@ namespace lf2 {
 
 namespace {
 
-constexpr int PC_WARPS = 16;                     // consumer warps
+// Launch shape (measured at 512^3 with 134M particles: 31 x 1 2.79 ms,
+// 24 x 1 2.81, 16 x 2 2.84, 8 x 4 3.78; two chunk buffers instead of three
+// cost 9%)
+#ifndef LF2_PIPE_WARPS
+#define LF2_PIPE_WARPS 31
+#endif
+#ifndef LF2_PIPE_ITEMS
+#define LF2_PIPE_ITEMS 1
+#endif
+constexpr int PC_WARPS = LF2_PIPE_WARPS;         // consumer warps
 constexpr int PC_THREADS = PC_WARPS * 32;        // consumer threads
 constexpr int P_THREADS = PC_THREADS + 32;       // + one producer warp
-constexpr int W_ITEMS = 2;                       // consecutive slots per lane
+constexpr int W_ITEMS = LF2_PIPE_ITEMS;          // consecutive slots per lane
 constexpr int WSUB = 32 * W_ITEMS;               // slots per warp per chunk
 constexpr int CHUNK = PC_WARPS * WSUB;           // particles per chunk buffer
 constexpr int FX = 20;                           // padded tile row (floats)
 constexpr int FCOMP = FX * TILE * TILE;          // floats per component of a tile buffer
 constexpr uint32_t FBYTES = 3u * FCOMP * 4u;     // bytes one tile copy delivers
 constexpr int FSTRIDE = (FBYTES + 1023) & ~1023; // tile buffer stride in shared memory
-constexpr int MAX_STAGES = 4;
+#ifndef LF2_PIPE_MAX_STAGES
+#define LF2_PIPE_MAX_STAGES 4
+#endif
+constexpr int MAX_STAGES = LF2_PIPE_MAX_STAGES;  // chunk buffers (as many as fit, up to this)
 constexpr long long WAIT_CYCLES = 4000000000LL;  // about 2 s at the boost clock
 
 struct Job {
@@ -126,6 +138,19 @@ __device__ __forceinline__ void tma_tile4(void* dst, const CUtensorMap* map, int
 }
 
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
+
+// x + carry wrapped into [0, n): two selects cover |carry| <= n, the general
+// case (a particle that crosses the whole lattice in one step) is out of line.
+__device__ __noinline__ int wrap_far(int x, int carry, int n) { return wrap_add(x, carry, n); }
+
+__device__ __forceinline__ int wrap_near(int x, int carry, int n)
+{
+  int v = x + carry;
+  v += v < 0 ? n : 0;
+  v -= v >= n ? n : 0;
+  if ((unsigned)v >= (unsigned)n) v = wrap_far(x, carry, n);
+  return v;
+}
 
 // Chunk buffer layout: key, ox, oy, oz, vx, vy, vz [, mass] [, id], CHUNK
 // entries each.
@@ -346,35 +371,23 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
       const int n = min(CHUNK, cnt - c0);
       const int i0 = warp * WSUB + W_ITEMS * lane;
-      uint32_t key[W_ITEMS] = {key0, key0};
-      float ox[W_ITEMS] = {0.f, 0.f}, oy[W_ITEMS] = {0.f, 0.f}, oz[W_ITEMS] = {0.f, 0.f};
-      float vx[W_ITEMS] = {0.f, 0.f}, vy[W_ITEMS] = {0.f, 0.f}, vz[W_ITEMS] = {0.f, 0.f};
-      float m[W_ITEMS] = {0.f, 0.f};
-      int64_t id[W_ITEMS] = {0, 0};
+      uint32_t key[W_ITEMS];
+      float ox[W_ITEMS], oy[W_ITEMS], oz[W_ITEMS], vx[W_ITEMS], vy[W_ITEMS], vz[W_ITEMS];
+      float m[W_ITEMS];
+      int64_t id[W_ITEMS];
       bool act[W_ITEMS];
 #pragma unroll
-      for (int j = 0; j < W_ITEMS; j++) act[j] = i0 + j < n;
-      if (act[0]) {
-        if (act[1]) {
-          const uint2 k2 = *reinterpret_cast<const uint2*>(cv.key + i0);
-          const float2 a = *reinterpret_cast<const float2*>(cv.ox + i0);
-          const float2 bb = *reinterpret_cast<const float2*>(cv.oy + i0);
-          const float2 cc = *reinterpret_cast<const float2*>(cv.oz + i0);
-          const float2 d = *reinterpret_cast<const float2*>(cv.vx + i0);
-          const float2 e = *reinterpret_cast<const float2*>(cv.vy + i0);
-          const float2 f = *reinterpret_cast<const float2*>(cv.vz + i0);
-          key[0] = k2.x, key[1] = k2.y;
-          ox[0] = a.x, ox[1] = a.y, oy[0] = bb.x, oy[1] = bb.y, oz[0] = cc.x, oz[1] = cc.y;
-          vx[0] = d.x, vx[1] = d.y, vy[0] = e.x, vy[1] = e.y, vz[0] = f.x, vz[1] = f.y;
-        } else {
-          key[0] = cv.key[i0];
-          ox[0] = cv.ox[i0], oy[0] = cv.oy[i0], oz[0] = cv.oz[i0];
-          vx[0] = cv.vx[i0], vy[0] = cv.vy[i0], vz[0] = cv.vz[i0];
-        }
-#pragma unroll
-        for (int j = 0; j < W_ITEMS; j++) {
-          if (act[j] && has_m) m[j] = cv.m[i0 + j];
-          if (act[j] && has_id) id[j] = cv.id[i0 + j];
+      for (int j = 0; j < W_ITEMS; j++) {
+        act[j] = i0 + j < n;
+        key[j] = key0;
+        ox[j] = oy[j] = oz[j] = vx[j] = vy[j] = vz[j] = m[j] = 0.0f;
+        id[j] = 0;
+        if (act[j]) {
+          key[j] = cv.key[i0 + j];
+          ox[j] = cv.ox[i0 + j], oy[j] = cv.oy[i0 + j], oz[j] = cv.oz[i0 + j];
+          vx[j] = cv.vx[i0 + j], vy[j] = cv.vy[i0 + j], vz[j] = cv.vz[i0 + j];
+          if (has_m) m[j] = cv.m[i0 + j];
+          if (has_id) id[j] = cv.id[i0 + j];
         }
       }
       __syncwarp();
@@ -383,8 +396,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       bool stay[W_ITEMS];
 #pragma unroll
       for (int j = 0; j < W_ITEMS; j++) {
-        int x, y, z;
-        unpack_key(g, key[j], x, y, z);
+        const int x = (int)(key[j] & g.mask[0]), y = (int)((key[j] >> g.shift[1]) & g.mask[1]),
+                  z = (int)((key[j] >> g.shift[2]) & g.mask[2]);
         const int t0 = (x - x0) + FX * ((y - y0) + TILE * (z - z0));
         const float gx = __fsub_rn(1.0f, ox[j]), gy = __fsub_rn(1.0f, oy[j]),
                     gz = __fsub_rn(1.0f, oz[j]);
@@ -402,57 +415,51 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         vx[j] = __fmaf_rn(mp.dtk, a0, vx[j]);
         vy[j] = __fmaf_rn(mp.dtk, a1, vy[j]);
         vz[j] = __fmaf_rn(mp.dtk, a2, vz[j]);
-        if (act[j])
-          maxv2 = fmaxf(maxv2, __fadd_rn(__fadd_rn(__fmul_rn(vx[j], vx[j]), __fmul_rn(vy[j], vy[j])),
-                                         __fmul_rn(vz[j], vz[j])));
-        float o[3] = {ox[j], oy[j], oz[j]};
-        const float vv[3] = {vx[j], vy[j], vz[j]};
-        int xyz[3] = {x, y, z};
-        bool finite = true;
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          float od = __fmaf_rn(mp.dtn, vv[d], o[d]);
-          finite = finite && isfinite(od);
-          const float fl = floorf(od);
-          od = __fsub_rn(od, fl);
-          int carry = (int)fl;
-          if (od >= 1.0f) {
-            od = 0.0f;
-            carry += 1;
-          }
-          o[d] = od;
-          xyz[d] = finite ? wrap_add(xyz[d], carry, g.n[d]) : xyz[d];
-        }
-        stay[j] = true;
+        const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(vx[j], vx[j]), __fmul_rn(vy[j], vy[j])),
+                                   __fmul_rn(vz[j], vz[j]));
+        maxv2 = fmaxf(maxv2, act[j] ? v2 : 0.0f);
+        // drift in cell units: o += dtn v, integer part carried into the cell
+        const float px = __fmaf_rn(mp.dtn, vx[j], ox[j]), py = __fmaf_rn(mp.dtn, vy[j], oy[j]),
+                    pz = __fmaf_rn(mp.dtn, vz[j], oz[j]);
+        const bool finite = fabsf(px) <= 3.402823466e38f && fabsf(py) <= 3.402823466e38f &&
+                            fabsf(pz) <= 3.402823466e38f;
+        const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+        float rx = __fsub_rn(px, fx), ry = __fsub_rn(py, fy), rz = __fsub_rn(pz, fz);
+        int kx = (int)fx, ky = (int)fy, kz = (int)fz;
+        kx += rx >= 1.0f, ky += ry >= 1.0f, kz += rz >= 1.0f;
+        rx = rx >= 1.0f ? 0.0f : rx, ry = ry >= 1.0f ? 0.0f : ry, rz = rz >= 1.0f ? 0.0f : rz;
+        const int nx = wrap_near(x, finite ? kx : 0, g.n[0]);
+        const int ny = wrap_near(y, finite ? ky : 0, g.n[1]);
+        const int nz = wrap_near(z, finite ? kz : 0, g.n[2]);
         if (finite) {
-          ox[j] = o[0];
-          oy[j] = o[1];
-          oz[j] = o[2];
-          key[j] = pack_key(g, xyz[0], xyz[1], xyz[2]);
-          stay[j] = brick_of(g, xyz[0], xyz[1], xyz[2]) == b;
-        } else if (act[j]) {
-          set_flag(flags, ERR_NONFINITE);
+          ox[j] = rx, oy[j] = ry, oz[j] = rz;
+          key[j] = pack_key(g, nx, ny, nz);
         }
+        stay[j] = ((nx / BRICK) == bx) & ((ny / BRICK) == by) & ((nz / BRICK) == bz);
+        if (!finite && act[j]) set_flag(flags, ERR_NONFINITE);
       }
 
       // stayers: lane-major order inside the warp, slots from the brick cursor
       const unsigned lt = (1u << lane) - 1u;
-      const unsigned s0 = __ballot_sync(0xffffffffu, act[0] && stay[0]);
-      const unsigned s1 = __ballot_sync(0xffffffffu, act[1] && stay[1]);
-      const int ns = __popc(s0) + __popc(s1);
-      const unsigned m0 = __ballot_sync(0xffffffffu, act[0] && !stay[0]);
-      const unsigned m1 = __ballot_sync(0xffffffffu, act[1] && !stay[1]);
-      const int nmv = __popc(m0) + __popc(m1);
+      unsigned sb[W_ITEMS], mb[W_ITEMS];
+      int ns = 0, nmv = 0, sq = 0, mqo = 0;
+#pragma unroll
+      for (int j = 0; j < W_ITEMS; j++) {
+        sb[j] = __ballot_sync(0xffffffffu, act[j] && stay[j]);
+        mb[j] = __ballot_sync(0xffffffffu, act[j] && !stay[j]);
+        ns += __popc(sb[j]);
+        nmv += __popc(mb[j]);
+        sq += __popc(sb[j] & lt);
+        mqo += __popc(mb[j] & lt);
+      }
       int sbase = 0;
       unsigned long long mbase = 0;
       if (lane == 0) {
         if (ns) sbase = atomicAdd(&s_cursor[fs], ns);
         if (nmv) mbase = atomicAdd(mov_count, (unsigned long long)nmv);
       }
-      sbase = __shfl_sync(0xffffffffu, sbase, 0);
-      mbase = __shfl_sync(0xffffffffu, mbase, 0);
-      int sq = sbase + __popc(s0 & lt) + __popc(s1 & lt);
-      long long mq = (long long)mbase + __popc(m0 & lt) + __popc(m1 & lt);
+      sq += __shfl_sync(0xffffffffu, sbase, 0);
+      long long mq = (long long)__shfl_sync(0xffffffffu, mbase, 0) + mqo;
 #pragma unroll
       for (int j = 0; j < W_ITEMS; j++) {
         if (!act[j]) continue;
