@@ -353,7 +353,7 @@ def main():
     per_launch_ms = phases[dom][0] / max(1, phases[dom][1])
     if dom == "move":
         ab = alg_bytes_move(npart, nsites)
-        kname = "k_move<kick,drift>"
+        kname = "k_move_pipe" if ctx.last_move_kernel() == 2 else "k_move<kick,drift>"
     else:
         ab = alg_bytes_deposit(npart, nsites)
         kname = "k_deposit<scalar>"

@@ -179,6 +179,9 @@ lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
  * LF2_ERR_UNSUPPORTED).  Both give the same particles (the order of the
  * particles inside a brick may differ); no reference counterpart. */
 lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
+/* Kernel the last lf2_step used for its kick-drift-rebin pass: 1 per-brick,
+ * 2 pipelined, 0 before the first step. */
+lf2_status lf2_last_move_kernel(lf2_ctx* ctx, int* which);
 /* FP64 conservation sums over all particles: total mass, momentum sum m v
  * and max |v| (cout_particle_velocity_stats, LATfield2_Particles.hpp:
  * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */

@@ -217,6 +217,13 @@ class Context:
         2 persistent TMA-pipelined."""
         self._check(_lib.load().lf2_set_move_kernel(self.h, int(which)), "set_move_kernel")
 
+    def last_move_kernel(self):
+        """Kernel of the last step's kick-drift-rebin pass: 1 per-brick,
+        2 pipelined, 0 before the first step."""
+        w = _c.c_int()
+        self._check(_lib.load().lf2_last_move_kernel(self.h, _c.byref(w)), "last_move_kernel")
+        return w.value
+
     def conservation(self):
         m = _c.c_double()
         mom = (_c.c_double * 3)()

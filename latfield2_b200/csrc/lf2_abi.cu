@@ -732,6 +732,7 @@ lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift
   const bool pipe = c->move_kernel == 2 || (c->move_kernel == 0 && move_pipe_eligible(c, F->data));
   if (c->move_kernel == 2 && !move_pipe_eligible(c, F->data))
     return fail(c, LF2_ERR_UNSUPPORTED, "pipelined move needs n0 % 4 == 0, n >= 32, aligned F");
+  c->last_move_kernel = pipe ? 2 : 1;
   {
     PhaseScope ps(c, PH_MOVE);
     LF2_CUDA(c, pipe ? launch_move_pipe(c, F->data, mp) : launch_move(c, F->data, true, true, mp));
@@ -745,6 +746,13 @@ lf2_status lf2_set_move_kernel(lf2_ctx* c, int which)
 {
   if (!c || which < 0 || which > 2) return LF2_ERR_ARG;
   c->move_kernel = which;
+  return LF2_OK;
+}
+
+lf2_status lf2_last_move_kernel(lf2_ctx* c, int* which)
+{
+  if (!c || !which) return LF2_ERR_ARG;
+  *which = c->last_move_kernel;
   return LF2_OK;
 }
 

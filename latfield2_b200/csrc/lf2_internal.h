@@ -101,6 +101,7 @@ struct lf2_ctx {
   // pipelined fused move (lf2_move_pipe.cu)
   int num_sms = 0;
   int move_kernel = 0;               // 0 auto, 1 per-brick k_move, 2 pipelined
+  int last_move_kernel = 0;          // kernel of the last kick-drift pass (1 or 2)
   int* work = nullptr;               // device brick counter
   const float* tmap_src = nullptr;   // field the cached tensor map describes
   alignas(64) unsigned char tmap_bytes[128];
