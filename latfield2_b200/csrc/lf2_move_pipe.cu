@@ -8,7 +8,8 @@
 // buffer.  What differs is how the data reaches the SM and how the work is
 // shared:
 //
-//   * one CTA per SM; the last warp is the producer, the others consumers;
+//   * one CTA per SM: consumer warps, one producer warp (a single thread)
+//     and one patch warp;
 //   * bricks are taken from a global counter (load balance for clustered
 //     particle distributions); empty bricks cost one atomic;
 //   * the producer loads each brick's (BRICK+1)^3 vertex tile of F with one
@@ -19,8 +20,9 @@
 //     signalled on mbarriers, so the next brick's tile and the next chunks
 //     stream in while the consumers work on the current ones;
 //   * vertices that wrap around the periodic boundary lie outside the tensor
-//     and arrive as zeros; the producer patches those planes with plain loads
-//     before it releases the tile;
+//     and arrive as zeros; the patch warp fills those planes with plain loads
+//     before it releases the tile to the consumers, off the producer's path;
+//   * the producer fetches brick indices and segment bounds one brick ahead;
 //   * consumer warps never wait for one another: each takes its own slice of
 //     every chunk and reserves its output slots with atomics.  The order of
 //     the stayers inside a brick therefore follows the warps' timing.
@@ -38,18 +40,18 @@ namespace lf2 {
 
 namespace {
 
-// Launch shape (measured at 512^3 with 134M particles: 31 x 1 2.79 ms,
-// 24 x 1 2.81, 16 x 2 2.84, 8 x 4 3.78; two chunk buffers instead of three
-// cost 9%)
+// Launch shape: consumer warps x particles per lane (measured at 512^3 with
+// 134M particles before the patch warp existed: 31 x 1 2.79 ms, 24 x 1 2.81,
+// 16 x 2 2.84, 8 x 4 3.78; two chunk buffers instead of three cost 9%)
 #ifndef LF2_PIPE_WARPS
-#define LF2_PIPE_WARPS 31
+#define LF2_PIPE_WARPS 30
 #endif
 #ifndef LF2_PIPE_ITEMS
 #define LF2_PIPE_ITEMS 1
 #endif
 constexpr int PC_WARPS = LF2_PIPE_WARPS;         // consumer warps
 constexpr int PC_THREADS = PC_WARPS * 32;        // consumer threads
-constexpr int P_THREADS = PC_THREADS + 32;       // + one producer warp
+constexpr int P_THREADS = PC_THREADS + 64;       // + producer warp + patch warp
 constexpr int W_ITEMS = LF2_PIPE_ITEMS;          // consecutive slots per lane
 constexpr int WSUB = 32 * W_ITEMS;               // slots per warp per chunk
 constexpr int CHUNK = PC_WARPS * WSUB;           // particles per chunk buffer
@@ -103,19 +105,35 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
   return ok != 0;
 }
 
+// try_wait that lets the hardware suspend the thread for up to `ns`
+// nanoseconds while the phase is incomplete
+__device__ __forceinline__ bool mbar_try_hint(uint64_t* bar, uint32_t parity, uint32_t ns)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for the phase with the given parity; false (and the timeout flag)
-// when it has not completed within WAIT_CYCLES.
+// when it has not completed within WAIT_CYCLES.  The waiting thread is
+// suspended between polls (measured: 2% faster than a plain poll loop).
 __device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* flags)
 {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_try(bar, parity)) {
+  for (;;) {
+    if (mbar_try_hint(bar, parity, 20000u)) return true;
     if (clock64() - t0 > WAIT_CYCLES) {
       set_flag(flags, ERR_TIMEOUT);
       return false;
     }
   }
-  return true;
 }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
@@ -193,9 +211,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                 int stage_bytes)
 {
   extern __shared__ unsigned char dyn[];
-  // full_f: tile ready for the consumers; tma_f: tile copy landed (edge
-  // bricks, before the producer patches the wrapped planes); empty_f: all
-  // consumer warps are done with the brick; full_p / empty_p: chunk ring.
+  // tma_f: tile copy landed (or the end of the bricks); full_f: tile
+  // patched and ready for the consumers; empty_f: all consumer warps are
+  // done with the brick; full_p / empty_p: chunk ring.
   __shared__ uint64_t full_f[2], tma_f[2], empty_f[2], full_p[MAX_STAGES], empty_p[MAX_STAGES];
   __shared__ Job job[2];
   __shared__ int s_cursor[2];     // stayers written back so far (per tile buffer)
@@ -223,102 +241,48 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
   if (warp == PC_WARPS) {
     // ------------------------------------------------------------ producer
-    long long fk = 0, pk = 0;  // tile buffers and chunk buffers handed out so far
-    unsigned te = 0;           // bit s: parity of the next tma_f[s] phase
+    // One thread.  Brick indices and their segments are fetched one brick
+    // ahead, so that their latency overlaps the issue of the current brick.
+    if (lane != 0) return;
+    long long fk = 0;           // tile buffers handed out so far
+    int pps = 0;                // next chunk buffer
+    uint32_t ppar = 0;          // parity of the current round through the ring
+    bool wrapped = false;       // every buffer has been used once
+    long long b = atomicAdd(work, 1);
+    int cnt = b < g.nbricks ? LF2_BRICK_COUNT(v, b) : 0;
+    long long base = b < g.nbricks ? v.seg_start[b] : 0;
+    long long bn = b < g.nbricks ? atomicAdd(work, 1) : b;
     for (;;) {
-      int state = 0;           // 0 brick posted, 1 empty brick, 2 finished, 3 timed out
-      int edge = 0, cnt = 0;
-      long long b = 0, base = 0;
+      const bool nvalid = bn < g.nbricks;
+      const int cntn = nvalid ? LF2_BRICK_COUNT(v, bn) : 0;
+      const long long basen = nvalid ? v.seg_start[bn] : 0;
+      const long long bnn = nvalid ? atomicAdd(work, 1) : bn;
       const int fs = (int)(fk & 1);
-      if (lane == 0) {
-        b = atomicAdd(work, 1);
-        if (b >= g.nbricks) {
-          if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) {
-            state = 3;
-          } else {
-            job[fs].b = -1;
-            mbar_arrive(&full_f[fs]);
-            state = 2;
-          }
-        } else if ((cnt = LF2_BRICK_COUNT(v, b)) == 0) {
-          brick_maxv2[b] = 0.0f;
-          state = 1;
-        } else if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) {
-          state = 3;
-        } else {
-          base = v.seg_start[b];
-          job[fs].b = b;
-          job[fs].base = base;
-          job[fs].cnt = cnt;
-          s_cursor[fs] = 0;
-          s_done[fs] = 0;
-          s_maxv2[fs] = 0u;
-          int bx, by, bz;
-          brick_coords(g, b, bx, by, bz);
-          edge = bx * BRICK + brick_extent(g.n[0], bx) == g.n[0] ||
-                 by * BRICK + brick_extent(g.n[1], by) == g.n[1] ||
-                 bz * BRICK + brick_extent(g.n[2], bz) == g.n[2];
-          uint64_t* bar = edge ? &tma_f[fs] : &full_f[fs];
-          mbar_arrive_tx(bar, FBYTES);
-          tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, bar);
-        }
+      if (b >= g.nbricks) {
+        if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
+        job[fs].b = -1;
+        mbar_arrive(&tma_f[fs]);  // the patch warp passes it on to the consumers
+        return;
       }
-      state = __shfl_sync(0xffffffffu, state, 0);
-      if (state >= 2) return;
-      if (state == 1) continue;
-      edge = __shfl_sync(0xffffffffu, edge, 0);
-      b = __shfl_sync(0xffffffffu, b, 0);
-      if (edge) {
-        // Vertex planes on the upper periodic boundary lie outside the
-        // tensor and arrive as zeros: plane i = ex holds x = 0 (likewise y, z).
-        if (!warp_wait(&tma_f[fs], (te >> fs) & 1u, flags, lane)) return;
-        te ^= 1u << fs;
-        float* ft = reinterpret_cast<float*>(sm + fs * FSTRIDE);
+      if (cnt == 0) {
+        brick_maxv2[b] = 0.0f;
+      } else {
+        if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
+        job[fs].b = b;
+        job[fs].base = base;
+        job[fs].cnt = cnt;
+        s_cursor[fs] = 0;
+        s_done[fs] = 0;
+        s_maxv2[fs] = 0u;
         int bx, by, bz;
         brick_coords(g, b, bx, by, bz);
-        const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-        const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
-                  ez = brick_extent(g.n[2], bz);
-        const bool wx = x0 + ex == g.n[0], wy = y0 + ey == g.n[1], wz = z0 + ez == g.n[2];
-        const int np_ = TILE * TILE;
-        for (int t = lane; t < 3 * np_; t += 32) {
-          const int pl = t / np_, r = t % np_, u = r % TILE, w = r / TILE;
-          int i, j, k;
-          if (pl == 0) {
-            if (!wx) continue;
-            i = ex, j = u, k = w;
-          } else if (pl == 1) {
-            if (!wy) continue;
-            i = u, j = ey, k = w;
-          } else {
-            if (!wz) continue;
-            i = u, j = w, k = ez;
-          }
-          if (i > ex || j > ey || k > ez) continue;
-          const int gx = x0 + i < g.n[0] ? x0 + i : 0;
-          const int gy = y0 + j < g.n[1] ? y0 + j : 0;
-          const int gz = z0 + k < g.n[2] ? z0 + k : 0;
-          const int64_t s = site_index(g, gx, gy, gz);
-          const int o = i + FX * (j + TILE * k);
-          ft[o] = __ldg(F + s);
-          ft[FCOMP + o] = __ldg(F + g.nsites + s);
-          ft[2 * FCOMP + o] = __ldg(F + 2 * g.nsites + s);
-        }
-        // the buffer is later overwritten by a tile copy (async proxy)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&full_f[fs]);
-      }
-      fk++;
-      int ok = 1;
-      if (lane == 0) {
-        for (int c0 = 0; c0 < cnt && ok; c0 += CHUNK) {
-          const int ps = (int)(pk % nst);
-          const long long use = pk / nst;
-          if (use > 0 && !mbar_wait(&empty_p[ps], (uint32_t)((use - 1) & 1), flags)) {
-            ok = 0;
-            break;
-          }
+        mbar_arrive_tx(&tma_f[fs], FBYTES);
+        tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
+        fk++;
+        for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
+          const int ps = pps;
+          // the previous round's phase of this buffer's empty barrier
+          if (wrapped && !mbar_wait(&empty_p[ps], ppar ^ 1u, flags)) return;
           const int n = min(CHUNK, cnt - c0);
           const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
           const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
@@ -334,10 +298,82 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           bulk_g2s(cv.vz, v.a.vz + p, n4 * 4u, &full_p[ps]);
           if (has_m) bulk_g2s(cv.m, v.a.mass + p, n4 * 4u, &full_p[ps]);
           if (has_id) bulk_g2s(cv.id, v.a.id + p, n4 * 8u, &full_p[ps]);
-          pk++;
+          if (++pps == nst) {
+            pps = 0;
+            ppar ^= 1u;
+            wrapped = true;
+          }
         }
       }
-      if (!__shfl_sync(0xffffffffu, ok, 0)) return;
+      b = bn, cnt = cntn, base = basen, bn = bnn;
+    }
+  }
+
+  if (warp == PC_WARPS + 1) {
+    // ------------------------------------------------------------ patch warp
+    // Takes every landed tile, and for a brick on the upper periodic
+    // boundary fills the vertex planes that lie outside the tensor (they
+    // arrive as zeros): plane i = ex holds x = 0, likewise y and z.  Then it
+    // releases the tile to the consumers.
+    long long fk = 0;
+    for (;;) {
+      const int fs = (int)(fk & 1);
+      if (!warp_wait(&tma_f[fs], (uint32_t)((fk >> 1) & 1), flags, lane)) return;
+      const Job jb = job[fs];
+      if (jb.b < 0) {
+        if (lane == 0) mbar_arrive(&full_f[fs]);
+        return;
+      }
+      int bx, by, bz;
+      brick_coords(g, jb.b, bx, by, bz);
+      const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+      const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+                ez = brick_extent(g.n[2], bz);
+      const bool wx = x0 + ex == g.n[0], wy = y0 + ey == g.n[1], wz = z0 + ez == g.n[2];
+      if (wx || wy || wz) {
+        float* ft = reinterpret_cast<float*>(sm + fs * FSTRIDE);
+        constexpr int NP = TILE * TILE, NT = 3 * NP, U = 7;  // U loads in flight per lane
+        for (int t0 = lane; t0 < NT; t0 += 32 * U) {
+          float val[U][3];
+          int dst[U];
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            dst[u] = -1;
+            const int t = t0 + 32 * u;
+            if (t >= NT) continue;
+            const int pl = t / NP, r = t % NP, p0 = r % TILE, p1 = r / TILE;
+            int i, j, k;
+            bool on;
+            if (pl == 0)
+              i = ex, j = p0, k = p1, on = wx;
+            else if (pl == 1)
+              i = p0, j = ey, k = p1, on = wy;
+            else
+              i = p0, j = p1, k = ez, on = wz;
+            if (!on || i > ex || j > ey || k > ez) continue;
+            const int gx = x0 + i < g.n[0] ? x0 + i : 0;
+            const int gy = y0 + j < g.n[1] ? y0 + j : 0;
+            const int gz = z0 + k < g.n[2] ? z0 + k : 0;
+            const int64_t s = site_index(g, gx, gy, gz);
+            dst[u] = i + FX * (j + TILE * k);
+            val[u][0] = __ldg(F + s);
+            val[u][1] = __ldg(F + g.nsites + s);
+            val[u][2] = __ldg(F + 2 * g.nsites + s);
+          }
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            if (dst[u] < 0) continue;
+            ft[dst[u]] = val[u][0];
+            ft[FCOMP + dst[u]] = val[u][1];
+            ft[2 * FCOMP + dst[u]] = val[u][2];
+          }
+        }
+        // the buffer is later overwritten by a tile copy (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full_f[fs]);
+      fk++;
     }
   }
 
@@ -349,7 +385,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   // count and max |v|^2 and hands the tile buffer back.  In-place writes
   // never reach a slot whose chunk has not been copied in: the cursor never
   // exceeds the number of particles of the chunks already in the ring.
-  long long fk = 0, pk = 0;
+  long long fk = 0;
+  int cps = 0;          // chunk buffer of the next chunk
+  uint32_t cpar = 0;    // parity of its full barrier's phase
   for (;;) {
     const int fs = (int)(fk & 1);
     if (!warp_wait(&full_f[fs], (uint32_t)((fk >> 1) & 1), flags, lane)) return;
@@ -365,9 +403,12 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
     float maxv2 = 0.0f;
     for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
-      const int ps = (int)(pk % nst);
-      if (!warp_wait(&full_p[ps], (uint32_t)((pk / nst) & 1), flags, lane)) return;
-      pk++;
+      const int ps = cps;
+      if (!warp_wait(&full_p[ps], cpar, flags, lane)) return;
+      if (++cps == nst) {
+        cps = 0;
+        cpar ^= 1u;
+      }
       const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
       const int n = min(CHUNK, cnt - c0);
       const int i0 = warp * WSUB + W_ITEMS * lane;
