@@ -22,7 +22,9 @@
 //   * vertices that wrap around the periodic boundary lie outside the tensor
 //     and arrive as zeros; the patch warp fills those planes with plain loads
 //     before it releases the tile to the consumers, off the producer's path;
-//   * the producer fetches brick indices and segment bounds one brick ahead;
+//   * the producer fetches brick indices and segment bounds ahead and posts
+//     a brick's tile copy as soon as a tile buffer frees up, between the
+//     chunk copies of the brick before;
 //   * consumer warps never wait for one another: each takes its own slice of
 //     every chunk and reserves its output slots with atomics.  The order of
 //     the stayers inside a brick therefore follows the warps' timing.
@@ -59,6 +61,11 @@ constexpr int FX = 20;                           // padded tile row (floats)
 constexpr int FCOMP = FX * TILE * TILE;          // floats per component of a tile buffer
 constexpr uint32_t FBYTES = 3u * FCOMP * 4u;     // bytes one tile copy delivers
 constexpr int FSTRIDE = (FBYTES + 1023) & ~1023; // tile buffer stride in shared memory
+#ifndef LF2_PIPE_FSTAGES
+#define LF2_PIPE_FSTAGES 2
+#endif
+constexpr int NF = LF2_PIPE_FSTAGES;             // tile buffers (1 or 2)
+static_assert(NF == 1 || NF == 2, "one or two tile buffers");
 #ifndef LF2_PIPE_MAX_STAGES
 #define LF2_PIPE_MAX_STAGES 4
 #endif
@@ -98,6 +105,20 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// non-blocking test of a phase
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(saddr(bar)), "r"(parity)
@@ -222,7 +243,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
   unsigned char* sm = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  unsigned char* pbuf = sm + 2 * FSTRIDE;
+  unsigned char* pbuf = sm + NF * FSTRIDE;
 
   const Geom& g = v.g;
   const bool has_m = v.a.mass != nullptr, has_id = v.a.id != nullptr;
@@ -241,72 +262,121 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 
   if (warp == PC_WARPS) {
     // ------------------------------------------------------------ producer
-    // One thread.  Brick indices and their segments are fetched one brick
-    // ahead, so that their latency overlaps the issue of the current brick.
+    // One thread.  It posts a brick (job and tile copy) as soon as a tile
+    // buffer is free, polling for that while it issues the chunks of the
+    // brick before; brick indices and segment bounds are fetched ahead.
     if (lane != 0) return;
-    long long fk = 0;           // tile buffers handed out so far
+    long long fk = 0;           // bricks posted so far (tile buffer fk % NF)
     int pps = 0;                // next chunk buffer
     uint32_t ppar = 0;          // parity of the current round through the ring
     bool wrapped = false;       // every buffer has been used once
-    long long b = atomicAdd(work, 1);
-    int cnt = b < g.nbricks ? LF2_BRICK_COUNT(v, b) : 0;
-    long long base = b < g.nbricks ? v.seg_start[b] : 0;
-    long long bn = b < g.nbricks ? atomicAdd(work, 1) : b;
-    for (;;) {
-      const bool nvalid = bn < g.nbricks;
-      const int cntn = nvalid ? LF2_BRICK_COUNT(v, bn) : 0;
-      const long long basen = nvalid ? v.seg_start[bn] : 0;
-      const long long bnn = nvalid ? atomicAdd(work, 1) : bn;
-      const int fs = (int)(fk & 1);
-      if (b >= g.nbricks) {
-        if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
-        job[fs].b = -1;
+    // q0: next brick with its count and segment start loaded; q1: the index
+    // after it
+    long long q0 = atomicAdd(work, 1);
+    int cq0 = q0 < g.nbricks ? LF2_BRICK_COUNT(v, q0) : 0;
+    long long bq0 = q0 < g.nbricks ? v.seg_start[q0] : 0;
+    long long q1 = q0 < g.nbricks ? atomicAdd(work, 1) : q0;
+    // the next brick with particles (b = -1 after the last)
+    auto next_brick = [&](long long& b, int& cnt, long long& base) {
+      for (;;) {
+        b = q0, cnt = cq0, base = bq0;
+        q0 = q1;
+        if (q0 < g.nbricks) {
+          cq0 = LF2_BRICK_COUNT(v, q0);
+          bq0 = v.seg_start[q0];
+          q1 = atomicAdd(work, 1);
+        }
+        if (b >= g.nbricks) {
+          b = -1;
+          return;
+        }
+        if (cnt > 0) return;
+        brick_maxv2[b] = 0.0f;
+      }
+    };
+    auto post = [&](long long b, int cnt, long long base) {
+      const int fs = (int)(fk % NF);
+      job[fs].b = b;
+      fk++;
+      if (b < 0) {
         mbar_arrive(&tma_f[fs]);  // the patch warp passes it on to the consumers
         return;
       }
-      if (cnt == 0) {
-        brick_maxv2[b] = 0.0f;
-      } else {
-        if (fk >= 2 && !mbar_wait(&empty_f[fs], (uint32_t)(((fk >> 1) - 1) & 1), flags)) return;
-        job[fs].b = b;
-        job[fs].base = base;
-        job[fs].cnt = cnt;
-        s_cursor[fs] = 0;
-        s_done[fs] = 0;
-        s_maxv2[fs] = 0u;
-        int bx, by, bz;
-        brick_coords(g, b, bx, by, bz);
-        mbar_arrive_tx(&tma_f[fs], FBYTES);
-        tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
-        fk++;
-        for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
-          const int ps = pps;
-          // the previous round's phase of this buffer's empty barrier
-          if (wrapped && !mbar_wait(&empty_p[ps], ppar ^ 1u, flags)) return;
-          const int n = min(CHUNK, cnt - c0);
-          const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
-          const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
-          const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
-          const long long p = base + c0;
-          mbar_arrive_tx(&full_p[ps], bytes);
-          bulk_g2s(cv.key, v.a.key + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.ox, v.a.ox + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.oy, v.a.oy + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.oz, v.a.oz + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.vx, v.a.vx + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.vy, v.a.vy + p, n4 * 4u, &full_p[ps]);
-          bulk_g2s(cv.vz, v.a.vz + p, n4 * 4u, &full_p[ps]);
-          if (has_m) bulk_g2s(cv.m, v.a.mass + p, n4 * 4u, &full_p[ps]);
-          if (has_id) bulk_g2s(cv.id, v.a.id + p, n4 * 8u, &full_p[ps]);
-          if (++pps == nst) {
-            pps = 0;
-            ppar ^= 1u;
-            wrapped = true;
+      job[fs].base = base;
+      job[fs].cnt = cnt;
+      s_cursor[fs] = 0;
+      s_done[fs] = 0;
+      s_maxv2[fs] = 0u;
+      int bx, by, bz;
+      brick_coords(g, b, bx, by, bz);
+      mbar_arrive_tx(&tma_f[fs], FBYTES);
+      tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
+    };
+    // tile buffer of the next post free?
+    auto tile_free = [&]() {
+      return fk < NF || mbar_test(&empty_f[fk % NF], (uint32_t)(((fk / NF) - 1) & 1));
+    };
+    long long cb, nb_;
+    int ccnt, ncnt;
+    long long cbase, nbase;
+    next_brick(cb, ccnt, cbase);
+    post(cb, ccnt, cbase);
+    next_brick(nb_, ncnt, nbase);
+    bool nposted = false;
+    while (cb >= 0) {
+      for (int c0 = 0; c0 < ccnt; c0 += CHUNK) {
+        const int ps = pps;
+        if (wrapped) {
+          // the previous round's phase of this buffer's empty barrier; post
+          // the next brick meanwhile if its tile buffer frees up
+          const long long t0 = clock64();
+          while (!mbar_test(&empty_p[ps], ppar ^ 1u)) {
+            if (!nposted && tile_free()) {
+              post(nb_, ncnt, nbase);
+              nposted = true;
+            }
+            if (clock64() - t0 > WAIT_CYCLES) {
+              set_flag(flags, ERR_TIMEOUT);
+              return;
+            }
+            __nanosleep(64);
           }
         }
+        if (!nposted && tile_free()) {
+          post(nb_, ncnt, nbase);
+          nposted = true;
+        }
+        const int n = min(CHUNK, ccnt - c0);
+        const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
+        const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
+        const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
+        const long long p = cbase + c0;
+        mbar_arrive_tx(&full_p[ps], bytes);
+        bulk_g2s(cv.key, v.a.key + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.ox, v.a.ox + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.oy, v.a.oy + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.oz, v.a.oz + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.vx, v.a.vx + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.vy, v.a.vy + p, n4 * 4u, &full_p[ps]);
+        bulk_g2s(cv.vz, v.a.vz + p, n4 * 4u, &full_p[ps]);
+        if (has_m) bulk_g2s(cv.m, v.a.mass + p, n4 * 4u, &full_p[ps]);
+        if (has_id) bulk_g2s(cv.id, v.a.id + p, n4 * 8u, &full_p[ps]);
+        if (++pps == nst) {
+          pps = 0;
+          ppar ^= 1u;
+          wrapped = true;
+        }
       }
-      b = bn, cnt = cntn, base = basen, bn = bnn;
+      if (!nposted) {
+        const int fs = (int)(fk % NF);
+        if (fk >= NF && !mbar_wait(&empty_f[fs], (uint32_t)(((fk / NF) - 1) & 1), flags)) return;
+        post(nb_, ncnt, nbase);
+      }
+      cb = nb_, ccnt = ncnt, cbase = nbase;
+      if (cb >= 0) next_brick(nb_, ncnt, nbase);
+      nposted = false;
     }
+    return;
   }
 
   if (warp == PC_WARPS + 1) {
@@ -317,8 +387,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     // releases the tile to the consumers.
     long long fk = 0;
     for (;;) {
-      const int fs = (int)(fk & 1);
-      if (!warp_wait(&tma_f[fs], (uint32_t)((fk >> 1) & 1), flags, lane)) return;
+      const int fs = (int)(fk % NF);
+      if (!warp_wait(&tma_f[fs], (uint32_t)((fk / NF) & 1), flags, lane)) return;
       const Job jb = job[fs];
       if (jb.b < 0) {
         if (lane == 0) mbar_arrive(&full_f[fs]);
@@ -389,8 +459,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   int cps = 0;          // chunk buffer of the next chunk
   uint32_t cpar = 0;    // parity of its full barrier's phase
   for (;;) {
-    const int fs = (int)(fk & 1);
-    if (!warp_wait(&full_f[fs], (uint32_t)((fk >> 1) & 1), flags, lane)) return;
+    const int fs = (int)(fk % NF);
+    if (!warp_wait(&full_f[fs], (uint32_t)((fk / NF) & 1), flags, lane)) return;
     const Job jb = job[fs];
     if (jb.b < 0) return;
     const int64_t b = jb.b;
@@ -609,11 +679,11 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp)
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   const size_t sb = stage_bytes_for(c);
-  const size_t fixed = 1024 + 2 * (size_t)FSTRIDE + 2048;  // alignment slack, tiles, static
+  const size_t fixed = 1024 + NF * (size_t)FSTRIDE + 2048;  // alignment slack, tiles, static
   int nst = (int)(((size_t)optin > fixed ? (size_t)optin - fixed : 0) / sb);
   nst = nst > MAX_STAGES ? MAX_STAGES : nst;
   if (nst < 2) return cudaErrorInvalidConfiguration;
-  const size_t smem = 1024 + 2 * (size_t)FSTRIDE + (size_t)nst * sb;
+  const size_t smem = 1024 + NF * (size_t)FSTRIDE + (size_t)nst * sb;
   cudaError_t e = cudaFuncSetAttribute(k_move_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
