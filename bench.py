@@ -281,6 +281,22 @@ def reference_arm(args, rank):
 
 
 # ------------------------------------------------------------------- ours
+def replica_throughput(ms_local, npart, steps, pg=None, device="cpu"):
+    """Whole-job time and throughput of N replicas: the time is the maximum
+    over the ranks (every rank takes part in the same all-reduce), the
+    throughput counts the particles of all ranks.  pg is torch.distributed
+    (any backend) or None for one rank."""
+    import torch
+    world = 1
+    ms = float(ms_local)
+    if pg is not None:
+        world = pg.get_world_size()
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, npart * world * steps / (ms / 1e3)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -340,12 +356,8 @@ def main():
     ms = e0.elapsed_time(e1)
     phases = ctx.profile_read()
     ctx.profile(False)
-    if pg is not None:
-        t = torch.tensor([ms], device=device)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms, value = replica_throughput(ms, npart, args.steps, pg, device)
     ms_step = ms / args.steps
-    value = npart * world * args.steps / (ms / 1e3)
 
     # dominant kernel and its roofline (algorithmic bytes per launch / mean launch time)
     peak, peak_kind = peaks()
@@ -387,11 +399,9 @@ def main():
         ctx.gather_kick(Fh, 0.0, want_max_v=True)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
-    if pg is not None:
-        t = torch.tensor([t_e2e], device=device)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e = {"value": npart * world * args.e2e_steps / t_e2e, "unit": UNIT,
+    t_e2e_ms, e2e_value = replica_throughput(1e3 * t_e2e, npart, args.e2e_steps, pg, device)
+    t_e2e = t_e2e_ms / 1e3
+    e2e = {"value": e2e_value, "unit": UNIT,
            "h2d_bytes_per_step": 3 * nsites * 4, "d2h_bytes_per_step": nsites * 4 + 8,
            "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
            "path": "lf2_field_import(F, host) + lf2_step + lf2_field_export(rho, host) + "
