@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true",
+                    help="skip the FP32-mode run of the same particles (fixed-point workloads)")
     return ap.parse_args()
 
 
@@ -281,6 +283,28 @@ def reference_arm(args, rank):
 
 
 # ------------------------------------------------------------------- ours
+def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
+    """Device time per lf2_step of the same particles with FP32 atomic
+    deposits (CUDA events on the launching stream)."""
+    import torch
+    import latfield2_b200 as L
+    cell, off, vel = case
+    ctx = L.Context(n, box=1.0, mode=L.DEPOSIT_FP32, device=local)
+    ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
+    Fh, rho = ctx.field(3, F), ctx.field(1)
+    for _ in range(warmup):
+        ctx.step(Fh, dtau, dtau, rho)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        ctx.step(Fh, dtau, dtau, rho)
+    e1.record()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
 def replica_throughput(ms_local, npart, steps, pg=None, device="cpu"):
     """Whole-job time and throughput of N replicas: the time is the maximum
     over the ranks (every rank takes part in the same all-reduce), the
@@ -327,6 +351,7 @@ def main():
     nsites = n[0] * n[1] * n[2]
     ctx = L.Context(n, box=1.0, mode=mode, device=local)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
+    fp32_case = (cell, off, vel) if (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) else None
     del cell, off, vel
     Fh = ctx.field(3, F)
     rho = ctx.field(1)
@@ -409,6 +434,18 @@ def main():
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
 
+    # the same particles and steps with FP32 atomic deposits
+    fixed_vs_fp32 = None
+    if fp32_case is not None:
+        del ctx, Fh, rho
+        torch.cuda.empty_cache()
+        ms32 = fp32_step_ms(n, fp32_case, F, npart, dtau, args.warmup, args.steps, local)
+        ms32, _ = replica_throughput(ms32 * args.steps, npart, args.steps, pg, device)
+        ms32 /= args.steps
+        fixed_vs_fp32 = {"fixed_ms_per_step": ms_step, "fp32_ms_per_step": ms32,
+                         "ratio": ms_step / ms32}
+    del fp32_case
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -432,6 +469,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
+            "fixed_vs_fp32": fixed_vs_fp32,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
