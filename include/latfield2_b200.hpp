@@ -1,0 +1,702 @@
+/* latfield2_b200.hpp -- header-only C++ layer with the names and signatures
+ * of LATfield2's particle path, over the C ABI of lf2gpu.h.
+ *
+ * Code written against the reference's particle interface compiles against
+ * this header instead of LATfield2.hpp for that path:
+ *
+ *   Lattice lat(3, N, 1), lat_part(3, N, 0);             LATfield2_Lattice_decl.hpp:17-57
+ *   Field<Real> rho(lat, 1), F(lat, 3);                  LATfield2_Field_decl.hpp:75-98
+ *   Particles<part_simple, part_simple_info, part_simple_dataType> parts;
+ *   parts.initialize(info, type, &lat_part, boxSize);    LATfield2_Particles.hpp:358-428
+ *   parts.addParticle_global(p);                         :500-540
+ *   projection_init(&rho);                               projections.hpp:31-34
+ *   scalarProjectionCIC_project(&parts, &rho);           :75-184
+ *   scalarProjectionCIC_comm(&rho);                      :194-300
+ *   F(x, c) = ...;  F.updateHalo();                      LATfield2_Field_decl.hpp:889-935
+ *   parts.updateVel(cic_gather_kick, dtau, &Fp, 1);      LATfield2_Particles.hpp:752-893
+ *   parts.moveParticles(move_particles_simple, dtau);    :1810-2803, move_function.hpp:15-32
+ *
+ * Where the data live:
+ *   - Particles live on the GPU.  addParticle_global stages them on the host;
+ *     they are uploaded before the next GPU operation.
+ *   - A Field keeps a host array in the reference layout (halo, components
+ *     interleaved, Real) and, once a particle operation has used it, a device
+ *     copy in the Particles' context.
+ *   - The two sides are brought together at the reference's own
+ *     synchronisation points:
+ *     - updateHalo() fills the host halo and marks the host values as the
+ *       current ones, so the next particle operation uploads them;
+ *     - the *_comm functions bring a projection back to the host array.
+ *
+ * Only the library's kernels run on the GPU: updateVel accepts
+ * cic_gather_kick and moveParticles accepts move_particles_simple (matched
+ * by function identity).  Any other callback raises std::invalid_argument;
+ * the reference runs such callbacks on the host per particle, and this layer
+ * has no host path.
+ *
+ * Errors of the C ABI are raised as std::runtime_error carrying
+ * lf2_last_error(); the reference exits or throws in the same places.
+ * One GPU, one process: the MPI process grid of the reference is 1 x 1.
+ */
+#ifndef LATFIELD2_B200_HPP
+#define LATFIELD2_B200_HPP
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <ostream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "lf2gpu.h"
+
+namespace LATfield2 {
+
+#ifdef SINGLE
+typedef float Real;
+#else
+typedef double Real;
+#endif
+
+// LATfield2_Particles.hpp:76-86, projections.hpp:38-39, LATfield2_Field.hpp:16-17
+#ifndef GLOBAL_MASS
+#define GLOBAL_MASS 0
+#define INDIVIDUAL_MASS 1
+#define NO_MASS 2
+#endif
+static int const FROM_PART = INDIVIDUAL_MASS;
+static int const FROM_INFO = GLOBAL_MASS;
+static int const symmetric = 1;
+static int const unsymmetric = 0;
+
+namespace lf2detail {
+
+inline void check(const lf2_ctx* ctx, lf2_status s, const char* what)
+{
+  if (s == LF2_OK) return;
+  std::string msg = std::string(what) + ": status " + std::to_string(s);
+  if (ctx) msg += std::string(": ") + lf2_last_error(ctx);
+  throw std::runtime_error(msg);
+}
+
+// A particle type with a `mass` member carries individual masses
+// (INDIVIDUAL_MASS, LATfield2_Particles.hpp:400-425).
+template <class T, class = void>
+struct has_mass : std::false_type {};
+template <class T>
+struct has_mass<T, decltype((void)std::declval<T&>().mass, void())> : std::true_type {};
+
+template <class T>
+float mass_of(const T& p, std::true_type)
+{
+  return (float)p.mass;
+}
+template <class T>
+float mass_of(const T&, std::false_type)
+{
+  return 0.0f;
+}
+
+}  // namespace lf2detail
+
+// ------------------------------------------------------------------ Lattice
+// 3-D periodic lattice of size[0] x size[1] x size[2] sites with a halo of
+// `halo` sites (LATfield2_Lattice_decl.hpp:17-135).  One process: the local
+// sublattice is the whole lattice.
+class Lattice {
+ public:
+  Lattice() {}
+  Lattice(int dim, const int* size, int halo) { initialize(dim, size, halo); }
+  Lattice(int dim, const int size, int halo) { initialize(dim, size, halo); }
+  void initialize(int dim, const int* size, int halo)
+  {
+    if (dim != 3) throw std::invalid_argument("Lattice: only 3 dimensions are provided");
+    for (int d = 0; d < 3; d++) size_[d] = size[d];
+    halo_ = halo;
+  }
+  void initialize(int dim, const int size, int halo)
+  {
+    const int s[3] = {size, size, size};
+    initialize(dim, s, halo);
+  }
+  int dim() { return 3; }
+  int halo() { return halo_; }
+  int* size() { return size_; }
+  int size(int direction) { return size_[direction]; }
+  int* sizeLocal() { return size_; }
+  int sizeLocal(int direction) { return size_[direction]; }
+  long sites() { return (long)size_[0] * size_[1] * size_[2]; }
+  long sitesGross() { return (long)gross(0) * gross(1) * gross(2); }
+  long sitesLocal() { return sites(); }
+  long sitesLocalGross() { return sitesGross(); }
+  // index step of one site in a direction of the halo'd lattice
+  long jump(int direction) { return direction == 0 ? 1 : direction == 1 ? gross(0) : (long)gross(0) * gross(1); }
+  int gross(int d) const { return size_[d] + 2 * halo_; }
+
+ private:
+  int size_[3] = {0, 0, 0};
+  int halo_ = 0;
+};
+
+// --------------------------------------------------------------------- Site
+// A site of a lattice, walked with first()/test()/next() over the local
+// sites (LATfield2_Site_decl.hpp:19-195); index() addresses the halo'd
+// arrays of the fields on that lattice.
+class Site {
+ public:
+  Site() {}
+  explicit Site(Lattice& lattice) { initialize(lattice); }
+  Site(Lattice& lattice, long index) { initialize(lattice, index); }
+  void initialize(Lattice& lattice) { lat_ = &lattice; first(); }
+  void initialize(Lattice& lattice, long index)
+  {
+    lat_ = &lattice;
+    setIndex(index);
+  }
+  void first()
+  {
+    c_[0] = c_[1] = c_[2] = 0;
+    reindex();
+  }
+  bool test() { return c_[2] < lat_->size(2); }
+  void next()
+  {
+    if (++c_[0] < lat_->size(0)) {
+      index_ += 1;
+      return;
+    }
+    c_[0] = 0;
+    if (++c_[1] >= lat_->size(1)) {
+      c_[1] = 0;
+      ++c_[2];
+    }
+    reindex();
+  }
+  int coord(int direction) const { return c_[direction]; }
+  long index() const { return index_; }
+  void setIndex(long index)
+  {
+    index_ = index;
+    long r = index;
+    for (int d = 0; d < 3; d++) {
+      c_[d] = (int)(r % lat_->gross(d)) - lat_->halo();
+      r /= lat_->gross(d);
+    }
+  }
+  bool setCoord(int x, int y, int z)
+  {
+    c_[0] = x, c_[1] = y, c_[2] = z;
+    reindex();
+    return true;
+  }
+  // neighbour in +direction / -direction (may be a halo site)
+  Site operator+(int direction) const
+  {
+    Site s(*this);
+    s.c_[direction] += 1;
+    s.index_ += lat_->jump(direction);
+    return s;
+  }
+  Site operator-(int direction) const
+  {
+    Site s(*this);
+    s.c_[direction] -= 1;
+    s.index_ -= lat_->jump(direction);
+    return s;
+  }
+  Lattice& lattice() const { return *lat_; }
+
+ private:
+  void reindex()
+  {
+    const int h = lat_->halo();
+    index_ = (long)(c_[0] + h) + (long)lat_->gross(0) * ((c_[1] + h) + (long)lat_->gross(1) * (c_[2] + h));
+  }
+  Lattice* lat_ = nullptr;
+  long index_ = 0;
+  int c_[3] = {0, 0, 0};
+};
+
+// -------------------------------------------------------------------- Field
+// A field of Real on a lattice: `components` values per site, or a rows x
+// cols matrix (symmetric: rows*(rows+1)/2 values, order 00,01,02,11,12,22
+// for 3x3; LATfield2_Field_decl.hpp:75-208, :772-788).  The host array is
+// laid out like the reference's: halo'd sites, components interleaved.
+template <class FieldType>
+class Field {
+  static_assert(std::is_same<FieldType, Real>::value,
+                "the GPU path provides Field<Real> only");
+
+ public:
+  Field() {}
+  Field(Lattice& lattice, int components = 1) { initialize(lattice, components); }
+  Field(Lattice& lattice, int rows, int cols, int symmetry = unsymmetric)
+  {
+    initialize(lattice, rows, cols, symmetry);
+  }
+  ~Field() { release_device(); }
+  Field(const Field&) = delete;
+  Field& operator=(const Field&) = delete;
+
+  void initialize(Lattice& lattice, int components = 1)
+  {
+    lat_ = &lattice;
+    rows_ = components, cols_ = 1, symmetry_ = unsymmetric;
+    components_ = components;
+    alloc();
+  }
+  void initialize(Lattice& lattice, int rows, int cols, int symmetry = unsymmetric)
+  {
+    lat_ = &lattice;
+    rows_ = rows, cols_ = cols, symmetry_ = symmetry;
+    components_ = symmetry == symmetric ? rows * (rows + 1) / 2 : rows * cols;
+    alloc();
+  }
+  void alloc()
+  {
+    if ((long)data_.size() != lat_->sitesGross() * components_)
+      data_.assign((size_t)(lat_->sitesGross() * components_), FieldType(0));
+  }
+  void dealloc()
+  {
+    release_device();
+    std::vector<FieldType>().swap(data_);
+  }
+
+  FieldType& operator()(long index) { return data_[(size_t)(index * components_)]; }
+  FieldType& operator()(long index, int component)
+  {
+    return data_[(size_t)(index * components_ + component)];
+  }
+  FieldType& operator()(long index, int i, int j) { return (*this)(index, matrix_index(i, j)); }
+  FieldType& operator()(const Site& site) { return (*this)(site.index()); }
+  FieldType& operator()(const Site& site, int component) { return (*this)(site.index(), component); }
+  FieldType& operator()(const Site& site, int i, int j) { return (*this)(site.index(), i, j); }
+
+  // Periodic halo on the host; the host values become the current ones
+  // (uploaded before the next particle operation that reads this field).
+  void updateHalo()
+  {
+    if (device_newer_) pull();
+    const int h = lat_->halo();
+    if (h > 0) fill_halo();
+    device_newer_ = false;
+    host_newer_ = true;
+  }
+
+  int components() const { return components_; }
+  int rows() const { return rows_; }
+  int cols() const { return cols_; }
+  int symmetry() const { return symmetry_; }
+  Lattice& lattice() { return *lat_; }
+  FieldType* data() { return data_.data(); }
+
+  // ---- GPU side (not in the reference) ----
+  // The field's device copy in the given context, with the host values
+  // uploaded first when they are the current ones.
+  // The field holds a reference to the context, so that the context outlives
+  // the field's device copy whatever the order of destruction.
+  lf2_field lf2_handle(const std::shared_ptr<lf2_ctx>& owner, bool upload = true)
+  {
+    lf2_ctx* ctx = owner.get();
+    if (ctx_ != ctx) {
+      if (ctx_ && device_newer_) pull();
+      release_device();
+      lf2detail::check(ctx, lf2_field_create(ctx, components_, &dev_), "lf2_field_create");
+      owner_ = owner;
+      ctx_ = ctx;
+      host_newer_ = true;
+    }
+    if (upload && host_newer_) {
+      lf2detail::check(ctx_, lf2_field_import(ctx_, dev_, data_.data(), lat_->halo(), sizeof(FieldType),
+                                              LF2_PTR_HOST),
+                       "lf2_field_import");
+      host_newer_ = false;
+    }
+    return dev_;
+  }
+  // a particle operation has written the device copy
+  void mark_device_written()
+  {
+    device_newer_ = true;
+    host_newer_ = false;
+  }
+  // device copy -> host array (halo filled periodically)
+  void pull()
+  {
+    if (!ctx_) return;
+    lf2detail::check(ctx_, lf2_field_export(ctx_, dev_, data_.data(), lat_->halo(), sizeof(FieldType), 1,
+                                            LF2_PTR_HOST),
+                     "lf2_field_export");
+    device_newer_ = false;
+  }
+
+ private:
+  int matrix_index(int i, int j) const
+  {
+    if (symmetry_ == symmetric) {
+      const int a = i < j ? i : j, b = i < j ? j : i;
+      return (b - a) + a * rows_ - a * (a - 1) / 2;
+    }
+    return j * rows_ + i;
+  }
+  void fill_halo()
+  {
+    const int h = lat_->halo();
+    const int g[3] = {lat_->gross(0), lat_->gross(1), lat_->gross(2)};
+    const int n[3] = {lat_->size(0), lat_->size(1), lat_->size(2)};
+    for (int z = 0; z < g[2]; z++)
+      for (int y = 0; y < g[1]; y++)
+        for (int x = 0; x < g[0]; x++) {
+          if (x >= h && x < h + n[0] && y >= h && y < h + n[1] && z >= h && z < h + n[2]) continue;
+          const int sx = ((x - h) % n[0] + n[0]) % n[0] + h;
+          const int sy = ((y - h) % n[1] + n[1]) % n[1] + h;
+          const int sz = ((z - h) % n[2] + n[2]) % n[2] + h;
+          const long dst = x + (long)g[0] * (y + (long)g[1] * z);
+          const long src = sx + (long)g[0] * (sy + (long)g[1] * sz);
+          for (int c = 0; c < components_; c++)
+            data_[(size_t)(dst * components_ + c)] = data_[(size_t)(src * components_ + c)];
+        }
+  }
+  void release_device()
+  {
+    if (ctx_ && dev_) lf2_field_destroy(ctx_, dev_);
+    ctx_ = nullptr;
+    dev_ = nullptr;
+    owner_.reset();
+  }
+
+  Lattice* lat_ = nullptr;
+  int components_ = 0, rows_ = 0, cols_ = 1, symmetry_ = unsymmetric;
+  std::vector<FieldType> data_;
+  std::shared_ptr<lf2_ctx> owner_;
+  lf2_ctx* ctx_ = nullptr;
+  lf2_field dev_ = nullptr;
+  bool host_newer_ = true;
+  bool device_newer_ = false;
+};
+
+// ---------------------------------------------------------- particle types
+// LATfield2_particle_simple.hpp:40-82 (the HDF5 datatype structure is empty
+// here: no HDF5 on this path).
+struct part_simple {
+  long ID;
+  Real pos[3];
+  Real vel[3];
+};
+inline std::ostream& operator<<(std::ostream& os, const part_simple& p)
+{
+  os << "ID: " << p.ID << " , Pos: (" << p.pos[0] << "," << p.pos[1] << "," << p.pos[2]
+     << ") , Vel: (" << p.vel[0] << "," << p.vel[1] << "," << p.vel[2] << ")";
+  return os;
+}
+struct part_simple_info {
+  double mass;
+  int relativistic;
+  int type_name_size;
+  char type_name[64];
+};
+struct part_simple_dataType {};
+
+// ------------------------------------------------------------ callbacks
+// move_particles_simple (move_function.hpp:15-32): pos += dtau * vel.  The
+// GPU runs it inside moveParticles; a direct call updates one particle.
+template <class part, class part_info>
+void move_particles_simple_t(double dtau, double, part* p, double*, part_info, Field<Real>**, Site*, int,
+                             double*, double*, int)
+{
+  for (int l = 0; l < 3; l++) p->pos[l] += dtau * p->vel[l];
+}
+
+// The CIC gather-kick: vel_c += dtau * sum over the 8 cell corners of
+// w * F_c(corner), w the product of the 1-D CIC weights (frac or 1 - frac),
+// F = fields[0] with 3 components, sites[0] the particle's cell in F's
+// lattice.  Returns |v|^2 (the quantity updateVel maximises).  The GPU runs
+// it inside updateVel; a direct call kicks one particle on the host arrays.
+template <class part, class part_info>
+Real cic_gather_kick_t(double dtau, double, part* p, double* frac, part_info, Field<Real>** fields,
+                       Site* sites, int, double*, double*, int)
+{
+  Field<Real>& F = *fields[0];
+  Real a[3] = {0, 0, 0};
+  for (int k = 0; k < 8; k++) {
+    const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+    Site s = sites[0];
+    if (cx) s = s + 0;
+    if (cy) s = s + 1;
+    if (cz) s = s + 2;
+    const Real w = (Real)((cx ? frac[0] : 1 - frac[0]) * (cy ? frac[1] : 1 - frac[1]) *
+                          (cz ? frac[2] : 1 - frac[2]));
+    for (int c = 0; c < 3; c++) a[c] += w * F(s, c);
+  }
+  Real v2 = 0;
+  for (int c = 0; c < 3; c++) {
+    p->vel[c] += dtau * a[c];
+    v2 += p->vel[c] * p->vel[c];
+  }
+  return v2;
+}
+
+inline void move_particles_simple(double dtau, double res, part_simple* p, double* frac,
+                                  part_simple_info info, Field<Real>** fields, Site* sites, int nfield,
+                                  double* params, double* outputs, int noutputs)
+{
+  move_particles_simple_t<part_simple, part_simple_info>(dtau, res, p, frac, info, fields, sites, nfield,
+                                                         params, outputs, noutputs);
+}
+
+inline Real cic_gather_kick(double dtau, double res, part_simple* p, double* frac, part_simple_info info,
+                            Field<Real>** fields, Site* sites, int nfield, double* params,
+                            double* outputs, int noutputs)
+{
+  return cic_gather_kick_t<part_simple, part_simple_info>(dtau, res, p, frac, info, fields, sites, nfield,
+                                                          params, outputs, noutputs);
+}
+
+namespace lf2detail {
+typedef Real (*kick_simple_fn)(double, double, part_simple*, double*, part_simple_info, Field<Real>**,
+                               Site*, int, double*, double*, int);
+typedef void (*move_simple_fn)(double, double, part_simple*, double*, part_simple_info, Field<Real>**,
+                               Site*, int, double*, double*, int);
+inline bool is_simple_kick(kick_simple_fn f) { return f == &cic_gather_kick; }
+template <class F>
+bool is_simple_kick(F)
+{
+  return false;
+}
+inline bool is_simple_move(move_simple_fn f) { return f == &move_particles_simple; }
+template <class F>
+bool is_simple_move(F)
+{
+  return false;
+}
+}  // namespace lf2detail
+
+// ---------------------------------------------------------------- Particles
+// LATfield2_Particles.hpp:131-344 for particles that live on the GPU.
+template <class part, class part_info, class part_dataType>
+class Particles {
+ public:
+  typedef Real (*kick_fn)(double, double, part*, double*, part_info, Field<Real>**, Site*, int, double*,
+                          double*, int);
+  typedef void (*move_fn)(double, double, part*, double*, part_info, Field<Real>**, Site*, int, double*,
+                          double*, int);
+
+  Particles() {}
+  Particles(const Particles&) = delete;
+  Particles& operator=(const Particles&) = delete;
+
+  // The deposit mode is the int64 fixed point (bit-exact and independent of
+  // particle order); define LF2_COMPAT_FP32_DEPOSIT for FP32 atomics.
+  void initialize(part_info info, part_dataType, Lattice* lat_part, Real boxSize[3], int device = 0)
+  {
+    info_ = info;
+    lat_ = lat_part;
+    for (int d = 0; d < 3; d++) box_[d] = boxSize[d];
+    res_ = (Real)(boxSize[0] / lat_part->size(0));
+#ifdef LF2_COMPAT_FP32_DEPOSIT
+    const int mode = LF2_DEPOSIT_FP32;
+#else
+    const int mode = LF2_DEPOSIT_FIXED64;
+#endif
+    lf2_ctx* c = nullptr;
+    lf2detail::check(nullptr, lf2_create(&c, device, lat_part->size(), box_, mode, nullptr), "lf2_create");
+    owner_.reset(c, [](lf2_ctx* p) { lf2_destroy(p); });
+    ctx_ = c;
+    on_device_ = 0;
+  }
+
+  bool addParticle_global(part newPart) { return addParticle_global(newPart, false); }
+  bool addParticle_global(part newPart, bool assignID)
+  {
+    if (assignID) newPart.ID = (long)(on_device_ + ids_.size());
+    for (int d = 0; d < 3; d++) {
+      Real x = newPart.pos[d];
+      if (x < 0 || x >= box_[d]) return false;  // outside the box (the reference drops it too)
+      pos_.push_back((double)x);
+      vel_.push_back((double)newPart.vel[d]);
+    }
+    ids_.push_back((int64_t)newPart.ID);
+    mass_.push_back(lf2detail::mass_of(newPart, lf2detail::has_mass<part>()));
+    return true;
+  }
+
+  long numParticles()
+  {
+    sync();
+    int64_t n = 0;
+    lf2detail::check(ctx_, lf2_particles_count(ctx_, &n), "lf2_particles_count");
+    return (long)n;
+  }
+
+  // updateVel with the CIC gather-kick: fields[0] is the 3-component force.
+  // Returns sqrt(max |v|^2) like the reference.
+  Real updateVel(kick_fn updateVel_funct, double dtau, Field<Real>** fields = NULL, int nfields = 0,
+                 double* params = NULL, double* output = NULL, int* reduce_type = NULL, int noutput = 0)
+  {
+    (void)params, (void)output, (void)reduce_type;
+    if (!(updateVel_funct == &cic_gather_kick_t<part, part_info> ||
+          lf2detail::is_simple_kick(updateVel_funct)))
+      throw std::invalid_argument("updateVel: only cic_gather_kick runs on the GPU");
+    if (nfields < 1 || !fields || fields[0]->components() != 3 || noutput != 0)
+      throw std::invalid_argument("updateVel: cic_gather_kick takes one 3-component field, no outputs");
+    check_field(fields[0], "updateVel");
+    sync();
+    double maxv = 0.0;
+    lf2_field F = fields[0]->lf2_handle(owner_);
+    lf2detail::check(ctx_, lf2_gather_kick(ctx_, F, dtau, &maxv), "lf2_gather_kick");
+    return (Real)maxv;
+  }
+
+  void moveParticles(move_fn move_funct, double dtau, Field<Real>** fields = NULL, int nfields = 0,
+                     double* params = NULL, double* output = NULL, int* reduce_type = NULL,
+                     int noutput = 0)
+  {
+    (void)fields, (void)nfields, (void)params, (void)output, (void)reduce_type, (void)noutput;
+    if (!(move_funct == &move_particles_simple_t<part, part_info> ||
+          lf2detail::is_simple_move(move_funct)))
+      throw std::invalid_argument("moveParticles: only move_particles_simple runs on the GPU");
+    sync();
+    lf2detail::check(ctx_, lf2_drift_rebin(ctx_, dtau), "lf2_drift_rebin");
+  }
+
+  Lattice& lattice() { return *lat_; }
+  Real res() { return res_; }
+  // a field used with these particles covers the same sites
+  void check_field(Field<Real>* f, const char* what)
+  {
+    for (int d = 0; d < 3; d++)
+      if (f->lattice().size(d) != lat_->size(d))
+        throw std::invalid_argument(std::string(what) + ": field and particle lattices differ in size");
+  }
+  part_info* parts_info() { return &info_; }
+
+  // ---- GPU side (not in the reference) ----
+  lf2_ctx* lf2_context()
+  {
+    sync();
+    return ctx_;
+  }
+  const std::shared_ptr<lf2_ctx>& lf2_context_owner()
+  {
+    sync();
+    return owner_;
+  }
+  // All particles (ID, position in box units, velocity), in storage order.
+  void getParticles(std::vector<part>& out)
+  {
+    sync();
+    const long n = numParticles();
+    std::vector<Real> pos((size_t)(3 * n)), vel((size_t)(3 * n));
+    std::vector<int64_t> id((size_t)n);
+    lf2detail::check(ctx_, lf2_particles_get_pos(ctx_, pos.data(), vel.data(), sizeof(Real), id.data()),
+                     "lf2_particles_get_pos");
+    out.assign((size_t)n, part());
+    for (long i = 0; i < n; i++) {
+      out[(size_t)i].ID = (long)id[(size_t)i];
+      for (int d = 0; d < 3; d++) {
+        out[(size_t)i].pos[d] = pos[(size_t)(3 * i + d)];
+        out[(size_t)i].vel[d] = vel[(size_t)(3 * i + d)];
+      }
+    }
+  }
+  // Uploads the particles staged by addParticle_global (with those already
+  // on the GPU when there are some).
+  void sync()
+  {
+    if (!ctx_) throw std::logic_error("Particles: initialize() first");
+    if (ids_.empty()) return;
+    if (on_device_ > 0 && lf2detail::has_mass<part>::value)
+      // the GPU does not hand individual masses back with the positions
+      throw std::logic_error("Particles: adding particles with individual masses after the upload");
+    if (on_device_ > 0) {
+      const size_t old = (size_t)on_device_;
+      std::vector<double> p(3 * old), v(3 * old);
+      std::vector<int64_t> id(old);
+      lf2detail::check(ctx_, lf2_particles_get_pos(ctx_, p.data(), v.data(), 8, id.data()),
+                       "lf2_particles_get_pos");
+      pos_.insert(pos_.begin(), p.begin(), p.end());
+      vel_.insert(vel_.begin(), v.begin(), v.end());
+      ids_.insert(ids_.begin(), id.begin(), id.end());
+    }
+    const bool individual = lf2detail::has_mass<part>::value;
+    lf2detail::check(ctx_,
+                     lf2_particles_set_pos(ctx_, (int64_t)ids_.size(), pos_.data(), vel_.data(), 8,
+                                           individual ? mass_.data() : nullptr,
+                                           individual ? 0.0 : info_.mass, ids_.data()),
+                     "lf2_particles_set_pos");
+    on_device_ = (int64_t)ids_.size();
+    pos_.clear(), vel_.clear(), ids_.clear(), mass_.clear();
+  }
+
+ private:
+  std::shared_ptr<lf2_ctx> owner_;  // released by the last of the particles and their fields
+  lf2_ctx* ctx_ = nullptr;
+  Lattice* lat_ = nullptr;
+  part_info info_{};
+  double box_[3] = {1, 1, 1};
+  Real res_ = 1;
+  int64_t on_device_ = 0;
+  std::vector<double> pos_, vel_;
+  std::vector<int64_t> ids_;
+  std::vector<float> mass_;
+};
+
+// -------------------------------------------------------------- projections
+// projection_init (projections.hpp:31-34): the GPU deposits overwrite the
+// field, so nothing is needed here.
+inline void projection_init(Field<Real>*) {}
+
+template <class part, class part_info, class part_dataType>
+void scalarProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* rho,
+                                 size_t* oset = NULL, int flag_where = FROM_INFO)
+{
+  (void)oset;
+  if (flag_where == FROM_PART && !lf2detail::has_mass<part>::value)
+    throw std::invalid_argument("scalarProjectionCIC_project: the particle type has no mass member");
+  parts->check_field(rho, "scalarProjectionCIC_project");
+  const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
+  lf2_ctx* ctx = owner.get();
+  lf2detail::check(ctx, lf2_deposit_scalar(ctx, rho->lf2_handle(owner, false)), "lf2_deposit_scalar");
+  rho->mark_device_written();
+}
+
+template <class part, class part_info, class part_dataType>
+void vectorProjectionCICNGP_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* vel,
+                                    size_t* oset = NULL, int flag_where = FROM_INFO)
+{
+  (void)oset, (void)flag_where;
+  parts->check_field(vel, "vectorProjectionCICNGP_project");
+  const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
+  lf2_ctx* ctx = owner.get();
+  lf2detail::check(ctx, lf2_deposit_vector_cicngp(ctx, vel->lf2_handle(owner, false)),
+                   "lf2_deposit_vector_cicngp");
+  vel->mark_device_written();
+}
+
+template <class part, class part_info, class part_dataType>
+void symtensorProjectionCICNGP_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* Tij,
+                                       size_t* oset = NULL, int flag_where = FROM_INFO)
+{
+  (void)oset, (void)flag_where;
+  parts->check_field(Tij, "symtensorProjectionCICNGP_project");
+  const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
+  lf2_ctx* ctx = owner.get();
+  lf2detail::check(ctx, lf2_deposit_symtensor_cicngp(ctx, Tij->lf2_handle(owner, false)),
+                   "lf2_deposit_symtensor_cicngp");
+  Tij->mark_device_written();
+}
+
+// The *_comm functions (projections.hpp:194-300, :558-681, :856-976): the
+// periodic fold is part of the GPU deposit; here the result comes back to
+// the host array (with its halo filled).
+inline void scalarProjectionCIC_comm(Field<Real>* rho) { rho->pull(); }
+inline void vectorProjectionCICNGP_comm(Field<Real>* vel) { vel->pull(); }
+inline void symtensorProjectionCICNGP_comm(Field<Real>* Tij) { Tij->pull(); }
+
+}  // namespace LATfield2
+
+#endif  // LATFIELD2_B200_HPP

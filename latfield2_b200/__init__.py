@@ -2,8 +2,9 @@
 
 CIC deposit (scalar, vector CIC-NGP, symmetric-tensor CIC-NGP), CIC gather
 with kick, drift and rebin of brick-binned particles, written as CUDA kernels
-behind the C ABI in include/lf2gpu.h.  `latfield2_b200.particles` mirrors the
-reference's Particles / Field / projection interface on top of that ABI.
+behind the C ABI in include/lf2gpu.h.  `Context` and `FieldHandle` are the
+Python binding of that ABI; include/latfield2_b200.hpp gives C++ code the
+reference's Lattice / Field / Particles / projection names over it.
 """
 from ._lib import (DEPOSIT_FIXED64, DEPOSIT_FP32, LF2Error, library_path, load)  # noqa: F401
 from .core import Context, FieldHandle  # noqa: F401

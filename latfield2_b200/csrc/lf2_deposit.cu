@@ -27,7 +27,10 @@ namespace lf2 {
 
 namespace {
 
-constexpr int DEP_THREADS = 256;
+#ifndef LF2_DEP_THREADS
+#define LF2_DEP_THREADS 256
+#endif
+constexpr int DEP_THREADS = LF2_DEP_THREADS;
 
 template <int KIND>
 struct Comps;
