@@ -219,6 +219,76 @@ def _cpu_worker(seconds, n, npart, seed):
     return npart * steps / dt, steps
 
 
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "lf2_ref_driver_double")
+
+
+def _ref_grid(cores):
+    """Largest power-of-two process grid g0 x g1 (both >= 2) with at most
+    `cores` ranks (the MPI stand-in forks up to 64)."""
+    best = None
+    for g0 in (2, 4, 8):
+        for g1 in (2, 4, 8):
+            if g0 * g1 <= min(cores, 64) and (best is None or g0 * g1 > best[0] * best[1]):
+                best = (g0, g1)
+    return best
+
+
+def _ref_run(inp, grid, steps, timeout):
+    """One run of the reference driver's timing mode; its ranks form their own
+    process group, stopped as a whole on a timeout."""
+    import signal
+    import subprocess
+    env = dict(os.environ, LF2_MINIMPI_NP=str(grid[0] * grid[1]), LF2_REF_STEPS=str(steps))
+    p = subprocess.Popen([REF_DRIVER, inp, inp + ".out"], env=env, stdin=subprocess.DEVNULL,
+                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, start_new_session=True)
+    try:
+        out, _ = p.communicate(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, signal.SIGKILL)
+        p.wait()
+        return None
+    if p.returncode != 0:
+        return None
+    for line in out.decode().splitlines():
+        if line.startswith("{"):
+            return json.loads(line)
+    return None
+
+
+def cpu_baseline_reference(seconds, cores, n=64, npart=64 ** 3):
+    """The reference's own particle path (its headers compiled by
+    oracle/build_ref.sh, double) on a bounded sample: a 64^3 lattice with
+    262,144 uniform particles, K steps of scalarProjectionCIC_project + _comm,
+    updateVel with the CIC kick and moveParticles, on a g0 x g1 process grid
+    of forked ranks.  K is chosen for about `seconds` of work.  Returns
+    (updates/s, steps, ranks) or None when the driver or 4 cores are not
+    there."""
+    import tempfile
+    import numpy as np
+    grid = _ref_grid(cores)
+    if grid is None or not os.access(REF_DRIVER, os.X_OK):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden as G
+    rng = np.random.default_rng(1)
+    pos = rng.random((npart, 3))
+    vel = 0.01 * rng.standard_normal((npart, 3))
+    F = 0.01 * rng.standard_normal((n, n, n, 3))
+    ids = np.arange(npart, dtype=np.int64)
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.bin")
+        G.write_input(inp, n, 1, grid, 1.0 / npart, G.OP_SCALAR | G.OP_KICK | G.OP_MOVE, 0.1, 0.1,
+                      ids, pos, vel, F)
+        probe = _ref_run(inp, grid, 5, 300)
+        if probe is None:
+            return None
+        steps = max(5, min(5000, int(5 * seconds / max(probe["seconds"], 1e-6))))
+        r = _ref_run(inp, grid, steps, 20 * seconds + 120)
+        if r is None:
+            return None
+    return npart * r["steps"] / r["seconds"], r["steps"], r["ranks"]
+
+
 def adjoint_ratio(device, steps=8, reps=3):
     """Differentiable chain at 128^3 with 2,097,152 uniform particles and
     per-particle masses (1/Np)(1 + 0.1 U(-1,1)): 8 kick-drift steps of
@@ -259,11 +329,27 @@ def adjoint_ratio(device, steps=8, reps=3):
 
 
 def reference_arm(args, rank):
+    """The reference's CPU particle path on the host cores (rank 0 only): its
+    own code compiled from its headers when oracle/_ref is there, else the C
+    restatement of it (oracle/, one process per core)."""
     if rank != 0:
         return
-    procs = os.cpu_count() or 1
     t0 = time.perf_counter()
-    ups, steps = cpu_baseline_port(args.cpu_seconds, procs=procs)
+    cores = os.cpu_count() or 1
+    ref = cpu_baseline_reference(args.cpu_seconds, cores)
+    if ref is not None:
+        ups, steps, used = ref
+        kind = "reference"
+        sample = (f"{used} ranks ({_ref_grid(cores)[0]}x{_ref_grid(cores)[1]} process grid, forked "
+                  f"MPI stand-in) x 64^3 lattice, 262,144 uniform particles, {steps} steps of "
+                  "scalarProjectionCIC_project+_comm, updateVel CIC kick, moveParticles "
+                  "(the reference's own headers, double)")
+    else:
+        used = cores
+        ups, steps = cpu_baseline_port(args.cpu_seconds, procs=cores)
+        kind = "port"
+        sample = (f"{cores} processes x 64^3 lattice, 262,144 uniform particles, {steps} steps of "
+                  "deposit+comm, updateVel CIC kick, move (CPU restatement of the reference, double)")
     wall = time.perf_counter() - t0
     w = WORKLOADS[args.workload]
     line = {
@@ -272,10 +358,7 @@ def reference_arm(args, rank):
         "ms_per_step": 1e3 * w["npart"] / ups, "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": {"workload": args.workload, "lattice": w["n"],
                                         "particles": w["npart"]},
-        "cpu_baseline": {"value": ups, "unit": UNIT, "cores": procs, "kind": "port",
-                         "sample": f"{procs} processes x 64^3 lattice, 262,144 uniform particles, "
-                                   f"{steps} steps of deposit+comm, updateVel CIC kick, move "
-                                   f"(CPU restatement of the reference, double)"},
+        "cpu_baseline": {"value": ups, "unit": UNIT, "cores": used, "kind": kind, "sample": sample},
         "e2e": {"value": ups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": wall,
     }
@@ -449,11 +532,20 @@ def main():
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            ups, steps = cpu_baseline_port(args.cpu_seconds, procs=1)
-            cpu = {"value": ups, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"64^3 lattice, 262,144 uniform particles, {steps} steps of "
-                             "deposit+comm, updateVel CIC kick, move (CPU restatement of the "
-                             "reference, double, 1 thread)"}
+            ref = cpu_baseline_reference(args.cpu_seconds, 4)
+            if ref is not None:
+                ups, steps, used = ref
+                cpu = {"value": ups, "unit": UNIT, "cores": used, "kind": "reference",
+                       "sample": f"{used} ranks (2x2 process grid) x 64^3 lattice, 262,144 uniform "
+                                 f"particles, {steps} steps of scalarProjectionCIC_project+_comm, "
+                                 "updateVel CIC kick, moveParticles (the reference's own headers, "
+                                 "double)"}
+            else:
+                ups, steps = cpu_baseline_port(args.cpu_seconds, procs=1)
+                cpu = {"value": ups, "unit": UNIT, "cores": 1, "kind": "port",
+                       "sample": f"64^3 lattice, 262,144 uniform particles, {steps} steps of "
+                                 "deposit+comm, updateVel CIC kick, move (CPU restatement of the "
+                                 "reference, double, 1 thread)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,

@@ -26,6 +26,7 @@
 //        int64 nloc, nloc x {id, pos[3], vel[3]}; for the move: int64 nloc,
 //        nloc x {id, pos[3], vel[3]}.
 #include <cstdint>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -195,6 +196,33 @@ int main(int argc, char** argv)
     F.updateHalo();
   }
   fclose(in);
+
+  // Timing mode (LF2_REF_STEPS=K): K particle-mesh steps of the reference as
+  // a user's loop runs them -- scalarProjectionCIC_project + _comm, updateVel
+  // with the CIC kick, moveParticles -- between two barriers; rank 0 prints
+  // the wall time as one JSON line.  Nothing is written.
+  if (const char* ks = getenv("LF2_REF_STEPS")) {
+    const int steps = atoi(ks);
+    Field<Real> rho(lat, 1);
+    Field<Real>* fl[1] = {&F};
+    double out1[1];
+    int red[1] = {SUM};
+    parallel.barrier();
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int s = 0; s < steps; s++) {
+      projection_init(&rho);
+      scalarProjectionCIC_project(&parts, &rho);
+      scalarProjectionCIC_comm(&rho);
+      parts.updateVel(&cic_kick, dtk, fl, 1, NULL, out1, red, 1);
+      parts.moveParticles(&move_particles_simple, dtm);
+    }
+    parallel.barrier();
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (parallel.rank() == 0)
+      printf("{\"seconds\": %.6f, \"steps\": %d, \"particles\": %lld, \"ranks\": %d}\n", sec, steps,
+             (long long)np, g0 * g1);
+    return 0;
+  }
 
   const std::string out_name = std::string(argv[2]) + "." + std::to_string(parallel.rank());
   FILE* o = fopen(out_name.c_str(), "wb");

@@ -53,3 +53,18 @@ def test_replica_throughput_one_rank():
     import bench
     ms, value = bench.replica_throughput(20.0, 500, 4)
     assert ms == 20.0 and value == pytest.approx(500 * 4 / 0.020)
+
+
+def test_reference_cpu_baseline_runs_the_reference():
+    """The CPU baseline runs the reference's own particle path (compiled from
+    its headers into oracle/_ref by oracle/build_ref.sh) on a 2x2 grid of
+    forked ranks; without that build the bench falls back to the port."""
+    import bench
+    if not os.access(bench.REF_DRIVER, os.X_OK):
+        pytest.skip("oracle/_ref not built (the reference sources are absent)")
+    assert bench._ref_grid(4) == (2, 2) and bench._ref_grid(3) is None
+    assert bench._ref_grid(200) == (8, 8)
+    r = bench.cpu_baseline_reference(0.5, 4)
+    assert r is not None
+    ups, steps, ranks = r
+    assert ranks == 4 and steps >= 5 and ups > 0
