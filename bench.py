@@ -448,6 +448,7 @@ def main():
     ctx.profile_read()
     ctx.profile(True)
     l0 = ctx.kernel_launches()
+    rb0 = ctx.rebin_stats()
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -460,6 +461,9 @@ def main():
         torch.cuda.synchronize()
         barrier()
     launches = ctx.kernel_launches() - l0
+    rb1 = ctx.rebin_stats()
+    rebin = {"repacks": rb1[0] - rb0[0], "relocations": rb1[1] - rb0[1],
+             "movers_last_step": rb1[2]}
     ctx.synchronize()  # raises if a kernel flagged an error
     ms = e0.elapsed_time(e1)
     phases = ctx.profile_read()
@@ -561,7 +565,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
-            "fixed_vs_fp32": fixed_vs_fp32,
+            "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

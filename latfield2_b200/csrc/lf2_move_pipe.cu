@@ -501,6 +501,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           if (has_id) id[j] = cv.id[i0 + j];
         }
       }
+      // The buffer is refilled by a bulk copy (async proxy) once every warp
+      // has released it: order this warp's reads (generic proxy) before that.
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty_p[ps]);  // this warp's slots are read
 
@@ -601,6 +604,10 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     }
 
     for (int o = 16; o > 0; o >>= 1) maxv2 = fmaxf(maxv2, __shfl_xor_sync(0xffffffffu, maxv2, o));
+    // likewise for the tile: the next tile copy into this buffer follows
+    // this warp's last read of it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
     if (lane == 0) {
       atomicMax(&s_maxv2[fs], __float_as_uint(maxv2));  // non-negative floats order as integers
       __threadfence_block();
