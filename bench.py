@@ -24,6 +24,7 @@ Multi-GPU (torchrun): every rank advances its own replica of the workload
 (weak scaling, no collective on the data path); time is the max over ranks.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -53,7 +54,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -366,6 +367,81 @@ def reference_arm(args, rank):
 
 
 # ------------------------------------------------------------------- ours
+def e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, steps, pg, device, barrier):
+    """Particle updates/s with the force field uploaded from pinned host memory
+    and the density and max |v| downloaded to pinned host memory every step.
+    Three streams: host->device copies of the next step's input, the step
+    (lf2_field_import from the device copy, lf2_step, lf2_field_export to a
+    device buffer, lf2_last_max_velocity), device->host copies of the
+    result."""
+    import numpy as np
+    import torch
+    from latfield2_b200 import _lib
+    lib = _lib.load()
+    Fref = np.ascontiguousarray(F.cpu().numpy().reshape(3, n[2], n[1], n[0]).transpose(1, 2, 3, 0))
+    Fpin = torch.from_numpy(Fref).reshape(-1).pin_memory()  # reference layout (z, y, x, c)
+    s_cmp, s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ctx.synchronize()
+    ctx.set_stream(s_cmp.cuda_stream)
+    Fd = [Fh, ctx.field(3)]
+    Fin = [torch.empty(3 * nsites, device=device) for _ in range(2)]
+    rho_dev = [torch.empty(nsites, device=device) for _ in range(2)]
+    mv_dev = [torch.empty(1, dtype=torch.float64, device=device) for _ in range(2)]
+    rho_pin = [torch.empty(nsites).pin_memory() for _ in range(2)]
+    mv_pin = [torch.empty(1, dtype=torch.float64).pin_memory() for _ in range(2)]
+    ev = {k: [torch.cuda.Event() for _ in range(2)] for k in ("in", "used", "res", "host")}
+
+    def upload(k):
+        b = k % 2
+        if k >= 2:
+            s_in.wait_event(ev["used"][b])  # step k-2 has read its input buffer
+        with torch.cuda.stream(s_in):
+            Fin[b].copy_(Fpin, non_blocking=True)
+        ev["in"][b].record(s_in)
+
+    def run(k):
+        b = k % 2
+        s_cmp.wait_event(ev["in"][b])
+        if k >= 2:
+            s_cmp.wait_event(ev["host"][b])  # step k-2's result has left the device buffer
+        _lib.check(ctx.h, lib.lf2_field_import(ctx.h, Fd[b].h, ctypes.c_void_p(Fin[b].data_ptr()), 0, 4,
+                                               _lib.PTR_DEVICE), "import")
+        ev["used"][b].record(s_cmp)
+        ctx.step(Fd[b], dtau, dtau, rho)
+        _lib.check(ctx.h, lib.lf2_field_export(ctx.h, rho.h, ctypes.c_void_p(rho_dev[b].data_ptr()), 0, 4, 0,
+                                               _lib.PTR_DEVICE), "export")
+        ctx.last_max_velocity(mv_dev[b])
+        ev["res"][b].record(s_cmp)
+        s_out.wait_event(ev["res"][b])
+        with torch.cuda.stream(s_out):
+            rho_pin[b].copy_(rho_dev[b], non_blocking=True)
+            mv_pin[b].copy_(mv_dev[b], non_blocking=True)
+        ev["host"][b].record(s_out)
+
+    def loop(k_steps):
+        upload(0)
+        for k in range(k_steps):
+            if k + 1 < k_steps:
+                upload(k + 1)
+            run(k)
+        torch.cuda.synchronize()
+
+    loop(2)  # warm-up: allocations and first copies
+    barrier()
+    t0 = time.perf_counter()
+    loop(steps)
+    t = time.perf_counter() - t0
+    ctx.set_stream(None)
+    assert np.isfinite(float(mv_pin[(steps - 1) % 2][0]))
+    ms, value = replica_throughput(1e3 * t, npart, steps, pg, device)
+    return {"value": value, "unit": UNIT, "h2d_bytes_per_step": 3 * nsites * 4,
+            "d2h_bytes_per_step": nsites * 4 + 8, "ms_per_step": ms / steps, "steps": steps,
+            "path": "per step: pinned host F -> device (copy stream), lf2_field_import + lf2_step + "
+                    "lf2_field_export + lf2_last_max_velocity (compute stream), rho and max|v| -> "
+                    "pinned host (copy stream); copies of step k+1's input and step k's result "
+                    "overlap step k"}
+
+
 def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
     """Device time per lf2_step of the same particles with FP32 atomic
     deposits (CUDA events on the launching stream)."""
@@ -491,33 +567,12 @@ def main():
                      "frac": step_ab / (ms_step / 1e3) / 1e9 / peak}
     phase_ms = {k: v[0] / args.steps for k, v in phases.items()}
 
-    # end to end through the C ABI with host buffers: the force field comes
-    # from pinned host memory, the density and max |v| go back to the host
-    Fhost = F.cpu().pin_memory()
-    rho_host = torch.empty(nsites, dtype=torch.float32).pin_memory()
-    Fnp = Fhost.numpy().reshape(3, n[2], n[1], n[0]).transpose(1, 2, 3, 0)
-    Fref = np.ascontiguousarray(Fnp)  # reference layout (z, y, x, c), halo 0
-    Fpin = torch.from_numpy(Fref).pin_memory()
-    Fpin_np = Fpin.numpy()
-    rho_np = rho_host.numpy().reshape(n[2], n[1], n[0], 1)
-    ctx.step(Fh, dtau, dtau, rho)
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        Fh.import_(Fpin_np, halo=0)
-        ctx.step(Fh, dtau, dtau, rho)
-        _export_into(rho, rho_np)
-        ctx.gather_kick(Fh, 0.0, want_max_v=True)
-    torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    t_e2e_ms, e2e_value = replica_throughput(1e3 * t_e2e, npart, args.e2e_steps, pg, device)
-    t_e2e = t_e2e_ms / 1e3
-    e2e = {"value": e2e_value, "unit": UNIT,
-           "h2d_bytes_per_step": 3 * nsites * 4, "d2h_bytes_per_step": nsites * 4 + 8,
-           "ms_per_step": 1e3 * t_e2e / args.e2e_steps, "steps": args.e2e_steps,
-           "path": "lf2_field_import(F, host) + lf2_step + lf2_field_export(rho, host) + "
-                   "lf2_gather_kick(max_v)"}
+    # End to end through the C ABI with host buffers: every step the force
+    # field comes from pinned host memory (the reference layout) and the
+    # density and max |v| go back to pinned host memory.  The copies of step
+    # k+1's input and of step k's result run on their own streams while step
+    # k computes (two buffers each way).
+    e2e = e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, args.e2e_steps, pg, device, barrier)
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
 
@@ -571,15 +626,6 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
-
-
-def _export_into(field, out):
-    """lf2_field_export straight into a pinned host array."""
-    from latfield2_b200 import _lib
-    from latfield2_b200.core import _ptr
-    p, kind = _ptr(out)
-    _lib.check(field.ctx.h, _lib.load().lf2_field_export(field.ctx.h, field.h, p, 0, 4, 0, kind),
-               "export")
 
 
 if __name__ == "__main__":

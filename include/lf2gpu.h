@@ -74,6 +74,8 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3],
                       const double box[3], int deposit_mode, void* stream);
 lf2_status lf2_destroy(lf2_ctx* ctx);
 const char* lf2_last_error(const lf2_ctx* ctx);
+/* Later calls run on `stream`.  Work already queued on the previous stream
+ * is not waited for: order it first (lf2_synchronize, or an event). */
 lf2_status lf2_set_stream(lf2_ctx* ctx, void* stream);
 /* Waits for the context's stream and turns raised device flags into
  * LF2_ERR_STATE. */
@@ -182,6 +184,12 @@ lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
 /* Kernel the last lf2_step used for its kick-drift-rebin pass: 1 per-brick,
  * 2 pipelined, 0 before the first step. */
 lf2_status lf2_last_move_kernel(lf2_ctx* ctx, int* which);
+/* max |v| after the last kick (lf2_step or lf2_gather_kick): the value
+ * updateVel returns (LATfield2_Particles.hpp:870-893), from the per-brick
+ * maxima the kick already computed.  ptr_kind LF2_PTR_HOST: waits and writes
+ * *max_v; LF2_PTR_DEVICE: max_v is device memory, written in stream order
+ * without waiting. */
+lf2_status lf2_last_max_velocity(lf2_ctx* ctx, double* max_v, int ptr_kind);
 /* FP64 conservation sums over all particles: total mass, momentum sum m v
  * and max |v| (cout_particle_velocity_stats, LATfield2_Particles.hpp:
  * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */

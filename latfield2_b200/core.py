@@ -217,6 +217,19 @@ class Context:
         2 persistent TMA-pipelined."""
         self._check(_lib.load().lf2_set_move_kernel(self.h, int(which)), "set_move_kernel")
 
+    def last_max_velocity(self, out=None):
+        """max |v| after the last kick.  With a CUDA float64 tensor `out` the
+        value is written there in stream order (no wait); otherwise it is
+        returned."""
+        if out is not None:
+            self._check(_lib.load().lf2_last_max_velocity(self.h, _c.c_void_p(out.data_ptr()),
+                                                          _lib.PTR_DEVICE), "last_max_velocity")
+            return out
+        v = _c.c_double()
+        self._check(_lib.load().lf2_last_max_velocity(self.h, _c.byref(v), _lib.PTR_HOST),
+                    "last_max_velocity")
+        return v.value
+
     def last_move_kernel(self):
         """Kernel of the last step's kick-drift-rebin pass: 1 per-brick,
         2 pipelined, 0 before the first step."""

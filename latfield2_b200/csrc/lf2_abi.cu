@@ -749,6 +749,20 @@ lf2_status lf2_set_move_kernel(lf2_ctx* c, int which)
   return LF2_OK;
 }
 
+lf2_status lf2_last_max_velocity(lf2_ctx* c, double* max_v, int ptr_kind)
+{
+  if (!c || !max_v || (ptr_kind != LF2_PTR_HOST && ptr_kind != LF2_PTR_DEVICE)) return LF2_ERR_ARG;
+  if (ptr_kind == LF2_PTR_DEVICE) {
+    LF2_CUDA(c, launch_maxv_to_device(c, max_v));
+    return LF2_OK;
+  }
+  LF2_CUDA(c, launch_reduce_maxv(c));
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  *max_v = std::sqrt(c->h_stats[0]);
+  return LF2_OK;
+}
+
 lf2_status lf2_last_move_kernel(lf2_ctx* c, int* which)
 {
   if (!c || !which) return LF2_ERR_ARG;

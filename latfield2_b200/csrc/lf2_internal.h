@@ -149,6 +149,7 @@ cudaError_t launch_heap_reset(lf2_ctx* c);
 cudaError_t launch_move(lf2_ctx* c, const float* F, bool kick, bool drift, MoveParams mp);
 cudaError_t launch_insert(lf2_ctx* c);
 cudaError_t launch_reduce_maxv(lf2_ctx* c);
+cudaError_t launch_maxv_to_device(lf2_ctx* c, double* dst);
 
 // lf2_move_pipe.cu
 bool move_pipe_eligible(const lf2_ctx* c, const float* F);

@@ -407,4 +407,17 @@ cudaError_t launch_reduce_maxv(lf2_ctx* c)
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_sqrt_to(double* dst, const double* src) { *dst = sqrt(*src); }
+}  // namespace
+
+cudaError_t launch_maxv_to_device(lf2_ctx* c, double* dst)
+{
+  cudaError_t e = launch_reduce_maxv(c);
+  if (e != cudaSuccess) return e;
+  c->launches += 1;
+  k_sqrt_to<<<1, 1, 0, c->stream>>>(dst, c->stats);
+  return cudaGetLastError();
+}
+
 }  // namespace lf2

@@ -443,3 +443,25 @@ def test_medium_lattice_mass_and_properties(cuda, mode):
     ref = O.state_deposit_f64(n, cell.cpu().numpy(), off.cpu().numpy(), res, gmass=1.0 / (1 << 21))
     assert normalized_error(got.reshape(-1), ref) < (1e-6 if mode == 1 else 1e-5)
     assert mean_relative_error(got.reshape(-1), ref) < (1e-5 if mode == 1 else 1e-4)
+
+
+def test_last_max_velocity_matches_the_kick(cuda):
+    """lf2_last_max_velocity after lf2_step equals what lf2_gather_kick with
+    dtau 0 returns on the same particles (the same per-brick maxima), on the
+    host path and, written in stream order, on the device path."""
+    import torch
+    n = (64, 64, 64)
+    cell, off, vel = small_case(n, 120000, seed=41, vel_sigma=0.03)
+    F = np.random.default_rng(4).standard_normal((3, 64, 64, 64)).astype(np.float32)
+    ctx = _ctx(n, 1)
+    _load(ctx, cell, off, vel, 1.0 / 120000)
+    Fh = ctx.field(3, torch.from_numpy(F).cuda())
+    rho = ctx.field(1)
+    ctx.step(Fh, 0.05, 0.2, rho)
+    host = ctx.last_max_velocity()
+    dev = ctx.last_max_velocity(torch.zeros(1, dtype=torch.float64, device="cuda"))
+    torch.cuda.synchronize()
+    assert float(dev[0]) == host
+    assert ctx.gather_kick(Fh, 0.0, want_max_v=True) == host
+    v = ctx.get_particles()["vel"].astype(np.float64)
+    assert host == pytest.approx(float(np.sqrt((v ** 2).sum(1).max())), rel=1e-6)
