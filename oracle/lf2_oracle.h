@@ -58,6 +58,14 @@ extern "C" {
         const int64_t* cell_start, const R* pos, const R* vel,                 \
         const double* pmass, double gmass, R* t);                              \
   void lf2o_symtensor_cicngp_comm_##S(R* t, const int n[3], int halo);        \
+  void lf2o_vector_cic_project_##S(const int n[3], int halo, R res,            \
+        const int64_t* cell_start, const R* pos, const R* vel,                 \
+        const double* pmass, double gmass, R* v);                              \
+  void lf2o_vector_cic_comm_##S(R* v, const int n[3], int halo);              \
+  void lf2o_vecvec_cic_project_##S(const int n[3], int halo, R res,            \
+        const int64_t* cell_start, const R* pos, const R* vel,                 \
+        const double* pmass, double gmass, R* t);                              \
+  void lf2o_vecvec_cic_comm_##S(R* t, const int n[3], int halo);              \
   void lf2o_update_halo_##S(R* f, const int n[3], int halo, int comps);       \
   double lf2o_update_vel_cic_##S(const int n[3], int halo,                     \
         const int64_t* cell_start, const R* pos, R* vel, const R* F,           \

@@ -135,6 +135,32 @@ def symtensor_cicngp(n, halo, res, cs, pos, vel, pmass=None, gmass=0.0, prec="d"
     return t
 
 
+def _full_cic(name, comps, n, halo, res, cs, pos, vel, pmass, gmass, prec, comm):
+    dt, ct, s = _real(prec)
+    f = projection_init(n, halo, comps, prec)
+    pos = np.ascontiguousarray(pos, dt)
+    vel = np.ascontiguousarray(vel, dt)
+    pm = None if pmass is None else np.ascontiguousarray(pmass, np.float64)
+    L = lib()
+    getattr(L, f"lf2o_{name}_project_{s}")(_n3(n), _i(halo), ct(res), _p(cs), _p(pos), _p(vel),
+                                           _p(pm), _d(gmass), _p(f))
+    if comm:
+        getattr(L, f"lf2o_{name}_comm_{s}")(_p(f), _n3(n), _i(halo))
+    return f
+
+
+def vector_cic(n, halo, res, cs, pos, vel, pmass=None, gmass=0.0, prec="d", comm=True):
+    """projection_init + vectorProjectionCIC_project (+ _comm): m v / res^3 on
+    the links, staggered CIC along each component's own dim."""
+    return _full_cic("vector_cic", 3, n, halo, res, cs, pos, vel, pmass, gmass, prec, comm)
+
+
+def vecvec_cic(n, halo, res, cs, pos, vel, pmass=None, gmass=0.0, prec="d", comm=True):
+    """projection_init + VecVecProjectionCIC_project (+ _comm): symmetric
+    m v_i v_j / res^3, components 00,01,02,11,12,22."""
+    return _full_cic("vecvec_cic", 6, n, halo, res, cs, pos, vel, pmass, gmass, prec, comm)
+
+
 def update_halo(f, n, halo, prec="d"):
     """Field::updateHalo on a reference-layout array (in place)."""
     _, _, s = _real(prec)

@@ -7,7 +7,8 @@
 // them, both outside the reference sources:
 //  - a partList<part_simple> specialisation that also answers `.size != 0`:
 //    vectorProjectionCICNGP_project and symtensorProjectionCICNGP_project
-//    test `parts->field()(xPart).size != 0` (projections.hpp:473, :761), a
+//    test `parts->field()(xPart).size != 0` (projections.hpp:473, :761,
+//    :1038, :1414), a
 //    member the shipped partList no longer has (LATfield2_Particles.hpp:
 //    97-103); here it means "the list is not empty", the intent of the test;
 //  - the CIC gather-kick callback for updateVel (the reference ships only the
@@ -21,10 +22,12 @@
 //        if ops & OP_KICK: n^3 x 3 doubles, the force field F[z][y][x][c].
 // Output (one file per rank, <prefix>.<rank>): int32 rank, int32 coordSkip0
 //        (z offset), int32 coordSkip1 (y offset), int32 sizeLocal[3], int32 halo,
-//        then per op in bit order: the local gross field (double) for each
-//        deposit and for the halo-filled F; for the kick: double max_v,
+//        then the local gross field (double) of each requested deposit in the
+//        order scalar, vector CIC-NGP, symtensor CIC-NGP, vector CIC,
+//        VecVec CIC, then the halo-filled F; for the kick: double max_v,
 //        int64 nloc, nloc x {id, pos[3], vel[3]}; for the move: int64 nloc,
-//        nloc x {id, pos[3], vel[3]}.
+//        nloc x {id, pos[3], vel[3]}.  The vector-CIC and VecVec-CIC folds
+//        (sendUpDown) need a process grid of at least 2x2.
 #include <cstdint>
 #include <chrono>
 #include <cstdio>
@@ -54,7 +57,16 @@ struct partList<part_simple> {
 };
 }  // namespace LATfield2
 
-enum { OP_SCALAR = 1, OP_VECTOR = 2, OP_TENSOR = 4, OP_HALO = 8, OP_KICK = 16, OP_MOVE = 32 };
+enum {
+  OP_SCALAR = 1,
+  OP_VECTOR = 2,
+  OP_TENSOR = 4,
+  OP_HALO = 8,
+  OP_KICK = 16,
+  OP_MOVE = 32,
+  OP_VECCIC = 64,
+  OP_VECVEC = 128
+};
 
 // CIC gather of the 3-component field at the cell corners and kick, in the
 // callback signature of Particles::updateVel (LATfield2_Particles.hpp:753).
@@ -258,6 +270,20 @@ int main(int argc, char** argv)
     projection_init(&T);
     symtensorProjectionCICNGP_project(&parts, &T);
     symtensorProjectionCICNGP_comm(&T);
+    write_field(o, T);
+  }
+  if (ops & OP_VECCIC) {
+    Field<Real> V(lat, 3);
+    projection_init(&V);
+    vectorProjectionCIC_project(&parts, &V);
+    vectorProjectionCIC_comm(&V);
+    write_field(o, V);
+  }
+  if (ops & OP_VECVEC) {
+    Field<Real> T(lat, 3, 3, symmetric);
+    projection_init(&T);
+    VecVecProjectionCIC_project(&parts, &T);
+    VecVecProjectionCIC_comm(&T);
     write_field(o, T);
   }
   if (ops & OP_HALO) write_field(o, F);

@@ -8,6 +8,8 @@ Each case writes <case>_<build>.npz with the inputs (lattice, particles,
 force field, time steps) and the reference's outputs:
   rho, vec, ten     deposits after *_project + *_comm, interior sites,
                     shape (n, n, n, comps) indexed [z, y, x, c]
+  vcic, vv          vectorProjectionCIC and VecVecProjectionCIC, same form
+                    (multi-rank cases only: their halo folds need a 2x2 grid)
   F_halo            the force field after Field::updateHalo, full gross array
                     (single-rank cases only)
   maxv, kick_*      updateVel with the CIC gather-kick callback
@@ -29,6 +31,10 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref")
 
 OP_SCALAR, OP_VECTOR, OP_TENSOR, OP_HALO, OP_KICK, OP_MOVE = 1, 2, 4, 8, 16, 32
+OP_VECCIC, OP_VECVEC = 64, 128
+# fields in the order the driver writes them: (op, key, components)
+FIELD_OPS = ((OP_SCALAR, "rho", 1), (OP_VECTOR, "vec", 3), (OP_TENSOR, "ten", 6),
+             (OP_VECCIC, "vcic", 3), (OP_VECVEC, "vv", 6))
 
 CASES = [
     # name, n, halo, grid, npart, clustered, vel sigma, dtau kick, dtau move, ops
@@ -37,7 +43,9 @@ CASES = [
     ("clustered12", 12, 2, (1, 1), 2000, True, 0.2, 0.1, 0.0,
      OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_HALO | OP_KICK),
     ("ranks16", 16, 1, (2, 2), 2500, True, 0.02, 0.05, 0.6,
-     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_KICK | OP_MOVE),
+     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_VECCIC | OP_VECVEC | OP_KICK | OP_MOVE),
+    ("ranks20", 20, 2, (2, 2), 3000, True, 0.3, 0.0, 0.0,
+     OP_SCALAR | OP_VECCIC | OP_VECVEC),
 ]
 
 
@@ -96,7 +104,7 @@ def read_rank(path, n, ops, comps_of):
         off += m * 56
         return rec.copy()
 
-    for op, comps in ((OP_SCALAR, 1), (OP_VECTOR, 3), (OP_TENSOR, 6), (OP_HALO, 3)):
+    for op, _, comps in FIELD_OPS + ((OP_HALO, "F_halo", 3),):
         if ops & op:
             out[op] = field(comps)
     if ops & OP_KICK:
@@ -148,7 +156,7 @@ def run_case(name, n, halo, grid, npart, clustered, vsig, dtk, dtm, ops, build, 
                  for r in range(grid[0] * grid[1])]
     res = dict(n=n, halo=halo, grid=np.array(grid), gmass=gmass, dtau_kick=dtk, dtau_move=dtm,
                ops=ops, ids=ids, pos=pos, vel=vel, F=F)
-    for op, key, comps in ((OP_SCALAR, "rho", 1), (OP_VECTOR, "vec", 3), (OP_TENSOR, "ten", 6)):
+    for op, key, comps in FIELD_OPS:
         if ops & op:
             res[key] = assemble(ranks, n, op, comps)
     if ops & OP_HALO:

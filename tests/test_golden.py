@@ -4,8 +4,11 @@ from its sources (see tests/golden/make_golden.py).
 
 Single-rank cases must match bit for bit: the oracle restates the reference's
 arithmetic statement by statement and rebuilds its per-cell list order.  The
-2x2-rank case folds the halos through messages in a different order, so its
-deposits are compared to a tight tolerance; its moves are bit-exact.
+2x2-rank cases fold the halos through messages in a different order, so
+their deposits are compared to a tight tolerance; their moves are bit-exact.
+The full-CIC projections (vectorProjectionCIC, VecVecProjectionCIC) exist only
+in the 2x2 cases: their reference folds (sendUpDown) cannot run on a grid with
+one rank along a dim.
 """
 import glob
 import os
@@ -36,9 +39,13 @@ def ref_cells(n, posR, R):
 
 def test_fixtures_present():
     names = {os.path.basename(p) for p in CASES}
-    for case in ("uniform8", "clustered12", "ranks16"):
+    for case in ("uniform8", "clustered12", "ranks16", "ranks20"):
         for b in ("double", "single"):
             assert f"{case}_{b}.npz" in names
+    for b in ("double", "single"):
+        for case in ("ranks16", "ranks20"):
+            g = load(os.path.join(HERE, f"{case}_{b}.npz"))
+            assert "vcic" in g and "vv" in g
 
 
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
@@ -58,7 +65,8 @@ def test_oracle_matches_reference(path):
     pos_l, vel_l, ids_l = posR[order], velR[order].copy(), ids[order]
 
     tol = 0.0 if single_rank else (1e-13 if prec == "d" else 1e-6)
-    for key, fn in (("rho", O.scalar_cic), ("vec", O.vector_cicngp), ("ten", O.symtensor_cicngp)):
+    for key, fn in (("rho", O.scalar_cic), ("vec", O.vector_cicngp), ("ten", O.symtensor_cicngp),
+                    ("vcic", O.vector_cic), ("vv", O.vecvec_cic)):
         if key not in g:
             continue
         if key == "rho":
@@ -100,6 +108,27 @@ def test_oracle_matches_reference(path):
         np.testing.assert_array_equal(g["move_id"], np.sort(ids))
         np.testing.assert_array_equal(p.astype(np.float64), g["move_pos"])
         np.testing.assert_array_equal(v.astype(np.float64), g["move_vel"])
+
+
+def test_full_cic_projections_conserve_momentum_and_stress():
+    """Sum over sites of the vector-CIC field is the total momentum m sum v /
+    res^3 and of the VecVec field the total m sum v_i v_j / res^3: the
+    staggered weights of a particle sum to one along every dim."""
+    for path in CASES:
+        g = load(path)
+        if "vcic" not in g:
+            continue
+        n = int(g["n"])
+        tol = 1e-12 if path.endswith("_double.npz") else 1e-4
+        scale = float(g["gmass"]) * n ** 3
+        v = g["vel"]
+        mom = scale * v.sum(axis=0)
+        np.testing.assert_allclose(g["vcic"].reshape(-1, 3).sum(axis=0), mom,
+                                   rtol=tol, atol=tol * np.abs(mom).max())
+        pairs = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+        want = np.array([scale * (v[:, i] * v[:, j]).sum() for i, j in pairs])
+        np.testing.assert_allclose(g["vv"].reshape(-1, 6).sum(axis=0), want,
+                                   rtol=tol, atol=tol * np.abs(want).max())
 
 
 def test_reference_conserves_mass_in_every_fixture():
