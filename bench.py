@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-projections", action="store_true",
+                    help="skip timing the full-CIC vector and VecVec projections")
     ap.add_argument("--no-fp32", action="store_true",
                     help="skip the FP32-mode run of the same particles (fixed-point workloads)")
     return ap.parse_args()
@@ -442,6 +444,38 @@ def e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, steps, pg, device, ba
                     "overlap step k"}
 
 
+def full_cic_projections(ctx, npart, nsites, peak, reps=5):
+    """vectorProjectionCIC and VecVecProjectionCIC of the bench's particles
+    (after the timed steps): mean over `reps` deposits after one warm-up call,
+    tile pass and boundary fix-up timed by the library's phase events.
+    Algorithmic bytes: each particle's key, offsets and velocities read once
+    (28 B), the field written once (4 B per component and site); the inputs
+    are larger than L2."""
+    out = {}
+    for name, comps in (("vector_cic", 3), ("vecvec_cic", 6)):
+        f = ctx.field(comps)
+        dep = getattr(ctx, "deposit_" + name)
+        dep(f)
+        ctx.synchronize()
+        ctx.profile_read()
+        ctx.profile(True)
+        for _ in range(reps):
+            dep(f)
+        ctx.synchronize()
+        ph = ctx.profile_read()
+        ctx.profile(False)
+        tile = ph["deposit_tile"][0] / reps
+        fix = ph["deposit_fixup"][0] / reps
+        ms = tile + fix
+        ab = npart * 28 + nsites * 4 * comps
+        out[name] = {"ms": ms, "tile_ms": tile, "fixup_ms": fix,
+                     "particle_deposits_per_s": npart / (ms / 1e3), "alg_bytes": ab,
+                     "achieved_gbs": ab / (ms / 1e3) / 1e9,
+                     "frac_of_hbm": ab / (ms / 1e3) / 1e9 / peak}
+        del f
+    return out
+
+
 def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
     """Device time per lf2_step of the same particles with FP32 atomic
     deposits (CUDA events on the launching stream)."""
@@ -574,6 +608,8 @@ def main():
     # k computes (two buffers each way).
     e2e = e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, args.e2e_steps, pg, device, barrier)
 
+    proj = None if args.no_projections else full_cic_projections(ctx, npart, nsites, peak)
+
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
 
     # the same particles and steps with FP32 atomic deposits
@@ -620,7 +656,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
-            "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin,
+            "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin, "projections": proj,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

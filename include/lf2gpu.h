@@ -154,10 +154,22 @@ lf2_status lf2_halo_fill(lf2_ctx* ctx, void* data, int comps, int halo,
  *            CIC across).  FP32 mode.
  *   tensor : symtensorProjectionCICNGP_project/_comm (:708-976),
  *            T_ii = m v_i^2 at vertices (CIC), T_ij = m v_i v_j on the (i,j)
- *            plaquette (CIC along the third dim).  FP32 mode. */
+ *            plaquette (CIC along the third dim).  FP32 mode.
+ *   vector CIC : vectorProjectionCIC_project/_comm (:978-1349), m v / res^3,
+ *            component i on the link x + e_i/2 with CIC on the staggered
+ *            (link-centred) grid along i and CIC across; both halos folded.
+ *            FP32 mode.
+ *   VecVec CIC : VecVecProjectionCIC_project/_comm (:1355-1814), symmetric
+ *            m v_i v_j / res^3 (components 00,01,02,11,12,22): T_ii CIC at the
+ *            vertices, T_ij on the (i,j) plaquette centre with staggered CIC
+ *            along i and j.  FP32 mode.  The reference's folds for these two
+ *            need a process grid of at least 2x2; this library's fold is the
+ *            periodic one those grids compute. */
 lf2_status lf2_deposit_scalar(lf2_ctx* ctx, lf2_field rho);
 lf2_status lf2_deposit_vector_cicngp(lf2_ctx* ctx, lf2_field v);
 lf2_status lf2_deposit_symtensor_cicngp(lf2_ctx* ctx, lf2_field t);
+lf2_status lf2_deposit_vector_cic(lf2_ctx* ctx, lf2_field v);
+lf2_status lf2_deposit_vecvec_cic(lf2_ctx* ctx, lf2_field t);
 
 /* ---------------------------------------------------------- particle moves
  * Particles::updateVel(cic_kick, dtau, &F, 1) (LATfield2_Particles.hpp:

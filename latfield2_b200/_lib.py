@@ -63,6 +63,8 @@ SIGNATURES = {
     "lf2_deposit_scalar": [c_void_p, c_void_p],
     "lf2_deposit_vector_cicngp": [c_void_p, c_void_p],
     "lf2_deposit_symtensor_cicngp": [c_void_p, c_void_p],
+    "lf2_deposit_vector_cic": [c_void_p, c_void_p],
+    "lf2_deposit_vecvec_cic": [c_void_p, c_void_p],
     "lf2_gather_kick": [c_void_p, c_void_p, c_double, P(c_double)],
     "lf2_drift_rebin": [c_void_p, c_double],
     "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],

@@ -198,6 +198,14 @@ class Context:
     def deposit_symtensor(self, f):
         self._check(_lib.load().lf2_deposit_symtensor_cicngp(self.h, f.h), "deposit_symtensor")
 
+    def deposit_vector_cic(self, f):
+        """vectorProjectionCIC: m v / res^3 on the links, 3 components."""
+        self._check(_lib.load().lf2_deposit_vector_cic(self.h, f.h), "deposit_vector_cic")
+
+    def deposit_vecvec_cic(self, f):
+        """VecVecProjectionCIC: symmetric m v_i v_j / res^3, 6 components."""
+        self._check(_lib.load().lf2_deposit_vecvec_cic(self.h, f.h), "deposit_vecvec_cic")
+
     def gather_kick(self, F, dtau, want_max_v=False):
         mv = _c.c_double()
         self._check(_lib.load().lf2_gather_kick(self.h, F.h, float(dtau),

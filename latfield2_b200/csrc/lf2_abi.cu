@@ -671,11 +671,13 @@ static lf2_status deposit(lf2_ctx* c, lf2_field f, int kind, int comps)
   LF2_TRY(ensure_spill(c, comps));
   {
     PhaseScope ps(c, PH_DEPOSIT);
-    LF2_CUDA(c, launch_deposit(c, kind, f->data, 0));
+    LF2_CUDA(c, kind >= 3 ? launch_deposit_full(c, kind, f->data, 0)
+                          : launch_deposit(c, kind, f->data, 0));
   }
   {
     PhaseScope ps(c, PH_FIXUP);
-    LF2_CUDA(c, launch_deposit(c, kind, f->data, 1));
+    LF2_CUDA(c, kind >= 3 ? launch_deposit_full(c, kind, f->data, 1)
+                          : launch_deposit(c, kind, f->data, 1));
   }
   return LF2_OK;
 }
@@ -683,6 +685,8 @@ static lf2_status deposit(lf2_ctx* c, lf2_field f, int kind, int comps)
 lf2_status lf2_deposit_scalar(lf2_ctx* c, lf2_field rho) { return deposit(c, rho, 0, 1); }
 lf2_status lf2_deposit_vector_cicngp(lf2_ctx* c, lf2_field v) { return deposit(c, v, 1, 3); }
 lf2_status lf2_deposit_symtensor_cicngp(lf2_ctx* c, lf2_field t) { return deposit(c, t, 2, 6); }
+lf2_status lf2_deposit_vector_cic(lf2_ctx* c, lf2_field v) { return deposit(c, v, 3, 3); }
+lf2_status lf2_deposit_vecvec_cic(lf2_ctx* c, lf2_field t) { return deposit(c, t, 4, 6); }
 
 static lf2_status rebin_tail(lf2_ctx* c)
 {

@@ -1,0 +1,278 @@
+// lf2_deposit_full.cu -- the full-CIC (staggered) projections of the
+// brick-binned particles.
+//
+//   kind 3  vector CIC   vectorProjectionCIC_project/_comm (projections.hpp:978-1349)
+//   kind 4  VecVec CIC   VecVecProjectionCIC_project/_comm (:1355-1814)
+//
+// Component c of the vector field (m v_c / res^3) lives on the link
+// x + e_c/2 and is stored at site x; T_ij (i < j) lives on the plaquette
+// centre x + (e_i + e_j)/2 and T_ii on the vertex, both stored at site x.
+// Along a staggered dim a particle in cell l at in-cell offset o lies between
+// the links of sites l - 1 + g and l + g, g = (o >= 1/2); with s = o - 1/2 the
+// lower link gets td = (g ? 1 - s : -s), the upper one tu = 1 - td.  Along a
+// vertex dim the weights are the ordinary CIC ones, 1 - o at l and o at l + 1.
+//
+// One CTA per brick accumulates its particles (FP32 shared atomics) into a
+// tile of (BRICK+2)^3 vertices whose origin is one site below the brick, so
+// the lower staggered neighbours are inside it.  The flush then writes
+//   - every vertex the brick owns (tile coordinates 1..e in all dims) to the
+//     field: the final value for the interior, a partial sum on the brick's
+//     boundary;
+//   - the outer layer (a tile coordinate 0 or e+1) to a per-brick store.
+// k_fixup_full adds, to every owned boundary vertex, the outer-layer values
+// of the up to 26 neighbour bricks that reach it, in a fixed order.  This is
+// the periodic fold of both halos that the reference's *_comm functions do;
+// no global atomics are used and no field has to be cleared first.
+#include <cuda_runtime.h>
+
+#include "lf2_internal.h"
+
+namespace lf2 {
+
+namespace {
+
+constexpr int FT = BRICK + 2;                         // tile vertices per dim
+constexpr int FT3 = FT * FT * FT;                     // 5832 for BRICK = 16
+constexpr int FOUTER = FT3 - BRICK * BRICK * BRICK;   // outer layer, 1736
+
+// The outer-layer store reuses the deposit shell store, which is sized for
+// SHELL 8-byte slots per component and brick.
+static_assert(FOUTER * sizeof(float) <= SHELL * sizeof(uint64_t), "outer store fits the shell store");
+
+// Index of an outer-layer vertex (u0, u1, u2) of the canonical FT^3 tile, in
+// which a tile coordinate equal to the brick extent + 1 has been mapped to
+// FT - 1 (so bricks with e < BRICK use the same layout).  Slabs: the two z
+// faces (2 FT^2), the two y faces without them (2 (FT-2) FT), the two x faces
+// without either (2 (FT-2)^2).
+__host__ __device__ inline int outer_index(int u0, int u1, int u2)
+{
+  if (u2 == 0 || u2 == FT - 1) return (u2 != 0) * FT * FT + u1 * FT + u0;
+  if (u1 == 0 || u1 == FT - 1) return 2 * FT * FT + ((u1 != 0) * (FT - 2) + (u2 - 1)) * FT + u0;
+  return 2 * FT * FT + 2 * (FT - 2) * FT + ((u0 != 0) * (FT - 2) + (u2 - 1)) * (FT - 2) + (u1 - 1);
+}
+
+static_assert(2 * FT * FT + 2 * (FT - 2) * FT + 2 * (FT - 2) * (FT - 2) == FOUTER,
+              "outer slab sizes");
+
+template <int KIND>
+struct FullCfg;
+template <>
+struct FullCfg<3> {
+  static constexpr int comps = 3;
+  static constexpr int threads = 256;  // 70 KB tile: 3 CTAs per SM
+};
+template <>
+struct FullCfg<4> {
+  static constexpr int comps = 6;
+  static constexpr int threads = 512;  // 140 KB tile: 1 CTA per SM
+};
+
+__device__ __forceinline__ int tile_at(int t0, int t1, int t2) { return t0 + FT * (t1 + FT * t2); }
+
+template <int KIND>
+__global__ void __launch_bounds__(FullCfg<KIND>::threads)
+    k_deposit_full(StoreView v, DepositParams dp, float* __restrict__ out,
+                   float* __restrict__ outer)
+{
+  constexpr int C = FullCfg<KIND>::comps;
+  extern __shared__ __align__(16) float tile[];
+
+  const Geom& g = v.g;
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int e[3] = {brick_extent(g.n[0], bx), brick_extent(g.n[1], by),
+                    brick_extent(g.n[2], bz)};
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+  const int64_t base = v.seg_start[b];
+  const int cnt = LF2_BRICK_COUNT(v, b);
+
+  for (int t = threadIdx.x; t < C * FT3; t += blockDim.x) tile[t] = 0.0f;
+  __syncthreads();
+
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int64_t p = base + i;
+    int x, y, z;
+    unpack_key(g, v.a.key[p], x, y, z);
+    const float o[3] = {v.a.ox[p], v.a.oy[p], v.a.oz[p]};
+    const float vel[3] = {v.a.vx[p], v.a.vy[p], v.a.vz[p]};
+    const float mf = dp.has_mass ? __fmul_rn(v.a.mass[p], dp.inv_vol) : dp.mf;
+    const int l[3] = {x - x0, y - y0, z - z0};
+    // per dim: vertex weights (sd, su) at tile coordinates ls, ls + 1 and
+    // staggered weights (td, tu) at lt, lt + 1
+    float sw[3][2], tw[3][2];
+    int ls[3], lt[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      sw[d][1] = o[d];
+      sw[d][0] = __fsub_rn(1.0f, o[d]);
+      const float s = __fsub_rn(o[d], 0.5f);
+      const int gd = s >= 0.0f;
+      if (gd) {
+        tw[d][1] = s;
+        tw[d][0] = __fsub_rn(1.0f, s);
+      } else {
+        tw[d][0] = -s;
+        tw[d][1] = __fsub_rn(1.0f, tw[d][0]);
+      }
+      ls[d] = l[d] + 1;
+      lt[d] = l[d] + gd;
+    }
+    if (KIND == 3) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float mv = __fmul_rn(mf, vel[c]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+          const float w0 = c == 0 ? tw[0][b0] : sw[0][b0];
+          const float w1 = c == 1 ? tw[1][b1] : sw[1][b1];
+          const float w2 = c == 2 ? tw[2][b2] : sw[2][b2];
+          const int t0 = (c == 0 ? lt[0] : ls[0]) + b0;
+          const int t1 = (c == 1 ? lt[1] : ls[1]) + b1;
+          const int t2 = (c == 2 ? lt[2] : ls[2]) + b2;
+          atomicAdd(&tile[c * FT3 + tile_at(t0, t1, t2)],
+                    __fmul_rn(__fmul_rn(__fmul_rn(mv, w0), w1), w2));
+        }
+      }
+    } else {
+      // T_ii at the vertices (components 0, 3, 5)
+      constexpr int diag[3] = {0, 3, 5};
+#pragma unroll
+      for (int i2 = 0; i2 < 3; i2++) {
+        const float m2 = __fmul_rn(__fmul_rn(mf, vel[i2]), vel[i2]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+          atomicAdd(&tile[diag[i2] * FT3 + tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2)],
+                    __fmul_rn(__fmul_rn(__fmul_rn(m2, sw[0][b0]), sw[1][b1]), sw[2][b2]));
+        }
+      }
+      // T_ij on the plaquettes: (0,1) -> 1, (0,2) -> 2, (1,2) -> 4
+      constexpr int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, pc[3] = {1, 2, 4};
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const float mm = __fmul_rn(__fmul_rn(mf, vel[pa[q]]), vel[pb[q]]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+          float w[3];
+          int t[3];
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const bool st = d == pa[q] || d == pb[q];
+            w[d] = st ? tw[d][bb[d]] : sw[d][bb[d]];
+            t[d] = (st ? lt[d] : ls[d]) + bb[d];
+          }
+          atomicAdd(&tile[pc[q] * FT3 + tile_at(t[0], t[1], t[2])],
+                    __fmul_rn(__fmul_rn(__fmul_rn(mm, w[0]), w[1]), w[2]));
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  float* os = outer + (size_t)b * C * FOUTER;
+  for (int t = threadIdx.x; t < FT3; t += blockDim.x) {
+    const int t0 = t % FT, t1 = (t / FT) % FT, t2 = t / (FT * FT);
+    if (t0 > e[0] + 1 || t1 > e[1] + 1 || t2 > e[2] + 1) continue;
+    const bool own = t0 >= 1 && t0 <= e[0] && t1 >= 1 && t1 <= e[1] && t2 >= 1 && t2 <= e[2];
+    if (own) {
+      const int64_t s = site_index(g, x0 + t0 - 1, y0 + t1 - 1, z0 + t2 - 1);
+#pragma unroll
+      for (int c = 0; c < C; c++) out[c * g.nsites + s] = tile[c * FT3 + t];
+    } else {
+      const int oi = outer_index(t0 == e[0] + 1 ? FT - 1 : t0, t1 == e[1] + 1 ? FT - 1 : t1,
+                                 t2 == e[2] + 1 ? FT - 1 : t2);
+#pragma unroll
+      for (int c = 0; c < C; c++) os[c * FOUTER + oi] = tile[c * FT3 + t];
+    }
+  }
+}
+
+// One CTA per brick: every owned vertex on the brick's boundary adds the
+// outer-layer values of the neighbour bricks that reach it.  Along a dim the
+// neighbour offset is -1 (allowed when the vertex is the brick's first, read
+// at the neighbour's tile coordinate e'+1), +1 (the brick's last vertex, read
+// at coordinate 0) or 0 (same coordinate); the 26 non-zero offsets are taken
+// in z, y, x order after the brick's own partial sum.
+template <int C>
+__global__ void __launch_bounds__(256)
+    k_fixup_full(Geom g, const float* __restrict__ outer, float* __restrict__ out)
+{
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+            ez = brick_extent(g.n[2], bz);
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+  const int nown = ex * ey * ez;
+  for (int f = threadIdx.x; f < nown; f += blockDim.x) {
+    const int i = f % ex, j = (f / ex) % ey, k = f / (ex * ey);
+    const bool lo[3] = {i == 0, j == 0, k == 0};
+    const bool hi[3] = {i == ex - 1, j == ey - 1, k == ez - 1};
+    if (!(lo[0] || lo[1] || lo[2] || hi[0] || hi[1] || hi[2])) continue;
+    const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
+    float acc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) acc[c] = out[c * g.nsites + site];
+    for (int dz = -1; dz <= 1; dz++) {
+      if ((dz < 0 && !lo[2]) || (dz > 0 && !hi[2])) continue;
+      const int nbz = wrap_add(bz, dz, g.nb[2]);
+      const int u2 = dz < 0 ? FT - 1 : (dz > 0 ? 0 : k + 1);
+      for (int dy = -1; dy <= 1; dy++) {
+        if ((dy < 0 && !lo[1]) || (dy > 0 && !hi[1])) continue;
+        const int nby = wrap_add(by, dy, g.nb[1]);
+        const int u1 = dy < 0 ? FT - 1 : (dy > 0 ? 0 : j + 1);
+        for (int dx = -1; dx <= 1; dx++) {
+          if ((dx < 0 && !lo[0]) || (dx > 0 && !hi[0])) continue;
+          if (dx == 0 && dy == 0 && dz == 0) continue;
+          const int nbx = wrap_add(bx, dx, g.nb[0]);
+          const int u0 = dx < 0 ? FT - 1 : (dx > 0 ? 0 : i + 1);
+          const int64_t nb = (int64_t)nbx + (int64_t)g.nb[0] * ((int64_t)nby + (int64_t)g.nb[1] * nbz);
+          const float* os = outer + (size_t)nb * C * FOUTER + outer_index(u0, u1, u2);
+#pragma unroll
+          for (int c = 0; c < C; c++) acc[c] = __fadd_rn(acc[c], os[c * FOUTER]);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++) out[c * g.nsites + site] = acc[c];
+  }
+}
+
+template <int KIND>
+cudaError_t run_full(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
+{
+  constexpr int C = FullCfg<KIND>::comps;
+  const unsigned nb = (unsigned)c->g.nbricks;
+  float* outer = reinterpret_cast<float*>(c->spill);
+  if (stage == 0) {
+    const size_t smem = (size_t)C * FT3 * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(k_deposit_full<KIND>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    c->launches += 1;
+    k_deposit_full<KIND><<<nb, FullCfg<KIND>::threads, smem, c->stream>>>(view(c), dp, out, outer);
+  } else {
+    c->launches += 1;
+    k_fixup_full<C><<<nb, 256, 0, c->stream>>>(c->g, outer, out);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_deposit_full(lf2_ctx* c, int kind, float* out, int stage)
+{
+  DepositParams dp;
+  const double vol = c->res * c->res * c->res;
+  dp.inv_vol = (float)(1.0 / vol);
+  dp.mf = (float)(c->gmass / vol);
+  dp.fixed_scale = 0.0f;
+  dp.inv_unit = 0.0f;
+  dp.has_mass = c->has_mass ? 1 : 0;
+  return kind == 3 ? run_full<3>(c, out, dp, stage) : run_full<4>(c, out, dp, stage);
+}
+
+}  // namespace lf2

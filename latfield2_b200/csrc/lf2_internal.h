@@ -159,6 +159,10 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
 cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
 
+// lf2_deposit_full.cu: kind 3 vector CIC, kind 4 VecVec CIC; stage 0 tile
+// pass (k_deposit_full), stage 1 boundary fix-up (k_fixup_full)
+cudaError_t launch_deposit_full(lf2_ctx* c, int kind, float* out, int stage);
+
 // lf2_pm.cu (differentiable chain; op codes documented there)
 cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
                       const float* mass, float gmass, const float* in_a, const float* in_b,

@@ -35,7 +35,7 @@ def test_deposits_match_reference(cuda, path, mode):
     ctx.deposit_scalar(rho)
     got = rho.export(0, np.float64)
     assert normalized_error(got, g["rho"]) < (1e-6 if mode == 1 else 1e-5)
-    if mode == 0:
+    if mode == 0 and "vec" in g:
         v, t = ctx.field(3), ctx.field(6)
         ctx.deposit_vector(v)
         ctx.deposit_symtensor(t)
@@ -45,10 +45,28 @@ def test_deposits_match_reference(cuda, path, mode):
             assert normalized_error(t.export(0, np.float64)[..., c], g["ten"][..., c]) < 1e-5
 
 
+@pytest.mark.parametrize("path", [p for p in CASES if "vcic" in np.load(p)],
+                         ids=lambda p: os.path.basename(p))
+def test_full_cic_deposits_match_reference(cuda, path):
+    """vectorProjectionCIC and VecVecProjectionCIC of the reference on a 2x2
+    process grid against the single-GPU deposits (FP32, 1e-5)."""
+    g = dict(np.load(path))
+    ctx = _ctx(g, 0)
+    v, t = ctx.field(3), ctx.field(6)
+    ctx.deposit_vector_cic(v)
+    ctx.deposit_vecvec_cic(t)
+    for c in range(3):
+        assert normalized_error(v.export(0, np.float64)[..., c], g["vcic"][..., c]) < 1e-5
+    for c in range(6):
+        assert normalized_error(t.export(0, np.float64)[..., c], g["vv"][..., c]) < 1e-5
+
+
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
 def test_kick_and_move_match_reference(cuda, path):
     import torch
     g = dict(np.load(path))
+    if "kick_vel" not in g:
+        pytest.skip("fixture holds deposits only")
     n = int(g["n"])
     ctx = _ctx(g, 1)
     F = torch.from_numpy(np.ascontiguousarray(g["F"].transpose(3, 0, 1, 2)).astype(np.float32)).cuda()
