@@ -690,12 +690,47 @@ void symtensorProjectionCICNGP_project(Particles<part, part_info, part_dataType>
   Tij->mark_device_written();
 }
 
-// The *_comm functions (projections.hpp:194-300, :558-681, :856-976): the
-// periodic fold is part of the GPU deposit; here the result comes back to
-// the host array (with its halo filled).
+// vectorProjectionCIC_project (projections.hpp:978-1190): m v / res^3 on
+// the links, CIC on the staggered grid along each component's own dim.
+template <class part, class part_info, class part_dataType>
+void vectorProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* vel,
+                                 size_t* oset = NULL, int flag_where = FROM_INFO)
+{
+  (void)oset, (void)flag_where;
+  parts->check_field(vel, "vectorProjectionCIC_project");
+  const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
+  lf2_ctx* ctx = owner.get();
+  lf2detail::check(ctx, lf2_deposit_vector_cic(ctx, vel->lf2_handle(owner, false)),
+                   "lf2_deposit_vector_cic");
+  vel->mark_device_written();
+}
+
+// VecVecProjectionCIC_project (projections.hpp:1355-1620): symmetric
+// m v_i v_j / res^3, T_ii on the vertices and T_ij on the (i,j) plaquettes.
+template <class part, class part_info, class part_dataType>
+void VecVecProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* Tij,
+                                 size_t* oset = NULL, int flag_where = FROM_INFO)
+{
+  (void)oset, (void)flag_where;
+  parts->check_field(Tij, "VecVecProjectionCIC_project");
+  const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
+  lf2_ctx* ctx = owner.get();
+  lf2detail::check(ctx, lf2_deposit_vecvec_cic(ctx, Tij->lf2_handle(owner, false)),
+                   "lf2_deposit_vecvec_cic");
+  Tij->mark_device_written();
+}
+
+// The *_comm functions (projections.hpp:194-300, :558-681, :856-976,
+// :1192-1349, :1624-1814): the periodic fold of both halos is part of the
+// GPU deposit; here the result comes back to the host array (with its halo
+// filled).  The reference's vectorProjectionCIC_comm and
+// VecVecProjectionCIC_comm need a process grid of at least 2x2 ranks; on
+// this one-GPU layer they give the periodic fold such grids compute.
 inline void scalarProjectionCIC_comm(Field<Real>* rho) { rho->pull(); }
 inline void vectorProjectionCICNGP_comm(Field<Real>* vel) { vel->pull(); }
 inline void symtensorProjectionCICNGP_comm(Field<Real>* Tij) { Tij->pull(); }
+inline void vectorProjectionCIC_comm(Field<Real>* vel) { vel->pull(); }
+inline void VecVecProjectionCIC_comm(Field<Real>* Tij) { Tij->pull(); }
 
 }  // namespace LATfield2
 

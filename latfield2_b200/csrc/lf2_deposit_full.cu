@@ -192,45 +192,76 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
 
 // One CTA per brick: every owned vertex on the brick's boundary adds the
 // outer-layer values of the neighbour bricks that reach it.  Along a dim the
-// neighbour offset is -1 (allowed when the vertex is the brick's first, read
-// at the neighbour's tile coordinate e'+1), +1 (the brick's last vertex, read
-// at coordinate 0) or 0 (same coordinate); the 26 non-zero offsets are taken
-// in z, y, x order after the brick's own partial sum.
+// neighbour offset is 0 (same coordinate), -1 (the brick's first vertex, read
+// at the neighbour's tile coordinate e'+1) or +1 (its last vertex, read at
+// coordinate 0); the non-zero combinations are added after the brick's own
+// partial sum, z outermost, -1 before 0 before +1.  Threads take the boundary vertices only: the two
+// z faces (rows along x), then the y faces between them (rows along x), then
+// the x faces between those (columns along y, so the neighbours' outer-layer
+// reads stay contiguous).
 template <int C>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_fixup_full(Geom g, const float* __restrict__ outer, float* __restrict__ out)
 {
   const int64_t b = blockIdx.x;
-  int bx, by, bz;
-  brick_coords(g, b, bx, by, bz);
-  const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
-            ez = brick_extent(g.n[2], bz);
-  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-  const int nown = ex * ey * ez;
-  for (int f = threadIdx.x; f < nown; f += blockDim.x) {
-    const int i = f % ex, j = (f / ex) % ey, k = f / (ex * ey);
-    const bool lo[3] = {i == 0, j == 0, k == 0};
-    const bool hi[3] = {i == ex - 1, j == ey - 1, k == ez - 1};
-    if (!(lo[0] || lo[1] || lo[2] || hi[0] || hi[1] || hi[2])) continue;
-    const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
+  int bc[3];
+  brick_coords(g, b, bc[0], bc[1], bc[2]);
+  const int e[3] = {brick_extent(g.n[0], bc[0]), brick_extent(g.n[1], bc[1]),
+                    brick_extent(g.n[2], bc[2])};
+  const int nzp = e[2] > 1 ? 2 : 1, nyp = e[1] > 1 ? 2 : 1, nxp = e[0] > 1 ? 2 : 1;
+  const int iz = e[2] > 2 ? e[2] - 2 : 0, iy = e[1] > 2 ? e[1] - 2 : 0;
+  const int nzf = nzp * e[0] * e[1];
+  const int nyf = iz * nyp * e[0];
+  const int total = nzf + nyf + iz * iy * nxp;
+  // neighbour brick coordinates per dim: [0] = own, [1] = below, [2] = above
+  int nbc[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    nbc[d][0] = bc[d];
+    nbc[d][1] = wrap_add(bc[d], -1, g.nb[d]);
+    nbc[d][2] = wrap_add(bc[d], 1, g.nb[d]);
+  }
+  for (int f = threadIdx.x; f < total; f += blockDim.x) {
+    int q[3];
+    if (f < nzf) {
+      q[0] = f % e[0];
+      q[1] = (f / e[0]) % e[1];
+      q[2] = f / (e[0] * e[1]) ? e[2] - 1 : 0;
+    } else if (f < nzf + nyf) {
+      const int r = f - nzf;
+      q[0] = r % e[0];
+      q[1] = (r / e[0]) % nyp ? e[1] - 1 : 0;
+      q[2] = 1 + r / (e[0] * nyp);
+    } else {
+      const int r = f - nzf - nyf;
+      q[1] = 1 + r % iy;
+      q[0] = (r / iy) % nxp ? e[0] - 1 : 0;
+      q[2] = 1 + r / (iy * nxp);
+    }
+    const bool lo[3] = {q[0] == 0, q[1] == 0, q[2] == 0};
+    const bool hi[3] = {q[0] == e[0] - 1, q[1] == e[1] - 1, q[2] == e[2] - 1};
+    const int64_t site = site_index(g, bc[0] * BRICK + q[0], bc[1] * BRICK + q[1],
+                                    bc[2] * BRICK + q[2]);
     float acc[C];
 #pragma unroll
     for (int c = 0; c < C; c++) acc[c] = out[c * g.nsites + site];
+#pragma unroll
     for (int dz = -1; dz <= 1; dz++) {
       if ((dz < 0 && !lo[2]) || (dz > 0 && !hi[2])) continue;
-      const int nbz = wrap_add(bz, dz, g.nb[2]);
-      const int u2 = dz < 0 ? FT - 1 : (dz > 0 ? 0 : k + 1);
+#pragma unroll
       for (int dy = -1; dy <= 1; dy++) {
         if ((dy < 0 && !lo[1]) || (dy > 0 && !hi[1])) continue;
-        const int nby = wrap_add(by, dy, g.nb[1]);
-        const int u1 = dy < 0 ? FT - 1 : (dy > 0 ? 0 : j + 1);
+#pragma unroll
         for (int dx = -1; dx <= 1; dx++) {
-          if ((dx < 0 && !lo[0]) || (dx > 0 && !hi[0])) continue;
-          if (dx == 0 && dy == 0 && dz == 0) continue;
-          const int nbx = wrap_add(bx, dx, g.nb[0]);
-          const int u0 = dx < 0 ? FT - 1 : (dx > 0 ? 0 : i + 1);
-          const int64_t nb = (int64_t)nbx + (int64_t)g.nb[0] * ((int64_t)nby + (int64_t)g.nb[1] * nbz);
-          const float* os = outer + (size_t)nb * C * FOUTER + outer_index(u0, u1, u2);
+          if ((dx < 0 && !lo[0]) || (dx > 0 && !hi[0]) || (dx == 0 && dy == 0 && dz == 0))
+            continue;
+          const int64_t nb = (int64_t)nbc[0][dx < 0 ? 1 : (dx > 0 ? 2 : 0)] +
+                             (int64_t)g.nb[0] * ((int64_t)nbc[1][dy < 0 ? 1 : (dy > 0 ? 2 : 0)] +
+                                                 (int64_t)g.nb[1] * nbc[2][dz < 0 ? 1 : (dz > 0 ? 2 : 0)]);
+          const int oi = outer_index(dx < 0 ? FT - 1 : (dx > 0 ? 0 : q[0] + 1),
+                                     dy < 0 ? FT - 1 : (dy > 0 ? 0 : q[1] + 1),
+                                     dz < 0 ? FT - 1 : (dz > 0 ? 0 : q[2] + 1));
+          const float* os = outer + (size_t)nb * C * FOUTER + oi;
 #pragma unroll
           for (int c = 0; c < C; c++) acc[c] = __fadd_rn(acc[c], os[c * FOUTER]);
         }

@@ -4,7 +4,8 @@
 //   compat_demo N NPART OUT
 //
 // Seeded particles in a unit box; one scalar projection, the CIC kick with a
-// force field set on the host, the drift, then the three projections again.
+// force field set on the host, the drift, then the scalar, vector CIC-NGP,
+// symtensor CIC-NGP, vector CIC and VecVec CIC projections.
 // Everything the checks need goes to OUT as raw arrays (see write_all).
 #include <cmath>
 #include <cstdint>
@@ -54,6 +55,7 @@ int main(int argc, char** argv)
 
   Lattice lat(3, N, 1), lat_part(3, N, 0);
   Field<Real> rho(lat, 1), F(lat, 3), B(lat, 3), Tij(lat, 3, 3, symmetric);
+  Field<Real> V(lat, 3), VV(lat, 3, 3, symmetric);
 
   part_simple_info info;
   info.mass = 1.0 / npart;
@@ -97,6 +99,10 @@ int main(int argc, char** argv)
   vectorProjectionCICNGP_comm(&B);
   symtensorProjectionCICNGP_project(&parts, &Tij);
   symtensorProjectionCICNGP_comm(&Tij);
+  vectorProjectionCIC_project(&parts, &V);
+  vectorProjectionCIC_comm(&V);
+  VecVecProjectionCIC_project(&parts, &VV);
+  VecVecProjectionCIC_comm(&VV);
 
   std::vector<part_simple> out;
   parts.getParticles(out);
@@ -115,6 +121,8 @@ int main(int argc, char** argv)
   put(fp, interior(rho));
   put(fp, interior(B));
   put(fp, interior(Tij));
+  put(fp, interior(V));
+  put(fp, interior(VV));
   fclose(fp);
   printf("ok %ld particles, max|v| %.6e, sizeof(Real) %zu\n", parts.numParticles(), maxv, sizeof(Real));
   return 0;

@@ -8,8 +8,9 @@ double and with -DSINGLE.
 
 GPU: the demo's results equal those of the same operations through the
 Python binding of the same library: fixed-point density and particles
-bit-exact, the FP32 vector and tensor projections within 1e-5 of the field
-maximum (the order of FP32 additions differs run to run)."""
+bit-exact, the FP32 vector and tensor projections (CIC-NGP and full CIC)
+within 1e-5 of the field maximum (the order of FP32 additions differs run to
+run)."""
 import os
 import struct
 import subprocess
@@ -56,7 +57,7 @@ def test_demo_matches_the_python_binding(cuda, tmp_path):
     n, npart = 32, 20000
     r = subprocess.run([exe, str(n), str(npart), out], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    (hdr, id0, pos0, vel0, rho0, Fv, id1, pos1, vel1, rho1, B, T) = _read(out)
+    (hdr, id0, pos0, vel0, rho0, Fv, id1, pos1, vel1, rho1, B, T, V, VV) = _read(out)
     N, count, dtau, maxv = int(hdr[0]), int(hdr[1]), hdr[2], hdr[3]
     assert N == n and count == npart
     ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64)
@@ -83,3 +84,7 @@ def test_demo_matches_the_python_binding(cuda, tmp_path):
     ctx.deposit_symtensor(t)
     assert normalized_error(B, v.export(0, np.float64).reshape(-1)) < 1e-5
     assert normalized_error(T, t.export(0, np.float64).reshape(-1)) < 1e-5
+    ctx.deposit_vector_cic(v)
+    ctx.deposit_vecvec_cic(t)
+    assert normalized_error(V, v.export(0, np.float64).reshape(-1)) < 1e-5
+    assert normalized_error(VV, t.export(0, np.float64).reshape(-1)) < 1e-5
