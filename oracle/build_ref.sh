@@ -12,11 +12,14 @@ fi
 mkdir -p "$HERE/_ref"
 CXX="${CXX:-g++}"
 FLAGS="-std=c++14 -O2 -ffp-contract=off -w -I$HERE/mpi_shim -I$REF"
+# The FFT build adds the FFTW-interface stand-in (oracle/fftw_shim) and -DFFT3D,
+# which brings in the reference's PlanFFT.
 for v in double single; do
   out="$HERE/_ref/lf2_ref_driver_$v"
-  extra=""
-  [ "$v" = single ] && extra="-DSINGLE"
-  if [ ! -x "$out" ] || [ "$HERE/ref_driver.cpp" -nt "$out" ] || [ "$HERE/mpi_shim/mpi.h" -nt "$out" ]; then
+  extra="-DFFT3D -I$HERE/fftw_shim"
+  [ "$v" = single ] && extra="$extra -DSINGLE"
+  if [ ! -x "$out" ] || [ "$HERE/ref_driver.cpp" -nt "$out" ] || [ "$HERE/mpi_shim/mpi.h" -nt "$out" ] ||
+     [ "$HERE/fftw_shim/fftw3.h" -nt "$out" ]; then
     $CXX $FLAGS $extra -o "$out" "$HERE/ref_driver.cpp"
   fi
 done

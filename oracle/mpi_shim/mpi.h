@@ -488,4 +488,44 @@ inline int MPI_Gather(const void* sendbuf, int scount, MPI_Datatype st_, void* r
   return MPI_SUCCESS;
 }
 
+// Root hands block i of sendbuf to member i.
+inline int MPI_Scatter(const void* sendbuf, int scount, MPI_Datatype st_, void* recvbuf, int rcount,
+                       MPI_Datatype rt, int root, MPI_Comm comm)
+{
+  using namespace lf2_minimpi;
+  const std::vector<int>& m = st().comms[comm];
+  const int me = my_index(m);
+  const size_t sbytes = (size_t)scount * type_size(st_);
+  const size_t rbytes = (size_t)rcount * type_size(rt);
+  if (me == root) {
+    for (size_t i = 0; i < m.size(); i++) {
+      const char* src = (const char*)sendbuf + i * sbytes;
+      if ((int)i == root) memcpy(recvbuf, src, rbytes);
+      else send_raw(m[i], comm, TAG_COLL - 4, src, sbytes);
+    }
+  } else {
+    recv_raw(m[root], comm, TAG_COLL - 4, recvbuf, rbytes);
+  }
+  return MPI_SUCCESS;
+}
+
+// Every member sends block j of sendbuf to member j and receives member i's
+// block for it into block i of recvbuf.  All sends are queued before the
+// receives (the blocks here are small enough for the socket buffers).
+inline int MPI_Alltoall(const void* sendbuf, int scount, MPI_Datatype st_, void* recvbuf, int rcount,
+                        MPI_Datatype rt, MPI_Comm comm)
+{
+  using namespace lf2_minimpi;
+  const std::vector<int>& m = st().comms[comm];
+  const int me = my_index(m);
+  const size_t sbytes = (size_t)scount * type_size(st_);
+  const size_t rbytes = (size_t)rcount * type_size(rt);
+  for (size_t j = 0; j < m.size(); j++)
+    if ((int)j != me) send_raw(m[j], comm, TAG_COLL - 5, (const char*)sendbuf + j * sbytes, sbytes);
+  memcpy((char*)recvbuf + me * rbytes, (const char*)sendbuf + me * sbytes, rbytes);
+  for (size_t i = 0; i < m.size(); i++)
+    if ((int)i != me) recv_raw(m[i], comm, TAG_COLL - 5, (char*)recvbuf + i * rbytes, rbytes);
+  return MPI_SUCCESS;
+}
+
 #endif

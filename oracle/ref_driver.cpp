@@ -28,6 +28,13 @@
 //        int64 nloc, nloc x {id, pos[3], vel[3]}; for the move: int64 nloc,
 //        nloc x {id, pos[3], vel[3]}.  The vector-CIC and VecVec-CIC folds
 //        (sendUpDown) need a process grid of at least 2x2.
+//        OP_FFT (built with -DFFT3D against oracle/fftw_shim): component 0 of
+//        F as a real field through PlanFFT::execute(FFT_FORWARD), written as
+//        int32 kSizeLocal[3], int32 kSkip[2] (storage dims 2 and 1), then the
+//        local k-field as (re, im) doubles; then FFT_BACKWARD of that k-field,
+//        the local gross real field.  OP_POISSON: the reference's Poisson
+//        example (examples/poissonSolver.cpp) on the same real field, res =
+//        1/n: the local gross potential.
 #include <cstdint>
 #include <chrono>
 #include <cstdio>
@@ -65,7 +72,9 @@ enum {
   OP_KICK = 16,
   OP_MOVE = 32,
   OP_VECCIC = 64,
-  OP_VECVEC = 128
+  OP_VECVEC = 128,
+  OP_FFT = 256,
+  OP_POISSON = 512
 };
 
 // CIC gather of the 3-component field at the cell corners and kick, in the
@@ -197,7 +206,7 @@ int main(int argc, char** argv)
   }
 
   Field<Real> F(lat, 3);
-  if (ops & (OP_HALO | OP_KICK)) {
+  if (ops & (OP_HALO | OP_KICK | OP_FFT | OP_POISSON)) {
     std::vector<double> Fg((size_t)n * n * n * 3);
     rd(in, Fg.data(), Fg.size());
     Site x(lat);
@@ -287,6 +296,49 @@ int main(int argc, char** argv)
     write_field(o, T);
   }
   if (ops & OP_HALO) write_field(o, F);
+#ifdef FFT3D
+  if (ops & (OP_FFT | OP_POISSON)) {
+    Lattice latK;
+    latK.initializeRealFFT(lat, 0);
+    Field<Real> r(lat, 1), back(lat, 1);
+    Field<Imag> rK(latK, 1), backK(latK, 1);
+    PlanFFT<Imag> plan(&r, &rK);
+    PlanFFT<Imag> planBack(&back, &backK);
+    Site x(lat);
+    for (x.first(); x.test(); x.next()) r(x) = F(x, 0);
+    plan.execute(FFT_FORWARD);
+    if (ops & OP_FFT) {
+      const int32_t ks[5] = {latK.sizeLocal(0), latK.sizeLocal(1), latK.sizeLocal(2),
+                             (int32_t)latK.coordSkip()[0], (int32_t)latK.coordSkip()[1]};
+      wr(o, ks, 5);
+      const long kg = latK.sitesLocalGross();
+      std::vector<double> buf(2 * kg);
+      for (long i = 0; i < kg; i++) {
+        buf[2 * i] = (double)rK(i).real();
+        buf[2 * i + 1] = (double)rK(i).imag();
+      }
+      wr(o, buf.data(), buf.size());
+      for (long i = 0; i < kg; i++) backK(i) = rK(i);
+      planBack.execute(FFT_BACKWARD);
+      write_field(o, back);
+    }
+    if (ops & OP_POISSON) {
+      // examples/poissonSolver.cpp, with the lattice of this run and res = 1/n
+      const double res = 1.0 / n, res2 = res * res;
+      rKSite k(latK);
+      k.first();
+      if (parallel.isRoot()) {
+        backK(k) = 0.0;
+        k.next();
+      }
+      for (; k.test(); k.next())
+        backK(k) = rK(k) / (2.0 * (cos(2.0 * M_PI * k.coord(0) / n) + cos(2.0 * M_PI * k.coord(1) / n) +
+                                   cos(2.0 * M_PI * k.coord(2) / n) - 3.0) / res2);
+      planBack.execute(FFT_BACKWARD);
+      write_field(o, back);
+    }
+  }
+#endif
   if (ops & OP_KICK) {
     Field<Real>* fl[1] = {&F};
     double out1[1];

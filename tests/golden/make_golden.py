@@ -10,6 +10,11 @@ force field, time steps) and the reference's outputs:
                     shape (n, n, n, comps) indexed [z, y, x, c]
   vcic, vv          vectorProjectionCIC and VecVecProjectionCIC, same form
                     (multi-rank cases only: their halo folds need a 2x2 grid)
+  fft_k             PlanFFT<Imag>::execute(FFT_FORWARD) of F[..., 0], the
+                    global k-field in the reference's storage order
+                    [ky][kz][kx] (kx = 0 .. n/2), complex
+  fft_back          FFT_BACKWARD of that k-field (unnormalised), [z][y][x]
+  poisson           the reference's Poisson example on F[..., 0] (res = 1/n)
   F_halo            the force field after Field::updateHalo, full gross array
                     (single-rank cases only)
   maxv, kick_*      updateVel with the CIC gather-kick callback
@@ -31,7 +36,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref")
 
 OP_SCALAR, OP_VECTOR, OP_TENSOR, OP_HALO, OP_KICK, OP_MOVE = 1, 2, 4, 8, 16, 32
-OP_VECCIC, OP_VECVEC = 64, 128
+OP_VECCIC, OP_VECVEC, OP_FFT, OP_POISSON = 64, 128, 256, 512
 # fields in the order the driver writes them: (op, key, components)
 FIELD_OPS = ((OP_SCALAR, "rho", 1), (OP_VECTOR, "vec", 3), (OP_TENSOR, "ten", 6),
              (OP_VECCIC, "vcic", 3), (OP_VECVEC, "vv", 6))
@@ -39,11 +44,12 @@ FIELD_OPS = ((OP_SCALAR, "rho", 1), (OP_VECTOR, "vec", 3), (OP_TENSOR, "ten", 6)
 CASES = [
     # name, n, halo, grid, npart, clustered, vel sigma, dtau kick, dtau move, ops
     ("uniform8", 8, 1, (1, 1), 300, False, 0.05, 0.05, 0.0,
-     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_HALO | OP_KICK),
+     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_HALO | OP_KICK | OP_FFT | OP_POISSON),
     ("clustered12", 12, 2, (1, 1), 2000, True, 0.2, 0.1, 0.0,
      OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_HALO | OP_KICK),
     ("ranks16", 16, 1, (2, 2), 2500, True, 0.02, 0.05, 0.6,
-     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_VECCIC | OP_VECVEC | OP_KICK | OP_MOVE),
+     OP_SCALAR | OP_VECTOR | OP_TENSOR | OP_VECCIC | OP_VECVEC | OP_KICK | OP_MOVE | OP_FFT |
+     OP_POISSON),
     ("ranks20", 20, 2, (2, 2), 3000, True, 0.3, 0.0, 0.0,
      OP_SCALAR | OP_VECCIC | OP_VECVEC),
 ]
@@ -73,7 +79,7 @@ def write_input(path, n, halo, grid, gmass, ops, dtk, dtm, ids, pos, vel, F):
         rec["pv"][:, :3] = pos
         rec["pv"][:, 3:] = vel
         f.write(rec.tobytes())
-        if ops & (OP_HALO | OP_KICK):
+        if ops & (OP_HALO | OP_KICK | OP_FFT | OP_POISSON):
             f.write(np.ascontiguousarray(F, "<f8").tobytes())
 
 
@@ -107,6 +113,16 @@ def read_rank(path, n, ops, comps_of):
     for op, _, comps in FIELD_OPS + ((OP_HALO, "F_halo", 3),):
         if ops & op:
             out[op] = field(comps)
+    if ops & OP_FFT:
+        k0, k1, k2, ks0, ks1 = take("<5i")
+        kg = k0 * k1 * k2
+        a = np.frombuffer(data, "<f8", 2 * kg, off).copy()
+        off += 16 * kg
+        out["k_size"], out["k_skip"] = (k0, k1, k2), (ks0, ks1)
+        out[OP_FFT] = (a[0::2] + 1j * a[1::2]).reshape(k2, k1, k0)
+        out["fft_back"] = field(1)
+    if ops & OP_POISSON:
+        out[OP_POISSON] = field(1)
     if ops & OP_KICK:
         (out["maxv"],) = take("<d")
         out[OP_KICK] = parts()
@@ -162,6 +178,17 @@ def run_case(name, n, halo, grid, npart, clustered, vsig, dtk, dtm, ops, build, 
     if ops & OP_HALO:
         assert len(ranks) == 1
         res["F_halo"] = ranks[0][OP_HALO]
+    if ops & OP_FFT:
+        K = np.full((n, n, n // 2 + 1), np.nan + 0j)
+        for r in ranks:
+            k0, k1, k2 = r["k_size"]
+            s0, s1 = r["k_skip"]
+            K[s0:s0 + k2, s1:s1 + k1, :k0] = r[OP_FFT]
+        assert not np.isnan(K).any()
+        res["fft_k"] = K
+        res["fft_back"] = assemble([dict(r, back=r["fft_back"]) for r in ranks], n, "back", 1)[..., 0]
+    if ops & OP_POISSON:
+        res["poisson"] = assemble(ranks, n, OP_POISSON, 1)[..., 0]
     if ops & OP_KICK:
         res["maxv"] = max(r["maxv"] for r in ranks)
         res["kick_id"], res["kick_pos"], res["kick_vel"] = sorted_parts(ranks, OP_KICK)

@@ -16,6 +16,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import fft_oracle as FO
 from oracle import oracle as O
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -129,6 +130,40 @@ def test_full_cic_projections_conserve_momentum_and_stress():
         want = np.array([scale * (v[:, i] * v[:, j]).sum() for i, j in pairs])
         np.testing.assert_allclose(g["vv"].reshape(-1, 6).sum(axis=0), want,
                                    rtol=tol, atol=tol * np.abs(want).max())
+
+
+@pytest.mark.parametrize("path", [p for p in CASES if "fft_k" in np.load(p)],
+                         ids=lambda p: os.path.basename(p))
+def test_fft_oracle_matches_reference(path):
+    """The reference's PlanFFT (forward and backward) and its Poisson example,
+    run on 1x1 and 2x2 grids, against the numpy restatement: round-off only
+    (the reference ran over a plain-DFT stand-in of FFTW)."""
+    g = load(path)
+    R, prec = real_of(path)
+    n = int(g["n"])
+    rho = g["F"][..., 0].astype(R).astype(np.float64)
+    tol = 1e-12 if prec == "d" else 1e-6
+    K = FO.rfft_ref(rho)
+    assert np.abs(K - g["fft_k"]).max() <= tol * np.abs(K).max()
+    back = FO.irfft_ref(g["fft_k"])
+    assert np.abs(back - g["fft_back"]).max() <= tol * np.abs(back).max()
+    phi = FO.poisson_example(rho, 1.0 / n)
+    assert np.abs(phi - g["poisson"]).max() <= tol * np.abs(phi).max()
+
+
+def test_pm_force_oracle_properties():
+    """The force of a point mass points at it and the potential satisfies the
+    7-point Poisson equation exactly (to round-off)."""
+    n = 16
+    res = 1.0 / n
+    rho = np.zeros((n, n, n))
+    rho[5, 6, 7] = 1.0
+    phi, F = FO.pm_force(rho, res, 2.0)
+    lap = sum(np.roll(phi, s, a) for a in range(3) for s in (1, -1)) - 6 * phi
+    np.testing.assert_allclose(lap / res ** 2, 2.0 * (rho - rho.mean()), atol=1e-9)
+    # x+1 neighbour of the mass: force along -x (towards the mass)
+    assert F[0][5, 6, 8] < 0 and F[0][5, 6, 6] > 0
+    assert abs(F.sum()) < 1e-9
 
 
 def test_reference_conserves_mass_in_every_fixture():
