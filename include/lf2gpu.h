@@ -40,6 +40,7 @@ extern "C" {
 
 typedef struct lf2_ctx lf2_ctx;
 typedef struct lf2_field_s* lf2_field;
+typedef struct lf2_kfield_s* lf2_kfield;
 typedef int lf2_status;
 
 #define LF2_OK 0
@@ -207,6 +208,36 @@ lf2_status lf2_last_max_velocity(lf2_ctx* ctx, double* max_v, int ptr_kind);
  * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */
 lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
                             double* max_v);
+
+/* ------------------------------------------------------ PM grid operator
+ * Fourier transforms of real fields on a cubic lattice, as PlanFFT<Imag>
+ * (LATfield2_PlanFFT_decl.hpp:83-230, :720-1050; LF2_ERR_ARG on other
+ * lattices), and a Poisson force built on them.
+ * A k-field holds the transform of a `comps`-component real field: the
+ * Field<Imag> of a Lattice initialised by initializeRealFFT (halo 0,
+ * LATfield2_Lattice.hpp:225-258), sizes (n/2+1, n, n).
+ *   kfield_export/import: the reference's storage order [k_y][k_z][k_x]
+ *     (outermost first; rKSite coord(1) = k_y, coord(2) = k_z,
+ *     LATfield2_Site.hpp:319-338), components interleaved, each value
+ *     (re, im) of real_bytes (4 or 8).
+ *   fft_forward  = execute(FFT_FORWARD):  K(k) = sum_x r(x) exp(-2 pi i k.x/n)
+ *   fft_backward = execute(FFT_BACKWARD): r(x) = sum_k K(k) exp(+2 pi i k.x/n)
+ *     over the Hermitian extension; neither is normalised; k is kept.
+ *   pm_force: phi solves the 7-point lattice Poisson equation
+ *     lap(phi) = coupling (rho - mean rho), with the Green's function of the
+ *     reference's Poisson example (examples/poissonSolver.cpp) normalised by
+ *     1/n^3; then F_i = -(phi(x+e_i) - phi(x-e_i)) / (2 res), periodic,
+ *     ready for lf2_gather_kick.  phi (1 component) may be NULL. */
+lf2_status lf2_kfield_create(lf2_ctx* ctx, int comps, lf2_kfield* out);
+lf2_status lf2_kfield_destroy(lf2_ctx* ctx, lf2_kfield k);
+lf2_status lf2_kfield_export(lf2_ctx* ctx, lf2_kfield k, void* dst,
+                             int real_bytes, int ptr_kind);
+lf2_status lf2_kfield_import(lf2_ctx* ctx, lf2_kfield k, const void* src,
+                             int real_bytes, int ptr_kind);
+lf2_status lf2_fft_forward(lf2_ctx* ctx, lf2_field r, lf2_kfield k);
+lf2_status lf2_fft_backward(lf2_ctx* ctx, lf2_kfield k, lf2_field r);
+lf2_status lf2_pm_force(lf2_ctx* ctx, lf2_field rho, lf2_field phi,
+                        lf2_field F, double coupling);
 
 /* ------------------------------------------------- differentiable PM chain
  * Particle kernels on arrays kept in the caller's order (no rebinning, so

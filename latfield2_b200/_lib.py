@@ -65,6 +65,13 @@ SIGNATURES = {
     "lf2_deposit_symtensor_cicngp": [c_void_p, c_void_p],
     "lf2_deposit_vector_cic": [c_void_p, c_void_p],
     "lf2_deposit_vecvec_cic": [c_void_p, c_void_p],
+    "lf2_kfield_create": [c_void_p, c_int, P(c_void_p)],
+    "lf2_kfield_destroy": [c_void_p, c_void_p],
+    "lf2_kfield_export": [c_void_p, c_void_p, c_void_p, c_int, c_int],
+    "lf2_kfield_import": [c_void_p, c_void_p, c_void_p, c_int, c_int],
+    "lf2_fft_forward": [c_void_p, c_void_p, c_void_p],
+    "lf2_fft_backward": [c_void_p, c_void_p, c_void_p],
+    "lf2_pm_force": [c_void_p, c_void_p, c_void_p, c_void_p, c_double],
     "lf2_gather_kick": [c_void_p, c_void_p, c_double, P(c_double)],
     "lf2_drift_rebin": [c_void_p, c_double],
     "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],

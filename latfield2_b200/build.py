@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblf2gpu.so")
 SOURCES = ["lf2_abi.cu", "lf2_store.cu", "lf2_move.cu", "lf2_move_pipe.cu", "lf2_deposit.cu",
-           "lf2_deposit_full.cu", "lf2_field.cu", "lf2_noalloc.cu", "lf2_pm.cu"]
+           "lf2_deposit_full.cu", "lf2_field.cu", "lf2_noalloc.cu", "lf2_pm.cu", "lf2_fft.cu"]
 HEADERS = ["lf2_common.cuh", "lf2_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -43,7 +43,7 @@ def build(force=False, verbose=False):
         return LIB
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
            "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcufft"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -90,6 +90,50 @@ class FieldHandle:
         _lib.check(self.ctx.h, _lib.load().lf2_field_zero(self.ctx.h, self.h), "zero")
 
 
+class KFieldHandle:
+    """A device k-field: the Fourier transform of a `comps`-component real
+    field (PlanFFT's Field<Imag>), complex64 on the device."""
+
+    def __init__(self, ctx, comps):
+        self.ctx = ctx
+        self.comps = comps
+        h = _c.c_void_p()
+        _lib.check(ctx.h, _lib.load().lf2_kfield_create(ctx.h, comps, _c.byref(h)), "kfield_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            _lib.load().lf2_kfield_destroy(self.ctx.h, self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _shape(self):
+        n = self.ctx.n
+        return (n[1], n[2], n[0] // 2 + 1, self.comps)
+
+    def export(self, dtype=np.complex128):
+        """Reference layout: shape (n, n, n/2+1, comps) indexed
+        [k_y][k_z][k_x][c], complex."""
+        out = np.empty(self._shape(), dtype=dtype)
+        p, kind = _ptr(out)
+        _lib.check(self.ctx.h, _lib.load().lf2_kfield_export(
+            self.ctx.h, self.h, p, out.itemsize // 2, kind), "kfield_export")
+        return out
+
+    def import_(self, arr):
+        arr = np.ascontiguousarray(arr)
+        if arr.shape != self._shape() or arr.dtype not in (np.complex64, np.complex128):
+            raise ValueError(f"k-field array must be complex with shape {self._shape()}")
+        p, kind = _ptr(arr)
+        _lib.check(self.ctx.h, _lib.load().lf2_kfield_import(
+            self.ctx.h, self.h, p, arr.itemsize // 2, kind), "kfield_import")
+
+
 class Context:
     def __init__(self, n, box=1.0, mode=_lib.DEPOSIT_FP32, device=0, stream=None):
         if np.isscalar(n):
@@ -183,6 +227,22 @@ class Context:
     # ------------------------------------------------------------------- fields
     def field(self, comps, tensor=None):
         return FieldHandle(self, comps, tensor)
+
+    def kfield(self, comps=1):
+        return KFieldHandle(self, comps)
+
+    def fft_forward(self, r, k):
+        """PlanFFT::execute(FFT_FORWARD): k = unnormalised transform of r."""
+        self._check(_lib.load().lf2_fft_forward(self.h, r.h, k.h), "fft_forward")
+
+    def fft_backward(self, k, r):
+        """PlanFFT::execute(FFT_BACKWARD): r = unnormalised inverse of k."""
+        self._check(_lib.load().lf2_fft_backward(self.h, k.h, r.h), "fft_backward")
+
+    def pm_force(self, rho, F, coupling=1.0, phi=None):
+        """F = -grad phi (central differences), lap7(phi) = coupling (rho - mean)."""
+        self._check(_lib.load().lf2_pm_force(self.h, rho.h, None if phi is None else phi.h, F.h,
+                                             float(coupling)), "pm_force")
 
     def halo_fill(self, tensor, comps, halo):
         self._check(_lib.load().lf2_halo_fill(self.h, _c.c_void_p(tensor.data_ptr()), comps, halo,

@@ -359,6 +359,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->ovf_state);
   cudaFree(c->spill);
   cudaFree(c->stencil_partial);
+  fft_release(c);
   cudaFreeHost(c->h_stats);
   cudaFreeHost(c->h_flags);
   cudaFreeHost(c->h_i64);

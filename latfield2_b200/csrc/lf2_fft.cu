@@ -1,0 +1,354 @@
+// lf2_fft.cu -- the PM grid operator on one GPU.
+//
+//  - PlanFFT<Imag> for a real field on a cubic lattice
+//    (LATfield2_PlanFFT_decl.hpp:720-1050): execute(FFT_FORWARD) and
+//    execute(FFT_BACKWARD), unnormalised, through cuFFT's 3-D R2C/C2R.  The
+//    reference distributes the transform over its process grid with explicit
+//    transposes; on one GPU the whole cube is one cuFFT plan.
+//  - k-fields: complex, kept in cuFFT's order [k_z][k_y][k_x] per component.
+//    Import/export convert to the reference's Field<Imag> on the lattice of
+//    Lattice::initializeRealFFT (halo 0), whose storage order is
+//    [k_y][k_z][k_x] (rKSite, LATfield2_Site.hpp:319-338), components
+//    interleaved.
+//  - lf2_pm_force: the Poisson solve of the reference's example
+//    (examples/poissonSolver.cpp: rho_k divided by the eigenvalue of the
+//    7-point lattice Laplacian, the k = 0 mode set to zero), normalised, and
+//    the central-difference force F_i = -(phi(x+e_i) - phi(x-e_i)) / (2 res):
+//    cuFFT R2C, k_green (Green's function, in place), cuFFT C2R, k_gradient.
+//    The Laplacian eigenvalue is evaluated as -4 sum_d sin^2(pi k_d / n) / res^2,
+//    which equals the example's 2 (sum_d cos(2 pi k_d / n) - 3) / res^2 without
+//    its cancellation at small k.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <new>
+#include <string>
+
+#include "lf2_internal.h"
+
+using namespace lf2;
+
+struct lf2_kfield_s {
+  int comps = 0;
+  float2* data = nullptr;  // comps x [n2][n1][n0/2+1]
+};
+
+namespace lf2 {
+
+namespace {
+
+lf2_status fft_fail(lf2_ctx* c, lf2_status code, const std::string& msg)
+{
+  if (c) c->err = msg;
+  return code;
+}
+
+#define FFT_CUDA(c, expr)                                                                   \
+  do {                                                                                      \
+    cudaError_t e_ = (expr);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fft_fail((c), LF2_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define FFT_CUFFT(c, expr)                                                                  \
+  do {                                                                                      \
+    cufftResult r_ = (expr);                                                                \
+    if (r_ != CUFFT_SUCCESS)                                                                \
+      return fft_fail((c), LF2_ERR_CUDA,                                                    \
+                      std::string(#expr ": cuFFT status ") + std::to_string((int)r_));      \
+  } while (0)
+
+#define FFT_TRY(expr)            \
+  do {                           \
+    lf2_status s_ = (expr);      \
+    if (s_ != LF2_OK) return s_; \
+  } while (0)
+
+inline int64_t k_sites(const lf2_ctx* c)
+{
+  return (int64_t)c->g.n[2] * c->g.n[1] * (c->g.n[0] / 2 + 1);
+}
+
+inline unsigned grid_for(int64_t n, int threads)
+{
+  const int64_t b = (n + threads - 1) / threads;
+  return (unsigned)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
+}
+
+bool field_ok(const lf2_field f, int comps) { return f && f->data && f->comps == comps; }
+
+lf2_status need_cubic(lf2_ctx* c)
+{
+  if (c->g.n[0] != c->g.n[1] || c->g.n[1] != c->g.n[2])
+    return fft_fail(c, LF2_ERR_ARG,
+                    "the FFT works on cubic lattices only (as PlanFFT::initialize, "
+                    "LATfield2_PlanFFT_decl.hpp:787-797)");
+  return LF2_OK;
+}
+
+lf2_status ensure_plans(lf2_ctx* c)
+{
+  FFT_TRY(need_cubic(c));
+  if (!c->fft_planned) {
+    cufftHandle a = 0, b = 0;
+    FFT_CUFFT(c, cufftPlan3d(&a, c->g.n[2], c->g.n[1], c->g.n[0], CUFFT_R2C));
+    const cufftResult rb = cufftPlan3d(&b, c->g.n[2], c->g.n[1], c->g.n[0], CUFFT_C2R);
+    if (rb != CUFFT_SUCCESS) {
+      cufftDestroy(a);
+      return fft_fail(c, LF2_ERR_CUDA, "cufftPlan3d (C2R): cuFFT status " + std::to_string((int)rb));
+    }
+    c->fft_r2c = a;
+    c->fft_c2r = b;
+    c->fft_planned = true;
+  }
+  FFT_CUFFT(c, cufftSetStream(c->fft_r2c, c->stream));
+  FFT_CUFFT(c, cufftSetStream(c->fft_c2r, c->stream));
+  return LF2_OK;
+}
+
+// One component of complex scratch (and, when asked, one of real scratch).
+lf2_status ensure_scratch(lf2_ctx* c, bool real_too)
+{
+  if (!c->fft_k) FFT_CUDA(c, cudaMalloc(&c->fft_k, sizeof(float2) * (size_t)k_sites(c)));
+  if (real_too && !c->fft_phi)
+    FFT_CUDA(c, cudaMalloc(&c->fft_phi, sizeof(float) * (size_t)c->g.nsites));
+  return LF2_OK;
+}
+
+// K[kz][ky][kx] *= coef / (s_x^2 + s_y^2 + s_z^2), s_d = sin(pi k_d / n); K_0 = 0.
+// coef = -coupling res^2 / (4 N) turns the unnormalised transform of rho
+// into the normalised potential phi_k.
+__global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
+{
+  const int64_t total = (int64_t)n * n * nkx;
+  const float inv_n = 1.0f / (float)n;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int kx = (int)(i % nkx);
+    const int64_t r = i / nkx;
+    const int ky = (int)(r % n), kz = (int)(r / n);
+    const float sx = sinpif((float)kx * inv_n), sy = sinpif((float)ky * inv_n),
+                sz = sinpif((float)kz * inv_n);
+    const float s2 = sx * sx + sy * sy + sz * sz;
+    const float f = i == 0 ? 0.0f : coef / s2;
+    const float2 v = K[i];
+    K[i] = make_float2(v.x * f, v.y * f);
+  }
+}
+
+// F_c = (phi(x - e_c) - phi(x + e_c)) * inv_2res, periodic, component-major.
+__global__ void k_gradient(const float* __restrict__ phi, float* __restrict__ F, Geom g,
+                           float inv_2res)
+{
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int64_t ns = g.nsites;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % n0);
+    const int64_t r = i / n0;
+    const int y = (int)(r % n1), z = (int)(r / n1);
+    const int64_t row = i - x;
+    const int64_t plane = i - (int64_t)y * n0;
+    const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+    const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
+    const int zp = z + 1 == n2 ? 0 : z + 1, zm = z == 0 ? n2 - 1 : z - 1;
+    const int64_t zs = (int64_t)n0 * n1;
+    const int64_t base_xy = i - (int64_t)z * zs;
+    F[i] = (phi[row + xm] - phi[row + xp]) * inv_2res;
+    F[ns + i] = (phi[plane + (int64_t)ym * n0] - phi[plane + (int64_t)yp * n0]) * inv_2res;
+    F[2 * ns + i] = (phi[base_xy + (int64_t)zm * zs] - phi[base_xy + (int64_t)zp * zs]) * inv_2res;
+  }
+}
+
+// Reference layout d = ((ky n + kz) nkx + kx) comps + c  <->  K[c][kz][ky][kx].
+template <class T>
+__global__ void k_kexport(const float2* __restrict__ K, int comps, int n, int nkx,
+                          T* __restrict__ dst)
+{
+  const int64_t nk = (int64_t)n * n * nkx;
+  const int64_t total = nk * comps;
+  for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(d % comps);
+    const int64_t s = d / comps;
+    const int kx = (int)(s % nkx);
+    const int64_t r = s / nkx;
+    const int kz = (int)(r % n), ky = (int)(r / n);
+    const float2 v = K[c * nk + ((int64_t)kz * n + ky) * nkx + kx];
+    dst[2 * d] = (T)v.x;
+    dst[2 * d + 1] = (T)v.y;
+  }
+}
+
+template <class T>
+__global__ void k_kimport(float2* __restrict__ K, int comps, int n, int nkx,
+                          const T* __restrict__ src)
+{
+  const int64_t nk = (int64_t)n * n * nkx;
+  const int64_t total = nk * comps;
+  for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(d % comps);
+    const int64_t s = d / comps;
+    const int kx = (int)(s % nkx);
+    const int64_t r = s / nkx;
+    const int kz = (int)(r % n), ky = (int)(r / n);
+    K[c * nk + ((int64_t)kz * n + ky) * nkx + kx] =
+        make_float2((float)src[2 * d], (float)src[2 * d + 1]);
+  }
+}
+
+}  // namespace
+
+void fft_release(lf2_ctx* c)
+{
+  if (c->fft_planned) {
+    cufftDestroy(c->fft_r2c);
+    cufftDestroy(c->fft_c2r);
+    c->fft_planned = false;
+  }
+  cudaFree(c->fft_k);
+  cudaFree(c->fft_phi);
+  c->fft_k = nullptr;
+  c->fft_phi = nullptr;
+}
+
+}  // namespace lf2
+
+extern "C" {
+
+lf2_status lf2_kfield_create(lf2_ctx* c, int comps, lf2_kfield* out)
+{
+  if (!c || !out || comps < 1 || comps > 64) return LF2_ERR_ARG;
+  lf2_kfield k = new (std::nothrow) lf2_kfield_s();
+  if (!k) return LF2_ERR_NOMEM;
+  k->comps = comps;
+  const size_t bytes = sizeof(float2) * (size_t)comps * (size_t)k_sites(c);
+  if (cudaMalloc(&k->data, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete k;
+    return fft_fail(c, LF2_ERR_NOMEM, "cannot allocate k-field");
+  }
+  FFT_CUDA(c, cudaMemsetAsync(k->data, 0, bytes, c->stream));
+  *out = k;
+  return LF2_OK;
+}
+
+lf2_status lf2_kfield_destroy(lf2_ctx* c, lf2_kfield k)
+{
+  if (!k) return LF2_OK;
+  if (c) cudaStreamSynchronize(c->stream);
+  cudaFree(k->data);
+  delete k;
+  return LF2_OK;
+}
+
+lf2_status lf2_kfield_export(lf2_ctx* c, lf2_kfield k, void* dst, int real_bytes, int ptr_kind)
+{
+  if (!c || !k || !k->data || !dst || (real_bytes != 4 && real_bytes != 8) ||
+      (ptr_kind != LF2_PTR_HOST && ptr_kind != LF2_PTR_DEVICE))
+    return LF2_ERR_ARG;
+  const int64_t total = k_sites(c) * k->comps;
+  const size_t bytes = (size_t)total * 2 * real_bytes;
+  void* d = dst;
+  if (ptr_kind == LF2_PTR_HOST) FFT_CUDA(c, cudaMallocAsync(&d, bytes, c->stream));
+  const int n = c->g.n[0], nkx = c->g.n[0] / 2 + 1;
+  c->launches += 1;
+  if (real_bytes == 4)
+    k_kexport<float><<<grid_for(total, 256), 256, 0, c->stream>>>(k->data, k->comps, n, nkx,
+                                                                  (float*)d);
+  else
+    k_kexport<double><<<grid_for(total, 256), 256, 0, c->stream>>>(k->data, k->comps, n, nkx,
+                                                                   (double*)d);
+  cudaError_t e = cudaGetLastError();
+  if (ptr_kind == LF2_PTR_HOST) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst, d, bytes, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  }
+  FFT_CUDA(c, e);
+  return LF2_OK;
+}
+
+lf2_status lf2_kfield_import(lf2_ctx* c, lf2_kfield k, const void* src, int real_bytes,
+                             int ptr_kind)
+{
+  if (!c || !k || !k->data || !src || (real_bytes != 4 && real_bytes != 8) ||
+      (ptr_kind != LF2_PTR_HOST && ptr_kind != LF2_PTR_DEVICE))
+    return LF2_ERR_ARG;
+  const int64_t total = k_sites(c) * k->comps;
+  const size_t bytes = (size_t)total * 2 * real_bytes;
+  void* d = const_cast<void*>(src);
+  if (ptr_kind == LF2_PTR_HOST) {
+    FFT_CUDA(c, cudaMallocAsync(&d, bytes, c->stream));
+    const cudaError_t e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(d, c->stream);
+      FFT_CUDA(c, e);
+    }
+  }
+  const int n = c->g.n[0], nkx = c->g.n[0] / 2 + 1;
+  c->launches += 1;
+  if (real_bytes == 4)
+    k_kimport<float><<<grid_for(total, 256), 256, 0, c->stream>>>(k->data, k->comps, n, nkx,
+                                                                  (const float*)d);
+  else
+    k_kimport<double><<<grid_for(total, 256), 256, 0, c->stream>>>(k->data, k->comps, n, nkx,
+                                                                   (const double*)d);
+  const cudaError_t e = cudaGetLastError();
+  if (ptr_kind == LF2_PTR_HOST) cudaFreeAsync(d, c->stream);
+  FFT_CUDA(c, e);
+  return LF2_OK;
+}
+
+lf2_status lf2_fft_forward(lf2_ctx* c, lf2_field r, lf2_kfield k)
+{
+  if (!c || !k || !k->data || !field_ok(r, k->comps)) return LF2_ERR_ARG;
+  FFT_TRY(ensure_plans(c));
+  const int64_t nk = k_sites(c);
+  for (int comp = 0; comp < k->comps; comp++)
+    FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, r->data + (size_t)comp * c->g.nsites,
+                              reinterpret_cast<cufftComplex*>(k->data + (size_t)comp * nk)));
+  return LF2_OK;
+}
+
+lf2_status lf2_fft_backward(lf2_ctx* c, lf2_kfield k, lf2_field r)
+{
+  if (!c || !k || !k->data || !field_ok(r, k->comps)) return LF2_ERR_ARG;
+  FFT_TRY(ensure_plans(c));
+  FFT_TRY(ensure_scratch(c, false));
+  const int64_t nk = k_sites(c);
+  // cuFFT's C2R overwrites its input; the reference keeps the k-field.
+  for (int comp = 0; comp < k->comps; comp++) {
+    FFT_CUDA(c, cudaMemcpyAsync(c->fft_k, k->data + (size_t)comp * nk, sizeof(float2) * nk,
+                                cudaMemcpyDeviceToDevice, c->stream));
+    FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k),
+                              r->data + (size_t)comp * c->g.nsites));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_force(lf2_ctx* c, lf2_field rho, lf2_field phi, lf2_field F, double coupling)
+{
+  if (!c || !field_ok(rho, 1) || !field_ok(F, 3) || (phi && !field_ok(phi, 1)))
+    return LF2_ERR_ARG;
+  FFT_TRY(ensure_plans(c));
+  FFT_TRY(ensure_scratch(c, phi == nullptr));
+  float* p = phi ? phi->data : c->fft_phi;
+  const int n = c->g.n[0], nkx = n / 2 + 1;
+  const int64_t nk = k_sites(c);
+  FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, rho->data, reinterpret_cast<cufftComplex*>(c->fft_k)));
+  const float coef = (float)(-coupling * c->res * c->res / (4.0 * (double)c->g.nsites));
+  c->launches += 1;
+  k_green<<<grid_for(nk, 256), 256, 0, c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx,
+                                                    coef);
+  FFT_CUDA(c, cudaGetLastError());
+  FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), p));
+  c->launches += 1;
+  k_gradient<<<grid_for(c->g.nsites, 256), 256, 0, c->stream>>>(p, F->data, c->g,
+                                                                (float)(0.5 / c->res));
+  FFT_CUDA(c, cudaGetLastError());
+  return LF2_OK;
+}
+
+}  // extern "C"

@@ -106,6 +106,13 @@ struct lf2_ctx {
   const float* tmap_src = nullptr;   // field the cached tensor map describes
   alignas(64) unsigned char tmap_bytes[128];
 
+  // PM grid operator (lf2_fft.cu)
+  int fft_r2c = 0;                   // cuFFT plan handles, valid when fft_planned
+  int fft_c2r = 0;
+  bool fft_planned = false;
+  float2* fft_k = nullptr;           // one component of complex scratch
+  float* fft_phi = nullptr;          // one component of real scratch
+
   // measurement (lf2_profile_*)
   int64_t launches = 0;              // kernels launched, all phases
   bool profiling = false;
@@ -158,6 +165,9 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
 // lf2_deposit.cu
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
 cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
+
+// lf2_fft.cu: releases the cuFFT plans and scratch of the context
+void fft_release(lf2_ctx* c);
 
 // lf2_deposit_full.cu: kind 3 vector CIC, kind 4 VecVec CIC; stage 0 tile
 // pass (k_deposit_full), stage 1 boundary fix-up (k_fixup_full)
