@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-projections", action="store_true",
                     help="skip timing the full-CIC vector and VecVec projections")
+    ap.add_argument("--no-pm", action="store_true",
+                    help="skip timing the PM grid operator (FFT Poisson force)")
     ap.add_argument("--no-fp32", action="store_true",
                     help="skip the FP32-mode run of the same particles (fixed-point workloads)")
     return ap.parse_args()
@@ -476,6 +478,44 @@ def full_cic_projections(ctx, npart, nsites, peak, reps=5):
     return out
 
 
+def pm_operator(ctx, rho, n, nsites, peak, reps=5):
+    """lf2_pm_force (R2C, Green's function, C2R, gradient) on the bench's own
+    density, and the bare PlanFFT-style transforms, each the mean of `reps`
+    calls after one warm-up, timed with CUDA events on the context's stream
+    (the default stream).  Algorithmic bytes of the force: rho read once and
+    the 3-component force written once (16 B per site); the FFT route itself
+    moves at least 40 B per site (transform, Green's function, inverse,
+    gradient)."""
+    import torch
+    if not (n[0] == n[1] == n[2]):
+        return None
+    F2 = ctx.field(3)
+    k = ctx.kfield(1)
+    back = ctx.field(1)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms = timed(lambda: ctx.pm_force(rho, F2, 1.0))
+    fwd = timed(lambda: ctx.fft_forward(rho, k))
+    bwd = timed(lambda: ctx.fft_backward(k, back))
+    ctx.synchronize()
+    ab = 16 * nsites
+    del F2, k, back
+    return {"ms": ms, "fft_forward_ms": fwd, "fft_backward_ms": bwd, "alg_bytes": ab,
+            "achieved_gbs": ab / (ms / 1e3) / 1e9, "frac_of_hbm": ab / (ms / 1e3) / 1e9 / peak,
+            "route_min_bytes": 40 * nsites,
+            "route_frac_of_hbm": 40 * nsites / (ms / 1e3) / 1e9 / peak}
+
+
 def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
     """Device time per lf2_step of the same particles with FP32 atomic
     deposits (CUDA events on the launching stream)."""
@@ -609,6 +649,7 @@ def main():
     e2e = e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, args.e2e_steps, pg, device, barrier)
 
     proj = None if args.no_projections else full_cic_projections(ctx, npart, nsites, peak)
+    pm = None if args.no_pm else pm_operator(ctx, rho, n, nsites, peak)
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
 
@@ -657,6 +698,7 @@ def main():
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
             "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin, "projections": proj,
+            "pm_operator": pm,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

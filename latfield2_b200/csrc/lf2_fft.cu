@@ -115,48 +115,57 @@ lf2_status ensure_scratch(lf2_ctx* c, bool real_too)
   return LF2_OK;
 }
 
-// K[kz][ky][kx] *= coef / (s_x^2 + s_y^2 + s_z^2), s_d = sin(pi k_d / n); K_0 = 0.
-// coef = -coupling res^2 / (4 N) turns the unnormalised transform of rho
-// into the normalised potential phi_k.
+// K[kz][ky][kx] *= coef / (s2(kx) + s2(ky) + s2(kz)), s2(k) = sin^2(pi k / n),
+// K_0 = 0.  coef = -coupling res^2 / (4 N) turns the unnormalised transform
+// of rho into the normalised potential phi_k.  One CTA walks rows (kz, ky);
+// the n values of s2 sit in a shared table (4 n bytes of dynamic shared
+// memory), so no transcendental or 64-bit division runs per element.
 __global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
 {
-  const int64_t total = (int64_t)n * n * nkx;
+  extern __shared__ float s2tab[];
   const float inv_n = 1.0f / (float)n;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int kx = (int)(i % nkx);
-    const int64_t r = i / nkx;
-    const int ky = (int)(r % n), kz = (int)(r / n);
-    const float sx = sinpif((float)kx * inv_n), sy = sinpif((float)ky * inv_n),
-                sz = sinpif((float)kz * inv_n);
-    const float s2 = sx * sx + sy * sy + sz * sz;
-    const float f = i == 0 ? 0.0f : coef / s2;
-    const float2 v = K[i];
-    K[i] = make_float2(v.x * f, v.y * f);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float s = sinpif((float)i * inv_n);
+    s2tab[i] = s * s;
+  }
+  __syncthreads();
+  const int rows = n * n;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int ky = row % n, kz = row / n;
+    const float syz = s2tab[ky] + s2tab[kz];
+    float2* Kr = K + (int64_t)row * nkx;
+    for (int kx = threadIdx.x; kx < nkx; kx += blockDim.x) {
+      const float f = (row == 0 && kx == 0) ? 0.0f : coef / (s2tab[kx] + syz);
+      const float2 v = Kr[kx];
+      Kr[kx] = make_float2(v.x * f, v.y * f);
+    }
   }
 }
 
 // F_c = (phi(x - e_c) - phi(x + e_c)) * inv_2res, periodic, component-major.
+// One CTA walks x-rows (z, y); threads run along x.
 __global__ void k_gradient(const float* __restrict__ phi, float* __restrict__ F, Geom g,
                            float inv_2res)
 {
   const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
   const int64_t ns = g.nsites;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ns;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % n0);
-    const int64_t r = i / n0;
-    const int y = (int)(r % n1), z = (int)(r / n1);
-    const int64_t row = i - x;
-    const int64_t plane = i - (int64_t)y * n0;
-    const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+  const int rows = n1 * n2;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int y = row % n1, z = row / n1;
     const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
     const int zp = z + 1 == n2 ? 0 : z + 1, zm = z == 0 ? n2 - 1 : z - 1;
-    const int64_t zs = (int64_t)n0 * n1;
-    const int64_t base_xy = i - (int64_t)z * zs;
-    F[i] = (phi[row + xm] - phi[row + xp]) * inv_2res;
-    F[ns + i] = (phi[plane + (int64_t)ym * n0] - phi[plane + (int64_t)yp * n0]) * inv_2res;
-    F[2 * ns + i] = (phi[base_xy + (int64_t)zm * zs] - phi[base_xy + (int64_t)zp * zs]) * inv_2res;
+    const float* pr = phi + (int64_t)row * n0;
+    const float* pyp = phi + ((int64_t)z * n1 + yp) * n0;
+    const float* pym = phi + ((int64_t)z * n1 + ym) * n0;
+    const float* pzp = phi + ((int64_t)zp * n1 + y) * n0;
+    const float* pzm = phi + ((int64_t)zm * n1 + y) * n0;
+    float* f0 = F + (int64_t)row * n0;
+    for (int x = threadIdx.x; x < n0; x += blockDim.x) {
+      const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+      f0[x] = (pr[xm] - pr[xp]) * inv_2res;
+      f0[ns + x] = (pym[x] - pyp[x]) * inv_2res;
+      f0[2 * ns + x] = (pzm[x] - pzp[x]) * inv_2res;
+    }
   }
 }
 
@@ -336,17 +345,18 @@ lf2_status lf2_pm_force(lf2_ctx* c, lf2_field rho, lf2_field phi, lf2_field F, d
   FFT_TRY(ensure_scratch(c, phi == nullptr));
   float* p = phi ? phi->data : c->fft_phi;
   const int n = c->g.n[0], nkx = n / 2 + 1;
-  const int64_t nk = k_sites(c);
   FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, rho->data, reinterpret_cast<cufftComplex*>(c->fft_k)));
   const float coef = (float)(-coupling * c->res * c->res / (4.0 * (double)c->g.nsites));
+  const int rows = n * n;
   c->launches += 1;
-  k_green<<<grid_for(nk, 256), 256, 0, c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx,
-                                                    coef);
+  k_green<<<rows < 148 * 8 ? rows : 148 * 8, 256, sizeof(float) * n, c->stream>>>(
+      reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
   FFT_CUDA(c, cudaGetLastError());
   FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), p));
   c->launches += 1;
-  k_gradient<<<grid_for(c->g.nsites, 256), 256, 0, c->stream>>>(p, F->data, c->g,
-                                                                (float)(0.5 / c->res));
+  const int grows = c->g.n[1] * c->g.n[2];
+  k_gradient<<<grows < 148 * 8 ? grows : 148 * 8, 256, 0, c->stream>>>(p, F->data, c->g,
+                                                                        (float)(0.5 / c->res));
   FFT_CUDA(c, cudaGetLastError());
   return LF2_OK;
 }
