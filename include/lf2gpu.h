@@ -227,7 +227,8 @@ lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
  *     lap(phi) = coupling (rho - mean rho), with the Green's function of the
  *     reference's Poisson example (examples/poissonSolver.cpp) normalised by
  *     1/n^3; then F_i = -(phi(x+e_i) - phi(x-e_i)) / (2 res), periodic,
- *     ready for lf2_gather_kick.  phi (1 component) may be NULL. */
+ *     ready for lf2_gather_kick.  phi (1 component) may be NULL.  Lattices up
+ *     to 1024^3 (LF2_ERR_ARG beyond). */
 lf2_status lf2_kfield_create(lf2_ctx* ctx, int comps, lf2_kfield* out);
 lf2_status lf2_kfield_destroy(lf2_ctx* ctx, lf2_kfield k);
 lf2_status lf2_kfield_export(lf2_ctx* ctx, lf2_kfield k, void* dst,

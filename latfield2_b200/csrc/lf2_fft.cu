@@ -117,9 +117,22 @@ lf2_status ensure_scratch(lf2_ctx* c, bool real_too)
 
 // K[kz][ky][kx] *= coef / (s2(kx) + s2(ky) + s2(kz)), s2(k) = sin^2(pi k / n),
 // K_0 = 0.  coef = -coupling res^2 / (4 N) turns the unnormalised transform
-// of rho into the normalised potential phi_k.  One CTA walks rows (kz, ky);
-// the n values of s2 sit in a shared table (4 n bytes of dynamic shared
-// memory), so no transcendental or 64-bit division runs per element.
+// of rho into the normalised potential phi_k.  The n values of s2 sit in a
+// shared table (4 n bytes of dynamic shared memory).  Each thread takes two
+// consecutive complex values (one 16-byte access; n^2 (n/2+1) is even for
+// even n, and an odd n takes the last value alone) and GREEN_ITEMS such pairs
+// at once, so several loads are in flight before the first store.
+constexpr int GREEN_ITEMS = 4;
+
+__device__ __forceinline__ float green_factor(const float* s2tab, uint32_t i, int n, int nkx,
+                                              float coef)
+{
+  const uint32_t row = i / (uint32_t)nkx;
+  const int kx = (int)(i - row * (uint32_t)nkx);
+  const int ky = (int)(row % (uint32_t)n), kz = (int)(row / (uint32_t)n);
+  return i == 0 ? 0.0f : coef / (s2tab[kx] + (s2tab[ky] + s2tab[kz]));
+}
+
 __global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
 {
   extern __shared__ float s2tab[];
@@ -129,21 +142,38 @@ __global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
     s2tab[i] = s * s;
   }
   __syncthreads();
-  const int rows = n * n;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-    const int ky = row % n, kz = row / n;
-    const float syz = s2tab[ky] + s2tab[kz];
-    float2* Kr = K + (int64_t)row * nkx;
-    for (int kx = threadIdx.x; kx < nkx; kx += blockDim.x) {
-      const float f = (row == 0 && kx == 0) ? 0.0f : coef / (s2tab[kx] + syz);
-      const float2 v = Kr[kx];
-      Kr[kx] = make_float2(v.x * f, v.y * f);
+  const uint32_t total = (uint32_t)n * (uint32_t)n * (uint32_t)nkx;
+  const uint32_t pairs = total / 2;
+  float4* K4 = reinterpret_cast<float4*>(K);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p0 = blockIdx.x * blockDim.x + threadIdx.x; p0 < pairs;
+       p0 += stride * GREEN_ITEMS) {
+    float4 v[GREEN_ITEMS];
+#pragma unroll
+    for (int j = 0; j < GREEN_ITEMS; j++) {
+      const uint32_t p = p0 + j * stride;
+      if (p < pairs) v[j] = K4[p];
     }
+#pragma unroll
+    for (int j = 0; j < GREEN_ITEMS; j++) {
+      const uint32_t p = p0 + j * stride;
+      if (p >= pairs) continue;
+      const float f0 = green_factor(s2tab, 2 * p, n, nkx, coef);
+      const float f1 = green_factor(s2tab, 2 * p + 1, n, nkx, coef);
+      K4[p] = make_float4(v[j].x * f0, v[j].y * f0, v[j].z * f1, v[j].w * f1);
+    }
+  }
+  if ((total & 1u) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const float f = green_factor(s2tab, total - 1, n, nkx, coef);
+    const float2 v = K[total - 1];
+    K[total - 1] = make_float2(v.x * f, v.y * f);
   }
 }
 
 // F_c = (phi(x - e_c) - phi(x + e_c)) * inv_2res, periodic, component-major.
-// One CTA walks x-rows (z, y); threads run along x.
+// One CTA walks x-rows (z, y).  VEC: each thread takes four consecutive x
+// with 16-byte loads and stores (n0 a multiple of 4); otherwise one x.
+template <bool VEC>
 __global__ void k_gradient(const float* __restrict__ phi, float* __restrict__ F, Geom g,
                            float inv_2res)
 {
@@ -160,11 +190,32 @@ __global__ void k_gradient(const float* __restrict__ phi, float* __restrict__ F,
     const float* pzp = phi + ((int64_t)zp * n1 + y) * n0;
     const float* pzm = phi + ((int64_t)zm * n1 + y) * n0;
     float* f0 = F + (int64_t)row * n0;
-    for (int x = threadIdx.x; x < n0; x += blockDim.x) {
-      const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
-      f0[x] = (pr[xm] - pr[xp]) * inv_2res;
-      f0[ns + x] = (pym[x] - pyp[x]) * inv_2res;
-      f0[2 * ns + x] = (pzm[x] - pzp[x]) * inv_2res;
+    if (VEC) {
+      for (int x = 4 * threadIdx.x; x < n0; x += 4 * blockDim.x) {
+        const float4 c = *reinterpret_cast<const float4*>(pr + x);
+        const float lft = pr[x == 0 ? n0 - 1 : x - 1];
+        const float rgt = pr[x + 4 == n0 ? 0 : x + 4];
+        const float4 a = *reinterpret_cast<const float4*>(pym + x);
+        const float4 b = *reinterpret_cast<const float4*>(pyp + x);
+        const float4 d = *reinterpret_cast<const float4*>(pzm + x);
+        const float4 e = *reinterpret_cast<const float4*>(pzp + x);
+        *reinterpret_cast<float4*>(f0 + x) =
+            make_float4((lft - c.y) * inv_2res, (c.x - c.z) * inv_2res, (c.y - c.w) * inv_2res,
+                        (c.z - rgt) * inv_2res);
+        *reinterpret_cast<float4*>(f0 + ns + x) =
+            make_float4((a.x - b.x) * inv_2res, (a.y - b.y) * inv_2res, (a.z - b.z) * inv_2res,
+                        (a.w - b.w) * inv_2res);
+        *reinterpret_cast<float4*>(f0 + 2 * ns + x) =
+            make_float4((d.x - e.x) * inv_2res, (d.y - e.y) * inv_2res, (d.z - e.z) * inv_2res,
+                        (d.w - e.w) * inv_2res);
+      }
+    } else {
+      for (int x = threadIdx.x; x < n0; x += blockDim.x) {
+        const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+        f0[x] = (pr[xm] - pr[xp]) * inv_2res;
+        f0[ns + x] = (pym[x] - pyp[x]) * inv_2res;
+        f0[2 * ns + x] = (pzm[x] - pzp[x]) * inv_2res;
+      }
     }
   }
 }
@@ -342,21 +393,29 @@ lf2_status lf2_pm_force(lf2_ctx* c, lf2_field rho, lf2_field phi, lf2_field F, d
   if (!c || !field_ok(rho, 1) || !field_ok(F, 3) || (phi && !field_ok(phi, 1)))
     return LF2_ERR_ARG;
   FFT_TRY(ensure_plans(c));
+  if (c->g.n[0] > 1024)
+    return fft_fail(c, LF2_ERR_ARG, "lf2_pm_force: lattices up to 1024^3 (32-bit k indices)");
   FFT_TRY(ensure_scratch(c, phi == nullptr));
   float* p = phi ? phi->data : c->fft_phi;
   const int n = c->g.n[0], nkx = n / 2 + 1;
   FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, rho->data, reinterpret_cast<cufftComplex*>(c->fft_k)));
   const float coef = (float)(-coupling * c->res * c->res / (4.0 * (double)c->g.nsites));
-  const int rows = n * n;
+  const int64_t pairs = (int64_t)n * n * nkx / 2;
   c->launches += 1;
-  k_green<<<rows < 148 * 8 ? rows : 148 * 8, 256, sizeof(float) * n, c->stream>>>(
-      reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
+  k_green<<<grid_for((pairs + GREEN_ITEMS - 1) / GREEN_ITEMS, 256), 256, sizeof(float) * n,
+            c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
   FFT_CUDA(c, cudaGetLastError());
   FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), p));
   c->launches += 1;
   const int grows = c->g.n[1] * c->g.n[2];
-  k_gradient<<<grows < 148 * 8 ? grows : 148 * 8, 256, 0, c->stream>>>(p, F->data, c->g,
-                                                                        (float)(0.5 / c->res));
+  const unsigned gblocks = grows < 148 * 8 ? grows : 148 * 8;
+  const bool vec = c->g.n[0] % 4 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(F->data) & 15) == 0;
+  const int gthreads = vec ? 128 : 256;
+  if (vec)
+    k_gradient<true><<<gblocks, gthreads, 0, c->stream>>>(p, F->data, c->g, (float)(0.5 / c->res));
+  else
+    k_gradient<false><<<gblocks, gthreads, 0, c->stream>>>(p, F->data, c->g, (float)(0.5 / c->res));
   FFT_CUDA(c, cudaGetLastError());
   return LF2_OK;
 }

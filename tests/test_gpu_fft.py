@@ -99,8 +99,11 @@ def test_fft_and_poisson_match_the_reference(cuda, path):
     assert normalized_error(phi.export()[..., 0] * n ** 3, g["poisson"]) < 1e-5
 
 
-@pytest.mark.parametrize("n", [16, 64])
+@pytest.mark.parametrize("n", [9, 10, 16, 64])
 def test_pm_force_matches_oracle(cuda, n):
+    """n = 9: an odd count of k values (the Green's function's last value
+    alone) and the one-site gradient path; n = 10: the one-site gradient path;
+    16, 64: the four-site path."""
     cell, off, vel = small_case((n, n, n), 20 * n ** 3 // 8, seed=3, clustered=True)
     ctx = _ctx(n)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / cell.shape[0])
@@ -137,6 +140,24 @@ def test_pm_force_at_size(cuda):
     for c in range(3):
         assert normalized_error(f[..., c], want_F[c]) < 1e-5, c
     assert np.abs(f.reshape(-1, 3).sum(axis=0)).max() < 1e-6 * np.abs(f).sum() / 3
+
+
+def test_pm_force_into_a_misaligned_field(cuda):
+    """A force field wrapped at an address that is not 16-byte aligned takes
+    the one-site gradient path and gives the same result."""
+    import torch
+    n = 32
+    cell, off, vel = small_case((n, n, n), 40000, seed=8, clustered=True)
+    ctx = _ctx(n)
+    ctx.set_particles(cell, off, vel, global_mass=1.0 / cell.shape[0])
+    rho = ctx.field(1)
+    ctx.deposit_scalar(rho)
+    F = ctx.field(3)
+    ctx.pm_force(rho, F, 1.0)
+    buf = torch.zeros(3 * n ** 3 + 1, dtype=torch.float32, device="cuda")
+    Fm = ctx.field(3, buf[1:])
+    ctx.pm_force(rho, Fm, 1.0)
+    np.testing.assert_array_equal(Fm.export(), F.export())
 
 
 def test_non_cubic_lattice_is_refused(cuda):
