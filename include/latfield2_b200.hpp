@@ -15,6 +15,9 @@
  *   F(x, c) = ...;  F.updateHalo();                      LATfield2_Field_decl.hpp:889-935
  *   parts.updateVel(cic_gather_kick, dtau, &Fp, 1);      LATfield2_Particles.hpp:752-893
  *   parts.moveParticles(move_particles_simple, dtau);    :1810-2803, move_function.hpp:15-32
+ *   latK.initializeRealFFT(lat, 0); rKSite k(latK);      LATfield2_Lattice.hpp:225-258
+ *   PlanFFT<Imag> plan(&rho, &rhoK);                      LATfield2_PlanFFT_decl.hpp:83-230
+ *   plan.execute(FFT_FORWARD); plan.execute(FFT_BACKWARD); :720-1050
  *
  * Where the data live:
  *   - Particles live on the GPU.  addParticle_global stages them on the host;
@@ -36,7 +39,8 @@
  *
  * Errors of the C ABI are raised as std::runtime_error carrying
  * lf2_last_error(); the reference exits or throws in the same places.
- * One GPU, one process: the MPI process grid of the reference is 1 x 1.
+ * One GPU, one process: the MPI process grid of the reference is 1 x 1
+ * (`parallel` is a one-process stand-in).
  */
 #ifndef LATFIELD2_B200_HPP
 #define LATFIELD2_B200_HPP
@@ -102,6 +106,87 @@ float mass_of(const T&, std::false_type)
 
 }  // namespace lf2detail
 
+// --------------------------------------------------------------------- Imag
+// Complex number of two Reals with the reference's operators (Imag.hpp:
+// 17-113).  As there, `Real - Imag` keeps the imaginary part's sign
+// (Imag.hpp:66) and `Imag / Imag` divides by the squared norm.
+class Imag {
+ public:
+  Imag() : data{0, 0} {}
+  Imag(Real a, Real b) : data{a, b} {}
+  Imag operator-() const { return Imag(-data[0], -data[1]); }
+  Imag operator+(Imag z) const { return Imag(data[0] + z.data[0], data[1] + z.data[1]); }
+  Imag operator-(Imag z) const { return Imag(data[0] - z.data[0], data[1] - z.data[1]); }
+  Imag operator*(Imag z) const
+  {
+    return Imag(data[0] * z.data[0] - data[1] * z.data[1], data[0] * z.data[1] + data[1] * z.data[0]);
+  }
+  Imag operator/(Imag z) const
+  {
+    const Real q = z.norm();
+    return Imag((data[0] * z.data[0] + data[1] * z.data[1]) / q,
+                (data[1] * z.data[0] - data[0] * z.data[1]) / q);
+  }
+  void operator=(Real r) { data[0] = r, data[1] = 0; }
+  friend Imag operator+(Imag z, Real a) { return Imag(z.data[0] + a, z.data[1]); }
+  friend Imag operator+(Real a, Imag z) { return Imag(z.data[0] + a, z.data[1]); }
+  friend Imag operator-(Imag z, Real a) { return Imag(z.data[0] - a, z.data[1]); }
+  friend Imag operator-(Real a, Imag z) { return Imag(a - z.data[0], z.data[1]); }
+  friend Imag operator*(Imag z, Real a) { return Imag(z.data[0] * a, z.data[1] * a); }
+  friend Imag operator*(Real a, Imag z) { return Imag(z.data[0] * a, z.data[1] * a); }
+  friend Imag operator/(Imag z, Real a) { return Imag(z.data[0] / a, z.data[1] / a); }
+  void operator+=(Imag z) { data[0] += z.data[0], data[1] += z.data[1]; }
+  void operator-=(Imag z) { data[0] -= z.data[0], data[1] -= z.data[1]; }
+  void operator*=(Imag z) { *this = *this * z; }
+  void operator+=(Real a) { data[0] += a; }
+  void operator-=(Real a) { data[0] -= a; }
+  void operator*=(Real a) { data[0] *= a, data[1] *= a; }
+  void operator/=(Real a) { data[0] /= a, data[1] /= a; }
+  Real& real() { return data[0]; }
+  Real& imag() { return data[1]; }
+  Real real() const { return data[0]; }
+  Real imag() const { return data[1]; }
+  Real norm() const { return data[0] * data[0] + data[1] * data[1]; }
+  Imag conj() const { return Imag(data[0], -data[1]); }
+  Real phase() const
+  {
+    return std::acos(data[0] / std::sqrt(norm())) * (data[1] < 0 ? -1 : 1);
+  }
+  friend Imag expi(Real x) { return Imag(std::cos(x), std::sin(x)); }
+  friend std::ostream& operator<<(std::ostream& os, const Imag& z)
+  {
+    return os << z.data[0] << " + i" << z.data[1];
+  }
+
+ private:
+  Real data[2];
+};
+
+// ----------------------------------------------------------------- parallel
+// The reference's process grid (LATfield2_parallel2d_decl.hpp) reduced to one
+// process: the whole lattice is local, reductions over processes are the
+// identity.  initialize(n, m) accepts only a 1 x 1 grid.
+class Parallel2d {
+ public:
+  void initialize(int proc0, int proc1)
+  {
+    if (proc0 * proc1 != 1)
+      throw std::invalid_argument("parallel.initialize: one GPU runs a 1 x 1 process grid");
+  }
+  bool isRoot() const { return true; }
+  int rank() const { return 0; }
+  int size() const { return 1; }
+  int root() const { return 0; }
+  void barrier() const {}
+  template <class T>
+  void sum(T&) const {}
+  template <class T>
+  void max(T&) const {}
+  template <class T>
+  void min(T&) const {}
+};
+inline Parallel2d parallel;  // C++17 inline variable: one object per program
+
 // ------------------------------------------------------------------ Lattice
 // 3-D periodic lattice of size[0] x size[1] x size[2] sites with a halo of
 // `halo` sites (LATfield2_Lattice_decl.hpp:17-135).  One process: the local
@@ -121,6 +206,17 @@ class Lattice {
   {
     const int s[3] = {size, size, size};
     initialize(dim, s, halo);
+  }
+  // The lattice of the Fourier transform of a real field on the cubic
+  // lattice `lat_real`: sizes (n/2+1, n, n) (Lattice::initializeRealFFT,
+  // LATfield2_Lattice.hpp:225-258).
+  void initializeRealFFT(Lattice& lat_real, int halo)
+  {
+    const int n = lat_real.size(0);
+    if (lat_real.size(1) != n || lat_real.size(2) != n)
+      throw std::invalid_argument("Lattice::initializeRealFFT: the real lattice is not cubic");
+    const int s[3] = {n / 2 + 1, n, n};
+    initialize(3, s, halo);
   }
   int dim() { return 3; }
   int halo() { return halo_; }
@@ -209,7 +305,7 @@ class Site {
   }
   Lattice& lattice() const { return *lat_; }
 
- private:
+ protected:
   void reindex()
   {
     const int h = lat_->halo();
@@ -220,6 +316,26 @@ class Site {
   int c_[3] = {0, 0, 0};
 };
 
+// ------------------------------------------------------------------- rKSite
+// A site of the Fourier lattice of initializeRealFFT.  Its storage dims are
+// (k_x, k_z, k_y); coord(1) returns k_y and coord(2) returns k_z, and
+// operator+/- and setCoord take directions in the same (x, y, z) sense
+// (LATfield2_Site.hpp:319-416).
+class rKSite : public Site {
+ public:
+  rKSite() {}
+  explicit rKSite(Lattice& lattice) : Site(lattice) {}
+  rKSite(Lattice& lattice, long index) : Site(lattice, index) {}
+  int coord(int direction) const { return Site::coord(storage_dim(direction)); }
+  rKSite operator+(int direction) const { return rKSite(Site::operator+(storage_dim(direction))); }
+  rKSite operator-(int direction) const { return rKSite(Site::operator-(storage_dim(direction))); }
+  bool setCoord(int x, int y, int z) { return Site::setCoord(x, z, y); }
+
+ private:
+  explicit rKSite(const Site& s) : Site(s) {}
+  static int storage_dim(int direction) { return direction == 0 ? 0 : 3 - direction; }
+};
+
 // -------------------------------------------------------------------- Field
 // A field of Real on a lattice: `components` values per site, or a rows x
 // cols matrix (symmetric: rows*(rows+1)/2 values, order 00,01,02,11,12,22
@@ -227,8 +343,8 @@ class Site {
 // laid out like the reference's: halo'd sites, components interleaved.
 template <class FieldType>
 class Field {
-  static_assert(std::is_same<FieldType, Real>::value,
-                "the GPU path provides Field<Real> only");
+  static_assert(std::is_same<FieldType, Real>::value || std::is_same<FieldType, Imag>::value,
+                "the GPU path provides Field<Real> and Field<Imag> (Fourier space)");
 
  public:
   Field() {}
@@ -258,7 +374,7 @@ class Field {
   void alloc()
   {
     if ((long)data_.size() != lat_->sitesGross() * components_)
-      data_.assign((size_t)(lat_->sitesGross() * components_), FieldType(0));
+      data_.assign((size_t)(lat_->sitesGross() * components_), FieldType());
   }
   void dealloc()
   {
@@ -301,6 +417,7 @@ class Field {
   // the field's device copy whatever the order of destruction.
   lf2_field lf2_handle(const std::shared_ptr<lf2_ctx>& owner, bool upload = true)
   {
+    static_assert(std::is_same<FieldType, Real>::value, "device copies exist for Field<Real>");
     lf2_ctx* ctx = owner.get();
     if (ctx_ != ctx) {
       if (ctx_ && device_newer_) pull();
@@ -324,6 +441,8 @@ class Field {
     device_newer_ = true;
     host_newer_ = false;
   }
+  // the context of the field's device copy (empty before the first GPU use)
+  const std::shared_ptr<lf2_ctx>& lf2_context_owner() const { return owner_; }
   // device copy -> host array (halo filled periodically)
   void pull()
   {
@@ -377,6 +496,147 @@ class Field {
   lf2_field dev_ = nullptr;
   bool host_newer_ = true;
   bool device_newer_ = false;
+};
+
+// ------------------------------------------------------------------ PlanFFT
+// LATfield2_PlanFFT.hpp:14-17
+const int FFT_FORWARD = 1;
+const int FFT_BACKWARD = -1;
+const int FFT_IN_PLACE = 16;
+const int FFT_OUT_OF_PLACE = -16;
+
+// Real-to-complex transforms between a Field<Real> on a cubic lattice and a
+// Field<Imag> on the lattice of initializeRealFFT (LATfield2_PlanFFT_decl.hpp:
+// 83-230, :720-1050), with the reference's storage order and normalisation
+// (neither direction normalised).  execute() runs on the GPU (lf2_fft_forward,
+// lf2_fft_backward) and leaves its result in the output field's host array, as
+// the reference does.  The plan uses the real field's GPU context when it
+// already has one (a field used by particle operations), otherwise a context
+// of its own.  FFT_IN_PLACE (one array shared by both fields in the reference)
+// gives the same values; the two fields keep separate arrays here.
+template <class compType>
+class PlanFFT {
+  static_assert(std::is_same<compType, Imag>::value, "PlanFFT<Imag> is provided");
+
+ public:
+  PlanFFT() {}
+  PlanFFT(Field<Real>* rfield, Field<Imag>* kfield, const int mem_type = FFT_OUT_OF_PLACE)
+  {
+    initialize(rfield, kfield, mem_type);
+  }
+  ~PlanFFT() { release(); }
+  PlanFFT(const PlanFFT&) = delete;
+  PlanFFT& operator=(const PlanFFT&) = delete;
+
+  void initialize(Field<Real>* rfield, Field<Imag>* kfield, const int mem_type = FFT_OUT_OF_PLACE)
+  {
+    (void)mem_type;
+    Lattice& lr = rfield->lattice();
+    Lattice& lk = kfield->lattice();
+    const int n = lr.size(0);
+    if (lr.size(1) != n || lr.size(2) != n)
+      throw std::invalid_argument("PlanFFT::initialize: the real lattice is not cubic");
+    if (lk.size(0) != n / 2 + 1 || lk.size(1) != n || lk.size(2) != n)
+      throw std::invalid_argument("PlanFFT::initialize: the Fourier lattice is not initializeRealFFT's");
+    if (rfield->components() != kfield->components())
+      throw std::invalid_argument("PlanFFT::initialize: the fields have different numbers of components");
+    release();
+    r_ = rfield;
+    k_ = kfield;
+  }
+
+  void execute(int fft_type)
+  {
+    if (!r_) throw std::logic_error("PlanFFT::execute: plan not initialised");
+    if (fft_type != FFT_FORWARD && fft_type != FFT_BACKWARD)
+      throw std::invalid_argument("PlanFFT::execute: FFT_FORWARD or FFT_BACKWARD");
+    bind();
+    lf2_ctx* ctx = owner_.get();
+    lf2_field rd = r_->lf2_handle(owner_, fft_type == FFT_FORWARD);
+    if (fft_type == FFT_FORWARD) {
+      lf2detail::check(ctx, lf2_fft_forward(ctx, rd, kdev_), "lf2_fft_forward");
+      k_to_host();
+    } else {
+      k_to_device();
+      lf2detail::check(ctx, lf2_fft_backward(ctx, kdev_, rd), "lf2_fft_backward");
+      r_->mark_device_written();
+      r_->pull();
+    }
+  }
+
+ private:
+  void bind()
+  {
+    if (!owner_) {
+      owner_ = r_->lf2_context_owner();
+      if (!owner_) {
+        const int n = r_->lattice().size(0);
+        const int ns[3] = {n, n, n};
+        const double box[3] = {1.0, 1.0, 1.0};
+        lf2_ctx* c = nullptr;
+        lf2detail::check(nullptr, lf2_create(&c, 0, ns, box, LF2_DEPOSIT_FP32, nullptr), "lf2_create");
+        owner_.reset(c, [](lf2_ctx* p) { lf2_destroy(p); });
+      }
+    }
+    if (!kdev_)
+      lf2detail::check(owner_.get(), lf2_kfield_create(owner_.get(), k_->components(), &kdev_),
+                       "lf2_kfield_create");
+  }
+  // the k-field without halo, in the reference's order, <-> the host array
+  // of k_ (which may have a halo)
+  void k_to_host()
+  {
+    lf2_ctx* ctx = owner_.get();
+    Lattice& lk = k_->lattice();
+    if (lk.halo() == 0) {
+      lf2detail::check(ctx, lf2_kfield_export(ctx, kdev_, k_->data(), sizeof(Real), LF2_PTR_HOST),
+                       "lf2_kfield_export");
+      return;
+    }
+    std::vector<Imag> tmp((size_t)lk.sites() * k_->components());
+    lf2detail::check(ctx, lf2_kfield_export(ctx, kdev_, tmp.data(), sizeof(Real), LF2_PTR_HOST),
+                     "lf2_kfield_export");
+    copy_halo(tmp, true);
+  }
+  void k_to_device()
+  {
+    lf2_ctx* ctx = owner_.get();
+    Lattice& lk = k_->lattice();
+    if (lk.halo() == 0) {
+      lf2detail::check(ctx, lf2_kfield_import(ctx, kdev_, k_->data(), sizeof(Real), LF2_PTR_HOST),
+                       "lf2_kfield_import");
+      return;
+    }
+    std::vector<Imag> tmp((size_t)lk.sites() * k_->components());
+    copy_halo(tmp, false);
+    lf2detail::check(ctx, lf2_kfield_import(ctx, kdev_, tmp.data(), sizeof(Real), LF2_PTR_HOST),
+                     "lf2_kfield_import");
+  }
+  void copy_halo(std::vector<Imag>& flat, bool to_field)
+  {
+    Lattice& lk = k_->lattice();
+    const int comps = k_->components();
+    Site s(lk);
+    long i = 0;
+    for (s.first(); s.test(); s.next(), i++)
+      for (int c = 0; c < comps; c++) {
+        Imag& f = (*k_)(s, c);
+        Imag& t = flat[(size_t)(i * comps + c)];
+        if (to_field) f = t;
+        else t = f;
+      }
+  }
+  void release()
+  {
+    if (kdev_ && owner_) lf2_kfield_destroy(owner_.get(), kdev_);
+    kdev_ = nullptr;
+    owner_.reset();
+  }
+
+  Field<Real>* r_ = nullptr;
+  Field<Imag>* k_ = nullptr;
+  std::shared_ptr<lf2_ctx> owner_;
+  lf2_kfield kdev_ = nullptr;
 };
 
 // ---------------------------------------------------------- particle types

@@ -1,7 +1,8 @@
-"""Builds tests/compat/compat_demo.cpp against include/latfield2_b200.hpp and
+"""Builds a demo of tests/compat/ (compat_demo.cpp, the particle path;
+poisson_demo.cpp, the FFT path) against include/latfield2_b200.hpp and
 liblf2gpu.so (no GPU needed to build):
 
-    python tests/compat/build_demo.py [--single] [--out PATH]
+    python tests/compat/build_demo.py [--single] [--source NAME.cpp] [--out PATH]
 """
 import argparse
 import os
@@ -12,12 +13,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
-def build(out, single=False):
+def build(out, single=False, source="compat_demo.cpp"):
     sys.path.insert(0, ROOT)
     from latfield2_b200 import build as B
     lib = B.build()
     cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
-           os.path.join(HERE, "compat_demo.cpp"), "-o", out, "-L", os.path.dirname(lib), "-llf2gpu",
+           os.path.join(HERE, source), "-o", out, "-L", os.path.dirname(lib), "-llf2gpu",
            "-Wl,-rpath," + os.path.dirname(lib)]
     if single:
         cmd.insert(1, "-DSINGLE")
@@ -28,6 +29,8 @@ def build(out, single=False):
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--single", action="store_true")
-    ap.add_argument("--out", default=os.path.join(HERE, "compat_demo"))
+    ap.add_argument("--source", default="compat_demo.cpp")
+    ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    print(build(a.out, a.single))
+    out = a.out or os.path.join(HERE, os.path.splitext(a.source)[0])
+    print(build(out, a.single, a.source))
