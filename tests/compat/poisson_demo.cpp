@@ -2,7 +2,7 @@
 // (Lattice::initializeRealFFT, rKSite, Field<Imag>, PlanFFT<Imag>), built
 // against include/latfield2_b200.hpp (the GPU path) instead of LATfield2.hpp.
 //
-//   poisson_demo N OUT
+//   poisson_demo N OUT [KHALO]
 //
 // rho is a smooth periodic density (two Gaussian bumps on a constant); phi_k
 // is rho_k divided by the eigenvalue of the 7-point lattice Laplacian, the
@@ -29,17 +29,18 @@ static void put(FILE* fp, const std::vector<double>& v)
 
 int main(int argc, char** argv)
 {
-  if (argc != 3) {
-    fprintf(stderr, "usage: poisson_demo N OUT\n");
+  if (argc != 3 && argc != 4) {
+    fprintf(stderr, "usage: poisson_demo N OUT [KHALO]\n");
     return 2;
   }
   const int N = atoi(argv[1]);
+  const int khalo = argc == 4 ? atoi(argv[3]) : 0;  // halo of the Fourier lattice
   const double res = 1.0 / N;
   parallel.initialize(1, 1);
 
   Lattice lat(3, N, 1);
   Lattice latK;
-  latK.initializeRealFFT(lat, 0);
+  latK.initializeRealFFT(lat, khalo);
   Field<Real> rho(lat, 1), phi(lat, 1);
   Field<Imag> rhoK(latK, 1), phiK(latK, 1);
   PlanFFT<Imag> planRho(&rho, &rhoK);

@@ -98,7 +98,8 @@ def test_demo_matches_the_python_binding(cuda, tmp_path):
 
 
 @pytest.mark.gpu
-def test_poisson_demo_matches_the_oracle(cuda, tmp_path):
+@pytest.mark.parametrize("khalo", [0, 1])
+def test_poisson_demo_matches_the_oracle(cuda, tmp_path, khalo):
     """The reference-style Poisson program (rKSite loop, PlanFFT forward and
     backward, updateHalo) on the GPU path: its rho_k is the oracle's forward
     transform in the reference's storage order, its phi the oracle's Poisson
@@ -108,7 +109,8 @@ def test_poisson_demo_matches_the_oracle(cuda, tmp_path):
     exe = build_demo.build(str(tmp_path / "poisson"), False, "poisson_demo.cpp")
     out = str(tmp_path / "poisson.bin")
     n = 32
-    r = subprocess.run([exe, str(n), out], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([exe, str(n), out, str(khalo)], capture_output=True, text=True,
+                       timeout=300)
     assert r.returncode == 0, r.stderr
     assert float(r.stdout.split()[3]) < 1e-4, r.stdout
     (hdr, rho, rhok, phi) = _read(out)
