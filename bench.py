@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -82,7 +83,9 @@ def peaks():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi sampling during the timed region (read-only query)."""
+    """nvidia-smi sampling during the timed region (read-only query).  The raw
+    samples go to LF2_CLOCKS_DIR (default: the system temp directory); the
+    JSON line carries their summary."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -90,7 +93,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(os.environ.get("LF2_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"lf2_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
