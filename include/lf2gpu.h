@@ -103,6 +103,27 @@ lf2_status lf2_particles_set_pos(lf2_ctx* ctx, int64_t n, const void* pos3,
                                  const void* vel3, int real_bytes,
                                  const float* mass, double global_mass,
                                  const int64_t* id);
+/* Slab decomposition (one rank per GPU, z split across ranks, one ghost
+ * cell plane below and above the rank's own planes): the particle
+ * migration of moveParticles (LATfield2_Particles.hpp:2176-2799) as two
+ * local operations around the exchange.
+ *   extract_z: every particle whose cell z lies outside [z_lo, z_hi] leaves
+ *     the store and is written (any order) as cell index, offsets (3 per
+ *     particle), velocities (3), mass and id, to DEVICE arrays of `capacity`
+ *     entries.  mass / id must be given exactly when the store carries them
+ *     (capacity 0: a count only, all arrays may be NULL).  *n_out receives
+ *     the number of such particles; when it exceeds capacity, nothing
+ *     changes and LF2_ERR_ARG is returned.
+ *   add: particles in the same format (host or device arrays) join the store;
+ *     a cell or offset out of range gives LF2_ERR_ARG and adds nothing.  The
+ *     store must exist (lf2_particles_set, possibly with 0 particles). */
+lf2_status lf2_particles_extract_z(lf2_ctx* ctx, int z_lo, int z_hi,
+                                   int64_t capacity, int32_t* cell, float* off3,
+                                   float* vel3, float* mass, int64_t* id,
+                                   int64_t* n_out);
+lf2_status lf2_particles_add(lf2_ctx* ctx, int64_t n, const int32_t* cell,
+                             const float* off3, const float* vel3,
+                             const float* mass, const int64_t* id, int ptr_kind);
 /* Particles::numParticles (LATfield2_Particles.hpp:316-320). */
 lf2_status lf2_particles_count(lf2_ctx* ctx, int64_t* n);
 /* Downloads the particles in storage order (brick by brick).  Any output

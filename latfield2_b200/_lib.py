@@ -65,6 +65,10 @@ SIGNATURES = {
     "lf2_deposit_symtensor_cicngp": [c_void_p, c_void_p],
     "lf2_deposit_vector_cic": [c_void_p, c_void_p],
     "lf2_deposit_vecvec_cic": [c_void_p, c_void_p],
+    "lf2_particles_extract_z": [c_void_p, c_int, c_int, c_i64, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p, P(c_i64)],
+    "lf2_particles_add": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                          c_int],
     "lf2_kfield_create": [c_void_p, c_int, P(c_void_p)],
     "lf2_kfield_destroy": [c_void_p, c_void_p],
     "lf2_kfield_export": [c_void_p, c_void_p, c_void_p, c_int, c_int],

@@ -145,6 +145,7 @@ class Context:
         self.nsites = self.n[0] * self.n[1] * self.n[2]
         self.res = self.box[0] / self.n[0]
         self.mode = mode
+        self.device = int(device)
         lib = _lib.load()
         h = _c.c_void_p()
         na = (_c.c_int * 3)(*self.n)
@@ -218,6 +219,44 @@ class Context:
         self._check(_lib.load().lf2_particles_get_pos(
             self.h, _ptr(pos)[0], _ptr(vel)[0], pos.itemsize, _ptr(i)[0]), "particles_get_pos")
         return (pos, vel, i) if ids else (pos, vel)
+
+    def extract_z(self, z_lo, z_hi, mass=False, ids=False):
+        """Removes every particle whose cell z lies outside [z_lo, z_hi] and
+        returns them as CUDA tensors {cell, off, vel[, mass][, id]} (the
+        migration step of a slab decomposition)."""
+        import torch
+        lib = _lib.load()
+        dev = torch.device("cuda", self.device)
+        n = _c.c_int64()
+        st = lib.lf2_particles_extract_z(self.h, int(z_lo), int(z_hi), 0, None, None, None, None,
+                                         None, _c.byref(n))
+        if st != 0 and n.value == 0:
+            self._check(st, "extract_z")
+        cap = n.value
+        out = {"cell": torch.empty(cap, dtype=torch.int32, device=dev),
+               "off": torch.empty((cap, 3), dtype=torch.float32, device=dev),
+               "vel": torch.empty((cap, 3), dtype=torch.float32, device=dev)}
+        if mass:
+            out["mass"] = torch.empty(cap, dtype=torch.float32, device=dev)
+        if ids:
+            out["id"] = torch.empty(cap, dtype=torch.int64, device=dev)
+        if cap == 0:
+            return out
+
+        def p(k):
+            return _c.c_void_p(out[k].data_ptr()) if k in out else None
+        self._check(lib.lf2_particles_extract_z(self.h, int(z_lo), int(z_hi), cap, p("cell"),
+                                                p("off"), p("vel"), p("mass"), p("id"),
+                                                _c.byref(n)), "extract_z")
+        return out
+
+    def add_particles(self, cell, off, vel, mass=None, ids=None):
+        """New particles (cell, offsets, velocities[, mass][, ids]) join the
+        store (numpy arrays or CUDA tensors)."""
+        kind = _same_kind(cell, off, vel, mass, ids)
+        self._check(_lib.load().lf2_particles_add(
+            self.h, int(cell.shape[0]), _ptr(cell)[0], _ptr(off)[0], _ptr(vel)[0], _ptr(mass)[0],
+            _ptr(ids)[0], kind), "particles_add")
 
     def cell_counts(self):
         out = np.empty(self.nsites, np.int32)

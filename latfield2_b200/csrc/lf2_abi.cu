@@ -448,6 +448,97 @@ lf2_status lf2_particles_set_pos(lf2_ctx* c, int64_t n, const void* pos3, const 
                      did);
 }
 
+static lf2_status rebin_tail(lf2_ctx* c);
+
+lf2_status lf2_particles_extract_z(lf2_ctx* c, int z_lo, int z_hi, int64_t capacity,
+                                   int32_t* cell, float* off3, float* vel3, float* mass,
+                                   int64_t* id, int64_t* n_out)
+{
+  if (!c || !n_out || capacity < 0 || z_lo > z_hi) return LF2_ERR_ARG;
+  if (capacity > 0 && (!cell || !off3 || !vel3)) return LF2_ERR_ARG;
+  if (capacity > 0 && ((mass != nullptr) != c->has_mass || (id != nullptr) != c->has_id))
+    return fail(c, LF2_ERR_ARG, "extract_z: give mass and id exactly when the store carries them");
+  *n_out = 0;
+  if (c->np == 0) return LF2_OK;
+  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  LF2_CUDA(c, launch_count_outside(c, z_lo, z_hi, c->mov_count));
+  unsigned long long n = 0;
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_i64, c->mov_count, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  memcpy(&n, c->h_i64, sizeof n);
+  *n_out = (int64_t)n;
+  if ((int64_t)n > capacity)
+    return fail(c, LF2_ERR_ARG, "extract_z: " + std::to_string(n) + " particles, capacity " +
+                                    std::to_string(capacity));
+  if (n == 0) return LF2_OK;
+  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  LF2_CUDA(c, launch_extract_outside(c, z_lo, z_hi, cell, off3, vel3, mass, id, c->mov_count));
+  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+  c->np -= (int64_t)n;
+  return LF2_OK;
+}
+
+lf2_status lf2_particles_add(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                             const float* vel3, const float* mass, const int64_t* id,
+                             int ptr_kind)
+{
+  if (!c || n < 0 || (n > 0 && (!cell || !off3 || !vel3))) return LF2_ERR_ARG;
+  if (c->capacity == 0)
+    return fail(c, LF2_ERR_ARG, "particles_add: create the store with lf2_particles_set first");
+  if (n == 0) return LF2_OK;
+  if ((mass != nullptr) != c->has_mass || (id != nullptr) != c->has_id)
+    return fail(c, LF2_ERR_ARG, "particles_add: give mass and id exactly when the store carries them");
+  if (c->np + n >= (1ll << 31)) return fail(c, LF2_ERR_UNSUPPORTED, "more than 2^31-1 particles");
+  Scratch s1(c), s2(c), s3(c), s4(c), s5(c);
+  const int32_t* dc;
+  const float *doff, *dvel, *dmass;
+  const int64_t* did;
+  LF2_TRY(stage_in(c, s1, cell, (size_t)n, ptr_kind, &dc));
+  LF2_TRY(stage_in(c, s2, off3, (size_t)n * 3, ptr_kind, &doff));
+  LF2_TRY(stage_in(c, s3, vel3, (size_t)n * 3, ptr_kind, &dvel));
+  LF2_TRY(stage_in(c, s4, mass, (size_t)n, ptr_kind, &dmass));
+  LF2_TRY(stage_in(c, s5, id, (size_t)n, ptr_kind, &did));
+  // check every input first: nothing changes when one is out of range
+  LF2_CUDA(c, launch_pack_movers(c, n, dc, doff, dvel, dmass, did, false));
+  if (check_flags(c) != LF2_OK) {
+    LF2_CUDA(c, cudaMemsetAsync(c->flags, 0, sizeof(uint32_t), c->stream));
+    return fail(c, LF2_ERR_ARG, "particles_add: a cell index or offset is out of range");
+  }
+  const int64_t total = c->np + n;
+  const int64_t need = total + (total >> 2) + 100 * c->g.nbricks + 1024;
+  if (n <= c->mov_capacity && need <= c->capacity) {
+    // through the mover path: pack, insert
+    LF2_CUDA(c, launch_pack_movers(c, n, dc, doff, dvel, dmass, did, true));
+    LF2_TRY(rebin_tail(c));
+    LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+    c->np = total;
+    return LF2_OK;
+  }
+  // the store is too small: reload the current particles and the new ones
+  Scratch tc(c), to(c), tv(c), tm(c), ti(c), st(c);
+  LF2_CUDA(c, tc.alloc(sizeof(int32_t) * total));
+  LF2_CUDA(c, to.alloc(sizeof(float) * 3 * total));
+  LF2_CUDA(c, tv.alloc(sizeof(float) * 3 * total));
+  if (c->has_mass) LF2_CUDA(c, tm.alloc(sizeof(float) * total));
+  if (c->has_id) LF2_CUDA(c, ti.alloc(sizeof(int64_t) * total));
+  LF2_CUDA(c, st.alloc(sizeof(int64_t) * (c->g.nbricks + 1)));
+  LF2_CUDA(c, launch_scan_counts(c, (int64_t*)st.p));
+  LF2_CUDA(c, launch_get(c, (int64_t*)st.p, (int32_t*)tc.p, (float*)to.p, (float*)tv.p,
+                         (float*)tm.p, (int64_t*)ti.p));
+  const int64_t np0 = c->np;
+  const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+  LF2_CUDA(c, cudaMemcpyAsync((int32_t*)tc.p + np0, dc, sizeof(int32_t) * n, d2d, c->stream));
+  LF2_CUDA(c, cudaMemcpyAsync((float*)to.p + 3 * np0, doff, sizeof(float) * 3 * n, d2d, c->stream));
+  LF2_CUDA(c, cudaMemcpyAsync((float*)tv.p + 3 * np0, dvel, sizeof(float) * 3 * n, d2d, c->stream));
+  if (c->has_mass)
+    LF2_CUDA(c, cudaMemcpyAsync((float*)tm.p + np0, dmass, sizeof(float) * n, d2d, c->stream));
+  if (c->has_id)
+    LF2_CUDA(c, cudaMemcpyAsync((int64_t*)ti.p + np0, did, sizeof(int64_t) * n, d2d, c->stream));
+  return load_device(c, total, (const int32_t*)tc.p, (const float*)to.p, (const float*)tv.p,
+                     (const float*)tm.p, c->gmass, (const int64_t*)ti.p);
+}
+
 lf2_status lf2_particles_count(lf2_ctx* c, int64_t* n)
 {
   if (!c || !n) return LF2_ERR_ARG;

@@ -166,6 +166,17 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
 cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
 
+// lf2_exchange.cu (slab decomposition): particles with cell z outside
+// [zlo, zhi] counted / moved out of the store; new particles into the mover
+// buffer for k_insert
+cudaError_t launch_count_outside(lf2_ctx* c, int zlo, int zhi, unsigned long long* n);
+cudaError_t launch_extract_outside(lf2_ctx* c, int zlo, int zhi, int32_t* cell, float* off3,
+                                   float* vel3, float* mass, int64_t* id,
+                                   unsigned long long* out_count);
+cudaError_t launch_pack_movers(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
+                               const float* vel3, const float* mass, const int64_t* id,
+                               bool write);
+
 // lf2_fft.cu: releases the cuFFT plans and scratch of the context
 void fft_release(lf2_ctx* c);
 

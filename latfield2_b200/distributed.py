@@ -1,0 +1,238 @@
+"""z-slab decomposition of the particle-mesh step over the ranks of a
+torch.distributed process group, one rank per GPU: the multi-GPU form of the
+path (LATfield2's Lattice splits z and y over a 2-D process grid,
+LATfield2_Lattice.hpp:88-94; here z alone is split).
+
+Rank r of R owns the cell planes [z0, z0 + nz) with nz = n2 / R and z0 = r nz.
+Its local lattice is (n0, n1, nz + 2): local plane p is global plane
+z0 + p - 1, so planes 1..nz are its own and planes 0 and nz+1 are ghost
+planes shared with the rank below and the rank above (periodic over the
+ranks).  x and y are not split.  One step does what lf2_step does on one GPU:
+
+  1. ghost planes of the force field: plane nz+1 <- plane 1 of the rank above,
+     plane 0 <- plane nz of the rank below (Field::updateHalo across ranks,
+     LATfield2_Field_decl.hpp:889-935);
+  2. kick, drift and rebin of the local particles in one pass.  A particle
+     moves less than one cell per step, so it ends on an own plane or on a
+     ghost plane.  The check after the pass is max |v| dtau < res (the whole
+     velocity, as the library reports max |v|); a larger move raises, since a
+     particle that left by more than one plane cannot be routed;
+  3. migration: particles on plane 0 go to the rank below (its plane nz),
+     particles on plane nz+1 to the rank above (its plane 1), as
+     moveParticles' exchange (LATfield2_Particles.hpp:2176-2799);
+  4. deposit of the own particles.  Their CIC weights reach vertex planes
+     1..nz+1, and plane nz+1 is added into plane 1 of the rank above: the
+     upper-halo fold of scalarProjectionCIC_comm (projections.hpp:194-300).
+
+Exchanges are point-to-point messages between neighbours (NCCL between GPUs,
+gloo between CPU processes).  A single rank exchanges with itself, which
+gives the periodic single-domain result.  The local work is done by an
+engine: CudaEngine (the library's Context) by default; any object with the
+same methods can stand in (the tests run the exchange logic on CPU processes
+with one).
+"""
+import numpy as np
+
+from . import _lib
+from .core import Context
+
+
+class CudaEngine:
+    """Local work on the GPU through the library's Context."""
+
+    def __init__(self, n_local, res, mode, device=0):
+        import torch
+        self.torch = torch
+        self.n = n_local
+        self.dev = torch.device("cuda", device)
+        box = tuple(res * v for v in n_local)
+        self.ctx = Context(n_local, box=box, mode=mode, device=device)
+        self.res = res
+        self.has_mass = self.has_id = False
+
+    def set_particles(self, cell, off, vel, mass, gmass, ids):
+        self.has_mass, self.has_id = mass is not None, ids is not None
+        self.ctx.set_particles(cell, off, vel, mass=mass, global_mass=gmass, ids=ids)
+
+    def new_field(self, comps):
+        t = self.torch.zeros((comps, self.n[2], self.n[1], self.n[0]), dtype=self.torch.float32,
+                             device=self.dev)
+        return t, self.ctx.field(comps, t)
+
+    def kick_drift(self, F, dtk, dtd):
+        self.ctx.step(F[1], dtk, dtd, None)
+        return self.ctx.last_max_velocity()
+
+    def deposit(self, rho):
+        self.ctx.deposit_scalar(rho[1])
+
+    def extract_outside(self, zlo, zhi):
+        return self.ctx.extract_z(zlo, zhi, mass=self.has_mass, ids=self.has_id)
+
+    def add(self, parts):
+        if int(parts["cell"].shape[0]) == 0:
+            return
+        self.ctx.add_particles(parts["cell"], parts["off"], parts["vel"], parts.get("mass"),
+                               parts.get("id"))
+
+    def particles(self):
+        return self.ctx.get_particles(mass=self.has_mass, ids=self.has_id)
+
+    def count(self):
+        return self.ctx.count()
+
+    def synchronize(self):
+        self.ctx.synchronize()
+
+
+class SlabDomain:
+    """The global lattice n = (n0, n1, n2) split in z over the ranks of
+    `group` (the default torch.distributed group when it is initialised,
+    else one rank).  n2 must be a multiple of the number of ranks."""
+
+    def __init__(self, n, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=None, device=0,
+                 group=None):
+        import torch.distributed as dist
+        self.dist = dist if dist.is_available() and dist.is_initialized() else None
+        self.group = group
+        self.size = self.dist.get_world_size(group) if self.dist else 1
+        self.rank = self.dist.get_rank(group) if self.dist else 0
+        self.n = tuple(int(v) for v in n)
+        if self.n[2] % self.size:
+            raise ValueError(f"n2 = {self.n[2]} is not a multiple of {self.size} ranks")
+        self.nz = self.n[2] // self.size
+        self.z0 = self.rank * self.nz
+        self.res = float(box) / self.n[0]
+        self.local_n = (self.n[0], self.n[1], self.nz + 2)
+        self.plane = self.n[0] * self.n[1]
+        cls = CudaEngine if engine is None else engine
+        self.engine = cls(self.local_n, self.res, mode, device)
+        self.up = (self.rank + 1) % self.size
+        self.down = (self.rank - 1) % self.size
+
+    # ------------------------------------------------------------ messages
+    def _shift(self, send, dst, recv, src):
+        """send -> rank dst while recv <- rank src (one batch; every rank
+        calls it with the same direction)."""
+        if self.size == 1:
+            recv.copy_(send)
+            return
+        ops = [self.dist.P2POp(self.dist.isend, send.contiguous(), dst, self.group),
+               self.dist.P2POp(self.dist.irecv, recv, src, self.group)]
+        for r in self.dist.batch_isend_irecv(ops):
+            r.wait()
+
+    def _shift_parts(self, parts, dst, src):
+        """A particle set (dict of tensors) to rank dst, one from rank src:
+        the counts first, then each array.  An empty array is neither sent
+        nor received (both ends know the count)."""
+        t = self.engine.torch
+        n = int(parts["cell"].shape[0])
+        n_send = t.tensor([n], dtype=t.int64, device=parts["cell"].device)
+        n_recv = t.zeros_like(n_send)
+        self._shift(n_send, dst, n_recv, src)
+        k = int(n_recv.item())
+        out = {}
+        for name in sorted(parts):
+            a = parts[name]
+            recv = t.empty((k,) + tuple(a.shape[1:]), dtype=a.dtype, device=a.device)
+            if self.size == 1:
+                recv.copy_(a)
+            else:
+                ops = []
+                if n:
+                    ops.append(self.dist.P2POp(self.dist.isend, a.contiguous(), dst, self.group))
+                if k:
+                    ops.append(self.dist.P2POp(self.dist.irecv, recv, src, self.group))
+                if ops:
+                    for r in self.dist.batch_isend_irecv(ops):
+                        r.wait()
+            out[name] = recv
+        return out
+
+    def _plane_buf(self, a):
+        t = self.engine.torch
+        return t.empty(tuple(a[:, 0].shape), dtype=a.dtype, device=a.device)
+
+    # ---------------------------------------------------------------- API
+    def set_particles(self, cell, off, vel, global_mass, ids=None):
+        """Global particles (numpy, cell indices of the global lattice); each
+        rank keeps those of its own planes."""
+        cell = np.asarray(cell, np.int64)
+        z = cell // self.plane
+        mine = (z >= self.z0) & (z < self.z0 + self.nz)
+        local = (cell[mine] + (1 - self.z0) * self.plane).astype(np.int32)
+        self.engine.set_particles(local, np.ascontiguousarray(np.asarray(off, np.float32)[mine]),
+                                  np.ascontiguousarray(np.asarray(vel, np.float32)[mine]), None,
+                                  float(global_mass),
+                                  None if ids is None else np.asarray(ids, np.int64)[mine])
+
+    def field(self, comps):
+        """A local field (comps, nz + 2, n1, n0): (array, engine handle)."""
+        return self.engine.new_field(comps)
+
+    def set_own_planes(self, f, global_array):
+        """f's own planes from a global array (comps, n2, n1, n0)."""
+        src = np.asarray(global_array, np.float32)[:, self.z0:self.z0 + self.nz]
+        f[0][:, 1:self.nz + 1] = self.engine.torch.from_numpy(np.ascontiguousarray(src)).to(
+            f[0].device)
+
+    def own_planes(self, f):
+        """f's own planes as numpy (comps, nz, n1, n0)."""
+        return f[0][:, 1:self.nz + 1].cpu().numpy()
+
+    def fill_ghosts(self, f):
+        a = f[0]
+        buf = self._plane_buf(a)
+        self._shift(a[:, 1], self.down, buf, self.up)           # plane nz+1 <- above's plane 1
+        a[:, self.nz + 1] = buf
+        buf = self._plane_buf(a)
+        self._shift(a[:, self.nz], self.up, buf, self.down)      # plane 0 <- below's plane nz
+        a[:, 0] = buf
+
+    def deposit(self, rho):
+        """Scalar CIC deposit of the own particles with the upper-plane fold;
+        the ghost planes of rho end at zero."""
+        self.engine.deposit(rho)
+        a = rho[0]
+        buf = self._plane_buf(a)
+        self._shift(a[:, self.nz + 1], self.up, buf, self.down)
+        a[:, 1] += buf
+        a[:, 0] = 0
+        a[:, self.nz + 1] = 0
+
+    def migrate(self):
+        out = self.engine.extract_outside(1, self.nz)
+        z = out["cell"] // self.plane
+        below = z == 0
+        above = z == self.nz + 1
+        if bool((~(below | above)).any()):
+            raise RuntimeError("a particle left the slab by more than one plane")
+        to_down = {k: v[below] for k, v in out.items()}
+        to_up = {k: v[above] for k, v in out.items()}
+        to_down["cell"] = to_down["cell"] + self.nz * self.plane
+        to_up["cell"] = to_up["cell"] - self.nz * self.plane
+        from_below = self._shift_parts(to_up, self.up, self.down)
+        from_above = self._shift_parts(to_down, self.down, self.up)
+        for p in (from_below, from_above):
+            self.engine.add(p)
+
+    def step(self, F, dtau_kick, dtau_drift, rho=None):
+        """fill_ghosts(F), kick + drift + rebin, migrate, and (rho given) deposit."""
+        self.fill_ghosts(F)
+        vmax = self.engine.kick_drift(F, dtau_kick, dtau_drift)
+        if vmax * dtau_drift / self.res >= 1.0:
+            raise RuntimeError(f"max |v| dtau = {vmax * dtau_drift / self.res:.3f} cells: the "
+                               "slab decomposition moves particles by less than one cell per step")
+        self.migrate()
+        if rho is not None:
+            self.deposit(rho)
+
+    def count(self):
+        return self.engine.count()
+
+    def particles_global(self):
+        """The local particles with global cell indices (numpy dict)."""
+        p = self.engine.particles()
+        p["cell"] = (np.asarray(p["cell"], np.int64) + (self.z0 - 1) * self.plane).astype(np.int32)
+        return p

@@ -1,0 +1,139 @@
+"""GPU side of the slab decomposition: lf2_particles_extract_z and
+lf2_particles_add through the C ABI, and latfield2_b200.distributed.SlabDomain
+on the CUDA engine with one rank (its neighbours are itself), against the
+plain single-GPU path on the same particles.
+
+Particles bit-exact by id (migration moves state, it does not recompute it);
+the density within 1e-6 of its maximum (the fold adds FP32 values).
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(n, mode=1):
+    import latfield2_b200 as L
+    return L.Context(n, box=tuple(v / n[0] for v in n), mode=mode)
+
+
+def _by_id(d):
+    o = np.argsort(d["id"])
+    return {k: np.asarray(v)[o] for k, v in d.items()}
+
+
+def _np(t):
+    return {k: v.cpu().numpy() for k, v in t.items()}
+
+
+def test_extract_and_add_back():
+    n = (32, 24, 40)
+    cell, off, vel = small_case(n, 50000, seed=5)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    ctx = _ctx(n)
+    ctx.set_particles(cell, off, vel, global_mass=1e-5, ids=ids)
+    before = _by_id(ctx.get_particles(ids=True))
+    counts0 = ctx.cell_counts()
+    out = _np(ctx.extract_z(7, 29, ids=True))
+    z = out["cell"] // (n[0] * n[1])
+    assert z.shape[0] > 10000 and np.all((z < 7) | (z > 29))
+    rest = ctx.get_particles(ids=True)
+    zr = rest["cell"] // (n[0] * n[1])
+    assert np.all((zr >= 7) & (zr <= 29))
+    assert ctx.count() == rest["cell"].shape[0] == cell.shape[0] - out["cell"].shape[0]
+    both = {k: np.concatenate([rest[k], out[k]]) for k in ("cell", "off", "vel", "id")}
+    both = _by_id(both)
+    for k in before:
+        np.testing.assert_array_equal(both[k], before[k])
+    # back in (device arrays), and the store is whole again
+    import torch
+    t = {k: torch.from_numpy(v).cuda() for k, v in out.items()}
+    ctx.add_particles(t["cell"], t["off"], t["vel"], ids=t["id"])
+    after = _by_id(ctx.get_particles(ids=True))
+    for k in before:
+        np.testing.assert_array_equal(after[k], before[k])
+    np.testing.assert_array_equal(ctx.cell_counts(), counts0)
+    # nothing outside: an empty result, no change
+    assert _np(ctx.extract_z(0, n[2] - 1, ids=True))["cell"].shape[0] == 0
+    assert ctx.count() == cell.shape[0]
+    # adding nothing is allowed (empty arrays, null pointers)
+    e = _np(ctx.extract_z(0, n[2] - 1, ids=True))
+    ctx.add_particles(e["cell"], e["off"], e["vel"], ids=e["id"])
+    assert ctx.count() == cell.shape[0]
+
+
+def test_add_beyond_the_store_reloads_and_bad_input_adds_nothing():
+    import latfield2_b200 as L
+    n = (32, 32, 32)
+    cell, off, vel = small_case(n, 1000, seed=6)
+    ids = np.arange(1000, dtype=np.int64)
+    ctx = _ctx(n)
+    ctx.set_particles(cell, off, vel, global_mass=1e-3, ids=ids)
+    c2, o2, v2 = small_case(n, 200000, seed=7, clustered=True)
+    ids2 = np.arange(1000, 201000, dtype=np.int64)
+    ctx.add_particles(c2, o2, v2, ids=ids2)
+    got = _by_id(ctx.get_particles(ids=True))
+    np.testing.assert_array_equal(got["id"], np.arange(201000))
+    np.testing.assert_array_equal(got["cell"], np.concatenate([cell, c2]))
+    np.testing.assert_array_equal(got["off"], np.concatenate([off, o2]))
+    bad_cell = np.array([0, n[0] * n[1] * n[2]], np.int32)
+    with pytest.raises(L.LF2Error, match="out of range"):
+        ctx.add_particles(bad_cell, np.zeros((2, 3), np.float32), np.zeros((2, 3), np.float32),
+                          ids=np.array([-1, -2], np.int64))
+    assert ctx.count() == 201000
+    ctx.synchronize()
+    # the same bad input through the mover path (room in the store): intact
+    ctx2 = _ctx(n)
+    ctx2.set_particles(cell, off, vel, global_mass=1e-3, ids=ids)
+    with pytest.raises(L.LF2Error, match="out of range"):
+        ctx2.add_particles(bad_cell, np.full((2, 3), 0.5, np.float32),
+                           np.zeros((2, 3), np.float32), ids=np.array([-1, -2], np.int64))
+    kept = _by_id(ctx2.get_particles(ids=True))
+    np.testing.assert_array_equal(kept["id"], ids)
+    np.testing.assert_array_equal(kept["cell"], cell)
+    ctx2.synchronize()
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (40, 24, 20)])
+def test_one_rank_slab_domain_equals_the_single_gpu_step(n):
+    """SlabDomain with one rank: ghost planes, migration across the periodic
+    z face (through extract/add) and the folded deposit give what lf2_step
+    gives on the whole lattice."""
+    import torch
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    steps, dtk, dtd = 5, 0.05, 0.02
+    res = 1.0 / n[0]
+    cell, off, _ = small_case(n, 60000, seed=11)
+    rng = np.random.default_rng(12)
+    vel = (rng.uniform(-0.55, 0.55, (cell.shape[0], 3)) * res / dtd).astype(np.float32)
+    F = (0.1 * rng.standard_normal((3, n[2], n[1], n[0]))).astype(np.float32)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    gm = 1.0 / cell.shape[0]
+
+    ref = _ctx(n)
+    ref.set_particles(cell, off, vel, global_mass=gm, ids=ids)
+    Fh = ref.field(3, torch.from_numpy(F).cuda())
+    rho_ref = ref.field(1)
+    for k in range(steps):
+        ref.step(Fh, dtk, dtd, rho_ref if k == steps - 1 else None)
+    want = _by_id(ref.get_particles(ids=True))
+
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64)
+    d.set_particles(cell, off, vel, gm, ids=ids)
+    Ff = d.field(3)
+    d.set_own_planes(Ff, F)
+    rho = d.field(1)
+    for k in range(steps):
+        d.step(Ff, dtk, dtd, rho if k == steps - 1 else None)
+    got = _by_id(d.particles_global())
+    for k in ("id", "cell", "off", "vel"):
+        np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    r = d.own_planes(rho)[0]
+    w = rho_ref.export_internal()[0]
+    assert np.abs(r - w).max() <= 1e-6 * np.abs(w).max()
+    zs = cell // (n[0] * n[1])
+    zf = want["cell"] // (n[0] * n[1])
+    assert np.sum(np.abs(zs[want["id"]] - zf) > n[2] // 2) > 50  # crossed the periodic z face
