@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-projections", action="store_true",
                     help="skip timing the full-CIC vector and VecVec projections")
+    ap.add_argument("--slab", action="store_true",
+                    help="also time the step through a one-rank slab domain (ghost planes, "
+                         "migration, folded deposit)")
     ap.add_argument("--no-pm", action="store_true",
                     help="skip timing the PM grid operator (FFT Poisson force)")
     ap.add_argument("--no-fp32", action="store_true",
@@ -520,6 +523,33 @@ def pm_operator(ctx, rho, n, nsites, peak, reps=5):
             "route_frac_of_hbm": 40 * nsites / (ms / 1e3) / 1e9 / peak}
 
 
+def slab_one_rank_ms(case, F, n, npart, dtau, warmup, steps, local):
+    """The same particles and steps through latfield2_b200.distributed.SlabDomain
+    with one rank (its neighbours are itself): kick-drift-rebin, ghost planes
+    of F, migration through the periodic z face (extract/add) and the folded
+    deposit.  CUDA events around `steps` steps after `warmup`."""
+    import torch
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    cell, off, vel = case
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64, device=local)
+    d.set_particles(cell.cpu().numpy(), off.cpu().numpy(), vel.cpu().numpy(), 1.0 / npart)
+    Ff = d.field(3)
+    Ff[0][:, 1:n[2] + 1] = F
+    rho = d.field(1)
+    for _ in range(warmup):
+        d.step(Ff, dtau, dtau, rho)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        d.step(Ff, dtau, dtau, rho)
+    e1.record()
+    torch.cuda.synchronize()
+    d.engine.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
 def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
     """Device time per lf2_step of the same particles with FP32 atomic
     deposits (CUDA events on the launching stream)."""
@@ -588,7 +618,8 @@ def main():
     nsites = n[0] * n[1] * n[2]
     ctx = L.Context(n, box=1.0, mode=mode, device=local)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
-    fp32_case = (cell, off, vel) if (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) else None
+    keep_case = (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) or args.slab
+    fp32_case = (cell, off, vel) if keep_case else None
     del cell, off, vel
     Fh = ctx.field(3, F)
     rho = ctx.field(1)
@@ -657,9 +688,16 @@ def main():
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
 
+    slab = None
+    if args.slab and fp32_case is not None:
+        sms = slab_one_rank_ms(fp32_case, F, n, npart, dtau, args.warmup, min(args.steps, 5), local)
+        slab = {"ms_per_step": sms, "vs_lf2_step": sms / ms_step, "ranks": 1,
+                "note": "one self-exchanging rank; the exchange calls run, no peer"}
+        torch.cuda.empty_cache()
+
     # the same particles and steps with FP32 atomic deposits
     fixed_vs_fp32 = None
-    if fp32_case is not None:
+    if fp32_case is not None and not args.no_fp32 and mode == L.DEPOSIT_FIXED64:
         del ctx, Fh, rho
         torch.cuda.empty_cache()
         ms32 = fp32_step_ms(n, fp32_case, F, npart, dtau, args.warmup, args.steps, local)
@@ -702,7 +740,7 @@ def main():
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
             "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin, "projections": proj,
-            "pm_operator": pm,
+            "pm_operator": pm, "slab_one_rank": slab,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
