@@ -318,18 +318,36 @@ __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* 
                          int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state,
                          uint32_t* flags)
 {
+  // Whole warps step through the movers together, so that the lanes heading
+  // for the same brick (consecutive movers mostly come from one source brick
+  // and go to a few neighbours) take their slots with one atomic per brick.
   const int64_t nm = (int64_t)*mov_count;
-  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
-       m += (int64_t)gridDim.x * blockDim.x) {
-    int x, y, z;
-    unpack_key(v.g, mov.key[m], x, y, z);
-    if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move
-      set_flag(flags, ERR_BAD_CELL);
-      placed[m] = 1;
-      continue;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp0 * 32; base < nm; base += nwarps * 32) {
+    const int64_t m = base + lane;
+    int64_t b = -1;
+    if (m < nm) {
+      int x, y, z;
+      unpack_key(v.g, mov.key[m], x, y, z);
+      if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move
+        set_flag(flags, ERR_BAD_CELL);
+        placed[m] = 1;
+      } else {
+        b = brick_of(v.g, x, y, z);
+      }
     }
-    const int64_t b = brick_of(v.g, x, y, z);
-    const int slot = atomicAdd(&v.count[b], 1);
+    const unsigned grp = __match_any_sync(0xffffffffu, b);
+    int slot = 0;
+    if (b >= 0) {
+      const int leader = __ffs(grp) - 1;
+      int first = 0;
+      if (lane == leader) first = atomicAdd(&v.count[b], __popc(grp));
+      slot = __shfl_sync(grp, first, leader) + __popc(grp & lt);
+    }
+    if (b < 0) continue;
     if (slot < v.cap[b]) {
       const int64_t q = v.seg_start[b] + slot;
       v.a.key[q] = mov.key[m];
