@@ -124,6 +124,17 @@ lf2_status lf2_particles_extract_z(lf2_ctx* ctx, int z_lo, int z_hi,
 lf2_status lf2_particles_add(lf2_ctx* ctx, int64_t n, const int32_t* cell,
                              const float* off3, const float* vel3,
                              const float* mass, const int64_t* id, int ptr_kind);
+/* Checkpoint of the particle store for an exact restart: the library's
+ * particle state (cell, offsets, velocities, mass, id) and the unit mass of
+ * the fixed-point deposit, written to / read from a little-endian file: an
+ * 80-byte header (int32 "LF2C", version 1, n[3], deposit mode, has_mass,
+ * has_id; double box[3], global mass, unit mass; int64 count), then the
+ * arrays (cell, offsets, velocities[, mass][, id]).  A run restored into a context of the same
+ * lattice, box and mode continues bit for bit.  The reference's own format
+ * (Particles::saveHDF5 / loadHDF5, LATfield2_Particles.hpp:2809-3045) is
+ * HDF5; its records (ID, pos, vel) come from lf2_particles_get_pos. */
+lf2_status lf2_checkpoint_save(lf2_ctx* ctx, const char* path);
+lf2_status lf2_checkpoint_load(lf2_ctx* ctx, const char* path);
 /* Particles::numParticles (LATfield2_Particles.hpp:316-320). */
 lf2_status lf2_particles_count(lf2_ctx* ctx, int64_t* n);
 /* Downloads the particles in storage order (brick by brick).  Any output

@@ -258,6 +258,14 @@ class Context:
             self.h, int(cell.shape[0]), _ptr(cell)[0], _ptr(off)[0], _ptr(vel)[0], _ptr(mass)[0],
             _ptr(ids)[0], kind), "particles_add")
 
+    def checkpoint_save(self, path):
+        """The particle store to `path` (exact restart)."""
+        self._check(_lib.load().lf2_checkpoint_save(self.h, str(path).encode()), "checkpoint_save")
+
+    def checkpoint_load(self, path):
+        """A store saved by checkpoint_save (same lattice, box and mode)."""
+        self._check(_lib.load().lf2_checkpoint_load(self.h, str(path).encode()), "checkpoint_load")
+
     def cell_counts(self):
         out = np.empty(self.nsites, np.int32)
         self._check(_lib.load().lf2_cell_counts(self.h, _ptr(out)[0], _lib.PTR_HOST), "cell_counts")

@@ -539,6 +539,86 @@ lf2_status lf2_particles_add(lf2_ctx* c, int64_t n, const int32_t* cell, const f
                      (const float*)tm.p, c->gmass, (const int64_t*)ti.p);
 }
 
+// Checkpoint file (little endian): int32 "LF2C", int32 version 1,
+// int32 n[3], int32 deposit mode, int32 has_mass, int32 has_id (32 bytes),
+// double box[3], double global mass, double unit mass of the fixed-point
+// deposit, int64 np (80 bytes in all); then np x int32 cell, np x 3 f32
+// offsets, np x 3 f32 velocities, [np x f32 mass], [np x int64 id]: the
+// store in brick order.
+static bool write_all(FILE* f, const void* p, size_t bytes)
+{
+  return bytes == 0 || fwrite(p, 1, bytes, f) == bytes;
+}
+static bool read_all(FILE* f, void* p, size_t bytes)
+{
+  return bytes == 0 || fread(p, 1, bytes, f) == bytes;
+}
+
+lf2_status lf2_checkpoint_save(lf2_ctx* c, const char* path)
+{
+  if (!c || !path) return LF2_ERR_ARG;
+  const int64_t n = c->np;
+  std::vector<int32_t> cell((size_t)n);
+  std::vector<float> off((size_t)n * 3), vel((size_t)n * 3), mass(c->has_mass ? (size_t)n : 0);
+  std::vector<int64_t> id(c->has_id ? (size_t)n : 0);
+  LF2_TRY(lf2_particles_get(c, cell.data(), off.data(), vel.data(),
+                            c->has_mass ? mass.data() : nullptr, c->has_id ? id.data() : nullptr,
+                            LF2_PTR_HOST));
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(c, LF2_ERR_ARG, std::string("checkpoint_save: cannot open ") + path);
+  const int32_t head[8] = {0x4332464c /* "LF2C" */, 1, c->g.n[0], c->g.n[1], c->g.n[2], c->mode,
+                           c->has_mass ? 1 : 0, c->has_id ? 1 : 0};
+  bool ok = write_all(f, head, sizeof head) && write_all(f, c->box, sizeof(double) * 3) &&
+            write_all(f, &c->gmass, sizeof(double)) &&
+            write_all(f, &c->m_unit, sizeof(double)) && write_all(f, &n, sizeof(int64_t)) &&
+            write_all(f, cell.data(), sizeof(int32_t) * cell.size()) &&
+            write_all(f, off.data(), sizeof(float) * off.size()) &&
+            write_all(f, vel.data(), sizeof(float) * vel.size()) &&
+            write_all(f, mass.data(), sizeof(float) * mass.size()) &&
+            write_all(f, id.data(), sizeof(int64_t) * id.size());
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(c, LF2_ERR_ARG, std::string("checkpoint_save: write failed: ") + path);
+  return LF2_OK;
+}
+
+lf2_status lf2_checkpoint_load(lf2_ctx* c, const char* path)
+{
+  if (!c || !path) return LF2_ERR_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(c, LF2_ERR_ARG, std::string("checkpoint_load: cannot open ") + path);
+  int32_t head[8];
+  double box[3], gmass = 0, m_unit = 1;
+  int64_t n = 0;
+  bool ok = read_all(f, head, sizeof head) && read_all(f, box, sizeof box) &&
+            read_all(f, &gmass, sizeof gmass) &&
+            read_all(f, &m_unit, sizeof m_unit) && read_all(f, &n, sizeof n);
+  if (!ok || head[0] != 0x4332464c || head[1] != 1 || n < 0 || n >= (1ll << 31)) {
+    fclose(f);
+    return fail(c, LF2_ERR_ARG, std::string("checkpoint_load: not a checkpoint: ") + path);
+  }
+  if (head[2] != c->g.n[0] || head[3] != c->g.n[1] || head[4] != c->g.n[2] || box[0] != c->box[0] ||
+      box[1] != c->box[1] || box[2] != c->box[2] || head[5] != c->mode) {
+    fclose(f);
+    return fail(c, LF2_ERR_ARG, "checkpoint_load: the checkpoint has another lattice, box or mode");
+  }
+  const bool has_mass = head[6] != 0, has_id = head[7] != 0;
+  std::vector<int32_t> cell((size_t)n);
+  std::vector<float> off((size_t)n * 3), vel((size_t)n * 3), mass(has_mass ? (size_t)n : 0);
+  std::vector<int64_t> id(has_id ? (size_t)n : 0);
+  ok = read_all(f, cell.data(), sizeof(int32_t) * cell.size()) &&
+       read_all(f, off.data(), sizeof(float) * off.size()) &&
+       read_all(f, vel.data(), sizeof(float) * vel.size()) &&
+       read_all(f, mass.data(), sizeof(float) * mass.size()) &&
+       read_all(f, id.data(), sizeof(int64_t) * id.size());
+  fclose(f);
+  if (!ok) return fail(c, LF2_ERR_ARG, std::string("checkpoint_load: truncated: ") + path);
+  LF2_TRY(lf2_particles_set(c, n, cell.data(), off.data(), vel.data(),
+                            has_mass ? mass.data() : nullptr, gmass, has_id ? id.data() : nullptr,
+                            LF2_PTR_HOST));
+  c->m_unit = m_unit;  // the fixed-point unit of the saved run, for a bit-exact restart
+  return LF2_OK;
+}
+
 lf2_status lf2_particles_count(lf2_ctx* c, int64_t* n)
 {
   if (!c || !n) return LF2_ERR_ARG;

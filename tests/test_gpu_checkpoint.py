@@ -1,0 +1,72 @@
+"""lf2_checkpoint_save / lf2_checkpoint_load: a run saved after some steps and
+restored into a fresh context continues bit for bit (particles by id, and
+the fixed-point density), with global and with per-particle masses; a
+checkpoint of another lattice is refused; the file header is the documented
+80-byte layout."""
+import struct
+
+import numpy as np
+import pytest
+import torch
+
+from tests.helpers import small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(n):
+    import latfield2_b200 as L
+    return L.Context(n, box=tuple(v / n[0] for v in n), mode=L.DEPOSIT_FIXED64)
+
+
+@pytest.mark.parametrize("per_particle_mass", [False, True])
+def test_restart_is_bit_exact(tmp_path, per_particle_mass):
+    n = (48, 40, 32)
+    cell, off, vel = small_case(n, 80000, seed=31, vel_sigma=0.05, clustered=True)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    mass = None
+    if per_particle_mass:
+        mass = (1.0 + 0.3 * np.random.default_rng(32).uniform(-1, 1, cell.shape[0])).astype(
+            np.float32) / cell.shape[0]
+    F = torch.from_numpy(np.random.default_rng(33).standard_normal((3, n[2], n[1], n[0]))
+                         .astype(np.float32) * 0.05).cuda()
+    a = _ctx(n)
+    a.set_particles(cell, off, vel, mass=mass, global_mass=0.0 if per_particle_mass else 1e-5,
+                    ids=ids)
+    Fa, rho_a = a.field(3, F), a.field(1)
+    for _ in range(3):
+        a.step(Fa, 0.05, 0.1, rho_a)
+    path = tmp_path / "run.lf2c"
+    a.checkpoint_save(path)
+    head = open(path, "rb").read(80)
+    magic, version, n0, n1, n2, mode, hm, hi = struct.unpack("<8i", head[:32])
+    assert (magic, version, (n0, n1, n2), hm, hi) == (0x4332464C, 1, n, int(per_particle_mass), 1)
+    assert struct.unpack("<q", head[72:80])[0] == cell.shape[0]
+
+    b = _ctx(n)
+    b.checkpoint_load(path)
+    Fb, rho_b = b.field(3, F.clone()), b.field(1)
+    for _ in range(4):
+        a.step(Fa, 0.05, 0.1, rho_a)
+        b.step(Fb, 0.05, 0.1, rho_b)
+    pa = a.get_particles(mass=per_particle_mass, ids=True)
+    pb = b.get_particles(mass=per_particle_mass, ids=True)
+    oa, ob = np.argsort(pa["id"]), np.argsort(pb["id"])
+    for k in pa:
+        np.testing.assert_array_equal(pa[k][oa], pb[k][ob], err_msg=k)
+    np.testing.assert_array_equal(rho_a.export_internal(), rho_b.export_internal())
+
+
+def test_other_lattice_is_refused(tmp_path):
+    import latfield2_b200 as L
+    a = _ctx((32, 32, 32))
+    cell, off, vel = small_case((32, 32, 32), 1000, seed=1)
+    a.set_particles(cell, off, vel, global_mass=1e-3)
+    p = tmp_path / "a.lf2c"
+    a.checkpoint_save(p)
+    b = _ctx((32, 32, 16))
+    with pytest.raises(L.LF2Error, match="another lattice"):
+        b.checkpoint_load(p)
+    (tmp_path / "junk").write_bytes(b"not a checkpoint at all" * 10)
+    with pytest.raises(L.LF2Error, match="not a checkpoint"):
+        a.checkpoint_load(tmp_path / "junk")
