@@ -56,15 +56,24 @@ static_assert(2 * FT * FT + 2 * (FT - 2) * FT + 2 * (FT - 2) * (FT - 2) == FOUTE
 
 template <int KIND>
 struct FullCfg;
+// Threads per CTA.  Measured at 512^3: 512 and 1024 (more warps on the same
+// tiles) gave 5.39 / 11.96 ms against 5.11 / 11.99 ms for these defaults;
+// the tile passes are bound by the shared atomic pipe, not by occupancy.
+#ifndef LF2_FULL_THREADS3
+#define LF2_FULL_THREADS3 256
+#endif
+#ifndef LF2_FULL_THREADS4
+#define LF2_FULL_THREADS4 512
+#endif
 template <>
 struct FullCfg<3> {
   static constexpr int comps = 3;
-  static constexpr int threads = 256;  // 70 KB tile: 3 CTAs per SM
+  static constexpr int threads = LF2_FULL_THREADS3;  // 70 KB tile: 3 CTAs per SM
 };
 template <>
 struct FullCfg<4> {
   static constexpr int comps = 6;
-  static constexpr int threads = 512;  // 140 KB tile: 1 CTA per SM
+  static constexpr int threads = LF2_FULL_THREADS4;  // 140 KB tile: 1 CTA per SM
 };
 
 __device__ __forceinline__ int tile_at(int t0, int t1, int t2) { return t0 + FT * (t1 + FT * t2); }
