@@ -13,8 +13,9 @@
 // vertex dim the weights are the ordinary CIC ones, 1 - o at l and o at l + 1.
 //
 // One CTA per brick accumulates its particles (FP32 shared atomics) into a
-// tile of (BRICK+2)^3 vertices whose origin is one site below the brick, so
-// the lower staggered neighbours are inside it.  The flush then writes
+// tile of (BRICK+2)^3 vertices per component whose origin is one site below
+// the brick, so the lower staggered neighbours are inside it (three
+// components per pass; VecVec takes two passes).  The flush then writes
 //   - every vertex the brick owns (tile coordinates 1..e in all dims) to the
 //     field: the final value for the interior, a partial sum on the brick's
 //     boundary;
@@ -54,36 +55,38 @@ __host__ __device__ inline int outer_index(int u0, int u1, int u2)
 static_assert(2 * FT * FT + 2 * (FT - 2) * FT + 2 * (FT - 2) * (FT - 2) == FOUTER,
               "outer slab sizes");
 
-template <int KIND>
-struct FullCfg;
-// Threads per CTA.  Measured at 512^3: 512 and 1024 (more warps on the same
-// tiles) gave 5.39 / 11.96 ms against 5.11 / 11.99 ms for these defaults;
-// the tile passes are bound by the shared atomic pipe, not by occupancy.
-#ifndef LF2_FULL_THREADS3
-#define LF2_FULL_THREADS3 256
+// Threads per CTA of a tile pass.  Measured at 512^3: 512 (more warps on the
+// same tiles) gave 5.39 ms against 5.11 ms for 256; the tile passes are bound
+// by the shared atomic pipe, not by occupancy.
+#ifndef LF2_FULL_THREADS
+#define LF2_FULL_THREADS 256
 #endif
-#ifndef LF2_FULL_THREADS4
-#define LF2_FULL_THREADS4 512
-#endif
-template <>
-struct FullCfg<3> {
-  static constexpr int comps = 3;
-  static constexpr int threads = LF2_FULL_THREADS3;  // 70 KB tile: 3 CTAs per SM
-};
-template <>
-struct FullCfg<4> {
-  static constexpr int comps = 6;
-  static constexpr int threads = LF2_FULL_THREADS4;  // 140 KB tile: 1 CTA per SM
+constexpr int FULL_THREADS = LF2_FULL_THREADS;
+
+// A tile pass accumulates three components (a 70 KB tile, 3 CTAs per SM):
+//   pass 0  the vector field, components 0, 1, 2 of 3;
+//   pass 1  VecVec T_00, T_11, T_22 (components 0, 3, 5 of 6), vertex CIC;
+//   pass 2  VecVec T_01, T_02, T_12 (components 1, 2, 4 of 6) on plaquettes.
+// Two passes for VecVec rather than one 140 KB six-component tile (one CTA
+// per SM): the shared atomic pipe stays busier, at the cost of reading the
+// particles twice.
+template <int PASS>
+struct FullPass {
+  static constexpr int total = PASS == 0 ? 3 : 6;  // components of the field
+  __device__ static constexpr int comp(int j)
+  {
+    return PASS == 0 ? j : PASS == 1 ? (j == 0 ? 0 : j == 1 ? 3 : 5) : (j == 0 ? 1 : j == 1 ? 2 : 4);
+  }
 };
 
 __device__ __forceinline__ int tile_at(int t0, int t1, int t2) { return t0 + FT * (t1 + FT * t2); }
 
-template <int KIND>
-__global__ void __launch_bounds__(FullCfg<KIND>::threads)
+template <int PASS>
+__global__ void __launch_bounds__(FULL_THREADS)
     k_deposit_full(StoreView v, DepositParams dp, float* __restrict__ out,
                    float* __restrict__ outer)
 {
-  constexpr int C = FullCfg<KIND>::comps;
+  constexpr int CT = FullPass<PASS>::total;
   extern __shared__ __align__(16) float tile[];
 
   const Geom& g = v.g;
@@ -96,7 +99,7 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
   const int64_t base = v.seg_start[b];
   const int cnt = LF2_BRICK_COUNT(v, b);
 
-  for (int t = threadIdx.x; t < C * FT3; t += blockDim.x) tile[t] = 0.0f;
+  for (int t = threadIdx.x; t < 3 * FT3; t += blockDim.x) tile[t] = 0.0f;
   __syncthreads();
 
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
@@ -127,7 +130,7 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
       ls[d] = l[d] + 1;
       lt[d] = l[d] + gd;
     }
-    if (KIND == 3) {
+    if (PASS == 0) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const float mv = __fmul_rn(mf, vel[c]);
@@ -144,21 +147,21 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
                     __fmul_rn(__fmul_rn(__fmul_rn(mv, w0), w1), w2));
         }
       }
-    } else {
-      // T_ii at the vertices (components 0, 3, 5)
-      constexpr int diag[3] = {0, 3, 5};
+    } else if (PASS == 1) {
+      // T_ii at the vertices
 #pragma unroll
       for (int i2 = 0; i2 < 3; i2++) {
         const float m2 = __fmul_rn(__fmul_rn(mf, vel[i2]), vel[i2]);
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
-          atomicAdd(&tile[diag[i2] * FT3 + tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2)],
+          atomicAdd(&tile[i2 * FT3 + tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2)],
                     __fmul_rn(__fmul_rn(__fmul_rn(m2, sw[0][b0]), sw[1][b1]), sw[2][b2]));
         }
       }
-      // T_ij on the plaquettes: (0,1) -> 1, (0,2) -> 2, (1,2) -> 4
-      constexpr int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, pc[3] = {1, 2, 4};
+    } else {
+      // T_ij on the plaquettes: (0,1), (0,2), (1,2)
+      constexpr int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
 #pragma unroll
       for (int q = 0; q < 3; q++) {
         const float mm = __fmul_rn(__fmul_rn(mf, vel[pa[q]]), vel[pb[q]]);
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
             w[d] = st ? tw[d][bb[d]] : sw[d][bb[d]];
             t[d] = (st ? lt[d] : ls[d]) + bb[d];
           }
-          atomicAdd(&tile[pc[q] * FT3 + tile_at(t[0], t[1], t[2])],
+          atomicAdd(&tile[q * FT3 + tile_at(t[0], t[1], t[2])],
                     __fmul_rn(__fmul_rn(__fmul_rn(mm, w[0]), w[1]), w[2]));
         }
       }
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
   }
   __syncthreads();
 
-  float* os = outer + (size_t)b * C * FOUTER;
+  float* os = outer + (size_t)b * CT * FOUTER;
   for (int t = threadIdx.x; t < FT3; t += blockDim.x) {
     const int t0 = t % FT, t1 = (t / FT) % FT, t2 = t / (FT * FT);
     if (t0 > e[0] + 1 || t1 > e[1] + 1 || t2 > e[2] + 1) continue;
@@ -189,12 +192,12 @@ __global__ void __launch_bounds__(FullCfg<KIND>::threads)
     if (own) {
       const int64_t s = site_index(g, x0 + t0 - 1, y0 + t1 - 1, z0 + t2 - 1);
 #pragma unroll
-      for (int c = 0; c < C; c++) out[c * g.nsites + s] = tile[c * FT3 + t];
+      for (int j = 0; j < 3; j++) out[FullPass<PASS>::comp(j) * g.nsites + s] = tile[j * FT3 + t];
     } else {
       const int oi = outer_index(t0 == e[0] + 1 ? FT - 1 : t0, t1 == e[1] + 1 ? FT - 1 : t1,
                                  t2 == e[2] + 1 ? FT - 1 : t2);
 #pragma unroll
-      for (int c = 0; c < C; c++) os[c * FOUTER + oi] = tile[c * FT3 + t];
+      for (int j = 0; j < 3; j++) os[FullPass<PASS>::comp(j) * FOUTER + oi] = tile[j * FT3 + t];
     }
   }
 }
@@ -281,23 +284,16 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
-template <int KIND>
-cudaError_t run_full(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
+template <int PASS>
+cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
 {
-  constexpr int C = FullCfg<KIND>::comps;
-  const unsigned nb = (unsigned)c->g.nbricks;
-  float* outer = reinterpret_cast<float*>(c->spill);
-  if (stage == 0) {
-    const size_t smem = (size_t)C * FT3 * sizeof(float);
-    cudaError_t e = cudaFuncSetAttribute(k_deposit_full<KIND>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    c->launches += 1;
-    k_deposit_full<KIND><<<nb, FullCfg<KIND>::threads, smem, c->stream>>>(view(c), dp, out, outer);
-  } else {
-    c->launches += 1;
-    k_fixup_full<C><<<nb, 256, 0, c->stream>>>(c->g, outer, out);
-  }
+  const size_t smem = (size_t)3 * FT3 * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_deposit_full<PASS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  c->launches += 1;
+  k_deposit_full<PASS><<<(unsigned)c->g.nbricks, FULL_THREADS, smem, c->stream>>>(
+      view(c), dp, out, reinterpret_cast<float*>(c->spill));
   return cudaGetLastError();
 }
 
@@ -312,7 +308,19 @@ cudaError_t launch_deposit_full(lf2_ctx* c, int kind, float* out, int stage)
   dp.fixed_scale = 0.0f;
   dp.inv_unit = 0.0f;
   dp.has_mass = c->has_mass ? 1 : 0;
-  return kind == 3 ? run_full<3>(c, out, dp, stage) : run_full<4>(c, out, dp, stage);
+  const unsigned nb = (unsigned)c->g.nbricks;
+  float* outer = reinterpret_cast<float*>(c->spill);
+  if (stage == 0) {
+    if (kind == 3) return tile_pass<0>(c, out, dp);
+    cudaError_t e = tile_pass<1>(c, out, dp);
+    return e != cudaSuccess ? e : tile_pass<2>(c, out, dp);
+  }
+  c->launches += 1;
+  if (kind == 3)
+    k_fixup_full<3><<<nb, 256, 0, c->stream>>>(c->g, outer, out);
+  else
+    k_fixup_full<6><<<nb, 256, 0, c->stream>>>(c->g, outer, out);
+  return cudaGetLastError();
 }
 
 }  // namespace lf2
