@@ -3,9 +3,16 @@
  *
  * This is the boundary that replaces the reference's header-only particle
  * path (particles/LATfield2_Particles.hpp, particles/projections.hpp,
- * LATfield2_Field_decl.hpp).  Plain C types only: pointers, sizes, status
- * codes.  The C++ compatibility layer (include/LATfield2.hpp) and the Python
- * package (latfield2_b200) are both written on top of these functions.
+ * LATfield2_Field_decl.hpp) and its real-to-complex Fourier transform
+ * (LATfield2_PlanFFT_decl.hpp).  Plain C types only: pointers, sizes, status
+ * codes.  The C++ compatibility layer (include/latfield2_b200.hpp) and the
+ * Python package (latfield2_b200) are both written on top of these functions.
+ *
+ * Sections: context; particles (set, get, the slab-exchange pair
+ * extract_z / add, checkpoint); fields; projections (scalar CIC, vector and
+ * symtensor CIC-NGP, full-CIC vector and VecVec); particle moves (kick,
+ * drift and rebin, the fused step); PM grid operator (k-fields, FFT, Poisson
+ * force); differentiable PM chain; the no-allocation deposit; measurement.
  *
  * Conventions
  *  - Every function returns an lf2_status: 0 on success, < 0 on failure;
