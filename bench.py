@@ -26,6 +26,7 @@ Multi-GPU (torchrun): every rank advances its own replica of the workload
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -301,13 +302,15 @@ def cpu_baseline_reference(seconds, cores, n=64, npart=64 ** 3):
     return npart * r["steps"] / r["seconds"], r["steps"], r["ranks"]
 
 
-def adjoint_ratio(device, steps=8, reps=3):
+def adjoint_ratio(device, steps=8, reps=3, operator="stencil"):
     """Differentiable chain at 128^3 with 2,097,152 uniform particles and
     per-particle masses (1/Np)(1 + 0.1 U(-1,1)): 8 kick-drift steps of
-    deposit -> periodic 27-point stencil (81 seeded weights) -> CIC gather ->
-    kick -> drift, loss = sum w_g rho_g(final), particle checkpoints every 2
-    steps.  Returns device times of the forward alone and of forward +
-    adjoint (CUDA events, median of `reps`)."""
+    deposit -> grid operator -> CIC gather -> kick -> drift, loss =
+    sum w_g rho_g(final), particle checkpoints every 2 steps.  The grid
+    operator is the periodic 27-point stencil (81 seeded weights) or, with
+    operator "pm", the FFT Poisson force (coupling 4 pi).  Returns device
+    times of the forward alone and of forward + adjoint (CUDA events, median
+    of `reps`)."""
     import torch
     import latfield2_b200 as L
     from latfield2_b200.autodiff import pm_chain_loss
@@ -326,7 +329,12 @@ def adjoint_ratio(device, steps=8, reps=3):
         leaves = [t.clone().requires_grad_(grad) for t in (pos, vel, m, S, w)]
         torch.cuda.synchronize()
         e0.record()
-        loss = pm_chain_loss(ctx, *leaves, steps=steps, dt=dt, checkpoint_every=2)
+        if operator == "pm":
+            loss = pm_chain_loss(ctx, leaves[0], leaves[1], leaves[2], None, leaves[4],
+                                 steps=steps, dt=dt, checkpoint_every=2, operator="pm",
+                                 coupling=4 * math.pi)
+        else:
+            loss = pm_chain_loss(ctx, *leaves, steps=steps, dt=dt, checkpoint_every=2)
         if grad:
             loss.backward()
         e1.record()
@@ -336,7 +344,9 @@ def adjoint_ratio(device, steps=8, reps=3):
     timed(True)
     fwd = sorted(timed(False) for _ in range(reps))[reps // 2]
     both = sorted(timed(True) for _ in range(reps))[reps // 2]
+    ctx.close()
     return {"workload": "128^3, 2,097,152 particles, 8 steps, checkpoint every 2",
+            "operator": "27-point stencil" if operator == "stencil" else "PM force (FFT)",
             "forward_ms": fwd, "forward_adjoint_ms": both, "ratio": both / fwd}
 
 
@@ -687,6 +697,8 @@ def main():
     pm = None if args.no_pm else pm_operator(ctx, rho, n, nsites, peak)
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
+    adj_pm = (adjoint_ratio(device, operator="pm")
+              if (rank == 0 and not args.no_adjoint and not args.no_pm) else None)
 
     slab = None
     if args.slab and fp32_case is not None:
@@ -739,6 +751,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
+            "adjoint_pm": adj_pm,
             "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin, "projections": proj,
             "pm_operator": pm, "slab_one_rank": slab,
         }

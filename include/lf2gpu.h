@@ -299,7 +299,13 @@ lf2_status lf2_pm_force(lf2_ctx* ctx, lf2_field rho, lf2_field phi,
  *   gather_adjoint   g_F4 (+=) CIC deposit of g_out3; g_off3 (+=)
  *   stencil27        F4_c(g) = sum_o S[c*27 + (dz+1)*9 + (dy+1)*3 + (dx+1)]
  *                    rho(g + o), periodic, S81 on the device
- *   stencil27_adjoint g_rho (+=) and g_S81 (+=) from g_F4 */
+ *   stencil27_adjoint g_rho (+=) and g_S81 (+=) from g_F4
+ *   pm_force4        the PM force of lf2_pm_force as the chain's grid
+ *                    operator: F4 = (F_x, F_y, F_z, 0) from rho (cubic
+ *                    lattices up to 1024^3)
+ *   pm_force4_adjoint g_rho (+=) from g_F4: the divergence
+ *                    g_phi(y) = sum_c (g_F_c(y+e_c) - g_F_c(y-e_c)) / (2 res),
+ *                    then the same Green's-function solve (self-adjoint) */
 lf2_status lf2_pm_deposit(lf2_ctx* ctx, int64_t np, const int32_t* cell,
                           const float* off3, const float* mass, double gmass,
                           float* rho);
@@ -322,6 +328,10 @@ lf2_status lf2_stencil27(lf2_ctx* ctx, const float* rho, const float* S81,
 lf2_status lf2_stencil27_adjoint(lf2_ctx* ctx, const float* rho,
                                  const float* S81, const float* g_F4,
                                  float* g_rho, float* g_S81);
+lf2_status lf2_pm_force4(lf2_ctx* ctx, const float* rho, float* F4,
+                         double coupling);
+lf2_status lf2_pm_force4_adjoint(lf2_ctx* ctx, const float* g_F4,
+                                 float* g_rho, double coupling);
 
 /* ---------------------------------------------------------- no allocation
  * Scalar CIC deposit that allocates no device memory.  It has no

@@ -95,6 +95,8 @@ SIGNATURES = {
                               c_void_p],
     "lf2_stencil27": [c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_stencil27_adjoint": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    "lf2_pm_force4": [c_void_p, c_void_p, c_void_p, c_double],
+    "lf2_pm_force4_adjoint": [c_void_p, c_void_p, c_void_p, c_double],
     "lf2_profile_enable": [c_void_p, c_int],
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],
     "lf2_kernel_launches": [c_void_p, P(c_i64)],

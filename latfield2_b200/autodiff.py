@@ -2,18 +2,23 @@
 
 Per step k (particles in the caller's order, no rebinning):
     rho_k   = deposit(x_k, m)                    lf2_pm_deposit      (CIC, projections.hpp:75-184)
-    F_k     = stencil27(rho_k, S)                lf2_stencil27       (the grid operator)
+    F_k     = stencil27(rho_k, S)                lf2_stencil27       (the grid operator), or
+    F_k     = pm_force(rho_k)                    lf2_pm_force4       (the FFT Poisson force)
     G_k     = gather(x_k, F_k)                   lf2_pm_gather       (CIC gather of updateVel)
     v_{k+1} = v_k + dt G_k ;  x_{k+1} = x_k + dt v_{k+1}             lf2_pm_kick_drift
 and finally rho_K = deposit(x_K, m), loss = sum_g w_g rho_K(g).
 
 `PMChain` is a torch.autograd.Function whose backward runs the hand-written
-adjoint kernels (lf2_pm_*_adjoint, lf2_stencil27_adjoint) in reverse.
+adjoint kernels (lf2_pm_*_adjoint, lf2_stencil27_adjoint,
+lf2_pm_force4_adjoint) in reverse.
 Particle states are checkpointed every `checkpoint_every` steps and the
 states in between are recomputed during the backward pass; the grid fields
 rho_k and F_k of every step are kept (4 floats per lattice site per step).
 Gradients are returned for the initial positions (box units), velocities,
-masses, the 81 stencil weights and the loss weights.
+masses, the 81 stencil weights (stencil operator only) and the loss weights.
+The PM operator solves lap7(phi) = coupling (rho - mean rho) by FFT and takes
+F = -grad phi by central differences (the operator of lf2_pm_force; cubic
+lattices).
 """
 import ctypes
 
@@ -82,12 +87,24 @@ class _Ops:
         _check(self.ctx, self.lib.lf2_stencil27_adjoint(self.ctx.h, _p(rho), _p(S), _p(g_F),
                                                         _p(g_rho), _p(g_S)), "stencil27_adjoint")
 
-    def fields(self, cell, off, m, S):
+    def pm_force(self, rho, F, coupling):
+        _check(self.ctx, self.lib.lf2_pm_force4(self.ctx.h, _p(rho), _p(F), coupling), "pm_force4")
+
+    def pm_force_adj(self, g_F, g_rho, coupling):
+        _check(self.ctx, self.lib.lf2_pm_force4_adjoint(self.ctx.h, _p(g_F), _p(g_rho), coupling),
+               "pm_force4_adjoint")
+
+    def fields(self, cell, off, m, S, coupling=None):
+        """rho and the float4-per-site force: the stencil S, or the PM force
+        when `coupling` is given."""
         dev = cell.device
         rho = torch.zeros(self.ns, dtype=torch.float32, device=dev)
         self.deposit(cell, off, m, rho)
         F = torch.empty(4 * self.ns, dtype=torch.float32, device=dev)  # float4 per site
-        self.stencil(rho, S, F)
+        if coupling is None:
+            self.stencil(rho, S, F)
+        else:
+            self.pm_force(rho, F, coupling)
         return rho, F
 
     def step(self, cell, off, vel, F, dt):
@@ -98,26 +115,26 @@ class _Ops:
 
 class PMChain(torch.autograd.Function):
     @staticmethod
-    def forward(fctx, pos0, vel0, mass, S, w, lf2ctx, steps, dt, checkpoint_every):
+    def forward(fctx, pos0, vel0, mass, S, w, lf2ctx, steps, dt, checkpoint_every, coupling):
         ops = _Ops(lf2ctx)
         n, res = lf2ctx.n, lf2ctx.res
         cell, off = positions_to_state(pos0.detach().to(torch.float64), n, res)
         vel = vel0.detach().to(torch.float32).contiguous().clone()
         m = mass.detach().to(torch.float32).contiguous()
-        S32 = S.detach().to(torch.float32).contiguous()
+        S32 = None if S is None else S.detach().to(torch.float32).contiguous()
         w32 = w.detach().to(torch.float32).contiguous().reshape(-1)
         ckpts, rhos, Fs = {}, [], []
         for k in range(steps):
             if k % checkpoint_every == 0:
                 ckpts[k] = (cell.clone(), off.clone(), vel.clone())
-            rho, F = ops.fields(cell, off, m, S32)
+            rho, F = ops.fields(cell, off, m, S32, coupling)
             rhos.append(rho)
             Fs.append(F)
             ops.step(cell, off, vel, F, dt)
         rhoK = torch.zeros(lf2ctx.nsites, dtype=torch.float32, device=cell.device)
         ops.deposit(cell, off, m, rhoK)
         loss = torch.dot(w32.to(torch.float64), rhoK.to(torch.float64))
-        fctx.lf2 = (lf2ctx, steps, dt, checkpoint_every, ckpts, rhos, Fs)
+        fctx.lf2 = (lf2ctx, steps, dt, checkpoint_every, ckpts, rhos, Fs, coupling)
         fctx.save_for_backward(cell, off, m, S32, w32, rhoK)
         fctx.pos_dtype = pos0.dtype
         fctx.vel_dtype = vel0.dtype
@@ -125,7 +142,7 @@ class PMChain(torch.autograd.Function):
 
     @staticmethod
     def backward(fctx, gloss):
-        lf2ctx, steps, dt, every, ckpts, rhos, Fs = fctx.lf2
+        lf2ctx, steps, dt, every, ckpts, rhos, Fs, coupling = fctx.lf2
         cellK, offK, m, S32, w32, rhoK = fctx.saved_tensors
         ops = _Ops(lf2ctx)
         dev = cellK.device
@@ -156,14 +173,28 @@ class PMChain(torch.autograd.Function):
             g_F = torch.zeros(4 * lf2ctx.nsites, dtype=torch.float32, device=dev)
             ops.gather_adj(cell_k, off_k, Fs[k], g_G, g_F, g_off)
             g_rho = torch.zeros(lf2ctx.nsites, dtype=torch.float32, device=dev)
-            ops.stencil_adj(rhos[k], S32, g_F, g_rho, g_S)
+            if coupling is None:
+                ops.stencil_adj(rhos[k], S32, g_F, g_rho, g_S)
+            else:
+                ops.pm_force_adj(g_F, g_rho, coupling)
             ops.deposit_adj(cell_k, off_k, m, g_rho, g_off, g_m)
         g_pos = (g_off.to(torch.float64) / res).to(fctx.pos_dtype)
         g_w = (rhoK * g).to(torch.float64)
-        return (g_pos, g_v.to(fctx.vel_dtype), g_m.to(torch.float64), g_S.to(torch.float64), g_w,
-                None, None, None, None)
+        g_S = None if S32 is None else g_S.to(torch.float64)
+        return (g_pos, g_v.to(fctx.vel_dtype), g_m.to(torch.float64), g_S, g_w,
+                None, None, None, None, None)
 
 
-def pm_chain_loss(ctx: Context, pos0, vel0, mass, S, w, steps=8, dt=0.1, checkpoint_every=2):
-    """Loss of the multi-step chain; differentiable in pos0, vel0, mass, S, w."""
-    return PMChain.apply(pos0, vel0, mass, S, w, ctx, steps, dt, checkpoint_every)
+def pm_chain_loss(ctx: Context, pos0, vel0, mass, S, w, steps=8, dt=0.1, checkpoint_every=2,
+                  operator="stencil", coupling=1.0):
+    """Loss of the multi-step chain; differentiable in pos0, vel0, mass, w and,
+    with operator "stencil", the 81 weights S.  operator "pm" uses the FFT
+    Poisson force with `coupling` instead (S is then ignored and may be None)."""
+    if operator == "stencil":
+        if S is None:
+            raise ValueError("the stencil operator needs its 81 weights S")
+        return PMChain.apply(pos0, vel0, mass, S, w, ctx, steps, dt, checkpoint_every, None)
+    if operator == "pm":
+        return PMChain.apply(pos0, vel0, mass, None, w, ctx, steps, dt, checkpoint_every,
+                             float(coupling))
+    raise ValueError(f"unknown grid operator {operator!r} (stencil or pm)")

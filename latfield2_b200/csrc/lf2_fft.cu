@@ -18,6 +18,11 @@
 //    The Laplacian eigenvalue is evaluated as -4 sum_d sin^2(pi k_d / n) / res^2,
 //    which equals the example's 2 (sum_d cos(2 pi k_d / n) - 3) / res^2 without
 //    its cancellation at small k.
+//  - lf2_pm_force4 / lf2_pm_force4_adjoint: the same operator as the grid
+//    operator of the differentiable chain (float4 per site), and its adjoint:
+//    the divergence of the incoming force gradient (k_divergence4) followed
+//    by the same Green's-function solve, which is self-adjoint (a
+//    convolution with a real kernel even in k).
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -258,6 +263,95 @@ __global__ void k_kimport(float2* __restrict__ K, int comps, int n, int nkx,
   }
 }
 
+// F4(x) = (F_x, F_y, F_z, 0) with F_c = (phi(x - e_c) - phi(x + e_c)) *
+// inv_2res, periodic: k_gradient for the float4-per-site layout of the
+// differentiable chain.
+__global__ void k_gradient4(const float* __restrict__ phi, float4* __restrict__ F4, Geom g,
+                            float inv_2res)
+{
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int rows = n1 * n2;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int y = row % n1, z = row / n1;
+    const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
+    const int zp = z + 1 == n2 ? 0 : z + 1, zm = z == 0 ? n2 - 1 : z - 1;
+    const float* pr = phi + (int64_t)row * n0;
+    const float* pyp = phi + ((int64_t)z * n1 + yp) * n0;
+    const float* pym = phi + ((int64_t)z * n1 + ym) * n0;
+    const float* pzp = phi + ((int64_t)zp * n1 + y) * n0;
+    const float* pzm = phi + ((int64_t)zm * n1 + y) * n0;
+    for (int x = threadIdx.x; x < n0; x += blockDim.x) {
+      const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+      F4[(int64_t)row * n0 + x] = make_float4((pr[xm] - pr[xp]) * inv_2res,
+                                              (pym[x] - pyp[x]) * inv_2res,
+                                              (pzm[x] - pzp[x]) * inv_2res, 0.0f);
+    }
+  }
+}
+
+// Adjoint of k_gradient4: phi enters F_c(y + e_c) with +inv_2res and
+// F_c(y - e_c) with -inv_2res, so
+// g_phi(y) = inv_2res sum_c (g_F_c(y + e_c) - g_F_c(y - e_c)).
+// The fourth component of g_F4 is not read.
+__global__ void k_divergence4(const float4* __restrict__ gF4, float* __restrict__ gphi, Geom g,
+                              float inv_2res)
+{
+  const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+  const int rows = n1 * n2;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int y = row % n1, z = row / n1;
+    const int yp = y + 1 == n1 ? 0 : y + 1, ym = y == 0 ? n1 - 1 : y - 1;
+    const int zp = z + 1 == n2 ? 0 : z + 1, zm = z == 0 ? n2 - 1 : z - 1;
+    const float4* r = gF4 + (int64_t)row * n0;
+    const float4* ryp = gF4 + ((int64_t)z * n1 + yp) * n0;
+    const float4* rym = gF4 + ((int64_t)z * n1 + ym) * n0;
+    const float4* rzp = gF4 + ((int64_t)zp * n1 + y) * n0;
+    const float4* rzm = gF4 + ((int64_t)zm * n1 + y) * n0;
+    for (int x = threadIdx.x; x < n0; x += blockDim.x) {
+      const int xp = x + 1 == n0 ? 0 : x + 1, xm = x == 0 ? n0 - 1 : x - 1;
+      const float d = (r[xp].x - r[xm].x) + (ryp[x].y - rym[x].y) + (rzp[x].z - rzm[x].z);
+      gphi[(int64_t)row * n0 + x] = d * inv_2res;
+    }
+  }
+}
+
+// dst += src over n floats.
+__global__ void k_accumulate(float* __restrict__ dst, const float* __restrict__ src, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] += src[i];
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Plans and scratch of the PM operator; lattices up to 1024^3 (k_green's
+// 32-bit k indices).
+lf2_status pm_prepare(lf2_ctx* c, const char* who, bool real_scratch)
+{
+  FFT_TRY(ensure_plans(c));
+  if (c->g.n[0] > 1024)
+    return fft_fail(c, LF2_ERR_ARG, std::string(who) + ": lattices up to 1024^3 (32-bit k indices)");
+  return ensure_scratch(c, real_scratch);
+}
+
+// dst = coupling-scaled Green's-function solve of src: R2C into fft_k,
+// k_green, C2R into dst.  dst may be src.
+lf2_status green_solve(lf2_ctx* c, const float* src, float* dst, double coupling)
+{
+  const int n = c->g.n[0], nkx = n / 2 + 1;
+  FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, const_cast<float*>(src),
+                            reinterpret_cast<cufftComplex*>(c->fft_k)));
+  const float coef = (float)(-coupling * c->res * c->res / (4.0 * (double)c->g.nsites));
+  const int64_t pairs = (int64_t)n * n * nkx / 2;
+  c->launches += 1;
+  k_green<<<grid_for((pairs + GREEN_ITEMS - 1) / GREEN_ITEMS, 256), 256, sizeof(float) * n,
+            c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
+  FFT_CUDA(c, cudaGetLastError());
+  FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), dst));
+  return LF2_OK;
+}
+
 }  // namespace
 
 void fft_release(lf2_ctx* c)
@@ -392,20 +486,9 @@ lf2_status lf2_pm_force(lf2_ctx* c, lf2_field rho, lf2_field phi, lf2_field F, d
 {
   if (!c || !field_ok(rho, 1) || !field_ok(F, 3) || (phi && !field_ok(phi, 1)))
     return LF2_ERR_ARG;
-  FFT_TRY(ensure_plans(c));
-  if (c->g.n[0] > 1024)
-    return fft_fail(c, LF2_ERR_ARG, "lf2_pm_force: lattices up to 1024^3 (32-bit k indices)");
-  FFT_TRY(ensure_scratch(c, phi == nullptr));
+  FFT_TRY(pm_prepare(c, "lf2_pm_force", phi == nullptr));
   float* p = phi ? phi->data : c->fft_phi;
-  const int n = c->g.n[0], nkx = n / 2 + 1;
-  FFT_CUFFT(c, cufftExecR2C(c->fft_r2c, rho->data, reinterpret_cast<cufftComplex*>(c->fft_k)));
-  const float coef = (float)(-coupling * c->res * c->res / (4.0 * (double)c->g.nsites));
-  const int64_t pairs = (int64_t)n * n * nkx / 2;
-  c->launches += 1;
-  k_green<<<grid_for((pairs + GREEN_ITEMS - 1) / GREEN_ITEMS, 256), 256, sizeof(float) * n,
-            c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
-  FFT_CUDA(c, cudaGetLastError());
-  FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), p));
+  FFT_TRY(green_solve(c, rho->data, p, coupling));
   c->launches += 1;
   const int grows = c->g.n[1] * c->g.n[2];
   const unsigned gblocks = grows < 148 * 8 ? grows : 148 * 8;
@@ -416,6 +499,38 @@ lf2_status lf2_pm_force(lf2_ctx* c, lf2_field rho, lf2_field phi, lf2_field F, d
     k_gradient<true><<<gblocks, gthreads, 0, c->stream>>>(p, F->data, c->g, (float)(0.5 / c->res));
   else
     k_gradient<false><<<gblocks, gthreads, 0, c->stream>>>(p, F->data, c->g, (float)(0.5 / c->res));
+  FFT_CUDA(c, cudaGetLastError());
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_force4(lf2_ctx* c, const float* rho, float* F4, double coupling)
+{
+  if (!c || !rho || !F4 || !aligned16(F4)) return LF2_ERR_ARG;
+  FFT_TRY(pm_prepare(c, "lf2_pm_force4", true));
+  FFT_TRY(green_solve(c, rho, c->fft_phi, coupling));
+  const int grows = c->g.n[1] * c->g.n[2];
+  c->launches += 1;
+  k_gradient4<<<grows < 148 * 8 ? grows : 148 * 8, 256, 0, c->stream>>>(
+      c->fft_phi, reinterpret_cast<float4*>(F4), c->g, (float)(0.5 / c->res));
+  FFT_CUDA(c, cudaGetLastError());
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_force4_adjoint(lf2_ctx* c, const float* g_F4, float* g_rho, double coupling)
+{
+  if (!c || !g_F4 || !g_rho || !aligned16(g_F4)) return LF2_ERR_ARG;
+  FFT_TRY(pm_prepare(c, "lf2_pm_force4_adjoint", true));
+  const int grows = c->g.n[1] * c->g.n[2];
+  c->launches += 1;
+  k_divergence4<<<grows < 148 * 8 ? grows : 148 * 8, 256, 0, c->stream>>>(
+      reinterpret_cast<const float4*>(g_F4), c->fft_phi, c->g, (float)(0.5 / c->res));
+  FFT_CUDA(c, cudaGetLastError());
+  // The Green's-function solve is a convolution with a real, even kernel:
+  // its own adjoint.  R2C reads fft_phi before C2R writes it back.
+  FFT_TRY(green_solve(c, c->fft_phi, c->fft_phi, coupling));
+  c->launches += 1;
+  k_accumulate<<<grid_for(c->g.nsites, 256), 256, 0, c->stream>>>(g_rho, c->fft_phi,
+                                                                   c->g.nsites);
   FFT_CUDA(c, cudaGetLastError());
   return LF2_OK;
 }

@@ -51,3 +51,59 @@ def test_fp64_gradient_matches_finite_differences():
         assert fd is not None
         an = float(sum((g * u).sum() for g, u in zip(grads, us)))
         assert an == pytest.approx(fd, rel=1e-5, abs=1e-6 * float(torch.sqrt(sum((g ** 2).sum() for g in grads))))
+
+
+def test_pm_force_matches_the_fft_oracle():
+    from oracle import fft_oracle as FO
+    n = 16
+    rho = torch.rand(n ** 3, generator=torch.Generator().manual_seed(2), dtype=torch.float64)
+    F = P.pm_force(rho, (n, n, n), 4 * np.pi)
+    _, ref = FO.pm_force(rho.reshape(n, n, n).numpy(), 1.0 / n, 4 * np.pi)
+    np.testing.assert_allclose(F.numpy(), ref.reshape(3, -1), rtol=0, atol=1e-14)
+
+
+def test_pm_force_adjoint_is_divergence_then_the_same_solve():
+    """The structure of lf2_pm_force4_adjoint: g_rho = G(div g_F), with
+    div_c the transpose of the central difference and G the Green's-function
+    solve itself (self-adjoint)."""
+    n = 12
+    g = torch.Generator().manual_seed(4)
+    rho = torch.randn(n ** 3, generator=g, dtype=torch.float64)
+    gF = torch.randn(3, n ** 3, generator=g, dtype=torch.float64)
+    r = rho.clone().requires_grad_(True)
+    (P.pm_force(r, (n, n, n), 3.0) * gF).sum().backward()
+    res = 1.0 / n
+    gf = gF.reshape(3, n, n, n)
+    div = sum(torch.roll(gf[c], -1, axis) - torch.roll(gf[c], 1, axis)
+              for c, axis in zip(range(3), (2, 1, 0))) / (2 * res)
+    # the forward operator's Green's-function solve, applied to the divergence
+    K = torch.fft.rfftn(div)
+    k = torch.arange(n, dtype=torch.float64)
+    cs = lambda t: torch.cos(2 * torch.pi * t / n)
+    lam = 2 * (cs(k[: n // 2 + 1])[None, None, :] + cs(k)[None, :, None] + cs(k)[:, None, None]
+               - 3) / res ** 2
+    lam[0, 0, 0] = 1.0
+    Gk = 3.0 / lam
+    Gk[0, 0, 0] = 0.0
+    want = torch.fft.irfftn(K * Gk, s=(n, n, n)).reshape(-1)
+    np.testing.assert_allclose(r.grad.numpy(), want.numpy(), rtol=0,
+                               atol=1e-12 * float(want.abs().max()))
+
+
+def test_fp64_pm_chain_gradient_matches_finite_differences():
+    n, pos, vel, m, S, w = _setup(n=8, npart=300, seed=6)
+    steps, dt, coupling = 4, 0.5, 4 * np.pi
+    leaves = [t.clone().requires_grad_(True) for t in (pos, vel, m)]
+    loss = P.chain_loss(*leaves, S, w, n, steps, dt, coupling=coupling)
+    grads = torch.autograd.grad(loss, leaves)
+    rng = np.random.default_rng(8)
+    gnorm = float(torch.sqrt(sum((g ** 2).sum() for g in grads)))
+    for _ in range(20):
+        us = [torch.from_numpy(rng.standard_normal(t.shape)) for t in (pos, vel, m)]
+        norm = float(torch.sqrt(sum((u ** 2).sum() for u in us)))
+        us = [u / norm for u in us] + [torch.zeros_like(S)]
+        fd, used = P.directional_fd([pos, vel, m, S], us, w, n, steps, dt, eps=1e-7,
+                                    coupling=coupling)
+        assert fd is not None
+        an = float(sum((g * u).sum() for g, u in zip(grads, us)))
+        assert an == pytest.approx(fd, rel=1e-5, abs=1e-6 * gnorm)

@@ -143,3 +143,82 @@ def test_chain_gradients_against_fp64(cuda, n, npart, ndir):
     scale = np.sqrt(np.mean(fd ** 2))
     assert np.max(np.abs(an_ref - fd)) < 1e-5 * scale  # the FP64 reference gradient
     assert np.max(np.abs(an_dev - fd)) < 5e-3 * scale  # the CUDA adjoint
+
+
+COUPLING = 4 * np.pi  # lap phi = 4 pi G rho with G = 1
+
+
+def test_pm_force4_and_its_adjoint(cuda):
+    """lf2_pm_force4 against the FP64 PM force, and lf2_pm_force4_adjoint
+    against its autograd gradient (2e-5 of the norm)."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops
+    for n in (24, 32):
+        ctx = L.Context((n, n, n), box=1.0)
+        ops = _Ops(ctx)
+        g = torch.Generator(device="cpu").manual_seed(n)
+        rho = (1.0 + torch.randn(n ** 3, generator=g, dtype=torch.float64)).to("cuda")
+        F4 = torch.full((n ** 3, 4), 7.0, device="cuda")
+        ops.pm_force(rho.float().contiguous(), F4, COUPLING)
+        ref = P.pm_force(rho, (n, n, n), COUPLING)
+        assert _rel(F4[:, :3].t(), ref) < 2e-5
+        assert float(F4[:, 3].abs().max()) == 0.0
+        gF = torch.randn(3, n ** 3, generator=g, dtype=torch.float64).to("cuda")
+        r = rho.clone().requires_grad_(True)
+        (P.pm_force(r, (n, n, n), COUPLING) * gF).sum().backward()
+        gF4 = torch.zeros(n ** 3, 4, device="cuda")
+        gF4[:, :3] = gF.float().t()
+        gF4[:, 3] = 5.0  # not read
+        g_rho = torch.ones(n ** 3, device="cuda")
+        ops.pm_force_adj(gF4, g_rho, COUPLING)
+        assert _rel(g_rho - 1.0, r.grad) < 2e-5  # accumulated
+        ctx.close()
+
+
+def test_pm_chain_gradients_against_fp64(cuda):
+    """The 8-step chain with the PM force as grid operator: gradients for
+    positions, velocities, masses and loss weights against the FP64 chain
+    (2e-3 of each norm) and central differences along 200 random
+    directions (5e-3 of their rms)."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import pm_chain_loss
+    n, npart, ndir, steps, dt = 32, 20000, 200, 8, 0.1
+    pos, vel, m, S, w = _case(n, npart, 9, "cuda")
+    cell, off = _state(pos, n)
+    posd = ((torch.stack([cell.long() % n, (cell.long() // n) % n, cell.long() // (n * n)], 1)
+             .double() + off.double()) / n)
+    vel, m, w = vel.float().double(), m.float().double(), w.float().double()
+    ctx = L.Context((n, n, n), box=1.0)
+    leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, w)]
+    loss = pm_chain_loss(ctx, leaves[0], leaves[1], leaves[2], None, leaves[3], steps=steps,
+                         dt=dt, checkpoint_every=2, operator="pm", coupling=COUPLING)
+    loss.backward()
+    got = [t.grad for t in leaves]
+    ref_leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, w)]
+    ref_loss = P.chain_loss(ref_leaves[0], ref_leaves[1], ref_leaves[2], None, ref_leaves[3],
+                            (n, n, n), steps, dt, coupling=COUPLING)
+    ref = torch.autograd.grad(ref_loss, ref_leaves)
+    assert float(loss.detach()) == pytest.approx(float(ref_loss.detach()), rel=2e-4)
+    for name, a, b in zip(("pos", "vel", "mass", "weights"), got, ref):
+        assert _rel(a, b) < 2e-3, name
+    rng = np.random.default_rng(12)
+    base = [posd, vel, m]
+    fd, an_dev, an_ref = [], [], []
+    for _ in range(ndir):
+        us = [torch.from_numpy(rng.standard_normal(tuple(t.shape))).to("cuda") for t in base]
+        nrm = float(torch.sqrt(sum((u ** 2).sum() for u in us)))
+        us = [u / nrm for u in us]
+        with torch.no_grad():
+            d, _ = P.directional_fd(base + [None], us + [None], w, (n, n, n), steps, dt,
+                                    eps=1e-7, coupling=COUPLING)
+        assert d is not None
+        fd.append(d)
+        an_dev.append(float(sum((g * u).sum() for g, u in zip(got[:3], us))))
+        an_ref.append(float(sum((g * u).sum() for g, u in zip(ref[:3], us))))
+    fd, an_dev, an_ref = map(np.array, (fd, an_dev, an_ref))
+    scale = np.sqrt(np.mean(fd ** 2))
+    assert np.max(np.abs(an_ref - fd)) < 1e-5 * scale
+    assert np.max(np.abs(an_dev - fd)) < 5e-3 * scale
+    ctx.close()
