@@ -48,6 +48,7 @@ extern "C" {
 typedef struct lf2_ctx lf2_ctx;
 typedef struct lf2_field_s* lf2_field;
 typedef struct lf2_kfield_s* lf2_kfield;
+typedef struct lf2_slab_fft_s* lf2_slab_fft;
 typedef int lf2_status;
 
 #define LF2_OK 0
@@ -278,6 +279,35 @@ lf2_status lf2_fft_forward(lf2_ctx* ctx, lf2_field r, lf2_kfield k);
 lf2_status lf2_fft_backward(lf2_ctx* ctx, lf2_kfield k, lf2_field r);
 lf2_status lf2_pm_force(lf2_ctx* ctx, lf2_field rho, lf2_field phi,
                         lf2_field F, double coupling);
+
+/* ------------------------------------------------ PM operator over z slabs
+ * The pieces of the PM force when the lattice is split in z over R ranks
+ * (the distributed PlanFFT, LATfield2_PlanFFT_decl.hpp:83-230, with a 1-D
+ * split: 2-D plane transforms, a transpose, 1-D line transforms).  The
+ * global lattice is n^3; a rank owns nz = n / R planes and, after the
+ * transpose, nky = n / R values of k_y.  Complex arrays hold (re, im) float
+ * pairs; nkx = n/2 + 1.  ctx is the rank's local context (planes n x n).
+ *   slab_fft_planes_r2c: planes [nz][n][n] -> A [nz][k_y n][k_x nkx], 2-D
+ *     R2C of every plane, unnormalised
+ *   slab_fft_planes_c2r: the inverse, unnormalised; A is overwritten
+ *   slab_fft_lines: B [z or k_z n][nky][nkx], 1-D C2C along the outer axis
+ *     in place, LF2_FFT_FORWARD (exp(-i...)) or LF2_FFT_BACKWARD,
+ *     unnormalised
+ *   slab_green: B [k_z][k_y - ky0][k_x] *= the Green's function of
+ *     lf2_pm_force (coupling, 1/n^3 included, zero mode removed); B 16-byte
+ *     aligned
+ *   pm_gradient: F_i = -(phi(x+e_i) - phi(x-e_i)) / (2 res) on ctx's
+ *     lattice, periodic (with filled ghost planes, exact on the own planes) */
+#define LF2_FFT_FORWARD 1
+#define LF2_FFT_BACKWARD (-1)
+lf2_status lf2_slab_fft_create(lf2_ctx* ctx, int n, int nz, int nky,
+                               lf2_slab_fft* out);
+lf2_status lf2_slab_fft_destroy(lf2_slab_fft p);
+lf2_status lf2_slab_fft_planes_r2c(lf2_slab_fft p, const float* planes, void* A);
+lf2_status lf2_slab_fft_planes_c2r(lf2_slab_fft p, void* A, float* planes);
+lf2_status lf2_slab_fft_lines(lf2_slab_fft p, void* B, int direction);
+lf2_status lf2_slab_green(lf2_slab_fft p, void* B, int ky0, double coupling);
+lf2_status lf2_pm_gradient(lf2_ctx* ctx, lf2_field phi, lf2_field F);
 
 /* ------------------------------------------------- differentiable PM chain
  * Particle kernels on arrays kept in the caller's order (no rebinning, so

@@ -3,10 +3,10 @@
 CIC deposits (scalar, vector and symmetric-tensor CIC-NGP, full-CIC vector
 and VecVec), CIC gather with kick, drift and rebin of brick-binned particles,
 and the PM grid operator (real-to-complex FFT and a Poisson force), written as
-CUDA kernels behind the C ABI in include/lf2gpu.h.  `Context`, `FieldHandle`
-and `KFieldHandle` are the Python binding of that ABI;
+CUDA kernels behind the C ABI in include/lf2gpu.h.  `Context`, `FieldHandle`,
+`KFieldHandle` and `SlabFFT` are the Python binding of that ABI;
 include/latfield2_b200.hpp gives C++ code the reference's Lattice / Field /
 Particles / projection names over it.
 """
 from ._lib import (DEPOSIT_FIXED64, DEPOSIT_FP32, LF2Error, library_path, load)  # noqa: F401
-from .core import Context, FieldHandle, KFieldHandle  # noqa: F401
+from .core import Context, FieldHandle, KFieldHandle, SlabFFT  # noqa: F401

@@ -18,6 +18,8 @@ LF2_ERR_UNSUPPORTED = -5
 
 DEPOSIT_FP32 = 0
 DEPOSIT_FIXED64 = 1
+FFT_FORWARD = 1
+FFT_BACKWARD = -1
 PTR_HOST = 0
 PTR_DEVICE = 1
 
@@ -96,6 +98,13 @@ SIGNATURES = {
     "lf2_stencil27": [c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_stencil27_adjoint": [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_pm_force4": [c_void_p, c_void_p, c_void_p, c_double],
+    "lf2_slab_fft_create": [c_void_p, c_int, c_int, c_int, P(c_void_p)],
+    "lf2_slab_fft_destroy": [c_void_p],
+    "lf2_slab_fft_planes_r2c": [c_void_p, c_void_p, c_void_p],
+    "lf2_slab_fft_planes_c2r": [c_void_p, c_void_p, c_void_p],
+    "lf2_slab_fft_lines": [c_void_p, c_void_p, c_int],
+    "lf2_slab_green": [c_void_p, c_void_p, c_int, c_double],
+    "lf2_pm_gradient": [c_void_p, c_void_p, c_void_p],
     "lf2_pm_force4_adjoint": [c_void_p, c_void_p, c_void_p, c_double],
     "lf2_profile_enable": [c_void_p, c_int],
     "lf2_profile_read": [c_void_p, P(c_double), P(c_i64)],

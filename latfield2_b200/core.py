@@ -134,6 +134,66 @@ class KFieldHandle:
             self.ctx.h, self.h, p, arr.itemsize // 2, kind), "kfield_import")
 
 
+class SlabFFT:
+    """The transforms of the PM operator over z slabs (lf2_slab_fft_*): 2-D
+    transforms of a rank's nz planes of an n^3 lattice, 1-D transforms along
+    the outer axis of a [n][nky][n/2+1] block, and the Green's function on
+    it.  Complex arrays are torch complex64 tensors on the context's device."""
+
+    def __init__(self, ctx, n, nz, nky):
+        self.ctx = ctx
+        h = _c.c_void_p()
+        ctx._check(_lib.load().lf2_slab_fft_create(ctx.h, int(n), int(nz), int(nky), _c.byref(h)),
+                   "slab_fft_create")
+        self.h = h
+        self.n, self.nz, self.nky = int(n), int(nz), int(nky)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().lf2_slab_fft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptr(t, shape, dtype):
+        if tuple(t.shape) != tuple(shape) or t.dtype != dtype or not t.is_contiguous():
+            raise ValueError(f"expected a contiguous {dtype} tensor of shape {shape}")
+        return _c.c_void_p(t.data_ptr())
+
+    def planes_r2c(self, planes, A):
+        import torch
+        n, nz = self.n, self.nz
+        self.ctx._check(_lib.load().lf2_slab_fft_planes_r2c(
+            self.h, self._ptr(planes, (nz, n, n), torch.float32),
+            self._ptr(A, (nz, n, n // 2 + 1), torch.complex64)), "slab_fft_planes_r2c")
+
+    def planes_c2r(self, A, planes):
+        import torch
+        n, nz = self.n, self.nz
+        self.ctx._check(_lib.load().lf2_slab_fft_planes_c2r(
+            self.h, self._ptr(A, (nz, n, n // 2 + 1), torch.complex64),
+            self._ptr(planes, (nz, n, n), torch.float32)), "slab_fft_planes_c2r")
+
+    def lines(self, B, direction):
+        import torch
+        n = self.n
+        self.ctx._check(_lib.load().lf2_slab_fft_lines(
+            self.h, self._ptr(B, (n, self.nky, n // 2 + 1), torch.complex64), int(direction)),
+            "slab_fft_lines")
+
+    def green(self, B, ky0, coupling):
+        import torch
+        n = self.n
+        self.ctx._check(_lib.load().lf2_slab_green(
+            self.h, self._ptr(B, (n, self.nky, n // 2 + 1), torch.complex64), int(ky0),
+            float(coupling)), "slab_green")
+
+
 class Context:
     def __init__(self, n, box=1.0, mode=_lib.DEPOSIT_FP32, device=0, stream=None):
         if np.isscalar(n):
@@ -290,6 +350,10 @@ class Context:
         """F = -grad phi (central differences), lap7(phi) = coupling (rho - mean)."""
         self._check(_lib.load().lf2_pm_force(self.h, rho.h, None if phi is None else phi.h, F.h,
                                              float(coupling)), "pm_force")
+
+    def pm_gradient(self, phi, F):
+        """F = -grad phi by central differences on this lattice (periodic)."""
+        self._check(_lib.load().lf2_pm_gradient(self.h, phi.h, F.h), "pm_gradient")
 
     def halo_fill(self, tensor, comps, halo):
         self._check(_lib.load().lf2_halo_fill(self.h, _c.c_void_p(tensor.data_ptr()), comps, halo,

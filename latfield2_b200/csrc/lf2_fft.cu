@@ -38,6 +38,13 @@ struct lf2_kfield_s {
   float2* data = nullptr;  // comps x [n2][n1][n0/2+1]
 };
 
+struct lf2_slab_fft_s {
+  lf2_ctx* c = nullptr;
+  int n = 0, nz = 0, nky = 0, nkx = 0;
+  cufftHandle r2c = 0, c2r = 0, lines = 0;
+  int planned = 0;  // bit 0 r2c, bit 1 c2r, bit 2 lines
+};
+
 namespace lf2 {
 
 namespace {
@@ -129,16 +136,18 @@ lf2_status ensure_scratch(lf2_ctx* c, bool real_too)
 // at once, so several loads are in flight before the first store.
 constexpr int GREEN_ITEMS = 4;
 
-__device__ __forceinline__ float green_factor(const float* s2tab, uint32_t i, int n, int nkx,
-                                              float coef)
+// K holds k_y in [ky0, ky0 + nky) of the k-cube: [k_z][k_y - ky0][k_x] (the
+// whole cube when nky = n and ky0 = 0).
+__device__ __forceinline__ float green_factor(const float* s2tab, uint32_t i, int nky, int nkx,
+                                              int ky0, float coef)
 {
   const uint32_t row = i / (uint32_t)nkx;
   const int kx = (int)(i - row * (uint32_t)nkx);
-  const int ky = (int)(row % (uint32_t)n), kz = (int)(row / (uint32_t)n);
-  return i == 0 ? 0.0f : coef / (s2tab[kx] + (s2tab[ky] + s2tab[kz]));
+  const int ky = ky0 + (int)(row % (uint32_t)nky), kz = (int)(row / (uint32_t)nky);
+  return (kx | ky | kz) == 0 ? 0.0f : coef / (s2tab[kx] + (s2tab[ky] + s2tab[kz]));
 }
 
-__global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
+__global__ void k_green(float2* __restrict__ K, int n, int nky, int nkx, int ky0, float coef)
 {
   extern __shared__ float s2tab[];
   const float inv_n = 1.0f / (float)n;
@@ -147,7 +156,7 @@ __global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
     s2tab[i] = s * s;
   }
   __syncthreads();
-  const uint32_t total = (uint32_t)n * (uint32_t)n * (uint32_t)nkx;
+  const uint32_t total = (uint32_t)n * (uint32_t)nky * (uint32_t)nkx;
   const uint32_t pairs = total / 2;
   float4* K4 = reinterpret_cast<float4*>(K);
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -163,13 +172,13 @@ __global__ void k_green(float2* __restrict__ K, int n, int nkx, float coef)
     for (int j = 0; j < GREEN_ITEMS; j++) {
       const uint32_t p = p0 + j * stride;
       if (p >= pairs) continue;
-      const float f0 = green_factor(s2tab, 2 * p, n, nkx, coef);
-      const float f1 = green_factor(s2tab, 2 * p + 1, n, nkx, coef);
+      const float f0 = green_factor(s2tab, 2 * p, nky, nkx, ky0, coef);
+      const float f1 = green_factor(s2tab, 2 * p + 1, nky, nkx, ky0, coef);
       K4[p] = make_float4(v[j].x * f0, v[j].y * f0, v[j].z * f1, v[j].w * f1);
     }
   }
   if ((total & 1u) && blockIdx.x == 0 && threadIdx.x == 0) {
-    const float f = green_factor(s2tab, total - 1, n, nkx, coef);
+    const float f = green_factor(s2tab, total - 1, nky, nkx, ky0, coef);
     const float2 v = K[total - 1];
     K[total - 1] = make_float2(v.x * f, v.y * f);
   }
@@ -346,7 +355,7 @@ lf2_status green_solve(lf2_ctx* c, const float* src, float* dst, double coupling
   const int64_t pairs = (int64_t)n * n * nkx / 2;
   c->launches += 1;
   k_green<<<grid_for((pairs + GREEN_ITEMS - 1) / GREEN_ITEMS, 256), 256, sizeof(float) * n,
-            c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, nkx, coef);
+            c->stream>>>(reinterpret_cast<float2*>(c->fft_k), n, n, nkx, 0, coef);
   FFT_CUDA(c, cudaGetLastError());
   FFT_CUFFT(c, cufftExecC2R(c->fft_c2r, reinterpret_cast<cufftComplex*>(c->fft_k), dst));
   return LF2_OK;
@@ -531,6 +540,108 @@ lf2_status lf2_pm_force4_adjoint(lf2_ctx* c, const float* g_F4, float* g_rho, do
   c->launches += 1;
   k_accumulate<<<grid_for(c->g.nsites, 256), 256, 0, c->stream>>>(g_rho, c->fft_phi,
                                                                    c->g.nsites);
+  FFT_CUDA(c, cudaGetLastError());
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_gradient(lf2_ctx* c, lf2_field phi, lf2_field F)
+{
+  if (!c || !field_ok(phi, 1) || !field_ok(F, 3)) return LF2_ERR_ARG;
+  c->launches += 1;
+  const int grows = c->g.n[1] * c->g.n[2];
+  k_gradient<false><<<grows < 148 * 8 ? grows : 148 * 8, 256, 0, c->stream>>>(
+      phi->data, F->data, c->g, (float)(0.5 / c->res));
+  FFT_CUDA(c, cudaGetLastError());
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_fft_destroy(lf2_slab_fft p)
+{
+  if (!p) return LF2_OK;
+  if (p->c) cudaStreamSynchronize(p->c->stream);
+  if (p->planned & 1) cufftDestroy(p->r2c);
+  if (p->planned & 2) cufftDestroy(p->c2r);
+  if (p->planned & 4) cufftDestroy(p->lines);
+  delete p;
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_fft_create(lf2_ctx* c, int n, int nz, int nky, lf2_slab_fft* out)
+{
+  if (!c || !out || n < 2 || n > 1024 || nz < 1 || nz > n || nky < 1 || nky > n)
+    return LF2_ERR_ARG;
+  if (c->g.n[0] != n || c->g.n[1] != n)
+    return fft_fail(c, LF2_ERR_ARG, "lf2_slab_fft_create: the planes must be n x n");
+  lf2_slab_fft p = new (std::nothrow) lf2_slab_fft_s();
+  if (!p) return LF2_ERR_NOMEM;
+  p->c = c;
+  p->n = n;
+  p->nz = nz;
+  p->nky = nky;
+  p->nkx = n / 2 + 1;
+  int dims[2] = {n, n};
+  int line[1] = {n};
+  const int S = nky * p->nkx;
+  cufftResult r = cufftPlanMany(&p->r2c, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_R2C, nz);
+  if (r == CUFFT_SUCCESS) {
+    p->planned |= 1;
+    r = cufftPlanMany(&p->c2r, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2R, nz);
+  }
+  if (r == CUFFT_SUCCESS) {
+    p->planned |= 2;
+    r = cufftPlanMany(&p->lines, 1, line, line, S, 1, line, S, 1, CUFFT_C2C, S);
+  }
+  if (r == CUFFT_SUCCESS) p->planned |= 4;
+  if (r != CUFFT_SUCCESS) {
+    lf2_slab_fft_destroy(p);
+    return fft_fail(c, LF2_ERR_CUDA, "lf2_slab_fft_create: cuFFT status " + std::to_string((int)r));
+  }
+  *out = p;
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_fft_planes_r2c(lf2_slab_fft p, const float* planes, void* A)
+{
+  if (!p || !planes || !A) return LF2_ERR_ARG;
+  lf2_ctx* c = p->c;
+  FFT_CUFFT(c, cufftSetStream(p->r2c, c->stream));
+  FFT_CUFFT(c, cufftExecR2C(p->r2c, const_cast<float*>(planes),
+                            reinterpret_cast<cufftComplex*>(A)));
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_fft_planes_c2r(lf2_slab_fft p, void* A, float* planes)
+{
+  if (!p || !planes || !A) return LF2_ERR_ARG;
+  lf2_ctx* c = p->c;
+  FFT_CUFFT(c, cufftSetStream(p->c2r, c->stream));
+  FFT_CUFFT(c, cufftExecC2R(p->c2r, reinterpret_cast<cufftComplex*>(A), planes));
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_fft_lines(lf2_slab_fft p, void* B, int direction)
+{
+  if (!p || !B || (direction != LF2_FFT_FORWARD && direction != LF2_FFT_BACKWARD))
+    return LF2_ERR_ARG;
+  lf2_ctx* c = p->c;
+  FFT_CUFFT(c, cufftSetStream(p->lines, c->stream));
+  cufftComplex* b = reinterpret_cast<cufftComplex*>(B);
+  FFT_CUFFT(c, cufftExecC2C(p->lines, b, b,
+                            direction == LF2_FFT_FORWARD ? CUFFT_FORWARD : CUFFT_INVERSE));
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_green(lf2_slab_fft p, void* B, int ky0, double coupling)
+{
+  if (!p || !B || ky0 < 0 || ky0 + p->nky > p->n || !aligned16(B)) return LF2_ERR_ARG;
+  lf2_ctx* c = p->c;
+  const int n = p->n;
+  const double res = c->res;
+  const float coef = (float)(-coupling * res * res / (4.0 * (double)n * n * n));
+  const int64_t pairs = (int64_t)n * p->nky * p->nkx / 2;
+  c->launches += 1;
+  k_green<<<grid_for((pairs + GREEN_ITEMS - 1) / GREEN_ITEMS, 256), 256, sizeof(float) * n,
+            c->stream>>>(reinterpret_cast<float2*>(B), n, p->nky, p->nkx, ky0, coef);
   FFT_CUDA(c, cudaGetLastError());
   return LF2_OK;
 }

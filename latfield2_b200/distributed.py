@@ -24,6 +24,23 @@ ranks).  x and y are not split.  One step does what lf2_step does on one GPU:
      1..nz+1, and plane nz+1 is added into plane 1 of the rank above: the
      upper-halo fold of scalarProjectionCIC_comm (projections.hpp:194-300).
 
+`project` deposits the other projections of the own particles with the same
+folds: the vector and symtensor CIC-NGP projections reach planes 1..nz+1 and
+fold upward as the scalar does (vectorProjectionCICNGP_comm,
+symtensorProjectionCICNGP_comm, projections.hpp:548-681, :845-976); the
+full-CIC projections reach planes 0..nz+1, so plane 0 is also added into
+plane nz of the rank below (the Up+Down fold of vectorProjectionCIC_comm and
+VecVecProjectionCIC_comm, projections.hpp:1192-1349, :1624-1814).
+
+`pm_force` is the PM operator of lf2_pm_force on the split lattice (cubic,
+n a multiple of R), in the manner of the distributed PlanFFT
+(LATfield2_PlanFFT_decl.hpp:83-230) with a 1-D split: every rank transforms
+its nz planes in 2-D, an all-to-all transpose gives rank r all n planes of
+k_y in [r nky, (r+1) nky) (nky = n / R), the 1-D transforms along z, the
+Green's function and the inverse 1-D transforms run there, the transpose
+goes back, the inverse 2-D transforms give phi on the own planes, and the
+central-difference gradient reads phi's ghost planes after fill_ghosts.
+
 Exchanges are point-to-point messages between neighbours (NCCL between GPUs,
 gloo between CPU processes).  A single rank exchanges with itself, which
 gives the periodic single-domain result.  The local work is done by an
@@ -66,8 +83,37 @@ class CudaEngine:
     def deposit(self, rho):
         self.ctx.deposit_scalar(rho[1])
 
+    def project(self, kind, f):
+        getattr(self.ctx, "deposit_" + kind)(f[1])
+
     def extract_outside(self, zlo, zhi):
         return self.ctx.extract_z(zlo, zhi, mass=self.has_mass, ids=self.has_id)
+
+    # the PM operator's pieces (SlabDomain.pm_force)
+    def fft_prepare(self, n, nz, nky):
+        from .core import SlabFFT
+        key = (n, nz, nky)
+        if getattr(self, "_fft_key", None) != key:
+            self._fft = SlabFFT(self.ctx, n, nz, nky)
+            self._fft_key = key
+
+    def complex_buffer(self, shape):
+        return self.torch.empty(shape, dtype=self.torch.complex64, device=self.dev)
+
+    def planes_r2c(self, planes, A):
+        self._fft.planes_r2c(planes, A)
+
+    def planes_c2r(self, A, planes):
+        self._fft.planes_c2r(A, planes)
+
+    def lines(self, B, direction):
+        self._fft.lines(B, direction)
+
+    def green(self, B, ky0, coupling):
+        self._fft.green(B, ky0, coupling)
+
+    def gradient(self, phi, F):
+        self.ctx.pm_gradient(phi[1], F[1])
 
     def add(self, parts):
         if int(parts["cell"].shape[0]) == 0:
@@ -200,6 +246,71 @@ class SlabDomain:
         a[:, 1] += buf
         a[:, 0] = 0
         a[:, self.nz + 1] = 0
+
+    # projection -> (components, writes the plane below its particles)
+    PROJECTIONS = {"vector": (3, False), "symtensor": (6, False),
+                   "vector_cic": (3, True), "vecvec_cic": (6, True)}
+
+    def project(self, kind, f):
+        """Projection `kind` (vector, symtensor: CIC-NGP; vector_cic,
+        vecvec_cic: full CIC) of the own particles into f, a field of this
+        domain with the projection's components, with the slab folds; the
+        ghost planes of f end at zero."""
+        if kind not in self.PROJECTIONS:
+            raise ValueError(f"unknown projection {kind!r}")
+        comps, lower = self.PROJECTIONS[kind]
+        a = f[0]
+        if int(a.shape[0]) != comps:
+            raise ValueError(f"{kind} needs a field of {comps} components, got {int(a.shape[0])}")
+        self.engine.project(kind, f)
+        buf = self._plane_buf(a)
+        self._shift(a[:, self.nz + 1], self.up, buf, self.down)   # -> plane 1 of the rank above
+        a[:, 1] += buf
+        if lower:
+            buf = self._plane_buf(a)
+            self._shift(a[:, 0], self.down, buf, self.up)         # -> plane nz of the rank below
+            a[:, self.nz] += buf
+        a[:, 0] = 0
+        a[:, self.nz + 1] = 0
+
+    def _all_to_all(self, send, recv):
+        """Block r of send (split along dim 0) to rank r, block s of recv
+        from rank s."""
+        if self.size == 1:
+            recv.copy_(send)
+            return
+        t = self.engine.torch
+        a, b = t.view_as_real(send), t.view_as_real(recv)
+        self.dist.all_to_all_single(b, a, group=self.group)
+
+    def pm_force(self, rho, F, coupling, phi=None):
+        """F (3 components) = -grad phi with lap7(phi) = coupling (rho - mean
+        rho) on the global lattice, from rho's own planes (after deposit);
+        phi (1 component), when given, receives the potential.  F's and
+        phi's ghost planes are filled."""
+        n = self.n[0]
+        if self.n[1] != n or self.n[2] != n:
+            raise ValueError("the PM operator needs a cubic lattice")
+        R, nz = self.size, self.nz
+        nky, nkx = n // R, n // 2 + 1
+        e = self.engine
+        e.fft_prepare(n, nz, nky)
+        A = e.complex_buffer((nz, n, nkx))
+        e.planes_r2c(rho[0][0, 1:nz + 1], A)
+        send = A.view(nz, R, nky, nkx).permute(1, 0, 2, 3).contiguous()  # [to rank][z][ky][kx]
+        B = e.complex_buffer((n, nky, nkx))                              # [z from all][ky][kx]
+        self._all_to_all(send, B.view(R, nz, nky, nkx))
+        e.lines(B, _lib.FFT_FORWARD)
+        e.green(B, self.rank * nky, coupling)
+        e.lines(B, _lib.FFT_BACKWARD)
+        back = e.complex_buffer((R, nz, nky, nkx))                       # [from rank][z][ky][kx]
+        self._all_to_all(B.view(R, nz, nky, nkx), back)
+        A = back.permute(1, 0, 2, 3).reshape(nz, n, nkx).contiguous()
+        p = phi if phi is not None else self.field(1)
+        e.planes_c2r(A, p[0][0, 1:nz + 1])
+        self.fill_ghosts(p)
+        e.gradient(p, F)
+        self.fill_ghosts(F)
 
     def migrate(self):
         out = self.engine.extract_outside(1, self.nz)

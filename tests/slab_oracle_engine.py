@@ -11,7 +11,8 @@ from latfield2_b200 import _lib
 class OracleEngine:
     """Local work on the CPU with the oracle's restatement of the device
     arithmetic (FP32 kick and drift, int64 fixed-point deposit), bit-exact
-    with CudaEngine; global particle mass and the fixed-point mode only."""
+    with CudaEngine, and the oracle's FP64 projections; global particle mass
+    and the fixed-point mode only."""
 
     def __init__(self, n_local, res, mode, device=None):
         import torch
@@ -52,6 +53,52 @@ class OracleEngine:
         acc = self.O.state_deposit_fixed(self.n, self.cell, self.off)
         scale = np.float32(2.0 ** -32 * self.gmass / (self.res ** 3))
         rho[0][0] = self.torch.from_numpy(self.O.fixed_to_f32(acc, scale).reshape(rho[0].shape[1:]))
+
+    def project(self, kind, f):
+        """The oracle's FP64 projection on the local periodic lattice (halo 1,
+        with its _comm fold), stored in FP32 as the device stores it."""
+        cs, order = self.O.lists_from_insertion(self.n, self.cell)
+        pos = self.O.state_to_pos(self.n, self.res, self.cell, self.off)[order]
+        vel = self.vel.astype(np.float64)[order]
+        fn = {"vector": self.O.vector_cicngp, "symtensor": self.O.symtensor_cicngp,
+              "vector_cic": self.O.vector_cic, "vecvec_cic": self.O.vecvec_cic}[kind]
+        g = self.O.interior(fn(self.n, 1, self.res, cs, pos, vel, gmass=self.gmass), self.n, 1)
+        f[0][:] = self.torch.from_numpy(g.astype(np.float32))
+
+    # the PM operator's pieces in FP64 numpy, stored in complex64 / FP32
+    def fft_prepare(self, n, nz, nky):
+        self.fft_n = n
+
+    def complex_buffer(self, shape):
+        return self.torch.empty(shape, dtype=self.torch.complex64)
+
+    def planes_r2c(self, planes, A):
+        a = np.fft.rfft2(planes.numpy().astype(np.float64), axes=(1, 2))
+        A.copy_(self.torch.from_numpy(a.astype(np.complex64)))
+
+    def planes_c2r(self, A, planes):
+        n = self.fft_n
+        r = np.fft.irfft2(A.numpy().astype(np.complex128), s=(n, n), axes=(1, 2)) * float(n * n)
+        planes.copy_(self.torch.from_numpy(r.astype(np.float32)))
+
+    def lines(self, B, direction):
+        b = B.numpy().astype(np.complex128)
+        b = np.fft.fft(b, axis=0) if direction == 1 else np.fft.ifft(b, axis=0) * b.shape[0]
+        B.copy_(self.torch.from_numpy(b.astype(np.complex64)))
+
+    def green(self, B, ky0, coupling):
+        from oracle import fft_oracle as FO
+        n = self.fft_n
+        nky = int(B.shape[1])
+        lam = FO.laplacian_eigenvalues(n, self.res)[:, ky0:ky0 + nky, :]
+        g = np.where(lam == 0.0, 0.0, coupling / np.where(lam == 0.0, 1.0, lam)) / float(n) ** 3
+        B.copy_(self.torch.from_numpy((B.numpy().astype(np.complex128) * g).astype(np.complex64)))
+
+    def gradient(self, phi, F):
+        p = phi[0][0].numpy().astype(np.float64)
+        for c, axis in enumerate((2, 1, 0)):
+            g = -(np.roll(p, -1, axis) - np.roll(p, 1, axis)) / (2.0 * self.res)
+            F[0][c] = self.torch.from_numpy(g.astype(np.float32))
 
     def extract_outside(self, zlo, zhi):
         z = self.cell // (self.n[0] * self.n[1])

@@ -137,3 +137,58 @@ def test_one_rank_slab_domain_equals_the_single_gpu_step(n):
     zs = cell // (n[0] * n[1])
     zf = want["cell"] // (n[0] * n[1])
     assert np.sum(np.abs(zs[want["id"]] - zf) > n[2] // 2) > 50  # crossed the periodic z face
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (40, 24, 20)])
+def test_one_rank_slab_projections_equal_the_single_gpu_deposits(n):
+    """SlabDomain.project with one rank (both folds go to itself) against the
+    library's deposits on the whole lattice: vector and symtensor CIC-NGP,
+    full-CIC vector and VecVec, within 1e-5 of each component's maximum
+    (FP32 shared atomics in another order, plus the FP32 fold)."""
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    cell, off, vel = small_case(n, 60000, seed=13)
+    gm = 1.0 / cell.shape[0]
+    ref = _ctx(n)
+    ref.set_particles(cell, off, vel, global_mass=gm)
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64)
+    d.set_particles(cell, off, vel, gm)
+    for kind, (comps, _) in SlabDomain.PROJECTIONS.items():
+        want = ref.field(comps)
+        getattr(ref, "deposit_" + kind)(want)
+        w = want.export_internal()
+        f = d.field(comps)
+        d.project(kind, f)
+        got = d.own_planes(f)
+        for c in range(comps):
+            assert np.abs(got[c] - w[c]).max() <= 1e-5 * np.abs(w[c]).max(), (kind, c)
+
+
+@pytest.mark.parametrize("n", [32, 48])
+def test_one_rank_slab_pm_force_equals_the_single_gpu_operator(n):
+    """SlabDomain.pm_force with one rank (the slab transforms through
+    lf2_slab_fft_*, lf2_slab_green and lf2_pm_gradient) against lf2_pm_force
+    on the whole lattice and against the FP64 oracle: 1e-5 of the maximum."""
+    import torch
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    from oracle import fft_oracle as FO
+    coupling = 4 * np.pi
+    rng = np.random.default_rng(n)
+    rho_g = (1.0 + rng.standard_normal((n, n, n))).astype(np.float32)
+    ref = _ctx((n, n, n))
+    Fr = ref.field(3)
+    ref.pm_force(ref.field(1, torch.from_numpy(rho_g.reshape(-1)).cuda()), Fr, coupling)
+    want = Fr.export_internal()
+    phi64, F64 = FO.pm_force(rho_g, 1.0 / n, coupling)
+    d = SlabDomain((n, n, n), box=1.0, mode=_lib.DEPOSIT_FIXED64)
+    rho = d.field(1)
+    d.set_own_planes(rho, rho_g[None])
+    F, phi = d.field(3), d.field(1)
+    d.pm_force(rho, F, coupling, phi)
+    got = d.own_planes(F)
+    for c in range(3):
+        scale = np.abs(F64[c]).max()
+        assert np.abs(got[c] - want[c]).max() <= 1e-5 * scale, c
+        assert np.abs(got[c] - F64[c]).max() <= 1e-5 * scale, c
+    assert np.abs(d.own_planes(phi)[0] - phi64).max() <= 1e-5 * np.abs(phi64).max()

@@ -8,7 +8,10 @@ Against a single-domain run of the same arithmetic on the whole lattice:
 particles (by id) bit-exact after several steps (the kick reads the same
 force values, the drift is per particle); the density within 1e-6 of its
 maximum (the fold adds two FP32 values where one domain converts one exact
-integer sum).
+integer sum).  The vector and symtensor CIC-NGP projections and the full-CIC
+vector and VecVec projections of the final state, each folded across the
+slab faces, within 1e-6 of their maximum of the oracle's FP64 projection on
+the whole lattice.
 """
 import os
 import socket
@@ -23,6 +26,8 @@ from tests.helpers import small_case
 N = (16, 12, 16)
 STEPS = 4
 DTK, DTD = 0.05, 0.02
+KINDS = {"vector": (3, O.vector_cicngp), "symtensor": (6, O.symtensor_cicngp),
+         "vector_cic": (3, O.vector_cic), "vecvec_cic": (6, O.vecvec_cic)}
 
 
 def _case():
@@ -61,7 +66,12 @@ def _run_domain(dist_initialised):
     for k in range(STEPS):
         d.step(Ff, DTK, DTD, rho if k == STEPS - 1 else None)
     p = d.particles_global()
-    return d.rank, d.z0, d.nz, p, d.own_planes(rho)[0]
+    proj = {}
+    for kind, (comps, _) in KINDS.items():
+        f = d.field(comps)
+        d.project(kind, f)
+        proj[kind] = d.own_planes(f)
+    return d.rank, d.z0, d.nz, p, d.own_planes(rho)[0], proj
 
 
 def _check(results):
@@ -74,9 +84,20 @@ def _check(results):
     np.testing.assert_array_equal(got["off"][order], o1)
     np.testing.assert_array_equal(got["vel"][order], v1)
     rho = np.zeros_like(rho1)
-    for _, z0, nz, _, r in results:
+    for _, z0, nz, _, r, _ in results:
         rho[z0:z0 + nz] = r
     assert np.abs(rho - rho1).max() <= 1e-6 * np.abs(rho1).max()
+    res = 1.0 / N[0]
+    cs, order = O.lists_from_insertion(N, c1)
+    pos = O.state_to_pos(N, res, c1, o1)[order]
+    vv = v1.astype(np.float64)[order]
+    for kind, (comps, fn) in KINDS.items():
+        want = O.interior(fn(N, 1, res, cs, pos, vv, gmass=1.0 / cell.shape[0]), N, 1)
+        got = np.zeros_like(want)
+        for _, z0, nz, _, _, proj in results:
+            got[:, z0:z0 + nz] = proj[kind]
+        for c in range(comps):
+            assert np.abs(got[c] - want[c]).max() <= 1e-6 * np.abs(want[c]).max(), (kind, c)
     # many particles changed slab (the periodic face included)
     nz = results[0][2]
     moved = (cell // (N[0] * N[1]) // nz) != (c1 // (N[0] * N[1]) // nz)
@@ -95,7 +116,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, out):
+def _worker(rank, world, port, out, fn="_run_domain"):
     import datetime
 
     import torch.distributed as dist
@@ -104,7 +125,7 @@ def _worker(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
     try:
-        out.put(_run_domain(True))
+        out.put(globals()[fn](True))
     finally:
         dist.destroy_process_group()
 
@@ -136,3 +157,56 @@ def test_too_fast_a_particle_is_refused():
     d.set_own_planes(Ff, F)
     with pytest.raises(RuntimeError, match="less than one cell"):
         d.step(Ff, DTK, DTD)
+
+
+NPM = 16
+COUPLING = 4 * np.pi
+
+
+def _pm_field():
+    rng = np.random.default_rng(31)
+    return (1.0 + rng.standard_normal((NPM, NPM, NPM))).astype(np.float32)
+
+
+def _run_pm(dist_initialised):
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    d = SlabDomain((NPM,) * 3, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=OracleEngine)
+    rho = d.field(1)
+    d.set_own_planes(rho, _pm_field()[None])
+    F, phi = d.field(3), d.field(1)
+    d.pm_force(rho, F, COUPLING, phi)
+    return d.rank, d.z0, d.nz, F[0].numpy().copy(), phi[0].numpy().copy()
+
+
+def _check_pm(results):
+    from oracle import fft_oracle as FO
+    phi_ref, F_ref = FO.pm_force(_pm_field(), 1.0 / NPM, COUPLING)
+    for _, z0, nz, F, phi in results:
+        planes = [(z0 - 1 + p) % NPM for p in range(nz + 2)]  # ghost planes included
+        for c in range(3):
+            assert np.abs(F[c] - F_ref[c][planes]).max() <= 1e-5 * np.abs(F_ref[c]).max(), c
+        assert np.abs(phi[0] - phi_ref[planes]).max() <= 1e-5 * np.abs(phi_ref).max()
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_pm_force_over_slabs(world):
+    """SlabDomain.pm_force (plane transforms, all-to-all transposes, line
+    transforms, Green's function, gradient with ghost planes) against the
+    single-domain FP64 PM force, on 1, 2 and 4 gloo ranks."""
+    if world == 1:
+        _check_pm([_run_pm(False)])
+        return
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, "_run_pm"))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    _check_pm(res)
