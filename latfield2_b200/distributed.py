@@ -342,6 +342,43 @@ class SlabDomain:
     def count(self):
         return self.engine.count()
 
+    def save_particles(self, path, global_mass, relativistic=0, type_name="part_simple"):
+        """All ranks' particles (which must carry IDs) as one snapshot in the
+        layout of Particles::saveHDF5 (latfield2_b200.snapshot): rank 0
+        gathers every rank's records, in rank order, and writes `path`."""
+        from . import snapshot as S
+        p = self.particles_global()
+        if "id" not in p:
+            raise ValueError("a snapshot needs particle IDs")
+        pos = S.cells_to_positions(p["cell"], p["off"], self.n, self.res)
+        data = S.records(p["cell"], pos, p["vel"], p["id"])
+        parts = [data]
+        if self.size > 1:
+            parts = [None] * self.size if self.rank == 0 else None
+            self.dist.gather_object(data, parts, dst=0, group=self.group)
+        if self.rank == 0:
+            box = tuple(self.res * v for v in self.n)
+            attrs, num, offs, size = S.description(self.n, box, self.size,
+                                                   [d.shape[0] for d in parts])
+            S.write(path, np.concatenate(parts), S.part_info(global_mass, relativistic, type_name),
+                    attrs, num, offs, size)
+        if self.size > 1:
+            self.dist.barrier(group=self.group)
+
+    def load_particles(self, path):
+        """Particles of a snapshot (saved from any number of ranks): every
+        rank reads it and keeps the particles of its own planes, as
+        Particles::loadHDF5 adds the records of the blocks that overlap its
+        box.  Returns the part_info record."""
+        from . import snapshot as S
+        snap = S.read(path)
+        S.check_box(snap, tuple(self.res * v for v in self.n))
+        ids, pos, vel = S.columns(snap["data"])
+        cell, off = S.positions_to_cells(pos, self.n, self.res)
+        info = snap["part_info"][0]
+        self.set_particles(cell, off, vel.astype(np.float32), float(info["mass"]), ids=ids)
+        return info
+
     def particles_global(self):
         """The local particles with global cell indices (numpy dict)."""
         p = self.engine.particles()

@@ -70,3 +70,45 @@ def test_other_lattice_is_refused(tmp_path):
     (tmp_path / "junk").write_bytes(b"not a checkpoint at all" * 10)
     with pytest.raises(L.LF2Error, match="not a checkpoint"):
         a.checkpoint_load(tmp_path / "junk")
+
+
+def test_snapshot_in_the_reference_layout_round_trips(tmp_path):
+    """latfield2_b200.snapshot: a Context's particles saved as part_simple
+    records and loaded into a fresh Context (bit-exact by ID: res is a power
+    of two), and a one-rank SlabDomain on the GPU saved and loaded the same
+    way, after steps that moved particles across cells."""
+    from latfield2_b200 import _lib
+    from latfield2_b200 import snapshot as S
+    from latfield2_b200.distributed import SlabDomain
+    n = (32, 32, 32)
+    cell, off, vel = small_case(n, 40000, seed=35, vel_sigma=0.05)
+    ids = np.arange(cell.shape[0], dtype=np.int64)[::-1].copy()
+    gm = 1.0 / cell.shape[0]
+    F = torch.from_numpy(np.random.default_rng(36).standard_normal((3, n[2], n[1], n[0]))
+                         .astype(np.float32) * 0.05).cuda()
+    a = _ctx(n)
+    a.set_particles(cell, off, vel, global_mass=gm, ids=ids)
+    Fa = a.field(3, F)
+    for _ in range(2):
+        a.step(Fa, 0.05, 0.1, None)
+    want = a.get_particles(ids=True)
+    path = tmp_path / "parts.npz"
+    S.save_context(path, a, gm)
+    snap = S.read(path)
+    assert snap["data"].shape[0] == cell.shape[0] and snap["part_info"]["mass"][0] == gm
+    assert np.all(np.diff(S.positions_to_cells(S.columns(snap["data"])[1], n, 1.0 / 32)[0]) >= 0)
+    b = _ctx(n)
+    S.load_context(path, b)
+    got = b.get_particles(ids=True)
+    o1, o2 = np.argsort(want["id"]), np.argsort(got["id"])
+    for k in ("id", "cell", "off", "vel"):
+        np.testing.assert_array_equal(got[k][o2], want[k][o1], err_msg=k)
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64)
+    d.set_particles(want["cell"], want["off"], want["vel"], gm, ids=want["id"])
+    d.save_particles(tmp_path / "slab.npz", gm)
+    c = _ctx(n)
+    S.load_context(tmp_path / "slab.npz", c)
+    got = c.get_particles(ids=True)
+    o3 = np.argsort(got["id"])
+    for k in ("id", "cell", "off", "vel"):
+        np.testing.assert_array_equal(got[k][o3], want[k][o1], err_msg=k)
