@@ -22,6 +22,13 @@ Reals, little-endian), so a writer with HDF5 at hand copies them one to one.
 Order: the reference writes a rank's particles cell by cell in site order
 and, inside a cell, in its list order.  The library does not keep list
 order, so particles inside a cell are written by increasing ID.
+
+Fields: Field::saveHDF5(filename, dataset_name = "data")
+(LATfield2_Field_decl.hpp:309-310, :1532-1544, written by save_hdf5,
+LATfield2_save_hdf5.h:15-140) stores one dataset of the global lattice,
+dims [z][y][x] and, with several components, an array type of comps Reals
+per site; save_field writes that array (shape (n2, n1, n0) or
+(n2, n1, n0, comps)) under the dataset name.
 """
 import numpy as np
 
@@ -153,3 +160,23 @@ def load_context(path, ctx):
     info = snap["part_info"][0]
     ctx.set_positions(pos, vel, global_mass=float(info["mass"]), ids=ids)
     return info
+
+
+def save_field(path, field, dataset_name="data", dtype=np.float64):
+    """A field (FieldHandle) as the dataset of Field::saveHDF5, halo excluded."""
+    a = field.export(halo=0, dtype=dtype)
+    if a.shape[3] == 1:
+        a = a[..., 0]
+    with open(path, "wb") as f:
+        np.savez(f, **{dataset_name: np.ascontiguousarray(a)})
+
+
+def load_field(path, field, dataset_name="data"):
+    """Field::loadHDF5: the dataset into `field` (same lattice and components)."""
+    with np.load(path, allow_pickle=False) as z:
+        a = z[dataset_name]
+    n = field.ctx.n
+    want = (n[2], n[1], n[0]) + (() if field.comps == 1 else (field.comps,))
+    if tuple(a.shape) != want:
+        raise ValueError(f"dataset {dataset_name!r} has shape {a.shape}, the field {want}")
+    field.import_(np.ascontiguousarray(a.reshape(n[2], n[1], n[0], field.comps)), halo=0)

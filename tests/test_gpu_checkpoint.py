@@ -112,3 +112,33 @@ def test_snapshot_in_the_reference_layout_round_trips(tmp_path):
     o3 = np.argsort(got["id"])
     for k in ("id", "cell", "off", "vel"):
         np.testing.assert_array_equal(got[k][o3], want[k][o1], err_msg=k)
+
+
+def test_field_snapshot_in_the_reference_layout(tmp_path):
+    """snapshot.save_field / load_field: the dataset of Field::saveHDF5
+    (dims [z][y][x], comps Reals per site) of a deposited density and of a
+    3-component field, back into fresh fields bit for bit (FP32 values
+    stored as double)."""
+    from latfield2_b200 import snapshot as S
+    n = (24, 20, 16)
+    cell, off, vel = small_case(n, 20000, seed=37)
+    a = _ctx(n)
+    a.set_particles(cell, off, vel, global_mass=1e-4)
+    rho = a.field(1)
+    a.deposit_scalar(rho)
+    v = a.field(3)
+    a.deposit_vector(v)
+    S.save_field(tmp_path / "rho.npz", rho)
+    S.save_field(tmp_path / "v.npz", v, dataset_name="vel")
+    with np.load(tmp_path / "rho.npz") as z:
+        assert z["data"].shape == (16, 20, 24) and z["data"].dtype == np.float64
+    with np.load(tmp_path / "v.npz") as z:
+        assert z["vel"].shape == (16, 20, 24, 3)
+    b = _ctx(n)
+    r2, v2 = b.field(1), b.field(3)
+    S.load_field(tmp_path / "rho.npz", r2)
+    S.load_field(tmp_path / "v.npz", v2, dataset_name="vel")
+    np.testing.assert_array_equal(r2.export_internal(), rho.export_internal())
+    np.testing.assert_array_equal(v2.export_internal(), v.export_internal())
+    with pytest.raises(ValueError, match="shape"):
+        S.load_field(tmp_path / "rho.npz", v2)
