@@ -142,10 +142,12 @@ def cells_to_positions(cell, off, n, res):
 
 
 def save_context(path, ctx, global_mass, relativistic=0, type_name="part_simple"):
-    """Particles of one Context (which must carry IDs) as a one-rank snapshot."""
-    cell = ctx.get_particles()["cell"]
-    pos, vel, ids = ctx.get_positions(np.float64, ids=True)
-    data = records(cell, pos, vel, ids)
+    """Particles of one Context (which must carry IDs) as a one-rank snapshot.
+    part_simple has no per-particle mass: a store with per-particle masses
+    keeps them only in lf2_checkpoint_save's format."""
+    p = ctx.get_particles(ids=True)
+    pos = cells_to_positions(p["cell"], p["off"], ctx.n, ctx.res)
+    data = records(p["cell"], pos, p["vel"], p["id"])
     attrs, num, offs, size = description(ctx.n, ctx.box, 1, [data.shape[0]])
     write(path, data, part_info(global_mass, relativistic, type_name), attrs, num, offs, size)
 

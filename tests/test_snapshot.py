@@ -163,3 +163,40 @@ def test_slab_save_on_two_ranks_restores_on_any_number(tmp_path, load_world):
     np.testing.assert_array_equal(parts["off"][order], off[want])
     np.testing.assert_array_equal(parts["vel"][order], vel[want])
     assert all(g[2] == 1.0 / cell.shape[0] for g in got)
+
+
+class _FakeContext:
+    """The Context methods the snapshot functions call, on host arrays."""
+
+    def __init__(self, n, box):
+        self.n, self.box, self.res = n, box, box[0] / n[0]
+        self.parts = None
+        self.loaded = None
+
+    def get_particles(self, ids=False):
+        return dict(self.parts)
+
+    def set_positions(self, pos, vel, global_mass=0.0, ids=None):
+        self.loaded = (pos, vel, global_mass, ids)
+
+
+def test_context_snapshot_functions_on_host_arrays(tmp_path):
+    cell, off, vel, ids = _case()
+    a = _FakeContext(N, (1.0, 0.75, 1.0))
+    a.parts = {"cell": cell, "off": off, "vel": vel, "id": ids}
+    S.save_context(tmp_path / "c.npz", a, 0.125, type_name="part_simple")
+    snap = S.read(tmp_path / "c.npz")
+    assert list(snap["numParts"]) == [cell.shape[0]] and list(snap["@grid_size"]) == [1, 1]
+    b = _FakeContext(N, (1.0, 0.75, 1.0))
+    info = S.load_context(tmp_path / "c.npz", b)
+    pos, v, gm, i = b.loaded
+    assert gm == 0.125 and info["type_name"] == b"part_simple"
+    c2, o2 = S.positions_to_cells(pos, N, 1.0 / 16)
+    order = np.argsort(i)
+    want = np.argsort(ids)
+    np.testing.assert_array_equal(i[order], ids[want])
+    np.testing.assert_array_equal(c2[order], cell[want])
+    np.testing.assert_array_equal(o2[order], off[want])
+    np.testing.assert_array_equal(v[order], vel[want].astype(np.float64))
+    with pytest.raises(ValueError, match="boxSize"):
+        S.load_context(tmp_path / "c.npz", _FakeContext(N, (1.0, 1.0, 1.0)))
