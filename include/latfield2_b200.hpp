@@ -47,6 +47,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <ostream>
@@ -403,6 +404,42 @@ class Field {
     host_newer_ = true;
   }
 
+  // Field::write (LATfield2_Field_decl.hpp:1179-1239): the lattice without
+  // halo, x fastest, components interleaved, raw FieldType values, no header
+  // (the file the reference's ranks write together; here one process holds
+  // the whole lattice).
+  void write(const std::string& filename)
+  {
+    if (device_newer_) pull();
+    std::FILE* f = std::fopen(filename.c_str(), "wb");
+    if (!f) throw std::runtime_error("Field::write: cannot open " + filename);
+    bool ok = true;
+    for (int z = 0; z < lat_->size(2) && ok; z++)
+      for (int y = 0; y < lat_->size(1) && ok; y++)
+        ok = std::fwrite(row(y, z), sizeof(FieldType), row_values(), f) == row_values();
+    if (std::fclose(f) != 0 || !ok) throw std::runtime_error("Field::write: cannot write " + filename);
+  }
+  // Field::read (LATfield2_Field_decl.hpp:1286-1345): a file of write's
+  // layout, then updateHalo.
+  void read(const std::string& filename)
+  {
+    std::FILE* f = std::fopen(filename.c_str(), "rb");
+    if (!f) throw std::runtime_error("Field::read: cannot open " + filename);
+    bool ok = true;
+    for (int z = 0; z < lat_->size(2) && ok; z++)
+      for (int y = 0; y < lat_->size(1) && ok; y++)
+        ok = std::fread(row(y, z), sizeof(FieldType), row_values(), f) == row_values();
+    std::fclose(f);
+    if (!ok) throw std::runtime_error("Field::read: short file " + filename);
+    device_newer_ = false;
+    host_newer_ = true;
+    updateHalo();
+  }
+  // Field::saveHDF5 / loadHDF5 of a build without HDF5
+  // (LATfield2_Field_decl.hpp:1532-1555): the binary file filename + "BIN".
+  void saveHDF5(const std::string& filename, const std::string& = "data") { write(filename + "BIN"); }
+  void loadHDF5(const std::string& filename, const std::string& = "data") { read(filename + "BIN"); }
+
   int components() const { return components_; }
   int rows() const { return rows_; }
   int cols() const { return cols_; }
@@ -462,6 +499,14 @@ class Field {
     }
     return j * rows_ + i;
   }
+  // first value of the x-row (y, z) of the interior, and the values in it
+  FieldType* row(int y, int z)
+  {
+    const int h = lat_->halo();
+    const long i = h + (long)lat_->gross(0) * ((y + h) + (long)lat_->gross(1) * (z + h));
+    return &data_[(size_t)(i * components_)];
+  }
+  size_t row_values() const { return (size_t)lat_->size(0) * components_; }
   void fill_halo()
   {
     const int h = lat_->halo();

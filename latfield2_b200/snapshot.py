@@ -28,7 +28,10 @@ Fields: Field::saveHDF5(filename, dataset_name = "data")
 LATfield2_save_hdf5.h:15-140) stores one dataset of the global lattice,
 dims [z][y][x] and, with several components, an array type of comps Reals
 per site; save_field writes that array (shape (n2, n1, n0) or
-(n2, n1, n0, comps)) under the dataset name.
+(n2, n1, n0, comps)) under the dataset name.  A build of the reference
+without HDF5 writes filename + "BIN" with Field::write instead
+(LATfield2_Field_decl.hpp:1179-1239): the same array as raw Reals, no
+header; write_field_binary / read_field_binary produce and read that file.
 """
 import numpy as np
 
@@ -182,3 +185,21 @@ def load_field(path, field, dataset_name="data"):
     if tuple(a.shape) != want:
         raise ValueError(f"dataset {dataset_name!r} has shape {a.shape}, the field {want}")
     field.import_(np.ascontiguousarray(a.reshape(n[2], n[1], n[0], field.comps)), halo=0)
+
+
+def write_field_binary(path, field, real_bytes=8):
+    """Field::write's file: the lattice without halo, [z][y][x][comps], raw
+    Reals of real_bytes (8 double, 4 SINGLE), no header."""
+    a = field.export(halo=0, dtype=np.float64 if real_bytes == 8 else np.float32)
+    with open(path, "wb") as f:
+        f.write(np.ascontiguousarray(a).tobytes())
+
+
+def read_field_binary(path, field, real_bytes=8):
+    """Field::read: a file of write_field_binary's layout into `field`."""
+    n = field.ctx.n
+    a = np.fromfile(path, dtype=np.float64 if real_bytes == 8 else np.float32)
+    if a.size != n[0] * n[1] * n[2] * field.comps:
+        raise ValueError(f"{path}: {a.size} values, the field has "
+                         f"{n[0] * n[1] * n[2] * field.comps}")
+    field.import_(a.reshape(n[2], n[1], n[0], field.comps), halo=0)

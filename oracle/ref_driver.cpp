@@ -35,6 +35,8 @@
 //        the local gross real field.  OP_POISSON: the reference's Poisson
 //        example (examples/poissonSolver.cpp) on the same real field, res =
 //        1/n: the local gross potential.
+//        With LF2_REF_FIELD_WRITE=<path>, the vector CIC-NGP field is also
+//        written to <path> by the reference's Field::write.
 #include <cstdint>
 #include <chrono>
 #include <cstdio>
@@ -273,6 +275,8 @@ int main(int argc, char** argv)
     vectorProjectionCICNGP_project(&parts, &B);
     vectorProjectionCICNGP_comm(&B);
     write_field(o, B);
+    // the reference's own binary field file (Field::write), when asked
+    if (const char* fw = getenv("LF2_REF_FIELD_WRITE")) B.write(fw);
   }
   if (ops & OP_TENSOR) {
     Field<Real> T(lat, 3, 3, symmetric);
