@@ -868,6 +868,32 @@ class Particles {
     lf2detail::check(ctx_, lf2_drift_rebin(ctx_, dtau), "lf2_drift_rebin");
   }
 
+  // Particles::saveHDF5 / loadHDF5 (LATfield2_Particles.hpp:2808-3045) for a
+  // restart.  HDF5 is not available to this layer: the particles go to
+  // filename_base + ".lf2c" in lf2_checkpoint_save's format (the library's
+  // state; a restored run continues bit for bit).  fileNumber must be 1 (one
+  // process).  loadHDF5 replaces the particles, as a restart into an empty
+  // set does in the reference (which adds the file's particles to the set).
+  // latfield2_b200.snapshot writes the reference's HDF5 datasets themselves.
+  void saveHDF5(const std::string& filename_base, int fileNumber)
+  {
+    one_file(fileNumber, "saveHDF5");
+    sync();
+    lf2detail::check(ctx_, lf2_checkpoint_save(ctx_, (filename_base + ".lf2c").c_str()),
+                     "lf2_checkpoint_save");
+  }
+  void loadHDF5(const std::string& filename_base, int fileNumber)
+  {
+    one_file(fileNumber, "loadHDF5");
+    if (!ctx_) throw std::logic_error("Particles: initialize() first");
+    pos_.clear(), vel_.clear(), ids_.clear(), mass_.clear();
+    lf2detail::check(ctx_, lf2_checkpoint_load(ctx_, (filename_base + ".lf2c").c_str()),
+                     "lf2_checkpoint_load");
+    int64_t n = 0;
+    lf2detail::check(ctx_, lf2_particles_count(ctx_, &n), "lf2_particles_count");
+    on_device_ = n;
+  }
+
   Lattice& lattice() { return *lat_; }
   Real res() { return res_; }
   // a field used with these particles covers the same sites
@@ -938,6 +964,12 @@ class Particles {
   }
 
  private:
+  static void one_file(int fileNumber, const char* what)
+  {
+    if (fileNumber != 1)
+      throw std::invalid_argument(std::string("Particles::") + what + ": one file (one process)");
+  }
+
   std::shared_ptr<lf2_ctx> owner_;  // released by the last of the particles and their fields
   lf2_ctx* ctx_ = nullptr;
   Lattice* lat_ = nullptr;

@@ -121,3 +121,21 @@ def test_poisson_demo_matches_the_oracle(cuda, tmp_path, khalo):
     assert normalized_error(k.real, want.real) < 1e-5
     assert normalized_error(k.imag, want.imag) < 1e-5
     assert normalized_error(phi.reshape(n, n, n), FO.poisson_example(rho, 1.0 / n)) < 1e-5
+
+
+def test_restart_demo_builds_against_the_header(tmp_path):
+    import build_demo
+    assert os.path.exists(build_demo.build(str(tmp_path / "restart_demo"),
+                                           source="restart_demo.cpp"))
+
+
+@pytest.mark.gpu
+def test_restart_through_particles_save_and_load(cuda, tmp_path):
+    """Particles::saveHDF5 / loadHDF5 of the C++ layer: a set restored from
+    the file continues bit for bit (tests/compat/restart_demo.cpp)."""
+    import build_demo
+    exe = build_demo.build(str(tmp_path / "restart_demo"), source="restart_demo.cpp")
+    r = subprocess.run([exe, "24", "20000", str(tmp_path)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
+    assert os.path.exists(tmp_path / "run.lf2c")
