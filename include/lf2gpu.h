@@ -297,7 +297,9 @@ lf2_status lf2_pm_force(lf2_ctx* ctx, lf2_field rho, lf2_field phi,
  *     lf2_pm_force (coupling, 1/n^3 included, zero mode removed); B 16-byte
  *     aligned
  *   pm_gradient: F_i = -(phi(x+e_i) - phi(x-e_i)) / (2 res) on ctx's
- *     lattice, periodic (with filled ghost planes, exact on the own planes) */
+ *     lattice, periodic (with filled ghost planes, exact on the own planes)
+ * The transforms run on ctx's stream.  A slab FFT belongs to its context:
+ * destroy it before the context. */
 #define LF2_FFT_FORWARD 1
 #define LF2_FFT_BACKWARD (-1)
 lf2_status lf2_slab_fft_create(lf2_ctx* ctx, int n, int nz, int nky,
