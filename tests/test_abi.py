@@ -62,6 +62,35 @@ def test_null_context_is_an_argument_error():
     assert lib.lf2_last_error(None) == b"null context"
 
 
+def test_next_row_entry_points_reject_null_arguments():
+    """The full-CIC, migration, checkpoint and PM-operator entry points
+    return LF2_ERR_ARG on a null context or handle before any device work."""
+    from latfield2_b200 import _lib
+    lib = _lib.load()
+    E = _lib.LF2_ERR_ARG
+    n = ctypes.c_int64()
+    assert lib.lf2_deposit_vector_cic(None, None) == E
+    assert lib.lf2_deposit_vecvec_cic(None, None) == E
+    assert lib.lf2_particles_extract_z(None, 0, 1, 0, None, None, None, None, None,
+                                       ctypes.byref(n)) == E
+    assert lib.lf2_particles_add(None, 0, None, None, None, None, None, 0) == E
+    assert lib.lf2_checkpoint_save(None, b"x") == E
+    assert lib.lf2_checkpoint_load(None, b"x") == E
+    assert lib.lf2_kfield_create(None, 1, None) == E
+    assert lib.lf2_fft_forward(None, None, None) == E
+    assert lib.lf2_pm_force(None, None, None, None, 1.0) == E
+    assert lib.lf2_pm_force4(None, None, None, 1.0) == E
+    assert lib.lf2_pm_force4_adjoint(None, None, None, 1.0) == E
+    assert lib.lf2_pm_gradient(None, None, None) == E
+    h = ctypes.c_void_p()
+    assert lib.lf2_slab_fft_create(None, 16, 4, 4, ctypes.byref(h)) == E
+    assert lib.lf2_slab_fft_planes_r2c(None, None, None) == E
+    assert lib.lf2_slab_fft_planes_c2r(None, None, None) == E
+    assert lib.lf2_slab_fft_lines(None, None, _lib.FFT_FORWARD) == E
+    assert lib.lf2_slab_green(None, None, 0, 1.0) == E
+    assert lib.lf2_slab_fft_destroy(None) == _lib.LF2_OK
+
+
 def test_sources_target_sm100a_only():
     from latfield2_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
