@@ -339,6 +339,14 @@ class SlabDomain:
         if rho is not None:
             self.deposit(rho)
 
+    def pm_step(self, rho, F, dtau_kick, dtau_drift, coupling):
+        """One self-consistent particle-mesh step over the slabs: deposit
+        rho from the particles, the PM force F from rho (pm_force), then
+        kick + drift + rebin and migration (step)."""
+        self.deposit(rho)
+        self.pm_force(rho, F, coupling)
+        self.step(F, dtau_kick, dtau_drift)
+
     def count(self):
         return self.engine.count()
 

@@ -210,3 +210,56 @@ def test_pm_force_over_slabs(world):
         p.join(timeout=60)
         assert p.exitcode == 0
     _check_pm(res)
+
+
+def _run_pm_steps(dist_initialised):
+    """Three self-consistent PM steps of clustered particles on the cubic
+    lattice NPM^3."""
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    cell, off, _ = small_case((NPM,) * 3, 4000, seed=51, clustered=True)
+    rng = np.random.default_rng(52)
+    vel = (0.1 * rng.standard_normal((cell.shape[0], 3)) / NPM / DTD).astype(np.float32)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    d = SlabDomain((NPM,) * 3, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=OracleEngine)
+    d.set_particles(cell, off, vel, 1.0 / cell.shape[0], ids=ids)
+    rho, F = d.field(1), d.field(3)
+    for _ in range(3):
+        d.pm_step(rho, F, 0.002, DTD, COUPLING)
+    return d.rank, d.particles_global()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_pm_steps_agree_on_any_number_of_ranks(world):
+    """pm_step (deposit, slab PM force, kick-drift, migration) on `world`
+    gloo ranks against one rank.  The transforms are per plane and per line,
+    so the rank count changes no FFT arithmetic; the deposit's fold at each
+    slab face adds two FP32 values where one rank converts one exact integer
+    sum, so forces, and the particles after three steps, agree to FP32
+    rounding (positions within 1e-6 of the box, velocities within 1e-5 of
+    their maximum), not bit for bit."""
+    from latfield2_b200 import snapshot as S
+    one = _run_pm_steps(False)[1]
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, "_run_pm_steps"))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    got = {k: np.concatenate([r[1][k] for r in res]) for k in ("id", "cell", "off", "vel")}
+    o1, o2 = np.argsort(one["id"]), np.argsort(got["id"])
+    np.testing.assert_array_equal(got["id"][o2], one["id"][o1])
+    res_ = 1.0 / NPM
+    p1 = S.cells_to_positions(one["cell"][o1], one["off"][o1], (NPM,) * 3, res_)
+    p2 = S.cells_to_positions(got["cell"][o2], got["off"][o2], (NPM,) * 3, res_)
+    d = np.abs(p1 - p2)
+    assert np.minimum(d, 1.0 - d).max() < 1e-6
+    v1, v2 = one["vel"][o1], got["vel"][o2]
+    assert np.abs(v1 - v2).max() <= 1e-5 * np.abs(v1).max()
+    assert (got["cell"][o2] != one["cell"][o1]).sum() <= 2  # a face crossing may differ
