@@ -306,7 +306,11 @@ class SlabDomain:
         back = e.complex_buffer((R, nz, nky, nkx))                       # [from rank][z][ky][kx]
         self._all_to_all(B.view(R, nz, nky, nkx), back)
         A = back.permute(1, 0, 2, 3).reshape(nz, n, nkx).contiguous()
-        p = phi if phi is not None else self.field(1)
+        if phi is None:
+            if getattr(self, "_phi", None) is None:
+                self._phi = self.field(1)  # scratch potential, kept for later calls
+            phi = self._phi
+        p = phi
         e.planes_c2r(A, p[0][0, 1:nz + 1])
         self.fill_ghosts(p)
         e.gradient(p, F)
