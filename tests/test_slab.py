@@ -263,3 +263,15 @@ def test_pm_steps_agree_on_any_number_of_ranks(world):
     v1, v2 = one["vel"][o1], got["vel"][o2]
     assert np.abs(v1 - v2).max() <= 1e-5 * np.abs(v1).max()
     assert (got["cell"][o2] != one["cell"][o1]).sum() <= 2  # a face crossing may differ
+
+
+def test_bad_requests_are_refused():
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    d = SlabDomain(N, engine=OracleEngine)  # N is not cubic
+    with pytest.raises(ValueError, match="cubic"):
+        d.pm_force(d.field(1), d.field(3), COUPLING)
+    with pytest.raises(ValueError, match="unknown projection"):
+        d.project("scalar", d.field(1))
+    with pytest.raises(ValueError, match="3 components"):
+        d.project("vector_cic", d.field(6))
