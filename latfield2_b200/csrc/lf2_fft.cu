@@ -1,4 +1,5 @@
-// lf2_fft.cu -- the PM grid operator on one GPU.
+// lf2_fft.cu -- the PM grid operator, on one GPU and as the pieces of its
+// z-slab form.
 //
 //  - PlanFFT<Imag> for a real field on a cubic lattice
 //    (LATfield2_PlanFFT_decl.hpp:720-1050): execute(FFT_FORWARD) and
@@ -23,6 +24,12 @@
 //    the divergence of the incoming force gradient (k_divergence4) followed
 //    by the same Green's-function solve, which is self-adjoint (a
 //    convolution with a real kernel even in k).
+//  - lf2_slab_fft_* / lf2_slab_green / lf2_pm_gradient: the pieces of the
+//    operator when z is split over ranks, after the distributed PlanFFT
+//    (LATfield2_PlanFFT_decl.hpp:83-230) with one split dim: batched 2-D
+//    plane transforms of a rank's planes, strided 1-D line transforms along z
+//    after the caller's transpose, k_green on a k_y slab, and the gradient
+//    on the rank's lattice with ghost planes.
 #include <cuda_runtime.h>
 #include <cufft.h>
 
