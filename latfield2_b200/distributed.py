@@ -151,6 +151,7 @@ class SlabDomain:
         self.res = float(box) / self.n[0]
         self.local_n = (self.n[0], self.n[1], self.nz + 2)
         self.plane = self.n[0] * self.n[1]
+        self.mode = mode
         cls = CudaEngine if engine is None else engine
         self.engine = cls(self.local_n, self.res, mode, device)
         self.up = (self.rank + 1) % self.size
@@ -236,14 +237,34 @@ class SlabDomain:
         self._shift(a[:, self.nz], self.up, buf, self.down)      # plane 0 <- below's plane nz
         a[:, 0] = buf
 
-    def deposit(self, rho):
+    def deposit(self, rho, exact=False):
         """Scalar CIC deposit of the own particles with the upper-plane fold;
-        the ghost planes of rho end at zero."""
-        self.engine.deposit(rho)
+        the ghost planes of rho end at zero.
+
+        The fold adds two FP32 values at every vertex of plane 1.  With
+        exact=True (fixed-point mode, nz >= 2) there is no fold: the rank
+        receives copies of the particles on the top plane of the rank below,
+        deposits them on its plane 0 together with its own particles, and
+        drops them again, so every own vertex converts its one exact integer
+        sum, as on a single domain (the density is then bit-identical to the
+        single-domain deposit whatever the number of ranks)."""
         a = rho[0]
-        buf = self._plane_buf(a)
-        self._shift(a[:, self.nz + 1], self.up, buf, self.down)
-        a[:, 1] += buf
+        if exact:
+            if self.mode != _lib.DEPOSIT_FIXED64 or self.nz < 2:
+                raise ValueError("exact deposits need the fixed-point mode and 2 or more planes "
+                                 "per rank")
+            top = self.engine.extract_outside(1, self.nz - 1)  # the own plane nz
+            self.engine.add(top)
+            ghost = {k: v.clone() for k, v in top.items()}
+            ghost["cell"] = ghost["cell"] - self.nz * self.plane  # -> plane 0 of the rank above
+            self.engine.add(self._shift_parts(ghost, self.up, self.down))
+            self.engine.deposit(rho)
+            self.engine.extract_outside(1, self.nz)  # the copies leave again
+        else:
+            self.engine.deposit(rho)
+            buf = self._plane_buf(a)
+            self._shift(a[:, self.nz + 1], self.up, buf, self.down)
+            a[:, 1] += buf
         a[:, 0] = 0
         a[:, self.nz + 1] = 0
 
@@ -343,11 +364,11 @@ class SlabDomain:
         if rho is not None:
             self.deposit(rho)
 
-    def pm_step(self, rho, F, dtau_kick, dtau_drift, coupling):
+    def pm_step(self, rho, F, dtau_kick, dtau_drift, coupling, exact=False):
         """One self-consistent particle-mesh step over the slabs: deposit
-        rho from the particles, the PM force F from rho (pm_force), then
-        kick + drift + rebin and migration (step)."""
-        self.deposit(rho)
+        rho from the particles (exact: see deposit), the PM force F from rho
+        (pm_force), then kick + drift + rebin and migration (step)."""
+        self.deposit(rho, exact)
         self.pm_force(rho, F, coupling)
         self.step(F, dtau_kick, dtau_drift)
 

@@ -275,3 +275,62 @@ def test_bad_requests_are_refused():
         d.project("scalar", d.field(1))
     with pytest.raises(ValueError, match="3 components"):
         d.project("vector_cic", d.field(6))
+
+
+def _run_exact(dist_initialised):
+    """Two exact pm_steps of clustered particles, then an exact deposit."""
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    cell, off, _ = small_case((NPM,) * 3, 4000, seed=61, clustered=True)
+    rng = np.random.default_rng(62)
+    vel = (0.1 * rng.standard_normal((cell.shape[0], 3)) / NPM / DTD).astype(np.float32)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    d = SlabDomain((NPM,) * 3, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=OracleEngine)
+    d.set_particles(cell, off, vel, 1.0 / cell.shape[0], ids=ids)
+    rho, F = d.field(1), d.field(3)
+    for _ in range(2):
+        d.pm_step(rho, F, 0.002, DTD, COUPLING, exact=True)
+    d.deposit(rho, exact=True)
+    return d.rank, d.z0, d.nz, d.particles_global(), d.own_planes(rho)[0], d.count()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_exact_deposits_make_the_steps_independent_of_the_rank_count(world):
+    """With exact=True the slab density is the single-domain fixed-point
+    deposit bit for bit, so pm_steps on 1, 2 and 4 ranks give the same
+    particles bit for bit; the ghost copies leave the stores again."""
+    one = _run_exact(False)
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, "_run_exact"))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=180) for _ in range(world)], key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    got = {k: np.concatenate([r[3][k] for r in res]) for k in ("id", "cell", "off", "vel")}
+    assert sum(r[5] for r in res) == one[5] == got["id"].shape[0]
+    o1, o2 = np.argsort(one[3]["id"]), np.argsort(got["id"])
+    for k in ("id", "cell", "off", "vel"):
+        np.testing.assert_array_equal(got[k][o2], one[3][k][o1], err_msg=k)
+    # the density: bit-identical to the single-domain fixed-point deposit
+    c, o = one[3]["cell"], one[3]["off"]
+    scale = np.float32(2.0 ** -32 * (1.0 / 4000) / (1.0 / NPM) ** 3)
+    want = O.fixed_to_f32(O.state_deposit_fixed((NPM,) * 3, c, o), scale).reshape((NPM,) * 3)
+    rho = np.zeros_like(want)
+    for _, z0, nz, _, r, _ in res:
+        rho[z0:z0 + nz] = r
+    np.testing.assert_array_equal(rho, want)
+    np.testing.assert_array_equal(one[4], want)
+
+
+def test_exact_deposit_needs_the_fixed_point_mode():
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    d = SlabDomain((NPM, NPM, 1), engine=OracleEngine)  # one plane per rank
+    with pytest.raises(ValueError, match="exact"):
+        d.deposit(d.field(1), exact=True)
