@@ -412,6 +412,61 @@ class SlabDomain:
         self.set_particles(cell, off, vel.astype(np.float32), float(info["mass"]), ids=ids)
         return info
 
+    def _field_global(self, f, dtype):
+        """f's own planes of every rank as one global array (n2, n1, n0,
+        comps) on rank 0 (None elsewhere)."""
+        a = np.ascontiguousarray(self.own_planes(f).astype(dtype))  # (comps, nz, n1, n0)
+        parts = [a]
+        if self.size > 1:
+            parts = [None] * self.size if self.rank == 0 else None
+            self.dist.gather_object(a, parts, dst=0, group=self.group)
+        if self.rank != 0:
+            return None
+        return np.ascontiguousarray(np.concatenate(parts, axis=1).transpose(1, 2, 3, 0))
+
+    def _barrier(self):
+        if self.size > 1:
+            self.dist.barrier(group=self.group)
+
+    def save_field(self, path, f, dataset_name="data", dtype=np.float64):
+        """The field as the dataset of Field::saveHDF5 (latfield2_b200.
+        snapshot.save_field), written by rank 0 from every rank's planes."""
+        g = self._field_global(f, dtype)
+        if g is not None:
+            with open(path, "wb") as fp:
+                np.savez(fp, **{dataset_name: g[..., 0] if g.shape[3] == 1 else g})
+        self._barrier()
+
+    def save_field_binary(self, path, f, real_bytes=8):
+        """The file of Field::write (latfield2_b200.snapshot.write_field_binary)
+        for the whole lattice, written by rank 0."""
+        g = self._field_global(f, np.float64 if real_bytes == 8 else np.float32)
+        if g is not None:
+            with open(path, "wb") as fp:
+                fp.write(g.tobytes())
+        self._barrier()
+
+    def _load_global(self, f, g):
+        comps = int(f[0].shape[0])
+        want = self.n[::-1] + (comps,)
+        g = g.reshape(self.n[2], self.n[1], self.n[0], -1)
+        if tuple(g.shape) != want:
+            raise ValueError(f"the file holds {g.shape}, the field {want}")
+        self.set_own_planes(f, g.transpose(3, 0, 1, 2))
+
+    def load_field(self, path, f, dataset_name="data"):
+        """Every rank reads its own planes of a save_field dataset, then the
+        ghost planes are filled (Field::loadHDF5 and updateHalo)."""
+        with np.load(path, allow_pickle=False) as z:
+            self._load_global(f, z[dataset_name])
+        self.fill_ghosts(f)
+
+    def load_field_binary(self, path, f, real_bytes=8):
+        """Field::read of a save_field_binary file, then the ghost planes."""
+        self._load_global(f, np.fromfile(path, dtype=np.float64 if real_bytes == 8 else
+                                         np.float32))
+        self.fill_ghosts(f)
+
     def particles_global(self):
         """The local particles with global cell indices (numpy dict)."""
         p = self.engine.particles()

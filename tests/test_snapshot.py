@@ -200,3 +200,35 @@ def test_context_snapshot_functions_on_host_arrays(tmp_path):
     np.testing.assert_array_equal(v[order], vel[want].astype(np.float64))
     with pytest.raises(ValueError, match="boxSize"):
         S.load_context(tmp_path / "c.npz", _FakeContext(N, (1.0, 1.0, 1.0)))
+
+
+def _fields(path):
+    """A 3-component field set from a global array on every rank, saved in
+    both layouts; then loaded into fresh fields."""
+    d = _domain()
+    g = np.arange(3 * N[0] * N[1] * N[2], dtype=np.float64).reshape(3, N[2], N[1], N[0]) / 7.0
+    f = d.field(3)
+    d.set_own_planes(f, g.astype(np.float32))
+    d.save_field(path + ".npz", f, dataset_name="vel")
+    d.save_field_binary(path + ".bin", f)
+    a, b = d.field(3), d.field(3)
+    d.load_field(path + ".npz", a, dataset_name="vel")
+    d.load_field_binary(path + ".bin", b)
+    return d.rank, d.own_planes(a), d.own_planes(b), a[0].numpy()[:, 0].copy(), d.z0
+
+
+@pytest.mark.parametrize("world", [1, 2])
+def test_slab_fields_in_the_reference_file_layouts(tmp_path, world):
+    path = str(tmp_path / "f")
+    res = _ranks(world, "_fields", path)
+    g = (np.arange(3 * N[0] * N[1] * N[2], dtype=np.float64).reshape(3, N[2], N[1], N[0])
+         / 7.0).astype(np.float32)
+    with np.load(path + ".npz") as z:
+        np.testing.assert_array_equal(z["vel"], g.transpose(1, 2, 3, 0).astype(np.float64))
+    np.testing.assert_array_equal(np.fromfile(path + ".bin").reshape(N[2], N[1], N[0], 3),
+                                  g.transpose(1, 2, 3, 0))
+    for _, a, b, ghost0, z0 in res:
+        nz = a.shape[1]
+        np.testing.assert_array_equal(a, g[:, z0:z0 + nz])
+        np.testing.assert_array_equal(b, g[:, z0:z0 + nz])
+        np.testing.assert_array_equal(ghost0, g[:, (z0 - 1) % N[2]])  # plane 0 = plane below
