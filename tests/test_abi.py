@@ -94,3 +94,25 @@ def test_next_row_entry_points_reject_null_arguments():
 def test_sources_target_sm100a_only():
     from latfield2_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_the_package_never_imports_the_oracle():
+    """The product (latfield2_b200/) runs on the CUDA library alone: no
+    module imports, loads or calls the oracle, which is test infrastructure."""
+    import ast
+    root = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "latfield2_b200")
+    for path in glob.glob(os.path.join(root, "**", "*.py"), recursive=True):
+        with open(path) as f:
+            tree = ast.parse(f.read(), path)
+        for node in ast.walk(tree):
+            if isinstance(node, ast.Import):
+                names = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom):
+                names = [node.module or ""]
+            else:
+                continue
+            assert not any(n.split(".")[0] == "oracle" for n in names), path
+        with open(path) as f:
+            src = f.read()
+        assert "liblf2oracle" not in src and "lf2_ref_driver" not in src, path
