@@ -127,6 +127,13 @@ class CudaEngine:
     def count(self):
         return self.ctx.count()
 
+    @property
+    def device(self):
+        return self.dev
+
+    def conservation(self):
+        return self.ctx.conservation()
+
     def synchronize(self):
         self.ctx.synchronize()
 
@@ -353,10 +360,32 @@ class SlabDomain:
         for p in (from_below, from_above):
             self.engine.add(p)
 
+    def _all_reduce(self, values, op):
+        """FP64 values reduced over the ranks (op "sum" or "max"); every rank
+        takes part, so that all of them act on the same result."""
+        if self.size == 1:
+            return np.asarray(values, np.float64)
+        t = self.engine.torch
+        x = t.tensor(np.asarray(values, np.float64), device=self.engine.device)
+        red = self.dist.ReduceOp.SUM if op == "sum" else self.dist.ReduceOp.MAX
+        self.dist.all_reduce(x, op=red, group=self.group)
+        return x.cpu().numpy()
+
+    def conservation(self):
+        """FP64 total mass, momentum sum and max |v| over all ranks (the
+        reductions of cout_particle_velocity_stats and updateVel's SUM/MAX
+        outputs, LATfield2_Particles.hpp:543-583, :645-743)."""
+        m, mom, vmax = self.engine.conservation()
+        s = self._all_reduce([m, mom[0], mom[1], mom[2]], "sum")
+        return float(s[0]), s[1:4], float(self._all_reduce([vmax], "max")[0])
+
     def step(self, F, dtau_kick, dtau_drift, rho=None):
-        """fill_ghosts(F), kick + drift + rebin, migrate, and (rho given) deposit."""
+        """fill_ghosts(F), kick + drift + rebin, migrate, and (rho given) deposit.
+        The speed check uses max |v| over all ranks, so that all ranks raise
+        together rather than leaving the others waiting in the migration."""
         self.fill_ghosts(F)
         vmax = self.engine.kick_drift(F, dtau_kick, dtau_drift)
+        vmax = float(self._all_reduce([vmax], "max")[0])
         if vmax * dtau_drift / self.res >= 1.0:
             raise RuntimeError(f"max |v| dtau = {vmax * dtau_drift / self.res:.3f} cells: the "
                                "slab decomposition moves particles by less than one cell per step")

@@ -128,5 +128,16 @@ class OracleEngine:
     def count(self):
         return int(self.cell.shape[0])
 
+    @property
+    def device(self):
+        return self.torch.device("cpu")
+
+    def conservation(self):
+        """FP64 mass, momentum sum and max |v| of the local particles."""
+        v = self.vel.astype(np.float64)
+        npart = v.shape[0]
+        vmax = float(np.sqrt((v * v).sum(axis=1).max())) if npart else 0.0
+        return self.gmass * npart, self.gmass * v.sum(axis=0), vmax
+
     def synchronize(self):
         pass

@@ -334,3 +334,50 @@ def test_exact_deposit_needs_the_fixed_point_mode():
     d = SlabDomain((NPM, NPM, 1), engine=OracleEngine)  # one plane per rank
     with pytest.raises(ValueError, match="exact"):
         d.deposit(d.field(1), exact=True)
+
+
+def _run_fast_on_one_rank(dist_initialised):
+    """Only the upper half of the box holds a particle that moves more than a
+    cell per step; every rank must raise, none may wait in the migration."""
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    cell, off, vel, F, ids = _case()
+    vel = vel * 0.5
+    z = cell // (N[0] * N[1])
+    fast = np.flatnonzero(z >= N[2] // 2)[0]
+    vel[fast] = np.array([0, 0, 3.0 / N[0] / DTD], np.float32)
+    d = SlabDomain(N, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=OracleEngine)
+    d.set_particles(cell, off, vel, 1.0 / cell.shape[0], ids=ids)
+    m, mom, vmax = d.conservation()
+    Ff = d.field(3)
+    d.set_own_planes(Ff, F)
+    try:
+        d.step(Ff, DTK, DTD)
+        outcome = "stepped"
+    except RuntimeError as e:
+        outcome = "raised" if "less than one cell" in str(e) else str(e)
+    return d.rank, outcome, m, mom, vmax
+
+
+def test_a_too_fast_particle_on_one_rank_stops_every_rank():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q, "_run_fast_on_one_rank"))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == ["raised", "raised"]
+    # the conservation sums are global and the same on every rank
+    cell, off, vel, F, ids = _case()
+    v = (vel * 0.5).astype(np.float64)
+    v[np.flatnonzero(cell // (N[0] * N[1]) >= N[2] // 2)[0]] = [0, 0, np.float32(3.0 / N[0] / DTD)]
+    for _, _, m, mom, vmax in res:
+        assert m == pytest.approx(1.0, rel=1e-12)
+        np.testing.assert_allclose(mom, v.sum(axis=0) / cell.shape[0], rtol=1e-10, atol=1e-15)
+        assert vmax == pytest.approx(float(np.sqrt((v * v).sum(axis=1).max())), rel=1e-12)
