@@ -349,7 +349,8 @@ class SlabDomain:
         z = out["cell"] // self.plane
         below = z == 0
         above = z == self.nz + 1
-        if bool((~(below | above)).any()):
+        lost = float(bool((~(below | above)).any()))
+        if self._all_reduce([lost], "max")[0] > 0:  # every rank raises, none waits
             raise RuntimeError("a particle left the slab by more than one plane")
         to_down = {k: v[below] for k, v in out.items()}
         to_up = {k: v[above] for k, v in out.items()}
