@@ -63,3 +63,41 @@ def internal_to_reference(F, halo):
     if halo:
         a = np.pad(a, ((halo, halo), (halo, halo), (halo, halo), (0, 0)), mode="wrap")
     return np.ascontiguousarray(a)
+
+
+def slab_potential_emulated(engine_cls, rho, ranks, coupling, device=None):
+    """The potential of the slab PM operator for `ranks` z slabs emulated in
+    one process, the ranks one after the other (no collectives, nothing that
+    waits): per rank an engine of the rank's local lattice, its plane
+    transforms, the all-to-all transposes done here by slicing, the line
+    transforms and the Green's function on each rank's k_y slab (ky0 = r nky).
+    rho: torch tensor (n, n, n) on the engines' device.  Returns phi (n, n, n)."""
+    import torch
+    from latfield2_b200 import _lib
+    n = int(rho.shape[0])
+    nz = nky = n // ranks
+    nkx = n // 2 + 1
+    res = 1.0 / n
+    kw = {} if device is None else {"device": device}
+    eng = [engine_cls((n, n, nz + 2), res, _lib.DEPOSIT_FIXED64, **kw) for _ in range(ranks)]
+    for e in eng:
+        e.fft_prepare(n, nz, nky)
+    A = []
+    for r, e in enumerate(eng):
+        a = e.complex_buffer((nz, n, nkx))
+        e.planes_r2c(rho[r * nz:(r + 1) * nz].contiguous(), a)
+        A.append(a)
+    B = []
+    for r, e in enumerate(eng):
+        b = torch.cat([A[s][:, r * nky:(r + 1) * nky, :] for s in range(ranks)], 0).contiguous()
+        e.lines(b, _lib.FFT_FORWARD)
+        e.green(b, r * nky, coupling)
+        e.lines(b, _lib.FFT_BACKWARD)
+        B.append(b)
+    phi = []
+    for s, e in enumerate(eng):
+        a = torch.cat([B[r][s * nz:(s + 1) * nz] for r in range(ranks)], 1).contiguous()
+        p = torch.empty((nz, n, n), dtype=torch.float32, device=rho.device)
+        e.planes_c2r(a, p)
+        phi.append(p)
+    return torch.cat(phi, 0)

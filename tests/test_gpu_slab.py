@@ -192,3 +192,23 @@ def test_one_rank_slab_pm_force_equals_the_single_gpu_operator(n):
         assert np.abs(got[c] - want[c]).max() <= 1e-5 * scale, c
         assert np.abs(got[c] - F64[c]).max() <= 1e-5 * scale, c
     assert np.abs(d.own_planes(phi)[0] - phi64).max() <= 1e-5 * np.abs(phi64).max()
+
+
+@pytest.mark.parametrize("ranks", [2, 4])
+def test_slab_pieces_with_several_ky_slabs_on_one_gpu(ranks):
+    """lf2_slab_fft_* and lf2_slab_green for 2 and 4 z slabs emulated in one
+    process on one GPU (the ranks one after the other, transposes by slicing;
+    nothing waits on another launch): k_y slabs with ky0 > 0, against the FP64
+    operator (1e-5 of the maximum).  The same emulation runs on the CPU in
+    tests/test_slab.py with the numpy engine."""
+    import torch
+    from latfield2_b200.distributed import CudaEngine
+    from oracle import fft_oracle as FO
+    from tests.helpers import slab_potential_emulated
+    n, coupling = 32, 4 * np.pi
+    rng = np.random.default_rng(70 + ranks)
+    rho = (1.0 + rng.standard_normal((n, n, n))).astype(np.float32)
+    phi = slab_potential_emulated(CudaEngine, torch.from_numpy(rho).cuda(), ranks, coupling,
+                                  device=0).cpu().numpy()
+    want = FO.pm_force(rho, 1.0 / n, coupling)[0]
+    assert np.abs(phi - want).max() <= 1e-5 * np.abs(want).max()

@@ -381,3 +381,17 @@ def test_a_too_fast_particle_on_one_rank_stops_every_rank():
         assert m == pytest.approx(1.0, rel=1e-12)
         np.testing.assert_allclose(mom, v.sum(axis=0) / cell.shape[0], rtol=1e-10, atol=1e-15)
         assert vmax == pytest.approx(float(np.sqrt((v * v).sum(axis=1).max())), rel=1e-12)
+
+
+@pytest.mark.parametrize("ranks", [2, 4])
+def test_slab_potential_emulated_in_one_process(ranks):
+    """The emulation that tests/test_gpu_slab.py runs on one GPU (k_y slabs
+    with ky0 > 0), here with the numpy engine, against the FP64 operator."""
+    import torch
+    from oracle import fft_oracle as FO
+    from tests.helpers import slab_potential_emulated
+    from tests.slab_oracle_engine import OracleEngine
+    rho = _pm_field()
+    phi = slab_potential_emulated(OracleEngine, torch.from_numpy(rho), ranks, COUPLING).numpy()
+    want = FO.pm_force(rho, 1.0 / NPM, COUPLING)[0]
+    assert np.abs(phi - want).max() <= 1e-5 * np.abs(want).max()
