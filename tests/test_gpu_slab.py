@@ -212,3 +212,25 @@ def test_slab_pieces_with_several_ky_slabs_on_one_gpu(ranks):
                                   device=0).cpu().numpy()
     want = FO.pm_force(rho, 1.0 / n, coupling)[0]
     assert np.abs(phi - want).max() <= 1e-5 * np.abs(want).max()
+
+
+def test_one_rank_exact_slab_deposit_is_the_single_gpu_deposit():
+    """SlabDomain.deposit(exact=True) with one rank (ghost copies of its own
+    top plane on plane 0, no FP32 fold) equals lf2_deposit_scalar on the
+    whole lattice bit for bit, and leaves the particle count unchanged."""
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    n = (32, 32, 32)
+    cell, off, vel = small_case(n, 60000, seed=17, clustered=True)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    gm = 1.0 / cell.shape[0]
+    ref = _ctx(n)
+    ref.set_particles(cell, off, vel, global_mass=gm, ids=ids)
+    want = ref.field(1)
+    ref.deposit_scalar(want)
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64)
+    d.set_particles(cell, off, vel, gm, ids=ids)
+    rho = d.field(1)
+    d.deposit(rho, exact=True)
+    np.testing.assert_array_equal(d.own_planes(rho)[0], want.export_internal()[0])
+    assert d.count() == cell.shape[0]
