@@ -14,7 +14,6 @@ time, as torch tensors on `device` (CPU tensors work for small cases).
   grf_gradient a Gaussian random scalar field with P(k) ~ k^-2 and its
                central-difference gradient at the vertices (3 components)
 """
-import math
 
 import torch
 
