@@ -6,7 +6,6 @@ import glob
 import os
 import re
 
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
