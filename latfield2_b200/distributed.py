@@ -41,8 +41,17 @@ Green's function and the inverse 1-D transforms run there, the transpose
 goes back, the inverse 2-D transforms give phi on the own planes, and the
 central-difference gradient reads phi's ghost planes after fill_ghosts.
 
+`deposit(rho, exact=True)` replaces the FP32 fold by ghost-particle copies
+(the top plane of the rank below), so that the fixed-point density is the
+single-domain one bit for bit.  `pm_step` chains deposit, pm_force and step.
+Checks that can fail on one rank (the speed limit, a lost particle) are
+reduced over all ranks first, so that every rank raises together.  Particle
+and field files in the reference's layouts are gathered on rank 0
+(save_particles, save_field, save_field_binary) and read back by every rank.
+
 Exchanges are point-to-point messages between neighbours (NCCL between GPUs,
-gloo between CPU processes).  A single rank exchanges with itself, which
+gloo between CPU processes), all-to-all for the FFT's transposes and
+all-reduce for the checks and conservation sums.  A single rank exchanges with itself, which
 gives the periodic single-domain result.  The local work is done by an
 engine: CudaEngine (the library's Context) by default; any object with the
 same methods can stand in (the tests run the exchange logic on CPU processes
