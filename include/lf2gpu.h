@@ -383,13 +383,20 @@ lf2_status lf2_pm_force4_adjoint(lf2_ctx* ctx, const float* g_F4,
  * scratch (the per-brick shell store) is a fixed 16 MiB device array inside
  * the library, present on every GPU that loads it until the process exits,
  * so lattices with more than LF2_NOALLOC_MAX_BRICKS bricks are rejected with
- * LF2_ERR_UNSUPPORTED.  The first call on a device looks the array's device
- * address up (once per device, with that device current); make that first
- * call before any stream capture.  Calls share the array: calls that overlap
- * on the GPU race and must be serialised.  The work is queued on `stream`
- * (NULL: default stream); with flags != NULL the call waits for it and
- * returns the device error bits (LF2_FLAG_BAD_CELL for a particle outside
- * its brick or with an offset outside [0,1)), with LF2_ERR_STATE if any. */
+ * LF2_ERR_UNSUPPORTED.  Every call looks the array's device address up in
+ * the current device's context (cudaGetSymbolAddress); make the first call
+ * on a device before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race and must be serialised.  The work is queued on
+ * `stream` (NULL: default stream).  brick_start is checked on the device:
+ * it must start at 0, never decrease and end at np or below; a brick whose
+ * range breaks that is clamped to [0, np] and reported.  With flags != NULL
+ * the call waits for the work and returns the device error bits
+ * (LF2_FLAG_BAD_CELL for a particle outside its brick, an offset outside
+ * [0,1) or a bad brick range), with LF2_ERR_STATE if any.  With flags ==
+ * NULL nothing is waited for and such errors are not reported: the call
+ * returns LF2_OK.  A runtime error left pending by an earlier, unrelated
+ * CUDA call is picked up by the launch checks and fails the call with
+ * LF2_ERR_CUDA. */
 #define LF2_NOALLOC_MAX_BRICKS 1363
 lf2_status lf2_deposit_scalar_noalloc(const int n[3], const double box[3],
                                       int deposit_mode, double particle_mass,

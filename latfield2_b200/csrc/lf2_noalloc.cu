@@ -14,8 +14,10 @@
 // exits.  Host code cannot use the array's name as a device address: the
 // name is a host-side stand-in, and a kernel given it would fault or, where
 // the GPU can reach host memory, silently use the wrong memory.  The device
-// address is therefore fetched once per device with cudaGetSymbolAddress,
-// with that device current, and passed to the kernels.
+// address is therefore looked up with cudaGetSymbolAddress, with the caller's
+// device current, on every call (the lookup is cheap next to two launches,
+// and a cached address would go stale if the device's context were reset and
+// the module reloaded), and passed to the kernels.
 //
 // All calls share the array and it keeps the contents of the last call.  The
 // deposit writes every shell slot it later reads and clears the error word
@@ -25,7 +27,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 #include "lf2_common.cuh"
 #include "lf2gpu.h"
@@ -46,29 +47,16 @@ struct NoallocSymbols {
   unsigned int* flags = nullptr;
 };
 
-constexpr int MAX_DEVICES = 64;
-NoallocSymbols g_symbols[MAX_DEVICES];
-std::mutex g_symbols_mutex;
-
-// Device addresses of the two arrays on the current device, looked up on the
-// first call made with that device current.
+// Device addresses of the two arrays in the current device's context.
 cudaError_t noalloc_symbols(NoallocSymbols* out)
 {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_shell);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_symbols_mutex);
-  NoallocSymbols& s = g_symbols[dev];
-  if (!s.shell) {
-    void* p = nullptr;
-    if ((e = cudaGetSymbolAddress(&p, g_noalloc_shell)) != cudaSuccess) return e;
-    void* q = nullptr;
-    if ((e = cudaGetSymbolAddress(&q, g_noalloc_flags)) != cudaSuccess) return e;
-    s.shell = static_cast<unsigned long long*>(p);
-    s.flags = static_cast<unsigned int*>(q);
-  }
-  *out = s;
+  void* q = nullptr;
+  if ((e = cudaGetSymbolAddress(&q, g_noalloc_flags)) != cudaSuccess) return e;
+  out->shell = static_cast<unsigned long long*>(p);
+  out->flags = static_cast<unsigned int*>(q);
   return cudaSuccess;
 }
 
@@ -79,9 +67,9 @@ struct NaParams {
 
 template <bool FIXED>
 __global__ void __launch_bounds__(NA_THREADS) k_deposit_noalloc(
-    Geom g, NaParams pp, const int32_t* __restrict__ cell, const float* __restrict__ off3,
-    const int64_t* __restrict__ brick_start, float* __restrict__ out,
-    unsigned long long* __restrict__ shell, unsigned int* flags)
+    Geom g, NaParams pp, int64_t np, const int32_t* __restrict__ cell,
+    const float* __restrict__ off3, const int64_t* __restrict__ brick_start,
+    float* __restrict__ out, unsigned long long* __restrict__ shell, unsigned int* flags)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   const int64_t b = blockIdx.x;
@@ -90,8 +78,17 @@ __global__ void __launch_bounds__(NA_THREADS) k_deposit_noalloc(
   const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
             ez = brick_extent(g.n[2], bz);
   const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
-  const int64_t base = brick_start[b];
-  const int64_t cnt = brick_start[b + 1] - base;
+  // The caller's brick offsets are checked, never trusted: they must start
+  // at 0, never decrease and never pass np.  A brick whose range breaks that
+  // is clamped to [0, np] (so nothing outside the particle arrays is read)
+  // and reported.
+  int64_t base = brick_start[b], end = brick_start[b + 1];
+  if ((b == 0 && base != 0) || base < 0 || end < base || end > np) {
+    if (threadIdx.x == 0) atomicOr(flags, ERR_BAD_CELL);
+    base = base < 0 ? 0 : (base > np ? np : base);
+    end = end < base ? base : (end > np ? np : end);
+  }
+  const int64_t cnt = end - base;
   const bool split = FIXED && cnt <= NA_SPLIT_MAX;
 
   uint32_t* lo = reinterpret_cast<uint32_t*>(smem);
@@ -281,16 +278,21 @@ extern "C" lf2_status lf2_deposit_scalar_noalloc(const int n[3], const double bo
   const size_t smem = (size_t)TILE3 * (fixed ? 8 : 4);
   const unsigned grid = (unsigned)g.nbricks;
 
+  // Each launch is checked right after it.  An error left pending by an
+  // earlier, unrelated runtime call is reported by the first check too, so
+  // such an error fails this call (and is cleared by it).
   if (cudaMemsetAsync(sym.flags, 0, sizeof(unsigned int), st) != cudaSuccess) return LF2_ERR_CUDA;
-  if (fixed) {
-    k_deposit_noalloc<true><<<grid, NA_THREADS, smem, st>>>(g, pp, cell, off3, brick_start, rho,
-                                                            sym.shell, sym.flags);
+  if (fixed)
+    k_deposit_noalloc<true><<<grid, NA_THREADS, smem, st>>>(g, pp, np, cell, off3, brick_start,
+                                                            rho, sym.shell, sym.flags);
+  else
+    k_deposit_noalloc<false><<<grid, NA_THREADS, smem, st>>>(g, pp, np, cell, off3, brick_start,
+                                                             rho, sym.shell, sym.flags);
+  if (cudaGetLastError() != cudaSuccess) return LF2_ERR_CUDA;
+  if (fixed)
     k_fixup_noalloc<true><<<grid, 256, 0, st>>>(g, sym.shell, pp.fixed_scale, rho, sym.flags);
-  } else {
-    k_deposit_noalloc<false><<<grid, NA_THREADS, smem, st>>>(g, pp, cell, off3, brick_start, rho,
-                                                             sym.shell, sym.flags);
+  else
     k_fixup_noalloc<false><<<grid, 256, 0, st>>>(g, sym.shell, pp.fixed_scale, rho, sym.flags);
-  }
   if (cudaGetLastError() != cudaSuccess) return LF2_ERR_CUDA;
   if (flags) {
     unsigned int f = 0;

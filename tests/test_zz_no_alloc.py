@@ -109,3 +109,69 @@ def test_noalloc_reports_particles_outside_their_brick(cuda):
     bc, bo, start = _bricked(n, cell, off)
     st, flags = _noalloc(n, 1, 1.0 / 2000, cell_t, off_t, torch.from_numpy(start).cuda(), rho_t)
     assert st == _lib.LF2_OK and flags == 0
+
+
+def test_noalloc_clamps_and_reports_a_brick_range_past_the_particles(cuda):
+    """A last brick offset beyond np is reported and never read past: the
+    particle arrays are backed by longer buffers, so the test itself stays in
+    bounds whatever the kernel does."""
+    import torch
+    from latfield2_b200 import _lib
+    n = (32, 32, 32)
+    cell, off, _ = small_case(n, 2000, seed=9)
+    bc, bo, start = _bricked(n, cell, off)
+    npart = bc.size
+    pad = 4096
+    cell_t = torch.zeros(npart + pad, dtype=torch.int32, device="cuda")
+    off_t = torch.zeros((npart + pad, 3), dtype=torch.float32, device="cuda")
+    cell_t[:npart] = torch.from_numpy(bc).cuda()
+    off_t[:npart] = torch.from_numpy(np.ascontiguousarray(bo)).cuda()
+    bad = start.copy()
+    bad[-1] = npart + pad  # the last brick claims slots past np
+    rho_t = torch.zeros(32 ** 3, dtype=torch.float32, device="cuda")
+    from latfield2_b200 import _lib as L
+    lib = L.load()
+    na = (ctypes.c_int * 3)(*n)
+    box = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    flags = ctypes.c_uint32(0)
+    bad_t = torch.from_numpy(bad).cuda()
+    st = lib.lf2_deposit_scalar_noalloc(
+        na, box, 1, 1.0 / npart, npart, ctypes.c_void_p(cell_t.data_ptr()),
+        ctypes.c_void_p(off_t.data_ptr()), ctypes.c_void_p(bad_t.data_ptr()),
+        ctypes.c_void_p(rho_t.data_ptr()), None, ctypes.byref(flags))
+    assert st == _lib.LF2_ERR_STATE and flags.value & _lib.FLAG_BAD_CELL
+    # offsets that decrease are reported the same way
+    bad = start.copy()
+    bad[3] = bad[2] - 1 if bad[2] > 0 else -1
+    bad_t = torch.from_numpy(bad).cuda()
+    st = lib.lf2_deposit_scalar_noalloc(
+        na, box, 1, 1.0 / npart, npart, ctypes.c_void_p(cell_t.data_ptr()),
+        ctypes.c_void_p(off_t.data_ptr()), ctypes.c_void_p(bad_t.data_ptr()),
+        ctypes.c_void_p(rho_t.data_ptr()), None, ctypes.byref(flags))
+    assert st == _lib.LF2_ERR_STATE and flags.value & _lib.FLAG_BAD_CELL
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_noalloc_without_flags_runs_asynchronously(cuda, mode):
+    """flags == NULL: the call only queues the work; after a synchronize the
+    result equals the context deposit's."""
+    import torch
+    from latfield2_b200 import _lib
+    n = (48, 48, 48)
+    cell, off, _ = small_case(n, 20000, seed=31, clustered=True)
+    mass = 1.0 / 20000
+    ref = _reference(n, mode, mass, cell, off)
+    bc, bo, start = _bricked(n, cell, off)
+    cell_t = torch.from_numpy(bc).cuda()
+    off_t = torch.from_numpy(np.ascontiguousarray(bo)).cuda()
+    start_t = torch.from_numpy(start).cuda()
+    for call in range(2):
+        rho_t = torch.full((n[2], n[1], n[0]), float("nan"), dtype=torch.float32, device="cuda")
+        st, _ = _noalloc(n, mode, mass, cell_t, off_t, start_t, rho_t, want_flags=False)
+        assert st == _lib.LF2_OK
+        torch.cuda.synchronize()
+        got = rho_t.cpu().numpy()
+        if mode == 1:
+            np.testing.assert_array_equal(got, ref)
+        else:
+            assert normalized_error(got, ref) < 1e-5, call
