@@ -246,13 +246,86 @@ def _ref_grid(cores):
     return best
 
 
-def _ref_run(inp, grid, steps, timeout):
-    """One run of the reference driver's timing mode; its ranks form their own
-    process group, stopped as a whole on a timeout."""
+def _write_reference_input(path, name, grid, ops, dtau):
+    """The workload's particles and force field for the reference driver,
+    generated on the host from the bench's seeds (same generators, shapes and
+    statistics as the GPU arm; torch's CPU and CUDA generators draw different
+    numbers) and written in chunks: header, np x {id, pos[3], vel[3]}
+    (double), F[z][y][x][c] (double)."""
+    import struct
+    import numpy as np
+    import torch
+    import latfield2_b200.workloads as W
+    w = WORKLOADS[name]
+    nn = w["n"]
+    n = (nn,) * 3
+    npart = w["npart"]
+    if w["dist"] == "lognormal":
+        cell, off = W.lognormal(n, npart, seed=3, device="cpu")
+    elif w["dist"] == "clumps":
+        cell, off = W.clumps(n, npart, 64, 0.01, seed=3, device="cpu")
+    elif w["dist"] == "halos":
+        cell, off = W.halos(n, npart, 1000, 0.002, seed=3, device="cpu")
+    else:
+        cell, off = W.uniform(n, npart, seed=3, device="cpu")
+    vel = W.velocities(npart, 0.01, seed=4, device="cpu")
+    F = W.grf_gradient(n, seed=2, device="cpu", amplitude=0.01)
+    tmp = path + ".part"
+    with open(tmp, "wb") as f:
+        f.write(b"LF2G")
+        f.write(struct.pack("<iiiii", 1, nn, 1, grid[0], grid[1]))
+        f.write(struct.pack("<ddi", 1.0, 1.0 / npart, ops))
+        f.write(struct.pack("<ddq", dtau, dtau, npart))
+        ch = 1 << 23
+        rec = torch.empty((ch, 7), dtype=torch.float64)  # id (int64 bits), pos[3], vel[3]
+        for i0 in range(0, npart, ch):
+            i1 = min(npart, i0 + ch)
+            r = rec[:i1 - i0]
+            c = cell[i0:i1].to(torch.int64)
+            xyz = torch.stack([c % nn, (c // nn) % nn, c // (nn * nn)], 1).to(torch.float64)
+            r[:, 1:4] = (xyz + off[i0:i1].to(torch.float64)) / nn
+            r[:, 4:7] = vel[i0:i1].to(torch.float64)
+            r.view(torch.int64)[:, 0] = torch.arange(i0, i1, dtype=torch.int64)
+            f.write(r.numpy().tobytes())
+        Fr = F.reshape(3, nn, nn, nn)
+        for z in range(nn):
+            f.write(Fr[:, z].permute(1, 2, 0).to(torch.float64).contiguous().numpy().tobytes())
+    os.replace(tmp, path)
+    del cell, off, vel, F
+    torch.set_num_threads(torch.get_num_threads())
+
+
+def cpu_reference_steps(name, cores, steps, warmup, timeout=1800):
+    """The reference's own particle path (its headers compiled by
+    oracle/build_ref.sh, double) on the full workload `name`: the driver's
+    timing mode runs `warmup` untimed and then `steps` timed steps of
+    scalarProjectionCIC_project + _comm, updateVel with the CIC kick and
+    moveParticles, each step between two barriers, on the largest
+    power-of-two process grid (both dims >= 2, moveParticles deadlocks on a
+    grid dim of 1) within `cores` forked ranks.  The input file is kept in the
+    temp directory for the next run on the same host.  Returns the driver's
+    JSON record plus the grid and set-up time, or None."""
+    import shutil
+    grid = _ref_grid(cores)
+    if grid is None or not os.access(REF_DRIVER, os.X_OK):
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden as G
+    w = WORKLOADS[name]
+    npart, nn = w["npart"], w["n"]
+    size = 68 + 56 * npart + 24 * nn ** 3
+    tdir = os.environ.get("LF2_REF_INPUT_DIR", tempfile.gettempdir())
+    path = os.path.join(tdir, f"lf2_ref_input_{name}_{grid[0]}x{grid[1]}.bin")
+    t0 = time.perf_counter()
+    if not (os.path.exists(path) and os.path.getsize(path) == size):
+        if shutil.disk_usage(tdir).free < size * 1.2:
+            return None
+        _write_reference_input(path, name, grid, G.OP_KICK | G.OP_MOVE, 0.1 * 64.0 / nn)
+    setup = time.perf_counter() - t0
     import signal
-    import subprocess
-    env = dict(os.environ, LF2_MINIMPI_NP=str(grid[0] * grid[1]), LF2_REF_STEPS=str(steps))
-    p = subprocess.Popen([REF_DRIVER, inp, inp + ".out"], env=env, stdin=subprocess.DEVNULL,
+    env = dict(os.environ, LF2_MINIMPI_NP=str(grid[0] * grid[1]), LF2_REF_STEPS=str(steps),
+               LF2_REF_WARMUP=str(warmup))
+    p = subprocess.Popen([REF_DRIVER, path, path + ".out"], env=env, stdin=subprocess.DEVNULL,
                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, start_new_session=True)
     try:
         out, _ = p.communicate(timeout=timeout)
@@ -262,44 +335,29 @@ def _ref_run(inp, grid, steps, timeout):
         return None
     if p.returncode != 0:
         return None
+    rec = None
     for line in out.decode().splitlines():
         if line.startswith("{"):
-            return json.loads(line)
-    return None
-
-
-def cpu_baseline_reference(seconds, cores, n=64, npart=64 ** 3):
-    """The reference's own particle path (its headers compiled by
-    oracle/build_ref.sh, double) on a bounded sample: a 64^3 lattice with
-    262,144 uniform particles, K steps of scalarProjectionCIC_project + _comm,
-    updateVel with the CIC kick and moveParticles, on a g0 x g1 process grid
-    of forked ranks.  K is chosen for about `seconds` of work.  Returns
-    (updates/s, steps, ranks) or None when the driver or 4 cores are not
-    there."""
-    import tempfile
-    import numpy as np
-    grid = _ref_grid(cores)
-    if grid is None or not os.access(REF_DRIVER, os.X_OK):
+            rec = json.loads(line)
+    if rec is None:
         return None
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    import make_golden as G
-    rng = np.random.default_rng(1)
-    pos = rng.random((npart, 3))
-    vel = 0.01 * rng.standard_normal((npart, 3))
-    F = 0.01 * rng.standard_normal((n, n, n, 3))
-    ids = np.arange(npart, dtype=np.int64)
-    with tempfile.TemporaryDirectory() as td:
-        inp = os.path.join(td, "in.bin")
-        G.write_input(inp, n, 1, grid, 1.0 / npart, G.OP_SCALAR | G.OP_KICK | G.OP_MOVE, 0.1, 0.1,
-                      ids, pos, vel, F)
-        probe = _ref_run(inp, grid, 5, 300)
-        if probe is None:
-            return None
-        steps = max(5, min(5000, int(5 * seconds / max(probe["seconds"], 1e-6))))
-        r = _ref_run(inp, grid, steps, 20 * seconds + 120)
-        if r is None:
-            return None
-    return npart * r["steps"] / r["seconds"], r["steps"], r["ranks"]
+    rec.update(grid=grid, setup_s=setup, wall_s=time.perf_counter() - t0)
+    return rec
+
+
+def cpu_reference_summary(name, rec):
+    w = WORKLOADS[name]
+    per = rec["step_seconds"]
+    return {
+        "value": w["npart"] * rec["steps"] / rec["seconds"], "unit": UNIT,
+        "cores": rec["ranks"], "kind": "reference",
+        "sample": (f"the {name} workload itself ({w['n']}^3 lattice, {w['npart']:,} {w['dist']} "
+                   f"particles): {rec['warmup']} untimed + {rec['steps']} timed steps of "
+                   "scalarProjectionCIC_project + _comm, updateVel with the CIC kick, "
+                   f"moveParticles; the reference's own headers (double) on {rec['ranks']} forked "
+                   f"ranks ({rec['grid'][0]}x{rec['grid'][1]} process grid), one per host core"),
+        "ms_per_step_median": 1e3 * statistics.median(per), "ms_per_step_min": 1e3 * min(per),
+    }
 
 
 def adjoint_ratio(device, steps=8, reps=3, operator="stencil"):
@@ -350,40 +408,53 @@ def adjoint_ratio(device, steps=8, reps=3, operator="stencil"):
             "forward_ms": fwd, "forward_adjoint_ms": both, "ratio": both / fwd}
 
 
+def workload_config(name):
+    """The `config` both arms print: what the workload is, nothing about how an
+    arm runs it (the deposit mode and the parallelism are separate keys)."""
+    w = WORKLOADS[name]
+    nsites = w["n"] ** 3
+    return {"workload": name, "lattice": w["n"], "particles": w["npart"], "distribution": w["dist"],
+            "step": "gather-kick + drift + rebin + scalar CIC deposit",
+            "l2": f"inputs larger than L2 ({alg_bytes_step(w['npart'], nsites) / 1e9:.1f} GB per step)"}
+
+
 def reference_arm(args, rank):
-    """The reference's CPU particle path on the host cores (rank 0 only): its
-    own code compiled from its headers when oracle/_ref is there, else the C
-    restatement of it (oracle/, one process per core)."""
+    """The reference's CPU particle path on the host cores (rank 0 only), on
+    the same workload and with the same steps as the GPU arm: its own code
+    compiled from its headers (oracle/_ref).  Without that build, the C
+    restatement of it (oracle/) on a bounded sample."""
     if rank != 0:
         return
     t0 = time.perf_counter()
     cores = os.cpu_count() or 1
-    ref = cpu_baseline_reference(args.cpu_seconds, cores)
-    if ref is not None:
-        ups, steps, used = ref
-        kind = "reference"
-        sample = (f"{used} ranks ({_ref_grid(cores)[0]}x{_ref_grid(cores)[1]} process grid, forked "
-                  f"MPI stand-in) x 64^3 lattice, 262,144 uniform particles, {steps} steps of "
-                  "scalarProjectionCIC_project+_comm, updateVel CIC kick, moveParticles "
-                  "(the reference's own headers, double)")
+    rec = cpu_reference_steps(args.workload, cores, args.steps, args.warmup)
+    if rec is not None:
+        cpu = cpu_reference_summary(args.workload, rec)
+        ups = cpu["value"]
+        ms_step = 1e3 * rec["seconds"] / rec["steps"]
+        extra = {"ms_per_step_median": cpu["ms_per_step_median"],
+                 "ms_per_step_min": cpu["ms_per_step_min"], "setup_s": rec["setup_s"],
+                 "parallelism": f"{rec['ranks']} MPI ranks ({rec['grid'][0]}x{rec['grid'][1]}), "
+                                "one per host core"}
     else:
-        used = cores
         ups, steps = cpu_baseline_port(args.cpu_seconds, procs=cores)
-        kind = "port"
-        sample = (f"{cores} processes x 64^3 lattice, 262,144 uniform particles, {steps} steps of "
-                  "deposit+comm, updateVel CIC kick, move (CPU restatement of the reference, double)")
-    wall = time.perf_counter() - t0
-    w = WORKLOADS[args.workload]
+        cpu = {"value": ups, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{cores} processes x 64^3 lattice, 262,144 uniform particles, {steps} "
+                         "steps of deposit+comm, updateVel CIC kick, move (CPU restatement of the "
+                         "reference, double): a bounded sample, not the workload itself"}
+        ms_step = 1e3 * 262144 / (ups / cores)
+        extra = {"parallelism": f"{cores} processes"}
     line = {
         "impl": "reference", "metric": METRIC, "value": ups, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "ms_per_step": 1e3 * w["npart"] / ups, "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": args.workload, "lattice": w["n"],
-                                        "particles": w["npart"]},
-        "cpu_baseline": {"value": ups, "unit": UNIT, "cores": used, "kind": kind, "sample": sample},
+        "ms_per_step": ms_step, "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": workload_config(args.workload),
+        "deposit_mode": "double accumulation (the reference's default build)",
+        "cpu_baseline": cpu,
         "e2e": {"value": ups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "wall_s": wall,
+        "wall_s": time.perf_counter() - t0,
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 
@@ -463,17 +534,22 @@ def e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, steps, pg, device, ba
                     "overlap step k"}
 
 
-def full_cic_projections(ctx, npart, nsites, peak, reps=5):
-    """vectorProjectionCIC and VecVecProjectionCIC of the bench's particles
-    (after the timed steps): mean over `reps` deposits after one warm-up call,
-    tile pass and boundary fix-up timed by the library's phase events.
-    Algorithmic bytes: each particle's key, offsets and velocities read once
-    (28 B), the field written once (4 B per component and site); the inputs
-    are larger than L2."""
+PROJECTIONS = (("scalar", "deposit_scalar", 1, 16), ("vector_cicngp", "deposit_vector", 3, 28),
+               ("symtensor_cicngp", "deposit_symtensor", 6, 28),
+               ("vector_cic", "deposit_vector_cic", 3, 28), ("vecvec_cic", "deposit_vecvec_cic", 6, 28))
+
+
+def projection_times(ctx, npart, nsites, peak, reps=5):
+    """Every projection of the bench's particles in the context's deposit
+    mode (after the timed steps): mean over `reps` deposits after one warm-up
+    call; tile pass(es) and fix-up timed by the library's phase events.
+    Algorithmic bytes: each particle's key and offsets (16 B), plus its
+    velocities for momentum and stress (28 B), read once; the field written
+    once (4 B per component and site).  The inputs are larger than L2."""
     out = {}
-    for name, comps in (("vector_cic", 3), ("vecvec_cic", 6)):
+    for name, meth, comps, pb in PROJECTIONS:
         f = ctx.field(comps)
-        dep = getattr(ctx, "deposit_" + name)
+        dep = getattr(ctx, meth)
         dep(f)
         ctx.synchronize()
         ctx.profile_read()
@@ -486,12 +562,72 @@ def full_cic_projections(ctx, npart, nsites, peak, reps=5):
         tile = ph["deposit_tile"][0] / reps
         fix = ph["deposit_fixup"][0] / reps
         ms = tile + fix
-        ab = npart * 28 + nsites * 4 * comps
+        ab = npart * pb + nsites * 4 * comps
         out[name] = {"ms": ms, "tile_ms": tile, "fixup_ms": fix,
                      "particle_deposits_per_s": npart / (ms / 1e3), "alg_bytes": ab,
                      "achieved_gbs": ab / (ms / 1e3) / 1e9,
                      "frac_of_hbm": ab / (ms / 1e3) / 1e9 / peak}
         del f
+    return out
+
+
+def fp64_density(cell, off, n, gmass):
+    """FP64 CIC density of the particles (cell, off on the device), the
+    measuring stick of the precision study: the weights of
+    scalarProjectionCIC_project (projections.hpp:142-179) in double, summed
+    with float64 atomics (torch index_add_), m / res^3 per particle."""
+    import torch
+    nsites = n[0] * n[1] * n[2]
+    c = cell.to(torch.int64)
+    x, y, z = c % n[0], (c // n[0]) % n[1], c // (n[0] * n[1])
+    o = off.to(torch.float64)
+    rho = torch.zeros(nsites, dtype=torch.float64, device=cell.device)
+    scale = gmass * n[0] * n[1] * n[2]  # m / res^3 in a unit box
+    for k in range(8):
+        bx, by, bz = (k >> 2) & 1, (k >> 1) & 1, k & 1
+        w = ((o[:, 0] if bx else 1.0 - o[:, 0]) * (o[:, 1] if by else 1.0 - o[:, 1]) *
+             (o[:, 2] if bz else 1.0 - o[:, 2]))
+        idx = ((x + bx) % n[0]) + n[0] * (((y + by) % n[1]) + n[1] * ((z + bz) % n[2]))
+        rho.index_add_(0, idx, w * scale)
+        del w, idx
+    return rho
+
+
+def precision_stats(got, ref, floor_frac=1e-2):
+    """Error of a density against the FP64 one: per vertex relative on the
+    vertices above floor_frac of the mean density, and normalised by the
+    field maximum (max and rms)."""
+    import torch
+    d = (got.to(torch.float64) - ref).abs()
+    m = ref > floor_frac * ref.mean()
+    rel = d[m] / ref[m]
+    mx = ref.abs().max()
+    return {"cell_max": float(rel.max()), "cell_rms": float(rel.square().mean().sqrt()),
+            "norm_max": float(d.max() / mx), "norm_rms": float(d.square().mean().sqrt() / mx),
+            "floor_frac": floor_frac, "cells_above_floor": int(m.sum())}
+
+
+def precision_study(n, case, npart, local):
+    """The density of the same particles in the three deposit modes against
+    the FP64 one (C3: 512^3, 134M log-normal particles)."""
+    import torch
+    import latfield2_b200 as L
+    cell, off, vel = case
+    ref = fp64_density(cell, off, n, 1.0 / npart)
+    out = {}
+    for name, mode in (("fixed", L.DEPOSIT_FIXED64), ("fp32", L.DEPOSIT_FP32),
+                       ("fp32_plain", L.DEPOSIT_FP32_PLAIN)):
+        ctx = L.Context(n, box=1.0, mode=mode, device=local)
+        ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
+        rho = torch.empty(n[0] * n[1] * n[2], dtype=torch.float32, device=cell.device)
+        ctx.deposit_scalar(ctx.field(1, rho))
+        ctx.synchronize()
+        out[name] = precision_stats(rho, ref)
+        ctx.close()
+        del rho
+    del ref
+    torch.cuda.empty_cache()
+    out["reference"] = "FP64 CIC density of the same particles (torch float64 on the device)"
     return out
 
 
@@ -560,13 +696,14 @@ def slab_one_rank_ms(case, F, n, npart, dtau, warmup, steps, local):
     return e0.elapsed_time(e1) / steps
 
 
-def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
-    """Device time per lf2_step of the same particles with FP32 atomic
-    deposits (CUDA events on the launching stream)."""
+def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local, mode, proj_peak=None):
+    """Device time per lf2_step of the same particles with an FP32 deposit
+    mode (CUDA events on the launching stream); with proj_peak, also the
+    projection times in that mode."""
     import torch
     import latfield2_b200 as L
     cell, off, vel = case
-    ctx = L.Context(n, box=1.0, mode=L.DEPOSIT_FP32, device=local)
+    ctx = L.Context(n, box=1.0, mode=mode, device=local)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
     Fh, rho = ctx.field(3, F), ctx.field(1)
     for _ in range(warmup):
@@ -579,7 +716,63 @@ def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local):
     e1.record()
     torch.cuda.synchronize()
     ctx.synchronize()
-    return e0.elapsed_time(e1) / steps
+    ms = e0.elapsed_time(e1) / steps
+    proj = None
+    if proj_peak is not None:
+        del Fh, rho
+        proj = projection_times(ctx, npart, n[0] * n[1] * n[2], proj_peak)
+    ctx.close()
+    return ms, proj
+
+
+def chain_step_times(n, case, npart, local, reps=2):
+    """One step of the differentiable particle-mesh chain on the workload's
+    own particles (caller order, per-particle state): deposit, PM force (FFT
+    Poisson solve, coupling 4 pi), CIC gather, kick, drift and the final
+    deposit of the loss, then its hand-written adjoint (autodiff.PMChain,
+    checkpoint every step).  Device times (CUDA events) of the forward alone
+    and of forward + adjoint, the median of `reps` after one warm-up."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import pm_chain_loss
+    cell, off, vel = case
+    nn = n[0]
+    c = cell.to(torch.int64)
+    pos = torch.stack([c % nn, (c // nn) % nn, c // (nn * nn)], 1).to(torch.float64)
+    del c
+    pos.add_(off.to(torch.float64)).div_(nn)
+    v = vel.to(torch.float64)
+    m = torch.full((npart,), 1.0 / npart, dtype=torch.float64, device=pos.device)
+    g = torch.Generator(device=pos.device).manual_seed(7)
+    w = torch.randn(nn ** 3, generator=g, device=pos.device, dtype=torch.float64)
+    ctx = L.Context(n, box=1.0, device=local)
+    dt = 0.1 * 64.0 / nn
+
+    def timed(grad):
+        leaves = [t.requires_grad_(grad) for t in (pos, v, m, w)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        loss = pm_chain_loss(ctx, leaves[0], leaves[1], leaves[2], None, leaves[3], steps=1, dt=dt,
+                             checkpoint_every=1, operator="pm", coupling=4 * math.pi)
+        if grad:
+            loss.backward()
+        e1.record()
+        torch.cuda.synchronize()
+        for t in leaves:
+            t.grad = None
+            t.requires_grad_(False)
+        del loss
+        return e0.elapsed_time(e1)
+
+    timed(True)
+    fwd = sorted(timed(False) for _ in range(reps))[reps // 2]
+    both = sorted(timed(True) for _ in range(reps))[reps // 2]
+    ctx.close()
+    del pos, v, m, w
+    torch.cuda.empty_cache()
+    return {"workload": f"{nn}^3, {npart:,} particles, 1 step, PM force (FFT), checkpoint every step",
+            "forward_ms": fwd, "forward_adjoint_ms": both, "ratio": both / fwd}
 
 
 def replica_throughput(ms_local, npart, steps, pg=None, device="cpu"):
@@ -628,7 +821,7 @@ def main():
     nsites = n[0] * n[1] * n[2]
     ctx = L.Context(n, box=1.0, mode=mode, device=local)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
-    keep_case = (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) or args.slab
+    keep_case = (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) or args.slab or args.workload == "c5"
     fp32_case = (cell, off, vel) if keep_case else None
     del cell, off, vel
     Fh = ctx.field(3, F)
@@ -693,7 +886,7 @@ def main():
     # k computes (two buffers each way).
     e2e = e2e_pipelined(ctx, Fh, rho, F, n, nsites, npart, dtau, args.e2e_steps, pg, device, barrier)
 
-    proj = None if args.no_projections else full_cic_projections(ctx, npart, nsites, peak)
+    proj = None if args.no_projections else {w["mode"]: projection_times(ctx, npart, nsites, peak)}
     pm = None if args.no_pm else pm_operator(ctx, rho, n, nsites, peak)
 
     adj = adjoint_ratio(device) if (rank == 0 and not args.no_adjoint) else None
@@ -707,53 +900,79 @@ def main():
                 "note": "one self-exchanging rank; the exchange calls run, no peer"}
         torch.cuda.empty_cache()
 
-    # the same particles and steps with FP32 atomic deposits
+    # the same particles and steps with the FP32 deposit modes: compensated
+    # atomics (within 1e-6) and the plain FP32-atomic form
     fixed_vs_fp32 = None
+    precision = None
     if fp32_case is not None and not args.no_fp32 and mode == L.DEPOSIT_FIXED64:
+        ctx.close()
         del ctx, Fh, rho
         torch.cuda.empty_cache()
-        ms32 = fp32_step_ms(n, fp32_case, F, npart, dtau, args.warmup, args.steps, local)
-        ms32, _ = replica_throughput(ms32 * args.steps, npart, args.steps, pg, device)
-        ms32 /= args.steps
-        fixed_vs_fp32 = {"fixed_ms_per_step": ms_step, "fp32_ms_per_step": ms32,
-                         "ratio": ms_step / ms32}
+        res32 = {}
+        for nm, md in (("fp32", L.DEPOSIT_FP32), ("fp32_plain", L.DEPOSIT_FP32_PLAIN)):
+            ms32, p32 = fp32_step_ms(n, fp32_case, F, npart, dtau, args.warmup, args.steps, local, md,
+                                     None if args.no_projections else peak)
+            ms32, _ = replica_throughput(ms32 * args.steps, npart, args.steps, pg, device)
+            res32[nm] = ms32 / args.steps
+            if proj is not None and p32 is not None:
+                proj[nm] = p32
+            torch.cuda.empty_cache()
+        fixed_vs_fp32 = {"fixed_ms_per_step": ms_step, "fp32_ms_per_step": res32["fp32"],
+                         "fp32_plain_ms_per_step": res32["fp32_plain"],
+                         "ratio": ms_step / res32["fp32"],
+                         "ratio_vs_plain": ms_step / res32["fp32_plain"]}
+        if args.workload in ("c3", "c3s"):
+            precision = precision_study(n, fp32_case, npart, local)
+    # C5: the full forward + adjoint step of the differentiable chain on the
+    # same particles, beside the library's fixed-point and plain FP32 forward
+    c5 = None
+    if args.workload == "c5" and fp32_case is not None and not args.no_adjoint and world == 1:
+        try:
+            chain = chain_step_times(n, fp32_case, npart, local)
+        except torch.cuda.OutOfMemoryError as e:  # the chain keeps every field of the step
+            torch.cuda.empty_cache()
+            chain = {"unavailable": f"out of device memory: {str(e).splitlines()[0]}",
+                     "forward_adjoint_ms": None}
+        c5 = {"forward_ms": ms_step,
+              "fp32_forward_ms": fixed_vs_fp32["fp32_plain_ms_per_step"] if fixed_vs_fp32 else None,
+              "forward_adjoint_ms": chain["forward_adjoint_ms"], "chain": chain,
+              "note": "forward_ms: lf2_step (kick, drift, rebin, fixed-point deposit); "
+                      "fp32_forward_ms: the same with the plain FP32-atomic deposit; "
+                      "forward_adjoint_ms: one step of the differentiable chain and its adjoint "
+                      "(chain.forward_ms its forward alone)"}
     del fp32_case
 
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            ref = cpu_baseline_reference(args.cpu_seconds, 4)
-            if ref is not None:
-                ups, steps, used = ref
-                cpu = {"value": ups, "unit": UNIT, "cores": used, "kind": "reference",
-                       "sample": f"{used} ranks (2x2 process grid) x 64^3 lattice, 262,144 uniform "
-                                 f"particles, {steps} steps of scalarProjectionCIC_project+_comm, "
-                                 "updateVel CIC kick, moveParticles (the reference's own headers, "
-                                 "double)"}
+            # the reference on the same workload and host cores as the reference
+            # arm, bounded to one untimed and two timed steps
+            rec = cpu_reference_steps(args.workload, os.cpu_count() or 1, 2, 1)
+            if rec is not None:
+                cpu = cpu_reference_summary(args.workload, rec)
             else:
                 ups, steps = cpu_baseline_port(args.cpu_seconds, procs=1)
                 cpu = {"value": ups, "unit": UNIT, "cores": 1, "kind": "port",
                        "sample": f"64^3 lattice, 262,144 uniform particles, {steps} steps of "
                                  "deposit+comm, updateVel CIC kick, move (CPU restatement of the "
-                                 "reference, double, 1 thread)"}
+                                 "reference, double, 1 thread): a bounded sample, not the workload"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (int64 fixed-point deposit)" if mode == L.DEPOSIT_FIXED64 else "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "lattice": n[0], "particles": npart,
-                       "distribution": w["dist"], "deposit": w["mode"],
-                       "step": "kick+drift+rebin+scalar deposit (lf2_step)",
-                       "l2": f"inputs larger than L2 ({step_ab / 1e9:.1f} GB per step)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": workload_config(args.workload),
+            "deposit_mode": w["mode"] + (" (int64 fixed point)" if w["mode"] == "fixed" else ""),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "roofline": roofline, "step_roofline": step_roofline, "phase_ms": phase_ms,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks.summary(),
             "gpu_launches": launches,
             "adjoint_forward_ratio": adj["ratio"] if adj else None, "adjoint": adj,
             "adjoint_pm": adj_pm,
-            "fixed_vs_fp32": fixed_vs_fp32, "rebin": rebin, "projections": proj,
-            "pm_operator": pm, "slab_one_rank": slab,
+            "fixed_vs_fp32": fixed_vs_fp32, "precision": precision, "rebin": rebin,
+            "projections": proj,
+            "pm_operator": pm, "slab_one_rank": slab, "c5": c5,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

@@ -58,8 +58,18 @@ typedef int lf2_status;
 #define LF2_ERR_NOMEM (-4)       /* device allocation failed */
 #define LF2_ERR_UNSUPPORTED (-5) /* combination not provided */
 
-#define LF2_DEPOSIT_FP32 0    /* FP32 shared-memory accumulation */
-#define LF2_DEPOSIT_FIXED64 1 /* int64 fixed point, 2^-32 of a unit mass */
+/* Deposit modes (lf2_create).  FP32: FP32 atomics whose rounding errors are
+ * recovered exactly and carried in a second FP32 word, so every vertex sum
+ * is within about 1e-7 of exact whatever the order (not bit-identical run to
+ * run).  FIXED64: int64 fixed point, bit-exact run to run; quantum 2^-32 of
+ * a unit mass (the global particle mass, or the mean of per-particle
+ * masses), times V for momentum and V^2 for stress, V the smallest power of
+ * two above every |v_i| of the particles.  FP32_PLAIN: FP32 atomics without
+ * compensation, the fastest FP32 form; unordered additions leave a few 1e-6
+ * of error in dense vertices. */
+#define LF2_DEPOSIT_FP32 0
+#define LF2_DEPOSIT_FIXED64 1
+#define LF2_DEPOSIT_FP32_PLAIN 2
 
 #define LF2_PTR_HOST 0
 #define LF2_PTR_DEVICE 1
@@ -234,6 +244,14 @@ lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
  * LF2_ERR_UNSUPPORTED).  Both give the same particles (the order of the
  * particles inside a brick may differ); no reference counterpart. */
 lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
+/* Bounded waits of the pipelined kernel (no reference counterpart): every
+ * wait on a copy or on another warp gives up after `cycles` SM clock cycles
+ * (0: the default, about 2 s), raises LF2_FLAG_TIMEOUT and leaves the kernel
+ * after the copies already issued have landed.  With stall != 0 the consumer
+ * warps first wait on a barrier that nothing completes, so that their limit
+ * runs out: the way the tests drive this path (the particles of an
+ * interrupted pass are not valid; load them again). */
+lf2_status lf2_set_wait_limit(lf2_ctx* ctx, int64_t cycles, int stall);
 /* Kernel the last lf2_step used for its kick-drift-rebin pass: 1 per-brick,
  * 2 pipelined, 0 before the first step. */
 lf2_status lf2_last_move_kernel(lf2_ctx* ctx, int* which);

@@ -8,5 +8,6 @@ CUDA kernels behind the C ABI in include/lf2gpu.h.  `Context`, `FieldHandle`,
 include/latfield2_b200.hpp gives C++ code the reference's Lattice / Field /
 Particles / projection names over it.
 """
-from ._lib import (DEPOSIT_FIXED64, DEPOSIT_FP32, LF2Error, library_path, load)  # noqa: F401
+from ._lib import (DEPOSIT_FIXED64, DEPOSIT_FP32, DEPOSIT_FP32_PLAIN, LF2Error, library_path,  # noqa: F401
+                   load)
 from .core import Context, FieldHandle, KFieldHandle, SlabFFT  # noqa: F401

@@ -16,8 +16,9 @@ LF2_ERR_STATE = -3
 LF2_ERR_NOMEM = -4
 LF2_ERR_UNSUPPORTED = -5
 
-DEPOSIT_FP32 = 0
-DEPOSIT_FIXED64 = 1
+DEPOSIT_FP32 = 0        # FP32 atomics with compensated (TwoSum) rounding errors
+DEPOSIT_FIXED64 = 1     # int64 fixed point, bit-exact run to run
+DEPOSIT_FP32_PLAIN = 2  # FP32 atomics without compensation (the speed reference)
 FFT_FORWARD = 1
 FFT_BACKWARD = -1
 PTR_HOST = 0
@@ -29,6 +30,7 @@ FLAG_MASS_RANGE = 0x4
 FLAG_REPACK = 0x8
 FLAG_CAPACITY = 0x10
 FLAG_FIXED_OVERFLOW = 0x20
+FLAG_TIMEOUT = 0x40
 NOALLOC_MAX_BRICKS = 1363
 
 c_void_p = ctypes.c_void_p
@@ -84,6 +86,7 @@ SIGNATURES = {
     "lf2_drift_rebin": [c_void_p, c_double],
     "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],
     "lf2_set_move_kernel": [c_void_p, c_int],
+    "lf2_set_wait_limit": [c_void_p, c_i64, c_int],
     "lf2_last_move_kernel": [c_void_p, P(c_int)],
     "lf2_last_max_velocity": [c_void_p, c_void_p, c_int],
     "lf2_conservation": [c_void_p, P(c_double), P(c_double), P(c_double)],

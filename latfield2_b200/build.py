@@ -14,7 +14,7 @@ LIB = os.path.join(HERE, "liblf2gpu.so")
 SOURCES = ["lf2_abi.cu", "lf2_store.cu", "lf2_move.cu", "lf2_move_pipe.cu", "lf2_deposit.cu",
            "lf2_deposit_full.cu", "lf2_field.cu", "lf2_noalloc.cu", "lf2_pm.cu", "lf2_fft.cu",
            "lf2_exchange.cu"]
-HEADERS = ["lf2_common.cuh", "lf2_internal.h"]
+HEADERS = ["lf2_common.cuh", "lf2_deposit_common.cuh", "lf2_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -396,6 +396,13 @@ class Context:
         2 persistent TMA-pipelined."""
         self._check(_lib.load().lf2_set_move_kernel(self.h, int(which)), "set_move_kernel")
 
+    def set_wait_limit(self, cycles=0, stall=False):
+        """Limit of the pipelined move's bounded waits in SM cycles (0: the
+        default, about 2 s); stall=True makes its consumers wait on a barrier
+        nothing completes (tests of the timeout path)."""
+        self._check(_lib.load().lf2_set_wait_limit(self.h, int(cycles), 1 if stall else 0),
+                    "set_wait_limit")
+
     def last_max_velocity(self, out=None):
         """max |v| after the last kick.  With a CUDA float64 tensor `out` the
         value is written there in stream order (no wait); otherwise it is

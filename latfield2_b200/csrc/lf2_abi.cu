@@ -149,9 +149,8 @@ lf2_status check_flags(lf2_ctx* c)
   return LF2_OK;
 }
 
-lf2_status ensure_spill(lf2_ctx* c, int comps)
+lf2_status ensure_spill(lf2_ctx* c, size_t need)
 {
-  const size_t need = deposit_spill_slots(c, comps);
   if (need <= c->spill_slots) return LF2_OK;
   if (c->spill) {
     LF2_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -253,7 +252,9 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   *out = nullptr;
   for (int d = 0; d < 3; d++)
     if (n[d] < 1 || !(box[d] > 0)) return LF2_ERR_ARG;
-  if (deposit_mode != LF2_DEPOSIT_FP32 && deposit_mode != LF2_DEPOSIT_FIXED64) return LF2_ERR_ARG;
+  if (deposit_mode != LF2_DEPOSIT_FP32 && deposit_mode != LF2_DEPOSIT_FIXED64 &&
+      deposit_mode != LF2_DEPOSIT_FP32_PLAIN)
+    return LF2_ERR_ARG;
   // get_lattice_resolution (particles_tools.hpp:6-19) demands equal
   // resolutions; equal here means to 1e-12 relative, so that box = res * n
   // computed in floating point is accepted for any n.
@@ -297,6 +298,7 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMalloc(&c->stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->vmax_bits, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->repack, sizeof(int32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->diag, sizeof(unsigned long long) * 3) == cudaSuccess;
   ok = ok && cudaMalloc(&c->heap_top, sizeof(unsigned long long)) == cudaSuccess;
@@ -351,6 +353,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->mov_count);
   cudaFree(c->work);
   cudaFree(c->flags);
+  cudaFree(c->vmax_bits);
   cudaFree(c->repack);
   cudaFree(c->diag);
   cudaFree(c->heap_top);
@@ -840,7 +843,8 @@ static lf2_status deposit(lf2_ctx* c, lf2_field f, int kind, int comps)
 {
   if (!valid_field(c, f)) return LF2_ERR_ARG;
   if (f->comps != comps) return fail(c, LF2_ERR_ARG, "field has the wrong number of components");
-  LF2_TRY(ensure_spill(c, comps));
+  LF2_TRY(ensure_spill(c, kind >= 3 ? deposit_full_spill_slots(c, comps)
+                                     : deposit_spill_slots(c, comps)));
   {
     PhaseScope ps(c, PH_DEPOSIT);
     LF2_CUDA(c, kind >= 3 ? launch_deposit_full(c, kind, f->data, 0)
@@ -915,6 +919,14 @@ lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift
   }
   LF2_TRY(rebin_tail(c));
   if (rho) LF2_TRY(deposit(c, rho, 0, 1));
+  return LF2_OK;
+}
+
+lf2_status lf2_set_wait_limit(lf2_ctx* c, int64_t cycles, int stall)
+{
+  if (!c || cycles < 0) return LF2_ERR_ARG;
+  c->wait_cycles = cycles;
+  c->wait_stall = stall ? 1 : 0;
   return LF2_OK;
 }
 

@@ -1,7 +1,7 @@
 // lf2_deposit.cu -- CIC deposits of the brick-binned particles.
 //
 //   kind 0  scalar CIC        scalarProjectionCIC_project/_comm
-//                             (projections.hpp:75-300), FP32 or int64 fixed point
+//                             (projections.hpp:75-300)
 //   kind 1  vector CIC-NGP    vectorProjectionCICNGP_project/_comm (:421-681)
 //   kind 2  symtensor CIC-NGP symtensorProjectionCICNGP_project/_comm (:708-976)
 //
@@ -14,13 +14,34 @@
 // k_fixup then finishes every owned vertex with a zero coordinate by summing
 // the shell values of the up to 8 bricks that touch it, in a fixed order.
 // The periodic upper-halo fold of the reference's *_comm functions is thus
-// part of the deposit, every vertex is written exactly once, no global
-// atomics are used, and the fixed-point result is bit-exact run to run.
+// part of the deposit, every vertex is written exactly once and no global
+// atomics are used.
+//
+// Three accumulation modes (the context's deposit mode):
+//   LF2_DEPOSIT_FP32        FP32 shared atomics with compensation: each add
+//                           returns the value it replaced, the rounding error
+//                           of that add is recovered exactly (TwoSum) and
+//                           accumulated in a second FP32 word.  hi + lo is the
+//                           sum to within the rounding of the terms (about
+//                           1e-7 relative), whatever the order.
+//   LF2_DEPOSIT_FIXED64     int64 fixed point: every contribution is rounded
+//                           once, deterministically, to an integer quantum;
+//                           the integer sums do not depend on the order, so
+//                           the result is bit-exact run to run.  Scalar: 2^-32
+//                           of a unit mass.  Momentum and stress are signed:
+//                           2^-32 of a unit mass times V (momentum) or V^2
+//                           (stress), V the smallest power of two above every
+//                           |v_i| of the particles (found on the device before
+//                           the deposit, k_vmax).
+//   LF2_DEPOSIT_FP32_PLAIN  FP32 shared atomics without compensation: the
+//                           speed reference; its sums in dense vertices carry
+//                           the rounding of unordered FP32 additions.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <type_traits>
 
+#include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
 namespace lf2 {
@@ -32,67 +53,49 @@ namespace {
 #endif
 constexpr int DEP_THREADS = LF2_DEP_THREADS;
 
+// Components of the field of a kind.
 template <int KIND>
-struct Comps;
-template <>
-struct Comps<0> { static constexpr int value = 1; };
-template <>
-struct Comps<1> { static constexpr int value = 3; };
-template <>
-struct Comps<2> { static constexpr int value = 6; };
+struct Comps { static constexpr int value = KIND == 0 ? 1 : KIND == 1 ? 3 : 6; };
+
+// A tile pass accumulates NC components of the field.  The plain mode keeps
+// one 32-bit word per vertex and component and does every kind in one pass
+// (the tensor's six components in a 118 KB tile); the compensated and the
+// fixed-point modes keep two words, so the tensor takes two passes of three
+// components (T_00, T_11, T_22 at the vertices, then T_01, T_02, T_12 on the
+// plaquettes), each with a 118 KB tile.
+template <int KIND, int PASS, int ACC>
+struct Pass {
+  static constexpr int NC = KIND == 0 ? 1 : KIND == 1 ? 3 : (ACC == ACC_PLAIN ? 6 : 3);
+  static constexpr int WORDS = ACC == ACC_PLAIN ? 1 : 2;
+  // field component of pass-local component j
+  __host__ __device__ static constexpr int comp(int j)
+  {
+    return KIND != 2 || ACC == ACC_PLAIN ? j
+           : PASS == 0                   ? (j == 0 ? 0 : j == 1 ? 3 : 5)
+                                         : (j == 0 ? 1 : j == 1 ? 2 : 4);
+  }
+  static constexpr size_t smem() { return (size_t)NC * WORDS * TILE3 * 4; }
+  // threads per CTA: a tile above 100 KB leaves room for one CTA per SM, so
+  // it gets twice the warps
+  static constexpr int THREADS = smem() > 100 * 1024 ? 2 * DEP_THREADS : DEP_THREADS;
+};
 
 __device__ __forceinline__ float sel(int b, float up, float dn) { return b ? up : dn; }
 
-// Fixed-point accumulation in shared memory.  Each 64-bit vertex sum is kept
-// as two 32-bit partial sums, lo = sum(q & 0xffff) and hi = sum(q >> 16), so
-// that every update is a native 32-bit shared-memory reduction; the sum is
-// lo + (hi << 16).  With q <= 2^32 per particle and corner, neither partial
-// sum can wrap while a brick holds at most 65535 particles (DEP_SPLIT_MAX);
-// larger bricks fall back to 64-bit shared atomics.
-constexpr int DEP_SPLIT_MAX = 65535;
-constexpr int DEP_ITEMS = 4;  // particles in flight per thread
-
-template <bool SPLIT>
-__device__ __forceinline__ void add_fixed(unsigned char* smem, int t, uint64_t q)
-{
-  if (SPLIT) {
-    uint32_t* lo = reinterpret_cast<uint32_t*>(smem);
-    uint32_t* hi = lo + TILE3;
-    atomicAdd(&lo[t], (uint32_t)(q & 0xffffu));
-    atomicAdd(&hi[t], (uint32_t)(q >> 16));
-  } else {
-    atomicAdd(reinterpret_cast<unsigned long long*>(smem) + t, (unsigned long long)q);
-  }
-}
-
-template <bool SPLIT>
-__device__ __forceinline__ void deposit_fixed_particle(unsigned char* smem, int t0, float fx,
-                                                       float fy, float fz, bool has_mass,
-                                                       uint64_t mq)
-{
-  // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle).
-  const uint32_t ux = __float2uint_rn(fx * 2147483648.0f);
-  const uint32_t uy = __float2uint_rn(fy * 2147483648.0f);
-  const uint32_t uz = __float2uint_rn(fz * 2147483648.0f);
-  const uint32_t qx[2] = {(1u << 31) - ux, ux};
-  const uint32_t qy[2] = {(1u << 31) - uy, uy};
-  const uint32_t qz[2] = {(1u << 31) - uz, uz};
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-    uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
-    if (has_mass) q = (q * mq + (1ull << 23)) >> 24;
-    add_fixed<SPLIT>(smem, t0 + cx + cy * TILE + cz * TILE * TILE, q);
-  }
-}
-
-template <int KIND, bool FIXED>
-__global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositParams dp,
+// ------------------------------------------------------------- tile pass
+template <int KIND, int PASS, int ACC>
+__global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(StoreView v, DepositParams dp,
                                                          float* __restrict__ out,
                                                          uint64_t* __restrict__ spill,
+                                                         const uint32_t* __restrict__ vmax_bits,
                                                          uint32_t* flags)
 {
+  using P = Pass<KIND, PASS, ACC>;
+  constexpr int NC = P::NC;
   constexpr int C = Comps<KIND>::value;
+  constexpr bool FIXED = ACC == ACC_FIXED;
+  constexpr bool SIGNED = KIND != 0;
+  constexpr int T = P::THREADS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
 
   const Geom& g = v.g;
@@ -104,23 +107,30 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
   const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
   const int64_t base = v.seg_start[b];
   const int cnt = LF2_BRICK_COUNT(v, b);
-  const bool split = FIXED && cnt <= DEP_SPLIT_MAX;
+  TileRef<TILE3> tr{smem_raw, FIXED && cnt <= split_max<SIGNED>(dp.has_mass != 0)};
+  // fixed point: velocity quantum and conversion scale for this field
+  int vexp = 0;
+  if (FIXED && KIND != 0) vexp = vexp_of(*vmax_bits);
+  const float vscale = vel_scale(vexp);
+  const float conv = FIXED ? ldexpf(dp.fixed_scale, KIND == 1 ? vexp : 2 * vexp) : 0.0f;
+  if (FIXED && threadIdx.x == 0 && b == 0 && !(conv > 0.0f && conv <= 3.402823466e38f))
+    set_flag(flags, ERR_FIXED_OVERFLOW);  // V^p / res^3 outside the FP32 range
 
   {
     uint32_t* z = reinterpret_cast<uint32_t*>(smem_raw);
-    const int words = FIXED ? 2 * TILE3 : C * TILE3;
+    constexpr int words = NC * P::WORDS * TILE3;
     for (int t = threadIdx.x; t < words; t += blockDim.x) z[t] = 0u;
   }
   __syncthreads();
 
-  float* facc = reinterpret_cast<float*>(smem_raw);
-  for (int c0 = 0; c0 < cnt; c0 += DEP_ITEMS * DEP_THREADS) {
-    uint32_t key[DEP_ITEMS];
-    float fx[DEP_ITEMS], fy[DEP_ITEMS], fz[DEP_ITEMS], m[DEP_ITEMS];
-    float vx[DEP_ITEMS], vy[DEP_ITEMS], vz[DEP_ITEMS];
+  constexpr int ITEMS = 4;  // particles in flight per thread
+  for (int c0 = 0; c0 < cnt; c0 += ITEMS * T) {
+    uint32_t key[ITEMS];
+    float fx[ITEMS], fy[ITEMS], fz[ITEMS], m[ITEMS];
+    float vx[ITEMS], vy[ITEMS], vz[ITEMS];
 #pragma unroll
-    for (int j = 0; j < DEP_ITEMS; j++) {
-      const int i = c0 + j * DEP_THREADS + threadIdx.x;
+    for (int j = 0; j < ITEMS; j++) {
+      const int i = c0 + j * T + threadIdx.x;
       if (i < cnt) {
         const int64_t p = base + i;
         key[j] = v.a.key[p];
@@ -136,25 +146,85 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
       }
     }
 #pragma unroll
-    for (int j = 0; j < DEP_ITEMS; j++) {
-      const int i = c0 + j * DEP_THREADS + threadIdx.x;
+    for (int j = 0; j < ITEMS; j++) {
+      const int i = c0 + j * T + threadIdx.x;
       if (i >= cnt) continue;
       int x, y, z;
       unpack_key(g, key[j], x, y, z);
       const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
-      if (KIND == 0 && FIXED) {
+      constexpr int TY = TILE, TZ = TILE * TILE;
+      if (FIXED) {
         uint64_t mq = 0;
-        if (dp.has_mass) {
-          const float mr = __fmul_rn(m[j], dp.inv_unit);
-          if (!(mr >= 0.0f && mr < 64.0f)) set_flag(flags, ERR_MASS_RANGE);
-          mq = (uint64_t)__float2uint_rn(fminf(fmaxf(mr, 0.0f), 63.0f) * 16777216.0f);
+        if (dp.has_mass) mq = mass_q(m[j], dp.inv_unit, flags);
+        const bool hm = dp.has_mass != 0;
+        // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle)
+        const uint32_t ux = weight_q(fx[j]), uy = weight_q(fy[j]), uz = weight_q(fz[j]);
+        const uint32_t qx[2] = {(1u << 31) - ux, ux};
+        const uint32_t qy[2] = {(1u << 31) - uy, uy};
+        const uint32_t qz[2] = {(1u << 31) - uz, uz};
+        constexpr uint32_t ONE = 1u << 31;
+        if (KIND == 0) {
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+            const uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
+            add_fixed(tr, 0, t0 + cx + cy * TY + cz * TZ, apply_mass_sign(q, hm, mq, false));
+          }
+        } else if (KIND == 1) {
+          // projections.hpp:501-544: component i is NGP along i, CIC across
+          const float vv[3] = {vx[j], vy[j], vz[j]};
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const uint32_t vq = vel_q(vv[c], vscale);
+            const bool neg = vv[c] < 0.0f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const int a = (k >> 1) & 1, bb = k & 1;
+              uint64_t w;
+              int t;
+              if (c == 0) w = fixed_corner(ONE, qy[a], qz[bb]), t = t0 + a * TY + bb * TZ;
+              else if (c == 1) w = fixed_corner(qx[a], ONE, qz[bb]), t = t0 + a + bb * TZ;
+              else w = fixed_corner(qx[a], qy[bb], ONE), t = t0 + a + bb * TY;
+              add_fixed(tr, c, t, apply_mass_sign(mul31(w, vq), hm, mq, neg));
+            }
+          }
+        } else if (PASS == 0) {
+          // projections.hpp:788-807: T_ii = m v_i^2 at the 8 vertices
+          const float vv[3] = {vx[j], vy[j], vz[j]};
+          uint64_t v2[3];
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const uint32_t q = vel_q(vv[d], vscale);
+            v2[d] = vel2_q(q, q);
+          }
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+            const uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+            const int t = t0 + cx + cy * TY + cz * TZ;
+#pragma unroll
+            for (int d = 0; d < 3; d++) add_fixed(tr, d, t, apply_mass_sign(mul31(w, v2[d]), hm, mq, false));
+          }
+        } else {
+          // projections.hpp:809-821: T_ij on the (i,j) plaquette, CIC along
+          // the third dim
+          const float vv[3] = {vx[j], vy[j], vz[j]};
+          const uint32_t q0 = vel_q(vv[0], vscale), q1 = vel_q(vv[1], vscale), q2 = vel_q(vv[2], vscale);
+          const uint64_t v01 = vel2_q(q0, q1), v02 = vel2_q(q0, q2), v12 = vel2_q(q1, q2);
+          const bool n01 = (vv[0] < 0.0f) != (vv[1] < 0.0f), n02 = (vv[0] < 0.0f) != (vv[2] < 0.0f),
+                     n12 = (vv[1] < 0.0f) != (vv[2] < 0.0f);
+          // (2^-31 weight) x (2^-31 velocity product), rounded to 2^-32
+          auto w1 = [](uint32_t a, uint64_t f) { return ((uint64_t)a * f + (1ull << 29)) >> 30; };
+          add_fixed(tr, 0, t0, apply_mass_sign(w1(qz[0], v01), hm, mq, n01));
+          add_fixed(tr, 0, t0 + TZ, apply_mass_sign(w1(qz[1], v01), hm, mq, n01));
+          add_fixed(tr, 1, t0, apply_mass_sign(w1(qy[0], v02), hm, mq, n02));
+          add_fixed(tr, 1, t0 + TY, apply_mass_sign(w1(qy[1], v02), hm, mq, n02));
+          add_fixed(tr, 2, t0, apply_mass_sign(w1(qx[0], v12), hm, mq, n12));
+          add_fixed(tr, 2, t0 + 1, apply_mass_sign(w1(qx[1], v12), hm, mq, n12));
         }
-        if (split)
-          deposit_fixed_particle<true>(smem_raw, t0, fx[j], fy[j], fz[j], dp.has_mass, mq);
-        else
-          deposit_fixed_particle<false>(smem_raw, t0, fx[j], fy[j], fz[j], dp.has_mass, mq);
         continue;
       }
+      // FP32 modes: the arithmetic of the reference's projections in FP32
       const float gx = __fsub_rn(1.0f, fx[j]), gy = __fsub_rn(1.0f, fy[j]),
                   gz = __fsub_rn(1.0f, fz[j]);
       const float ox = fx[j], oy = fy[j], oz = fz[j];
@@ -165,86 +235,99 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
           const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
           const float w = __fmul_rn(
               __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz)), mf);
-          atomicAdd(&facc[t0 + cx + cy * TILE + cz * TILE * TILE], w);
+          add_float<ACC>(tr, 0, t0 + cx + cy * TY + cz * TZ, w);
         }
       } else if (KIND == 1) {
         // projections.hpp:501-544: component i is NGP along i, CIC across.
         const float vxm = __fmul_rn(mf, vx[j]);
         const float vym = __fmul_rn(mf, vy[j]);
         const float vzm = __fmul_rn(mf, vz[j]);
-        constexpr int TY = TILE, TZ = TILE * TILE;
-        float* a0 = facc;
-        float* a1 = facc + TILE3;
-        float* a2 = facc + 2 * TILE3;
-        atomicAdd(&a0[t0], __fmul_rn(__fmul_rn(vxm, gy), gz));
-        atomicAdd(&a0[t0 + TY], __fmul_rn(__fmul_rn(vxm, oy), gz));
-        atomicAdd(&a0[t0 + TZ], __fmul_rn(__fmul_rn(vxm, gy), oz));
-        atomicAdd(&a0[t0 + TY + TZ], __fmul_rn(__fmul_rn(vxm, oy), oz));
-        atomicAdd(&a1[t0], __fmul_rn(__fmul_rn(vym, gx), gz));
-        atomicAdd(&a1[t0 + 1], __fmul_rn(__fmul_rn(vym, ox), gz));
-        atomicAdd(&a1[t0 + TZ], __fmul_rn(__fmul_rn(vym, gx), oz));
-        atomicAdd(&a1[t0 + 1 + TZ], __fmul_rn(__fmul_rn(vym, ox), oz));
-        atomicAdd(&a2[t0], __fmul_rn(__fmul_rn(vzm, gx), gy));
-        atomicAdd(&a2[t0 + 1], __fmul_rn(__fmul_rn(vzm, ox), gy));
-        atomicAdd(&a2[t0 + TY], __fmul_rn(__fmul_rn(vzm, gx), oy));
-        atomicAdd(&a2[t0 + 1 + TY], __fmul_rn(__fmul_rn(vzm, ox), oy));
+        add_float<ACC>(tr, 0, t0, __fmul_rn(__fmul_rn(vxm, gy), gz));
+        add_float<ACC>(tr, 0, t0 + TY, __fmul_rn(__fmul_rn(vxm, oy), gz));
+        add_float<ACC>(tr, 0, t0 + TZ, __fmul_rn(__fmul_rn(vxm, gy), oz));
+        add_float<ACC>(tr, 0, t0 + TY + TZ, __fmul_rn(__fmul_rn(vxm, oy), oz));
+        add_float<ACC>(tr, 1, t0, __fmul_rn(__fmul_rn(vym, gx), gz));
+        add_float<ACC>(tr, 1, t0 + 1, __fmul_rn(__fmul_rn(vym, ox), gz));
+        add_float<ACC>(tr, 1, t0 + TZ, __fmul_rn(__fmul_rn(vym, gx), oz));
+        add_float<ACC>(tr, 1, t0 + 1 + TZ, __fmul_rn(__fmul_rn(vym, ox), oz));
+        add_float<ACC>(tr, 2, t0, __fmul_rn(__fmul_rn(vzm, gx), gy));
+        add_float<ACC>(tr, 2, t0 + 1, __fmul_rn(__fmul_rn(vzm, ox), gy));
+        add_float<ACC>(tr, 2, t0 + TY, __fmul_rn(__fmul_rn(vzm, gx), oy));
+        add_float<ACC>(tr, 2, t0 + 1 + TY, __fmul_rn(__fmul_rn(vzm, ox), oy));
       } else {
         // projections.hpp:786-843: T_ii at the 8 vertices, T_ij on plaquettes.
         const float vv[3] = {vx[j], vy[j], vz[j]};
-        constexpr int diag[3] = {0, 3, 5};
+        constexpr bool DIAG = ACC == ACC_PLAIN || PASS == 0;
+        constexpr bool OFF = ACC == ACC_PLAIN || PASS == 1;
+        if (DIAG) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-          const float mv2 = __fmul_rn(__fmul_rn(mf, vv[d]), vv[d]);
-          float* a = facc + diag[d] * TILE3;
+          for (int d = 0; d < 3; d++) {
+            // pass-local component of T_dd: 0, 3, 5 in the six-component
+            // plain tile, 0, 1, 2 in the diagonal pass
+            const int jd = ACC == ACC_PLAIN ? (d == 0 ? 0 : d == 1 ? 3 : 5) : d;
+            const float mv2 = __fmul_rn(__fmul_rn(mf, vv[d]), vv[d]);
 #pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-            const float w = __fmul_rn(
-                __fmul_rn(__fmul_rn(mv2, sel(cx, ox, gx)), sel(cy, oy, gy)), sel(cz, oz, gz));
-            atomicAdd(&a[t0 + cx + cy * TILE + cz * TILE * TILE], w);
+            for (int k = 0; k < 8; k++) {
+              const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+              const float w = __fmul_rn(
+                  __fmul_rn(__fmul_rn(mv2, sel(cx, ox, gx)), sel(cy, oy, gy)), sel(cz, oz, gz));
+              add_float<ACC>(tr, jd, t0 + cx + cy * TY + cz * TZ, w);
+            }
           }
         }
-        const float m01 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[1]);
-        const float m02 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[2]);
-        const float m12 = __fmul_rn(__fmul_rn(mf, vv[1]), vv[2]);
-        atomicAdd(&facc[1 * TILE3 + t0], __fmul_rn(m01, gz));
-        atomicAdd(&facc[1 * TILE3 + t0 + TILE * TILE], __fmul_rn(m01, oz));
-        atomicAdd(&facc[2 * TILE3 + t0], __fmul_rn(m02, gy));
-        atomicAdd(&facc[2 * TILE3 + t0 + TILE], __fmul_rn(m02, oy));
-        atomicAdd(&facc[4 * TILE3 + t0], __fmul_rn(m12, gx));
-        atomicAdd(&facc[4 * TILE3 + t0 + 1], __fmul_rn(m12, ox));
+        if (OFF) {
+          const int j01 = ACC == ACC_PLAIN ? 1 : 0, j02 = ACC == ACC_PLAIN ? 2 : 1,
+                    j12 = ACC == ACC_PLAIN ? 4 : 2;
+          const float m01 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[1]);
+          const float m02 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[2]);
+          const float m12 = __fmul_rn(__fmul_rn(mf, vv[1]), vv[2]);
+          add_float<ACC>(tr, j01, t0, __fmul_rn(m01, gz));
+          add_float<ACC>(tr, j01, t0 + TZ, __fmul_rn(m01, oz));
+          add_float<ACC>(tr, j02, t0, __fmul_rn(m02, gy));
+          add_float<ACC>(tr, j02, t0 + TY, __fmul_rn(m02, oy));
+          add_float<ACC>(tr, j12, t0, __fmul_rn(m12, gx));
+          add_float<ACC>(tr, j12, t0 + 1, __fmul_rn(m12, ox));
+        }
       }
     }
   }
   __syncthreads();
 
-  // Flush: interior vertices to the field, shell vertices to the shell store.
+  // Flush: interior vertices to the field, shell vertices to the shell store
+  // (8-byte slots: the integer sum, hi and lo, or the plain float).
   uint64_t* sp = spill + (size_t)b * C * SHELL;
-  const uint32_t* lo = reinterpret_cast<const uint32_t*>(smem_raw);
-  const unsigned long long* a64 = reinterpret_cast<const unsigned long long*>(smem_raw);
+  const float* facc = reinterpret_cast<const float*>(smem_raw);
   for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
-    const int i = t % TILE, j = (t / TILE) % TILE, k = t / (TILE * TILE);
-    if (i > ex || j > ey || k > ez) continue;
-    const bool shell = i == 0 || i == ex || j == 0 || j == ey || k == 0 || k == ez;
-    if (FIXED) {
-      const uint64_t q = split ? (uint64_t)lo[t] + ((uint64_t)lo[TILE3 + t] << 16) : a64[t];
-      if (shell) {
-        sp[shell_index(i == ex ? BRICK : i, j == ey ? BRICK : j, k == ez ? BRICK : k)] = q;
+    const int i = t % TILE, jj = (t / TILE) % TILE, k = t / (TILE * TILE);
+    if (i > ex || jj > ey || k > ez) continue;
+    const bool shell = i == 0 || i == ex || jj == 0 || jj == ey || k == 0 || k == ez;
+    const int si =
+        shell ? shell_index(i == ex ? BRICK : i, jj == ey ? BRICK : jj, k == ez ? BRICK : k) : 0;
+    const int64_t s = site_index(g, x0 + i, y0 + jj, z0 + k);
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      const int c = P::comp(j);
+      if (FIXED) {
+        const long long q = tile_fixed<SIGNED>(tr, j, t);
+        if (shell) {
+          sp[(size_t)c * SHELL + si] = (uint64_t)q;
+        } else {
+          if (!SIGNED && q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+          out[(size_t)c * g.nsites + s] = __fmul_rn(__ll2float_rn(q), conv);
+        }
+      } else if (ACC == ACC_COMP) {
+        const float hi = facc[(size_t)j * 2 * TILE3 + t], lo = facc[(size_t)j * 2 * TILE3 + TILE3 + t];
+        if (shell)
+          reinterpret_cast<float2*>(sp)[(size_t)c * SHELL + si] = make_float2(hi, lo);
+        else
+          out[(size_t)c * g.nsites + s] = __fadd_rn(hi, lo);
       } else {
-        if ((long long)q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-        out[site_index(g, x0 + i, y0 + j, z0 + k)] = __fmul_rn(__ll2float_rn((long long)q),
-                                                               dp.fixed_scale);
+        const float f = facc[(size_t)j * TILE3 + t];
+        if (shell)
+          reinterpret_cast<float*>(sp)[(size_t)c * SHELL + si] = f;
+        else
+          out[(size_t)c * g.nsites + s] = f;
       }
-      continue;
-    }
-    if (shell) {
-      const int si = shell_index(i == ex ? BRICK : i, j == ey ? BRICK : j, k == ez ? BRICK : k);
-#pragma unroll
-      for (int c = 0; c < C; c++) reinterpret_cast<float*>(sp)[c * SHELL + si] = facc[c * TILE3 + t];
-    } else {
-      const int64_t s = site_index(g, x0 + i, y0 + j, z0 + k);
-#pragma unroll
-      for (int c = 0; c < C; c++) out[c * g.nsites + s] = facc[c * TILE3 + t];
     }
   }
 }
@@ -252,11 +335,16 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit(StoreView v, DepositPar
 // One CTA per brick: every owned vertex with a zero coordinate sums the shell
 // values of the bricks that touch it: its own tile (subset 0) and, for every
 // non-empty subset S of the dims where its coordinate is 0, the lower
-// neighbour brick across S at tile coordinate BRICK in those dims.
-template <int C, bool FIXED>
+// neighbour brick across S at tile coordinate BRICK in those dims.  The sum
+// runs in that fixed order: exact integers (fixed point), a compensated FP32
+// sum of the hi and lo words, or plain FP32 additions.
+template <int KIND, int ACC>
 __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_scale,
-                        float* __restrict__ out, uint32_t* flags)
+                        const uint32_t* __restrict__ vmax_bits, float* __restrict__ out,
+                        uint32_t* flags)
 {
+  constexpr int C = Comps<KIND>::value;
+  constexpr bool SIGNED = KIND != 0;
   const int64_t b = blockIdx.x;
   int bx, by, bz;
   brick_coords(g, b, bx, by, bz);
@@ -266,6 +354,11 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
   const int bxm = bx ? bx - 1 : g.nb[0] - 1;
   const int bym = by ? by - 1 : g.nb[1] - 1;
   const int bzm = bz ? bz - 1 : g.nb[2] - 1;
+  float conv = 0.0f;
+  if (ACC == ACC_FIXED) {
+    const int vexp = KIND != 0 ? vexp_of(*vmax_bits) : 0;
+    conv = ldexpf(fixed_scale, KIND == 0 ? 0 : KIND == 1 ? vexp : 2 * vexp);
+  }
   const int nface = ey * ez + (ex - 1) * ez + (ex - 1) * (ey - 1);
   for (int f = threadIdx.x; f < nface; f += blockDim.x) {
     int i, j, k;
@@ -285,12 +378,13 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
       j = 1 + r / (ex - 1);
     }
     const int zmask = (i == 0 ? 1 : 0) | (j == 0 ? 2 : 0) | (k == 0 ? 4 : 0);
-    uint64_t qs[C];
-    float fs[C];
+    long long qs[C];
+    float fs[C], fc[C];
 #pragma unroll
     for (int c = 0; c < C; c++) {
       qs[c] = 0;
       fs[c] = 0.0f;
+      fc[c] = 0.0f;
     }
     for (int s = 0; s < 8; s++) {
       if ((s & zmask) != s) continue;
@@ -300,19 +394,24 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
       const uint64_t* sp = spill + (size_t)nb * C * SHELL;
 #pragma unroll
       for (int c = 0; c < C; c++) {
-        if (FIXED)
-          qs[c] += sp[c * SHELL + si];
-        else
+        if (ACC == ACC_FIXED) {
+          qs[c] += (long long)sp[c * SHELL + si];
+        } else if (ACC == ACC_COMP) {
+          const float2 hl = reinterpret_cast<const float2*>(sp)[c * SHELL + si];
+          comp_acc(fs[c], fc[c], hl.x, hl.y);
+        } else {
           fs[c] = __fadd_rn(fs[c], reinterpret_cast<const float*>(sp)[c * SHELL + si]);
+        }
       }
     }
     const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
 #pragma unroll
     for (int c = 0; c < C; c++) {
-      if (FIXED) {
-        const long long q = (long long)qs[c];
-        if (q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-        out[c * g.nsites + site] = __fmul_rn(__ll2float_rn(q), fixed_scale);
+      if (ACC == ACC_FIXED) {
+        if (!SIGNED && qs[c] < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+        out[c * g.nsites + site] = __fmul_rn(__ll2float_rn(qs[c]), conv);
+      } else if (ACC == ACC_COMP) {
+        out[c * g.nsites + site] = __fadd_rn(fs[c], fc[c]);
       } else {
         out[c * g.nsites + site] = fs[c];
       }
@@ -320,24 +419,70 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
   }
 }
 
-template <int KIND, bool FIXED>
+// Largest |v_i| of the stored particles, as the bits of a non-negative float
+// (they order as unsigned integers); a non-finite velocity raises the flag.
+__global__ void __launch_bounds__(256) k_vmax(StoreView v, uint32_t* vmax_bits, uint32_t* flags)
+{
+  const int64_t b = blockIdx.x;
+  const int64_t base = v.seg_start[b];
+  const int cnt = LF2_BRICK_COUNT(v, b);
+  uint32_t m = 0u;
+  bool bad = false;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int64_t p = base + i;
+    const uint32_t a = __float_as_uint(v.a.vx[p]) & 0x7fffffffu;
+    const uint32_t c = __float_as_uint(v.a.vy[p]) & 0x7fffffffu;
+    const uint32_t d = __float_as_uint(v.a.vz[p]) & 0x7fffffffu;
+    const uint32_t mm = max(a, max(c, d));
+    bad |= mm >= 0x7f800000u;
+    m = max(m, mm);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) set_flag(flags, ERR_NONFINITE);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(vmax_bits, m);
+}
+
+template <int KIND, int PASS, int ACC>
+cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
+{
+  using P = Pass<KIND, PASS, ACC>;
+  const size_t smem = P::smem();
+  cudaError_t e = cudaFuncSetAttribute(k_deposit<KIND, PASS, ACC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  c->launches += 1;
+  k_deposit<KIND, PASS, ACC><<<(unsigned)c->g.nbricks, P::THREADS, smem, c->stream>>>(
+      view(c), dp, out, c->spill, c->vmax_bits, c->flags);
+  return cudaGetLastError();
+}
+
+template <int KIND, int ACC>
 cudaError_t run(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
 {
-  constexpr int C = Comps<KIND>::value;
   const unsigned nb = (unsigned)c->g.nbricks;
   if (stage == 0) {
-    const size_t smem = (size_t)C * TILE3 * (FIXED ? sizeof(unsigned long long) : sizeof(float));
-    cudaError_t e = cudaFuncSetAttribute(k_deposit<KIND, FIXED>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    c->launches += 1;
-    k_deposit<KIND, FIXED><<<nb, DEP_THREADS, smem, c->stream>>>(view(c), dp, out, c->spill,
-                                                                 c->flags);
-  } else {
-    c->launches += 1;
-    k_fixup<C, FIXED><<<nb, 256, 0, c->stream>>>(c->g, c->spill, dp.fixed_scale, out, c->flags);
+    if (ACC == ACC_FIXED && KIND != 0) {
+      cudaError_t e = launch_vmax(c);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = tile_pass<KIND, 0, ACC>(c, out, dp);
+    if constexpr (KIND == 2 && ACC != ACC_PLAIN) {
+      if (e == cudaSuccess) e = tile_pass<KIND, 1, ACC>(c, out, dp);
+    }
+    return e;
   }
+  c->launches += 1;
+  k_fixup<KIND, ACC><<<nb, 256, 0, c->stream>>>(c->g, c->spill, dp.fixed_scale, c->vmax_bits, out,
+                                                c->flags);
   return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t run_mode(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
+{
+  if (c->mode == LF2_DEPOSIT_FIXED64) return run<KIND, ACC_FIXED>(c, out, dp, stage);
+  if (c->mode == LF2_DEPOSIT_FP32_PLAIN) return run<KIND, ACC_PLAIN>(c, out, dp, stage);
+  return run<KIND, ACC_COMP>(c, out, dp, stage);
 }
 
 }  // namespace
@@ -348,7 +493,16 @@ size_t deposit_spill_slots(const lf2_ctx* c, int comps)
   return (size_t)c->g.nbricks * (size_t)comps * SHELL;
 }
 
-cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage)
+cudaError_t launch_vmax(lf2_ctx* c)
+{
+  cudaError_t e = cudaMemsetAsync(c->vmax_bits, 0, sizeof(uint32_t), c->stream);
+  if (e != cudaSuccess) return e;
+  c->launches += 1;
+  k_vmax<<<(unsigned)c->g.nbricks, 256, 0, c->stream>>>(view(c), c->vmax_bits, c->flags);
+  return cudaGetLastError();
+}
+
+DepositParams deposit_params(const lf2_ctx* c)
 {
   DepositParams dp;
   const double vol = c->res * c->res * c->res;
@@ -357,10 +511,15 @@ cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage)
   dp.fixed_scale = (float)(std::ldexp(1.0, -32) * c->m_unit / vol);
   dp.inv_unit = (float)(1.0 / c->m_unit);
   dp.has_mass = c->has_mass ? 1 : 0;
-  const bool fixed = kind == 0 && c->mode == LF2_DEPOSIT_FIXED64;
-  if (kind == 0) return fixed ? run<0, true>(c, out, dp, stage) : run<0, false>(c, out, dp, stage);
-  if (kind == 1) return run<1, false>(c, out, dp, stage);
-  return run<2, false>(c, out, dp, stage);
+  return dp;
+}
+
+cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage)
+{
+  const DepositParams dp = deposit_params(c);
+  if (kind == 0) return run_mode<0>(c, out, dp, stage);
+  if (kind == 1) return run_mode<1>(c, out, dp, stage);
+  return run_mode<2>(c, out, dp, stage);
 }
 
 }  // namespace lf2

@@ -1,0 +1,151 @@
+// lf2_deposit_common.cuh -- accumulation helpers shared by the deposit tile
+// passes of lf2_deposit.cu (CIC and CIC-NGP projections) and
+// lf2_deposit_full.cu (full-CIC projections): the compensated FP32 add, the
+// split fixed-point accumulation and the deterministic integer weights of the
+// fixed-point mode.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lf2_common.cuh"
+#include "lf2gpu.h"
+
+namespace lf2 {
+
+enum : int {
+  ACC_COMP = LF2_DEPOSIT_FP32,
+  ACC_FIXED = LF2_DEPOSIT_FIXED64,
+  ACC_PLAIN = LF2_DEPOSIT_FP32_PLAIN
+};
+
+// ------------------------------------------------------------ accumulation
+// Fixed point: each 64-bit vertex sum is kept as two 32-bit partial sums,
+// lo = sum(q & 0xffff) and hi = sum(q >> 16) (arithmetic shift), so that every
+// update is a native 32-bit shared-memory reduction; the sum is
+// lo + hi * 2^16, hi read as unsigned (scalar, q >= 0) or as signed (momentum
+// and stress).  Neither partial sum may wrap: per particle and vertex
+// |q| <= 2^32 * M with M = 1 for a global mass and M = 64 with per-particle
+// masses (relative mass < 64), so the split is exact for bricks of at most
+// split_max particles; larger bricks use 64-bit shared atomics.
+template <bool SIGNED>
+__host__ __device__ inline int split_max(bool has_mass)
+{
+  return SIGNED ? (has_mass ? 511 : 32767) : (has_mass ? 1023 : 65535);
+}
+
+// A tile of N vertices per component in shared memory: component j occupies
+// words [2 j N, 2 (j + 1) N) (two 32-bit words per vertex), or [j N, (j+1) N)
+// in the plain mode.
+template <int N>
+struct TileRef {
+  unsigned char* smem;
+  bool split;
+};
+
+template <int N>
+__device__ __forceinline__ void add_fixed(TileRef<N> tr, int j, int t, long long q)
+{
+  if (tr.split) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(tr.smem) + (size_t)j * 2 * N;
+    atomicAdd(&w[t], (uint32_t)((unsigned long long)q & 0xffffu));
+    atomicAdd(&w[N + t], (uint32_t)(q >> 16));
+  } else {
+    atomicAdd(reinterpret_cast<unsigned long long*>(tr.smem) + (size_t)j * N + t,
+              (unsigned long long)q);
+  }
+}
+
+// Compensated FP32 add: the atomic returns the value it replaced, so the
+// rounding error of the stored sum fl(old + w) is recovered exactly by
+// Knuth's TwoSum and added to the second word.
+__device__ __forceinline__ void add_comp(float* hi, float* lo, float w)
+{
+  const float old = atomicAdd(hi, w);
+  const float s = __fadd_rn(old, w);
+  const float bb = __fsub_rn(s, old);
+  const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bb)), __fsub_rn(w, bb));
+  atomicAdd(lo, err);
+}
+
+// (s, c) += (h, l): TwoSum of s and h, the error and l carried in c.
+__device__ __forceinline__ void comp_acc(float& s, float& c, float h, float l)
+{
+  const float t = __fadd_rn(s, h);
+  const float bb = __fsub_rn(t, s);
+  const float err = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bb)), __fsub_rn(h, bb));
+  s = t;
+  c = __fadd_rn(c, __fadd_rn(err, l));
+}
+
+template <int ACC, int N>
+__device__ __forceinline__ void add_float(TileRef<N> tr, int j, int t, float w)
+{
+  float* f = reinterpret_cast<float*>(tr.smem);
+  if (ACC == ACC_PLAIN) {
+    atomicAdd(&f[(size_t)j * N + t], w);
+  } else {
+    add_comp(&f[(size_t)j * 2 * N + t], &f[(size_t)j * 2 * N + N + t], w);
+  }
+}
+
+// Integer vertex sum of component j.
+template <bool SIGNED, int N>
+__device__ __forceinline__ long long tile_fixed(const TileRef<N>& tr, int j, int t)
+{
+  if (tr.split) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(tr.smem) + (size_t)j * 2 * N;
+    const long long hi = SIGNED ? (long long)(int32_t)w[N + t] : (long long)w[N + t];
+    return (long long)w[t] + hi * 65536ll;
+  }
+  return (long long)reinterpret_cast<const unsigned long long*>(tr.smem)[(size_t)j * N + t];
+}
+
+// ----------------------------------------------------- fixed-point weights
+// 1-D weight in units of 2^-31 (lf2o_fixed_weight in the oracle).
+__device__ __forceinline__ uint32_t weight_q(float w) { return __float2uint_rn(w * 2147483648.0f); }
+
+// Velocity in units of 2^-31 V (V = 2^e > |v|): |v| 2^(31-e) is exact in FP32
+// and below 2^31; rounded to the nearest integer.
+__device__ __forceinline__ uint32_t vel_q(float v, float vscale)
+{
+  return __float2uint_rn(fabsf(v) * vscale);
+}
+
+// Product of two such velocities in units of 2^-31 V^2, rounded.
+__device__ __forceinline__ uint64_t vel2_q(uint32_t a, uint32_t b)
+{
+  return ((uint64_t)a * (uint64_t)b + (1ull << 30)) >> 31;
+}
+
+// w (2^-32 units) times a factor in 2^-31 units, rounded to 2^-32 units.
+__device__ __forceinline__ uint64_t mul31(uint64_t w, uint64_t f) { return (w * f + (1ull << 30)) >> 31; }
+
+// Per-particle relative mass m / m_unit in units of 2^-24 (range-checked).
+__device__ __forceinline__ uint64_t mass_q(float m, float inv_unit, uint32_t* flags)
+{
+  const float mr = __fmul_rn(m, inv_unit);
+  if (!(mr >= 0.0f && mr < 64.0f)) set_flag(flags, ERR_MASS_RANGE);
+  return (uint64_t)__float2uint_rn(fminf(fmaxf(mr, 0.0f), 63.0f) * 16777216.0f);
+}
+
+__device__ __forceinline__ long long apply_mass_sign(uint64_t q, bool has_mass, uint64_t mq, bool neg)
+{
+  if (has_mass) q = (q * mq + (1ull << 23)) >> 24;
+  return neg ? -(long long)q : (long long)q;
+}
+
+// Scale 2^(31-e) as an FP32 (e within [-96, 128]).
+__device__ __forceinline__ float vel_scale(int e) { return ldexpf(1.0f, 31 - e); }
+
+// Exponent e of V = 2^e, the smallest power of two above the largest |v_i|
+// (bits of a non-negative float; 0 when every velocity is 0), at least
+// 2^-96 so that 2^(31-e) stays a finite FP32.
+__host__ __device__ inline int vexp_of(uint32_t bits)
+{
+  if (bits == 0u) return 0;
+  const int e = (int)((bits >> 23) & 0xffu) - 126;
+  return e < -96 ? -96 : e;
+}
+
+}  // namespace lf2

@@ -24,8 +24,20 @@
 // of the up to 26 neighbour bricks that reach it, in a fixed order.  This is
 // the periodic fold of both halos that the reference's *_comm functions do;
 // no global atomics are used and no field has to be cleared first.
+//
+// The three deposit modes of lf2_deposit.cu apply here too.  The plain FP32
+// mode keeps one word per vertex and writes the brick's own boundary
+// vertices to the field as partial sums, which the fix-up completes.  The
+// compensated FP32 and the fixed-point modes keep two words per vertex (the
+// hi/lo pair, or the split integer sum) and write every tile vertex that
+// another brick can reach -- the own boundary vertices (tile coordinate 1 or
+// e) and the outer layer (0 or e+1), a shell two vertices thick -- to the
+// store; the fix-up then sums the own and the neighbours' values in one
+// fixed order (exact integers, or a compensated FP32 sum) and writes the
+// boundary vertices once.
 #include <cuda_runtime.h>
 
+#include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
 namespace lf2 {
@@ -54,6 +66,26 @@ __host__ __device__ inline int outer_index(int u0, int u1, int u2)
 
 static_assert(2 * FT * FT + 2 * (FT - 2) * FT + 2 * (FT - 2) * (FT - 2) == FOUTER,
               "outer slab sizes");
+
+// The shell two vertices thick of the compensated and fixed-point modes:
+// tile vertices with a coordinate in {0, 1, e, e+1}.  Canonical coordinates
+// map e to FT - 2 and e + 1 to FT - 1 (so bricks with e < BRICK share one
+// layout); the shell is the two z slabs pairs (4 FT^2), then the y slab pairs
+// between them (4 (FT-4) FT), then the x slab pairs between those
+// (4 (FT-4)^2): 3088 slots for BRICK = 16.
+constexpr int FSHELL = FT3 - (FT - 4) * (FT - 4) * (FT - 4);
+static_assert(4 * FT * FT + 4 * (FT - 4) * FT + 4 * (FT - 4) * (FT - 4) == FSHELL, "thick slabs");
+
+__host__ __device__ inline int canon(int t, int e) { return t == e + 1 ? FT - 1 : (t == e ? FT - 2 : t); }
+__host__ __device__ inline bool in_thick(int u) { return u < 2 || u >= FT - 2; }
+__host__ __device__ inline int thick_slot(int u) { return u < 2 ? u : u - (FT - 4); }
+
+__host__ __device__ inline int thick_index(int u0, int u1, int u2)
+{
+  if (in_thick(u2)) return thick_slot(u2) * FT * FT + u1 * FT + u0;
+  if (in_thick(u1)) return 4 * FT * FT + (thick_slot(u1) * (FT - 4) + (u2 - 2)) * FT + u0;
+  return 4 * FT * FT + 4 * (FT - 4) * FT + (thick_slot(u0) * (FT - 4) + (u2 - 2)) * (FT - 4) + (u1 - 2);
+}
 
 // Threads per CTA of a tile pass.  Measured at 512^3: 512 (more warps on the
 // same tiles) gave 5.39 ms against 5.11 ms for 256; the tile passes are bound
@@ -284,6 +316,342 @@ __global__ void __launch_bounds__(256, 4)
   }
 }
 
+// Compensated FP32 and fixed-point tile pass: the same weights and vertices
+// as k_deposit_full, two words per vertex (140 KB for three components, one
+// CTA per SM with 512 threads), and every vertex another brick can reach goes
+// to the thick-shell store.
+constexpr int FULL2_THREADS = 512;
+
+template <int PASS, int ACC>
+__global__ void __launch_bounds__(FULL2_THREADS)
+    k_deposit_full2(StoreView v, DepositParams dp, float* __restrict__ out,
+                    uint64_t* __restrict__ store, const uint32_t* __restrict__ vmax_bits,
+                    uint32_t* flags)
+{
+  constexpr int CT = FullPass<PASS>::total;
+  constexpr bool FIXED = ACC == ACC_FIXED;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+
+  const Geom& g = v.g;
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int e[3] = {brick_extent(g.n[0], bx), brick_extent(g.n[1], by),
+                    brick_extent(g.n[2], bz)};
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+  const int64_t base = v.seg_start[b];
+  const int cnt = LF2_BRICK_COUNT(v, b);
+  TileRef<FT3> tr{smem_raw, FIXED && cnt <= split_max<true>(dp.has_mass != 0)};
+  int vexp = 0;
+  if (FIXED) vexp = vexp_of(*vmax_bits);
+  const float vscale = vel_scale(vexp);
+  const float conv = FIXED ? ldexpf(dp.fixed_scale, PASS == 0 ? vexp : 2 * vexp) : 0.0f;
+  if (FIXED && threadIdx.x == 0 && b == 0 && !(conv > 0.0f && conv <= 3.402823466e38f))
+    set_flag(flags, ERR_FIXED_OVERFLOW);
+
+  {
+    uint32_t* zw = reinterpret_cast<uint32_t*>(smem_raw);
+    for (int t = threadIdx.x; t < 3 * 2 * FT3; t += blockDim.x) zw[t] = 0u;
+  }
+  __syncthreads();
+
+  constexpr int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const int64_t p = base + i;
+    int x, y, z;
+    unpack_key(g, v.a.key[p], x, y, z);
+    const float o[3] = {v.a.ox[p], v.a.oy[p], v.a.oz[p]};
+    const float vel[3] = {v.a.vx[p], v.a.vy[p], v.a.vz[p]};
+    const int l[3] = {x - x0, y - y0, z - z0};
+    int ls[3], lt[3], gd[3];
+    float s[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      s[d] = __fsub_rn(o[d], 0.5f);
+      gd[d] = s[d] >= 0.0f;
+      ls[d] = l[d] + 1;
+      lt[d] = l[d] + gd[d];
+    }
+    if (FIXED) {
+      const bool hm = dp.has_mass != 0;
+      const uint64_t mq = hm ? mass_q(v.a.mass[p], dp.inv_unit, flags) : 0;
+      // vertex weights sq and staggered weights tq in units of 2^-31
+      uint32_t sq[3][2], tq[3][2], vq[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const uint32_t u = weight_q(o[d]);
+        sq[d][0] = (1u << 31) - u;
+        sq[d][1] = u;
+        const uint32_t us = weight_q(fabsf(s[d]));
+        tq[d][0] = gd[d] ? (1u << 31) - us : us;
+        tq[d][1] = gd[d] ? us : (1u << 31) - us;
+        vq[d] = vel_q(vel[d], vscale);
+      }
+      if (PASS == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const bool neg = vel[c] < 0.0f;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+            const uint64_t w = fixed_corner(c == 0 ? tq[0][b0] : sq[0][b0],
+                                            c == 1 ? tq[1][b1] : sq[1][b1],
+                                            c == 2 ? tq[2][b2] : sq[2][b2]);
+            const int t = tile_at((c == 0 ? lt[0] : ls[0]) + b0, (c == 1 ? lt[1] : ls[1]) + b1,
+                                  (c == 2 ? lt[2] : ls[2]) + b2);
+            add_fixed(tr, c, t, apply_mass_sign(mul31(w, vq[c]), hm, mq, neg));
+          }
+        }
+      } else if (PASS == 1) {
+        uint64_t v2[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) v2[d] = vel2_q(vq[d], vq[d]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+          const uint64_t w = fixed_corner(sq[0][b0], sq[1][b1], sq[2][b2]);
+          const int t = tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2);
+#pragma unroll
+          for (int d = 0; d < 3; d++) add_fixed(tr, d, t, apply_mass_sign(mul31(w, v2[d]), hm, mq, false));
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          const uint64_t vv = vel2_q(vq[pa[q]], vq[pb[q]]);
+          const bool neg = (vel[pa[q]] < 0.0f) != (vel[pb[q]] < 0.0f);
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+            uint32_t w[3];
+            int t[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              const bool st = d == pa[q] || d == pb[q];
+              w[d] = st ? tq[d][bb[d]] : sq[d][bb[d]];
+              t[d] = (st ? lt[d] : ls[d]) + bb[d];
+            }
+            add_fixed(tr, q, tile_at(t[0], t[1], t[2]),
+                      apply_mass_sign(mul31(fixed_corner(w[0], w[1], w[2]), vv), hm, mq, neg));
+          }
+        }
+      }
+      continue;
+    }
+    // compensated FP32: the arithmetic of k_deposit_full
+    const float mf = dp.has_mass ? __fmul_rn(v.a.mass[p], dp.inv_vol) : dp.mf;
+    float sw[3][2], tw[3][2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      sw[d][1] = o[d];
+      sw[d][0] = __fsub_rn(1.0f, o[d]);
+      if (gd[d]) {
+        tw[d][1] = s[d];
+        tw[d][0] = __fsub_rn(1.0f, s[d]);
+      } else {
+        tw[d][0] = -s[d];
+        tw[d][1] = __fsub_rn(1.0f, tw[d][0]);
+      }
+    }
+    if (PASS == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float mv = __fmul_rn(mf, vel[c]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+          const float w0 = c == 0 ? tw[0][b0] : sw[0][b0];
+          const float w1 = c == 1 ? tw[1][b1] : sw[1][b1];
+          const float w2 = c == 2 ? tw[2][b2] : sw[2][b2];
+          const int t = tile_at((c == 0 ? lt[0] : ls[0]) + b0, (c == 1 ? lt[1] : ls[1]) + b1,
+                                (c == 2 ? lt[2] : ls[2]) + b2);
+          add_float<ACC>(tr, c, t, __fmul_rn(__fmul_rn(__fmul_rn(mv, w0), w1), w2));
+        }
+      }
+    } else if (PASS == 1) {
+#pragma unroll
+      for (int i2 = 0; i2 < 3; i2++) {
+        const float m2 = __fmul_rn(__fmul_rn(mf, vel[i2]), vel[i2]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+          add_float<ACC>(tr, i2, tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2),
+                         __fmul_rn(__fmul_rn(__fmul_rn(m2, sw[0][b0]), sw[1][b1]), sw[2][b2]));
+        }
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const float mm = __fmul_rn(__fmul_rn(mf, vel[pa[q]]), vel[pb[q]]);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+          float w[3];
+          int t[3];
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            const bool st = d == pa[q] || d == pb[q];
+            w[d] = st ? tw[d][bb[d]] : sw[d][bb[d]];
+            t[d] = (st ? lt[d] : ls[d]) + bb[d];
+          }
+          add_float<ACC>(tr, q, tile_at(t[0], t[1], t[2]),
+                         __fmul_rn(__fmul_rn(__fmul_rn(mm, w[0]), w[1]), w[2]));
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // Flush: private vertices (every tile coordinate in [2, e-1]) to the field,
+  // the thick shell to the store.
+  uint64_t* st = store + (size_t)b * CT * FSHELL;
+  const float* facc = reinterpret_cast<const float*>(smem_raw);
+  for (int t = threadIdx.x; t < FT3; t += blockDim.x) {
+    const int t0 = t % FT, t1 = (t / FT) % FT, t2 = t / (FT * FT);
+    if (t0 > e[0] + 1 || t1 > e[1] + 1 || t2 > e[2] + 1) continue;
+    const bool priv = t0 >= 2 && t0 < e[0] && t1 >= 2 && t1 < e[1] && t2 >= 2 && t2 < e[2];
+    const int si = priv ? 0 : thick_index(canon(t0, e[0]), canon(t1, e[1]), canon(t2, e[2]));
+    const int64_t site = priv ? site_index(g, x0 + t0 - 1, y0 + t1 - 1, z0 + t2 - 1) : 0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const int c = FullPass<PASS>::comp(j);
+      if (FIXED) {
+        const long long q = tile_fixed<true>(tr, j, t);
+        if (priv) out[(size_t)c * g.nsites + site] = __fmul_rn(__ll2float_rn(q), conv);
+        else st[(size_t)c * FSHELL + si] = (uint64_t)q;
+      } else {
+        const float hi = facc[(size_t)j * 2 * FT3 + t], lo = facc[(size_t)j * 2 * FT3 + FT3 + t];
+        if (priv) out[(size_t)c * g.nsites + site] = __fadd_rn(hi, lo);
+        else reinterpret_cast<float2*>(st)[(size_t)c * FSHELL + si] = make_float2(hi, lo);
+      }
+    }
+  }
+}
+
+// Fix-up of the compensated and fixed-point modes: every owned boundary
+// vertex is the sum of the thick-shell values of its own brick and of the up
+// to 26 neighbours that reach it, z outermost, -1 before 0 before +1 (own
+// brick included at 0, 0, 0).  Same enumeration of the boundary vertices as
+// k_fixup_full.
+template <int C, int ACC>
+__global__ void __launch_bounds__(256, 4)
+    k_fixup_full2(Geom g, const uint64_t* __restrict__ store, float fixed_scale,
+                  const uint32_t* __restrict__ vmax_bits, float* __restrict__ out)
+{
+  const int64_t b = blockIdx.x;
+  int bc[3];
+  brick_coords(g, b, bc[0], bc[1], bc[2]);
+  const int e[3] = {brick_extent(g.n[0], bc[0]), brick_extent(g.n[1], bc[1]),
+                    brick_extent(g.n[2], bc[2])};
+  const int nzp = e[2] > 1 ? 2 : 1, nyp = e[1] > 1 ? 2 : 1, nxp = e[0] > 1 ? 2 : 1;
+  const int iz = e[2] > 2 ? e[2] - 2 : 0, iy = e[1] > 2 ? e[1] - 2 : 0;
+  const int nzf = nzp * e[0] * e[1];
+  const int nyf = iz * nyp * e[0];
+  const int total = nzf + nyf + iz * iy * nxp;
+  int nbc[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    nbc[d][0] = bc[d];
+    nbc[d][1] = wrap_add(bc[d], -1, g.nb[d]);
+    nbc[d][2] = wrap_add(bc[d], 1, g.nb[d]);
+  }
+  float conv = 0.0f;
+  if (ACC == ACC_FIXED) {
+    const int vexp = vexp_of(*vmax_bits);
+    conv = ldexpf(fixed_scale, C == 3 ? vexp : 2 * vexp);
+  }
+  for (int f = threadIdx.x; f < total; f += blockDim.x) {
+    int q[3];
+    if (f < nzf) {
+      q[0] = f % e[0];
+      q[1] = (f / e[0]) % e[1];
+      q[2] = f / (e[0] * e[1]) ? e[2] - 1 : 0;
+    } else if (f < nzf + nyf) {
+      const int r = f - nzf;
+      q[0] = r % e[0];
+      q[1] = (r / e[0]) % nyp ? e[1] - 1 : 0;
+      q[2] = 1 + r / (e[0] * nyp);
+    } else {
+      const int r = f - nzf - nyf;
+      q[1] = 1 + r % iy;
+      q[0] = (r / iy) % nxp ? e[0] - 1 : 0;
+      q[2] = 1 + r / (iy * nxp);
+    }
+    const bool lo[3] = {q[0] == 0, q[1] == 0, q[2] == 0};
+    const bool hi[3] = {q[0] == e[0] - 1, q[1] == e[1] - 1, q[2] == e[2] - 1};
+    const int64_t site = site_index(g, bc[0] * BRICK + q[0], bc[1] * BRICK + q[1],
+                                    bc[2] * BRICK + q[2]);
+    long long qs[C];
+    float fs[C], fc[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) qs[c] = 0, fs[c] = 0.0f, fc[c] = 0.0f;
+#pragma unroll
+    for (int dz = -1; dz <= 1; dz++) {
+      if ((dz < 0 && !lo[2]) || (dz > 0 && !hi[2])) continue;
+#pragma unroll
+      for (int dy = -1; dy <= 1; dy++) {
+        if ((dy < 0 && !lo[1]) || (dy > 0 && !hi[1])) continue;
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+          if ((dx < 0 && !lo[0]) || (dx > 0 && !hi[0])) continue;
+          const int64_t nb = (int64_t)nbc[0][dx < 0 ? 1 : (dx > 0 ? 2 : 0)] +
+                             (int64_t)g.nb[0] * ((int64_t)nbc[1][dy < 0 ? 1 : (dy > 0 ? 2 : 0)] +
+                                                 (int64_t)g.nb[1] * nbc[2][dz < 0 ? 1 : (dz > 0 ? 2 : 0)]);
+          const int si = thick_index(dx < 0 ? FT - 1 : (dx > 0 ? 0 : canon(q[0] + 1, e[0])),
+                                     dy < 0 ? FT - 1 : (dy > 0 ? 0 : canon(q[1] + 1, e[1])),
+                                     dz < 0 ? FT - 1 : (dz > 0 ? 0 : canon(q[2] + 1, e[2])));
+          const uint64_t* sp = store + (size_t)nb * C * FSHELL + si;
+#pragma unroll
+          for (int c = 0; c < C; c++) {
+            if (ACC == ACC_FIXED) {
+              qs[c] += (long long)sp[(size_t)c * FSHELL];
+            } else {
+              const float2 hl = reinterpret_cast<const float2*>(sp)[(size_t)c * FSHELL];
+              comp_acc(fs[c], fc[c], hl.x, hl.y);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < C; c++)
+      out[c * g.nsites + site] = ACC == ACC_FIXED ? __fmul_rn(__ll2float_rn(qs[c]), conv)
+                                                  : __fadd_rn(fs[c], fc[c]);
+  }
+}
+
+template <int PASS, int ACC>
+cudaError_t tile_pass2(lf2_ctx* c, float* out, const DepositParams& dp)
+{
+  const size_t smem = (size_t)3 * 2 * FT3 * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_deposit_full2<PASS, ACC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  c->launches += 1;
+  k_deposit_full2<PASS, ACC><<<(unsigned)c->g.nbricks, FULL2_THREADS, smem, c->stream>>>(
+      view(c), dp, out, c->spill, c->vmax_bits, c->flags);
+  return cudaGetLastError();
+}
+
+template <int ACC>
+cudaError_t run2(lf2_ctx* c, int kind, float* out, const DepositParams& dp, int stage)
+{
+  const unsigned nb = (unsigned)c->g.nbricks;
+  if (stage == 0) {
+    cudaError_t e = cudaSuccess;
+    if (ACC == ACC_FIXED) e = launch_vmax(c);
+    if (e != cudaSuccess) return e;
+    if (kind == 3) return tile_pass2<0, ACC>(c, out, dp);
+    e = tile_pass2<1, ACC>(c, out, dp);
+    return e != cudaSuccess ? e : tile_pass2<2, ACC>(c, out, dp);
+  }
+  c->launches += 1;
+  if (kind == 3)
+    k_fixup_full2<3, ACC><<<nb, 256, 0, c->stream>>>(c->g, c->spill, dp.fixed_scale, c->vmax_bits, out);
+  else
+    k_fixup_full2<6, ACC><<<nb, 256, 0, c->stream>>>(c->g, c->spill, dp.fixed_scale, c->vmax_bits, out);
+  return cudaGetLastError();
+}
+
 template <int PASS>
 cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
 {
@@ -299,15 +667,18 @@ cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
 
 }  // namespace
 
+// Store slots (8 bytes each) a full-CIC deposit of `comps` components needs
+// in the context's deposit mode.
+size_t deposit_full_spill_slots(const lf2_ctx* c, int comps)
+{
+  return (size_t)c->g.nbricks * (size_t)comps * (c->mode == LF2_DEPOSIT_FP32_PLAIN ? SHELL : FSHELL);
+}
+
 cudaError_t launch_deposit_full(lf2_ctx* c, int kind, float* out, int stage)
 {
-  DepositParams dp;
-  const double vol = c->res * c->res * c->res;
-  dp.inv_vol = (float)(1.0 / vol);
-  dp.mf = (float)(c->gmass / vol);
-  dp.fixed_scale = 0.0f;
-  dp.inv_unit = 0.0f;
-  dp.has_mass = c->has_mass ? 1 : 0;
+  const DepositParams dp = deposit_params(c);
+  if (c->mode == LF2_DEPOSIT_FIXED64) return run2<ACC_FIXED>(c, kind, out, dp, stage);
+  if (c->mode == LF2_DEPOSIT_FP32) return run2<ACC_COMP>(c, kind, out, dp, stage);
   const unsigned nb = (unsigned)c->g.nbricks;
   float* outer = reinterpret_cast<float*>(c->spill);
   if (stage == 0) {

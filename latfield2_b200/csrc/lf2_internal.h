@@ -92,6 +92,7 @@ struct lf2_ctx {
   double* brick_sums = nullptr;      // [nbricks * 5]
   double* stats = nullptr;           // [8] device
   uint64_t* spill = nullptr;         // deposit shell store (8-byte slots)
+  uint32_t* vmax_bits = nullptr;     // device: largest |v_i| (float bits), fixed-point deposits
   float* stencil_partial = nullptr;  // per-CTA partial sums of the stencil weight gradient
   size_t spill_slots = 0;
   double* h_stats = nullptr;         // pinned [8]
@@ -103,6 +104,8 @@ struct lf2_ctx {
   int move_kernel = 0;               // 0 auto, 1 per-brick k_move, 2 pipelined
   int last_move_kernel = 0;          // kernel of the last kick-drift pass (1 or 2)
   int* work = nullptr;               // device brick counter
+  int64_t wait_cycles = 0;           // limit of its bounded waits (0: about 2 s)
+  int wait_stall = 0;                // consumers first wait on a barrier nothing completes
   const float* tmap_src = nullptr;   // field the cached tensor map describes
   alignas(64) unsigned char tmap_bytes[128];
 
@@ -165,6 +168,9 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
 // lf2_deposit.cu
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
 cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
+// largest |v_i| of the store into c->vmax_bits (fixed-point momentum/stress)
+cudaError_t launch_vmax(lf2_ctx* c);
+DepositParams deposit_params(const lf2_ctx* c);
 
 // lf2_exchange.cu (slab decomposition): particles with cell z outside
 // [zlo, zhi] counted / moved out of the store; new particles into the mover
@@ -183,6 +189,8 @@ void fft_release(lf2_ctx* c);
 // lf2_deposit_full.cu: kind 3 vector CIC, kind 4 VecVec CIC; stage 0 tile
 // pass (k_deposit_full), stage 1 boundary fix-up (k_fixup_full)
 cudaError_t launch_deposit_full(lf2_ctx* c, int kind, float* out, int stage);
+size_t deposit_full_spill_slots(const lf2_ctx* c, int comps);
+size_t deposit_spill_slots(const lf2_ctx* c, int comps);
 
 // lf2_pm.cu (differentiable chain; op codes documented there)
 cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,

@@ -30,7 +30,12 @@
 //     the stayers inside a brick therefore follows the warps' timing.
 //
 // Every mbarrier wait is bounded (LF2_FLAG_TIMEOUT, then the warp returns).
-// No cluster multicast is used.
+// A producer that gives up, or that has posted its last copy, first waits
+// (with the full limit) for every bulk and tensor copy it has issued to land,
+// so the CTA never exits with a copy still writing its shared memory.  The
+// limit of the other waits is a launch parameter (lf2_set_wait_limit); for
+// the tests of this path the consumers can be made to wait on a barrier that
+// nothing completes.  No cluster multicast is used.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -142,15 +147,16 @@ __device__ __forceinline__ bool mbar_try_hint(uint64_t* bar, uint32_t parity, ui
 }
 
 // Wait for the phase with the given parity; false (and the timeout flag)
-// when it has not completed within WAIT_CYCLES.  The waiting thread is
+// when it has not completed within `limit` cycles.  The waiting thread is
 // suspended between polls (measured: 2% faster than a plain poll loop).
-__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* flags)
+__device__ __noinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t* flags,
+                                       long long limit)
 {
   if (mbar_try(bar, parity)) return true;
   const long long t0 = clock64();
   for (;;) {
     if (mbar_try_hint(bar, parity, 20000u)) return true;
-    if (clock64() - t0 > WAIT_CYCLES) {
+    if (clock64() - t0 > limit) {
       set_flag(flags, ERR_TIMEOUT);
       return false;
     }
@@ -216,10 +222,11 @@ __device__ __forceinline__ ChunkView chunk_view(unsigned char* p, bool has_m)
 
 // Bounded wait by lane 0 of the calling warp; the outcome is broadcast so the
 // warp stays together, and every lane then acquires the completed phase.
-__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, uint32_t* flags, int lane)
+__device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, uint32_t* flags, int lane,
+                                          long long limit)
 {
   int ok = 1;
-  if (lane == 0) ok = mbar_wait(bar, parity, flags);
+  if (lane == 0) ok = mbar_wait(bar, parity, flags, limit);
   ok = __shfl_sync(0xffffffffu, ok, 0);
   if (ok) mbar_try(bar, parity);
   return ok != 0;
@@ -229,13 +236,14 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     k_move_pipe(const __grid_constant__ CUtensorMap tmF, StoreView v, const float* __restrict__ F,
                 MoveParams mp, PartArrays mov, unsigned long long* mov_count,
                 float* __restrict__ brick_maxv2, uint32_t* flags, int* work, int nst,
-                int stage_bytes)
+                int stage_bytes, long long wait_limit, int stall)
 {
   extern __shared__ unsigned char dyn[];
   // tma_f: tile copy landed (or the end of the bricks); full_f: tile
   // patched and ready for the consumers; empty_f: all consumer warps are
   // done with the brick; full_p / empty_p: chunk ring.
   __shared__ uint64_t full_f[2], tma_f[2], empty_f[2], full_p[MAX_STAGES], empty_p[MAX_STAGES];
+  __shared__ uint64_t never;  // completed by nothing: the consumers' stall of the timeout tests
   __shared__ Job job[2];
   __shared__ int s_cursor[2];     // stayers written back so far (per tile buffer)
   __shared__ int s_done[2];       // consumer warps finished with the brick
@@ -256,6 +264,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       mbar_init(&empty_f[s], 1);
     }
     for (int s = 0; s < nst; s++) mbar_init(&full_p[s], 1), mbar_init(&empty_p[s], PC_WARPS);
+    mbar_init(&never, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -270,6 +279,17 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     int pps = 0;                // next chunk buffer
     uint32_t ppar = 0;          // parity of the current round through the ring
     bool wrapped = false;       // every buffer has been used once
+    // the phase (parity) the last copy into each chunk buffer and tile buffer
+    // completes, to wait for every copy in flight before the thread exits
+    bool st_busy[MAX_STAGES], tl_busy[2] = {false, false};
+    uint32_t st_par[MAX_STAGES], tl_par[2] = {0u, 0u};
+    for (int s = 0; s < MAX_STAGES; s++) st_busy[s] = false, st_par[s] = 0u;
+    auto drain = [&]() {
+      for (int s = 0; s < nst; s++)
+        if (st_busy[s]) mbar_wait(&full_p[s], st_par[s], flags, WAIT_CYCLES);
+      for (int f = 0; f < NF; f++)
+        if (tl_busy[f]) mbar_wait(&tma_f[f], tl_par[f], flags, WAIT_CYCLES);
+    };
     // q0: next brick with its count and segment start loaded; q1: the index
     // after it
     long long q0 = atomicAdd(work, 1);
@@ -297,6 +317,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     auto post = [&](long long b, int cnt, long long base) {
       const int fs = (int)(fk % NF);
       job[fs].b = b;
+      tl_par[fs] = (uint32_t)((fk / NF) & 1);
+      tl_busy[fs] = b >= 0;
       fk++;
       if (b < 0) {
         mbar_arrive(&tma_f[fs]);  // the patch warp passes it on to the consumers
@@ -335,8 +357,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
               post(nb_, ncnt, nbase);
               nposted = true;
             }
-            if (clock64() - t0 > WAIT_CYCLES) {
+            if (clock64() - t0 > wait_limit) {
               set_flag(flags, ERR_TIMEOUT);
+              drain();
               return;
             }
             __nanosleep(64);
@@ -351,6 +374,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
         const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
         const long long p = cbase + c0;
+        st_busy[ps] = true;
+        st_par[ps] = ppar;
         mbar_arrive_tx(&full_p[ps], bytes);
         bulk_g2s(cv.key, v.a.key + p, n4 * 4u, &full_p[ps]);
         bulk_g2s(cv.ox, v.a.ox + p, n4 * 4u, &full_p[ps]);
@@ -369,13 +394,17 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       }
       if (!nposted) {
         const int fs = (int)(fk % NF);
-        if (fk >= NF && !mbar_wait(&empty_f[fs], (uint32_t)(((fk / NF) - 1) & 1), flags)) return;
+        if (fk >= NF && !mbar_wait(&empty_f[fs], (uint32_t)(((fk / NF) - 1) & 1), flags, wait_limit)) {
+          drain();
+          return;
+        }
         post(nb_, ncnt, nbase);
       }
       cb = nb_, ccnt = ncnt, cbase = nbase;
       if (cb >= 0) next_brick(nb_, ncnt, nbase);
       nposted = false;
     }
+    drain();
     return;
   }
 
@@ -388,7 +417,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     long long fk = 0;
     for (;;) {
       const int fs = (int)(fk % NF);
-      if (!warp_wait(&tma_f[fs], (uint32_t)((fk / NF) & 1), flags, lane)) return;
+      if (!warp_wait(&tma_f[fs], (uint32_t)((fk / NF) & 1), flags, lane, wait_limit)) return;
       const Job jb = job[fs];
       if (jb.b < 0) {
         if (lane == 0) mbar_arrive(&full_f[fs]);
@@ -458,9 +487,10 @@ __global__ void __launch_bounds__(P_THREADS, 1)
   long long fk = 0;
   int cps = 0;          // chunk buffer of the next chunk
   uint32_t cpar = 0;    // parity of its full barrier's phase
+  if (stall && !warp_wait(&never, 0u, flags, lane, wait_limit)) return;
   for (;;) {
     const int fs = (int)(fk % NF);
-    if (!warp_wait(&full_f[fs], (uint32_t)((fk / NF) & 1), flags, lane)) return;
+    if (!warp_wait(&full_f[fs], (uint32_t)((fk / NF) & 1), flags, lane, wait_limit)) return;
     const Job jb = job[fs];
     if (jb.b < 0) return;
     const int64_t b = jb.b;
@@ -474,7 +504,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     float maxv2 = 0.0f;
     for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
       const int ps = cps;
-      if (!warp_wait(&full_p[ps], cpar, flags, lane)) return;
+      if (!warp_wait(&full_p[ps], cpar, flags, lane, wait_limit)) return;
       if (++cps == nst) {
         cps = 0;
         cpar ^= 1u;
@@ -697,9 +727,9 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp)
   e = cudaMemsetAsync(c->work, 0, sizeof(int), c->stream);
   if (e != cudaSuccess) return e;
   c->launches += 1;
-  k_move_pipe<<<c->num_sms, P_THREADS, smem, c->stream>>>(*map, view(c), F, mp, c->mov, c->mov_count,
-                                                          c->brick_maxv2, c->flags, c->work, nst,
-                                                          (int)sb);
+  k_move_pipe<<<c->num_sms, P_THREADS, smem, c->stream>>>(
+      *map, view(c), F, mp, c->mov, c->mov_count, c->brick_maxv2, c->flags, c->work, nst, (int)sb,
+      c->wait_cycles > 0 ? (long long)c->wait_cycles : WAIT_CYCLES, c->wait_stall);
   return cudaGetLastError();
 }
 

@@ -222,3 +222,165 @@ void lf2o_rebin_lists(int64_t ncells, int64_t np, const int64_t* cs_old,
   free(head);
   free(next);
 }
+
+/* ------------------------------------------------------------------------
+ * Fixed-point momentum and stress deposits (device arithmetic restated).
+ * Velocities are quantised against V = 2^e, the smallest power of two above
+ * every |v_i| (lf2o_vexp); contributions are signed integers in units of
+ * 2^-32 of a unit mass times V (momentum) or V^2 (stress), each rounded
+ * once, so the sums are the device's bit for bit.  The vertex placement
+ * follows the projections of the reference:
+ *   kind 1  vectorProjectionCICNGP (projections.hpp:501-544)
+ *   kind 2  symtensorProjectionCICNGP (:786-843)
+ *   kind 3  vectorProjectionCIC (:1052-1190, staggered weights via gridChoice)
+ *   kind 4  VecVecProjectionCIC (:1355-1620)
+ */
+int lf2o_vexp(int64_t np, const float* vel)
+{
+  uint32_t m = 0;
+  for (int64_t i = 0; i < 3 * np; i++) {
+    float a = fabsf(vel[i]);
+    uint32_t b;
+    memcpy(&b, &a, 4);
+    if (b > m) m = b;
+  }
+  if (m == 0) return 0;
+  int e = (int)((m >> 23) & 0xffu) - 126;
+  return e < -96 ? -96 : e;
+}
+
+static inline uint32_t wq(float w) { return (uint32_t)lrintf(w * 2147483648.0f); }
+
+static inline uint64_t corner3(uint32_t a, uint32_t b, uint32_t c)
+{
+  const unsigned __int128 prod = (unsigned __int128)((uint64_t)a * (uint64_t)b) * c;
+  return (uint64_t)((prod + ((unsigned __int128)1 << 60)) >> 61);
+}
+
+static inline uint64_t mul31(uint64_t w, uint64_t f) { return (w * f + (1ull << 30)) >> 31; }
+
+static inline int64_t signed_q(uint64_t q, const float* mrel, int64_t p, int neg)
+{
+  if (mrel) {
+    float mr = mrel[p];
+    mr = mr < 0.0f ? 0.0f : (mr > 63.0f ? 63.0f : mr);
+    const uint64_t mq = (uint64_t)lrintf(mr * 16777216.0f);
+    q = (q * mq + (1ull << 23)) >> 24;
+  }
+  return neg ? -(int64_t)q : (int64_t)q;
+}
+
+void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
+                                   const int32_t* cell, const float* off,
+                                   const float* vel, const float* mrel, int vexp,
+                                   int64_t* acc)
+{
+  const long ns = (long)n[0] * n[1] * n[2];
+  const float vscale = ldexpf(1.0f, 31 - vexp);
+  const uint32_t ONE = 1u << 31;
+  for (int64_t p = 0; p < np; p++) {
+    long xyz[3];
+    cell_coords(n, cell[p], xyz);
+    const float* o = off + 3 * p;
+    const float* v = vel + 3 * p;
+    uint32_t sq[3][2], tq[3][2], vq[3];
+    long vs[3][2], ts[3][2]; /* vertex and staggered coordinates */
+    for (int d = 0; d < 3; d++) {
+      const uint32_t u = wq(o[d]);
+      sq[d][0] = ONE - u;
+      sq[d][1] = u;
+      const float sd = o[d] - 0.5f;
+      const int gd = sd >= 0.0f;
+      const uint32_t us = wq(fabsf(sd));
+      tq[d][0] = gd ? ONE - us : us;
+      tq[d][1] = gd ? us : ONE - us;
+      vq[d] = (uint32_t)lrintf(fabsf(v[d]) * vscale);
+      vs[d][0] = xyz[d];
+      vs[d][1] = wrapi(xyz[d] + 1, n[d]);
+      ts[d][0] = wrapi(xyz[d] - 1 + gd, n[d]);
+      ts[d][1] = wrapi(xyz[d] + gd, n[d]);
+    }
+#define SITE(a, b, c) ((a) + (long)n[0] * ((b) + (long)n[1] * (c)))
+    if (kind == 1) {
+      for (int c = 0; c < 3; c++) {
+        const int neg = v[c] < 0.0f;
+        for (int k = 0; k < 4; k++) {
+          const int a = (k >> 1) & 1, b = k & 1;
+          uint64_t w;
+          long site;
+          if (c == 0) w = corner3(ONE, sq[1][a], sq[2][b]), site = SITE(xyz[0], vs[1][a], vs[2][b]);
+          else if (c == 1) w = corner3(sq[0][a], ONE, sq[2][b]), site = SITE(vs[0][a], xyz[1], vs[2][b]);
+          else w = corner3(sq[0][a], sq[1][b], ONE), site = SITE(vs[0][a], vs[1][b], xyz[2]);
+          acc[c * ns + site] += signed_q(mul31(w, vq[c]), mrel, p, neg);
+        }
+      }
+    } else if (kind == 2) {
+      static const int diag[3] = {0, 3, 5};
+      for (int k = 0; k < 8; k++) {
+        const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+        const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
+        const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
+        for (int d = 0; d < 3; d++) {
+          const uint64_t v2 = ((uint64_t)vq[d] * vq[d] + (1ull << 30)) >> 31;
+          acc[diag[d] * ns + site] += signed_q(mul31(w, v2), mrel, p, 0);
+        }
+      }
+      /* T_ij on the (i,j) plaquette, CIC along the third dim k */
+      static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, pk[3] = {2, 1, 0}, comp[3] = {1, 2, 4};
+      for (int q = 0; q < 3; q++) {
+        const uint64_t vv = ((uint64_t)vq[pa[q]] * vq[pb[q]] + (1ull << 30)) >> 31;
+        const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
+        for (int b = 0; b < 2; b++) {
+          const uint64_t qq = ((uint64_t)sq[pk[q]][b] * vv + (1ull << 29)) >> 30;
+          long c3[3] = {xyz[0], xyz[1], xyz[2]};
+          c3[pk[q]] = vs[pk[q]][b];
+          acc[comp[q] * ns + SITE(c3[0], c3[1], c3[2])] += signed_q(qq, mrel, p, neg);
+        }
+      }
+    } else if (kind == 3) {
+      for (int c = 0; c < 3; c++) {
+        const int neg = v[c] < 0.0f;
+        for (int k = 0; k < 8; k++) {
+          const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+          uint32_t w[3];
+          long cc[3];
+          for (int d = 0; d < 3; d++) {
+            w[d] = d == c ? tq[d][bb[d]] : sq[d][bb[d]];
+            cc[d] = d == c ? ts[d][bb[d]] : vs[d][bb[d]];
+          }
+          acc[c * ns + SITE(cc[0], cc[1], cc[2])] +=
+              signed_q(mul31(corner3(w[0], w[1], w[2]), vq[c]), mrel, p, neg);
+        }
+      }
+    } else if (kind == 4) {
+      static const int diag[3] = {0, 3, 5};
+      for (int k = 0; k < 8; k++) {
+        const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+        const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
+        const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
+        for (int d = 0; d < 3; d++) {
+          const uint64_t v2 = ((uint64_t)vq[d] * vq[d] + (1ull << 30)) >> 31;
+          acc[diag[d] * ns + site] += signed_q(mul31(w, v2), mrel, p, 0);
+        }
+      }
+      static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, comp[3] = {1, 2, 4};
+      for (int q = 0; q < 3; q++) {
+        const uint64_t vv = ((uint64_t)vq[pa[q]] * vq[pb[q]] + (1ull << 30)) >> 31;
+        const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
+        for (int k = 0; k < 8; k++) {
+          const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+          uint32_t w[3];
+          long cc[3];
+          for (int d = 0; d < 3; d++) {
+            const int st = d == pa[q] || d == pb[q];
+            w[d] = st ? tq[d][bb[d]] : sq[d][bb[d]];
+            cc[d] = st ? ts[d][bb[d]] : vs[d][bb[d]];
+          }
+          acc[comp[q] * ns + SITE(cc[0], cc[1], cc[2])] +=
+              signed_q(mul31(corner3(w[0], w[1], w[2]), vv), mrel, p, neg);
+        }
+      }
+    }
+#undef SITE
+  }
+}

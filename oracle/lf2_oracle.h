@@ -127,6 +127,19 @@ void lf2o_state_deposit_f64(const int n[3], int64_t np, const int32_t* cell,
                             const float* off, const float* mass, double gmass,
                             double res, double* rho);
 
+/* Exponent e of the fixed-point velocity unit V = 2^e: the smallest power of
+ * two above every |v_i| (0 when all are 0), at least -96. */
+int lf2o_vexp(int64_t np, const float* vel);
+
+/* Fixed-point momentum / stress deposit of the device path (kinds 1 vector
+ * CIC-NGP, 2 symtensor CIC-NGP, 3 vector CIC, 4 VecVec CIC) into a
+ * component-major int64 accumulator (3 or 6 components, internal layout).
+ * Quantum: 2^-32 of a unit mass times V (kinds 1, 3) or V^2 (2, 4). */
+void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
+                                   const int32_t* cell, const float* off,
+                                   const float* vel, const float* mrel, int vexp,
+                                   int64_t* acc);
+
 #ifdef __cplusplus
 }
 #endif

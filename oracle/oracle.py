@@ -215,6 +215,37 @@ def state_deposit_fixed(n, cell, off, mrel=None):
     return acc
 
 
+def vexp(vel):
+    """Exponent e of the fixed-point velocity unit V = 2^e of a deposit."""
+    v = np.ascontiguousarray(vel, np.float32)
+    return int(lib().lf2o_vexp(_i64(v.shape[0]), _p(v)))
+
+
+def state_deposit_fixed_kind(kind, n, cell, off, vel, mrel=None, e=None):
+    """Fixed-point momentum (kinds 1, 3) or stress (2, 4) deposit: int64
+    accumulator (comps, n2, n1, n0) and the exponent of V used."""
+    cell = np.ascontiguousarray(cell, np.int32)
+    off = np.ascontiguousarray(off, np.float32)
+    vel = np.ascontiguousarray(vel, np.float32)
+    mr = None if mrel is None else np.ascontiguousarray(mrel, np.float32)
+    if e is None:
+        e = vexp(vel)
+    comps = 3 if kind in (1, 3) else 6
+    acc = np.zeros(comps * int(n[0]) * int(n[1]) * int(n[2]), np.int64)
+    lib().lf2o_state_deposit_fixed_kind(_i(kind), _n3(n), _i64(cell.shape[0]), _p(cell), _p(off),
+                                        _p(vel), _p(mr), _i(e), _p(acc))
+    return acc.reshape(comps, int(n[2]), int(n[1]), int(n[0])), e
+
+
+def fixed_kind_to_f32(acc, kind, e, gmass, res):
+    """Converts a momentum / stress accumulator as the device does:
+    (float)q * (2^-32 m_unit / res^3 as FP32) * V^p, V^p an exact power of 2."""
+    p = 1 if kind in (1, 3) else 2
+    scale = np.float32(2.0 ** -32 * gmass / (res * res * res))
+    scale = np.float32(np.ldexp(scale, p * e))
+    return (acc.astype(np.float32) * scale).astype(np.float32)
+
+
 def fixed_to_f32(acc, scale):
     out = np.empty(acc.shape[0], np.float32)
     lib().lf2o_state_fixed_to_f32(_i64(acc.shape[0]), _p(acc), _f(scale), _p(out))

@@ -193,57 +193,95 @@ int main(int argc, char** argv)
   Particles<part_simple, part_simple_info, part_simple_dataType> parts;
   parts.initialize(info, dtype, &lat_part, boxSize);
 
-  for (int64_t i = 0; i < np; i++) {
-    int64_t id;
-    double pv[6];
-    rd(in, &id, 1);
-    rd(in, pv, 6);
-    part_simple p;
-    p.ID = id;
-    for (int l = 0; l < 3; l++) {
-      p.pos[l] = (Real)pv[l];
-      p.vel[l] = (Real)pv[3 + l];
+  // Every rank reads every particle (in chunks of records) and offers it to
+  // addParticle_global, which keeps the ones in its local domain.
+  {
+    const int64_t CH = 1 << 16;
+    std::vector<unsigned char> buf((size_t)CH * 56);
+    for (int64_t i0 = 0; i0 < np; i0 += CH) {
+      const int64_t m = np - i0 < CH ? np - i0 : CH;
+      rd(in, buf.data(), (size_t)m * 56);
+      for (int64_t i = 0; i < m; i++) {
+        int64_t id;
+        double pv[6];
+        memcpy(&id, &buf[(size_t)i * 56], 8);
+        memcpy(pv, &buf[(size_t)i * 56 + 8], 48);
+        part_simple p;
+        p.ID = id;
+        for (int l = 0; l < 3; l++) {
+          p.pos[l] = (Real)pv[l];
+          p.vel[l] = (Real)pv[3 + l];
+        }
+        parts.addParticle_global(p);
+      }
     }
-    parts.addParticle_global(p);
   }
 
+  // The force field, read one z plane at a time; each rank keeps its sites.
   Field<Real> F(lat, 3);
   if (ops & (OP_HALO | OP_KICK | OP_FFT | OP_POISSON)) {
-    std::vector<double> Fg((size_t)n * n * n * 3);
-    rd(in, Fg.data(), Fg.size());
+    std::vector<double> plane((size_t)n * n * 3);
+    const long z0 = lat.coordSkip()[0], z1 = z0 + lat.sizeLocal(2);
+    const long y0 = lat.coordSkip()[1], y1 = y0 + lat.sizeLocal(1);
     Site x(lat);
-    for (x.first(); x.test(); x.next()) {
-      const long gx = x.coord(0), gy = x.coord(1), gz = x.coord(2);
-      for (int c = 0; c < 3; c++) F(x, c) = (Real)Fg[((gz * n + gy) * (size_t)n + gx) * 3 + c];
+    for (long gz = 0; gz < n; gz++) {
+      rd(in, plane.data(), plane.size());
+      if (gz < z0 || gz >= z1) continue;
+      for (long gy = y0; gy < y1; gy++)
+        for (long gx = 0; gx < n; gx++) {
+          int c3[3] = {(int)gx, (int)gy, (int)gz};
+          if (!x.setCoord(c3)) continue;
+          for (int c = 0; c < 3; c++) F(x, c) = (Real)plane[(gy * (size_t)n + gx) * 3 + c];
+        }
     }
     F.updateHalo();
   }
   fclose(in);
 
-  // Timing mode (LF2_REF_STEPS=K): K particle-mesh steps of the reference as
-  // a user's loop runs them -- scalarProjectionCIC_project + _comm, updateVel
-  // with the CIC kick, moveParticles -- between two barriers; rank 0 prints
-  // the wall time as one JSON line.  Nothing is written.
+  // Timing mode (LF2_REF_STEPS=K, LF2_REF_WARMUP=W): W untimed steps, then K
+  // particle-mesh steps of the reference as a user's loop runs them --
+  // scalarProjectionCIC_project + _comm, updateVel with the CIC kick,
+  // moveParticles -- each between two barriers; rank 0 prints the total and
+  // the per-step wall times as one JSON line.  Nothing is written.
   if (const char* ks = getenv("LF2_REF_STEPS")) {
     const int steps = atoi(ks);
+    const char* ws = getenv("LF2_REF_WARMUP");
+    const int warm = ws ? atoi(ws) : 0;
     Field<Real> rho(lat, 1);
     Field<Real>* fl[1] = {&F};
     double out1[1];
     int red[1] = {SUM};
-    parallel.barrier();
-    const auto t0 = std::chrono::steady_clock::now();
-    for (int s = 0; s < steps; s++) {
+    std::vector<double> per;
+    double sec = 0.0;
+    for (int s = 0; s < warm + steps; s++) {
+      parallel.barrier();
+      const auto t0 = std::chrono::steady_clock::now();
       projection_init(&rho);
       scalarProjectionCIC_project(&parts, &rho);
       scalarProjectionCIC_comm(&rho);
       parts.updateVel(&cic_kick, dtk, fl, 1, NULL, out1, red, 1);
       parts.moveParticles(&move_particles_simple, dtm);
+      parallel.barrier();
+      const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (s >= warm) {
+        per.push_back(dt);
+        sec += dt;
+      }
     }
-    parallel.barrier();
-    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    if (parallel.rank() == 0)
-      printf("{\"seconds\": %.6f, \"steps\": %d, \"particles\": %lld, \"ranks\": %d}\n", sec, steps,
-             (long long)np, g0 * g1);
+    long nloc = 0;
+    {
+      Site xp(parts.lattice());
+      for (xp.first(); xp.test(); xp.next())
+        for (auto it = parts.field()(xp).parts.begin(); it != parts.field()(xp).parts.end(); ++it) nloc++;
+    }
+    parallel.sum(nloc);
+    if (parallel.rank() == 0) {
+      printf("{\"seconds\": %.6f, \"steps\": %d, \"warmup\": %d, \"particles\": %lld, "
+             "\"particles_after\": %ld, \"ranks\": %d, \"step_seconds\": [",
+             sec, steps, warm, (long long)np, nloc, g0 * g1);
+      for (size_t i = 0; i < per.size(); i++) printf("%s%.6f", i ? ", " : "", per[i]);
+      printf("]}\n");
+    }
     return 0;
   }
 

@@ -51,6 +51,27 @@ def mean_relative_error(got, ref, floor_frac=1e-3):
     return float(np.max(np.abs(got[m] - ref[m]) / np.abs(ref[m])))
 
 
+def precision(got, ref, mag=None, floor_frac=1e-2):
+    """Error of a deposited field against its FP64 reference.
+      norm_max / norm_rms: |got - ref| over the field's maximum |ref|;
+      cell_max / cell_rms: per-vertex |got - ref| / mag, over the vertices
+        where mag exceeds floor_frac of its mean.  mag is the vertex's sum of
+        |contributions| (the FP64 deposit of |m v|, |m v_i v_j|; for the
+        density mag = ref): the relative error of a sum, which stays defined
+        where signed contributions cancel.
+    """
+    got = np.asarray(got, np.float64).reshape(-1)
+    ref = np.asarray(ref, np.float64).reshape(-1)
+    mag = np.abs(ref) if mag is None else np.asarray(mag, np.float64).reshape(-1)
+    d = np.abs(got - ref)
+    scale = max(float(np.max(np.abs(ref))), 1e-300)
+    m = mag > floor_frac * float(np.mean(mag))
+    rel = d[m] / mag[m] if np.any(m) else np.zeros(1)
+    return {"norm_max": float(np.max(d) / scale), "norm_rms": float(np.sqrt(np.mean(d * d)) / scale),
+            "cell_max": float(np.max(rel)), "cell_rms": float(np.sqrt(np.mean(rel * rel))),
+            "floor_frac": floor_frac, "cells_above_floor": int(np.count_nonzero(m))}
+
+
 def by_id(d, ids_key="id"):
     order = np.argsort(d[ids_key], kind="stable")
     return {k: v[order] for k, v in d.items()}

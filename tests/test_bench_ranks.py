@@ -55,16 +55,22 @@ def test_replica_throughput_one_rank():
     assert ms == 20.0 and value == pytest.approx(500 * 4 / 0.020)
 
 
-def test_reference_cpu_baseline_runs_the_reference():
-    """The CPU baseline runs the reference's own particle path (compiled from
-    its headers into oracle/_ref by oracle/build_ref.sh) on a 2x2 grid of
-    forked ranks; without that build the bench falls back to the port."""
+def test_reference_cpu_baseline_runs_the_reference(tmp_path, monkeypatch):
+    """The CPU baseline and the reference arm run the reference's own particle
+    path (compiled from its headers into oracle/_ref by oracle/build_ref.sh) on
+    the bench's workload, a 2x2 grid of forked ranks here (the 64^3 uniform
+    workload), with per-step times; without that build the bench falls back
+    to the port."""
     import bench
     if not os.access(bench.REF_DRIVER, os.X_OK):
         pytest.skip("oracle/_ref not built (the reference sources are absent)")
     assert bench._ref_grid(4) == (2, 2) and bench._ref_grid(3) is None
     assert bench._ref_grid(200) == (8, 8)
-    r = bench.cpu_baseline_reference(0.5, 4)
+    monkeypatch.setenv("LF2_REF_INPUT_DIR", str(tmp_path))
+    r = bench.cpu_reference_steps("c1", 4, 3, 1)
     assert r is not None
-    ups, steps, ranks = r
-    assert ranks == 4 and steps >= 5 and ups > 0
+    assert r["ranks"] == 4 and r["steps"] == 3 and r["warmup"] == 1
+    assert len(r["step_seconds"]) == 3 and r["particles_after"] == 64 ** 3
+    cpu = bench.cpu_reference_summary("c1", r)
+    assert cpu["kind"] == "reference" and cpu["cores"] == 4 and cpu["value"] > 0
+    assert bench.workload_config("c3")["particles"] == 512 ** 3

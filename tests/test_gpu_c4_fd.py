@@ -1,0 +1,84 @@
+"""Configuration C4 at full size: the differentiable particle-mesh chain at
+128^3 with 2,097,152 particles (per-particle masses (1/Np)(1 + 0.1 U(-1,1)),
+the seeded 27-point stencil as grid operator, 8 kick-drift steps,
+checkpoints every 2 steps).
+
+The CUDA adjoint's gradients for the initial positions, velocities, masses,
+stencil weights and loss weights are compared with the FP64 reference
+gradient (oracle/pm_chain.py, autograd in float64), and both with FP64
+central finite differences along 1,000 random directions.  CIC is only
+piecewise smooth, so each direction's eps is shrunk until no particle
+changes cell between the two evaluations; a direction that finds no such
+eps down to 1e-12 is skipped, and at most 5% may be.
+
+Tolerances: the FP64 gradient agrees with the differences within 1e-4 of
+their rms; the CUDA adjoint (FP32 particle state through 8 steps) within
+1e-2 of the rms, median 3e-3; gradient norms within 5e-3 (positions,
+velocities, masses) and 2e-3 (stencil weights) of the FP64 ones.
+"""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_c4_chain_against_fp64_finite_differences_on_1000_directions(cuda):
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import pm_chain_loss, positions_to_state
+    from oracle import pm_chain as P
+    n, npart, steps, dirs = 128, 1 << 21, 8, 1000
+    dt = 0.1 * 64.0 / n
+    dev = "cuda"
+    g = torch.Generator(device=dev).manual_seed(41)
+    pos = torch.rand(npart, 3, generator=g, device=dev, dtype=torch.float64)
+    vel = (0.01 * torch.randn(npart, 3, generator=g, device=dev, dtype=torch.float64)).float().double()
+    m = ((1.0 + 0.1 * (2 * torch.rand(npart, generator=g, device=dev, dtype=torch.float64) - 1))
+         / npart).float().double()
+    S = (0.02 * torch.randn(81, generator=g, device=dev, dtype=torch.float64)).float().double()
+    w = torch.randn(n ** 3, generator=g, device=dev, dtype=torch.float64).float().double()
+    # positions exactly representable in the device state (cell + FP32 offset)
+    cell, off = positions_to_state(pos, (n, n, n), 1.0 / n)
+    c = cell.long()
+    pos = (torch.stack([c % n, (c // n) % n, c // (n * n)], 1).double() + off.double()) / n
+    ctx = L.Context((n, n, n), box=1.0)
+    leaves = [t.clone().requires_grad_(True) for t in (pos, vel, m, S, w)]
+    pm_chain_loss(ctx, *leaves, steps=steps, dt=dt, checkpoint_every=2).backward()
+    got = [t.grad for t in leaves]
+    ref_leaves = [t.clone().requires_grad_(True) for t in (pos, vel, m, S, w)]
+    ref = torch.autograd.grad(P.chain_loss(*ref_leaves, (n, n, n), steps, dt), ref_leaves)
+    rel = {k: float((a_ - b_).norm() / b_.norm())
+           for k, a_, b_ in zip(("pos", "vel", "mass", "stencil", "weights"), got, ref)}
+    rng = np.random.default_rng(11)
+    base = [pos, vel, m, S]
+    fd, dv, rf = [], [], []
+    t0 = time.time()
+    for _ in range(dirs):
+        us = [torch.from_numpy(rng.standard_normal(tuple(t.shape))).to(dev) for t in base]
+        nrm = float(torch.sqrt(sum((u ** 2).sum() for u in us)))
+        us = [u / nrm for u in us]
+        with torch.no_grad():
+            d, _ = P.directional_fd(base, us, w, (n, n, n), steps, dt, eps=1e-7)
+        if d is None:
+            continue
+        fd.append(d)
+        dv.append(float(sum((gg * u).sum() for gg, u in zip(got[:4], us))))
+        rf.append(float(sum((gg * u).sum() for gg, u in zip(ref[:4], us))))
+    fd, dv, rf = map(np.array, (fd, dv, rf))
+    scale = float(np.sqrt(np.mean(fd ** 2)))
+    out = {"directions_used": len(fd), "grad_rel_err_vs_fp64": rel,
+           "fd_max_err_ref_over_rms": float(np.max(np.abs(rf - fd)) / scale),
+           "fd_max_err_cuda_over_rms": float(np.max(np.abs(dv - fd)) / scale),
+           "fd_median_rel_err_cuda": float(np.median(np.abs(dv - fd) / np.abs(fd))),
+           "seconds": time.time() - t0}
+    print("C4 finite-difference check:", out)
+    ctx.close()
+    assert len(fd) >= 0.95 * dirs, out
+    assert out["fd_max_err_ref_over_rms"] < 1e-4, out
+    assert out["fd_max_err_cuda_over_rms"] < 1e-2, out
+    assert out["fd_median_rel_err_cuda"] < 3e-3, out
+    for k in ("pos", "vel", "mass"):
+        assert rel[k] < 5e-3, (k, out)
+    assert rel["stencil"] < 2e-3 and rel["weights"] < 1e-5, out

@@ -1,7 +1,7 @@
 """The CUDA path against the reference's own outputs (tests/golden/, written
 by the reference compiled from its sources): deposits, kick and move on the
-same particles.  Tolerances as in test_gpu_parity.py: fixed-point deposit
-1e-6 and FP32 deposits 1e-5 of the field maximum; velocities 2e-6 of the
+same particles.  Tolerances as in test_gpu_parity.py: fixed-point and FP32
+(compensated) deposits 1e-6 of the field maximum; velocities 2e-6 of the
 maximum; positions 1e-6 of a cell, cells identical except within 1e-4 cells
 of a face."""
 import glob
@@ -34,31 +34,33 @@ def test_deposits_match_reference(cuda, path, mode):
     rho = ctx.field(1)
     ctx.deposit_scalar(rho)
     got = rho.export(0, np.float64)
-    assert normalized_error(got, g["rho"]) < (1e-6 if mode == 1 else 1e-5)
-    if mode == 0 and "vec" in g:
+    assert normalized_error(got, g["rho"]) < 1e-6
+    if "vec" in g:
         v, t = ctx.field(3), ctx.field(6)
         ctx.deposit_vector(v)
         ctx.deposit_symtensor(t)
         for c in range(3):
-            assert normalized_error(v.export(0, np.float64)[..., c], g["vec"][..., c]) < 1e-5
+            assert normalized_error(v.export(0, np.float64)[..., c], g["vec"][..., c]) < 1e-6
         for c in range(6):
-            assert normalized_error(t.export(0, np.float64)[..., c], g["ten"][..., c]) < 1e-5
+            assert normalized_error(t.export(0, np.float64)[..., c], g["ten"][..., c]) < 1e-6
 
 
 @pytest.mark.parametrize("path", [p for p in CASES if "vcic" in np.load(p)],
                          ids=lambda p: os.path.basename(p))
-def test_full_cic_deposits_match_reference(cuda, path):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_full_cic_deposits_match_reference(cuda, path, mode):
     """vectorProjectionCIC and VecVecProjectionCIC of the reference on a 2x2
-    process grid against the single-GPU deposits (FP32, 1e-5)."""
+    process grid against the single-GPU deposits (FP32 and fixed point,
+    1e-6)."""
     g = dict(np.load(path))
-    ctx = _ctx(g, 0)
+    ctx = _ctx(g, mode)
     v, t = ctx.field(3), ctx.field(6)
     ctx.deposit_vector_cic(v)
     ctx.deposit_vecvec_cic(t)
     for c in range(3):
-        assert normalized_error(v.export(0, np.float64)[..., c], g["vcic"][..., c]) < 1e-5
+        assert normalized_error(v.export(0, np.float64)[..., c], g["vcic"][..., c]) < 1e-6
     for c in range(6):
-        assert normalized_error(t.export(0, np.float64)[..., c], g["vv"][..., c]) < 1e-5
+        assert normalized_error(t.export(0, np.float64)[..., c], g["vv"][..., c]) < 1e-6
 
 
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])

@@ -130,3 +130,41 @@ def test_pipelined_move_long_run_equals_per_brick(cuda):
         np.testing.assert_array_equal(a[kk], b[kk])
     np.testing.assert_array_equal(ra, rb)
     assert sa[1] > 0  # bricks were relocated
+
+
+def test_a_wait_that_runs_out_is_reported_and_the_context_recovers(cuda):
+    """The bounded-wait path: with the consumers stalled on a barrier that
+    nothing completes and a limit of about 10 us, the pass gives up (the
+    producer waits for its copies first), the status is LF2_ERR_STATE with
+    LF2_FLAG_TIMEOUT, and after a reload the same context steps bit-exactly
+    against the oracle with the default limit."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200 import _lib
+    n = (32, 32, 32)
+    cell, off, vel = small_case(n, 20000, seed=7, vel_sigma=0.03)
+    F = np.random.default_rng(8).standard_normal((3, 32, 32, 32)).astype(np.float32)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    ctx = L.Context(n, box=1.0, mode=1)
+    ctx.set_particles(cell, off, vel, global_mass=1.0 / 20000, ids=ids)
+    ctx.set_move_kernel(2)
+    Fh = ctx.field(3, torch.from_numpy(F).cuda())
+    rho = ctx.field(1)
+    ctx.set_wait_limit(20000, stall=True)
+    ctx.step(Fh, 0.05, 0.2, rho)
+    with pytest.raises(_lib.LF2Error) as err:
+        ctx.synchronize()
+    assert err.value.status == _lib.LF2_ERR_STATE
+    assert ctx.flags() & _lib.FLAG_TIMEOUT
+    ctx.set_wait_limit(0)
+    ctx.set_particles(cell, off, vel, global_mass=1.0 / 20000, ids=ids)
+    assert ctx.flags() == 0
+    ctx.step(Fh, 0.05, 0.2, rho)
+    ctx.synchronize()
+    assert ctx.last_move_kernel() == 2
+    got = by_id(ctx.get_particles(ids=True))
+    v = O.state_kick(n, cell, off, vel, F, np.float32(0.05))
+    c, o, _ = O.state_drift(n, cell, off, v, np.float32(0.2 * 32))
+    np.testing.assert_array_equal(got["vel"], v)
+    np.testing.assert_array_equal(got["cell"], c)
+    np.testing.assert_array_equal(got["off"], o)

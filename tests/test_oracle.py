@@ -210,3 +210,34 @@ def test_cell_xyz_roundtrip():
     c = np.arange(105)
     xyz = cell_xyz(n, c)
     assert np.all(xyz[:, 0] + 5 * (xyz[:, 1] + 7 * xyz[:, 2]) == c)
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3, 4])
+@pytest.mark.parametrize("clustered", [False, True])
+def test_fixed_point_momentum_and_stress_match_the_reference_projections(kind, clustered):
+    """The integer restatement of the fixed-point momentum / stress deposits
+    (layer B) puts every contribution on the vertex the reference's
+    projection does (layer A, FP64), to the quantum of the fixed point."""
+    n = (12, 10, 9)
+    cell, off, vel = small_case(n, 3000, seed=60 + kind, vel_sigma=0.2, clustered=clustered)
+    res = 1.0 / n[0]
+    gm = 1.0 / 3000
+    acc, e = O.state_deposit_fixed_kind(kind, n, cell, off, vel)
+    got = O.fixed_kind_to_f32(acc, kind, e, gm, res)
+    cs, order = O.lists_from_insertion(n, cell)
+    pos = positions(n, res, cell, off)[order]
+    v = vel.astype(np.float64)[order]
+    fn = {1: O.vector_cicngp, 2: O.symtensor_cicngp, 3: O.vector_cic, 4: O.vecvec_cic}[kind]
+    ref = O.interior(fn(n, 1, res, cs, pos, v, gmass=gm), n, 1)
+    for c in range(ref.shape[0]):
+        assert normalized_error(got[c], ref[c]) < 1e-6, c
+
+
+def test_fixed_point_velocity_unit():
+    """V = 2^e is the smallest power of two above every |v_i|."""
+    for vmax, e in ((0.02, -5), (0.5, 0), (1.0, 1), (3.0, 2), (2.0 ** -30, -29)):
+        v = np.array([[vmax, -vmax / 3, 0.0]], np.float32)
+        assert O.vexp(v) == e, (vmax, O.vexp(v))
+        assert 2.0 ** (e - 1) <= vmax < 2.0 ** e
+    assert O.vexp(np.zeros((4, 3), np.float32)) == 0
+    assert O.vexp(np.full((1, 3), 1e-35, np.float32)) == -96
