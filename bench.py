@@ -863,9 +863,12 @@ def main():
     peak, peak_kind = peaks()
     dom = max(("move", "deposit_tile"), key=lambda p: phases[p][0])
     per_launch_ms = phases[dom][0] / max(1, phases[dom][1])
+    mk = ctx.last_move_kernel()
     if dom == "move":
         ab = alg_bytes_move(npart, nsites)
-        kname = "k_move_pipe" if ctx.last_move_kernel() == 2 else "k_move<kick,drift>"
+        kname = {1: "k_move<kick,drift>", 2: "k_move_pipe"}.get(mk, "k_move_pipe<fused deposit>")
+        if mk == 3:
+            ab += nsites * 4  # the density is written by the same pass (rim vertices later)
     else:
         ab = alg_bytes_deposit(npart, nsites)
         kname = "k_deposit<scalar>"

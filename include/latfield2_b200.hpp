@@ -45,7 +45,9 @@
 #ifndef LATFIELD2_B200_HPP
 #define LATFIELD2_B200_HPP
 
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -74,6 +76,15 @@ typedef double Real;
 #endif
 static int const FROM_PART = INDIVIDUAL_MASS;
 static int const FROM_INFO = GLOBAL_MASS;
+// reduction types of updateVel / moveParticles outputs (LATfield2_Particles.hpp:81-86)
+#ifndef SUM
+#define SUM 1
+#define MIN 2
+#define MAX 4
+#define SUM_LOCAL 8
+#define MIN_LOCAL 16
+#define MAX_LOCAL 32
+#endif
 static int const symmetric = 1;
 static int const unsymmetric = 0;
 
@@ -104,6 +115,27 @@ float mass_of(const T&, std::false_type)
 {
   return 0.0f;
 }
+
+// A projection's global mass (oset / FROM_INFO) for the duration of one
+// deposit, when it differs from the particles' part_info mass.
+struct MassScope {
+  lf2_ctx* ctx;
+  double restore;
+  bool set = false;
+  MassScope(lf2_ctx* c, double mass, double current) : ctx(c), restore(current)
+  {
+    if (mass >= 0.0 && mass != current) {
+      check(ctx, lf2_set_global_mass(ctx, mass), "lf2_set_global_mass");
+      set = true;
+    }
+  }
+  ~MassScope()
+  {
+    if (set) lf2_set_global_mass(ctx, restore);
+  }
+  MassScope(const MassScope&) = delete;
+  MassScope& operator=(const MassScope&) = delete;
+};
 
 }  // namespace lf2detail
 
@@ -723,7 +755,7 @@ void move_particles_simple_t(double dtau, double, part* p, double*, part_info, F
 // it inside updateVel; a direct call kicks one particle on the host arrays.
 template <class part, class part_info>
 Real cic_gather_kick_t(double dtau, double, part* p, double* frac, part_info, Field<Real>** fields,
-                       Site* sites, int, double*, double*, int)
+                       Site* sites, int, double*, double* outputs, int noutputs)
 {
   Field<Real>& F = *fields[0];
   Real a[3] = {0, 0, 0};
@@ -738,11 +770,25 @@ Real cic_gather_kick_t(double dtau, double, part* p, double* frac, part_info, Fi
     for (int c = 0; c < 3; c++) a[c] += w * F(s, c);
   }
   Real v2 = 0;
+  double v2d = 0.0;
   for (int c = 0; c < 3; c++) {
     p->vel[c] += dtau * a[c];
     v2 += p->vel[c] * p->vel[c];
+    v2d += (double)p->vel[c] * (double)p->vel[c];
   }
+  if (noutputs > 0) outputs[0] = v2d;  // the per-particle output updateVel reduces
   return v2;
+}
+
+// The same kick in the signature of updateVel's mappingClass overload
+// (LATfield2_Particles.hpp:191-200): the mapping object is not used.
+template <class part, class part_info, class mappingClass>
+Real cic_gather_kick_mapped(double dtau, double res, part* p, double* frac, part_info info,
+                            Field<Real>** fields, Site* sites, mappingClass*, int nfield,
+                            double* params, double* outputs, int noutputs)
+{
+  return cic_gather_kick_t<part, part_info>(dtau, res, p, frac, info, fields, sites, nfield, params,
+                                            outputs, noutputs);
 }
 
 inline void move_particles_simple(double dtau, double res, part_simple* p, double* frac,
@@ -838,21 +884,98 @@ class Particles {
   }
 
   // updateVel with the CIC gather-kick: fields[0] is the 3-component force.
-  // Returns sqrt(max |v|^2) like the reference.
+  // Returns sqrt(max |v|^2) like the reference.  The kick reports |v|^2 as
+  // its per-particle output 0; output[0] receives its SUM, MIN or MAX over
+  // the particles (FP64 on the GPU) as reduce_type[0] says; further outputs
+  // are not written by the kick and keep the reduction's starting value
+  // (0, 9223372036854775807, -9223372036854775807), as in the reference.
   Real updateVel(kick_fn updateVel_funct, double dtau, Field<Real>** fields = NULL, int nfields = 0,
                  double* params = NULL, double* output = NULL, int* reduce_type = NULL, int noutput = 0)
   {
-    (void)params, (void)output, (void)reduce_type;
+    (void)params;
     if (!(updateVel_funct == &cic_gather_kick_t<part, part_info> ||
           lf2detail::is_simple_kick(updateVel_funct)))
       throw std::invalid_argument("updateVel: only cic_gather_kick runs on the GPU");
-    if (nfields < 1 || !fields || fields[0]->components() != 3 || noutput != 0)
-      throw std::invalid_argument("updateVel: cic_gather_kick takes one 3-component field, no outputs");
+    return gpu_kick(dtau, fields, nfields, output, reduce_type, noutput);
+  }
+
+  // The mappingClass overload (LATfield2_Particles.hpp:191-200, :609-750):
+  // the callback takes the mapping object after the sites.
+  template <typename mappingClass>
+  Real updateVel(Real (*updateVel_funct)(double, double, part*, double*, part_info, Field<Real>**, Site*,
+                                         mappingClass*, int, double*, double*, int),
+                 double dtau, Field<Real>** fields = NULL, int nfields = 0, mappingClass* mc = NULL,
+                 double* params = NULL, double* output = NULL, int* reduce_type = NULL, int noutput = 0)
+  {
+    (void)mc, (void)params;
+    if (updateVel_funct != &cic_gather_kick_mapped<part, part_info, mappingClass>)
+      throw std::invalid_argument("updateVel: only cic_gather_kick_mapped runs on the GPU");
+    return gpu_kick(dtau, fields, nfields, output, reduce_type, noutput);
+  }
+
+  // The global mass a projection deposits with, after checking oset and
+  // flag_where (projections.hpp:115-126, :458-459, :746-747) against what
+  // the GPU store holds: positions, velocities (`vel`) and the mass member
+  // of particle types that have one.  oset NULL: the particle type's own
+  // mass.  FROM_INFO: the double at byte oset[0] of part_info, for particles
+  // without individual masses.  FROM_PART: oset[0] must be the mass member.
+  // oset[1] (momentum and stress) must be `vel`.  Returns a negative value
+  // for individual masses.
+  double projection_mass(const size_t* oset, int flag_where, bool reads_vel, const char* what)
+  {
+    const bool individual = lf2detail::has_mass<part>::value;
+    if (!oset) return individual ? -1.0 : (double)info_.mass;
+    if (reads_vel && oset[1] != offsetof(part, vel))
+      throw std::invalid_argument(std::string(what) +
+                                  ": oset[1] must be the vel member: the GPU store holds only vel");
+    if (flag_where == FROM_INFO) {
+      if (individual)
+        throw std::invalid_argument(std::string(what) +
+                                    ": FROM_INFO for particles with individual masses is not provided");
+      return *reinterpret_cast<const double*>(reinterpret_cast<const char*>(&info_) + oset[0]);
+    }
+    if (flag_where == FROM_PART) {
+      if (!individual || oset[0] != mass_offset())
+        throw std::invalid_argument(std::string(what) +
+                                    ": FROM_PART must name the particle type's mass member");
+      return -1.0;
+    }
+    throw std::invalid_argument(std::string(what) + ": flag_where is FROM_INFO or FROM_PART");
+  }
+  // the global mass the GPU store was loaded with
+  double global_mass() const { return gmass_dev_; }
+
+  // LATfield2_Particles.hpp:400-425: how the projections find the mass.
+  int mass_type() const { return lf2detail::has_mass<part>::value ? INDIVIDUAL_MASS : GLOBAL_MASS; }
+  size_t mass_offset() const { return mass_offset_of(lf2detail::has_mass<part>()); }
+
+  // The part of updateVel the GPU does: the CIC kick, then the output
+  // reductions.
+  Real gpu_kick(double dtau, Field<Real>** fields, int nfields, double* output, int* reduce_type,
+                int noutput)
+  {
+    if (nfields < 1 || !fields || fields[0]->components() != 3)
+      throw std::invalid_argument("updateVel: cic_gather_kick takes one 3-component field");
+    if (noutput > 0 && (!output || !reduce_type))
+      throw std::invalid_argument("updateVel: outputs need output and reduce_type arrays");
     check_field(fields[0], "updateVel");
     sync();
     double maxv = 0.0;
     lf2_field F = fields[0]->lf2_handle(owner_);
     lf2detail::check(ctx_, lf2_gather_kick(ctx_, F, dtau, &maxv), "lf2_gather_kick");
+    if (noutput > 0) {
+      double s = 0.0, mn = 0.0, mx = 0.0;
+      lf2detail::check(ctx_, lf2_velocity_reductions(ctx_, &s, &mn, &mx), "lf2_velocity_reductions");
+      const bool any = numParticles() > 0;
+      for (int i = 0; i < noutput; i++) {
+        if (reduce_type[i] & (SUM | SUM_LOCAL))
+          output[i] = (i == 0 && any) ? s : 0.0;
+        else if (reduce_type[i] & (MIN | MIN_LOCAL))
+          output[i] = (i == 0 && any) ? std::min(mn, 9223372036854775807.0) : 9223372036854775807.0;
+        else if (reduce_type[i] & (MAX | MAX_LOCAL))
+          output[i] = (i == 0 && any) ? mx : -9223372036854775807.0;
+      }
+    }
     return (Real)maxv;
   }
 
@@ -959,11 +1082,19 @@ class Particles {
                                            individual ? mass_.data() : nullptr,
                                            individual ? 0.0 : info_.mass, ids_.data()),
                      "lf2_particles_set_pos");
+    gmass_dev_ = individual ? 0.0 : (double)info_.mass;
     on_device_ = (int64_t)ids_.size();
     pos_.clear(), vel_.clear(), ids_.clear(), mass_.clear();
   }
 
  private:
+  template <class P = part>
+  static size_t mass_offset_of(std::true_type)
+  {
+    return offsetof(P, mass);
+  }
+  static size_t mass_offset_of(std::false_type) { return offsetof(part_info, mass); }
+
   static void one_file(int fileNumber, const char* what)
   {
     if (fileNumber != 1)
@@ -977,6 +1108,7 @@ class Particles {
   double box_[3] = {1, 1, 1};
   Real res_ = 1;
   int64_t on_device_ = 0;
+  double gmass_dev_ = 0.0;
   std::vector<double> pos_, vel_;
   std::vector<int64_t> ids_;
   std::vector<float> mass_;
@@ -991,12 +1123,12 @@ template <class part, class part_info, class part_dataType>
 void scalarProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* rho,
                                  size_t* oset = NULL, int flag_where = FROM_INFO)
 {
-  (void)oset;
-  if (flag_where == FROM_PART && !lf2detail::has_mass<part>::value)
-    throw std::invalid_argument("scalarProjectionCIC_project: the particle type has no mass member");
   parts->check_field(rho, "scalarProjectionCIC_project");
   const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
   lf2_ctx* ctx = owner.get();
+  lf2detail::MassScope ms(ctx, parts->projection_mass(oset, flag_where, false,
+                                                      "scalarProjectionCIC_project"),
+                          parts->global_mass());
   lf2detail::check(ctx, lf2_deposit_scalar(ctx, rho->lf2_handle(owner, false)), "lf2_deposit_scalar");
   rho->mark_device_written();
 }
@@ -1005,10 +1137,11 @@ template <class part, class part_info, class part_dataType>
 void vectorProjectionCICNGP_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* vel,
                                     size_t* oset = NULL, int flag_where = FROM_INFO)
 {
-  (void)oset, (void)flag_where;
   parts->check_field(vel, "vectorProjectionCICNGP_project");
   const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
   lf2_ctx* ctx = owner.get();
+  lf2detail::MassScope ms(ctx, parts->projection_mass(oset, flag_where, true, "vectorProjectionCICNGP_project"),
+                          parts->global_mass());
   lf2detail::check(ctx, lf2_deposit_vector_cicngp(ctx, vel->lf2_handle(owner, false)),
                    "lf2_deposit_vector_cicngp");
   vel->mark_device_written();
@@ -1018,10 +1151,11 @@ template <class part, class part_info, class part_dataType>
 void symtensorProjectionCICNGP_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* Tij,
                                        size_t* oset = NULL, int flag_where = FROM_INFO)
 {
-  (void)oset, (void)flag_where;
   parts->check_field(Tij, "symtensorProjectionCICNGP_project");
   const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
   lf2_ctx* ctx = owner.get();
+  lf2detail::MassScope ms(ctx, parts->projection_mass(oset, flag_where, true, "symtensorProjectionCICNGP_project"),
+                          parts->global_mass());
   lf2detail::check(ctx, lf2_deposit_symtensor_cicngp(ctx, Tij->lf2_handle(owner, false)),
                    "lf2_deposit_symtensor_cicngp");
   Tij->mark_device_written();
@@ -1033,10 +1167,11 @@ template <class part, class part_info, class part_dataType>
 void vectorProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* vel,
                                  size_t* oset = NULL, int flag_where = FROM_INFO)
 {
-  (void)oset, (void)flag_where;
   parts->check_field(vel, "vectorProjectionCIC_project");
   const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
   lf2_ctx* ctx = owner.get();
+  lf2detail::MassScope ms(ctx, parts->projection_mass(oset, flag_where, true, "vectorProjectionCIC_project"),
+                          parts->global_mass());
   lf2detail::check(ctx, lf2_deposit_vector_cic(ctx, vel->lf2_handle(owner, false)),
                    "lf2_deposit_vector_cic");
   vel->mark_device_written();
@@ -1048,10 +1183,11 @@ template <class part, class part_info, class part_dataType>
 void VecVecProjectionCIC_project(Particles<part, part_info, part_dataType>* parts, Field<Real>* Tij,
                                  size_t* oset = NULL, int flag_where = FROM_INFO)
 {
-  (void)oset, (void)flag_where;
   parts->check_field(Tij, "VecVecProjectionCIC_project");
   const std::shared_ptr<lf2_ctx>& owner = parts->lf2_context_owner();
   lf2_ctx* ctx = owner.get();
+  lf2detail::MassScope ms(ctx, parts->projection_mass(oset, flag_where, true, "VecVecProjectionCIC_project"),
+                          parts->global_mass());
   lf2detail::check(ctx, lf2_deposit_vecvec_cic(ctx, Tij->lf2_handle(owner, false)),
                    "lf2_deposit_vecvec_cic");
   Tij->mark_device_written();

@@ -121,6 +121,13 @@ lf2_status lf2_particles_set_pos(lf2_ctx* ctx, int64_t n, const void* pos3,
                                  const void* vel3, int real_bytes,
                                  const float* mass, double global_mass,
                                  const int64_t* id);
+/* The global particle mass (part_info.mass of GLOBAL_MASS types) used by
+ * later deposits and conservation sums; for particles without individual
+ * masses it is also the unit of the fixed-point deposit.  The projections'
+ * oset / FROM_INFO argument (projections.hpp:115-126) in the C++ layer sets
+ * it for one deposit.  LF2_ERR_ARG when the particles carry individual
+ * masses or mass <= 0. */
+lf2_status lf2_set_global_mass(lf2_ctx* ctx, double mass);
 /* Slab decomposition (one rank per GPU, z split across ranks, one ghost
  * cell plane below and above the rank's own planes): the particle
  * migration of moveParticles (LATfield2_Particles.hpp:2176-2799) as two
@@ -234,15 +241,21 @@ lf2_status lf2_gather_kick(lf2_ctx* ctx, lf2_field F, double dtau,
  * pos += dtau * vel, periodic wrap and rebin into cells. */
 lf2_status lf2_drift_rebin(lf2_ctx* ctx, double dtau);
 /* One fused kick-drift-rebin pass (updateVel then moveParticles) followed,
- * when rho is not NULL, by the scalar deposit of the new positions. */
+ * when rho is not NULL, by the scalar deposit of the new positions.  In the
+ * fixed-point mode, with the pipelined kernel, the deposit of the particles
+ * that stay in their brick is fused into the pass (the movers' share is
+ * added by a separate kernel); the density is the same bit for bit. */
 lf2_status lf2_step(lf2_ctx* ctx, lf2_field F, double dtau_kick,
                     double dtau_drift, lf2_field rho);
 /* Kernel of lf2_step's kick-drift-rebin pass: 0 automatic (the persistent
- * TMA-pipelined kernel where the lattice allows it, else the per-brick
- * kernel), 1 the per-brick kernel, 2 the pipelined kernel (needs
- * n0 % 4 == 0, every n >= 32 and F 16-byte aligned, else
- * LF2_ERR_UNSUPPORTED).  Both give the same particles (the order of the
- * particles inside a brick may differ); no reference counterpart. */
+ * TMA-pipelined kernel where the lattice allows it, with the deposit fused
+ * in for the fixed-point mode, else the per-brick kernel), 1 the per-brick
+ * kernel, 2 the pipelined kernel without the fused deposit, 3 the pipelined
+ * kernel with the fused deposit (pipelined kernels need n0 % 4 == 0, every
+ * n >= 32 and F 16-byte aligned; the fused deposit the fixed-point mode,
+ * else LF2_ERR_UNSUPPORTED).  All give the same particles (the order of the
+ * particles inside a brick may differ) and the same fixed-point density; no
+ * reference counterpart. */
 lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
 /* Bounded waits of the pipelined kernel (no reference counterpart): every
  * wait on a copy or on another warp gives up after `cycles` SM clock cycles
@@ -253,7 +266,7 @@ lf2_status lf2_set_move_kernel(lf2_ctx* ctx, int which);
  * interrupted pass are not valid; load them again). */
 lf2_status lf2_set_wait_limit(lf2_ctx* ctx, int64_t cycles, int stall);
 /* Kernel the last lf2_step used for its kick-drift-rebin pass: 1 per-brick,
- * 2 pipelined, 0 before the first step. */
+ * 2 pipelined, 3 pipelined with the fused deposit, 0 before the first step. */
 lf2_status lf2_last_move_kernel(lf2_ctx* ctx, int* which);
 /* max |v| after the last kick (lf2_step or lf2_gather_kick): the value
  * updateVel returns (LATfield2_Particles.hpp:870-893), from the per-brick
@@ -266,6 +279,13 @@ lf2_status lf2_last_max_velocity(lf2_ctx* ctx, double* max_v, int ptr_kind);
  * 543-583, and the SUM/MAX outputs of updateVel).  Any pointer may be NULL. */
 lf2_status lf2_conservation(lf2_ctx* ctx, double* mass, double mom[3],
                             double* max_v);
+/* FP64 SUM, MIN and MAX over all particles of |v|^2 (|v|^2 in double from
+ * the FP32 components): the reductions updateVel applies (reduce_type SUM,
+ * MIN, MAX, LATfield2_Particles.hpp:786-893) to the output the library's
+ * kick reports per particle.  MIN over no particles is +infinity.  Any
+ * pointer may be NULL; synchronises. */
+lf2_status lf2_velocity_reductions(lf2_ctx* ctx, double* sum_v2,
+                                   double* min_v2, double* max_v2);
 
 /* ------------------------------------------------------ PM grid operator
  * Fourier transforms of real fields on a cubic lattice, as PlanFFT<Imag>

@@ -87,9 +87,11 @@ SIGNATURES = {
     "lf2_step": [c_void_p, c_void_p, c_double, c_double, c_void_p],
     "lf2_set_move_kernel": [c_void_p, c_int],
     "lf2_set_wait_limit": [c_void_p, c_i64, c_int],
+    "lf2_set_global_mass": [c_void_p, c_double],
     "lf2_last_move_kernel": [c_void_p, P(c_int)],
     "lf2_last_max_velocity": [c_void_p, c_void_p, c_int],
     "lf2_conservation": [c_void_p, P(c_double), P(c_double), P(c_double)],
+    "lf2_velocity_reductions": [c_void_p, P(c_double), P(c_double), P(c_double)],
     "lf2_pm_deposit": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p],
     "lf2_pm_gather": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_pm_kick_drift": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,

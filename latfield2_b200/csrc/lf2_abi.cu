@@ -6,6 +6,7 @@
 // lf2_deposit.cu and lf2_field.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -294,11 +295,12 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMalloc(&c->cap_alt, sizeof(int32_t) * nb) == cudaSuccess;
   ok = ok && cudaMalloc(&c->fill, sizeof(int32_t) * nb) == cudaSuccess;
   ok = ok && cudaMalloc(&c->brick_maxv2, sizeof(float) * nb) == cudaSuccess;
-  ok = ok && cudaMalloc(&c->brick_sums, sizeof(double) * 5 * nb) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->brick_sums, sizeof(double) * 7 * nb) == cudaSuccess;
   ok = ok && cudaMalloc(&c->stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->vmax_bits, sizeof(uint32_t)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->redep, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->repack, sizeof(int32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->diag, sizeof(unsigned long long) * 3) == cudaSuccess;
   ok = ok && cudaMalloc(&c->heap_top, sizeof(unsigned long long)) == cudaSuccess;
@@ -354,6 +356,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->work);
   cudaFree(c->flags);
   cudaFree(c->vmax_bits);
+  cudaFree(c->redep);
   cudaFree(c->repack);
   cudaFree(c->diag);
   cudaFree(c->heap_top);
@@ -450,6 +453,12 @@ lf2_status lf2_particles_set_pos(lf2_ctx* c, int64_t n, const void* pos3, const 
   return load_device(c, n, (const int32_t*)sc.p, (const float*)so.p, dvel, dmass, global_mass,
                      did);
 }
+
+// Whether the automatic kernel choice fuses the fixed-point deposit into the
+// pipelined pass.
+#ifndef LF2_FUSED_AUTO
+#define LF2_FUSED_AUTO 0
+#endif
 
 static lf2_status rebin_tail(lf2_ctx* c);
 
@@ -864,6 +873,12 @@ lf2_status lf2_deposit_symtensor_cicngp(lf2_ctx* c, lf2_field t) { return deposi
 lf2_status lf2_deposit_vector_cic(lf2_ctx* c, lf2_field v) { return deposit(c, v, 3, 3); }
 lf2_status lf2_deposit_vecvec_cic(lf2_ctx* c, lf2_field t) { return deposit(c, t, 4, 6); }
 
+// Whether the automatic kernel choice fuses the fixed-point deposit into the
+// pipelined pass.
+#ifndef LF2_FUSED_AUTO
+#define LF2_FUSED_AUTO 0
+#endif
+
 static lf2_status rebin_tail(lf2_ctx* c)
 {
   PhaseScope ps(c, PH_INSERT);
@@ -909,16 +924,55 @@ lf2_status lf2_step(lf2_ctx* c, lf2_field F, double dtau_kick, double dtau_drift
   if (F->comps != 3) return fail(c, LF2_ERR_ARG, "the kick field needs 3 components");
   MoveParams mp{(float)dtau_kick, (float)(dtau_drift / c->res)};
   LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
-  const bool pipe = c->move_kernel == 2 || (c->move_kernel == 0 && move_pipe_eligible(c, F->data));
-  if (c->move_kernel == 2 && !move_pipe_eligible(c, F->data))
+  if ((c->move_kernel == 2 || c->move_kernel == 3) && !move_pipe_eligible(c, F->data))
     return fail(c, LF2_ERR_UNSUPPORTED, "pipelined move needs n0 % 4 == 0, n >= 32, aligned F");
-  c->last_move_kernel = pipe ? 2 : 1;
+  if (c->move_kernel == 3 && !move_dep_eligible(c, F->data))
+    return fail(c, LF2_ERR_UNSUPPORTED, "the fused deposit needs the fixed-point mode and room "
+                                        "for its tile");
+  const bool pipe = c->move_kernel >= 2 || (c->move_kernel == 0 && move_pipe_eligible(c, F->data));
+  // the fixed-point scalar deposit fused into the pipelined pass (automatic
+  // when eligible, or kernel 3), finished by the movers' rim atomics and the
+  // rim fix-up; redone by the tile pass if a mover went past the rim
+  const bool fused = rho && valid_field(c, rho) && rho->comps == 1 && pipe &&
+                     (c->move_kernel == 3 || (c->move_kernel == 0 && LF2_FUSED_AUTO)) &&
+                     move_dep_eligible(c, F->data);
+  c->last_move_kernel = fused ? 3 : (pipe ? 2 : 1);
+  if (!fused) {
+    {
+      PhaseScope ps(c, PH_MOVE);
+      LF2_CUDA(c, pipe ? launch_move_pipe(c, F->data, mp, nullptr)
+                       : launch_move(c, F->data, true, true, mp));
+    }
+    LF2_TRY(rebin_tail(c));
+    if (rho) LF2_TRY(deposit(c, rho, 0, 1));
+    return LF2_OK;
+  }
+  LF2_TRY(ensure_spill(c, std::max(rim_store_slots(c), deposit_spill_slots(c, 1))));
+  LF2_CUDA(c, cudaMemsetAsync(c->redep, 0, sizeof(uint32_t), c->stream));
   {
     PhaseScope ps(c, PH_MOVE);
-    LF2_CUDA(c, pipe ? launch_move_pipe(c, F->data, mp) : launch_move(c, F->data, true, true, mp));
+    LF2_CUDA(c, launch_move_pipe(c, F->data, mp, rho->data));
+  }
+  {
+    PhaseScope ps(c, PH_FIXUP);
+    LF2_CUDA(c, launch_dep_movers(c));
+    LF2_CUDA(c, launch_fixup_rim(c, rho->data));
   }
   LF2_TRY(rebin_tail(c));
-  if (rho) LF2_TRY(deposit(c, rho, 0, 1));
+  {
+    PhaseScope ps(c, PH_DEPOSIT);  // runs only when redep was raised
+    LF2_CUDA(c, launch_deposit(c, 0, rho->data, 0, c->redep));
+    LF2_CUDA(c, launch_deposit(c, 0, rho->data, 1, c->redep));
+  }
+  return LF2_OK;
+}
+
+lf2_status lf2_set_global_mass(lf2_ctx* c, double mass)
+{
+  if (!c || !(mass > 0)) return LF2_ERR_ARG;
+  if (c->has_mass) return fail(c, LF2_ERR_ARG, "set_global_mass: the particles carry individual masses");
+  c->gmass = mass;
+  c->m_unit = mass;
   return LF2_OK;
 }
 
@@ -932,7 +986,7 @@ lf2_status lf2_set_wait_limit(lf2_ctx* c, int64_t cycles, int stall)
 
 lf2_status lf2_set_move_kernel(lf2_ctx* c, int which)
 {
-  if (!c || which < 0 || which > 2) return LF2_ERR_ARG;
+  if (!c || which < 0 || which > 3) return LF2_ERR_ARG;
   c->move_kernel = which;
   return LF2_OK;
 }
@@ -969,6 +1023,19 @@ lf2_status lf2_conservation(lf2_ctx* c, double* mass, double mom[3], double* max
   if (mom)
     for (int d = 0; d < 3; d++) mom[d] = c->h_stats[2 + d];
   if (max_v) *max_v = std::sqrt(c->h_stats[5]);
+  return LF2_OK;
+}
+
+lf2_status lf2_velocity_reductions(lf2_ctx* c, double* sum_v2, double* min_v2, double* max_v2)
+{
+  if (!c) return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_conservation(c));
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_stats, c->stats, sizeof(double) * 8, cudaMemcpyDeviceToHost,
+                              c->stream));
+  LF2_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (sum_v2) *sum_v2 = c->h_stats[6];
+  if (min_v2) *min_v2 = c->h_stats[7];
+  if (max_v2) *max_v2 = c->h_stats[5];
   return LF2_OK;
 }
 

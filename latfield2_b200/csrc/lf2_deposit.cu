@@ -88,8 +88,10 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
                                                          float* __restrict__ out,
                                                          uint64_t* __restrict__ spill,
                                                          const uint32_t* __restrict__ vmax_bits,
-                                                         uint32_t* flags)
+                                                         uint32_t* flags, const uint32_t* gate)
 {
+  // gate: run only when the word is set (the redo of a fused deposit)
+  if (gate && *gate == 0u) return;
   using P = Pass<KIND, PASS, ACC>;
   constexpr int NC = P::NC;
   constexpr int C = Comps<KIND>::value;
@@ -341,8 +343,9 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
 template <int KIND, int ACC>
 __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_scale,
                         const uint32_t* __restrict__ vmax_bits, float* __restrict__ out,
-                        uint32_t* flags)
+                        uint32_t* flags, const uint32_t* gate)
 {
+  if (gate && *gate == 0u) return;
   constexpr int C = Comps<KIND>::value;
   constexpr bool SIGNED = KIND != 0;
   const int64_t b = blockIdx.x;
@@ -443,7 +446,7 @@ __global__ void __launch_bounds__(256) k_vmax(StoreView v, uint32_t* vmax_bits, 
 }
 
 template <int KIND, int PASS, int ACC>
-cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
+cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp, const uint32_t* gate)
 {
   using P = Pass<KIND, PASS, ACC>;
   const size_t smem = P::smem();
@@ -452,12 +455,12 @@ cudaError_t tile_pass(lf2_ctx* c, float* out, const DepositParams& dp)
   if (e != cudaSuccess) return e;
   c->launches += 1;
   k_deposit<KIND, PASS, ACC><<<(unsigned)c->g.nbricks, P::THREADS, smem, c->stream>>>(
-      view(c), dp, out, c->spill, c->vmax_bits, c->flags);
+      view(c), dp, out, c->spill, c->vmax_bits, c->flags, gate);
   return cudaGetLastError();
 }
 
 template <int KIND, int ACC>
-cudaError_t run(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
+cudaError_t run(lf2_ctx* c, float* out, const DepositParams& dp, int stage, const uint32_t* gate)
 {
   const unsigned nb = (unsigned)c->g.nbricks;
   if (stage == 0) {
@@ -465,24 +468,24 @@ cudaError_t run(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
       cudaError_t e = launch_vmax(c);
       if (e != cudaSuccess) return e;
     }
-    cudaError_t e = tile_pass<KIND, 0, ACC>(c, out, dp);
+    cudaError_t e = tile_pass<KIND, 0, ACC>(c, out, dp, gate);
     if constexpr (KIND == 2 && ACC != ACC_PLAIN) {
-      if (e == cudaSuccess) e = tile_pass<KIND, 1, ACC>(c, out, dp);
+      if (e == cudaSuccess) e = tile_pass<KIND, 1, ACC>(c, out, dp, gate);
     }
     return e;
   }
   c->launches += 1;
   k_fixup<KIND, ACC><<<nb, 256, 0, c->stream>>>(c->g, c->spill, dp.fixed_scale, c->vmax_bits, out,
-                                                c->flags);
+                                                c->flags, gate);
   return cudaGetLastError();
 }
 
 template <int KIND>
-cudaError_t run_mode(lf2_ctx* c, float* out, const DepositParams& dp, int stage)
+cudaError_t run_mode(lf2_ctx* c, float* out, const DepositParams& dp, int stage, const uint32_t* gate)
 {
-  if (c->mode == LF2_DEPOSIT_FIXED64) return run<KIND, ACC_FIXED>(c, out, dp, stage);
-  if (c->mode == LF2_DEPOSIT_FP32_PLAIN) return run<KIND, ACC_PLAIN>(c, out, dp, stage);
-  return run<KIND, ACC_COMP>(c, out, dp, stage);
+  if (c->mode == LF2_DEPOSIT_FIXED64) return run<KIND, ACC_FIXED>(c, out, dp, stage, gate);
+  if (c->mode == LF2_DEPOSIT_FP32_PLAIN) return run<KIND, ACC_PLAIN>(c, out, dp, stage, gate);
+  return run<KIND, ACC_COMP>(c, out, dp, stage, gate);
 }
 
 }  // namespace
@@ -514,12 +517,12 @@ DepositParams deposit_params(const lf2_ctx* c)
   return dp;
 }
 
-cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage)
+cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage, const uint32_t* gate)
 {
   const DepositParams dp = deposit_params(c);
-  if (kind == 0) return run_mode<0>(c, out, dp, stage);
-  if (kind == 1) return run_mode<1>(c, out, dp, stage);
-  return run_mode<2>(c, out, dp, stage);
+  if (kind == 0) return run_mode<0>(c, out, dp, stage, gate);
+  if (kind == 1) return run_mode<1>(c, out, dp, stage, gate);
+  return run_mode<2>(c, out, dp, stage, gate);
 }
 
 }  // namespace lf2

@@ -86,57 +86,71 @@ __global__ void k_halo_fill(Geom g, int comps, T* __restrict__ data, int halo)
 
 // FP64 sums per brick: mass, m*vx, m*vy, m*vz and max |v|^2, then a fixed-order
 // reduction over bricks (one CTA) so the totals are reproducible.
+// Per brick, in a fixed order: mass, momentum (3), max |v|^2, sum |v|^2,
+// min |v|^2 (FP64; |v|^2 in double from the FP32 components, as the
+// reference's callbacks compute it).
+constexpr int NSUM = 7;
+
 __global__ void __launch_bounds__(256) k_brick_sums(StoreView v, double gmass, double* out)
 {
-  __shared__ double sh[5][256];
+  __shared__ double sh[NSUM][256];
   const int64_t b = blockIdx.x;
   const int64_t base = v.seg_start[b];
   const int cnt = LF2_BRICK_COUNT(v, b);
-  double s[5] = {0, 0, 0, 0, 0};
+  double s[NSUM] = {0, 0, 0, 0, 0, 0, INFINITY};
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
     const int64_t p = base + i;
     const double m = v.a.mass ? (double)v.a.mass[p] : gmass;
     const double vx = v.a.vx[p], vy = v.a.vy[p], vz = v.a.vz[p];
+    const double v2 = vx * vx + vy * vy + vz * vz;
     s[0] += m;
     s[1] += m * vx;
     s[2] += m * vy;
     s[3] += m * vz;
-    s[4] = fmax(s[4], vx * vx + vy * vy + vz * vz);
+    s[4] = fmax(s[4], v2);
+    s[5] += v2;
+    s[6] = fmin(s[6], v2);
   }
-  for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = s[k];
+  for (int k = 0; k < NSUM; k++) sh[k][threadIdx.x] = s[k];
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o) {
       for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
       sh[4][threadIdx.x] = fmax(sh[4][threadIdx.x], sh[4][threadIdx.x + o]);
+      sh[5][threadIdx.x] += sh[5][threadIdx.x + o];
+      sh[6][threadIdx.x] = fmin(sh[6][threadIdx.x], sh[6][threadIdx.x + o]);
     }
     __syncthreads();
   }
-  if (threadIdx.x < 5) out[b * 5 + threadIdx.x] = sh[threadIdx.x][0];
+  if (threadIdx.x < NSUM) out[b * NSUM + threadIdx.x] = sh[threadIdx.x][0];
 }
 
-__global__ void __launch_bounds__(1024) k_sum_bricks(int64_t nb, const double* __restrict__ in,
-                                                     double* stats)
+__global__ void __launch_bounds__(512) k_sum_bricks(int64_t nb, const double* __restrict__ in,
+                                                    double* stats)
 {
-  __shared__ double sh[5][1024];
+  __shared__ double sh[NSUM][512];
   const int t = threadIdx.x;
   const int64_t per = (nb + blockDim.x - 1) / blockDim.x;
   const int64_t lo = t * per, hi = min(nb, lo + per);
-  double s[5] = {0, 0, 0, 0, 0};
+  double s[NSUM] = {0, 0, 0, 0, 0, 0, INFINITY};
   for (int64_t b = lo; b < hi; b++) {
-    for (int k = 0; k < 4; k++) s[k] += in[b * 5 + k];
-    s[4] = fmax(s[4], in[b * 5 + 4]);
+    for (int k = 0; k < 4; k++) s[k] += in[b * NSUM + k];
+    s[4] = fmax(s[4], in[b * NSUM + 4]);
+    s[5] += in[b * NSUM + 5];
+    s[6] = fmin(s[6], in[b * NSUM + 6]);
   }
-  for (int k = 0; k < 5; k++) sh[k][t] = s[k];
+  for (int k = 0; k < NSUM; k++) sh[k][t] = s[k];
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (t < o) {
       for (int k = 0; k < 4; k++) sh[k][t] += sh[k][t + o];
       sh[4][t] = fmax(sh[4][t], sh[4][t + o]);
+      sh[5][t] += sh[5][t + o];
+      sh[6][t] = fmin(sh[6][t], sh[6][t + o]);
     }
     __syncthreads();
   }
-  if (t < 5) stats[1 + t] = sh[t][0];
+  if (t < NSUM) stats[1 + t] = sh[t][0];
 }
 
 }  // namespace
@@ -187,7 +201,7 @@ cudaError_t launch_conservation(lf2_ctx* c)
 {
   c->launches += 2;
   k_brick_sums<<<(unsigned)c->g.nbricks, 256, 0, c->stream>>>(view(c), c->gmass, c->brick_sums);
-  k_sum_bricks<<<1, 1024, 0, c->stream>>>(c->g.nbricks, c->brick_sums, c->stats);
+  k_sum_bricks<<<1, 512, 0, c->stream>>>(c->g.nbricks, c->brick_sums, c->stats);
   return cudaGetLastError();
 }
 

@@ -93,6 +93,7 @@ struct lf2_ctx {
   double* stats = nullptr;           // [8] device
   uint64_t* spill = nullptr;         // deposit shell store (8-byte slots)
   uint32_t* vmax_bits = nullptr;     // device: largest |v_i| (float bits), fixed-point deposits
+  uint32_t* redep = nullptr;         // device: the fused deposit must be redone by the tile pass
   float* stencil_partial = nullptr;  // per-CTA partial sums of the stencil weight gradient
   size_t spill_slots = 0;
   double* h_stats = nullptr;         // pinned [8]
@@ -161,13 +162,19 @@ cudaError_t launch_insert(lf2_ctx* c);
 cudaError_t launch_reduce_maxv(lf2_ctx* c);
 cudaError_t launch_maxv_to_device(lf2_ctx* c, double* dst);
 
-// lf2_move_pipe.cu
+// lf2_move_pipe.cu (rho != nullptr: the fixed-point scalar deposit fused in;
+// its rim store is c->spill, rim_store_slots(c) slots)
 bool move_pipe_eligible(const lf2_ctx* c, const float* F);
-cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp);
+bool move_dep_eligible(const lf2_ctx* c, const float* F);
+size_t rim_store_slots(const lf2_ctx* c);
+cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp, float* rho);
+cudaError_t launch_dep_movers(lf2_ctx* c);
+cudaError_t launch_fixup_rim(lf2_ctx* c, float* rho);
 
 // lf2_deposit.cu
 // stage 0: tile pass (k_deposit), stage 1: face fix-up (k_fixup)
-cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage);
+cudaError_t launch_deposit(lf2_ctx* c, int kind, float* out, int stage,
+                           const uint32_t* gate = nullptr);
 // largest |v_i| of the store into c->vmax_bits (fixed-point momentum/stress)
 cudaError_t launch_vmax(lf2_ctx* c);
 DepositParams deposit_params(const lf2_ctx* c);

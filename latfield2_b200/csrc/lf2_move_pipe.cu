@@ -39,8 +39,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <mutex>
 
+#include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
 namespace lf2 {
@@ -56,16 +58,24 @@ namespace {
 #ifndef LF2_PIPE_ITEMS
 #define LF2_PIPE_ITEMS 1
 #endif
-constexpr int PC_WARPS = LF2_PIPE_WARPS;         // consumer warps
-constexpr int PC_THREADS = PC_WARPS * 32;        // consumer threads
-constexpr int P_THREADS = PC_THREADS + 64;       // + producer warp + patch warp
+// The kernel is a template of its consumer warps (WARPS; each takes WSUB
+// slots of every chunk, CHUNK = WARPS * WSUB) plus a producer warp and a
+// patch warp.
 constexpr int W_ITEMS = LF2_PIPE_ITEMS;          // consecutive slots per lane
 constexpr int WSUB = 32 * W_ITEMS;               // slots per warp per chunk
-constexpr int CHUNK = PC_WARPS * WSUB;           // particles per chunk buffer
 constexpr int FX = 20;                           // padded tile row (floats)
 constexpr int FCOMP = FX * TILE * TILE;          // floats per component of a tile buffer
 constexpr uint32_t FBYTES = 3u * FCOMP * 4u;     // bytes one tile copy delivers
 constexpr int FSTRIDE = (FBYTES + 1023) & ~1023; // tile buffer stride in shared memory
+constexpr int FSTRIDE_DEP = (FBYTES + 127) & ~127; // the same in the fused-deposit layout
+// Fused deposit (lf2_step with the fixed-point scalar deposit): one split
+// fixed-point tile of the brick's (BRICK+1)^3 vertices, two 32-bit words per
+// vertex, between the vertex tiles and the chunk ring.
+constexpr int DEP_BYTES = 2 * TILE3 * 4;
+// Vertices of a brick's tile that movers from the neighbour bricks can reach
+// (a coordinate in {0, 1, e-1, e}): they go to the per-brick rim store, the
+// others (every coordinate in [2, e-2]) are final after the fused pass.
+constexpr int RIM = TILE3 - (BRICK - 3) * (BRICK - 3) * (BRICK - 3);
 #ifndef LF2_PIPE_FSTAGES
 #define LF2_PIPE_FSTAGES 2
 #endif
@@ -205,20 +215,50 @@ struct ChunkView {
   int64_t* id;
 };
 
-__device__ __forceinline__ ChunkView chunk_view(unsigned char* p, bool has_m)
+__device__ __forceinline__ ChunkView chunk_view(unsigned char* p, bool has_m, int chunk)
 {
   ChunkView c;
   c.key = reinterpret_cast<uint32_t*>(p);
-  c.ox = reinterpret_cast<float*>(p + 1 * CHUNK * 4);
-  c.oy = reinterpret_cast<float*>(p + 2 * CHUNK * 4);
-  c.oz = reinterpret_cast<float*>(p + 3 * CHUNK * 4);
-  c.vx = reinterpret_cast<float*>(p + 4 * CHUNK * 4);
-  c.vy = reinterpret_cast<float*>(p + 5 * CHUNK * 4);
-  c.vz = reinterpret_cast<float*>(p + 6 * CHUNK * 4);
-  c.m = reinterpret_cast<float*>(p + 7 * CHUNK * 4);
-  c.id = reinterpret_cast<int64_t*>(p + (has_m ? 8 : 7) * CHUNK * 4);
+  c.ox = reinterpret_cast<float*>(p + 1 * chunk * 4);
+  c.oy = reinterpret_cast<float*>(p + 2 * chunk * 4);
+  c.oz = reinterpret_cast<float*>(p + 3 * chunk * 4);
+  c.vx = reinterpret_cast<float*>(p + 4 * chunk * 4);
+  c.vy = reinterpret_cast<float*>(p + 5 * chunk * 4);
+  c.vz = reinterpret_cast<float*>(p + 6 * chunk * 4);
+  c.m = reinterpret_cast<float*>(p + 7 * chunk * 4);
+  c.id = reinterpret_cast<int64_t*>(p + (has_m ? 8 : 7) * chunk * 4);
   return c;
 }
+
+// Canonical coordinate of a tile vertex in the rim store layout: e -> BRICK,
+// e - 1 -> BRICK - 1 (when >= 2), so that bricks with e < BRICK share it.
+__host__ __device__ inline int rim_canon(int t, int e)
+{
+  return t == e ? BRICK : (t == e - 1 && t >= 2 ? BRICK - 1 : t);
+}
+__host__ __device__ inline bool rim_layer(int u) { return u < 2 || u >= BRICK - 1; }
+__host__ __device__ inline int rim_slot(int u) { return u < 2 ? u : u - (BRICK - 3); }
+// Index of a rim vertex (canonical coordinates): the two z slab pairs
+// (4 TILE^2), then the y slab pairs between them (4 (BRICK-3) TILE), then the
+// x slab pairs between those (4 (BRICK-3)^2): 2716 slots for BRICK = 16.
+__host__ __device__ inline int rim_index(int u0, int u1, int u2)
+{
+  constexpr int I = BRICK - 3;
+  if (rim_layer(u2)) return rim_slot(u2) * TILE * TILE + u1 * TILE + u0;
+  if (rim_layer(u1)) return 4 * TILE * TILE + (rim_slot(u1) * I + (u2 - 2)) * TILE + u0;
+  return 4 * TILE * TILE + 4 * I * TILE + (rim_slot(u0) * I + (u2 - 2)) * I + (u1 - 2);
+}
+static_assert(4 * TILE * TILE + 4 * (BRICK - 3) * TILE + 4 * (BRICK - 3) * (BRICK - 3) == RIM,
+              "rim slab sizes");
+
+// Outputs of the fused deposit.
+struct DepOut {
+  float* rho;        // density (private vertices written by the fused pass)
+  uint64_t* rim;     // [nbricks * RIM] integer sums of the rim vertices
+  float scale;       // 2^-32 * unit mass / res^3
+  float inv_unit;    // 1 / unit mass (per-particle masses)
+  int split_max;     // bricks up to this count accumulate in two 32-bit words
+};
 
 // Bounded wait by lane 0 of the calling warp; the outcome is broadcast so the
 // warp stays together, and every lane then acquires the completed phase.
@@ -232,26 +272,33 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, uint32
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(P_THREADS, 1)
+template <int WARPS, bool DEP>
+__global__ void __launch_bounds__(WARPS * 32 + 64, 1)
     k_move_pipe(const __grid_constant__ CUtensorMap tmF, StoreView v, const float* __restrict__ F,
                 MoveParams mp, PartArrays mov, unsigned long long* mov_count,
                 float* __restrict__ brick_maxv2, uint32_t* flags, int* work, int nst,
-                int stage_bytes, long long wait_limit, int stall)
+                int stage_bytes, long long wait_limit, int stall, DepOut dep)
 {
+  constexpr int CHUNK = WARPS * WSUB;            // particles per chunk buffer
+  constexpr int PC_WARPS = WARPS;                // consumer warps
+  constexpr int FST = DEP ? FSTRIDE_DEP : FSTRIDE;
+  constexpr uintptr_t ALIGN = DEP ? 127 : 1023;
   extern __shared__ unsigned char dyn[];
   // tma_f: tile copy landed (or the end of the bricks); full_f: tile
   // patched and ready for the consumers; empty_f: all consumer warps are
   // done with the brick; full_p / empty_p: chunk ring.
   __shared__ uint64_t full_f[2], tma_f[2], empty_f[2], full_p[MAX_STAGES], empty_p[MAX_STAGES];
   __shared__ uint64_t never;  // completed by nothing: the consumers' stall of the timeout tests
+  __shared__ uint64_t dep_in, dep_clean;  // fused deposit: all deposits of the brick in; tile clean
   __shared__ Job job[2];
   __shared__ int s_cursor[2];     // stayers written back so far (per tile buffer)
   __shared__ int s_done[2];       // consumer warps finished with the brick
   __shared__ unsigned s_maxv2[2]; // max |v|^2 of the brick (bits of a non-negative float)
 
   unsigned char* sm = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  unsigned char* pbuf = sm + NF * FSTRIDE;
+      (reinterpret_cast<uintptr_t>(dyn) + ALIGN) & ~ALIGN);
+  uint32_t* dtile = reinterpret_cast<uint32_t*>(sm + NF * FST);  // DEP: [lo | hi] x TILE3
+  unsigned char* pbuf = sm + NF * FST + (DEP ? DEP_BYTES : 0);
 
   const Geom& g = v.g;
   const bool has_m = v.a.mass != nullptr, has_id = v.a.id != nullptr;
@@ -265,8 +312,12 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     }
     for (int s = 0; s < nst; s++) mbar_init(&full_p[s], 1), mbar_init(&empty_p[s], PC_WARPS);
     mbar_init(&never, 1);
+    mbar_init(&dep_in, PC_WARPS);
+    mbar_init(&dep_clean, PC_WARPS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (DEP)
+    for (int t = threadIdx.x; t < 2 * TILE3; t += blockDim.x) dtile[t] = 0u;
   __syncthreads();
 
   if (warp == PC_WARPS) {
@@ -310,7 +361,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           b = -1;
           return;
         }
-        if (cnt > 0) return;
+        if (cnt > 0 || DEP) return;  // the fused deposit writes empty bricks too
         brick_maxv2[b] = 0.0f;
       }
     };
@@ -329,10 +380,15 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       s_cursor[fs] = 0;
       s_done[fs] = 0;
       s_maxv2[fs] = 0u;
+      if (cnt == 0) {  // an empty brick (fused deposit): no tile to load
+        tl_busy[fs] = false;
+        mbar_arrive(&tma_f[fs]);
+        return;
+      }
       int bx, by, bz;
       brick_coords(g, b, bx, by, bz);
       mbar_arrive_tx(&tma_f[fs], FBYTES);
-      tma_tile4(sm + fs * FSTRIDE, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
+      tma_tile4(sm + fs * FST, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
     };
     // tile buffer of the next post free?
     auto tile_free = [&]() {
@@ -372,7 +428,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         const int n = min(CHUNK, ccnt - c0);
         const uint32_t n4 = (uint32_t)((n + 3) & ~3);  // segments hold a multiple of 4 slots
         const uint32_t bytes = n4 * 4u * (7u + (has_m ? 1u : 0u)) + (has_id ? n4 * 8u : 0u);
-        const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
+        const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m, CHUNK);
         const long long p = cbase + c0;
         st_busy[ps] = true;
         st_par[ps] = ppar;
@@ -429,8 +485,8 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
                 ez = brick_extent(g.n[2], bz);
       const bool wx = x0 + ex == g.n[0], wy = y0 + ey == g.n[1], wz = z0 + ez == g.n[2];
-      if (wx || wy || wz) {
-        float* ft = reinterpret_cast<float*>(sm + fs * FSTRIDE);
+      if (jb.cnt > 0 && (wx || wy || wz)) {
+        float* ft = reinterpret_cast<float*>(sm + fs * FST);
         constexpr int NP = TILE * TILE, NT = 3 * NP, U = 7;  // U loads in flight per lane
         for (int t0 = lane; t0 < NT; t0 += 32 * U) {
           float val[U][3];
@@ -495,11 +551,12 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     if (jb.b < 0) return;
     const int64_t b = jb.b;
     const int cnt = jb.cnt;
-    const float* ft = reinterpret_cast<const float*>(sm + fs * FSTRIDE);
+    const float* ft = reinterpret_cast<const float*>(sm + fs * FST);
     int bx, by, bz;
     brick_coords(g, b, bx, by, bz);
     const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
     const uint32_t key0 = pack_key(g, x0, y0, z0);  // a harmless key for empty lanes
+    const bool dsplit = DEP && cnt <= dep.split_max;  // fused deposit: split 32-bit sums
 
     float maxv2 = 0.0f;
     for (int c0 = 0; c0 < cnt; c0 += CHUNK) {
@@ -509,7 +566,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         cps = 0;
         cpar ^= 1u;
       }
-      const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m);
+      const ChunkView cv = chunk_view(pbuf + (size_t)ps * stage_bytes, has_m, CHUNK);
       const int n = min(CHUNK, cnt - c0);
       const int i0 = warp * WSUB + W_ITEMS * lane;
       uint32_t key[W_ITEMS];
@@ -618,6 +675,31 @@ __global__ void __launch_bounds__(P_THREADS, 1)
           v.a.vz[q] = vz[j];
           if (has_m) v.a.mass[q] = m[j];
           if (has_id) v.a.id[q] = id[j];
+          if constexpr (DEP) {
+            // the stayer's fixed-point CIC weights at its new position into
+            // the brick's tile (the arithmetic of k_deposit, order-free sums)
+            int nx, ny, nz;
+            unpack_key(g, key[j], nx, ny, nz);
+            const int t0 = (nx - x0) + TILE * ((ny - y0) + TILE * (nz - z0));
+            const uint64_t mq = has_m ? mass_q(m[j], dep.inv_unit, flags) : 0;
+            const uint32_t ux = weight_q(ox[j]), uy = weight_q(oy[j]), uz = weight_q(oz[j]);
+            const uint32_t qx[2] = {(1u << 31) - ux, ux};
+            const uint32_t qy[2] = {(1u << 31) - uy, uy};
+            const uint32_t qz[2] = {(1u << 31) - uz, uz};
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+              uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+              if (has_m) w = (w * mq + (1ull << 23)) >> 24;
+              const int t = t0 + cx + cy * TILE + cz * TILE * TILE;
+              if (dsplit) {
+                atomicAdd(&dtile[t], (uint32_t)(w & 0xffffu));
+                atomicAdd(&dtile[TILE3 + t], (uint32_t)(w >> 16));
+              } else {
+                atomicAdd(reinterpret_cast<unsigned long long*>(dtile) + t, (unsigned long long)w);
+              }
+            }
+          }
         } else {
           const int64_t q = mq++;
           mov.key[q] = key[j];
@@ -649,7 +731,128 @@ __global__ void __launch_bounds__(P_THREADS, 1)
       }
     }
     __syncwarp();
+    if constexpr (DEP) {
+      // Every consumer warp's deposits of the brick are in the tile once all
+      // have arrived; then each flushes a share of the vertices (private ones
+      // to the density, the rim to the rim store) and clears them, and the
+      // tile is clean for the next brick once all have arrived again.  Both
+      // waits are bounded like the others.
+      const uint32_t par = (uint32_t)(fk & 1);
+      if (lane == 0) mbar_arrive(&dep_in);
+      if (!warp_wait(&dep_in, par, flags, lane, wait_limit)) return;
+      const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
+                ez = brick_extent(g.n[2], bz);
+      uint64_t* rs = dep.rim + (size_t)b * RIM;
+      unsigned long long* d64 = reinterpret_cast<unsigned long long*>(dtile);
+      for (int t = warp * 32 + lane; t < TILE3; t += PC_WARPS * 32) {
+        uint64_t q;
+        if (dsplit) {
+          q = (uint64_t)dtile[t] + ((uint64_t)dtile[TILE3 + t] << 16);
+          dtile[t] = 0u;
+          dtile[TILE3 + t] = 0u;
+        } else {
+          q = d64[t];
+          d64[t] = 0ull;
+        }
+        const int i = t % TILE, jj = (t / TILE) % TILE, k = t / (TILE * TILE);
+        if (i > ex || jj > ey || k > ez) continue;
+        if (i >= 2 && i <= ex - 2 && jj >= 2 && jj <= ey - 2 && k >= 2 && k <= ez - 2) {
+          if ((long long)q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+          dep.rho[site_index(g, x0 + i, y0 + jj, z0 + k)] =
+              __fmul_rn(__ll2float_rn((long long)q), dep.scale);
+        } else {
+          rs[rim_index(rim_canon(i, ex), rim_canon(jj, ey), rim_canon(k, ez))] = q;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&dep_clean);
+      if (!warp_wait(&dep_clean, par, flags, lane, wait_limit)) return;
+    }
     fk++;
+  }
+}
+
+// Fused deposit, second half: the movers of the last pass (the mover buffer)
+// add their fixed-point CIC weights to the rim store of the brick they moved
+// into, with 64-bit atomics (integer sums, so the order does not matter).  A
+// mover that moved more than one cell into its brick reaches a private
+// vertex there, which the fused pass has already written: it raises `redep`,
+// and the whole deposit is then redone by the tile and fix-up kernels.
+__global__ void __launch_bounds__(256) k_dep_movers(Geom g, PartArrays mov,
+                                                    const unsigned long long* __restrict__ mov_count,
+                                                    uint64_t* __restrict__ rim, float inv_unit,
+                                                    uint32_t* redep, uint32_t* flags)
+{
+  const int64_t nm = (int64_t)*mov_count;
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    int x, y, z;
+    unpack_key(g, mov.key[m], x, y, z);
+    if (x >= g.n[0] || y >= g.n[1] || z >= g.n[2]) continue;  // flagged by k_insert
+    const int bx = x / BRICK, by = y / BRICK, bz = z / BRICK;
+    const int e[3] = {brick_extent(g.n[0], bx), brick_extent(g.n[1], by), brick_extent(g.n[2], bz)};
+    const int l[3] = {x - bx * BRICK, y - by * BRICK, z - bz * BRICK};
+    const int64_t b = (int64_t)bx + (int64_t)g.nb[0] * ((int64_t)by + (int64_t)g.nb[1] * bz);
+    const uint64_t mq = mov.mass ? mass_q(mov.mass[m], inv_unit, flags) : 0;
+    const uint32_t ux = weight_q(mov.ox[m]), uy = weight_q(mov.oy[m]), uz = weight_q(mov.oz[m]);
+    const uint32_t qx[2] = {(1u << 31) - ux, ux};
+    const uint32_t qy[2] = {(1u << 31) - uy, uy};
+    const uint32_t qz[2] = {(1u << 31) - uz, uz};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+      const int u0 = rim_canon(l[0] + cx, e[0]), u1 = rim_canon(l[1] + cy, e[1]),
+                u2 = rim_canon(l[2] + cz, e[2]);
+      if (!(rim_layer(u0) || rim_layer(u1) || rim_layer(u2))) {
+        atomicOr(redep, 1u);
+        continue;
+      }
+      uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+      if (mov.mass) w = (w * mq + (1ull << 23)) >> 24;
+      atomicAdd(reinterpret_cast<unsigned long long*>(rim) + (size_t)b * RIM + rim_index(u0, u1, u2),
+                (unsigned long long)w);
+    }
+  }
+}
+
+// Fused deposit, last part: every owned vertex of a brick that movers can
+// reach (a coordinate in {0, 1, e-1}) is its own rim value plus, for every
+// non-empty subset S of the dims where its coordinate is 0, the rim value of
+// the lower neighbour across S at coordinate e' (canonical BRICK) in those
+// dims, summed in a fixed order; then converted like the tile pass.
+__global__ void __launch_bounds__(256) k_fixup_rim(Geom g, const uint64_t* __restrict__ rim,
+                                                   float scale, float* __restrict__ out,
+                                                   uint32_t* flags)
+{
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int e[3] = {brick_extent(g.n[0], bx), brick_extent(g.n[1], by), brick_extent(g.n[2], bz)};
+  const int bm[3] = {bx ? bx - 1 : g.nb[0] - 1, by ? by - 1 : g.nb[1] - 1, bz ? bz - 1 : g.nb[2] - 1};
+  const int bc[3] = {bx, by, bz};
+  const int nown = e[0] * e[1] * e[2];
+  for (int f = threadIdx.x; f < nown; f += blockDim.x) {
+    const int q[3] = {f % e[0], (f / e[0]) % e[1], f / (e[0] * e[1])};
+    if (q[0] >= 2 && q[0] <= e[0] - 2 && q[1] >= 2 && q[1] <= e[1] - 2 && q[2] >= 2 &&
+        q[2] <= e[2] - 2)
+      continue;  // private: written by the fused pass
+    const int zmask = (q[0] == 0 ? 1 : 0) | (q[1] == 0 ? 2 : 0) | (q[2] == 0 ? 4 : 0);
+    long long sum = 0;
+    for (int s = 0; s < 8; s++) {
+      if ((s & zmask) != s) continue;
+      int nb3[3], u[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const bool lower = (s >> d) & 1;
+        nb3[d] = lower ? bm[d] : bc[d];
+        u[d] = lower ? BRICK : rim_canon(q[d], e[d]);
+      }
+      const int64_t nb = (int64_t)nb3[0] + (int64_t)g.nb[0] * ((int64_t)nb3[1] + (int64_t)g.nb[1] * nb3[2]);
+      sum += (long long)rim[(size_t)nb * RIM + rim_index(u[0], u[1], u[2])];
+    }
+    if (sum < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+    out[site_index(g, bc[0] * BRICK + q[0], bc[1] * BRICK + q[1], bc[2] * BRICK + q[2])] =
+        __fmul_rn(__ll2float_rn(sum), scale);
   }
 }
 
@@ -673,12 +876,39 @@ EncodeTiledFn encode_fn()
   return fn;
 }
 
-size_t stage_bytes_for(const lf2_ctx* c)
+#ifndef LF2_PIPE_DEP_WARPS
+#define LF2_PIPE_DEP_WARPS 30
+#endif
+constexpr int DEP_WARPS = LF2_PIPE_DEP_WARPS;  // consumer warps of the fused-deposit kernel
+constexpr int STATIC_SMEM = 256;               // the kernel's static shared memory, rounded up
+
+size_t stage_bytes_for(const lf2_ctx* c, int warps)
 {
-  return (size_t)CHUNK * (28 + (c->has_mass ? 4 : 0) + (c->has_id ? 8 : 0));
+  return (size_t)warps * WSUB * (28 + (c->has_mass ? 4 : 0) + (c->has_id ? 8 : 0));
+}
+
+// Chunk buffers that fit beside the vertex tiles (and the deposit tile).
+int stages_for(const lf2_ctx* c, bool dep)
+{
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const size_t sb = stage_bytes_for(c, dep ? DEP_WARPS : LF2_PIPE_WARPS);
+  const size_t fixed = dep ? 128 + NF * (size_t)FSTRIDE_DEP + DEP_BYTES + STATIC_SMEM
+                           : 1024 + NF * (size_t)FSTRIDE + 2048;
+  int nst = (int)(((size_t)optin > fixed ? (size_t)optin - fixed : 0) / sb);
+  return nst > MAX_STAGES ? MAX_STAGES : nst;
 }
 
 }  // namespace
+
+size_t rim_store_slots(const lf2_ctx* c) { return (size_t)c->g.nbricks * RIM; }
+
+// Whether lf2_step can fuse the fixed-point scalar deposit into the
+// pipelined pass: the deposit tile and two chunk buffers must fit.
+bool move_dep_eligible(const lf2_ctx* c, const float* F)
+{
+  return move_pipe_eligible(c, F) && c->mode == LF2_DEPOSIT_FIXED64 && stages_for(c, true) >= 2;
+}
 
 // Whether lf2_step's fused move can take the pipelined kernel: a 4-D tensor
 // map needs 16-byte aligned rows (n0 % 4 == 0) and base, and the lattice is
@@ -691,7 +921,7 @@ bool move_pipe_eligible(const lf2_ctx* c, const float* F)
   return encode_fn() != nullptr;
 }
 
-cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp)
+cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp, float* rho)
 {
   static_assert(sizeof(CUtensorMap) <= sizeof(c->tmap_bytes), "tensor map storage");
   CUtensorMap* map = reinterpret_cast<CUtensorMap*>(c->tmap_bytes);
@@ -713,23 +943,50 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp)
     }
     c->tmap_src = F;
   }
-  int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
-  const size_t sb = stage_bytes_for(c);
-  const size_t fixed = 1024 + NF * (size_t)FSTRIDE + 2048;  // alignment slack, tiles, static
-  int nst = (int)(((size_t)optin > fixed ? (size_t)optin - fixed : 0) / sb);
-  nst = nst > MAX_STAGES ? MAX_STAGES : nst;
+  const bool dep = rho != nullptr;
+  const int warps = dep ? DEP_WARPS : LF2_PIPE_WARPS;
+  const size_t sb = stage_bytes_for(c, warps);
+  const int nst = stages_for(c, dep);
   if (nst < 2) return cudaErrorInvalidConfiguration;
-  const size_t smem = 1024 + NF * (size_t)FSTRIDE + (size_t)nst * sb;
-  cudaError_t e = cudaFuncSetAttribute(k_move_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  const size_t smem = dep ? 128 + NF * (size_t)FSTRIDE_DEP + DEP_BYTES + (size_t)nst * sb
+                          : 1024 + NF * (size_t)FSTRIDE + (size_t)nst * sb;
+  DepOut d{};
+  if (dep) {
+    const double vol = c->res * c->res * c->res;
+    d.rho = rho;
+    d.rim = c->spill;
+    d.scale = (float)(std::ldexp(1.0, -32) * c->m_unit / vol);
+    d.inv_unit = (float)(1.0 / c->m_unit);
+    d.split_max = split_max<false>(c->has_mass);
+  }
+  auto kern = dep ? k_move_pipe<DEP_WARPS, true> : k_move_pipe<LF2_PIPE_WARPS, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(c->work, 0, sizeof(int), c->stream);
   if (e != cudaSuccess) return e;
   c->launches += 1;
-  k_move_pipe<<<c->num_sms, P_THREADS, smem, c->stream>>>(
+  kern<<<c->num_sms, warps * 32 + 64, smem, c->stream>>>(
       *map, view(c), F, mp, c->mov, c->mov_count, c->brick_maxv2, c->flags, c->work, nst, (int)sb,
-      c->wait_cycles > 0 ? (long long)c->wait_cycles : WAIT_CYCLES, c->wait_stall);
+      c->wait_cycles > 0 ? (long long)c->wait_cycles : WAIT_CYCLES, c->wait_stall, d);
+  return cudaGetLastError();
+}
+
+// The movers' part and the rim fix-up of the fused deposit (after the fused
+// pass; `redep` cleared before it).
+cudaError_t launch_dep_movers(lf2_ctx* c)
+{
+  c->launches += 1;
+  k_dep_movers<<<c->num_sms * 4, 256, 0, c->stream>>>(c->g, c->mov, c->mov_count, c->spill,
+                                                      (float)(1.0 / c->m_unit), c->redep, c->flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixup_rim(lf2_ctx* c, float* rho)
+{
+  const double vol = c->res * c->res * c->res;
+  c->launches += 1;
+  k_fixup_rim<<<(unsigned)c->g.nbricks, 256, 0, c->stream>>>(
+      c->g, c->spill, (float)(std::ldexp(1.0, -32) * c->m_unit / vol), rho, c->flags);
   return cudaGetLastError();
 }
 

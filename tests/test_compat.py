@@ -139,3 +139,54 @@ def test_restart_through_particles_save_and_load(cuda, tmp_path):
                        timeout=300)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
     assert os.path.exists(tmp_path / "run.lf2c")
+
+
+def test_outputs_demo_builds_against_the_header(tmp_path):
+    import build_demo
+    for single in (False, True):
+        out = str(tmp_path / ("outputs_single" if single else "outputs_double"))
+        assert os.path.exists(build_demo.build(out, single, "outputs_demo.cpp"))
+
+
+@pytest.mark.gpu
+def test_update_vel_outputs_mapping_overload_and_oset(cuda, tmp_path):
+    """tests/compat/outputs_demo.cpp: updateVel's SUM / MIN / MAX outputs of
+    the kick's |v|^2 (FP64 on the GPU) against FP64 sums of the Python
+    binding's velocities; the mappingClass overload kicks like the plain one;
+    a projection with the part_info mass at its offset, doubled, gives twice
+    the density bit for bit; offsets the GPU store does not hold are
+    refused."""
+    import torch
+    import build_demo
+    import latfield2_b200 as L
+    exe = build_demo.build(str(tmp_path / "outputs"), False, "outputs_demo.cpp")
+    out = str(tmp_path / "outputs.bin")
+    n, npart = 32, 20000
+    r = subprocess.run([exe, str(n), str(npart), out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    hdr, id0, pos0, vel0, Fv, rho, rho2, B = _read(out)
+    dtau = hdr[2]
+    assert int(hdr[10]) == 2  # both bad offsets refused
+    ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64)
+    ctx.set_positions(pos0.reshape(-1, 3), vel0.reshape(-1, 3), global_mass=1.0 / npart,
+                      ids=id0.astype(np.int64))
+    Fi = torch.from_numpy(np.ascontiguousarray(
+        Fv.reshape(n, n, n, 3).transpose(3, 0, 1, 2)).astype(np.float32)).cuda()
+    F = ctx.field(3, Fi)
+    sums = []
+    for k in range(2):
+        mv = ctx.gather_kick(F, dtau, want_max_v=True)
+        assert mv == hdr[3 + k]
+        _, vel, _ = ctx.get_positions(ids=True)
+        v2 = np.sum(vel.astype(np.float64) ** 2, axis=1)
+        sums.append((v2.sum(), v2.min(), v2.max()))
+    assert hdr[5] == pytest.approx(sums[0][0], rel=1e-12)
+    assert hdr[6] == sums[0][1] and hdr[7] == sums[0][2]
+    assert hdr[8] == sums[1][2] and hdr[9] == pytest.approx(sums[1][0], rel=1e-12)
+    d = ctx.field(1)
+    ctx.deposit_scalar(d)
+    np.testing.assert_array_equal(d.export(0, np.float64).reshape(-1), rho)
+    np.testing.assert_array_equal(rho2, 2 * rho)
+    v = ctx.field(3)
+    ctx.deposit_vector(v)
+    np.testing.assert_array_equal(v.export(0, np.float64).reshape(-1), B)

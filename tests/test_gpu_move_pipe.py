@@ -168,3 +168,52 @@ def test_a_wait_that_runs_out_is_reported_and_the_context_recovers(cuda):
     np.testing.assert_array_equal(got["vel"], v)
     np.testing.assert_array_equal(got["cell"], c)
     np.testing.assert_array_equal(got["off"], o)
+
+
+@pytest.mark.parametrize("n,npart,clustered,with_mass,dtau", [
+    ((32, 32, 32), 30000, False, False, 0.2),
+    ((48, 40, 36), 50000, False, True, 0.2),
+    ((64, 64, 64), 200000, True, False, 0.2),
+    ((64, 48, 80), 120000, True, True, 0.2),
+    ((32, 32, 32), 30000, False, False, 60.0),  # particles cross several cells: the redo path
+])
+def test_fused_deposit_equals_the_separate_deposit_and_the_oracle(cuda, n, npart, clustered,
+                                                                   with_mass, dtau):
+    """lf2_step with the fixed-point deposit fused into the pipelined pass
+    (kernel 3) against the pipelined pass followed by the tile deposit
+    (kernel 2): the same particles and the same density bits, step after step,
+    and the oracle's integer deposit of the oracle's particles."""
+    import torch
+    cell, off, vel = small_case(n, npart, seed=202, vel_sigma=0.03, clustered=clustered)
+    rng = np.random.default_rng(6)
+    mass = (1.0 + 0.1 * rng.random(npart)).astype(np.float32) / npart if with_mass else None
+    F = rng.standard_normal((3, n[2], n[1], n[0])).astype(np.float32)
+    a, b = _pair(n, cell, off, vel, mass)
+    a.set_move_kernel(3)
+    b.set_move_kernel(2)
+    Ft = torch.from_numpy(F).cuda()
+    Fa, Fb = a.field(3, Ft), b.field(3, Ft)
+    ra, rb = a.field(1), b.field(1)
+    res = 1.0 / n[0]
+    c, o, v = cell.copy(), off.copy(), vel.copy()
+    for _ in range(3):
+        a.step(Fa, 0.05, dtau, ra)
+        b.step(Fb, 0.05, dtau, rb)
+        assert a.last_move_kernel() == 3 and b.last_move_kernel() == 2
+        v = O.state_kick(n, c, o, v, F, np.float32(0.05))
+        c, o, _ = O.state_drift(n, c, o, v, np.float32(dtau / res))
+        np.testing.assert_array_equal(ra.export_internal(), rb.export_internal())
+    a.synchronize()
+    b.synchronize()
+    ga = by_id(a.get_particles(ids=True))
+    np.testing.assert_array_equal(ga["cell"], c)
+    np.testing.assert_array_equal(ga["off"], o)
+    np.testing.assert_array_equal(ga["vel"], v)
+    unit = 1.0 / npart
+    mrel = None
+    if with_mass:
+        unit = float(np.sum(mass.astype(np.float64)) / npart)
+        mrel = (mass * np.float32(1.0 / unit)).astype(np.float32)
+    exact = O.fixed_to_f32(O.state_deposit_fixed(n, c, o, mrel),
+                           np.float32(2.0 ** -32 * unit / res ** 3))
+    np.testing.assert_array_equal(ra.export_internal().reshape(-1), exact)
