@@ -59,6 +59,9 @@
 #include <vector>
 
 #include "lf2gpu.h"
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
 
 namespace LATfield2 {
 
@@ -826,6 +829,134 @@ bool is_simple_move(F)
 }
 }  // namespace lf2detail
 
+#ifdef __CUDACC__
+// ------------------------------------------------------- user physics on the GPU
+// updateVel and moveParticles also take a functor whose operator() is a
+// __device__ function with the reference's callback arguments
+// (LATfield2_Particles.hpp:752-893, :1810-2803):
+//   Real operator()(double dtau, double res, part* p, double* frac, part_info info,
+//                   F** fields, S* sites, int nfields, double* params,
+//                   double* outputs, int noutputs) const      (kick; returns |v|^2)
+//   void operator()(... same ...) const                       (move)
+// F and S are lf2dev::Field and lf2dev::Site: (*fields[i])(sites[i] + dir, c),
+// sites[i] - dir, sites[i].coord(d) work as on the reference's Field and Site
+// (periodic; the GPU field, FP32).  The particle is a copy of `part` filled
+// from the GPU store (ID, pos in box units, vel, mass for types with one);
+// a kick may change vel, a move pos (any distance: the particles are rebinned
+// afterwards).  params must be memory the GPU can read (device, managed or
+// mapped pinned memory).  Per-particle outputs are reduced with reduce_type
+// (SUM, MIN, MAX) into output.  Compile the user's file with nvcc.
+namespace lf2dev {
+struct Site {
+  int x[3];
+  int n[3];
+  __host__ __device__ Site operator+(int d) const
+  {
+    Site s = *this;
+    s.x[d] = x[d] + 1 == n[d] ? 0 : x[d] + 1;
+    return s;
+  }
+  __host__ __device__ Site operator-(int d) const
+  {
+    Site s = *this;
+    s.x[d] = x[d] == 0 ? n[d] - 1 : x[d] - 1;
+    return s;
+  }
+  __host__ __device__ int coord(int d) const { return x[d]; }
+  __host__ __device__ long index() const { return x[0] + (long)n[0] * (x[1] + (long)n[1] * x[2]); }
+};
+struct Field {
+  float* data;
+  int comps;
+  long nsites;
+  __device__ float& operator()(const Site& s, int c = 0) const { return data[c * nsites + s.index()]; }
+  __host__ __device__ int components() const { return comps; }
+};
+constexpr int MAX_FIELDS = 8;
+constexpr int MAX_OUTPUTS = 8;
+
+__device__ inline void reduce_out(double* dst, int type, double v)
+{
+  if (type & (SUM | SUM_LOCAL)) {
+    atomicAdd(dst, v);
+    return;
+  }
+  const bool mn = (type & (MIN | MIN_LOCAL)) != 0;
+  if (!mn && !(type & (MAX | MAX_LOCAL))) return;
+  unsigned long long* a = reinterpret_cast<unsigned long long*>(dst);
+  unsigned long long old = *a;
+  for (;;) {  // compare-and-swap: every failed attempt means another thread progressed
+    const double cur = __longlong_as_double((long long)old);
+    if (mn ? !(v < cur) : !(v > cur)) return;
+    const unsigned long long got = atomicCAS(a, old, (unsigned long long)__double_as_longlong(v));
+    if (got == old) return;
+    old = got;
+  }
+}
+
+template <class T>
+__device__ inline void set_mass(T& p, float m, std::true_type)
+{
+  p.mass = m;
+}
+template <class T>
+__device__ inline void set_mass(T&, float, std::false_type)
+{
+}
+
+template <class Fn, class part, class part_info, bool MOVE>
+__global__ void k_user(Fn fn, int64_t np, int32_t* cell, float* off3, float* vel3, const float* mass,
+                       const int64_t* id, part_info info, double dtau, double res, int n0, int n1,
+                       int n2, const Field* fields, int nfields, double* params, int noutput,
+                       const int* red, double* red_out, unsigned long long* maxv2)
+{
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int c = cell[p];
+    const int xyz[3] = {c % n0, (c / n0) % n1, c / (n0 * n1)};
+    part q{};
+    q.ID = (long)id[p];
+    double frac[3];
+    for (int d = 0; d < 3; d++) {
+      frac[d] = (double)off3[3 * p + d];
+      q.pos[d] = (Real)(((double)xyz[d] + frac[d]) * res);
+      q.vel[d] = (Real)vel3[3 * p + d];
+    }
+    set_mass(q, mass ? mass[p] : 0.0f, lf2detail::has_mass<part>());
+    Site s[MAX_FIELDS];
+    Field* fp[MAX_FIELDS];
+    for (int f = 0; f < nfields; f++) {
+      s[f] = Site{{xyz[0], xyz[1], xyz[2]}, {n0, n1, n2}};
+      fp[f] = const_cast<Field*>(&fields[f]);
+    }
+    double outs[MAX_OUTPUTS];
+    for (int i = 0; i < noutput; i++) outs[i] = 0.0;
+    if constexpr (MOVE) {
+      fn(dtau, res, &q, frac, info, fp, s, nfields, params, outs, noutput);
+      // the new position back into cell + in-cell offset
+      const int nn[3] = {n0, n1, n2};
+      int k[3];
+      for (int d = 0; d < 3; d++) {
+        const double u = (double)q.pos[d] / res;
+        double fl = floor(u);
+        float o = (float)(u - fl);
+        if (o >= 1.0f) o = 0.0f, fl += 1.0;
+        long kk = (long)fl % nn[d];
+        k[d] = (int)(kk < 0 ? kk + nn[d] : kk);
+        off3[3 * p + d] = o;
+      }
+      cell[p] = k[0] + n0 * (k[1] + n1 * k[2]);
+    } else {
+      const double v2 = (double)fn(dtau, res, &q, frac, info, fp, s, nfields, params, outs, noutput);
+      atomicMax(maxv2, (unsigned long long)__double_as_longlong(v2 > 0 ? v2 : 0.0));
+    }
+    for (int d = 0; d < 3; d++) vel3[3 * p + d] = (float)q.vel[d];
+    for (int i = 0; i < noutput; i++) reduce_out(&red_out[i], red[i], outs[i]);
+  }
+}
+}  // namespace lf2dev
+#endif
+
 // ---------------------------------------------------------------- Particles
 // LATfield2_Particles.hpp:131-344 for particles that live on the GPU.
 template <class part, class part_info, class part_dataType>
@@ -948,6 +1079,104 @@ class Particles {
   // LATfield2_Particles.hpp:400-425: how the projections find the mass.
   int mass_type() const { return lf2detail::has_mass<part>::value ? INDIVIDUAL_MASS : GLOBAL_MASS; }
   size_t mass_offset() const { return mass_offset_of(lf2detail::has_mass<part>()); }
+
+#ifdef __CUDACC__
+  // user physics on the GPU (a functor with a __device__ operator(); see
+  // lf2dev above)
+  template <class Kick, typename std::enable_if<!std::is_convertible<Kick, kick_fn>::value, int>::type = 0>
+  Real updateVel(Kick kick, double dtau, Field<Real>** fields = NULL, int nfields = 0,
+                 double* params = NULL, double* output = NULL, int* reduce_type = NULL, int noutput = 0)
+  {
+    return (Real)run_user<Kick, false>(kick, dtau, fields, nfields, params, output, reduce_type,
+                                       noutput);
+  }
+  template <class Move, typename std::enable_if<!std::is_convertible<Move, move_fn>::value, int>::type = 0>
+  void moveParticles(Move move, double dtau, Field<Real>** fields = NULL, int nfields = 0,
+                     double* params = NULL, double* output = NULL, int* reduce_type = NULL,
+                     int noutput = 0)
+  {
+    run_user<Move, true>(move, dtau, fields, nfields, params, output, reduce_type, noutput);
+  }
+
+  template <class Fn, bool MOVE>
+  double run_user(Fn fn, double dtau, Field<Real>** fields, int nfields, double* params,
+                  double* output, int* reduce_type, int noutput)
+  {
+    if (nfields < 0 || nfields > lf2dev::MAX_FIELDS || noutput < 0 || noutput > lf2dev::MAX_OUTPUTS)
+      throw std::invalid_argument("user physics: at most 8 fields and 8 outputs");
+    if (noutput > 0 && (!output || !reduce_type))
+      throw std::invalid_argument("user physics: outputs need output and reduce_type arrays");
+    for (int f = 0; f < nfields; f++) check_field(fields[f], "user physics");
+    sync();
+    const int64_t np = numParticles();
+    const bool hm = lf2detail::has_mass<part>::value;
+    std::vector<lf2dev::Field> fv((size_t)nfields);
+    for (int f = 0; f < nfields; f++) {
+      float* data = nullptr;
+      lf2detail::check(ctx_, lf2_field_device_ptr(ctx_, fields[f]->lf2_handle(owner_), &data),
+                       "lf2_field_device_ptr");
+      fv[(size_t)f] = lf2dev::Field{data, fields[f]->components(),
+                                    (long)lat_->size(0) * lat_->size(1) * lat_->size(2)};
+    }
+    std::vector<double> red0((size_t)noutput);
+    for (int i = 0; i < noutput; i++)
+      red0[(size_t)i] = (reduce_type[i] & (MIN | MIN_LOCAL))   ? 9223372036854775807.0
+                        : (reduce_type[i] & (MAX | MAX_LOCAL)) ? -9223372036854775807.0
+                                                               : 0.0;
+    // scratch for the particles in storage order and the call's arguments
+    const size_t n = (size_t)(np > 0 ? np : 1);
+    const size_t bytes = n * (4 + 12 + 12 + 8 + (hm ? 4 : 0)) + sizeof(lf2dev::Field) * 8 +
+                         (sizeof(int) + sizeof(double)) * 8 + 8 + 256 * 8;
+    char* buf = nullptr;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) throw std::runtime_error("user physics: cudaMalloc");
+    std::unique_ptr<char, void (*)(char*)> guard(buf, [](char* q) { cudaFree(q); });
+    char* at = buf;
+    auto take = [&](size_t b) {
+      char* r = at;
+      at += (b + 255) & ~(size_t)255;
+      return r;
+    };
+    int32_t* d_cell = (int32_t*)take(n * 4);
+    float* d_off = (float*)take(n * 12);
+    float* d_vel = (float*)take(n * 12);
+    int64_t* d_id = (int64_t*)take(n * 8);
+    float* d_mass = hm ? (float*)take(n * 4) : nullptr;
+    lf2dev::Field* d_f = (lf2dev::Field*)take(sizeof(lf2dev::Field) * 8);
+    int* d_red = (int*)take(sizeof(int) * 8);
+    double* d_out = (double*)take(sizeof(double) * 8);
+    unsigned long long* d_max = (unsigned long long*)take(8);
+    if (np > 0) {
+      lf2detail::check(ctx_, lf2_particles_get(ctx_, d_cell, d_off, d_vel, d_mass, d_id, LF2_PTR_DEVICE),
+                       "lf2_particles_get");
+      lf2detail::check(ctx_, lf2_synchronize(ctx_), "lf2_synchronize");
+      bool ok = true;
+      if (nfields) ok &= cudaMemcpy(d_f, fv.data(), sizeof(lf2dev::Field) * nfields, cudaMemcpyHostToDevice) == cudaSuccess;
+      if (noutput) {
+        ok &= cudaMemcpy(d_red, reduce_type, sizeof(int) * noutput, cudaMemcpyHostToDevice) == cudaSuccess;
+        ok &= cudaMemcpy(d_out, red0.data(), sizeof(double) * noutput, cudaMemcpyHostToDevice) == cudaSuccess;
+      }
+      ok &= cudaMemset(d_max, 0, 8) == cudaSuccess;
+      if (!ok) throw std::runtime_error("user physics: copies to the GPU failed");
+      const int grid = (int)std::min<int64_t>((np + 255) / 256, 148 * 16);
+      lf2dev::k_user<Fn, part, part_info, MOVE><<<grid, 256>>>(
+          fn, np, d_cell, d_off, d_vel, d_mass, d_id, info_, dtau, (double)res_, lat_->size(0),
+          lat_->size(1), lat_->size(2), d_f, nfields, params, noutput, d_red, d_out, d_max);
+      if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+        throw std::runtime_error("user physics: the kernel failed");
+      lf2detail::check(ctx_, lf2_particles_set(ctx_, np, d_cell, d_off, d_vel, d_mass, gmass_dev_, d_id,
+                                               LF2_PTR_DEVICE),
+                       "lf2_particles_set");
+    }
+    unsigned long long mx = 0;
+    if (noutput && np > 0) cudaMemcpy(output, d_out, sizeof(double) * noutput, cudaMemcpyDeviceToHost);
+    else
+      for (int i = 0; i < noutput; i++) output[i] = red0[(size_t)i];
+    if (np > 0) cudaMemcpy(&mx, d_max, 8, cudaMemcpyDeviceToHost);
+    double mx2 = 0.0;
+    std::memcpy(&mx2, &mx, sizeof mx2);
+    return std::sqrt(mx2);
+  }
+#endif
 
   // The part of updateVel the GPU does: the CIC kick, then the output
   // reductions.

@@ -1,6 +1,7 @@
 """Builds a demo of tests/compat/ (compat_demo.cpp, the particle path;
-poisson_demo.cpp, the FFT path) against include/latfield2_b200.hpp and
-liblf2gpu.so (no GPU needed to build):
+poisson_demo.cpp, the FFT path; device_physics_demo.cu, user physics on the
+GPU) against include/latfield2_b200.hpp and liblf2gpu.so (no GPU needed to
+build):
 
     python tests/compat/build_demo.py [--single] [--source NAME.cpp] [--out PATH]
 """
@@ -14,12 +15,19 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
 def build(out, single=False, source="compat_demo.cpp"):
+    """.cpp sources build with g++; .cu sources (user physics on the GPU)
+    with nvcc for sm_100a."""
     sys.path.insert(0, ROOT)
     from latfield2_b200 import build as B
     lib = B.build()
-    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
-           os.path.join(HERE, source), "-o", out, "-L", os.path.dirname(lib), "-llf2gpu",
-           "-Wl,-rpath," + os.path.dirname(lib)]
+    if source.endswith(".cu"):
+        cmd = [B.nvcc(), *B.ARCH, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+               os.path.join(HERE, source), "-o", out, "-L", os.path.dirname(lib), "-llf2gpu",
+               "-Xlinker", "-rpath=" + os.path.dirname(lib)]
+    else:
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+               os.path.join(HERE, source), "-o", out, "-L", os.path.dirname(lib), "-llf2gpu",
+               "-Wl,-rpath," + os.path.dirname(lib)]
     if single:
         cmd.insert(1, "-DSINGLE")
     subprocess.run(cmd, check=True)

@@ -190,3 +190,52 @@ def test_update_vel_outputs_mapping_overload_and_oset(cuda, tmp_path):
     v = ctx.field(3)
     ctx.deposit_vector(v)
     np.testing.assert_array_equal(v.export(0, np.float64).reshape(-1), B)
+
+
+def test_device_physics_demo_builds_with_nvcc(tmp_path):
+    import build_demo
+    for single in (False, True):
+        out = str(tmp_path / ("device_single" if single else "device_double"))
+        assert os.path.exists(build_demo.build(out, single, "device_physics_demo.cu"))
+
+
+@pytest.mark.gpu
+def test_user_physics_runs_on_the_gpu(cuda, tmp_path):
+    """tests/compat/device_physics_demo.cu: a user's kick and drift, written as
+    functors with __device__ operator() and the reference's callback
+    arguments, run through updateVel / moveParticles on the GPU.  They compute
+    the CIC kick and pos += dtau vel in double, so they agree with the
+    library's FP32 kick and drift to FP32 rounding: velocities within 1e-6 of
+    their scale, positions within 1e-6 of a cell; the SUM and MAX outputs of
+    |v|^2 match FP64 sums of the velocities."""
+    import torch
+    import build_demo
+    import latfield2_b200 as L
+    exe = build_demo.build(str(tmp_path / "device_physics"), False, "device_physics_demo.cu")
+    out = str(tmp_path / "device_physics.bin")
+    n, npart = 32, 20000
+    r = subprocess.run([exe, str(n), str(npart), out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    hdr, id0, pos0, vel0, Fv, id1, pos1, vel1 = _read(out)
+    dtau = hdr[2]
+    assert int(hdr[1]) == npart
+    ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64)
+    ctx.set_positions(pos0.reshape(-1, 3), vel0.reshape(-1, 3), global_mass=1.0 / npart,
+                      ids=id0.astype(np.int64))
+    Fi = torch.from_numpy(np.ascontiguousarray(
+        Fv.reshape(n, n, n, 3).transpose(3, 0, 1, 2)).astype(np.float32)).cuda()
+    F = ctx.field(3, Fi)
+    ctx.gather_kick(F, dtau)
+    ctx.drift_rebin(dtau)
+    pos, vel, ids = ctx.get_positions(ids=True)
+    k, k1 = np.argsort(ids), np.argsort(id1)
+    np.testing.assert_array_equal(ids[k], id1[k1].astype(np.int64))
+    v_user, p_user = vel1.reshape(-1, 3)[k1], pos1.reshape(-1, 3)[k1]
+    assert np.max(np.abs(vel[k] - v_user)) <= 1e-6 * np.max(np.abs(vel))
+    d = np.abs(pos[k] - p_user)
+    d = np.minimum(d, 1.0 - d)  # periodic
+    assert np.max(d) <= 1e-6 / n
+    v2 = np.sum(v_user.astype(np.float64) ** 2, axis=1)
+    assert hdr[4] == pytest.approx(v2.sum(), rel=1e-6)
+    assert hdr[5] == pytest.approx(v2.max(), rel=1e-6)
+    assert hdr[3] == pytest.approx(np.sqrt(v2.max()), rel=1e-6)
