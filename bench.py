@@ -20,8 +20,9 @@ Velocities N(0, 0.01^2) box units per time; drift dtau = 0.1 * 64/N so the
 rms displacement per step (0.064 cells) matches the 64^3 reference case; the
 kick uses the central-difference gradient of a Gaussian random field.
 
-Multi-GPU (torchrun): every rank advances its own replica of the workload
-(weak scaling, no collective on the data path); time is the max over ranks.
+Multi-GPU (torchrun, N > 1): the workload is split into N z slabs, one per
+rank (latfield2_b200.distributed.SlabDomain: ghost planes, migration, folded
+deposit over NCCL), strong scaling; time is the max over ranks.
 """
 import argparse
 import ctypes
@@ -69,6 +70,9 @@ def parse():
                     help="skip timing the PM grid operator (FFT Poisson force)")
     ap.add_argument("--no-fp32", action="store_true",
                     help="skip the FP32-mode run of the same particles (fixed-point workloads)")
+    ap.add_argument("--move-kernel", type=int, default=0,
+                    help="lf2_set_move_kernel for the timed steps: 0 automatic, 1 per-brick, "
+                         "2 pipelined, 3 pipelined with the fused deposit")
     return ap.parse_args()
 
 
@@ -775,6 +779,36 @@ def chain_step_times(n, case, npart, local, reps=2):
             "forward_ms": fwd, "forward_adjoint_ms": both, "ratio": both / fwd}
 
 
+def slab_scaling(args, n, cell, off, vel, F, npart, dtau, local, pg, device):
+    """N > 1: the workload split into N z slabs, one per rank
+    (latfield2_b200.distributed.SlabDomain): ghost planes of F, kick-drift-
+    rebin, particle migration between neighbours and the folded fixed-point
+    deposit every step, over NCCL.  Strong scaling: the same lattice and
+    particles whatever N.  Device time per step is the maximum over ranks."""
+    import torch
+    from latfield2_b200 import _lib
+    from latfield2_b200.distributed import SlabDomain
+    d = SlabDomain(n, box=1.0, mode=_lib.DEPOSIT_FIXED64, device=local)
+    d.set_particles(cell.cpu().numpy(), off.cpu().numpy(), vel.cpu().numpy(), 1.0 / npart)
+    Ff = d.field(3)
+    Ff[0][:, 1:d.nz + 1] = F.reshape(3, n[2], n[1], n[0])[:, d.z0:d.z0 + d.nz]
+    rho = d.field(1)
+    for _ in range(args.warmup):
+        d.step(Ff, dtau, dtau, rho)
+    torch.cuda.synchronize()
+    pg.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d.step(Ff, dtau, dtau, rho)
+    e1.record()
+    torch.cuda.synchronize()
+    pg.barrier()
+    ms, value = replica_throughput(e0.elapsed_time(e1), npart, args.steps, pg, device)
+    value /= pg.get_world_size()  # one set of particles for the whole job
+    return ms / args.steps, value, d.count()
+
+
 def replica_throughput(ms_local, npart, steps, pg=None, device="cpu"):
     """Whole-job time and throughput of N replicas: the time is the maximum
     over the ranks (every rank takes part in the same all-reduce), the
@@ -819,8 +853,37 @@ def main():
     n, cell, off, vel, F = make_workload(args.workload, device)
     npart = int(cell.shape[0])
     nsites = n[0] * n[1] * n[2]
+    if world > 1:
+        # the domain decomposition over the ranks (strong scaling)
+        peak, peak_kind = peaks()
+        dtau = 0.1 * 64.0 / n[0]
+        with ClockSampler(local) as clocks:
+            ms_step, value, local_count = slab_scaling(args, n, cell, off, vel, F, npart, dtau, local,
+                                                       pg, device)
+        if rank == 0:
+            step_ab = alg_bytes_step(npart, nsites)
+            line = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32 (int64 fixed-point deposit)",
+                "data": "synthetic (seeded)", "config": workload_config(args.workload),
+                "deposit_mode": "fixed (int64 fixed point)",
+                "parallelism": f"z slabs over {world} GPUs (SlabDomain: ghost planes, migration, "
+                               "folded deposit; NCCL point-to-point)",
+                "roofline": {"bound": "hbm", "kernel": "whole step", "unit": "GB/s",
+                             "achieved": step_ab / (ms_step / 1e3) / 1e9, "peak": peak * world,
+                             "frac": step_ab / (ms_step / 1e3) / 1e9 / (peak * world),
+                             "peak_source": peak_kind, "traffic": None},
+                "cpu_baseline": None, "e2e": None, "clocks": clocks.summary(),
+                "particles_rank0": local_count,
+            }
+            print(json.dumps(line), flush=True)
+        pg.barrier()
+        pg.destroy_process_group()
+        return
     ctx = L.Context(n, box=1.0, mode=mode, device=local)
     ctx.set_particles(cell, off, vel, global_mass=1.0 / npart)
+    ctx.set_move_kernel(args.move_kernel)
     keep_case = (mode == L.DEPOSIT_FIXED64 and not args.no_fp32) or args.slab or args.workload == "c5"
     fp32_case = (cell, off, vel) if keep_case else None
     del cell, off, vel

@@ -71,7 +71,10 @@ constexpr int FSTRIDE_DEP = (FBYTES + 127) & ~127; // the same in the fused-depo
 // Fused deposit (lf2_step with the fixed-point scalar deposit): one split
 // fixed-point tile of the brick's (BRICK+1)^3 vertices, two 32-bit words per
 // vertex, between the vertex tiles and the chunk ring.
-constexpr int DEP_BYTES = 2 * TILE3 * 4;
+// Rounded up to 128 bytes: the chunk ring after it is the destination of
+// bulk copies, which must start on a 16-byte boundary.
+constexpr int DEP_BYTES = (2 * TILE3 * 4 + 127) & ~127;
+static_assert(FSTRIDE_DEP % 128 == 0 && DEP_BYTES % 128 == 0, "bulk-copy destinations stay aligned");
 // Vertices of a brick's tile that movers from the neighbour bricks can reach
 // (a coordinate in {0, 1, e-1, e}): they go to the per-brick rim store, the
 // others (every coordinate in [2, e-2]) are final after the fused pass.
@@ -877,7 +880,7 @@ EncodeTiledFn encode_fn()
 }
 
 #ifndef LF2_PIPE_DEP_WARPS
-#define LF2_PIPE_DEP_WARPS 30
+#define LF2_PIPE_DEP_WARPS 20
 #endif
 constexpr int DEP_WARPS = LF2_PIPE_DEP_WARPS;  // consumer warps of the fused-deposit kernel
 constexpr int STATIC_SMEM = 256;               // the kernel's static shared memory, rounded up
