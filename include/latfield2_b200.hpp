@@ -779,7 +779,9 @@ Real cic_gather_kick_t(double dtau, double, part* p, double* frac, part_info, Fi
     v2 += p->vel[c] * p->vel[c];
     v2d += (double)p->vel[c] * (double)p->vel[c];
   }
-  if (noutputs > 0) outputs[0] = v2d;  // the per-particle output updateVel reduces
+  // the per-particle outputs updateVel reduces: |v|^2 in every slot, each
+  // slot reduced with its own reduce_type
+  for (int i = 0; i < noutputs; i++) outputs[i] = v2d;
   return v2;
 }
 
@@ -1016,10 +1018,10 @@ class Particles {
 
   // updateVel with the CIC gather-kick: fields[0] is the 3-component force.
   // Returns sqrt(max |v|^2) like the reference.  The kick reports |v|^2 as
-  // its per-particle output 0; output[0] receives its SUM, MIN or MAX over
-  // the particles (FP64 on the GPU) as reduce_type[0] says; further outputs
-  // are not written by the kick and keep the reduction's starting value
-  // (0, 9223372036854775807, -9223372036854775807), as in the reference.
+  // each of its per-particle outputs; output[i] receives its SUM, MIN or MAX
+  // over the particles (FP64 on the GPU) as reduce_type[i] says.  With no
+  // particles every output keeps the reduction's starting value (0,
+  // 9223372036854775807, -9223372036854775807), as in the reference.
   Real updateVel(kick_fn updateVel_funct, double dtau, Field<Real>** fields = NULL, int nfields = 0,
                  double* params = NULL, double* output = NULL, int* reduce_type = NULL, int noutput = 0)
   {
@@ -1198,11 +1200,11 @@ class Particles {
       const bool any = numParticles() > 0;
       for (int i = 0; i < noutput; i++) {
         if (reduce_type[i] & (SUM | SUM_LOCAL))
-          output[i] = (i == 0 && any) ? s : 0.0;
+          output[i] = any ? s : 0.0;
         else if (reduce_type[i] & (MIN | MIN_LOCAL))
-          output[i] = (i == 0 && any) ? std::min(mn, 9223372036854775807.0) : 9223372036854775807.0;
+          output[i] = any ? std::min(mn, 9223372036854775807.0) : 9223372036854775807.0;
         else if (reduce_type[i] & (MAX | MAX_LOCAL))
-          output[i] = (i == 0 && any) ? mx : -9223372036854775807.0;
+          output[i] = any ? mx : -9223372036854775807.0;
       }
     }
     return (Real)maxv;
