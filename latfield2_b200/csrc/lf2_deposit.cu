@@ -125,173 +125,193 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
   }
   __syncthreads();
 
+  // The particle loop, instantiated for the split fixed-point tile (or not)
+  // and for per-particle masses (or a global mass), chosen once per CTA.
   constexpr int ITEMS = 4;  // particles in flight per thread
-  for (int c0 = 0; c0 < cnt; c0 += ITEMS * T) {
-    uint32_t key[ITEMS];
-    float fx[ITEMS], fy[ITEMS], fz[ITEMS], m[ITEMS];
-    float vx[ITEMS], vy[ITEMS], vz[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const int i = c0 + j * T + threadIdx.x;
-      if (i < cnt) {
-        const int64_t p = base + i;
-        key[j] = v.a.key[p];
-        fx[j] = v.a.ox[p];
-        fy[j] = v.a.oy[p];
-        fz[j] = v.a.oz[p];
-        m[j] = dp.has_mass ? v.a.mass[p] : 0.0f;
-        if (KIND != 0) {
-          vx[j] = v.a.vx[p];
-          vy[j] = v.a.vy[p];
-          vz[j] = v.a.vz[p];
+  auto particles = [&](auto split_c, auto hm_c) {
+    constexpr bool SPLIT = decltype(split_c)::value;
+    constexpr bool HM = decltype(hm_c)::value;
+    for (int c0 = 0; c0 < cnt; c0 += ITEMS * T) {
+      uint32_t key[ITEMS];
+      float fx[ITEMS], fy[ITEMS], fz[ITEMS], m[ITEMS];
+      float vx[ITEMS], vy[ITEMS], vz[ITEMS];
+  #pragma unroll
+      for (int j = 0; j < ITEMS; j++) {
+        const int i = c0 + j * T + threadIdx.x;
+        if (i < cnt) {
+          const int64_t p = base + i;
+          key[j] = v.a.key[p];
+          fx[j] = v.a.ox[p];
+          fy[j] = v.a.oy[p];
+          fz[j] = v.a.oz[p];
+          m[j] = HM ? v.a.mass[p] : 0.0f;
+          if (KIND != 0) {
+            vx[j] = v.a.vx[p];
+            vy[j] = v.a.vy[p];
+            vz[j] = v.a.vz[p];
+          }
         }
       }
-    }
-#pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const int i = c0 + j * T + threadIdx.x;
-      if (i >= cnt) continue;
-      int x, y, z;
-      unpack_key(g, key[j], x, y, z);
-      const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
-      constexpr int TY = TILE, TZ = TILE * TILE;
-      if (FIXED) {
-        uint64_t mq = 0;
-        if (dp.has_mass) mq = mass_q(m[j], dp.inv_unit, flags);
-        const bool hm = dp.has_mass != 0;
-        // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle)
-        const uint32_t ux = weight_q(fx[j]), uy = weight_q(fy[j]), uz = weight_q(fz[j]);
-        const uint32_t qx[2] = {(1u << 31) - ux, ux};
-        const uint32_t qy[2] = {(1u << 31) - uy, uy};
-        const uint32_t qz[2] = {(1u << 31) - uz, uz};
-        constexpr uint32_t ONE = 1u << 31;
-        if (KIND == 0) {
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-            const uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
-            add_fixed(tr, 0, t0 + cx + cy * TY + cz * TZ, apply_mass_sign(q, hm, mq, false));
-          }
-        } else if (KIND == 1) {
-          // projections.hpp:501-544: component i is NGP along i, CIC across
-          const float vv[3] = {vx[j], vy[j], vz[j]};
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            const uint32_t vq = vel_q(vv[c], vscale);
-            const bool neg = vv[c] < 0.0f;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-              const int a = (k >> 1) & 1, bb = k & 1;
-              uint64_t w;
-              int t;
-              if (c == 0) w = fixed_corner(ONE, qy[a], qz[bb]), t = t0 + a * TY + bb * TZ;
-              else if (c == 1) w = fixed_corner(qx[a], ONE, qz[bb]), t = t0 + a + bb * TZ;
-              else w = fixed_corner(qx[a], qy[bb], ONE), t = t0 + a + bb * TY;
-              add_fixed(tr, c, t, apply_mass_sign(mul31(w, vq), hm, mq, neg));
-            }
-          }
-        } else if (PASS == 0) {
-          // projections.hpp:788-807: T_ii = m v_i^2 at the 8 vertices
-          const float vv[3] = {vx[j], vy[j], vz[j]};
-          uint64_t v2[3];
-#pragma unroll
-          for (int d = 0; d < 3; d++) {
-            const uint32_t q = vel_q(vv[d], vscale);
-            v2[d] = vel2_q(q, q);
-          }
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-            const uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
-            const int t = t0 + cx + cy * TY + cz * TZ;
-#pragma unroll
-            for (int d = 0; d < 3; d++) add_fixed(tr, d, t, apply_mass_sign(mul31(w, v2[d]), hm, mq, false));
-          }
-        } else {
-          // projections.hpp:809-821: T_ij on the (i,j) plaquette, CIC along
-          // the third dim
-          const float vv[3] = {vx[j], vy[j], vz[j]};
-          const uint32_t q0 = vel_q(vv[0], vscale), q1 = vel_q(vv[1], vscale), q2 = vel_q(vv[2], vscale);
-          const uint64_t v01 = vel2_q(q0, q1), v02 = vel2_q(q0, q2), v12 = vel2_q(q1, q2);
-          const bool n01 = (vv[0] < 0.0f) != (vv[1] < 0.0f), n02 = (vv[0] < 0.0f) != (vv[2] < 0.0f),
-                     n12 = (vv[1] < 0.0f) != (vv[2] < 0.0f);
-          // (2^-31 weight) x (2^-31 velocity product), rounded to 2^-32
-          auto w1 = [](uint32_t a, uint64_t f) { return ((uint64_t)a * f + (1ull << 29)) >> 30; };
-          add_fixed(tr, 0, t0, apply_mass_sign(w1(qz[0], v01), hm, mq, n01));
-          add_fixed(tr, 0, t0 + TZ, apply_mass_sign(w1(qz[1], v01), hm, mq, n01));
-          add_fixed(tr, 1, t0, apply_mass_sign(w1(qy[0], v02), hm, mq, n02));
-          add_fixed(tr, 1, t0 + TY, apply_mass_sign(w1(qy[1], v02), hm, mq, n02));
-          add_fixed(tr, 2, t0, apply_mass_sign(w1(qx[0], v12), hm, mq, n12));
-          add_fixed(tr, 2, t0 + 1, apply_mass_sign(w1(qx[1], v12), hm, mq, n12));
-        }
-        continue;
-      }
-      // FP32 modes: the arithmetic of the reference's projections in FP32
-      const float gx = __fsub_rn(1.0f, fx[j]), gy = __fsub_rn(1.0f, fy[j]),
-                  gz = __fsub_rn(1.0f, fz[j]);
-      const float ox = fx[j], oy = fy[j], oz = fz[j];
-      const float mf = dp.has_mass ? __fmul_rn(m[j], dp.inv_vol) : dp.mf;
-      if (KIND == 0) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-          const float w = __fmul_rn(
-              __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz)), mf);
-          add_float<ACC>(tr, 0, t0 + cx + cy * TY + cz * TZ, w);
-        }
-      } else if (KIND == 1) {
-        // projections.hpp:501-544: component i is NGP along i, CIC across.
-        const float vxm = __fmul_rn(mf, vx[j]);
-        const float vym = __fmul_rn(mf, vy[j]);
-        const float vzm = __fmul_rn(mf, vz[j]);
-        add_float<ACC>(tr, 0, t0, __fmul_rn(__fmul_rn(vxm, gy), gz));
-        add_float<ACC>(tr, 0, t0 + TY, __fmul_rn(__fmul_rn(vxm, oy), gz));
-        add_float<ACC>(tr, 0, t0 + TZ, __fmul_rn(__fmul_rn(vxm, gy), oz));
-        add_float<ACC>(tr, 0, t0 + TY + TZ, __fmul_rn(__fmul_rn(vxm, oy), oz));
-        add_float<ACC>(tr, 1, t0, __fmul_rn(__fmul_rn(vym, gx), gz));
-        add_float<ACC>(tr, 1, t0 + 1, __fmul_rn(__fmul_rn(vym, ox), gz));
-        add_float<ACC>(tr, 1, t0 + TZ, __fmul_rn(__fmul_rn(vym, gx), oz));
-        add_float<ACC>(tr, 1, t0 + 1 + TZ, __fmul_rn(__fmul_rn(vym, ox), oz));
-        add_float<ACC>(tr, 2, t0, __fmul_rn(__fmul_rn(vzm, gx), gy));
-        add_float<ACC>(tr, 2, t0 + 1, __fmul_rn(__fmul_rn(vzm, ox), gy));
-        add_float<ACC>(tr, 2, t0 + TY, __fmul_rn(__fmul_rn(vzm, gx), oy));
-        add_float<ACC>(tr, 2, t0 + 1 + TY, __fmul_rn(__fmul_rn(vzm, ox), oy));
-      } else {
-        // projections.hpp:786-843: T_ii at the 8 vertices, T_ij on plaquettes.
-        const float vv[3] = {vx[j], vy[j], vz[j]};
-        constexpr bool DIAG = ACC == ACC_PLAIN || PASS == 0;
-        constexpr bool OFF = ACC == ACC_PLAIN || PASS == 1;
-        if (DIAG) {
-#pragma unroll
-          for (int d = 0; d < 3; d++) {
-            // pass-local component of T_dd: 0, 3, 5 in the six-component
-            // plain tile, 0, 1, 2 in the diagonal pass
-            const int jd = ACC == ACC_PLAIN ? (d == 0 ? 0 : d == 1 ? 3 : 5) : d;
-            const float mv2 = __fmul_rn(__fmul_rn(mf, vv[d]), vv[d]);
-#pragma unroll
+  #pragma unroll
+      for (int j = 0; j < ITEMS; j++) {
+        const int i = c0 + j * T + threadIdx.x;
+        if (i >= cnt) continue;
+        int x, y, z;
+        unpack_key(g, key[j], x, y, z);
+        const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
+        constexpr int TY = TILE, TZ = TILE * TILE;
+        if (FIXED) {
+          uint64_t mq = 0;
+          if (HM) mq = mass_q(m[j], dp.inv_unit, flags);
+          // 1-D weights in units of 2^-31 (lf2o_fixed_weight in the oracle)
+          const uint32_t ux = weight_q(fx[j]), uy = weight_q(fy[j]), uz = weight_q(fz[j]);
+          const uint32_t qx[2] = {(1u << 31) - ux, ux};
+          const uint32_t qy[2] = {(1u << 31) - uy, uy};
+          const uint32_t qz[2] = {(1u << 31) - uz, uz};
+          constexpr uint32_t ONE = 1u << 31;
+          if (KIND == 0) {
+            const uint64_t pxy[4] = {(uint64_t)qx[0] * qy[0], (uint64_t)qx[0] * qy[1],
+                                     (uint64_t)qx[1] * qy[0], (uint64_t)qx[1] * qy[1]};
+  #pragma unroll
             for (int k = 0; k < 8; k++) {
               const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
-              const float w = __fmul_rn(
-                  __fmul_rn(__fmul_rn(mv2, sel(cx, ox, gx)), sel(cy, oy, gy)), sel(cz, oz, gz));
-              add_float<ACC>(tr, jd, t0 + cx + cy * TY + cz * TZ, w);
+              const int t = t0 + cx + cy * TY + cz * TZ;
+              if (SPLIT && !HM) {
+                add_corner_split<TILE3>(reinterpret_cast<uint32_t*>(smem_raw), t, pxy[cx * 2 + cy], qz[cz]);
+              } else {
+                const uint64_t q = fixed_corner(qx[cx], qy[cy], qz[cz]);
+                add_fixed_t<SPLIT, TILE3>(smem_raw, 0, t, mass_sign_t<HM>(q, mq, false));
+              }
+            }
+          } else if (KIND == 1) {
+            // projections.hpp:501-544: component i is NGP along i, CIC across
+            const float vv[3] = {vx[j], vy[j], vz[j]};
+  #pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const uint32_t vq = vel_q(vv[c], vscale);
+              const bool neg = vv[c] < 0.0f;
+  #pragma unroll
+              for (int k = 0; k < 4; k++) {
+                const int a = (k >> 1) & 1, bb = k & 1;
+                uint64_t w;
+                int t;
+                if (c == 0) w = fixed_corner(ONE, qy[a], qz[bb]), t = t0 + a * TY + bb * TZ;
+                else if (c == 1) w = fixed_corner(qx[a], ONE, qz[bb]), t = t0 + a + bb * TZ;
+                else w = fixed_corner(qx[a], qy[bb], ONE), t = t0 + a + bb * TY;
+                add_fixed_t<SPLIT, TILE3>(smem_raw, c, t, mass_sign_t<HM>(mul31(w, vq), mq, neg));
+              }
+            }
+          } else if (PASS == 0) {
+            // projections.hpp:788-807: T_ii = m v_i^2 at the 8 vertices
+            const float vv[3] = {vx[j], vy[j], vz[j]};
+            uint64_t v2[3];
+  #pragma unroll
+            for (int d = 0; d < 3; d++) {
+              const uint32_t q = vel_q(vv[d], vscale);
+              v2[d] = vel2_q(q, q);
+            }
+  #pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+              const uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+              const int t = t0 + cx + cy * TY + cz * TZ;
+  #pragma unroll
+              for (int d = 0; d < 3; d++) add_fixed_t<SPLIT, TILE3>(smem_raw, d, t, mass_sign_t<HM>(mul31(w, v2[d]), mq, false));
+            }
+          } else {
+            // projections.hpp:809-821: T_ij on the (i,j) plaquette, CIC along
+            // the third dim
+            const float vv[3] = {vx[j], vy[j], vz[j]};
+            const uint32_t q0 = vel_q(vv[0], vscale), q1 = vel_q(vv[1], vscale), q2 = vel_q(vv[2], vscale);
+            const uint64_t v01 = vel2_q(q0, q1), v02 = vel2_q(q0, q2), v12 = vel2_q(q1, q2);
+            const bool n01 = (vv[0] < 0.0f) != (vv[1] < 0.0f), n02 = (vv[0] < 0.0f) != (vv[2] < 0.0f),
+                       n12 = (vv[1] < 0.0f) != (vv[2] < 0.0f);
+            // (2^-31 weight) x (2^-31 velocity product), rounded to 2^-32
+            auto w1 = [](uint32_t a, uint64_t f) { return ((uint64_t)a * f + (1ull << 29)) >> 30; };
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 0, t0, mass_sign_t<HM>(w1(qz[0], v01), mq, n01));
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 0, t0 + TZ, mass_sign_t<HM>(w1(qz[1], v01), mq, n01));
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 1, t0, mass_sign_t<HM>(w1(qy[0], v02), mq, n02));
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 1, t0 + TY, mass_sign_t<HM>(w1(qy[1], v02), mq, n02));
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 2, t0, mass_sign_t<HM>(w1(qx[0], v12), mq, n12));
+            add_fixed_t<SPLIT, TILE3>(smem_raw, 2, t0 + 1, mass_sign_t<HM>(w1(qx[1], v12), mq, n12));
+          }
+          continue;
+        }
+        // FP32 modes: the arithmetic of the reference's projections in FP32
+        const float gx = __fsub_rn(1.0f, fx[j]), gy = __fsub_rn(1.0f, fy[j]),
+                    gz = __fsub_rn(1.0f, fz[j]);
+        const float ox = fx[j], oy = fy[j], oz = fz[j];
+        const float mf = HM ? __fmul_rn(m[j], dp.inv_vol) : dp.mf;
+        if (KIND == 0) {
+  #pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+            const float w = __fmul_rn(
+                __fmul_rn(__fmul_rn(sel(cx, ox, gx), sel(cy, oy, gy)), sel(cz, oz, gz)), mf);
+            add_float<ACC>(tr, 0, t0 + cx + cy * TY + cz * TZ, w);
+          }
+        } else if (KIND == 1) {
+          // projections.hpp:501-544: component i is NGP along i, CIC across.
+          const float vxm = __fmul_rn(mf, vx[j]);
+          const float vym = __fmul_rn(mf, vy[j]);
+          const float vzm = __fmul_rn(mf, vz[j]);
+          add_float<ACC>(tr, 0, t0, __fmul_rn(__fmul_rn(vxm, gy), gz));
+          add_float<ACC>(tr, 0, t0 + TY, __fmul_rn(__fmul_rn(vxm, oy), gz));
+          add_float<ACC>(tr, 0, t0 + TZ, __fmul_rn(__fmul_rn(vxm, gy), oz));
+          add_float<ACC>(tr, 0, t0 + TY + TZ, __fmul_rn(__fmul_rn(vxm, oy), oz));
+          add_float<ACC>(tr, 1, t0, __fmul_rn(__fmul_rn(vym, gx), gz));
+          add_float<ACC>(tr, 1, t0 + 1, __fmul_rn(__fmul_rn(vym, ox), gz));
+          add_float<ACC>(tr, 1, t0 + TZ, __fmul_rn(__fmul_rn(vym, gx), oz));
+          add_float<ACC>(tr, 1, t0 + 1 + TZ, __fmul_rn(__fmul_rn(vym, ox), oz));
+          add_float<ACC>(tr, 2, t0, __fmul_rn(__fmul_rn(vzm, gx), gy));
+          add_float<ACC>(tr, 2, t0 + 1, __fmul_rn(__fmul_rn(vzm, ox), gy));
+          add_float<ACC>(tr, 2, t0 + TY, __fmul_rn(__fmul_rn(vzm, gx), oy));
+          add_float<ACC>(tr, 2, t0 + 1 + TY, __fmul_rn(__fmul_rn(vzm, ox), oy));
+        } else {
+          // projections.hpp:786-843: T_ii at the 8 vertices, T_ij on plaquettes.
+          const float vv[3] = {vx[j], vy[j], vz[j]};
+          constexpr bool DIAG = ACC == ACC_PLAIN || PASS == 0;
+          constexpr bool OFF = ACC == ACC_PLAIN || PASS == 1;
+          if (DIAG) {
+  #pragma unroll
+            for (int d = 0; d < 3; d++) {
+              // pass-local component of T_dd: 0, 3, 5 in the six-component
+              // plain tile, 0, 1, 2 in the diagonal pass
+              const int jd = ACC == ACC_PLAIN ? (d == 0 ? 0 : d == 1 ? 3 : 5) : d;
+              const float mv2 = __fmul_rn(__fmul_rn(mf, vv[d]), vv[d]);
+  #pragma unroll
+              for (int k = 0; k < 8; k++) {
+                const int cx = (k >> 2) & 1, cy = (k >> 1) & 1, cz = k & 1;
+                const float w = __fmul_rn(
+                    __fmul_rn(__fmul_rn(mv2, sel(cx, ox, gx)), sel(cy, oy, gy)), sel(cz, oz, gz));
+                add_float<ACC>(tr, jd, t0 + cx + cy * TY + cz * TZ, w);
+              }
             }
           }
-        }
-        if (OFF) {
-          const int j01 = ACC == ACC_PLAIN ? 1 : 0, j02 = ACC == ACC_PLAIN ? 2 : 1,
-                    j12 = ACC == ACC_PLAIN ? 4 : 2;
-          const float m01 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[1]);
-          const float m02 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[2]);
-          const float m12 = __fmul_rn(__fmul_rn(mf, vv[1]), vv[2]);
-          add_float<ACC>(tr, j01, t0, __fmul_rn(m01, gz));
-          add_float<ACC>(tr, j01, t0 + TZ, __fmul_rn(m01, oz));
-          add_float<ACC>(tr, j02, t0, __fmul_rn(m02, gy));
-          add_float<ACC>(tr, j02, t0 + TY, __fmul_rn(m02, oy));
-          add_float<ACC>(tr, j12, t0, __fmul_rn(m12, gx));
-          add_float<ACC>(tr, j12, t0 + 1, __fmul_rn(m12, ox));
+          if (OFF) {
+            const int j01 = ACC == ACC_PLAIN ? 1 : 0, j02 = ACC == ACC_PLAIN ? 2 : 1,
+                      j12 = ACC == ACC_PLAIN ? 4 : 2;
+            const float m01 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[1]);
+            const float m02 = __fmul_rn(__fmul_rn(mf, vv[0]), vv[2]);
+            const float m12 = __fmul_rn(__fmul_rn(mf, vv[1]), vv[2]);
+            add_float<ACC>(tr, j01, t0, __fmul_rn(m01, gz));
+            add_float<ACC>(tr, j01, t0 + TZ, __fmul_rn(m01, oz));
+            add_float<ACC>(tr, j02, t0, __fmul_rn(m02, gy));
+            add_float<ACC>(tr, j02, t0 + TY, __fmul_rn(m02, oy));
+            add_float<ACC>(tr, j12, t0, __fmul_rn(m12, gx));
+            add_float<ACC>(tr, j12, t0 + 1, __fmul_rn(m12, ox));
+          }
         }
       }
     }
+  };
+  const bool hm_rt = dp.has_mass != 0;
+  if (FIXED && tr.split) {
+    if (hm_rt) particles(std::true_type{}, std::true_type{});
+    else particles(std::true_type{}, std::false_type{});
+  } else {
+    if (hm_rt) particles(std::false_type{}, std::true_type{});
+    else particles(std::false_type{}, std::false_type{});
   }
   __syncthreads();
 

@@ -56,6 +56,20 @@ __device__ __forceinline__ void add_fixed(TileRef<N> tr, int j, int t, long long
   }
 }
 
+// The same with the split decided at compile time (the tile passes
+// instantiate their particle loop once per choice, per CTA).
+template <bool SPLIT, int N>
+__device__ __forceinline__ void add_fixed_t(unsigned char* smem, int j, int t, long long q)
+{
+  if (SPLIT) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(smem) + (size_t)j * 2 * N;
+    atomicAdd(&w[t], (uint32_t)((unsigned long long)q & 0xffffu));
+    atomicAdd(&w[N + t], (uint32_t)(q >> 16));
+  } else {
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem) + (size_t)j * N + t, (unsigned long long)q);
+  }
+}
+
 // Compensated FP32 add: the atomic returns the value it replaced, so the
 // rounding error of the stored sum fl(old + w) is recovered exactly by
 // Knuth's TwoSum and added to the second word.
@@ -133,6 +147,26 @@ __device__ __forceinline__ long long apply_mass_sign(uint64_t q, bool has_mass, 
 {
   if (has_mass) q = (q * mq + (1ull << 23)) >> 24;
   return neg ? -(long long)q : (long long)q;
+}
+
+template <bool HM>
+__device__ __forceinline__ long long mass_sign_t(uint64_t q, uint64_t mq, bool neg)
+{
+  if (HM) q = (q * mq + (1ull << 23)) >> 24;
+  return neg ? -(long long)q : (long long)q;
+}
+
+// Scalar corner weight of a global-mass particle straight into the split
+// tile: q = fixed_corner(qx, qy, qz) with p = qx qy given, so that
+// q & 0xffff = bits [29, 45) and q >> 16 = bits [45, 64) of
+// h = ph qz + umulhi(pl, qz) + 2^28.
+template <int N>
+__device__ __forceinline__ void add_corner_split(uint32_t* tile, int t, uint64_t p, uint32_t qz)
+{
+  const uint64_t h = (uint64_t)(uint32_t)(p >> 32) * qz + __umulhi((uint32_t)p, qz) + (1ull << 28);
+  const uint32_t hl = (uint32_t)h, hh = (uint32_t)(h >> 32);
+  atomicAdd(&tile[t], __funnelshift_r(hl, hh, 29) & 0xffffu);
+  atomicAdd(&tile[N + t], hh >> 13);
 }
 
 // Scale 2^(31-e) as an FP32 (e within [-96, 128]).

@@ -37,7 +37,8 @@ struct UserKick {
       p->vel[c] += (Real)(g * dtau * a[c]);
       v2 += (double)p->vel[c] * p->vel[c];
     }
-    if (noutputs > 0) outputs[0] = v2;
+    // |v|^2 into every output slot; updateVel reduces slot i with reduce_type[i]
+    for (int i = 0; i < noutputs; i++) outputs[i] = v2;
     return (Real)v2;
   }
 };

@@ -12,8 +12,12 @@ changes cell between the two evaluations; a direction that finds no such
 eps down to 1e-12 is skipped, and at most 5% may be.
 
 Tolerances: the FP64 gradient agrees with the differences within 1e-4 of
-their rms; the CUDA adjoint (FP32 particle state through 8 steps) within
-1e-2 of the rms, median 3e-3; gradient norms within 5e-3 (positions,
+their rms plus the rounding noise of the difference itself, 4 sigma_L / (2
+eps): sigma_L is the spread of the FP64 loss over repeated evaluations of
+the same inputs (its sums run in a different order each time), and it
+dominates for the directions that need eps <= 1e-9 to keep every particle in
+its cell.  The CUDA adjoint (FP32 particle state through 8 steps) agrees
+within 1e-2 of the rms, median 3e-3; gradient norms within 5e-3 (positions,
 velocities, masses) and 2e-3 (stencil weights) of the FP64 ones.
 """
 import time
@@ -51,32 +55,46 @@ def test_c4_chain_against_fp64_finite_differences_on_1000_directions(cuda):
     ref = torch.autograd.grad(P.chain_loss(*ref_leaves, (n, n, n), steps, dt), ref_leaves)
     rel = {k: float((a_ - b_).norm() / b_.norm())
            for k, a_, b_ in zip(("pos", "vel", "mass", "stencil", "weights"), got, ref)}
-    rng = np.random.default_rng(11)
+    gdir = torch.Generator(device=dev).manual_seed(11)  # the random directions
     base = [pos, vel, m, S]
-    fd, dv, rf = [], [], []
+    fd, dv, rf, used = [], [], [], []
     t0 = time.time()
+    with torch.no_grad():
+        ref_cells = P.reference_cells(base, w, (n, n, n), steps, dt)
+        l0 = [float(P.chain_loss(*base, w, (n, n, n), steps, dt)) for _ in range(4)]
+    sigma = max(abs(x - l0[0]) for x in l0)  # rounding noise of one FP64 loss
     for _ in range(dirs):
-        us = [torch.from_numpy(rng.standard_normal(tuple(t.shape))).to(dev) for t in base]
+        us = [torch.randn(tuple(t.shape), generator=gdir, device=dev, dtype=torch.float64)
+              for t in base]
         nrm = float(torch.sqrt(sum((u ** 2).sum() for u in us)))
         us = [u / nrm for u in us]
         with torch.no_grad():
-            d, _ = P.directional_fd(base, us, w, (n, n, n), steps, dt, eps=1e-7)
+            d, e = P.directional_fd(base, us, w, (n, n, n), steps, dt, eps=1e-7,
+                                    ref_cells=ref_cells)
         if d is None:
             continue
         fd.append(d)
+        used.append(e)
         dv.append(float(sum((gg * u).sum() for gg, u in zip(got[:4], us))))
         rf.append(float(sum((gg * u).sum() for gg, u in zip(ref[:4], us))))
-    fd, dv, rf = map(np.array, (fd, dv, rf))
+    fd, dv, rf, used = map(np.array, (fd, dv, rf, used))
     scale = float(np.sqrt(np.mean(fd ** 2)))
+    noise = 4.0 * sigma / (2.0 * used)  # rounding noise of each central difference
+    excess = np.abs(rf - fd) - (1e-4 * scale + noise)
     out = {"directions_used": len(fd), "grad_rel_err_vs_fp64": rel,
+           "loss_noise_sigma": sigma,
+           "eps_used": {f"{e:.0e}": int(np.sum(used == e)) for e in sorted(set(used.tolist()))},
            "fd_max_err_ref_over_rms": float(np.max(np.abs(rf - fd)) / scale),
+           "fd_max_err_ref_over_rms_eps_ge_1e-8": float(np.max(np.abs(rf - fd)[used >= 0.99e-8],
+                                                               initial=0.0) / scale),
+           "fd_worst_excess_over_bound": float(np.max(excess) / scale),
            "fd_max_err_cuda_over_rms": float(np.max(np.abs(dv - fd)) / scale),
            "fd_median_rel_err_cuda": float(np.median(np.abs(dv - fd) / np.abs(fd))),
            "seconds": time.time() - t0}
     print("C4 finite-difference check:", out)
     ctx.close()
     assert len(fd) >= 0.95 * dirs, out
-    assert out["fd_max_err_ref_over_rms"] < 1e-4, out
+    assert np.all(excess < 0), out
     assert out["fd_max_err_cuda_over_rms"] < 1e-2, out
     assert out["fd_median_rel_err_cuda"] < 3e-3, out
     for k in ("pos", "vel", "mass"):
