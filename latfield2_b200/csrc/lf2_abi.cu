@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -177,6 +178,10 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
   // the same size as the slack
   const int64_t need = n + (n >> 2) + 100 * nb + 1024;
   const int64_t mov_need = n > 0 ? n : 1;  // every particle may change brick
+  // the kernels index slots with 32-bit integers
+  if (need > (int64_t)UINT32_MAX)
+    return fail(c, LF2_ERR_UNSUPPORTED, "the particle store is limited to 2^32 - 1 slots (" +
+                                            std::to_string(n) + " particles requested)");
   if (need > c->capacity || has_mass != c->has_mass || has_id != c->has_id ||
       mov_need > c->mov_capacity) {
     LF2_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -73,11 +73,15 @@ __host__ __device__ inline int64_t brick_of(const Geom& g, int x, int y, int z)
          (int64_t)g.nb[0] * ((int64_t)(y / BRICK) + (int64_t)g.nb[1] * (z / BRICK));
 }
 
+// Brick indices fit in 32 bits (a lattice holds at most 2^31 bricks), so
+// the coordinates come from 32-bit unsigned divisions.
 __host__ __device__ inline void brick_coords(const Geom& g, int64_t b, int& bx, int& by, int& bz)
 {
-  bx = (int)(b % g.nb[0]);
-  by = (int)((b / g.nb[0]) % g.nb[1]);
-  bz = (int)(b / ((int64_t)g.nb[0] * g.nb[1]));
+  const uint32_t u = (uint32_t)b, n0 = (uint32_t)g.nb[0], n1 = (uint32_t)g.nb[1];
+  const uint32_t r = u / n0;
+  bx = (int)(u - r * n0);
+  bz = (int)(r / n1);
+  by = (int)(r - (uint32_t)bz * n1);
 }
 
 // Cells (and owned vertices) of a brick along one dim: BRICK except for the

@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
   int vexp = 0;
   if (FIXED && KIND != 0) vexp = vexp_of(*vmax_bits);
   const float vscale = vel_scale(vexp);
-  const float conv = FIXED ? ldexpf(dp.fixed_scale, KIND == 1 ? vexp : 2 * vexp) : 0.0f;
+  const float conv =
+      FIXED ? ldexpf(dp.fixed_scale, (KIND == 1 ? vexp : 2 * vexp) - (KIND != 0 ? 16 : 0)) : 0.0f;
   if (FIXED && threadIdx.x == 0 && b == 0 && !(conv > 0.0f && conv <= 3.402823466e38f))
     set_flag(flags, ERR_FIXED_OVERFLOW);  // V^p / res^3 outside the FP32 range
 
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
       for (int j = 0; j < ITEMS; j++) {
         const int i = c0 + j * T + threadIdx.x;
         if (i < cnt) {
-          const int64_t p = base + i;
+          const uint32_t p = (uint32_t)base + (uint32_t)i;  // slots fit in 32 bits
           key[j] = v.a.key[p];
           fx[j] = v.a.ox[p];
           fy[j] = v.a.oy[p];
@@ -198,17 +199,17 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
                 if (c == 0) w = fixed_corner(ONE, qy[a], qz[bb]), t = t0 + a * TY + bb * TZ;
                 else if (c == 1) w = fixed_corner(qx[a], ONE, qz[bb]), t = t0 + a + bb * TZ;
                 else w = fixed_corner(qx[a], qy[bb], ONE), t = t0 + a + bb * TY;
-                add_fixed_t<SPLIT, TILE3>(smem_raw, c, t, mass_sign_t<HM>(mul31(w, vq), mq, neg));
+                add_fixed48_t<SPLIT, TILE3>(smem_raw, c, t, mass_sign48_t<HM>(mul_wv48(w, vq), mq, neg));
               }
             }
           } else if (PASS == 0) {
             // projections.hpp:788-807: T_ii = m v_i^2 at the 8 vertices
             const float vv[3] = {vx[j], vy[j], vz[j]};
-            uint64_t v2[3];
+            uint64_t v2[3];  // exact squares, 2^-62 V^2 units
   #pragma unroll
             for (int d = 0; d < 3; d++) {
-              const uint32_t q = vel_q(vv[d], vscale);
-              v2[d] = vel2_q(q, q);
+              const uint64_t q = vel_q(vv[d], vscale);
+              v2[d] = q * q;
             }
   #pragma unroll
             for (int k = 0; k < 8; k++) {
@@ -216,24 +217,25 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
               const uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
               const int t = t0 + cx + cy * TY + cz * TZ;
   #pragma unroll
-              for (int d = 0; d < 3; d++) add_fixed_t<SPLIT, TILE3>(smem_raw, d, t, mass_sign_t<HM>(mul31(w, v2[d]), mq, false));
+              for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, TILE3>(smem_raw, d, t, mass_sign48_t<HM>(mul_wvv48(w, v2[d]), mq, false));
             }
           } else {
             // projections.hpp:809-821: T_ij on the (i,j) plaquette, CIC along
             // the third dim
             const float vv[3] = {vx[j], vy[j], vz[j]};
             const uint32_t q0 = vel_q(vv[0], vscale), q1 = vel_q(vv[1], vscale), q2 = vel_q(vv[2], vscale);
-            const uint64_t v01 = vel2_q(q0, q1), v02 = vel2_q(q0, q2), v12 = vel2_q(q1, q2);
+            // exact velocity products, 2^-62 V^2 units
+            const uint64_t v01 = (uint64_t)q0 * q1, v02 = (uint64_t)q0 * q2, v12 = (uint64_t)q1 * q2;
             const bool n01 = (vv[0] < 0.0f) != (vv[1] < 0.0f), n02 = (vv[0] < 0.0f) != (vv[2] < 0.0f),
                        n12 = (vv[1] < 0.0f) != (vv[2] < 0.0f);
-            // (2^-31 weight) x (2^-31 velocity product), rounded to 2^-32
-            auto w1 = [](uint32_t a, uint64_t f) { return ((uint64_t)a * f + (1ull << 29)) >> 30; };
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 0, t0, mass_sign_t<HM>(w1(qz[0], v01), mq, n01));
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 0, t0 + TZ, mass_sign_t<HM>(w1(qz[1], v01), mq, n01));
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 1, t0, mass_sign_t<HM>(w1(qy[0], v02), mq, n02));
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 1, t0 + TY, mass_sign_t<HM>(w1(qy[1], v02), mq, n02));
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 2, t0, mass_sign_t<HM>(w1(qx[0], v12), mq, n12));
-            add_fixed_t<SPLIT, TILE3>(smem_raw, 2, t0 + 1, mass_sign_t<HM>(w1(qx[1], v12), mq, n12));
+            // (2^-31 weight) x (2^-62 velocity product), rounded to 2^-48
+            auto w1 = [](uint32_t a, uint64_t f) { return mul_avv48(a, f); };
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0, mass_sign48_t<HM>(w1(qz[0], v01), mq, n01));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0 + TZ, mass_sign48_t<HM>(w1(qz[1], v01), mq, n01));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0, mass_sign48_t<HM>(w1(qy[0], v02), mq, n02));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0 + TY, mass_sign48_t<HM>(w1(qy[1], v02), mq, n02));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0, mass_sign48_t<HM>(w1(qx[0], v12), mq, n12));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0 + 1, mass_sign48_t<HM>(w1(qx[1], v12), mq, n12));
           }
           continue;
         }
@@ -316,39 +318,68 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
   __syncthreads();
 
   // Flush: interior vertices to the field, shell vertices to the shell store
-  // (8-byte slots: the integer sum, hi and lo, or the plain float).
+  // (8-byte slots: the integer sum, hi and lo, or the plain float).  Two
+  // loops with constant divisors: the interior [1, e-1]^3 (walked as 15^3,
+  // skipping what lies beyond the extents), and the shell slots in their
+  // storage order (shell_index), so that those writes are contiguous.
   uint64_t* sp = spill + (size_t)b * C * SHELL;
   const float* facc = reinterpret_cast<const float*>(smem_raw);
-  for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
-    const int i = t % TILE, jj = (t / TILE) % TILE, k = t / (TILE * TILE);
-    if (i > ex || jj > ey || k > ez) continue;
-    const bool shell = i == 0 || i == ex || jj == 0 || jj == ey || k == 0 || k == ez;
-    const int si =
-        shell ? shell_index(i == ex ? BRICK : i, jj == ey ? BRICK : jj, k == ez ? BRICK : k) : 0;
-    const int64_t s = site_index(g, x0 + i, y0 + jj, z0 + k);
+  const int64_t site0 = site_index(g, x0, y0, z0);
+  const int64_t sy = g.n[0], sz = (int64_t)g.n[0] * g.n[1];
+  constexpr int I = BRICK - 1;
+  for (int u = threadIdx.x; u < I * I * I; u += blockDim.x) {
+    const int i = 1 + u % I, jj = 1 + (u / I) % I, k = 1 + u / (I * I);
+    if (i >= ex || jj >= ey || k >= ez) continue;
+    const int t = i + TILE * (jj + TILE * k);
+    const int64_t s = site0 + i + sy * jj + sz * k;
 #pragma unroll
     for (int j = 0; j < NC; j++) {
       const int c = P::comp(j);
       if (FIXED) {
         const long long q = tile_fixed<SIGNED>(tr, j, t);
-        if (shell) {
-          sp[(size_t)c * SHELL + si] = (uint64_t)q;
-        } else {
-          if (!SIGNED && q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-          out[(size_t)c * g.nsites + s] = __fmul_rn(__ll2float_rn(q), conv);
-        }
+        if (!SIGNED && q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+        out[(size_t)c * g.nsites + s] = __fmul_rn(__ll2float_rn(q), conv);
       } else if (ACC == ACC_COMP) {
-        const float hi = facc[(size_t)j * 2 * TILE3 + t], lo = facc[(size_t)j * 2 * TILE3 + TILE3 + t];
-        if (shell)
-          reinterpret_cast<float2*>(sp)[(size_t)c * SHELL + si] = make_float2(hi, lo);
-        else
-          out[(size_t)c * g.nsites + s] = __fadd_rn(hi, lo);
+        out[(size_t)c * g.nsites + s] =
+            __fadd_rn(facc[(size_t)j * 2 * TILE3 + t], facc[(size_t)j * 2 * TILE3 + TILE3 + t]);
       } else {
-        const float f = facc[(size_t)j * TILE3 + t];
-        if (shell)
-          reinterpret_cast<float*>(sp)[(size_t)c * SHELL + si] = f;
-        else
-          out[(size_t)c * g.nsites + s] = f;
+        out[(size_t)c * g.nsites + s] = facc[(size_t)j * TILE3 + t];
+      }
+    }
+  }
+  // canonical shell coordinate (0, 1..BRICK-1 or BRICK) -> tile coordinate,
+  // or -1 where the brick's extent e leaves it out
+  auto tile_of = [](int cc, int e) { return cc == BRICK ? e : (cc == 0 || cc < e ? cc : -1); };
+  for (int f = threadIdx.x; f < SHELL; f += blockDim.x) {
+    int ci, cj, ck;
+    if (f < 2 * TILE * TILE) {  // x faces: slot (i == BRICK) TILE^2 + k TILE + j
+      ci = f < TILE * TILE ? 0 : BRICK;
+      const int r = f % (TILE * TILE);
+      ck = r / TILE, cj = r % TILE;
+    } else if (f < 2 * TILE * TILE + 2 * I * TILE) {  // y faces: + (j == BRICK) I TILE + k I + i - 1
+      const int r = f - 2 * TILE * TILE;
+      cj = r < I * TILE ? 0 : BRICK;
+      const int r2 = r % (I * TILE);
+      ck = r2 / I, ci = 1 + r2 % I;
+    } else {  // z faces: + (k == BRICK) I^2 + (j - 1) I + i - 1
+      const int r = f - 2 * TILE * TILE - 2 * I * TILE;
+      ck = r < I * I ? 0 : BRICK;
+      const int r2 = r % (I * I);
+      cj = 1 + r2 / I, ci = 1 + r2 % I;
+    }
+    const int i = tile_of(ci, ex), jj = tile_of(cj, ey), k = tile_of(ck, ez);
+    if (i < 0 || jj < 0 || k < 0) continue;
+    const int t = i + TILE * (jj + TILE * k);
+#pragma unroll
+    for (int j = 0; j < NC; j++) {
+      const int c = P::comp(j);
+      if (FIXED) {
+        sp[(size_t)c * SHELL + f] = (uint64_t)tile_fixed<SIGNED>(tr, j, t);
+      } else if (ACC == ACC_COMP) {
+        reinterpret_cast<float2*>(sp)[(size_t)c * SHELL + f] =
+            make_float2(facc[(size_t)j * 2 * TILE3 + t], facc[(size_t)j * 2 * TILE3 + TILE3 + t]);
+      } else {
+        reinterpret_cast<float*>(sp)[(size_t)c * SHELL + f] = facc[(size_t)j * TILE3 + t];
       }
     }
   }
@@ -377,10 +408,19 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
   const int bxm = bx ? bx - 1 : g.nb[0] - 1;
   const int bym = by ? by - 1 : g.nb[1] - 1;
   const int bzm = bz ? bz - 1 : g.nb[2] - 1;
+  // the brick itself (s = 0) and its lower neighbours across every subset s
+  // of the dims (bit 0: x, 1: y, 2: z)
+  __shared__ uint32_t nbr[8];
+  if (threadIdx.x < 8) {
+    const int s = threadIdx.x;
+    nbr[s] = (uint32_t)((s & 1) ? bxm : bx) +
+             (uint32_t)g.nb[0] * ((uint32_t)((s & 2) ? bym : by) + (uint32_t)g.nb[1] * ((s & 4) ? bzm : bz));
+  }
+  __syncthreads();
   float conv = 0.0f;
   if (ACC == ACC_FIXED) {
     const int vexp = KIND != 0 ? vexp_of(*vmax_bits) : 0;
-    conv = ldexpf(fixed_scale, KIND == 0 ? 0 : KIND == 1 ? vexp : 2 * vexp);
+    conv = ldexpf(fixed_scale, KIND == 0 ? 0 : (KIND == 1 ? vexp : 2 * vexp) - 16);
   }
   const int nface = ey * ez + (ex - 1) * ez + (ex - 1) * (ey - 1);
   for (int f = threadIdx.x; f < nface; f += blockDim.x) {
@@ -409,12 +449,11 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
       fs[c] = 0.0f;
       fc[c] = 0.0f;
     }
-    for (int s = 0; s < 8; s++) {
-      if ((s & zmask) != s) continue;
-      const int nbx = (s & 1) ? bxm : bx, nby = (s & 2) ? bym : by, nbz = (s & 4) ? bzm : bz;
-      const int64_t nb = (int64_t)nbx + (int64_t)g.nb[0] * ((int64_t)nby + (int64_t)g.nb[1] * nbz);
+    // the subsets s of zmask in ascending order (s -> (s - zmask) & zmask)
+    for (int s = 0;; s = (s - zmask) & zmask) {
+      const uint32_t nb = nbr[s];
       const int si = shell_index((s & 1) ? BRICK : i, (s & 2) ? BRICK : j, (s & 4) ? BRICK : k);
-      const uint64_t* sp = spill + (size_t)nb * C * SHELL;
+      const uint64_t* sp = spill + (size_t)nb * (C * SHELL);
 #pragma unroll
       for (int c = 0; c < C; c++) {
         if (ACC == ACC_FIXED) {
@@ -426,6 +465,7 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
           fs[c] = __fadd_rn(fs[c], reinterpret_cast<const float*>(sp)[c * SHELL + si]);
         }
       }
+      if (s == zmask) break;
     }
     const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
 #pragma unroll

@@ -103,14 +103,36 @@ __device__ __forceinline__ void add_float(TileRef<N> tr, int j, int t, float w)
   }
 }
 
-// Integer vertex sum of component j.
+// Signed kinds (momentum and stress): contributions are in units of 2^-48
+// of a unit mass times V or V^2, |q| <= 2^48 for a global mass and 2^54 with
+// per-particle masses.  The split keeps lo = the low 32 bits of the sum
+// (every carry out of the 32-bit add, seen in the value the atomic returns,
+// goes to hi) and hi = the sum of (q >> 32) plus those carries, so the
+// vertex sum is hi 2^32 + lo exactly while hi stays within int32: bricks of
+// at most 32767 particles (511 with per-particle masses), split_max<true>.
+template <bool SPLIT, int N>
+__device__ __forceinline__ void add_fixed48_t(unsigned char* smem, int j, int t, long long q)
+{
+  if (SPLIT) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(smem) + (size_t)j * 2 * N;
+    const uint32_t lo = (uint32_t)(unsigned long long)q;
+    const uint32_t old = atomicAdd(&w[t], lo);
+    const int carry = (uint32_t)(old + lo) < old ? 1 : 0;
+    atomicAdd(reinterpret_cast<int*>(&w[N + t]), (int)(q >> 32) + carry);
+  } else {
+    atomicAdd(reinterpret_cast<unsigned long long*>(smem) + (size_t)j * N + t, (unsigned long long)q);
+  }
+}
+
+// Integer vertex sum of component j: the scalar's split (lo + hi 2^16) or
+// the signed kinds' split (hi 2^32 + lo, add_fixed48_t).
 template <bool SIGNED, int N>
 __device__ __forceinline__ long long tile_fixed(const TileRef<N>& tr, int j, int t)
 {
   if (tr.split) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(tr.smem) + (size_t)j * 2 * N;
-    const long long hi = SIGNED ? (long long)(int32_t)w[N + t] : (long long)w[N + t];
-    return (long long)w[t] + hi * 65536ll;
+    if (SIGNED) return (long long)(int32_t)w[N + t] * 4294967296ll + (long long)w[t];
+    return (long long)w[t] + (long long)w[N + t] * 65536ll;
   }
   return (long long)reinterpret_cast<const unsigned long long*>(tr.smem)[(size_t)j * N + t];
 }
@@ -134,6 +156,34 @@ __device__ __forceinline__ uint64_t vel2_q(uint32_t a, uint32_t b)
 
 // w (2^-32 units) times a factor in 2^-31 units, rounded to 2^-32 units.
 __device__ __forceinline__ uint64_t mul31(uint64_t w, uint64_t f) { return (w * f + (1ull << 30)) >> 31; }
+
+// Momentum: w (2^-32 units, <= 2^32) times a velocity (2^-31 V units,
+// < 2^31), rounded to 2^-48 V units.
+__device__ __forceinline__ uint64_t mul_wv48(uint64_t w, uint64_t f) { return (w * f + (1ull << 14)) >> 15; }
+
+// round(a * b / 2^s) for a product of up to 128 bits (32 <= s < 64), from
+// its two 64-bit halves.
+template <int S>
+__device__ __forceinline__ uint64_t mul_round(uint64_t a, uint64_t b)
+{
+  const uint64_t lo = a * b, hi = __umul64hi(a, b);
+  return ((lo >> S) | (hi << (64 - S))) + ((lo >> (S - 1)) & 1ull);
+}
+
+// Stress: w (2^-32 units) times the exact product of two velocities (2^-62
+// V^2 units, < 2^62), rounded to 2^-48 V^2 units; a 1-D weight (2^-31 units)
+// times that product likewise.
+__device__ __forceinline__ uint64_t mul_wvv48(uint64_t w, uint64_t vv) { return mul_round<46>(w, vv); }
+__device__ __forceinline__ uint64_t mul_avv48(uint64_t a, uint64_t vv) { return mul_round<45>(a, vv); }
+
+// Per-particle relative mass (2^-24 units) applied to a signed-kind
+// contribution (|q| <= 2^48, so the product needs 128 bits), then the sign.
+template <bool HM>
+__device__ __forceinline__ long long mass_sign48_t(uint64_t q, uint64_t mq, bool neg)
+{
+  if (HM) q = mul_round<24>(q, mq);
+  return neg ? -(long long)q : (long long)q;
+}
 
 // Per-particle relative mass m / m_unit in units of 2^-24 (range-checked).
 __device__ __forceinline__ uint64_t mass_q(float m, float inv_unit, uint32_t* flags)

@@ -37,6 +37,8 @@
 // boundary vertices once.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
@@ -345,7 +347,7 @@ __global__ void __launch_bounds__(FULL2_THREADS)
   int vexp = 0;
   if (FIXED) vexp = vexp_of(*vmax_bits);
   const float vscale = vel_scale(vexp);
-  const float conv = FIXED ? ldexpf(dp.fixed_scale, PASS == 0 ? vexp : 2 * vexp) : 0.0f;
+  const float conv = FIXED ? ldexpf(dp.fixed_scale, (PASS == 0 ? vexp : 2 * vexp) - 16) : 0.0f;
   if (FIXED && threadIdx.x == 0 && b == 0 && !(conv > 0.0f && conv <= 3.402823466e38f))
     set_flag(flags, ERR_FIXED_OVERFLOW);
 
@@ -356,148 +358,162 @@ __global__ void __launch_bounds__(FULL2_THREADS)
   __syncthreads();
 
   constexpr int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
-  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const int64_t p = base + i;
-    int x, y, z;
-    unpack_key(g, v.a.key[p], x, y, z);
-    const float o[3] = {v.a.ox[p], v.a.oy[p], v.a.oz[p]};
-    const float vel[3] = {v.a.vx[p], v.a.vy[p], v.a.vz[p]};
-    const int l[3] = {x - x0, y - y0, z - z0};
-    int ls[3], lt[3], gd[3];
-    float s[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      s[d] = __fsub_rn(o[d], 0.5f);
-      gd[d] = s[d] >= 0.0f;
-      ls[d] = l[d] + 1;
-      lt[d] = l[d] + gd[d];
-    }
-    if (FIXED) {
-      const bool hm = dp.has_mass != 0;
-      const uint64_t mq = hm ? mass_q(v.a.mass[p], dp.inv_unit, flags) : 0;
-      // vertex weights sq and staggered weights tq in units of 2^-31
-      uint32_t sq[3][2], tq[3][2], vq[3];
-#pragma unroll
+  // the particle loop, instantiated per CTA for the split tile (or not) and
+  // for per-particle masses (or a global mass)
+  auto particles = [&](auto split_c, auto hm_c) {
+    constexpr bool SPLIT = decltype(split_c)::value;
+    constexpr bool HM = decltype(hm_c)::value;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const uint32_t p = (uint32_t)base + (uint32_t)i;  // slots fit in 32 bits
+      int x, y, z;
+      unpack_key(g, v.a.key[p], x, y, z);
+      const float o[3] = {v.a.ox[p], v.a.oy[p], v.a.oz[p]};
+      const float vel[3] = {v.a.vx[p], v.a.vy[p], v.a.vz[p]};
+      const int l[3] = {x - x0, y - y0, z - z0};
+      int ls[3], lt[3], gd[3];
+      float s[3];
+  #pragma unroll
       for (int d = 0; d < 3; d++) {
-        const uint32_t u = weight_q(o[d]);
-        sq[d][0] = (1u << 31) - u;
-        sq[d][1] = u;
-        const uint32_t us = weight_q(fabsf(s[d]));
-        tq[d][0] = gd[d] ? (1u << 31) - us : us;
-        tq[d][1] = gd[d] ? us : (1u << 31) - us;
-        vq[d] = vel_q(vel[d], vscale);
+        s[d] = __fsub_rn(o[d], 0.5f);
+        gd[d] = s[d] >= 0.0f;
+        ls[d] = l[d] + 1;
+        lt[d] = l[d] + gd[d];
       }
-      if (PASS == 0) {
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          const bool neg = vel[c] < 0.0f;
-#pragma unroll
+      if (FIXED) {
+        const uint64_t mq = HM ? mass_q(v.a.mass[p], dp.inv_unit, flags) : 0;
+        // vertex weights sq and staggered weights tq in units of 2^-31
+        uint32_t sq[3][2], tq[3][2], vq[3];
+  #pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const uint32_t u = weight_q(o[d]);
+          sq[d][0] = (1u << 31) - u;
+          sq[d][1] = u;
+          const uint32_t us = weight_q(fabsf(s[d]));
+          tq[d][0] = gd[d] ? (1u << 31) - us : us;
+          tq[d][1] = gd[d] ? us : (1u << 31) - us;
+          vq[d] = vel_q(vel[d], vscale);
+        }
+        if (PASS == 0) {
+  #pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const bool neg = vel[c] < 0.0f;
+  #pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+              const uint64_t w = fixed_corner(c == 0 ? tq[0][b0] : sq[0][b0],
+                                              c == 1 ? tq[1][b1] : sq[1][b1],
+                                              c == 2 ? tq[2][b2] : sq[2][b2]);
+              const int t = tile_at((c == 0 ? lt[0] : ls[0]) + b0, (c == 1 ? lt[1] : ls[1]) + b1,
+                                    (c == 2 ? lt[2] : ls[2]) + b2);
+              add_fixed48_t<SPLIT, FT3>(smem_raw, c, t, mass_sign48_t<HM>(mul_wv48(w, vq[c]), mq, neg));
+            }
+          }
+        } else if (PASS == 1) {
+          uint64_t v2[3];
+  #pragma unroll
+          for (int d = 0; d < 3; d++) v2[d] = (uint64_t)vq[d] * vq[d];  // exact, 2^-62 V^2 units
+  #pragma unroll
           for (int k = 0; k < 8; k++) {
             const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
-            const uint64_t w = fixed_corner(c == 0 ? tq[0][b0] : sq[0][b0],
-                                            c == 1 ? tq[1][b1] : sq[1][b1],
-                                            c == 2 ? tq[2][b2] : sq[2][b2]);
+            const uint64_t w = fixed_corner(sq[0][b0], sq[1][b1], sq[2][b2]);
+            const int t = tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2);
+  #pragma unroll
+            for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, FT3>(smem_raw, d, t, mass_sign48_t<HM>(mul_wvv48(w, v2[d]), mq, false));
+          }
+        } else {
+  #pragma unroll
+          for (int q = 0; q < 3; q++) {
+            const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];  // exact, 2^-62 V^2 units
+            const bool neg = (vel[pa[q]] < 0.0f) != (vel[pb[q]] < 0.0f);
+  #pragma unroll
+            for (int k = 0; k < 8; k++) {
+              const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
+              uint32_t w[3];
+              int t[3];
+  #pragma unroll
+              for (int d = 0; d < 3; d++) {
+                const bool st = d == pa[q] || d == pb[q];
+                w[d] = st ? tq[d][bb[d]] : sq[d][bb[d]];
+                t[d] = (st ? lt[d] : ls[d]) + bb[d];
+              }
+              add_fixed48_t<SPLIT, FT3>(smem_raw, q, tile_at(t[0], t[1], t[2]),
+                                        mass_sign48_t<HM>(mul_wvv48(fixed_corner(w[0], w[1], w[2]), vv),
+                                                          mq, neg));
+            }
+          }
+        }
+        continue;
+      }
+      // compensated FP32: the arithmetic of k_deposit_full
+      const float mf = HM ? __fmul_rn(v.a.mass[p], dp.inv_vol) : dp.mf;
+      float sw[3][2], tw[3][2];
+  #pragma unroll
+      for (int d = 0; d < 3; d++) {
+        sw[d][1] = o[d];
+        sw[d][0] = __fsub_rn(1.0f, o[d]);
+        if (gd[d]) {
+          tw[d][1] = s[d];
+          tw[d][0] = __fsub_rn(1.0f, s[d]);
+        } else {
+          tw[d][0] = -s[d];
+          tw[d][1] = __fsub_rn(1.0f, tw[d][0]);
+        }
+      }
+      if (PASS == 0) {
+  #pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float mv = __fmul_rn(mf, vel[c]);
+  #pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+            const float w0 = c == 0 ? tw[0][b0] : sw[0][b0];
+            const float w1 = c == 1 ? tw[1][b1] : sw[1][b1];
+            const float w2 = c == 2 ? tw[2][b2] : sw[2][b2];
             const int t = tile_at((c == 0 ? lt[0] : ls[0]) + b0, (c == 1 ? lt[1] : ls[1]) + b1,
                                   (c == 2 ? lt[2] : ls[2]) + b2);
-            add_fixed(tr, c, t, apply_mass_sign(mul31(w, vq[c]), hm, mq, neg));
+            add_float<ACC>(tr, c, t, __fmul_rn(__fmul_rn(__fmul_rn(mv, w0), w1), w2));
           }
         }
       } else if (PASS == 1) {
-        uint64_t v2[3];
-#pragma unroll
-        for (int d = 0; d < 3; d++) v2[d] = vel2_q(vq[d], vq[d]);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
-          const uint64_t w = fixed_corner(sq[0][b0], sq[1][b1], sq[2][b2]);
-          const int t = tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2);
-#pragma unroll
-          for (int d = 0; d < 3; d++) add_fixed(tr, d, t, apply_mass_sign(mul31(w, v2[d]), hm, mq, false));
+  #pragma unroll
+        for (int i2 = 0; i2 < 3; i2++) {
+          const float m2 = __fmul_rn(__fmul_rn(mf, vel[i2]), vel[i2]);
+  #pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
+            add_float<ACC>(tr, i2, tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2),
+                           __fmul_rn(__fmul_rn(__fmul_rn(m2, sw[0][b0]), sw[1][b1]), sw[2][b2]));
+          }
         }
       } else {
-#pragma unroll
+  #pragma unroll
         for (int q = 0; q < 3; q++) {
-          const uint64_t vv = vel2_q(vq[pa[q]], vq[pb[q]]);
-          const bool neg = (vel[pa[q]] < 0.0f) != (vel[pb[q]] < 0.0f);
-#pragma unroll
+          const float mm = __fmul_rn(__fmul_rn(mf, vel[pa[q]]), vel[pb[q]]);
+  #pragma unroll
           for (int k = 0; k < 8; k++) {
             const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
-            uint32_t w[3];
+            float w[3];
             int t[3];
-#pragma unroll
+  #pragma unroll
             for (int d = 0; d < 3; d++) {
               const bool st = d == pa[q] || d == pb[q];
-              w[d] = st ? tq[d][bb[d]] : sq[d][bb[d]];
+              w[d] = st ? tw[d][bb[d]] : sw[d][bb[d]];
               t[d] = (st ? lt[d] : ls[d]) + bb[d];
             }
-            add_fixed(tr, q, tile_at(t[0], t[1], t[2]),
-                      apply_mass_sign(mul31(fixed_corner(w[0], w[1], w[2]), vv), hm, mq, neg));
+            add_float<ACC>(tr, q, tile_at(t[0], t[1], t[2]),
+                           __fmul_rn(__fmul_rn(__fmul_rn(mm, w[0]), w[1]), w[2]));
           }
         }
       }
-      continue;
     }
-    // compensated FP32: the arithmetic of k_deposit_full
-    const float mf = dp.has_mass ? __fmul_rn(v.a.mass[p], dp.inv_vol) : dp.mf;
-    float sw[3][2], tw[3][2];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      sw[d][1] = o[d];
-      sw[d][0] = __fsub_rn(1.0f, o[d]);
-      if (gd[d]) {
-        tw[d][1] = s[d];
-        tw[d][0] = __fsub_rn(1.0f, s[d]);
-      } else {
-        tw[d][0] = -s[d];
-        tw[d][1] = __fsub_rn(1.0f, tw[d][0]);
-      }
-    }
-    if (PASS == 0) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const float mv = __fmul_rn(mf, vel[c]);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
-          const float w0 = c == 0 ? tw[0][b0] : sw[0][b0];
-          const float w1 = c == 1 ? tw[1][b1] : sw[1][b1];
-          const float w2 = c == 2 ? tw[2][b2] : sw[2][b2];
-          const int t = tile_at((c == 0 ? lt[0] : ls[0]) + b0, (c == 1 ? lt[1] : ls[1]) + b1,
-                                (c == 2 ? lt[2] : ls[2]) + b2);
-          add_float<ACC>(tr, c, t, __fmul_rn(__fmul_rn(__fmul_rn(mv, w0), w1), w2));
-        }
-      }
-    } else if (PASS == 1) {
-#pragma unroll
-      for (int i2 = 0; i2 < 3; i2++) {
-        const float m2 = __fmul_rn(__fmul_rn(mf, vel[i2]), vel[i2]);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
-          add_float<ACC>(tr, i2, tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2),
-                         __fmul_rn(__fmul_rn(__fmul_rn(m2, sw[0][b0]), sw[1][b1]), sw[2][b2]));
-        }
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 3; q++) {
-        const float mm = __fmul_rn(__fmul_rn(mf, vel[pa[q]]), vel[pb[q]]);
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
-          float w[3];
-          int t[3];
-#pragma unroll
-          for (int d = 0; d < 3; d++) {
-            const bool st = d == pa[q] || d == pb[q];
-            w[d] = st ? tw[d][bb[d]] : sw[d][bb[d]];
-            t[d] = (st ? lt[d] : ls[d]) + bb[d];
-          }
-          add_float<ACC>(tr, q, tile_at(t[0], t[1], t[2]),
-                         __fmul_rn(__fmul_rn(__fmul_rn(mm, w[0]), w[1]), w[2]));
-        }
-      }
-    }
+  };
+  const bool hm_rt = dp.has_mass != 0;
+  if (FIXED && tr.split) {
+    if (hm_rt) particles(std::true_type{}, std::true_type{});
+    else particles(std::true_type{}, std::false_type{});
+  } else {
+    if (hm_rt) particles(std::false_type{}, std::true_type{});
+    else particles(std::false_type{}, std::false_type{});
   }
   __syncthreads();
 
@@ -557,7 +573,7 @@ __global__ void __launch_bounds__(256, 4)
   float conv = 0.0f;
   if (ACC == ACC_FIXED) {
     const int vexp = vexp_of(*vmax_bits);
-    conv = ldexpf(fixed_scale, C == 3 ? vexp : 2 * vexp);
+    conv = ldexpf(fixed_scale, (C == 3 ? vexp : 2 * vexp) - 16);
   }
   for (int f = threadIdx.x; f < total; f += blockDim.x) {
     int q[3];

@@ -94,6 +94,7 @@ struct Job {
   long long b;     // brick, or -1: no more bricks
   long long base;  // first slot of the brick's segment
   int cnt;         // particles
+  int bx, by, bz;  // brick coordinates
 };
 
 __device__ __forceinline__ uint32_t saddr(const void* p)
@@ -269,13 +270,14 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, uint32
                                           long long limit)
 {
   int ok = 1;
-  if (lane == 0) ok = mbar_wait(bar, parity, flags, limit);
+  // the first poll inline; the bounded wait out of line
+  if (lane == 0 && !mbar_try(bar, parity)) ok = mbar_wait(bar, parity, flags, limit);
   ok = __shfl_sync(0xffffffffu, ok, 0);
   if (ok) mbar_try(bar, parity);
   return ok != 0;
 }
 
-template <int WARPS, bool DEP>
+template <int WARPS, bool DEP, bool HM, bool HID>
 __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
     k_move_pipe(const __grid_constant__ CUtensorMap tmF, StoreView v, const float* __restrict__ F,
                 MoveParams mp, PartArrays mov, unsigned long long* mov_count,
@@ -285,8 +287,8 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
   constexpr int CHUNK = WARPS * WSUB;            // particles per chunk buffer
   constexpr int PC_WARPS = WARPS;                // consumer warps
   constexpr int FST = DEP ? FSTRIDE_DEP : FSTRIDE;
-  constexpr uintptr_t ALIGN = DEP ? 127 : 1023;
-  extern __shared__ unsigned char dyn[];
+  constexpr uint32_t ALIGN = DEP ? 127 : 1023;
+  extern __shared__ __align__(128) unsigned char dyn[];
   // tma_f: tile copy landed (or the end of the bricks); full_f: tile
   // patched and ready for the consumers; empty_f: all consumer warps are
   // done with the brick; full_p / empty_p: chunk ring.
@@ -298,13 +300,18 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
   __shared__ int s_done[2];       // consumer warps finished with the brick
   __shared__ unsigned s_maxv2[2]; // max |v|^2 of the brick (bits of a non-negative float)
 
-  unsigned char* sm = reinterpret_cast<unsigned char*>(
-      (reinterpret_cast<uintptr_t>(dyn) + ALIGN) & ~ALIGN);
+  // Aligned base of the tile buffers, by an offset from the shared array
+  // itself (not through an integer cast), so that every access below stays
+  // a shared-memory access.
+  const uint32_t mis = saddr(dyn) & ALIGN;
+  unsigned char* sm = dyn + (mis ? ALIGN + 1 - mis : 0u);
   uint32_t* dtile = reinterpret_cast<uint32_t*>(sm + NF * FST);  // DEP: [lo | hi] x TILE3
   unsigned char* pbuf = sm + NF * FST + (DEP ? DEP_BYTES : 0);
 
   const Geom& g = v.g;
-  const bool has_m = v.a.mass != nullptr, has_id = v.a.id != nullptr;
+  // per-particle masses and IDs (the store carries them or not), fixed at
+  // compile time
+  constexpr bool has_m = HM, has_id = HID;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   if (threadIdx.x == 0) {
@@ -380,6 +387,7 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
       }
       job[fs].base = base;
       job[fs].cnt = cnt;
+      brick_coords(g, b, job[fs].bx, job[fs].by, job[fs].bz);
       s_cursor[fs] = 0;
       s_done[fs] = 0;
       s_maxv2[fs] = 0u;
@@ -388,10 +396,9 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
         mbar_arrive(&tma_f[fs]);
         return;
       }
-      int bx, by, bz;
-      brick_coords(g, b, bx, by, bz);
       mbar_arrive_tx(&tma_f[fs], FBYTES);
-      tma_tile4(sm + fs * FST, &tmF, bx * BRICK, by * BRICK, bz * BRICK, 0, &tma_f[fs]);
+      tma_tile4(sm + fs * FST, &tmF, job[fs].bx * BRICK, job[fs].by * BRICK, job[fs].bz * BRICK, 0,
+                &tma_f[fs]);
     };
     // tile buffer of the next post free?
     auto tile_free = [&]() {
@@ -482,8 +489,7 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
         if (lane == 0) mbar_arrive(&full_f[fs]);
         return;
       }
-      int bx, by, bz;
-      brick_coords(g, jb.b, bx, by, bz);
+      const int bx = jb.bx, by = jb.by, bz = jb.bz;
       const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
       const int ex = brick_extent(g.n[0], bx), ey = brick_extent(g.n[1], by),
                 ez = brick_extent(g.n[2], bz);
@@ -536,6 +542,9 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
   }
 
   // -------------------------------------------------------------- consumers
+  // lattice sizes that are powers of two wrap with the key's bit masks
+  const bool pow2 = g.n[0] == (int)g.mask[0] + 1 && g.n[1] == (int)g.mask[1] + 1 &&
+                    g.n[2] == (int)g.mask[2] + 1;
   // Each warp takes slots [warp * WSUB, (warp + 1) * WSUB) of every chunk of
   // the brick and works on its own: stayers are written back in place at
   // slots taken from the brick's shared cursor, movers at slots taken from
@@ -555,9 +564,10 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
     const int64_t b = jb.b;
     const int cnt = jb.cnt;
     const float* ft = reinterpret_cast<const float*>(sm + fs * FST);
-    int bx, by, bz;
-    brick_coords(g, b, bx, by, bz);
+    const int bx = jb.bx, by = jb.by, bz = jb.bz;
     const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+    // slot indices fit in 32 bits (the store holds fewer than 2^32 slots)
+    const uint32_t base32 = (uint32_t)jb.base;
     const uint32_t key0 = pack_key(g, x0, y0, z0);  // a harmless key for empty lanes
     const bool dsplit = DEP && cnt <= dep.split_max;  // fused deposit: split 32-bit sums
 
@@ -632,9 +642,16 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
         int kx = (int)fx, ky = (int)fy, kz = (int)fz;
         kx += rx >= 1.0f, ky += ry >= 1.0f, kz += rz >= 1.0f;
         rx = rx >= 1.0f ? 0.0f : rx, ry = ry >= 1.0f ? 0.0f : ry, rz = rz >= 1.0f ? 0.0f : rz;
-        const int nx = wrap_near(x, finite ? kx : 0, g.n[0]);
-        const int ny = wrap_near(y, finite ? ky : 0, g.n[1]);
-        const int nz = wrap_near(z, finite ? kz : 0, g.n[2]);
+        int nx, ny, nz;
+        if (pow2) {  // the periodic wrap is the key's bit mask
+          nx = (x + (finite ? kx : 0)) & (int)g.mask[0];
+          ny = (y + (finite ? ky : 0)) & (int)g.mask[1];
+          nz = (z + (finite ? kz : 0)) & (int)g.mask[2];
+        } else {
+          nx = wrap_near(x, finite ? kx : 0, g.n[0]);
+          ny = wrap_near(y, finite ? ky : 0, g.n[1]);
+          nz = wrap_near(z, finite ? kz : 0, g.n[2]);
+        }
         if (finite) {
           ox[j] = rx, oy[j] = ry, oz[j] = rz;
           key[j] = pack_key(g, nx, ny, nz);
@@ -657,18 +674,18 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
         mqo += __popc(mb[j] & lt);
       }
       int sbase = 0;
-      unsigned long long mbase = 0;
+      uint32_t mbase = 0;  // mover slots stay below 2^32 like the store's
       if (lane == 0) {
         if (ns) sbase = atomicAdd(&s_cursor[fs], ns);
-        if (nmv) mbase = atomicAdd(mov_count, (unsigned long long)nmv);
+        if (nmv) mbase = (uint32_t)atomicAdd(mov_count, (unsigned long long)nmv);
       }
       sq += __shfl_sync(0xffffffffu, sbase, 0);
-      long long mq = (long long)__shfl_sync(0xffffffffu, mbase, 0) + mqo;
+      uint32_t mq = __shfl_sync(0xffffffffu, mbase, 0) + (uint32_t)mqo;
 #pragma unroll
       for (int j = 0; j < W_ITEMS; j++) {
         if (!act[j]) continue;
         if (stay[j]) {
-          const int64_t q = jb.base + sq++;
+          const uint32_t q = base32 + (uint32_t)sq++;
           v.a.key[q] = key[j];
           v.a.ox[q] = ox[j];
           v.a.oy[q] = oy[j];
@@ -704,7 +721,7 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
             }
           }
         } else {
-          const int64_t q = mq++;
+          const uint32_t q = mq++;
           mov.key[q] = key[j];
           mov.ox[q] = ox[j];
           mov.oy[q] = oy[j];
@@ -712,8 +729,8 @@ __global__ void __launch_bounds__(WARPS * 32 + 64, 1)
           mov.vx[q] = vx[j];
           mov.vy[q] = vy[j];
           mov.vz[q] = vz[j];
-          if (mov.mass) mov.mass[q] = m[j];
-          if (mov.id) mov.id[q] = id[j];
+          if (has_m) mov.mass[q] = m[j];
+          if (has_id) mov.id[q] = id[j];
         }
       }
     }
@@ -823,6 +840,13 @@ __global__ void __launch_bounds__(256) k_dep_movers(Geom g, PartArrays mov,
 // non-empty subset S of the dims where its coordinate is 0, the rim value of
 // the lower neighbour across S at coordinate e' (canonical BRICK) in those
 // dims, summed in a fixed order; then converted like the tile pass.
+//
+// The rim-owned vertices are enumerated directly: with R(e) the coordinates
+// {0, 1, e-1} of [0, e) (all of them when e <= 3) and P(e) = [2, e-2] the
+// others, they are z in R (any x, y), then z in P with y in R (any x), then
+// y, z in P with x in R: 3e^2 + 3e(e-3) + 3(e-3)^2 = 1899 for e = 16.
+__device__ __forceinline__ int rim_coord(int r, int e) { return r < 2 ? r : e - 1; }
+
 __global__ void __launch_bounds__(256) k_fixup_rim(Geom g, const uint64_t* __restrict__ rim,
                                                    float scale, float* __restrict__ out,
                                                    uint32_t* flags)
@@ -833,12 +857,29 @@ __global__ void __launch_bounds__(256) k_fixup_rim(Geom g, const uint64_t* __res
   const int e[3] = {brick_extent(g.n[0], bx), brick_extent(g.n[1], by), brick_extent(g.n[2], bz)};
   const int bm[3] = {bx ? bx - 1 : g.nb[0] - 1, by ? by - 1 : g.nb[1] - 1, bz ? bz - 1 : g.nb[2] - 1};
   const int bc[3] = {bx, by, bz};
-  const int nown = e[0] * e[1] * e[2];
-  for (int f = threadIdx.x; f < nown; f += blockDim.x) {
-    const int q[3] = {f % e[0], (f / e[0]) % e[1], f / (e[0] * e[1])};
-    if (q[0] >= 2 && q[0] <= e[0] - 2 && q[1] >= 2 && q[1] <= e[1] - 2 && q[2] >= 2 &&
-        q[2] <= e[2] - 2)
-      continue;  // private: written by the fused pass
+  int nr[3], np[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) nr[d] = min(e[d], 3), np[d] = e[d] - nr[d];
+  const int n1 = nr[2] * e[1] * e[0];          // z in R
+  const int n2 = n1 + np[2] * nr[1] * e[0];    // z in P, y in R
+  const int n3 = n2 + np[2] * np[1] * nr[0];   // y, z in P, x in R
+  for (int f = threadIdx.x; f < n3; f += blockDim.x) {
+    int q[3];
+    if (f < n1) {
+      q[0] = f % e[0];
+      q[1] = (f / e[0]) % e[1];
+      q[2] = rim_coord(f / (e[0] * e[1]), e[2]);
+    } else if (f < n2) {
+      const int r = f - n1;
+      q[0] = r % e[0];
+      q[1] = rim_coord((r / e[0]) % nr[1], e[1]);
+      q[2] = 2 + r / (e[0] * nr[1]);
+    } else {
+      const int r = f - n2;
+      q[0] = rim_coord(r % nr[0], e[0]);
+      q[1] = 2 + (r / nr[0]) % np[1];
+      q[2] = 2 + r / (nr[0] * np[1]);
+    }
     const int zmask = (q[0] == 0 ? 1 : 0) | (q[1] == 0 ? 2 : 0) | (q[2] == 0 ? 4 : 0);
     long long sum = 0;
     for (int s = 0; s < 8; s++) {
@@ -962,7 +1003,13 @@ cudaError_t launch_move_pipe(lf2_ctx* c, const float* F, MoveParams mp, float* r
     d.inv_unit = (float)(1.0 / c->m_unit);
     d.split_max = split_max<false>(c->has_mass);
   }
-  auto kern = dep ? k_move_pipe<DEP_WARPS, true> : k_move_pipe<LF2_PIPE_WARPS, false>;
+  using Kern = decltype(&k_move_pipe<LF2_PIPE_WARPS, false, false, false>);
+  const Kern kerns[2][4] = {
+      {k_move_pipe<LF2_PIPE_WARPS, false, false, false>, k_move_pipe<LF2_PIPE_WARPS, false, true, false>,
+       k_move_pipe<LF2_PIPE_WARPS, false, false, true>, k_move_pipe<LF2_PIPE_WARPS, false, true, true>},
+      {k_move_pipe<DEP_WARPS, true, false, false>, k_move_pipe<DEP_WARPS, true, true, false>,
+       k_move_pipe<DEP_WARPS, true, false, true>, k_move_pipe<DEP_WARPS, true, true, true>}};
+  const Kern kern = kerns[dep ? 1 : 0][(c->has_mass ? 1 : 0) + (c->has_id ? 2 : 0)];
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(c->work, 0, sizeof(int), c->stream);

@@ -226,9 +226,12 @@ void lf2o_rebin_lists(int64_t ncells, int64_t np, const int64_t* cs_old,
 /* ------------------------------------------------------------------------
  * Fixed-point momentum and stress deposits (device arithmetic restated).
  * Velocities are quantised against V = 2^e, the smallest power of two above
- * every |v_i| (lf2o_vexp); contributions are signed integers in units of
- * 2^-32 of a unit mass times V (momentum) or V^2 (stress), each rounded
- * once, so the sums are the device's bit for bit.  The vertex placement
+ * every |v_i| (lf2o_vexp), to 2^-31 V; products of two of them are kept
+ * exact (2^-62 V^2).  Contributions are signed integers in units of 2^-48 of
+ * a unit mass times V (momentum) or V^2 (stress), each rounded once from the
+ * exact product of the weight and the velocity term (a per-particle mass,
+ * in 2^-24 units, rounds it once more), so the sums are the device's bit for
+ * bit.  The vertex placement
  * follows the projections of the reference:
  *   kind 1  vectorProjectionCICNGP (projections.hpp:501-544)
  *   kind 2  symtensorProjectionCICNGP (:786-843)
@@ -257,7 +260,18 @@ static inline uint64_t corner3(uint32_t a, uint32_t b, uint32_t c)
   return (uint64_t)((prod + ((unsigned __int128)1 << 60)) >> 61);
 }
 
-static inline uint64_t mul31(uint64_t w, uint64_t f) { return (w * f + (1ull << 30)) >> 31; }
+/* round(a b / 2^s), the product exact in 128 bits */
+static inline uint64_t mulr(uint64_t a, uint64_t b, int s)
+{
+  const unsigned __int128 prod = (unsigned __int128)a * b;
+  return (uint64_t)((prod + ((unsigned __int128)1 << (s - 1))) >> s);
+}
+/* weight (2^-32) x velocity (2^-31 V) -> 2^-48 V */
+static inline uint64_t mul_wv48(uint64_t w, uint64_t f) { return mulr(w, f, 15); }
+/* weight (2^-32) x velocity product (2^-62 V^2) -> 2^-48 V^2 */
+static inline uint64_t mul_wvv48(uint64_t w, uint64_t vv) { return mulr(w, vv, 46); }
+/* 1-D weight (2^-31) x velocity product (2^-62 V^2) -> 2^-48 V^2 */
+static inline uint64_t mul_avv48(uint64_t a, uint64_t vv) { return mulr(a, vv, 45); }
 
 static inline int64_t signed_q(uint64_t q, const float* mrel, int64_t p, int neg)
 {
@@ -265,7 +279,7 @@ static inline int64_t signed_q(uint64_t q, const float* mrel, int64_t p, int neg
     float mr = mrel[p];
     mr = mr < 0.0f ? 0.0f : (mr > 63.0f ? 63.0f : mr);
     const uint64_t mq = (uint64_t)lrintf(mr * 16777216.0f);
-    q = (q * mq + (1ull << 23)) >> 24;
+    q = mulr(q, mq, 24);
   }
   return neg ? -(int64_t)q : (int64_t)q;
 }
@@ -311,7 +325,7 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
           if (c == 0) w = corner3(ONE, sq[1][a], sq[2][b]), site = SITE(xyz[0], vs[1][a], vs[2][b]);
           else if (c == 1) w = corner3(sq[0][a], ONE, sq[2][b]), site = SITE(vs[0][a], xyz[1], vs[2][b]);
           else w = corner3(sq[0][a], sq[1][b], ONE), site = SITE(vs[0][a], vs[1][b], xyz[2]);
-          acc[c * ns + site] += signed_q(mul31(w, vq[c]), mrel, p, neg);
+          acc[c * ns + site] += signed_q(mul_wv48(w, vq[c]), mrel, p, neg);
         }
       }
     } else if (kind == 2) {
@@ -321,17 +335,17 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
         const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
         const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
         for (int d = 0; d < 3; d++) {
-          const uint64_t v2 = ((uint64_t)vq[d] * vq[d] + (1ull << 30)) >> 31;
-          acc[diag[d] * ns + site] += signed_q(mul31(w, v2), mrel, p, 0);
+          const uint64_t v2 = (uint64_t)vq[d] * vq[d];
+          acc[diag[d] * ns + site] += signed_q(mul_wvv48(w, v2), mrel, p, 0);
         }
       }
       /* T_ij on the (i,j) plaquette, CIC along the third dim k */
       static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, pk[3] = {2, 1, 0}, comp[3] = {1, 2, 4};
       for (int q = 0; q < 3; q++) {
-        const uint64_t vv = ((uint64_t)vq[pa[q]] * vq[pb[q]] + (1ull << 30)) >> 31;
+        const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];
         const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
         for (int b = 0; b < 2; b++) {
-          const uint64_t qq = ((uint64_t)sq[pk[q]][b] * vv + (1ull << 29)) >> 30;
+          const uint64_t qq = mul_avv48(sq[pk[q]][b], vv);
           long c3[3] = {xyz[0], xyz[1], xyz[2]};
           c3[pk[q]] = vs[pk[q]][b];
           acc[comp[q] * ns + SITE(c3[0], c3[1], c3[2])] += signed_q(qq, mrel, p, neg);
@@ -349,7 +363,7 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
             cc[d] = d == c ? ts[d][bb[d]] : vs[d][bb[d]];
           }
           acc[c * ns + SITE(cc[0], cc[1], cc[2])] +=
-              signed_q(mul31(corner3(w[0], w[1], w[2]), vq[c]), mrel, p, neg);
+              signed_q(mul_wv48(corner3(w[0], w[1], w[2]), vq[c]), mrel, p, neg);
         }
       }
     } else if (kind == 4) {
@@ -359,13 +373,13 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
         const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
         const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
         for (int d = 0; d < 3; d++) {
-          const uint64_t v2 = ((uint64_t)vq[d] * vq[d] + (1ull << 30)) >> 31;
-          acc[diag[d] * ns + site] += signed_q(mul31(w, v2), mrel, p, 0);
+          const uint64_t v2 = (uint64_t)vq[d] * vq[d];
+          acc[diag[d] * ns + site] += signed_q(mul_wvv48(w, v2), mrel, p, 0);
         }
       }
       static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, comp[3] = {1, 2, 4};
       for (int q = 0; q < 3; q++) {
-        const uint64_t vv = ((uint64_t)vq[pa[q]] * vq[pb[q]] + (1ull << 30)) >> 31;
+        const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];
         const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
         for (int k = 0; k < 8; k++) {
           const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
@@ -377,7 +391,7 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
             cc[d] = st ? ts[d][bb[d]] : vs[d][bb[d]];
           }
           acc[comp[q] * ns + SITE(cc[0], cc[1], cc[2])] +=
-              signed_q(mul31(corner3(w[0], w[1], w[2]), vv), mrel, p, neg);
+              signed_q(mul_wvv48(corner3(w[0], w[1], w[2]), vv), mrel, p, neg);
         }
       }
     }

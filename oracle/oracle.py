@@ -239,10 +239,11 @@ def state_deposit_fixed_kind(kind, n, cell, off, vel, mrel=None, e=None):
 
 def fixed_kind_to_f32(acc, kind, e, gmass, res):
     """Converts a momentum / stress accumulator as the device does:
-    (float)q * (2^-32 m_unit / res^3 as FP32) * V^p, V^p an exact power of 2."""
+    (float)q * (2^-32 m_unit / res^3 as FP32) * 2^-16 V^p, the accumulator
+    being in units of 2^-48 of a unit mass times V^p (an exact power of 2)."""
     p = 1 if kind in (1, 3) else 2
     scale = np.float32(2.0 ** -32 * gmass / (res * res * res))
-    scale = np.float32(np.ldexp(scale, p * e))
+    scale = np.float32(np.ldexp(scale, p * e - 16))
     return (acc.astype(np.float32) * scale).astype(np.float32)
 
 
