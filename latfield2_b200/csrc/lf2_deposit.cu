@@ -205,11 +205,11 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
           } else if (PASS == 0) {
             // projections.hpp:788-807: T_ii = m v_i^2 at the 8 vertices
             const float vv[3] = {vx[j], vy[j], vz[j]};
-            uint64_t v2[3];  // exact squares, 2^-62 V^2 units
+            double f2[3];  // v_d^2 2^-46 (times the relative mass), FP64
   #pragma unroll
             for (int d = 0; d < 3; d++) {
-              const uint64_t q = vel_q(vv[d], vscale);
-              v2[d] = q * q;
+              const uint32_t q = vel_q(vv[d], vscale);
+              f2[d] = stress_factor<HM>(q, q, 0x1p-46, mq);  // 2^-46
             }
   #pragma unroll
             for (int k = 0; k < 8; k++) {
@@ -217,25 +217,26 @@ __global__ void __launch_bounds__(Pass<KIND, PASS, ACC>::THREADS) k_deposit(Stor
               const uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
               const int t = t0 + cx + cy * TY + cz * TZ;
   #pragma unroll
-              for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, TILE3>(smem_raw, d, t, mass_sign48_t<HM>(mul_wvv48(w, v2[d]), mq, false));
+              for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, TILE3>(smem_raw, d, t, stress_q(w, f2[d], false));
             }
           } else {
             // projections.hpp:809-821: T_ij on the (i,j) plaquette, CIC along
             // the third dim
             const float vv[3] = {vx[j], vy[j], vz[j]};
             const uint32_t q0 = vel_q(vv[0], vscale), q1 = vel_q(vv[1], vscale), q2 = vel_q(vv[2], vscale);
-            // exact velocity products, 2^-62 V^2 units
-            const uint64_t v01 = (uint64_t)q0 * q1, v02 = (uint64_t)q0 * q2, v12 = (uint64_t)q1 * q2;
+            // velocity products times 2^-45 (FP64): a 1-D weight in 2^-31
+            // units times one of them is in 2^-48 V^2 units
+            const double v01 = stress_factor<HM>(q0, q1, 0x1p-45, mq),
+                         v02 = stress_factor<HM>(q0, q2, 0x1p-45, mq),
+                         v12 = stress_factor<HM>(q1, q2, 0x1p-45, mq);
             const bool n01 = (vv[0] < 0.0f) != (vv[1] < 0.0f), n02 = (vv[0] < 0.0f) != (vv[2] < 0.0f),
                        n12 = (vv[1] < 0.0f) != (vv[2] < 0.0f);
-            // (2^-31 weight) x (2^-62 velocity product), rounded to 2^-48
-            auto w1 = [](uint32_t a, uint64_t f) { return mul_avv48(a, f); };
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0, mass_sign48_t<HM>(w1(qz[0], v01), mq, n01));
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0 + TZ, mass_sign48_t<HM>(w1(qz[1], v01), mq, n01));
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0, mass_sign48_t<HM>(w1(qy[0], v02), mq, n02));
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0 + TY, mass_sign48_t<HM>(w1(qy[1], v02), mq, n02));
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0, mass_sign48_t<HM>(w1(qx[0], v12), mq, n12));
-            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0 + 1, mass_sign48_t<HM>(w1(qx[1], v12), mq, n12));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0, stress_q(qz[0], v01, n01));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 0, t0 + TZ, stress_q(qz[1], v01, n01));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0, stress_q(qy[0], v02, n02));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 1, t0 + TY, stress_q(qy[1], v02, n02));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0, stress_q(qx[0], v12, n12));
+            add_fixed48_t<SPLIT, TILE3>(smem_raw, 2, t0 + 1, stress_q(qx[1], v12, n12));
           }
           continue;
         }

@@ -176,6 +176,36 @@ __device__ __forceinline__ uint64_t mul_round(uint64_t a, uint64_t b)
 __device__ __forceinline__ uint64_t mul_wvv48(uint64_t w, uint64_t vv) { return mul_round<46>(w, vv); }
 __device__ __forceinline__ uint64_t mul_avv48(uint64_t a, uint64_t vv) { return mul_round<45>(a, vv); }
 
+// Stress contributions in FP64: the weight w (an integer below 2^52, exact
+// in double) times a per-particle factor f = v_a v_b 2^-s (times the
+// relative mass), both products rounded by IEEE double multiplication, then
+// rounded to the nearest integer (half to even): units of 2^-48 V^2.  The
+// sequence is deterministic and restated in the oracle operation by
+// operation.
+__device__ __forceinline__ double u2d_exact(uint64_t w)  // w < 2^52
+{
+  return __dadd_rn(__longlong_as_double((long long)(0x4330000000000000ull | w)), -4503599627370496.0);
+}
+__device__ __forceinline__ uint64_t d2u_rn(double x)  // 0 <= x < 2^51
+{
+  const double y = __dadd_rn(x, 6755399441055744.0);  // 1.5 * 2^52: integer part in the low bits
+  return ((uint64_t)__double_as_longlong(y) & 0xFFFFFFFFFFFFFull) - (1ull << 51);
+}
+// f = (v_a v_b) 2^-s, times m / m_unit when HM (mq: the relative mass in
+// 2^-24 units)
+template <bool HM>
+__device__ __forceinline__ double stress_factor(uint32_t va, uint32_t vb, double scale, uint64_t mq)
+{
+  double f = __dmul_rn(__dmul_rn(u2d_exact(va), u2d_exact(vb)), scale);
+  if (HM) f = __dmul_rn(f, __dmul_rn(u2d_exact(mq), 0x1p-24));  // 2^-24
+  return f;
+}
+__device__ __forceinline__ long long stress_q(uint64_t w, double f, bool neg)
+{
+  const long long q = (long long)d2u_rn(__dmul_rn(u2d_exact(w), f));
+  return neg ? -q : q;
+}
+
 // Per-particle relative mass (2^-24 units) applied to a signed-kind
 // contribution (|q| <= 2^48, so the product needs 128 bits), then the sign.
 template <bool HM>

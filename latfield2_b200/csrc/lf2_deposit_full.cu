@@ -409,21 +409,21 @@ __global__ void __launch_bounds__(FULL2_THREADS)
             }
           }
         } else if (PASS == 1) {
-          uint64_t v2[3];
+          double f2[3];  // v_d^2 2^-46 (times the relative mass), FP64
   #pragma unroll
-          for (int d = 0; d < 3; d++) v2[d] = (uint64_t)vq[d] * vq[d];  // exact, 2^-62 V^2 units
+          for (int d = 0; d < 3; d++) f2[d] = stress_factor<HM>(vq[d], vq[d], 0x1p-46, mq);
   #pragma unroll
           for (int k = 0; k < 8; k++) {
             const int b0 = (k >> 2) & 1, b1 = (k >> 1) & 1, b2 = k & 1;
             const uint64_t w = fixed_corner(sq[0][b0], sq[1][b1], sq[2][b2]);
             const int t = tile_at(ls[0] + b0, ls[1] + b1, ls[2] + b2);
   #pragma unroll
-            for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, FT3>(smem_raw, d, t, mass_sign48_t<HM>(mul_wvv48(w, v2[d]), mq, false));
+            for (int d = 0; d < 3; d++) add_fixed48_t<SPLIT, FT3>(smem_raw, d, t, stress_q(w, f2[d], false));
           }
         } else {
   #pragma unroll
           for (int q = 0; q < 3; q++) {
-            const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];  // exact, 2^-62 V^2 units
+            const double vv = stress_factor<HM>(vq[pa[q]], vq[pb[q]], 0x1p-46, mq);  // 2^-46
             const bool neg = (vel[pa[q]] < 0.0f) != (vel[pb[q]] < 0.0f);
   #pragma unroll
             for (int k = 0; k < 8; k++) {
@@ -437,8 +437,7 @@ __global__ void __launch_bounds__(FULL2_THREADS)
                 t[d] = (st ? lt[d] : ls[d]) + bb[d];
               }
               add_fixed48_t<SPLIT, FT3>(smem_raw, q, tile_at(t[0], t[1], t[2]),
-                                        mass_sign48_t<HM>(mul_wvv48(fixed_corner(w[0], w[1], w[2]), vv),
-                                                          mq, neg));
+                                        stress_q(fixed_corner(w[0], w[1], w[2]), vv, neg));
             }
           }
         }

@@ -226,12 +226,11 @@ void lf2o_rebin_lists(int64_t ncells, int64_t np, const int64_t* cs_old,
 /* ------------------------------------------------------------------------
  * Fixed-point momentum and stress deposits (device arithmetic restated).
  * Velocities are quantised against V = 2^e, the smallest power of two above
- * every |v_i| (lf2o_vexp), to 2^-31 V; products of two of them are kept
- * exact (2^-62 V^2).  Contributions are signed integers in units of 2^-48 of
- * a unit mass times V (momentum) or V^2 (stress), each rounded once from the
- * exact product of the weight and the velocity term (a per-particle mass,
- * in 2^-24 units, rounds it once more), so the sums are the device's bit for
- * bit.  The vertex placement
+ * every |v_i| (lf2o_vexp), to 2^-31 V.  Contributions are signed integers in
+ * units of 2^-48 of a unit mass times V (momentum: the exact integer product
+ * of weight and velocity, rounded once; a per-particle mass in 2^-24 units
+ * rounds it once more) or V^2 (stress: stress_q, in FP64), so the sums are
+ * the device's bit for bit.  The vertex placement
  * follows the projections of the reference:
  *   kind 1  vectorProjectionCICNGP (projections.hpp:501-544)
  *   kind 2  symtensorProjectionCICNGP (:786-843)
@@ -268,10 +267,34 @@ static inline uint64_t mulr(uint64_t a, uint64_t b, int s)
 }
 /* weight (2^-32) x velocity (2^-31 V) -> 2^-48 V */
 static inline uint64_t mul_wv48(uint64_t w, uint64_t f) { return mulr(w, f, 15); }
-/* weight (2^-32) x velocity product (2^-62 V^2) -> 2^-48 V^2 */
-static inline uint64_t mul_wvv48(uint64_t w, uint64_t vv) { return mulr(w, vv, 46); }
-/* 1-D weight (2^-31) x velocity product (2^-62 V^2) -> 2^-48 V^2 */
-static inline uint64_t mul_avv48(uint64_t a, uint64_t vv) { return mulr(a, vv, 45); }
+
+/* Stress contributions in FP64 (the device's stress_q): the weight w (an
+ * integer below 2^52, exact as a double) times a per-particle factor
+ * f = (v_a v_b) 2^-s [times (mq 2^-24), the relative mass], each product
+ * rounded by IEEE double multiplication, then rounded to the nearest
+ * integer, half to even (1.5 2^52 added and its low mantissa bits taken, as
+ * the device does).  Units of 2^-48 V^2. */
+static inline uint64_t mq_of(const float* mrel, int64_t p)
+{
+  float mr = mrel[p];
+  mr = mr < 0.0f ? 0.0f : (mr > 63.0f ? 63.0f : mr);
+  return (uint64_t)lrintf(mr * 16777216.0f);
+}
+static inline double stress_factor(uint32_t va, uint32_t vb, int s, const float* mrel, int64_t p)
+{
+  double f = ((double)va * (double)vb) * ldexp(1.0, -s);
+  if (mrel) f = f * ((double)mq_of(mrel, p) * ldexp(1.0, -24));
+  return f;
+}
+static inline int64_t stress_q(uint64_t w, double f, int neg)
+{
+  double y = (double)w * f;
+  y = y + 6755399441055744.0;
+  uint64_t bits;
+  memcpy(&bits, &y, 8);
+  const int64_t q = (int64_t)((bits & 0xFFFFFFFFFFFFFull) - (1ull << 51));
+  return neg ? -q : q;
+}
 
 static inline int64_t signed_q(uint64_t q, const float* mrel, int64_t p, int neg)
 {
@@ -335,20 +358,18 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
         const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
         const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
         for (int d = 0; d < 3; d++) {
-          const uint64_t v2 = (uint64_t)vq[d] * vq[d];
-          acc[diag[d] * ns + site] += signed_q(mul_wvv48(w, v2), mrel, p, 0);
+          acc[diag[d] * ns + site] += stress_q(w, stress_factor(vq[d], vq[d], 46, mrel, p), 0);
         }
       }
       /* T_ij on the (i,j) plaquette, CIC along the third dim k */
       static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, pk[3] = {2, 1, 0}, comp[3] = {1, 2, 4};
       for (int q = 0; q < 3; q++) {
-        const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];
+        const double vv = stress_factor(vq[pa[q]], vq[pb[q]], 45, mrel, p);
         const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
         for (int b = 0; b < 2; b++) {
-          const uint64_t qq = mul_avv48(sq[pk[q]][b], vv);
           long c3[3] = {xyz[0], xyz[1], xyz[2]};
           c3[pk[q]] = vs[pk[q]][b];
-          acc[comp[q] * ns + SITE(c3[0], c3[1], c3[2])] += signed_q(qq, mrel, p, neg);
+          acc[comp[q] * ns + SITE(c3[0], c3[1], c3[2])] += stress_q(sq[pk[q]][b], vv, neg);
         }
       }
     } else if (kind == 3) {
@@ -373,13 +394,12 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
         const uint64_t w = corner3(sq[0][bx], sq[1][by], sq[2][bz]);
         const long site = SITE(vs[0][bx], vs[1][by], vs[2][bz]);
         for (int d = 0; d < 3; d++) {
-          const uint64_t v2 = (uint64_t)vq[d] * vq[d];
-          acc[diag[d] * ns + site] += signed_q(mul_wvv48(w, v2), mrel, p, 0);
+          acc[diag[d] * ns + site] += stress_q(w, stress_factor(vq[d], vq[d], 46, mrel, p), 0);
         }
       }
       static const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2}, comp[3] = {1, 2, 4};
       for (int q = 0; q < 3; q++) {
-        const uint64_t vv = (uint64_t)vq[pa[q]] * vq[pb[q]];
+        const double vv = stress_factor(vq[pa[q]], vq[pb[q]], 46, mrel, p);
         const int neg = (v[pa[q]] < 0.0f) != (v[pb[q]] < 0.0f);
         for (int k = 0; k < 8; k++) {
           const int bb[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
@@ -390,8 +410,7 @@ void lf2o_state_deposit_fixed_kind(int kind, const int n[3], int64_t np,
             w[d] = st ? tq[d][bb[d]] : sq[d][bb[d]];
             cc[d] = st ? ts[d][bb[d]] : vs[d][bb[d]];
           }
-          acc[comp[q] * ns + SITE(cc[0], cc[1], cc[2])] +=
-              signed_q(mul_wvv48(corner3(w[0], w[1], w[2]), vv), mrel, p, neg);
+          acc[comp[q] * ns + SITE(cc[0], cc[1], cc[2])] += stress_q(corner3(w[0], w[1], w[2]), vv, neg);
         }
       }
     }
