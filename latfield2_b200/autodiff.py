@@ -1,6 +1,7 @@
 """Differentiable multi-step particle-mesh chain on the CUDA kernels.
 
-Per step k (particles in the caller's order, no rebinning):
+Per step k (particles ordered by their initial cell, no rebinning; the
+gradients come back in the caller's order):
     rho_k   = deposit(x_k, m)                    lf2_pm_deposit      (CIC, projections.hpp:75-184)
     F_k     = stencil27(rho_k, S)                lf2_stencil27       (the grid operator), or
     F_k     = pm_force(rho_k)                    lf2_pm_force4       (the FFT Poisson force)
@@ -119,8 +120,14 @@ class PMChain(torch.autograd.Function):
         ops = _Ops(lf2ctx)
         n, res = lf2ctx.n, lf2ctx.res
         cell, off = positions_to_state(pos0.detach().to(torch.float64), n, res)
-        vel = vel0.detach().to(torch.float32).contiguous().clone()
-        m = mass.detach().to(torch.float32).contiguous()
+        # the chain runs on the particles ordered by cell (the deposits' and
+        # gathers' accesses are then local); the gradients go back to the
+        # caller's order at the end of the backward pass
+        order = torch.argsort(cell)
+        cell = cell[order].contiguous()
+        off = off[order].contiguous()
+        vel = vel0.detach().to(torch.float32)[order].contiguous()
+        m = mass.detach().to(torch.float32)[order].contiguous()
         S32 = None if S is None else S.detach().to(torch.float32).contiguous()
         w32 = w.detach().to(torch.float32).contiguous().reshape(-1)
         ckpts, rhos, Fs = {}, [], []
@@ -135,7 +142,7 @@ class PMChain(torch.autograd.Function):
         ops.deposit(cell, off, m, rhoK)
         loss = torch.dot(w32.to(torch.float64), rhoK.to(torch.float64))
         fctx.lf2 = (lf2ctx, steps, dt, checkpoint_every, ckpts, rhos, Fs, coupling)
-        fctx.save_for_backward(cell, off, m, S32, w32, rhoK)
+        fctx.save_for_backward(cell, off, m, S32, w32, rhoK, order)
         fctx.pos_dtype = pos0.dtype
         fctx.vel_dtype = vel0.dtype
         return loss
@@ -143,7 +150,7 @@ class PMChain(torch.autograd.Function):
     @staticmethod
     def backward(fctx, gloss):
         lf2ctx, steps, dt, every, ckpts, rhos, Fs, coupling = fctx.lf2
-        cellK, offK, m, S32, w32, rhoK = fctx.saved_tensors
+        cellK, offK, m, S32, w32, rhoK, order = fctx.saved_tensors
         ops = _Ops(lf2ctx)
         dev = cellK.device
         res = lf2ctx.res
@@ -178,10 +185,15 @@ class PMChain(torch.autograd.Function):
             else:
                 ops.pm_force_adj(g_F, g_rho, coupling)
             ops.deposit_adj(cell_k, off_k, m, g_rho, g_off, g_m)
-        g_pos = (g_off.to(torch.float64) / res).to(fctx.pos_dtype)
+        def caller_order(t, dtype):
+            out = torch.empty(t.shape, dtype=dtype, device=t.device)
+            out[order] = t.to(dtype)
+            return out
+
+        g_pos = caller_order(g_off.to(torch.float64) / res, fctx.pos_dtype)
         g_w = (rhoK * g).to(torch.float64)
         g_S = None if S32 is None else g_S.to(torch.float64)
-        return (g_pos, g_v.to(fctx.vel_dtype), g_m.to(torch.float64), g_S, g_w,
+        return (g_pos, caller_order(g_v, fctx.vel_dtype), caller_order(g_m, torch.float64), g_S, g_w,
                 None, None, None, None, None)
 
 
