@@ -63,8 +63,9 @@ typedef int lf2_status;
  * is within about 1e-7 of exact whatever the order (not bit-identical run to
  * run).  FIXED64: int64 fixed point, bit-exact run to run; quantum 2^-32 of
  * a unit mass (the global particle mass, or the mean of per-particle
- * masses), times V for momentum and V^2 for stress, V the smallest power of
- * two above every |v_i| of the particles.  FP32_PLAIN: FP32 atomics without
+ * masses) for the density, 2^-48 of a unit mass times V for momentum and
+ * times V^2 for stress, V the smallest power of two above every |v_i| of the
+ * particles.  FP32_PLAIN: FP32 atomics without
  * compensation, the fastest FP32 form; unordered additions leave a few 1e-6
  * of error in dense vertices. */
 #define LF2_DEPOSIT_FP32 0
@@ -108,7 +109,8 @@ lf2_status lf2_get_flags(lf2_ctx* ctx, uint32_t* flags, int clear);
  * [0, n0*n1*n2); off3/vel3 are AoS (3 per particle).  mass may be NULL
  * (global mass `global_mass`, the part_info mass, GLOBAL_MASS) or hold one
  * FP32 mass per particle (INDIVIDUAL_MASS, :400-425).  id may be NULL (no
- * IDs carried). */
+ * IDs carried).  The store holds at most 2^32 - 1 slots (about 1.25 n plus
+ * 100 per brick): larger sets are refused with LF2_ERR_UNSUPPORTED. */
 lf2_status lf2_particles_set(lf2_ctx* ctx, int64_t n, const int32_t* cell,
                              const float* off3, const float* vel3,
                              const float* mass, double global_mass,
