@@ -901,16 +901,20 @@ def main():
     l0 = ctx.kernel_launches()
     rb0 = ctx.rebin_stats()
 
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # one event between consecutive steps (the library runs on torch's current
+    # stream): the total over the K steps and each step's own time
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    e0, e1 = evs[0], evs[-1]
     with ClockSampler(local) as clocks:
         barrier()
         torch.cuda.synchronize()
         e0.record()
-        for _ in range(args.steps):
+        for k in range(args.steps):
             ctx.step(Fh, dtau, dtau, rho)
-        e1.record()
+            evs[k + 1].record()
         torch.cuda.synchronize()
         barrier()
+    step_times = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     launches = ctx.kernel_launches() - l0
     rb1 = ctx.rebin_stats()
     rebin = {"repacks": rb1[0] - rb0[0], "relocations": rb1[1] - rb0[1],
@@ -1026,6 +1030,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step_median": statistics.median(step_times), "ms_per_step_min": min(step_times),
             "dtype": "f32 (int64 fixed-point deposit)" if mode == L.DEPOSIT_FIXED64 else "f32",
             "data": "synthetic (seeded)",
             "config": workload_config(args.workload),
