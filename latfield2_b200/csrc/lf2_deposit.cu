@@ -424,8 +424,8 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
     conv = ldexpf(fixed_scale, KIND == 0 ? 0 : (KIND == 1 ? vexp : 2 * vexp) - 16);
   }
   const int nface = ey * ez + (ex - 1) * ez + (ex - 1) * (ey - 1);
-  for (int f = threadIdx.x; f < nface; f += blockDim.x) {
-    int i, j, k;
+  // owned face vertex number f -> tile coordinates
+  auto face_vertex = [&](int f, int& i, int& j, int& k) {
     if (f < ey * ez) {  // x face: i = 0
       i = 0;
       j = f % ey;
@@ -441,43 +441,105 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
       i = 1 + r % (ex - 1);
       j = 1 + r / (ex - 1);
     }
-    const int zmask = (i == 0 ? 1 : 0) | (j == 0 ? 2 : 0) | (k == 0 ? 4 : 0);
-    long long qs[C];
-    float fs[C], fc[C];
+  };
+  if constexpr (C == 1) {
+    // One component: two vertices per thread, all their shell reads issued
+    // before any is used (the pass is bound by the latency of these
+    // scattered reads).  Subset s of a vertex's zero coordinates is read
+    // when (s & zmask) == s; the sum runs over s in ascending order.
+    const float* spf = reinterpret_cast<const float*>(spill);
+    for (int f0 = threadIdx.x; f0 < nface; f0 += 2 * blockDim.x) {
+      int vi[2], vj[2], vk[2], zm[2];
+      bool on[2];
 #pragma unroll
-    for (int c = 0; c < C; c++) {
-      qs[c] = 0;
-      fs[c] = 0.0f;
-      fc[c] = 0.0f;
-    }
-    // the subsets s of zmask in ascending order (s -> (s - zmask) & zmask)
-    for (int s = 0;; s = (s - zmask) & zmask) {
-      const uint32_t nb = nbr[s];
-      const int si = shell_index((s & 1) ? BRICK : i, (s & 2) ? BRICK : j, (s & 4) ? BRICK : k);
-      const uint64_t* sp = spill + (size_t)nb * (C * SHELL);
+      for (int h = 0; h < 2; h++) {
+        const int f = f0 + h * blockDim.x;
+        on[h] = f < nface;
+        vi[h] = vj[h] = vk[h] = 0;
+        if (on[h]) face_vertex(f, vi[h], vj[h], vk[h]);
+        zm[h] = on[h] ? (vi[h] == 0 ? 1 : 0) | (vj[h] == 0 ? 2 : 0) | (vk[h] == 0 ? 4 : 0) : 0;
+      }
+      long long qa = 0, qb = 0;
+      float fa = 0.0f, ca = 0.0f, fb = 0.0f, cb = 0.0f;
+      auto read = [&](int h, int s) -> uint64_t {
+        const int si = shell_index((s & 1) ? BRICK : vi[h], (s & 2) ? BRICK : vj[h], (s & 4) ? BRICK : vk[h]);
+        // a brick's shell region is SHELL 8-byte slots; the plain mode
+        // fills its first SHELL floats
+        const size_t at = (size_t)nbr[s] * SHELL;
+        return ACC == ACC_PLAIN ? (uint64_t)__float_as_uint(spf[2 * at + si]) : spill[at + si];
+      };
+      auto add = [&](long long& q, float& fs, float& fc, uint64_t raw) {
+        if (ACC == ACC_FIXED)
+          q += (long long)raw;
+        else if (ACC == ACC_COMP)
+          comp_acc(fs, fc, __uint_as_float((uint32_t)raw), __uint_as_float((uint32_t)(raw >> 32)));
+        else
+          fs = __fadd_rn(fs, __uint_as_float((uint32_t)raw));
+      };
 #pragma unroll
-      for (int c = 0; c < C; c++) {
+      for (int s = 0; s < 8; s++) {
+        const bool ua = on[0] && (s & zm[0]) == s, ub = on[1] && (s & zm[1]) == s;
+        const uint64_t ra = ua ? read(0, s) : 0ull;
+        const uint64_t rb = ub ? read(1, s) : 0ull;
+        if (ua) add(qa, fa, ca, ra);
+        if (ub) add(qb, fb, cb, rb);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (!on[h]) continue;
+        const int64_t site = site_index(g, x0 + vi[h], y0 + vj[h], z0 + vk[h]);
+        const long long q = h ? qb : qa;
         if (ACC == ACC_FIXED) {
-          qs[c] += (long long)sp[c * SHELL + si];
-        } else if (ACC == ACC_COMP) {
-          const float2 hl = reinterpret_cast<const float2*>(sp)[c * SHELL + si];
-          comp_acc(fs[c], fc[c], hl.x, hl.y);
+          if (!SIGNED && q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+          out[site] = __fmul_rn(__ll2float_rn(q), conv);
         } else {
-          fs[c] = __fadd_rn(fs[c], reinterpret_cast<const float*>(sp)[c * SHELL + si]);
+          const float fs = h ? fb : fa, fc = h ? cb : ca;
+          out[site] = ACC == ACC_COMP ? __fadd_rn(fs, fc) : fs;
         }
       }
-      if (s == zmask) break;
     }
-    const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
-#pragma unroll
-    for (int c = 0; c < C; c++) {
-      if (ACC == ACC_FIXED) {
-        if (!SIGNED && qs[c] < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-        out[c * g.nsites + site] = __fmul_rn(__ll2float_rn(qs[c]), conv);
-      } else if (ACC == ACC_COMP) {
-        out[c * g.nsites + site] = __fadd_rn(fs[c], fc[c]);
-      } else {
-        out[c * g.nsites + site] = fs[c];
+  } else {
+    for (int f = threadIdx.x; f < nface; f += blockDim.x) {
+      int i, j, k;
+      face_vertex(f, i, j, k);
+      const int zmask = (i == 0 ? 1 : 0) | (j == 0 ? 2 : 0) | (k == 0 ? 4 : 0);
+      long long qs[C];
+      float fs[C], fc[C];
+  #pragma unroll
+      for (int c = 0; c < C; c++) {
+        qs[c] = 0;
+        fs[c] = 0.0f;
+        fc[c] = 0.0f;
+      }
+      // the subsets s of zmask in ascending order (s -> (s - zmask) & zmask)
+      for (int s = 0;; s = (s - zmask) & zmask) {
+        const uint32_t nb = nbr[s];
+        const int si = shell_index((s & 1) ? BRICK : i, (s & 2) ? BRICK : j, (s & 4) ? BRICK : k);
+        const uint64_t* sp = spill + (size_t)nb * (C * SHELL);
+  #pragma unroll
+        for (int c = 0; c < C; c++) {
+          if (ACC == ACC_FIXED) {
+            qs[c] += (long long)sp[c * SHELL + si];
+          } else if (ACC == ACC_COMP) {
+            const float2 hl = reinterpret_cast<const float2*>(sp)[c * SHELL + si];
+            comp_acc(fs[c], fc[c], hl.x, hl.y);
+          } else {
+            fs[c] = __fadd_rn(fs[c], reinterpret_cast<const float*>(sp)[c * SHELL + si]);
+          }
+        }
+        if (s == zmask) break;
+      }
+      const int64_t site = site_index(g, x0 + i, y0 + j, z0 + k);
+  #pragma unroll
+      for (int c = 0; c < C; c++) {
+        if (ACC == ACC_FIXED) {
+          if (!SIGNED && qs[c] < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+          out[c * g.nsites + site] = __fmul_rn(__ll2float_rn(qs[c]), conv);
+        } else if (ACC == ACC_COMP) {
+          out[c * g.nsites + site] = __fadd_rn(fs[c], fc[c]);
+        } else {
+          out[c * g.nsites + site] = fs[c];
+        }
       }
     }
   }

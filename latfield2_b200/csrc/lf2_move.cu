@@ -329,9 +329,11 @@ __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* 
   for (int64_t base = warp0 * 32; base < nm; base += nwarps * 32) {
     const int64_t m = base + lane;
     int64_t b = -1;
+    uint32_t key = 0;
     if (m < nm) {
       int x, y, z;
-      unpack_key(v.g, mov.key[m], x, y, z);
+      key = mov.key[m];
+      unpack_key(v.g, key, x, y, z);
       if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move
         set_flag(flags, ERR_BAD_CELL);
         placed[m] = 1;
@@ -350,15 +352,21 @@ __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* 
     if (b < 0) continue;
     if (slot < v.cap[b]) {
       const int64_t q = v.seg_start[b] + slot;
-      v.a.key[q] = mov.key[m];
-      v.a.ox[q] = mov.ox[m];
-      v.a.oy[q] = mov.oy[m];
-      v.a.oz[q] = mov.oz[m];
-      v.a.vx[q] = mov.vx[m];
-      v.a.vy[q] = mov.vy[m];
-      v.a.vz[q] = mov.vz[m];
-      if (v.a.mass) v.a.mass[q] = mov.mass[m];
-      if (v.a.id) v.a.id[q] = mov.id[m];
+      // every array read before any is written (the compiler cannot tell
+      // that the mover buffer and the store do not overlap)
+      const float ox = mov.ox[m], oy = mov.oy[m], oz = mov.oz[m];
+      const float vx = mov.vx[m], vy = mov.vy[m], vz = mov.vz[m];
+      const float ms = v.a.mass ? mov.mass[m] : 0.0f;
+      const int64_t id = v.a.id ? mov.id[m] : 0;
+      v.a.key[q] = key;
+      v.a.ox[q] = ox;
+      v.a.oy[q] = oy;
+      v.a.oz[q] = oz;
+      v.a.vx[q] = vx;
+      v.a.vy[q] = vy;
+      v.a.vz[q] = vz;
+      if (v.a.mass) v.a.mass[q] = ms;
+      if (v.a.id) v.a.id[q] = id;
       placed[m] = 1;
     } else {
       placed[m] = 0;  // the brick is full: it gets relocated (lf2_store.cu)

@@ -232,17 +232,64 @@ __global__ void __launch_bounds__(1024) k_repack_caps(int64_t nb, const int32_t*
   }
 }
 
+// One particle's arrays, read before any is written (source and destination
+// may be the same arrays, so interleaved loads and stores would wait for
+// each other).
+struct PartVal {
+  uint32_t key;
+  float ox, oy, oz, vx, vy, vz, m;
+  int64_t id;
+};
+
+__device__ inline PartVal load_particle(const PartArrays& s, int64_t ps)
+{
+  PartVal p;
+  p.key = s.key[ps];
+  p.ox = s.ox[ps];
+  p.oy = s.oy[ps];
+  p.oz = s.oz[ps];
+  p.vx = s.vx[ps];
+  p.vy = s.vy[ps];
+  p.vz = s.vz[ps];
+  p.m = s.mass ? s.mass[ps] : 0.0f;
+  p.id = s.id ? s.id[ps] : 0;
+  return p;
+}
+
+__device__ inline void store_particle(const PartArrays& d, int64_t pd, const PartVal& p)
+{
+  d.key[pd] = p.key;
+  d.ox[pd] = p.ox;
+  d.oy[pd] = p.oy;
+  d.oz[pd] = p.oz;
+  d.vx[pd] = p.vx;
+  d.vy[pd] = p.vy;
+  d.vz[pd] = p.vz;
+  if (d.mass) d.mass[pd] = p.m;
+  if (d.id) d.id[pd] = p.id;
+}
+
 __device__ inline void copy_particle(const PartArrays& s, int64_t ps, const PartArrays& d, int64_t pd)
 {
-  d.key[pd] = s.key[ps];
-  d.ox[pd] = s.ox[ps];
-  d.oy[pd] = s.oy[ps];
-  d.oz[pd] = s.oz[ps];
-  d.vx[pd] = s.vx[ps];
-  d.vy[pd] = s.vy[ps];
-  d.vz[pd] = s.vz[ps];
-  if (d.mass) d.mass[pd] = s.mass[ps];
-  if (d.id) d.id[pd] = s.id[ps];
+  store_particle(d, pd, load_particle(s, ps));
+}
+
+// Copies n consecutive particles, four per thread in flight.
+__device__ inline void copy_run(const PartArrays& s, int64_t s0, const PartArrays& d, int64_t d0, int n)
+{
+  for (int i = threadIdx.x; i < n; i += 4 * blockDim.x) {
+    PartVal v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = i + u * (int)blockDim.x;
+      if (k < n) v[u] = load_particle(s, s0 + k);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = i + u * (int)blockDim.x;
+      if (k < n) store_particle(d, d0 + k, v[u]);
+    }
+  }
 }
 
 // The per-brick repack kernels run on a small grid (grid-stride over bricks)
@@ -254,7 +301,7 @@ __global__ void k_repack_copy_out(StoreView v, PartArrays alt, const int64_t* __
   for (int64_t b = blockIdx.x; b < v.g.nbricks; b += gridDim.x) {
     const int placed = min(v.count[b], v.cap[b]);
     const int64_t s0 = v.seg_start[b], d0 = start_alt[b];
-    for (int i = threadIdx.x; i < placed; i += blockDim.x) copy_particle(v.a, s0 + i, alt, d0 + i);
+    copy_run(v.a, s0, alt, d0, placed);
     if (threadIdx.x == 0) fill[b] = placed;
   }
 }
@@ -283,7 +330,7 @@ __global__ void k_repack_copy_back(StoreView v, PartArrays alt, const int64_t* _
   for (int64_t b = blockIdx.x; b < v.g.nbricks; b += gridDim.x) {
     const int n = fill[b];
     const int64_t d0 = start_alt[b];
-    for (int i = threadIdx.x; i < n; i += blockDim.x) copy_particle(alt, d0 + i, v.a, d0 + i);
+    copy_run(alt, d0, v.a, d0, n);
     if (threadIdx.x == 0) v.count[b] = n;
   }
 }
@@ -340,7 +387,7 @@ __global__ void k_reloc(StoreView v, int64_t* seg_start, int32_t* cap, const int
     const long long d0 = s_new;
     if (d0 >= 0) {
       const int64_t s0 = seg_start[b];
-      for (int k = threadIdx.x; k < placed; k += blockDim.x) copy_particle(v.a, s0 + k, v.a, d0 + k);
+      copy_run(v.a, s0, v.a, d0, placed);
       __syncthreads();
       if (threadIdx.x == 0) {
         seg_start[b] = d0;
