@@ -731,7 +731,8 @@ def fp32_step_ms(n, case, F, npart, dtau, warmup, steps, local, mode, proj_peak=
 
 def chain_step_times(n, case, npart, local, reps=2):
     """One step of the differentiable particle-mesh chain on the workload's
-    own particles (caller order, per-particle state): deposit, PM force (FFT
+    own particles (per-particle state, in a context of the fixed-point mode:
+    the chain's deposits sum integer weights): deposit, PM force (FFT
     Poisson solve, coupling 4 pi), CIC gather, kick, drift and the final
     deposit of the loss, then its hand-written adjoint (autodiff.PMChain,
     checkpoint every step).  Device times (CUDA events) of the forward alone
@@ -749,7 +750,7 @@ def chain_step_times(n, case, npart, local, reps=2):
     m = torch.full((npart,), 1.0 / npart, dtype=torch.float64, device=pos.device)
     g = torch.Generator(device=pos.device).manual_seed(7)
     w = torch.randn(nn ** 3, generator=g, device=pos.device, dtype=torch.float64)
-    ctx = L.Context(n, box=1.0, device=local)
+    ctx = L.Context(n, box=1.0, mode=L.DEPOSIT_FIXED64, device=local)  # fixed-point deposits
     dt = 0.1 * 64.0 / nn
 
     def timed(grad):
@@ -997,6 +998,10 @@ def main():
     # same particles, beside the library's fixed-point and plain FP32 forward
     c5 = None
     if args.workload == "c5" and fp32_case is not None and not args.no_adjoint and world == 1:
+        if "ctx" in locals():  # the step's store and fields make room for the chain's state
+            ctx.close()
+            del ctx, Fh, rho
+            torch.cuda.empty_cache()
         try:
             chain = chain_step_times(n, fp32_case, npart, local)
         except torch.cuda.OutOfMemoryError as e:  # the chain keeps every field of the step
@@ -1008,8 +1013,8 @@ def main():
               "forward_adjoint_ms": chain["forward_adjoint_ms"], "chain": chain,
               "note": "forward_ms: lf2_step (kick, drift, rebin, fixed-point deposit); "
                       "fp32_forward_ms: the same with the plain FP32-atomic deposit; "
-                      "forward_adjoint_ms: one step of the differentiable chain and its adjoint "
-                      "(chain.forward_ms its forward alone)"}
+                      "forward_adjoint_ms: one step of the differentiable chain (fixed-point deposits) "
+                      "and its adjoint (chain.forward_ms its forward alone)"}
     del fp32_case
 
     if rank == 0:

@@ -363,7 +363,11 @@ lf2_status lf2_pm_gradient(lf2_ctx* ctx, lf2_field phi, lf2_field F);
  * (+=) are accumulated.  mass may be NULL (global mass gmass).
  * The force field F4 and its gradient g_F4 hold one float4 (x, y, z, unused)
  * per site, in site order, 16-byte aligned (LF2_ERR_ARG otherwise).
- *   deposit          rho (+=) m/res^3 W                (FP32 atomics)
+ *   deposit          rho (+=) m/res^3 W                (FP32 atomics; in a
+ *                    context of the fixed-point mode: 64-bit integer sums of
+ *                    the deterministic corner weights of lf2_deposit_scalar,
+ *                    times m / M in 2^-24 units with M the largest mass of
+ *                    the call, converted once, so independent of the order)
  *   gather           out3[p] = sum_k W_k F4(corner_k)
  *   kick_drift       vel += dt_kick * G3 (G3 may be NULL); off += dt_drift/res
  *                    * vel with the carry into cell

@@ -370,6 +370,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->ovf_state);
   cudaFree(c->spill);
   cudaFree(c->stencil_partial);
+  cudaFree(c->pm_acc);
   fft_release(c);
   cudaFreeHost(c->h_stats);
   cudaFreeHost(c->h_flags);

@@ -95,6 +95,7 @@ struct lf2_ctx {
   uint32_t* vmax_bits = nullptr;     // device: largest |v_i| (float bits), fixed-point deposits
   uint32_t* redep = nullptr;         // device: the fused deposit must be redone by the tile pass
   float* stencil_partial = nullptr;  // per-CTA partial sums of the stencil weight gradient
+  unsigned long long* pm_acc = nullptr; // chain's fixed-point deposit: [nsites] sums + max mass word
   size_t spill_slots = 0;
   double* h_stats = nullptr;         // pinned [8]
   uint32_t* h_flags = nullptr;       // pinned

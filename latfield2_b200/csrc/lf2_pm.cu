@@ -23,6 +23,7 @@
 // that a corner is one 16-byte load and one vector atomic.
 #include <cuda_runtime.h>
 
+#include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
 namespace lf2 {
@@ -76,6 +77,62 @@ __global__ void k_pm_deposit(Geom g, int64_t np, const int32_t* __restrict__ cel
     const float m = (mass ? mass[p] : gmass) * inv_vol;
 #pragma unroll
     for (int q = 0; q < 8; q++) atomicAdd(&rho[k.site[q]], k.w[q] * m);
+  }
+}
+
+// Fixed-point form of the chain's deposit (contexts in LF2_DEPOSIT_FIXED64):
+// every corner's weight is the library's deterministic integer weight
+// (fixed_corner, 2^-32 units), times the particle's mass relative to the
+// largest mass M of the call in 2^-24 units; the integer sums (64-bit global
+// atomics) do not depend on the order, and are converted once:
+// rho += (float)sum * (M / res^3 * 2^-32).
+__global__ void k_pm_mass_max(int64_t np, const float* __restrict__ mass, uint32_t* mmax)
+{
+  uint32_t m = 0u;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(fmaxf(mass[p], 0.0f)));  // non-negative floats order as integers
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(mmax, m);
+}
+
+__global__ void k_pm_deposit_fixed(Geom g, int64_t np, const int32_t* __restrict__ cell,
+                                   const float* __restrict__ off3, const float* __restrict__ mass,
+                                   const uint32_t* __restrict__ mmax, unsigned long long* __restrict__ acc)
+{
+  const float inv_m = mass ? 1.0f / __uint_as_float(*mmax) : 0.0f;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = cell[p];
+    const int x = c % g.n[0], y = (c / g.n[0]) % g.n[1], z = c / (g.n[0] * g.n[1]);
+    const int xs[2] = {x, x + 1 < g.n[0] ? x + 1 : 0};
+    const int ys[2] = {y, y + 1 < g.n[1] ? y + 1 : 0};
+    const int zs[2] = {z, z + 1 < g.n[2] ? z + 1 : 0};
+    const uint32_t ux = weight_q(off3[3 * p]), uy = weight_q(off3[3 * p + 1]), uz = weight_q(off3[3 * p + 2]);
+    const uint32_t qx[2] = {(1u << 31) - ux, ux}, qy[2] = {(1u << 31) - uy, uy}, qz[2] = {(1u << 31) - uz, uz};
+    const uint64_t mq = mass ? (uint64_t)__float2uint_rn(fminf(__fmul_rn(mass[p], inv_m), 1.0f) * 16777216.0f) : 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int bx = (q >> 2) & 1, by = (q >> 1) & 1, bz = q & 1;
+      uint64_t w = fixed_corner(qx[bx], qy[by], qz[bz]);
+      if (mass) w = (w * mq + (1ull << 23)) >> 24;
+      atomicAdd(&acc[site_index(g, xs[bx], ys[by], zs[bz])], (unsigned long long)w);
+    }
+  }
+}
+
+__global__ void k_pm_fixed_to_rho(int64_t ns, unsigned long long* __restrict__ acc, const float* mass,
+                                  const uint32_t* __restrict__ mmax, float gmass, float inv_vol,
+                                  float* __restrict__ rho, uint32_t* flags)
+{
+  const float m = mass ? __uint_as_float(*mmax) : gmass;
+  const float scale = ldexpf(__fmul_rn(m, inv_vol), -32);
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const long long q = (long long)acc[s];
+    if (q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+    rho[s] = __fadd_rn(rho[s], __fmul_rn(__ll2float_rn(q), scale));
+    acc[s] = 0ull;  // clean for the next call
   }
 }
 
@@ -351,6 +408,28 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
   const Geom g = c->g;
   switch (op) {
     case 0:  // deposit into out_a
+      if (c->mode == LF2_DEPOSIT_FIXED64) {
+        // integer sums in the context's scratch (zero between calls)
+        if (!c->pm_acc) {
+          cudaError_t e = cudaMalloc(&c->pm_acc, sizeof(unsigned long long) * (size_t)g.nsites + 256);
+          if (e != cudaSuccess) return e;
+          e = cudaMemsetAsync(c->pm_acc, 0, sizeof(unsigned long long) * (size_t)g.nsites + 256, c->stream);
+          if (e != cudaSuccess) return e;
+        }
+        uint32_t* mmax = reinterpret_cast<uint32_t*>(c->pm_acc + g.nsites);
+        if (mass) {
+          cudaError_t e = cudaMemsetAsync(mmax, 0, sizeof(uint32_t), c->stream);
+          if (e != cudaSuccess) return e;
+          c->launches += 1;
+          k_pm_mass_max<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(np, mass, mmax);
+        }
+        c->launches += 2;
+        k_pm_deposit_fixed<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3,
+                                                                                  mass, mmax, c->pm_acc);
+        k_pm_fixed_to_rho<<<grid_for(g.nsites, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+            g.nsites, c->pm_acc, mass, mmax, gmass, inv_vol, out_a, c->flags);
+        break;
+      }
       c->launches += 1;
       k_pm_deposit<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3, mass,
                                                                             gmass, inv_vol, out_a);

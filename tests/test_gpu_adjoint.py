@@ -222,3 +222,68 @@ def test_pm_chain_gradients_against_fp64(cuda):
     assert np.max(np.abs(an_ref - fd)) < 1e-5 * scale
     assert np.max(np.abs(an_dev - fd)) < 5e-3 * scale
     ctx.close()
+
+
+@pytest.mark.parametrize("masses", [False, True])
+def test_fixed_point_chain_deposit(cuda, masses):
+    """The chain's deposit in a context of the fixed-point mode: integer sums
+    of the library's corner weights (times the mass relative to the call's
+    largest mass), so the density is the same bits in any particle order and
+    within 1e-6 of the FP64 deposit; the 8-step chain's gradients match the
+    FP64 gradient as the FP32-mode chain's do (the adjoint kernels are
+    shared)."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops, pm_chain_loss
+    from tests.helpers import precision
+    n, npart = 32, 60000
+    pos, vel, m, S, w = _case(n, npart, 5, "cuda")
+    # a clump on top of the uniform particles: dense vertices
+    pos[: npart // 3] = (0.5 + 0.02 * torch.randn(npart // 3, 3, dtype=torch.float64,
+                                                  device="cuda")) % 1.0
+    ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64)
+    ops = _Ops(ctx)
+    cell, off = _state(pos, n)
+    m32 = m.float().contiguous()
+    gm = 1.0 / npart
+    posd = ((torch.stack([cell.long() % n, (cell.long() // n) % n, cell.long() // (n * n)], 1)
+             .double() + off.double()) / n)
+    mass = m32.double() if masses else torch.full((npart,), gm, dtype=torch.float64, device="cuda")
+    ref = P.deposit(posd, mass, (n, n, n)).cpu().numpy()
+    outs = []
+    for perm in (torch.arange(npart, device="cuda"), torch.randperm(npart, device="cuda")):
+        rho = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+        if masses:
+            ops.deposit(cell[perm].contiguous(), off[perm].contiguous(), m32[perm].contiguous(), rho)
+        else:
+            rc = ops.lib.lf2_pm_deposit(ctx.h, npart, ops_ptr(cell[perm].contiguous()),
+                                        ops_ptr(off[perm].contiguous()), None, gm, ops_ptr(rho))
+            assert rc == 0
+        torch.cuda.synchronize()
+        outs.append(rho.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])  # order-free integer sums
+    p = precision(outs[0], ref)
+    assert p["norm_max"] <= 1e-6 and p["cell_max"] <= 1e-6, p
+    ctx.synchronize()
+    ctx.close()
+    # the 8-step chain with the fixed-point deposits against the FP64 gradient
+    # (uniform particles, the tolerance of the FP32-mode chain's test)
+    n, npart = 32, 20000
+    pos, vel, m, S, w = _case(n, npart, 7, "cuda")
+    cell, off = _state(pos, n)
+    posd = ((torch.stack([cell.long() % n, (cell.long() // n) % n, cell.long() // (n * n)], 1)
+             .double() + off.double()) / n)
+    vel, m, S, w = vel.float().double(), m.float().double(), S.float().double(), w.float().double()
+    ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64)
+    leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, S, w)]
+    pm_chain_loss(ctx, *leaves, steps=8, dt=0.1, checkpoint_every=2).backward()
+    ref_leaves = [t.clone().requires_grad_(True) for t in (posd, vel, m, S, w)]
+    ref = torch.autograd.grad(P.chain_loss(*ref_leaves, (n, n, n), 8, 0.1), ref_leaves)
+    for name, a, b in zip(("pos", "vel", "mass", "stencil", "weights"), leaves, ref):
+        assert _rel(a.grad, b) < 2e-3, name
+    ctx.close()
+
+
+def ops_ptr(t):
+    import ctypes
+    return ctypes.c_void_p(t.data_ptr())
