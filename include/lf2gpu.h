@@ -8,8 +8,9 @@
  * codes.  The C++ compatibility layer (include/latfield2_b200.hpp) and the
  * Python package (latfield2_b200) are both written on top of these functions.
  *
- * Sections: context; particles (set, get, the slab-exchange pair
- * extract_z / add, checkpoint); fields; projections (scalar CIC, vector and
+ * Sections: context; particles (set, get, the slab exchange: extract_z /
+ * add and the migration records of slab_count / slab_extract / slab_insert,
+ * checkpoint); fields; projections (scalar CIC, vector and
  * symtensor CIC-NGP, full-CIC vector and VecVec); particle moves (kick,
  * drift and rebin, the fused step); PM grid operator (k-fields, FFT, Poisson
  * force); differentiable PM chain; the no-allocation deposit; measurement.
@@ -151,6 +152,37 @@ lf2_status lf2_particles_extract_z(lf2_ctx* ctx, int z_lo, int z_hi,
 lf2_status lf2_particles_add(lf2_ctx* ctx, int64_t n, const int32_t* cell,
                              const float* off3, const float* vel3,
                              const float* mass, const int64_t* id, int ptr_kind);
+/* The same migration in stream order, without host waits (the form a step
+ * over several GPUs uses: the caller reads the counts once, together with
+ * whatever else it needs, and sizes the messages from them).  A migration
+ * record is record_words = 7 + has_mass + 2 has_id 32-bit words: cell index,
+ * offsets (3) and velocities (3) as float bits[, mass][, id low word, id high
+ * word].  All pointers are DEVICE memory.
+ *   slab_count: counts[0..3] <- the particles with cell z below z_lo, above
+ *     z_hi, and more than one plane outside [z_lo, z_hi] (these cannot be
+ *     routed to a neighbour), and max |v|^2 after the last kick (0 before
+ *     any) as the bits of a float: non-negative floats order as their bits,
+ *     so an integer maximum over ranks is the float maximum.
+ *   slab_extract: the particles outside [z_lo, z_hi] leave the store, those
+ *     below z_lo as n_below records in `below`, those above z_hi as n_above
+ *     records in `above` (any order), each with the cell index it has in the
+ *     neighbouring slab's lattice: z moved by +nz (below) or -nz (above),
+ *     nz = z_hi - z_lo + 1.  n_below and n_above must be the counts
+ *     slab_count gave for the same store; a particle beyond them is lost and
+ *     raises LF2_FLAG_CAPACITY.
+ *   slab_insert: n_a records from `a` and n_b from `b` join the store through
+ *     the mover path.  A record with a cell index or offset out of range is
+ *     dropped and raises LF2_FLAG_BAD_CELL (the store is then not valid).
+ *     When the store lacks room the records go through lf2_particles_add,
+ *     which waits.
+ * Raised flags fail the context's next waiting call (lf2_synchronize) with
+ * LF2_ERR_STATE. */
+lf2_status lf2_slab_record_words(lf2_ctx* ctx, int* words);
+lf2_status lf2_slab_count(lf2_ctx* ctx, int z_lo, int z_hi, int64_t* counts);
+lf2_status lf2_slab_extract(lf2_ctx* ctx, int z_lo, int z_hi, int64_t n_below,
+                            uint32_t* below, int64_t n_above, uint32_t* above);
+lf2_status lf2_slab_insert(lf2_ctx* ctx, int64_t n_a, const uint32_t* a,
+                           int64_t n_b, const uint32_t* b);
 /* Checkpoint of the particle store for an exact restart: the library's
  * particle state (cell, offsets, velocities, mass, id) and the unit mass of
  * the fixed-point deposit, written to / read from a little-endian file: an

@@ -73,6 +73,10 @@ SIGNATURES = {
                                 c_void_p, c_void_p, P(c_i64)],
     "lf2_particles_add": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                           c_int],
+    "lf2_slab_record_words": [c_void_p, P(c_int)],
+    "lf2_slab_count": [c_void_p, c_int, c_int, c_void_p],
+    "lf2_slab_extract": [c_void_p, c_int, c_int, c_i64, c_void_p, c_i64, c_void_p],
+    "lf2_slab_insert": [c_void_p, c_i64, c_void_p, c_i64, c_void_p],
     "lf2_checkpoint_save": [c_void_p, ctypes.c_char_p],
     "lf2_checkpoint_load": [c_void_p, ctypes.c_char_p],
     "lf2_kfield_create": [c_void_p, c_int, P(c_void_p)],

@@ -310,6 +310,43 @@ class Context:
                                                 _c.byref(n)), "extract_z")
         return out
 
+    def slab_record_words(self):
+        """32-bit words of one migration record of this store."""
+        w = _c.c_int()
+        self._check(_lib.load().lf2_slab_record_words(self.h, _c.byref(w)), "slab_record_words")
+        return w.value
+
+    def slab_count(self, z_lo, z_hi, out):
+        """out[:4] (CUDA int64 tensor) <- the particles below z_lo, above
+        z_hi and more than one plane outside [z_lo, z_hi], and max |v|^2
+        after the last kick as float bits; in stream order (no wait)."""
+        self._check(_lib.load().lf2_slab_count(self.h, int(z_lo), int(z_hi),
+                                               _c.c_void_p(out.data_ptr())), "slab_count")
+        return out
+
+    def slab_extract(self, z_lo, z_hi, n_below, n_above, words=0):
+        """The particles outside [z_lo, z_hi] leave the store as migration
+        records (CUDA int32 tensors of (n, record_words)): those below z_lo
+        and those above z_hi, with the cell index of the neighbouring slab.
+        n_below / n_above are slab_count's counts; words, when given, is
+        slab_record_words().  No wait."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        w = words if words else self.slab_record_words()
+        below = torch.empty((int(n_below), w), dtype=torch.int32, device=dev)
+        above = torch.empty((int(n_above), w), dtype=torch.int32, device=dev)
+        self._check(_lib.load().lf2_slab_extract(
+            self.h, int(z_lo), int(z_hi), int(n_below), _c.c_void_p(below.data_ptr()),
+            int(n_above), _c.c_void_p(above.data_ptr())), "slab_extract")
+        return below, above
+
+    def slab_insert(self, a, b):
+        """Migration records a and b (CUDA int32 tensors of (n, record_words))
+        join the store; no wait unless the store must grow."""
+        self._check(_lib.load().lf2_slab_insert(
+            self.h, int(a.shape[0]), _c.c_void_p(a.data_ptr()), int(b.shape[0]),
+            _c.c_void_p(b.data_ptr())), "slab_insert")
+
     def add_particles(self, cell, off, vel, mass=None, ids=None):
         """New particles (cell, offsets, velocities[, mass][, ids]) join the
         store (numpy arrays or CUDA tensors)."""

@@ -169,6 +169,19 @@ lf2_status ensure_spill(lf2_ctx* c, size_t need)
 bool valid_field(lf2_ctx* c, lf2_field f) { return c && f && f->data; }
 
 // Common load path: inputs already on the device.
+// Slots of the mover buffer for a store loaded with n particles: every
+// particle may change brick in one step, and later inserts may grow the store
+// to the largest size that fits_store still accepts (about 1.11 n).
+static int64_t mover_slots(int64_t n, int64_t nb) { return n + (n >> 3) + 64 * nb + 1024; }
+
+// Whether a store of `total` particles fits the current allocation without a
+// reload: the mover buffer holds every particle, and a repack lays each brick
+// out at cap_of(count) <= count + count/8 + 35 slots, so it always fits.
+static bool fits_store(const lf2_ctx* c, int64_t total)
+{
+  return total <= c->mov_capacity && total + (total >> 3) + 36 * c->g.nbricks <= c->capacity;
+}
+
 lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
                        const float* vel3, const float* mass, double gmass, const int64_t* id)
 {
@@ -177,7 +190,7 @@ lf2_status load_device(lf2_ctx* c, int64_t n, const int32_t* cell, const float* 
   // segments (count + slack, rounded to 4) plus a relocation region of about
   // the same size as the slack
   const int64_t need = n + (n >> 2) + 100 * nb + 1024;
-  const int64_t mov_need = n > 0 ? n : 1;  // every particle may change brick
+  const int64_t mov_need = mover_slots(n, nb);
   // the kernels index slots with 32-bit integers
   if (need > (int64_t)UINT32_MAX)
     return fail(c, LF2_ERR_UNSUPPORTED, "the particle store is limited to 2^32 - 1 slots (" +
@@ -303,6 +316,7 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
   ok = ok && cudaMalloc(&c->brick_sums, sizeof(double) * 7 * nb) == cudaSuccess;
   ok = ok && cudaMalloc(&c->stats, sizeof(double) * 8) == cudaSuccess;
   ok = ok && cudaMalloc(&c->mov_count, sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && cudaMalloc(&c->mig, sizeof(unsigned long long) * 4) == cudaSuccess;
   ok = ok && cudaMalloc(&c->flags, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->vmax_bits, sizeof(uint32_t)) == cudaSuccess;
   ok = ok && cudaMalloc(&c->redep, sizeof(uint32_t)) == cudaSuccess;
@@ -328,6 +342,7 @@ lf2_status lf2_create(lf2_ctx** out, int device, const int n[3], const double bo
          cudaMemsetAsync(c->ovf_state, 0, sizeof(int32_t) * nb, c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->heap_top, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
          cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream) == cudaSuccess &&
+         cudaMemsetAsync(c->brick_maxv2, 0, sizeof(float) * nb, c->stream) == cudaSuccess &&
          cudaStreamSynchronize(c->stream) == cudaSuccess;
   }
   if (!ok) {
@@ -358,6 +373,7 @@ lf2_status lf2_destroy(lf2_ctx* c)
   cudaFree(c->brick_sums);
   cudaFree(c->stats);
   cudaFree(c->mov_count);
+  cudaFree(c->mig);
   cudaFree(c->work);
   cudaFree(c->flags);
   cudaFree(c->vmax_bits);
@@ -478,23 +494,85 @@ lf2_status lf2_particles_extract_z(lf2_ctx* c, int z_lo, int z_hi, int64_t capac
     return fail(c, LF2_ERR_ARG, "extract_z: give mass and id exactly when the store carries them");
   *n_out = 0;
   if (c->np == 0) return LF2_OK;
-  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
-  LF2_CUDA(c, launch_count_outside(c, z_lo, z_hi, c->mov_count));
-  unsigned long long n = 0;
-  LF2_CUDA(c, cudaMemcpyAsync(c->h_i64, c->mov_count, sizeof(unsigned long long),
+  LF2_CUDA(c, launch_count_outside(c, z_lo, z_hi, c->mig));
+  LF2_CUDA(c, cudaMemcpyAsync(c->h_i64, c->mig, 2 * sizeof(unsigned long long),
                               cudaMemcpyDeviceToHost, c->stream));
   LF2_CUDA(c, cudaStreamSynchronize(c->stream));
-  memcpy(&n, c->h_i64, sizeof n);
-  *n_out = (int64_t)n;
-  if ((int64_t)n > capacity)
+  const int64_t n = c->h_i64[0] + c->h_i64[1];
+  *n_out = n;
+  if (n > capacity)
     return fail(c, LF2_ERR_ARG, "extract_z: " + std::to_string(n) + " particles, capacity " +
                                     std::to_string(capacity));
   if (n == 0) return LF2_OK;
-  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
-  LF2_CUDA(c, launch_extract_outside(c, z_lo, z_hi, cell, off3, vel3, mass, id, c->mov_count));
-  LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
-  c->np -= (int64_t)n;
+  LF2_CUDA(c, cudaMemsetAsync(c->mig, 0, sizeof(unsigned long long), c->stream));
+  LF2_CUDA(c, launch_extract_outside(c, z_lo, z_hi, cell, off3, vel3, mass, id, c->mig));
+  c->np -= n;
   return LF2_OK;
+}
+
+lf2_status lf2_slab_record_words(lf2_ctx* c, int* words)
+{
+  if (!c || !words) return LF2_ERR_ARG;
+  *words = record_words(c);
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_count(lf2_ctx* c, int z_lo, int z_hi, int64_t* counts)
+{
+  if (!c || !counts || z_lo > z_hi) return LF2_ERR_ARG;
+  if (c->np == 0) {
+    LF2_CUDA(c, cudaMemsetAsync(counts, 0, 4 * sizeof(int64_t), c->stream));
+    return LF2_OK;
+  }
+  LF2_CUDA(c, launch_count_outside(c, z_lo, z_hi, (unsigned long long*)counts, true));
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_extract(lf2_ctx* c, int z_lo, int z_hi, int64_t n_below, uint32_t* below,
+                            int64_t n_above, uint32_t* above)
+{
+  if (!c || z_lo > z_hi || n_below < 0 || n_above < 0 || (n_below > 0 && !below) ||
+      (n_above > 0 && !above))
+    return LF2_ERR_ARG;
+  if (n_below + n_above > c->np)
+    return fail(c, LF2_ERR_ARG, "slab_extract: more particles than the store holds");
+  if (c->np == 0) return LF2_OK;
+  // launched whatever the counts, so that a particle beyond them is reported
+  LF2_CUDA(c, launch_extract_records(c, z_lo, z_hi, n_below, below, n_above, above, c->mig));
+  c->np -= n_below + n_above;
+  return LF2_OK;
+}
+
+lf2_status lf2_slab_insert(lf2_ctx* c, int64_t n_a, const uint32_t* a, int64_t n_b,
+                           const uint32_t* b)
+{
+  if (!c || n_a < 0 || n_b < 0 || (n_a > 0 && !a) || (n_b > 0 && !b)) return LF2_ERR_ARG;
+  if (c->capacity == 0)
+    return fail(c, LF2_ERR_ARG, "slab_insert: create the store with lf2_particles_set first");
+  const int64_t n = n_a + n_b;
+  if (n == 0) return LF2_OK;
+  if (c->np + n >= (1ll << 31)) return fail(c, LF2_ERR_UNSUPPORTED, "more than 2^31-1 particles");
+  const int64_t total = c->np + n;
+  if (fits_store(c, total)) {
+    // through the mover path, in stream order
+    LF2_CUDA(c, launch_pack_records(c, n_a, a, n_b, b));
+    LF2_TRY(rebin_tail(c));
+    LF2_CUDA(c, cudaMemsetAsync(c->mov_count, 0, sizeof(unsigned long long), c->stream));
+    c->np = total;
+    return LF2_OK;
+  }
+  // the store is too small: separate arrays, then the reloading add (it waits)
+  Scratch sc(c), so(c), sv(c), sm(c), si(c);
+  LF2_CUDA(c, sc.alloc(sizeof(int32_t) * n));
+  LF2_CUDA(c, so.alloc(sizeof(float) * 3 * n));
+  LF2_CUDA(c, sv.alloc(sizeof(float) * 3 * n));
+  if (c->has_mass) LF2_CUDA(c, sm.alloc(sizeof(float) * n));
+  if (c->has_id) LF2_CUDA(c, si.alloc(sizeof(int64_t) * n));
+  LF2_CUDA(c, launch_unpack_records(c, n_a, a, n_b, b, (int32_t*)sc.p, (float*)so.p, (float*)sv.p,
+                                    (float*)sm.p, (int64_t*)si.p));
+  return lf2_particles_add(c, n, (const int32_t*)sc.p, (const float*)so.p, (const float*)sv.p,
+                           c->has_mass ? (const float*)sm.p : nullptr,
+                           c->has_id ? (const int64_t*)si.p : nullptr, LF2_PTR_DEVICE);
 }
 
 lf2_status lf2_particles_add(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
@@ -524,8 +602,7 @@ lf2_status lf2_particles_add(lf2_ctx* c, int64_t n, const int32_t* cell, const f
     return fail(c, LF2_ERR_ARG, "particles_add: a cell index or offset is out of range");
   }
   const int64_t total = c->np + n;
-  const int64_t need = total + (total >> 2) + 100 * c->g.nbricks + 1024;
-  if (n <= c->mov_capacity && need <= c->capacity) {
+  if (fits_store(c, total)) {
     // through the mover path: pack, insert
     LF2_CUDA(c, launch_pack_movers(c, n, dc, doff, dvel, dmass, did, true));
     LF2_TRY(rebin_tail(c));

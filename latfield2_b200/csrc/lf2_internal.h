@@ -81,6 +81,7 @@ struct lf2_ctx {
   int32_t* cap_alt = nullptr;        // [nbricks]
   int32_t* fill = nullptr;           // [nbricks] scratch
   unsigned long long* mov_count = nullptr;
+  unsigned long long* mig = nullptr;  // device [4]: slab migration counters
   uint32_t* flags = nullptr;         // device error bits
   int32_t* repack = nullptr;         // device: 1 when the whole store must be repacked
   unsigned long long* diag = nullptr; // device [3]: repacks, movers of the last drift, relocations
@@ -181,15 +182,25 @@ cudaError_t launch_vmax(lf2_ctx* c);
 DepositParams deposit_params(const lf2_ctx* c);
 
 // lf2_exchange.cu (slab decomposition): particles with cell z outside
-// [zlo, zhi] counted / moved out of the store; new particles into the mover
-// buffer for k_insert
-cudaError_t launch_count_outside(lf2_ctx* c, int zlo, int zhi, unsigned long long* n);
+// [zlo, zhi] counted (below, above, more than one plane outside: 3 counters)
+// / moved out of the store; new particles into the mover buffer for k_insert
+cudaError_t launch_count_outside(lf2_ctx* c, int zlo, int zhi, unsigned long long* n,
+                                 bool max_v = false);
 cudaError_t launch_extract_outside(lf2_ctx* c, int zlo, int zhi, int32_t* cell, float* off3,
                                    float* vel3, float* mass, int64_t* id,
                                    unsigned long long* out_count);
 cudaError_t launch_pack_movers(lf2_ctx* c, int64_t n, const int32_t* cell, const float* off3,
                                const float* vel3, const float* mass, const int64_t* id,
                                bool write);
+// migration records (lf2_slab_*): 32-bit words per particle
+inline int record_words(const lf2_ctx* c) { return 7 + (c->has_mass ? 1 : 0) + (c->has_id ? 2 : 0); }
+cudaError_t launch_extract_records(lf2_ctx* c, int zlo, int zhi, int64_t n_below, uint32_t* below,
+                                   int64_t n_above, uint32_t* above, unsigned long long* ctr);
+cudaError_t launch_pack_records(lf2_ctx* c, int64_t na, const uint32_t* a, int64_t nb,
+                                const uint32_t* b);
+cudaError_t launch_unpack_records(lf2_ctx* c, int64_t na, const uint32_t* a, int64_t nb,
+                                  const uint32_t* b, int32_t* cell, float* off3, float* vel3,
+                                  float* mass, int64_t* id);
 
 // lf2_fft.cu: releases the cuFFT plans and scratch of the context
 void fft_release(lf2_ctx* c);

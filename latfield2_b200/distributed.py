@@ -78,6 +78,7 @@ class CudaEngine:
 
     def set_particles(self, cell, off, vel, mass, gmass, ids):
         self.has_mass, self.has_id = mass is not None, ids is not None
+        self._words = None
         self.ctx.set_particles(cell, off, vel, mass=mass, global_mass=gmass, ids=ids)
 
     def new_field(self, comps):
@@ -86,8 +87,9 @@ class CudaEngine:
         return t, self.ctx.field(comps, t)
 
     def kick_drift(self, F, dtk, dtd):
+        """Kick, drift and rebin (max |v| stays on the device, for the
+        migration's speed check)."""
         self.ctx.step(F[1], dtk, dtd, None)
-        return self.ctx.last_max_velocity()
 
     def deposit(self, rho):
         self.ctx.deposit_scalar(rho[1])
@@ -97,6 +99,23 @@ class CudaEngine:
 
     def extract_outside(self, zlo, zhi):
         return self.ctx.extract_z(zlo, zhi, mass=self.has_mass, ids=self.has_id)
+
+    # migration in stream order (SlabDomain.migrate)
+    def migration_counts(self, zlo, zhi):
+        """CUDA int64 tensor of 6: counts below, above and beyond one plane,
+        max |v|^2 after the last kick as float bits, and two words for the
+        caller (the neighbours' counts)."""
+        if getattr(self, "_counts", None) is None:
+            self._counts = self.torch.zeros(6, dtype=self.torch.int64, device=self.dev)
+        return self.ctx.slab_count(zlo, zhi, self._counts)
+
+    def extract_records(self, zlo, zhi, n_below, n_above):
+        if getattr(self, "_words", None) is None:
+            self._words = self.ctx.slab_record_words()
+        return self.ctx.slab_extract(zlo, zhi, n_below, n_above, self._words)
+
+    def insert_records(self, a, b):
+        self.ctx.slab_insert(a, b)
 
     # the PM operator's pieces (SlabDomain.pm_force)
     def fft_prepare(self, n, nz, nky):
@@ -244,14 +263,19 @@ class SlabDomain:
         """f's own planes as numpy (comps, nz, n1, n0)."""
         return f[0][:, 1:self.nz + 1].cpu().numpy()
 
+    def _from_neighbour(self, a, plane, dst, src):
+        """Plane `plane` of a (comps, planes, n1, n0) goes to rank dst; the
+        same plane of rank src is returned (the plane itself on one rank)."""
+        if self.size == 1:
+            return a[:, plane]
+        buf = self._plane_buf(a)
+        self._shift(a[:, plane], dst, buf, src)
+        return buf
+
     def fill_ghosts(self, f):
         a = f[0]
-        buf = self._plane_buf(a)
-        self._shift(a[:, 1], self.down, buf, self.up)           # plane nz+1 <- above's plane 1
-        a[:, self.nz + 1] = buf
-        buf = self._plane_buf(a)
-        self._shift(a[:, self.nz], self.up, buf, self.down)      # plane 0 <- below's plane nz
-        a[:, 0] = buf
+        a[:, self.nz + 1] = self._from_neighbour(a, 1, self.down, self.up)  # above's plane 1
+        a[:, 0] = self._from_neighbour(a, self.nz, self.up, self.down)      # below's plane nz
 
     def deposit(self, rho, exact=False):
         """Scalar CIC deposit of the own particles with the upper-plane fold;
@@ -278,9 +302,7 @@ class SlabDomain:
             self.engine.extract_outside(1, self.nz)  # the copies leave again
         else:
             self.engine.deposit(rho)
-            buf = self._plane_buf(a)
-            self._shift(a[:, self.nz + 1], self.up, buf, self.down)
-            a[:, 1] += buf
+            a[:, 1] += self._from_neighbour(a, self.nz + 1, self.up, self.down)
         a[:, 0] = 0
         a[:, self.nz + 1] = 0
 
@@ -300,13 +322,9 @@ class SlabDomain:
         if int(a.shape[0]) != comps:
             raise ValueError(f"{kind} needs a field of {comps} components, got {int(a.shape[0])}")
         self.engine.project(kind, f)
-        buf = self._plane_buf(a)
-        self._shift(a[:, self.nz + 1], self.up, buf, self.down)   # -> plane 1 of the rank above
-        a[:, 1] += buf
+        a[:, 1] += self._from_neighbour(a, self.nz + 1, self.up, self.down)  # rank above's
         if lower:
-            buf = self._plane_buf(a)
-            self._shift(a[:, 0], self.down, buf, self.up)         # -> plane nz of the rank below
-            a[:, self.nz] += buf
+            a[:, self.nz] += self._from_neighbour(a, 0, self.down, self.up)  # rank below's
         a[:, 0] = 0
         a[:, self.nz + 1] = 0
 
@@ -353,22 +371,53 @@ class SlabDomain:
         e.gradient(p, F)
         self.fill_ghosts(F)
 
-    def migrate(self):
-        out = self.engine.extract_outside(1, self.nz)
-        z = out["cell"] // self.plane
-        below = z == 0
-        above = z == self.nz + 1
-        lost = float(bool((~(below | above)).any()))
-        if self._all_reduce([lost], "max")[0] > 0:  # every rank raises, none waits
+    def _shift_records(self, send, dst, k_recv, src):
+        """Migration records (k, words) to rank dst while k_recv records come
+        from rank src, in one message each way; an empty set is neither sent
+        nor received (both ends know the counts)."""
+        t = self.engine.torch
+        recv = t.empty((int(k_recv), int(send.shape[1])), dtype=send.dtype, device=send.device)
+        ops = []
+        if int(send.shape[0]):
+            ops.append(self.dist.P2POp(self.dist.isend, send.contiguous(), dst, self.group))
+        if int(k_recv):
+            ops.append(self.dist.P2POp(self.dist.irecv, recv, src, self.group))
+        if ops:
+            for r in self.dist.batch_isend_irecv(ops):
+                r.wait()
+        return recv
+
+    def migrate(self, move_scale=0.0):
+        """Particles on a ghost plane go to the neighbour that owns it.  The
+        counts and checks stay on the device until one read per call (the
+        host's only wait): this rank's counts below and above, the counts
+        its neighbours will send (exchanged first), and two checks reduced
+        over the ranks, so that every rank raises together and none is left
+        waiting in the exchange: a particle more than one plane outside, and
+        (move_scale > 0: dtau / cell size of the last drift) max |v| after
+        the last kick times move_scale reaching 1.  The records then travel
+        in one message per direction, sized from the counts."""
+        buf = self.engine.migration_counts(1, self.nz)
+        # buf: below, above, beyond, max |v|^2 bits | from below, from above
+        if self.size > 1:
+            self.dist.all_reduce(buf[2:4], op=self.dist.ReduceOp.MAX, group=self.group)
+            self._shift(buf[1:2], self.up, buf[4:5], self.down)
+            self._shift(buf[0:1], self.down, buf[5:6], self.up)
+        host = buf.tolist()
+        vmax = float(np.sqrt(np.array([host[3]], np.uint32).view(np.float32)[0]))
+        if move_scale > 0 and vmax * move_scale >= 1.0:
+            raise RuntimeError(f"max |v| dtau = {vmax * move_scale:.3f} cells: the slab "
+                               "decomposition moves particles by less than one cell per step")
+        if host[2]:
             raise RuntimeError("a particle left the slab by more than one plane")
-        to_down = {k: v[below] for k, v in out.items()}
-        to_up = {k: v[above] for k, v in out.items()}
-        to_down["cell"] = to_down["cell"] + self.nz * self.plane
-        to_up["cell"] = to_up["cell"] - self.nz * self.plane
-        from_below = self._shift_parts(to_up, self.up, self.down)
-        from_above = self._shift_parts(to_down, self.down, self.up)
-        for p in (from_below, from_above):
-            self.engine.add(p)
+        n_below, n_above = host[0], host[1]
+        below, above = self.engine.extract_records(1, self.nz, n_below, n_above)
+        if self.size == 1:
+            from_below, from_above = above, below
+        else:
+            from_below = self._shift_records(above, self.up, host[4], self.down)
+            from_above = self._shift_records(below, self.down, host[5], self.up)
+        self.engine.insert_records(from_below, from_above)
 
     def _all_reduce(self, values, op):
         """FP64 values reduced over the ranks (op "sum" or "max"); every rank
@@ -390,16 +439,13 @@ class SlabDomain:
         return float(s[0]), s[1:4], float(self._all_reduce([vmax], "max")[0])
 
     def step(self, F, dtau_kick, dtau_drift, rho=None):
-        """fill_ghosts(F), kick + drift + rebin, migrate, and (rho given) deposit.
-        The speed check uses max |v| over all ranks, so that all ranks raise
-        together rather than leaving the others waiting in the migration."""
+        """fill_ghosts(F), kick + drift + rebin, migrate, and (rho given)
+        deposit.  The speed check (max |v| dtau below one cell, max |v| over
+        all ranks) travels with the migration's counts, so the host waits
+        once per step."""
         self.fill_ghosts(F)
-        vmax = self.engine.kick_drift(F, dtau_kick, dtau_drift)
-        vmax = float(self._all_reduce([vmax], "max")[0])
-        if vmax * dtau_drift / self.res >= 1.0:
-            raise RuntimeError(f"max |v| dtau = {vmax * dtau_drift / self.res:.3f} cells: the "
-                               "slab decomposition moves particles by less than one cell per step")
-        self.migrate()
+        self.engine.kick_drift(F, dtau_kick, dtau_drift)
+        self.migrate(abs(float(dtau_drift)) / self.res)
         if rho is not None:
             self.deposit(rho)
 

@@ -27,6 +27,7 @@ class OracleEngine:
         self.off = np.zeros((0, 3), np.float32)
         self.vel = np.zeros((0, 3), np.float32)
         self.ids = None
+        self.vmax = 0.0
 
     def set_particles(self, cell, off, vel, mass, gmass, ids):
         if mass is not None:
@@ -47,7 +48,7 @@ class OracleEngine:
             raise RuntimeError("non-finite particle state")
         self.cell, self.off, self.vel = c, o, v
         v64 = v.astype(np.float64)
-        return float(np.sqrt((v64 * v64).sum(axis=1).max())) if v.shape[0] else 0.0
+        self.vmax = float(np.sqrt((v64 * v64).sum(axis=1).max())) if v.shape[0] else 0.0
 
     def deposit(self, rho):
         acc = self.O.state_deposit_fixed(self.n, self.cell, self.off)
@@ -111,6 +112,45 @@ class OracleEngine:
             self.ids = self.ids[~out]
         self.cell, self.off, self.vel = self.cell[~out], self.off[~out], self.vel[~out]
         return parts
+
+    # migration records: int32 words (cell, offset and velocity bits, id
+    # low and high words), the library's record layout
+    def migration_counts(self, zlo, zhi):
+        z = self.cell // (self.n[0] * self.n[1])
+        far = (z < zlo - 1) | (z > zhi + 1)
+        v2 = int(np.array([self.vmax * self.vmax], np.float32).view(np.uint32)[0])
+        return self.torch.tensor([int((z < zlo).sum()), int((z > zhi).sum()), int(far.sum()),
+                                  v2, 0, 0], dtype=self.torch.int64)
+
+    def extract_records(self, zlo, zhi, n_below, n_above):
+        plane = self.n[0] * self.n[1]
+        z = self.cell // plane
+        lo, hi = z < zlo, z > zhi
+        if int(lo.sum()) != n_below or int(hi.sum()) != n_above:
+            raise RuntimeError("extract_records: counts differ from migration_counts")
+        nz = zhi - zlo + 1
+
+        def records(sel, dz):
+            cols = [(self.cell[sel] + dz * plane).astype(np.int32)[:, None],
+                    self.off[sel].view(np.int32), self.vel[sel].view(np.int32)]
+            if self.ids is not None:
+                cols.append(self.ids[sel].view(np.int32).reshape(-1, 2))
+            return self.torch.from_numpy(np.ascontiguousarray(np.concatenate(cols, axis=1)))
+
+        below, above = records(lo, nz), records(hi, -nz)
+        keep = ~(lo | hi)
+        self.cell, self.off, self.vel = self.cell[keep], self.off[keep], self.vel[keep]
+        if self.ids is not None:
+            self.ids = self.ids[keep]
+        return below, above
+
+    def insert_records(self, a, b):
+        r = np.concatenate([a.numpy(), b.numpy()])
+        self.cell = np.concatenate([self.cell, r[:, 0]])
+        self.off = np.concatenate([self.off, np.ascontiguousarray(r[:, 1:4]).view(np.float32)])
+        self.vel = np.concatenate([self.vel, np.ascontiguousarray(r[:, 4:7]).view(np.float32)])
+        if self.ids is not None:
+            self.ids = np.concatenate([self.ids, np.ascontiguousarray(r[:, 7:9]).view(np.int64)[:, 0]])
 
     def add(self, parts):
         self.cell = np.concatenate([self.cell, parts["cell"].numpy()])

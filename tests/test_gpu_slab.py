@@ -1,5 +1,6 @@
 """GPU side of the slab decomposition: lf2_particles_extract_z and
-lf2_particles_add through the C ABI, and latfield2_b200.distributed.SlabDomain
+lf2_particles_add, the migration records of lf2_slab_count / lf2_slab_extract
+/ lf2_slab_insert through the C ABI, and latfield2_b200.distributed.SlabDomain
 on the CUDA engine with one rank (its neighbours are itself), against the
 plain single-GPU path on the same particles.
 
@@ -234,3 +235,117 @@ def test_one_rank_exact_slab_deposit_is_the_single_gpu_deposit():
     d.deposit(rho, exact=True)
     np.testing.assert_array_equal(d.own_planes(rho)[0], want.export_internal()[0])
     assert d.count() == cell.shape[0]
+
+
+def _records(rec, has_mass, has_id):
+    """Migration records (int32 words) as separate numpy arrays."""
+    r = np.ascontiguousarray(rec.cpu().numpy())
+    out = {"cell": r[:, 0].copy(), "off": np.ascontiguousarray(r[:, 1:4]).view(np.float32),
+           "vel": np.ascontiguousarray(r[:, 4:7]).view(np.float32)}
+    w = 7
+    if has_mass:
+        out["mass"] = np.ascontiguousarray(r[:, w]).view(np.float32)
+        w += 1
+    if has_id:
+        out["id"] = np.ascontiguousarray(r[:, w:w + 2]).view(np.int64)[:, 0]
+    return out
+
+
+@pytest.mark.parametrize("masses", [False, True])
+def test_migration_records_count_extract_insert(masses):
+    """lf2_slab_count / lf2_slab_extract / lf2_slab_insert (the migration
+    without host waits): the counts, the records (bit-exact state, cell index
+    moved by -+nz planes into the neighbour's lattice), the store without
+    them, and the store with the records inserted."""
+    import torch
+    n = (32, 24, 40)
+    plane = n[0] * n[1]
+    cell, off, vel = small_case(n, 50000, seed=5)
+    ids = np.arange(cell.shape[0], dtype=np.int64)
+    mass = (np.random.default_rng(3).uniform(0.5, 2.0, cell.shape[0]).astype(np.float32)
+            if masses else None)
+    ctx = _ctx(n)
+    ctx.set_particles(cell, off, vel, mass=mass, global_mass=0.0 if masses else 1e-5, ids=ids)
+    assert ctx.slab_record_words() == 7 + masses + 2
+    z = cell // plane
+    zlo, zhi = 7, 29
+    nz = zhi - zlo + 1
+    lo, hi = z < zlo, z > zhi
+    counts = ctx.slab_count(zlo, zhi, torch.zeros(4, dtype=torch.int64, device="cuda"))
+    want = [lo.sum(), hi.sum(), ((z < zlo - 1) | (z > zhi + 1)).sum()]
+    assert counts.cpu().tolist() == [int(v) for v in want] + [0]  # no kick yet
+    # max |v|^2 of a kick (of nothing, no drift) as float bits
+    F0 = ctx.field(3, torch.zeros((3, n[2], n[1], n[0]), dtype=torch.float32, device="cuda"))
+    ctx.step(F0, 0.0, 0.0)
+    c4 = ctx.slab_count(zlo, zhi, torch.zeros(4, dtype=torch.int64, device="cuda")).cpu().tolist()
+    assert c4[:3] == [int(v) for v in want]
+    v2 = np.array([c4[3]], np.uint32).view(np.float32)[0]
+    assert np.sqrt(np.float64(v2)) == ctx.last_max_velocity()
+    below, above = ctx.slab_extract(zlo, zhi, int(want[0]), int(want[1]))
+    rb, ra = _records(below, masses, True), _records(above, masses, True)
+    for r, sel, dz in ((rb, lo, nz), (ra, hi, -nz)):
+        o = np.argsort(r["id"])
+        r = {k: v[o] for k, v in r.items()}
+        np.testing.assert_array_equal(r["id"], ids[sel])
+        np.testing.assert_array_equal(r["cell"], cell[sel] + dz * plane)
+        np.testing.assert_array_equal(r["off"], off[sel])
+        np.testing.assert_array_equal(r["vel"], vel[sel])
+        if masses:
+            np.testing.assert_array_equal(r["mass"], mass[sel])
+    inside = ~(lo | hi)
+    rest = _by_id(ctx.get_particles(mass=masses, ids=True))
+    np.testing.assert_array_equal(rest["id"], ids[inside])
+    np.testing.assert_array_equal(rest["cell"], cell[inside])
+    assert ctx.count() == int(inside.sum())
+    # the records back in, at their moved cells: the store holds every particle
+    ctx.slab_insert(above, below)
+    got = _by_id(ctx.get_particles(mass=masses, ids=True))
+    moved = cell + np.where(lo, nz, np.where(hi, -nz, 0)) * plane
+    np.testing.assert_array_equal(got["id"], ids)
+    np.testing.assert_array_equal(got["cell"], moved)
+    np.testing.assert_array_equal(got["off"], off)
+    np.testing.assert_array_equal(got["vel"], vel)
+    if masses:
+        np.testing.assert_array_equal(got["mass"], mass)
+    np.testing.assert_array_equal(ctx.cell_counts(), np.bincount(moved, minlength=np.prod(n)))
+    assert ctx.count() == cell.shape[0]
+    ctx.synchronize()
+
+
+def test_migration_records_reload_bad_record_and_short_counts():
+    """Insert beyond the store's room goes through the reloading add; a
+    record out of range raises LF2_FLAG_BAD_CELL; counts short of
+    slab_count's raise LF2_FLAG_CAPACITY (nothing is written past them)."""
+    import torch
+    import latfield2_b200 as L
+    n = (32, 32, 32)
+    cell, off, vel = small_case(n, 1000, seed=6)
+    ids = np.arange(1000, dtype=np.int64)
+    ctx = _ctx(n)
+    ctx.set_particles(cell, off, vel, global_mass=1e-3, ids=ids)
+    c2, o2, v2 = small_case(n, 200000, seed=7, clustered=True)
+    ids2 = np.arange(1000, 201000, dtype=np.int64)
+    rec = np.concatenate([c2[:, None], o2.view(np.int32), v2.view(np.int32),
+                          ids2.view(np.int32).reshape(-1, 2)], axis=1)
+    rec = torch.from_numpy(np.ascontiguousarray(rec)).cuda()
+    ctx.slab_insert(rec[:150000], rec[150000:])
+    got = _by_id(ctx.get_particles(ids=True))
+    np.testing.assert_array_equal(got["id"], np.arange(201000))
+    np.testing.assert_array_equal(got["cell"], np.concatenate([cell, c2]))
+    np.testing.assert_array_equal(got["vel"], np.concatenate([vel, v2]))
+    ctx.synchronize()
+    # a record out of range is dropped and reported
+    bad = rec[:4].clone()
+    bad[1, 0] = n[0] * n[1] * n[2]
+    ctx.slab_insert(bad, bad[:0])
+    with pytest.raises(L.LF2Error):
+        ctx.synchronize()
+    # short counts: the particles beyond them are reported
+    ctx3 = _ctx(n)
+    ctx3.set_particles(cell, off, vel, global_mass=1e-3, ids=ids)
+    z = cell // (n[0] * n[1])
+    nb = int((z < 4).sum())
+    assert nb > 2
+    ctx3.slab_extract(4, 31, nb - 2, 0)
+    with pytest.raises(L.LF2Error):
+        ctx3.synchronize()
