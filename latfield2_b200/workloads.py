@@ -86,7 +86,10 @@ def gaussian_field(n, seed, device="cpu", slope=-2.0):
 def lognormal(n, npart, seed, device="cpu", sigma_ln=2.0):
     delta = gaussian_field(n, seed, device)
     rho = torch.exp(sigma_ln * delta.to(torch.float64) - 0.5 * sigma_ln * sigma_ln).reshape(-1)
-    cdf = torch.cumsum(rho, 0)
+    # integer weights (2^-20 units of the mean density): their prefix sum is
+    # exact in any order, so the particles are the same bits in every run
+    # (a floating-point scan on the GPU rounds in a timing-dependent order)
+    cdf = torch.cumsum(torch.floor(rho * 1048576.0).to(torch.int64), 0).to(torch.float64)
     cdf = cdf / cdf[-1]
     g = _gen(seed + 1, device)
     u = torch.rand(npart, generator=g, device=device, dtype=torch.float64)

@@ -164,3 +164,18 @@ def test_c3_fixed_point_density_is_bit_exact_across_runs(cuda):
         torch.cuda.empty_cache()
     assert digests[0] == digests[1] == digests[2], digests
     assert digests[0][0] != digests[0][1]  # the steps changed the density
+
+
+def test_lognormal_workload_is_the_same_in_every_run(cuda):
+    """The log-normal particles come from an integer prefix sum, so that
+    runs (and processes) draw the same bits."""
+    import torch
+    import latfield2_b200.workloads as W
+    n = (128, 128, 128)
+    a = W.lognormal(n, 128 ** 3, seed=3, device="cuda")
+    b = W.lognormal(n, 128 ** 3, seed=3, device="cuda")
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    ca, _ = W.lognormal(n, 20000, seed=3, device="cpu")
+    cb, _ = W.lognormal(n, 20000, seed=3, device="cpu")
+    assert torch.equal(ca, cb)
