@@ -691,10 +691,12 @@ def slab_one_rank_ms(case, F, n, npart, dtau, warmup, steps, local):
         d.step(Ff, dtau, dtau, rho)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("slab_one_rank")  # the range a profiler can select
     e0.record()
     for _ in range(steps):
         d.step(Ff, dtau, dtau, rho)
     e1.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     d.engine.synchronize()
     return e0.elapsed_time(e1) / steps
@@ -966,7 +968,7 @@ def main():
 
     slab = None
     if args.slab and fp32_case is not None:
-        sms = slab_one_rank_ms(fp32_case, F, n, npart, dtau, args.warmup, min(args.steps, 5), local)
+        sms = slab_one_rank_ms(fp32_case, F, n, npart, dtau, args.warmup, min(args.steps, 10), local)
         slab = {"ms_per_step": sms, "vs_lf2_step": sms / ms_step, "ranks": 1,
                 "note": "one self-exchanging rank; the exchange calls run, no peer"}
         torch.cuda.empty_cache()
