@@ -366,7 +366,8 @@ __global__ void k_repack_clear(int32_t* repack, uint32_t* flags, unsigned long l
 // full repack.  Only when the region is exhausted does the whole store get
 // repacked (k_repack_*).
 
-__global__ void k_reloc(StoreView v, int64_t* seg_start, int32_t* cap, const int32_t* __restrict__ list,
+__global__ void __launch_bounds__(1024)
+    k_reloc(StoreView v, int64_t* seg_start, int32_t* cap, const int32_t* __restrict__ list,
                         const int32_t* __restrict__ nlist, int32_t* state, int32_t* fill,
                         unsigned long long* heap_top, int64_t capacity, int32_t* repack,
                         unsigned long long* diag)
@@ -523,7 +524,7 @@ cudaError_t launch_repack(lf2_ctx* c)
 {
   c->launches += 9;
   const int64_t nb = c->g.nbricks;
-  k_reloc<<<148, 256, 0, c->stream>>>(view(c), c->seg_start, c->cap, c->ovf_list, c->ovf_count,
+  k_reloc<<<148, 1024, 0, c->stream>>>(view(c), c->seg_start, c->cap, c->ovf_list, c->ovf_count,
                                       c->ovf_state, c->fill, c->heap_top, c->capacity, c->repack,
                                       c->diag);
   k_reloc_movers<<<148 * 2, 256, 0, c->stream>>>(c->g, c->mov, c->mov_placed, c->mov_count, c->cur,
