@@ -44,6 +44,11 @@
 #include "lf2_deposit_common.cuh"
 #include "lf2_internal.h"
 
+// Owned face vertices per thread and trip of the one-component fix-up.
+#ifndef FIX_V
+#define FIX_V 2
+#endif
+
 namespace lf2 {
 
 namespace {
@@ -443,24 +448,28 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
     }
   };
   if constexpr (C == 1) {
-    // One component: two vertices per thread, all their shell reads issued
+    // One component: FIX_V vertices per thread, all their shell reads issued
     // before any is used (the pass is bound by the latency of these
-    // scattered reads).  Subset s of a vertex's zero coordinates is read
+    // scattered reads; at 512^3, 2 per thread: 0.261 ms, 3: 0.287 ms, 4:
+    // 0.345 ms).  Subset s of a vertex's zero coordinates is read
     // when (s & zmask) == s; the sum runs over s in ascending order.
+    constexpr int FV = FIX_V;
     const float* spf = reinterpret_cast<const float*>(spill);
-    for (int f0 = threadIdx.x; f0 < nface; f0 += 2 * blockDim.x) {
-      int vi[2], vj[2], vk[2], zm[2];
-      bool on[2];
+    for (int f0 = threadIdx.x; f0 < nface; f0 += FV * blockDim.x) {
+      int vi[FV], vj[FV], vk[FV], zm[FV];
+      bool on[FV];
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < FV; h++) {
         const int f = f0 + h * blockDim.x;
         on[h] = f < nface;
         vi[h] = vj[h] = vk[h] = 0;
         if (on[h]) face_vertex(f, vi[h], vj[h], vk[h]);
         zm[h] = on[h] ? (vi[h] == 0 ? 1 : 0) | (vj[h] == 0 ? 2 : 0) | (vk[h] == 0 ? 4 : 0) : 0;
       }
-      long long qa = 0, qb = 0;
-      float fa = 0.0f, ca = 0.0f, fb = 0.0f, cb = 0.0f;
+      long long q[FV];
+      float fs[FV], fc[FV];
+#pragma unroll
+      for (int h = 0; h < FV; h++) q[h] = 0, fs[h] = 0.0f, fc[h] = 0.0f;
       auto read = [&](int h, int s) -> uint64_t {
         const int si = shell_index((s & 1) ? BRICK : vi[h], (s & 2) ? BRICK : vj[h], (s & 4) ? BRICK : vk[h]);
         // a brick's shell region is SHELL 8-byte slots; the plain mode
@@ -468,33 +477,31 @@ __global__ void k_fixup(Geom g, const uint64_t* __restrict__ spill, float fixed_
         const size_t at = (size_t)nbr[s] * SHELL;
         return ACC == ACC_PLAIN ? (uint64_t)__float_as_uint(spf[2 * at + si]) : spill[at + si];
       };
-      auto add = [&](long long& q, float& fs, float& fc, uint64_t raw) {
-        if (ACC == ACC_FIXED)
-          q += (long long)raw;
-        else if (ACC == ACC_COMP)
-          comp_acc(fs, fc, __uint_as_float((uint32_t)raw), __uint_as_float((uint32_t)(raw >> 32)));
-        else
-          fs = __fadd_rn(fs, __uint_as_float((uint32_t)raw));
-      };
 #pragma unroll
       for (int s = 0; s < 8; s++) {
-        const bool ua = on[0] && (s & zm[0]) == s, ub = on[1] && (s & zm[1]) == s;
-        const uint64_t ra = ua ? read(0, s) : 0ull;
-        const uint64_t rb = ub ? read(1, s) : 0ull;
-        if (ua) add(qa, fa, ca, ra);
-        if (ub) add(qb, fb, cb, rb);
+        uint64_t r[FV];
+#pragma unroll
+        for (int h = 0; h < FV; h++) r[h] = on[h] && (s & zm[h]) == s ? read(h, s) : 0ull;
+#pragma unroll
+        for (int h = 0; h < FV; h++) {
+          if (!(on[h] && (s & zm[h]) == s)) continue;
+          if (ACC == ACC_FIXED)
+            q[h] += (long long)r[h];
+          else if (ACC == ACC_COMP)
+            comp_acc(fs[h], fc[h], __uint_as_float((uint32_t)r[h]), __uint_as_float((uint32_t)(r[h] >> 32)));
+          else
+            fs[h] = __fadd_rn(fs[h], __uint_as_float((uint32_t)r[h]));
+        }
       }
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < FV; h++) {
         if (!on[h]) continue;
         const int64_t site = site_index(g, x0 + vi[h], y0 + vj[h], z0 + vk[h]);
-        const long long q = h ? qb : qa;
         if (ACC == ACC_FIXED) {
-          if (!SIGNED && q < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
-          out[site] = __fmul_rn(__ll2float_rn(q), conv);
+          if (!SIGNED && q[h] < 0) set_flag(flags, ERR_FIXED_OVERFLOW);
+          out[site] = __fmul_rn(__ll2float_rn(q[h]), conv);
         } else {
-          const float fs = h ? fb : fa, fc = h ? cb : ca;
-          out[site] = ACC == ACC_COMP ? __fadd_rn(fs, fc) : fs;
+          out[site] = ACC == ACC_COMP ? __fadd_rn(fs[h], fc[h]) : fs[h];
         }
       }
     }
