@@ -313,85 +313,64 @@ __global__ void __launch_bounds__(MOVE_THREADS) k_move(StoreView v, const float*
   }
 }
 
-// Movers into the free slots of their new brick, one slot atomic per mover
-// (grouping the lanes of one brick with a warp match first was no faster).
-// A lane takes INS_ITEMS movers per trip and issues every load they need
-// (the mover's arrays, its brick's segment start and capacity) before the
-// slot atomics, so that a trip waits for about two memory round trips, not
-// four.
-constexpr int INS_ITEMS = 2;
-
+// Movers into the free slots of their new brick.
 __global__ void k_insert(StoreView v, PartArrays mov, const unsigned long long* __restrict__ mov_count,
                          int32_t* placed, int32_t* ovf_list, int32_t* ovf_count, int32_t* ovf_state,
                          uint32_t* flags)
 {
+  // Whole warps step through the movers together, so that the lanes heading
+  // for the same brick (consecutive movers mostly come from one source brick
+  // and go to a few neighbours) take their slots with one atomic per brick.
   const int64_t nm = (int64_t)*mov_count;
   const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
   const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = warp0 * 32 * INS_ITEMS; base < nm; base += nwarps * 32 * INS_ITEMS) {
-    int64_t b[INS_ITEMS], seg[INS_ITEMS];
-    int cap[INS_ITEMS];
-    uint32_t key[INS_ITEMS];
-    float ox[INS_ITEMS], oy[INS_ITEMS], oz[INS_ITEMS], vx[INS_ITEMS], vy[INS_ITEMS], vz[INS_ITEMS];
-    float ms[INS_ITEMS];
-    int64_t id[INS_ITEMS];
-#pragma unroll
-    for (int j = 0; j < INS_ITEMS; j++) {
-      const int64_t m = base + j * 32 + lane;
-      b[j] = -1;
-      seg[j] = 0;
-      cap[j] = 0;
-      key[j] = 0;
-      ox[j] = oy[j] = oz[j] = vx[j] = vy[j] = vz[j] = ms[j] = 0.0f;
-      id[j] = 0;
-      if (m < nm) {
-        key[j] = mov.key[m];
-        // the mover's arrays, read before its slot is known (and before any
-        // store: the compiler cannot tell that the mover buffer and the store
-        // do not overlap)
-        ox[j] = mov.ox[m], oy[j] = mov.oy[m], oz[j] = mov.oz[m];
-        vx[j] = mov.vx[m], vy[j] = mov.vy[m], vz[j] = mov.vz[m];
-        if (v.a.mass) ms[j] = mov.mass[m];
-        if (v.a.id) id[j] = mov.id[m];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < INS_ITEMS; j++) {
-      const int64_t m = base + j * 32 + lane;
-      if (m >= nm) continue;
+  for (int64_t base = warp0 * 32; base < nm; base += nwarps * 32) {
+    const int64_t m = base + lane;
+    int64_t b = -1;
+    uint32_t key = 0;
+    if (m < nm) {
       int x, y, z;
-      unpack_key(v.g, key[j], x, y, z);
+      key = mov.key[m];
+      unpack_key(v.g, key, x, y, z);
       if (x >= v.g.n[0] || y >= v.g.n[1] || z >= v.g.n[2]) {  // only after a failed move
         set_flag(flags, ERR_BAD_CELL);
         placed[m] = 1;
       } else {
-        b[j] = brick_of(v.g, x, y, z);
-        seg[j] = v.seg_start[b[j]];
-        cap[j] = v.cap[b[j]];
+        b = brick_of(v.g, x, y, z);
       }
     }
-#pragma unroll
-    for (int j = 0; j < INS_ITEMS; j++) {
-      const int64_t m = base + j * 32 + lane;
-      if (b[j] < 0) continue;
-      const int slot = atomicAdd(&v.count[b[j]], 1);
-      if (slot < cap[j]) {
-        const int64_t q = seg[j] + slot;
-        v.a.key[q] = key[j];
-        v.a.ox[q] = ox[j];
-        v.a.oy[q] = oy[j];
-        v.a.oz[q] = oz[j];
-        v.a.vx[q] = vx[j];
-        v.a.vy[q] = vy[j];
-        v.a.vz[q] = vz[j];
-        if (v.a.mass) v.a.mass[q] = ms[j];
-        if (v.a.id) v.a.id[q] = id[j];
-        placed[m] = 1;
-      } else {
-        placed[m] = 0;  // the brick is full: it gets relocated (lf2_store.cu)
-        if (atomicExch(&ovf_state[b[j]], 1) == 0) ovf_list[atomicAdd(ovf_count, 1)] = (int32_t)b[j];
-      }
+    const unsigned grp = __match_any_sync(0xffffffffu, b);
+    int slot = 0;
+    if (b >= 0) {
+      const int leader = __ffs(grp) - 1;
+      int first = 0;
+      if (lane == leader) first = atomicAdd(&v.count[b], __popc(grp));
+      slot = __shfl_sync(grp, first, leader) + __popc(grp & lt);
+    }
+    if (b < 0) continue;
+    if (slot < v.cap[b]) {
+      const int64_t q = v.seg_start[b] + slot;
+      // every array read before any is written (the compiler cannot tell
+      // that the mover buffer and the store do not overlap)
+      const float ox = mov.ox[m], oy = mov.oy[m], oz = mov.oz[m];
+      const float vx = mov.vx[m], vy = mov.vy[m], vz = mov.vz[m];
+      const float ms = v.a.mass ? mov.mass[m] : 0.0f;
+      const int64_t id = v.a.id ? mov.id[m] : 0;
+      v.a.key[q] = key;
+      v.a.ox[q] = ox;
+      v.a.oy[q] = oy;
+      v.a.oz[q] = oz;
+      v.a.vx[q] = vx;
+      v.a.vy[q] = vy;
+      v.a.vz[q] = vz;
+      if (v.a.mass) v.a.mass[q] = ms;
+      if (v.a.id) v.a.id[q] = id;
+      placed[m] = 1;
+    } else {
+      placed[m] = 0;  // the brick is full: it gets relocated (lf2_store.cu)
+      if (atomicExch(&ovf_state[b], 1) == 0) ovf_list[atomicAdd(ovf_count, 1)] = (int32_t)b;
     }
   }
 }
