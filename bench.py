@@ -800,16 +800,41 @@ def slab_scaling(args, n, cell, off, vel, F, npart, dtau, local, pg, device):
         d.step(Ff, dtau, dtau, rho)
     torch.cuda.synchronize()
     pg.barrier()
+    l0 = d.engine.ctx.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         d.step(Ff, dtau, dtau, rho)
     e1.record()
     torch.cuda.synchronize()
+    launches = d.engine.ctx.kernel_launches() - l0
     pg.barrier()
     ms, value = replica_throughput(e0.elapsed_time(e1), npart, args.steps, pg, device)
     value /= pg.get_world_size()  # one set of particles for the whole job
-    return ms / args.steps, value, d.count()
+
+    # end to end: every step the rank's planes of F come from pinned host
+    # memory and its planes of rho go back to pinned host memory
+    own_F = Ff[0][:, 1:d.nz + 1]
+    F_pin = own_F.cpu().pin_memory()
+    rho_pin = torch.empty(tuple(rho[0][:, 1:d.nz + 1].shape), dtype=torch.float32).pin_memory()
+    k = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        own_F.copy_(F_pin, non_blocking=True)
+        d.step(Ff, dtau, dtau, rho)
+        rho_pin.copy_(rho[0][:, 1:d.nz + 1], non_blocking=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    ms_e2e, v_e2e = replica_throughput(1e3 * t, npart, k, pg, device)
+    e2e = {"value": v_e2e / pg.get_world_size(), "unit": UNIT,
+           "h2d_bytes_per_step": int(F_pin.numel()) * 4 * pg.get_world_size(),
+           "d2h_bytes_per_step": int(rho_pin.numel()) * 4 * pg.get_world_size(),
+           "ms_per_step": ms_e2e / k, "steps": k,
+           "path": "per step on every rank: its planes of F from pinned host memory, "
+                   "SlabDomain.step, its planes of rho to pinned host memory (one stream)"}
+    return ms / args.steps, value, d.count(), launches, e2e
 
 
 def replica_throughput(ms_local, npart, steps, pg=None, device="cpu"):
@@ -844,7 +869,8 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
         pg = dist
 
     def barrier():
@@ -861,8 +887,8 @@ def main():
         peak, peak_kind = peaks()
         dtau = 0.1 * 64.0 / n[0]
         with ClockSampler(local) as clocks:
-            ms_step, value, local_count = slab_scaling(args, n, cell, off, vel, F, npart, dtau, local,
-                                                       pg, device)
+            ms_step, value, local_count, launches, e2e = slab_scaling(args, n, cell, off, vel, F,
+                                                                      npart, dtau, local, pg, device)
         if rank == 0:
             step_ab = alg_bytes_step(npart, nsites)
             line = {
@@ -877,8 +903,8 @@ def main():
                              "achieved": step_ab / (ms_step / 1e3) / 1e9, "peak": peak * world,
                              "frac": step_ab / (ms_step / 1e3) / 1e9 / (peak * world),
                              "peak_source": peak_kind, "traffic": None},
-                "cpu_baseline": None, "e2e": None, "clocks": clocks.summary(),
-                "particles_rank0": local_count,
+                "cpu_baseline": None, "e2e": e2e, "clocks": clocks.summary(),
+                "gpu_launches": launches, "particles_rank0": local_count,
             }
             print(json.dumps(line), flush=True)
         pg.barrier()
