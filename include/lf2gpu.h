@@ -414,6 +414,49 @@ lf2_status lf2_pm_gradient(lf2_ctx* ctx, lf2_field phi, lf2_field F);
  *   pm_force4_adjoint g_rho (+=) from g_F4: the divergence
  *                    g_phi(y) = sum_c (g_F_c(y+e_c) - g_F_c(y-e_c)) / (2 res),
  *                    then the same Green's-function solve (self-adjoint) */
+/* The chain's particle state from box-unit FP64 positions, and its
+ * gradients back to the caller's order (all device pointers, no wait).  The
+ * permutations move one 32-byte record per particle (`records`: 32 bytes
+ * per particle, 16-byte aligned), a full sector each way:
+ *   pm_state_pack    caller order: the sort key of particle i (its brick
+ *                    times 4096 plus its cell's place in the brick, x
+ *                    fastest; LF2_ERR_UNSUPPORTED when nbricks * 4096 does
+ *                    not fit 31 bits) and its record: the cell of pos3[i]
+ *                    (u = pos * inv_res per dim, floor, the offset u -
+ *                    floor(u) rounded to FP32, an offset that rounds to 1
+ *                    carrying into the next cell, periodic wrap), offsets,
+ *                    velocity and mass rounded to FP32 (mass may be NULL: 0)
+ *   pm_state_unpack  slot i <- the record of particle order[i] (mass may be
+ *                    NULL: not written)
+ *   pm_brick_start   brick_start[b] (nbricks + 1 entries): the first slot of
+ *                    brick b among cells sorted by the pack's key
+ *   pm_grads_unorder g_pos3_out[order[i]] = g_off3[i] * inv_res,
+ *                    g_vel3_out[order[i]] = g_vel3[i], g_mass_out[order[i]] =
+ *                    g_mass[i], in FP64, through `records` as scratch
+ *   pm_deposit_bricks  pm_deposit of particles grouped by brick_start: one
+ *                    CTA per brick sums in a shared vertex tile and adds the
+ *                    tile to the field; a particle that has left its group's
+ *                    brick since is deposited on its own.  The same sums in
+ *                    the fixed-point mode; FP32 roundings in another order.
+ *                    brick_start must come from cells sorted by the key. */
+lf2_status lf2_pm_state_pack(lf2_ctx* ctx, int64_t np, const double* pos3,
+                             const double* vel3, const double* mass,
+                             double inv_res, int32_t* key, void* records);
+lf2_status lf2_pm_state_unpack(lf2_ctx* ctx, int64_t np, const int64_t* order,
+                               const void* records, int32_t* cell,
+                               float* off3, float* vel3, float* mass);
+lf2_status lf2_pm_brick_start(lf2_ctx* ctx, int64_t np, const int32_t* cell,
+                              int64_t* brick_start);
+lf2_status lf2_pm_grads_unorder(lf2_ctx* ctx, int64_t np,
+                                const int64_t* order, const float* g_off3,
+                                const float* g_vel3, const float* g_mass,
+                                double inv_res, void* records,
+                                double* g_pos3_out, double* g_vel3_out,
+                                double* g_mass_out);
+lf2_status lf2_pm_deposit_bricks(lf2_ctx* ctx, int64_t np, const int32_t* cell,
+                                 const float* off3, const float* mass,
+                                 double gmass, const int64_t* brick_start,
+                                 float* rho);
 lf2_status lf2_pm_deposit(lf2_ctx* ctx, int64_t np, const int32_t* cell,
                           const float* off3, const float* mass, double gmass,
                           float* rho);

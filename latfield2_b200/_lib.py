@@ -96,6 +96,15 @@ SIGNATURES = {
     "lf2_last_max_velocity": [c_void_p, c_void_p, c_int],
     "lf2_conservation": [c_void_p, P(c_double), P(c_double), P(c_double)],
     "lf2_velocity_reductions": [c_void_p, P(c_double), P(c_double), P(c_double)],
+    "lf2_pm_state_pack": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p,
+                          c_void_p],
+    "lf2_pm_state_unpack": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                            c_void_p],
+    "lf2_pm_brick_start": [c_void_p, c_i64, c_void_p, c_void_p],
+    "lf2_pm_grads_unorder": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                             c_void_p, c_void_p, c_void_p, c_void_p],
+    "lf2_pm_deposit_bricks": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p,
+                              c_void_p],
     "lf2_pm_deposit": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p],
     "lf2_pm_gather": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_pm_kick_drift": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,

@@ -1,7 +1,7 @@
 """Differentiable multi-step particle-mesh chain on the CUDA kernels.
 
-Per step k (particles ordered by their initial cell, no rebinning; the
-gradients come back in the caller's order):
+Per step k (particles ordered by their initial brick and cell, no
+rebinning; the gradients come back in the caller's order):
     rho_k   = deposit(x_k, m)                    lf2_pm_deposit      (CIC, projections.hpp:75-184)
     F_k     = stencil27(rho_k, S)                lf2_stencil27       (the grid operator), or
     F_k     = pm_force(rho_k)                    lf2_pm_force4       (the FFT Poisson force)
@@ -59,7 +59,58 @@ class _Ops:
         self.lib = _lib.load()
         self.ns = ctx.nsites
 
+    bricks = None  # brick_start of the sorted state: deposits run brick-tiled
+
+    def state_pack(self, pos, vel, mass, inv_res):
+        """Caller order: the sort keys (brick, then cell in the brick) and one
+        32-byte record per particle (cell, offsets, FP32 velocity and mass)."""
+        n = pos.shape[0]
+        key = torch.empty(n, dtype=torch.int32, device=pos.device)
+        rec = torch.empty(n * 8, dtype=torch.int32, device=pos.device)
+        _check(self.ctx, self.lib.lf2_pm_state_pack(self.ctx.h, n, _p(pos), _p(vel), _p(mass),
+                                                    inv_res, _p(key), _p(rec)), "pm_state_pack")
+        return key, rec
+
+    def state_unpack(self, order, rec):
+        """cell, offsets, FP32 velocities and masses of the particles `order`."""
+        n = order.numel()
+        dev = rec.device
+        cell = torch.empty(n, dtype=torch.int32, device=dev)
+        off = torch.empty(n, 3, dtype=torch.float32, device=dev)
+        vel32 = torch.empty(n, 3, dtype=torch.float32, device=dev)
+        m32 = torch.empty(n, dtype=torch.float32, device=dev)
+        _check(self.ctx, self.lib.lf2_pm_state_unpack(self.ctx.h, n, _p(order), _p(rec), _p(cell),
+                                                      _p(off), _p(vel32), _p(m32)),
+               "pm_state_unpack")
+        return cell, off, vel32, m32
+
+    def brick_start(self, cell):
+        """First slot of every brick among cells sorted by the pack's key."""
+        bs = torch.empty(self.ctx.nbricks + 1, dtype=torch.int64, device=cell.device)
+        _check(self.ctx, self.lib.lf2_pm_brick_start(self.ctx.h, cell.numel(), _p(cell), _p(bs)),
+               "pm_brick_start")
+        return bs
+
+    def grads_unorder(self, order, g_off, g_v, g_m, inv_res):
+        """FP64 gradients in the caller's order: positions (per box unit),
+        velocities, masses."""
+        n = order.numel()
+        dev = g_off.device
+        rec = torch.empty(n * 8, dtype=torch.int32, device=dev)
+        g_pos = torch.empty(n, 3, dtype=torch.float64, device=dev)
+        g_vel = torch.empty(n, 3, dtype=torch.float64, device=dev)
+        g_mass = torch.empty(n, dtype=torch.float64, device=dev)
+        _check(self.ctx, self.lib.lf2_pm_grads_unorder(self.ctx.h, n, _p(order), _p(g_off), _p(g_v),
+                                                       _p(g_m), inv_res, _p(rec), _p(g_pos),
+                                                       _p(g_vel), _p(g_mass)), "pm_grads_unorder")
+        return g_pos, g_vel, g_mass
+
     def deposit(self, cell, off, m, rho):
+        if self.bricks is not None:
+            _check(self.ctx, self.lib.lf2_pm_deposit_bricks(self.ctx.h, cell.numel(), _p(cell),
+                                                            _p(off), _p(m), 0.0, _p(self.bricks),
+                                                            _p(rho)), "pm_deposit_bricks")
+            return
         _check(self.ctx, self.lib.lf2_pm_deposit(self.ctx.h, cell.numel(), _p(cell), _p(off), _p(m),
                                                  0.0, _p(rho)), "pm_deposit")
 
@@ -118,16 +169,21 @@ class PMChain(torch.autograd.Function):
     @staticmethod
     def forward(fctx, pos0, vel0, mass, S, w, lf2ctx, steps, dt, checkpoint_every, coupling):
         ops = _Ops(lf2ctx)
-        n, res = lf2ctx.n, lf2ctx.res
-        cell, off = positions_to_state(pos0.detach().to(torch.float64), n, res)
-        # the chain runs on the particles ordered by cell (the deposits' and
-        # gathers' accesses are then local); the gradients go back to the
-        # caller's order at the end of the backward pass
-        order = torch.argsort(cell)
-        cell = cell[order].contiguous()
-        off = off[order].contiguous()
-        vel = vel0.detach().to(torch.float32)[order].contiguous()
-        m = mass.detach().to(torch.float32)[order].contiguous()
+        res = lf2ctx.res
+        # the chain runs on the particles ordered by brick and by cell inside
+        # it (the deposits sum each brick in a shared tile, and every access
+        # is local); the gradients go back to the caller's order at the end of
+        # the backward pass.  The permutations move one 32-byte record per
+        # particle.
+        key, rec = ops.state_pack(pos0.detach().to(torch.float64).contiguous(),
+                                  vel0.detach().to(torch.float64).contiguous(),
+                                  mass.detach().to(torch.float64).contiguous(), 1.0 / res)
+        order = torch.argsort(key)
+        del key
+        cell, off, vel, m = ops.state_unpack(order, rec)
+        del rec
+        # a particle that drifts out of its brick later is deposited on its own
+        ops.bricks = ops.brick_start(cell)
         S32 = None if S is None else S.detach().to(torch.float32).contiguous()
         w32 = w.detach().to(torch.float32).contiguous().reshape(-1)
         ckpts, rhos, Fs = {}, [], []
@@ -165,11 +221,16 @@ class PMChain(torch.autograd.Function):
         for k in range(steps - 1, -1, -1):
             k0 = (k // every) * every
             if k not in seg:
-                # replay the segment from its checkpoint, keeping each state
+                # replay the segment from its checkpoint (k is its last step:
+                # the segments are visited once, last first, so the
+                # checkpoint is consumed), keeping each state
                 seg = {}
-                c, o, v = (t.clone() for t in ckpts[k0])
-                for j in range(k0, min(k0 + every, steps)):
-                    seg[j] = (c.clone(), o.clone())
+                if k0 not in ckpts:
+                    raise RuntimeError("the chain's backward ran already: its checkpoints are "
+                                       "consumed (call backward once per forward)")
+                c, o, v = ckpts.pop(k0)
+                for j in range(k0, k + 1):
+                    seg[j] = (c.clone(), o.clone()) if j < k else (c, o)
                     if j < k:
                         ops.step(c, o, v, Fs[j], dt)
             cell_k, off_k = seg[k]
@@ -185,15 +246,11 @@ class PMChain(torch.autograd.Function):
             else:
                 ops.pm_force_adj(g_F, g_rho, coupling)
             ops.deposit_adj(cell_k, off_k, m, g_rho, g_off, g_m)
-        def caller_order(t, dtype):
-            out = torch.empty(t.shape, dtype=dtype, device=t.device)
-            out[order] = t.to(dtype)
-            return out
-
-        g_pos = caller_order(g_off.to(torch.float64) / res, fctx.pos_dtype)
+        g_pos, g_vel, g_mass = ops.grads_unorder(order, g_off, g_v, g_m, 1.0 / res)
+        del g_off, g_v, g_m
         g_w = (rhoK * g).to(torch.float64)
         g_S = None if S32 is None else g_S.to(torch.float64)
-        return (g_pos, caller_order(g_v, fctx.vel_dtype), caller_order(g_m, torch.float64), g_S, g_w,
+        return (g_pos.to(fctx.pos_dtype), g_vel.to(fctx.vel_dtype), g_mass, g_S, g_w,
                 None, None, None, None, None)
 
 

@@ -203,6 +203,9 @@ class Context:
         self.n = tuple(int(v) for v in n)
         self.box = tuple(float(b) for b in box)
         self.nsites = self.n[0] * self.n[1] * self.n[2]
+        self.nbricks = 1
+        for v in self.n:
+            self.nbricks *= -(-v // 16)  # bricks of 16^3 cells
         self.res = self.box[0] / self.n[0]
         self.mode = mode
         self.device = int(device)

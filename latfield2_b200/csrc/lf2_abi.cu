@@ -1138,6 +1138,59 @@ static lf2_status pm_call(lf2_ctx* c, int op, int64_t np, const int32_t* cell, c
   return LF2_OK;
 }
 
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+lf2_status lf2_pm_state_pack(lf2_ctx* c, int64_t np, const double* pos3, const double* vel3,
+                             const double* mass, double inv_res, int32_t* key, void* records)
+{
+  if (!c || np < 0 || !(inv_res > 0)) return LF2_ERR_ARG;
+  if (np > 0 && (!pos3 || !vel3 || !key || !records || !aligned16(records))) return LF2_ERR_ARG;
+  if (c->g.nbricks * 4096 > INT32_MAX)
+    return fail(c, LF2_ERR_UNSUPPORTED, "pm_state_pack: sort keys need nbricks * 4096 < 2^31");
+  LF2_CUDA(c, launch_pm_pack(c, np, pos3, vel3, mass, inv_res, key, records));
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_state_unpack(lf2_ctx* c, int64_t np, const int64_t* order, const void* records,
+                               int32_t* cell, float* off3, float* vel3, float* mass)
+{
+  if (!c || np < 0) return LF2_ERR_ARG;
+  if (np > 0 && (!order || !records || !aligned16(records) || !cell || !off3 || !vel3))
+    return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_pm_unpack(c, np, order, records, cell, off3, vel3, mass));
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_brick_start(lf2_ctx* c, int64_t np, const int32_t* cell, int64_t* brick_start)
+{
+  if (!c || np < 0 || !brick_start || (np > 0 && !cell)) return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_pm_brick_start(c, np, cell, brick_start));
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_grads_unorder(lf2_ctx* c, int64_t np, const int64_t* order, const float* g_off3,
+                                const float* g_vel3, const float* g_mass, double inv_res,
+                                void* records, double* g_pos3_out, double* g_vel3_out,
+                                double* g_mass_out)
+{
+  if (!c || np < 0) return LF2_ERR_ARG;
+  if (np > 0 && (!order || !g_off3 || !g_vel3 || !g_mass || !records || !aligned16(records) ||
+                 !g_pos3_out || !g_vel3_out || !g_mass_out))
+    return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_pm_grads_back(c, np, order, g_off3, g_vel3, g_mass, inv_res, records,
+                                   g_pos3_out, g_vel3_out, g_mass_out));
+  return LF2_OK;
+}
+
+lf2_status lf2_pm_deposit_bricks(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
+                                 const float* mass, double gmass, const int64_t* brick_start,
+                                 float* rho)
+{
+  if (!c || np < 0 || !brick_start || !rho || (np > 0 && (!cell || !off3))) return LF2_ERR_ARG;
+  LF2_CUDA(c, launch_pm_deposit(c, np, brick_start, cell, off3, mass, (float)gmass, rho));
+  return LF2_OK;
+}
+
 lf2_status lf2_pm_deposit(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
                           const float* mass, double gmass, float* rho)
 {

@@ -216,6 +216,20 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
                       const float* mass, float gmass, const float* in_a, const float* in_b,
                       float* out_a, float* out_b, float dta, float dtb, int32_t* cell_rw,
                       float* off_rw, float* vel_rw);
+// the chain's deposit, per particle or brick-tiled (brick_start given)
+cudaError_t launch_pm_deposit(lf2_ctx* c, int64_t np, const int64_t* brick_start, const int32_t* cell,
+                              const float* off3, const float* mass, float gmass, float* rho);
+// the chain's particle state: sort keys and 32-byte records in the caller's
+// order, the state in a given order, the bricks' first slots; gradients back
+// to the caller's order through the same records
+cudaError_t launch_pm_pack(lf2_ctx* c, int64_t np, const double* pos, const double* vel,
+                           const double* mass, double inv_res, int32_t* key, void* rec);
+cudaError_t launch_pm_unpack(lf2_ctx* c, int64_t np, const int64_t* order, const void* rec,
+                             int32_t* cell, float* off3, float* vel3, float* m);
+cudaError_t launch_pm_brick_start(lf2_ctx* c, int64_t np, const int32_t* cell, int64_t* brick_start);
+cudaError_t launch_pm_grads_back(lf2_ctx* c, int64_t np, const int64_t* order, const float* g_off3,
+                                 const float* g_vel3, const float* g_m, double inv_res, void* rec,
+                                 double* g_pos, double* g_vel, double* g_mass);
 cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, float* out,
                            float* partial);
 size_t stencil_partial_floats(const lf2_ctx* c);

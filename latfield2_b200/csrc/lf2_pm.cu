@@ -121,6 +121,139 @@ __global__ void k_pm_deposit_fixed(Geom g, int64_t np, const int32_t* __restrict
   }
 }
 
+// Brick-tiled forms of the two deposits, for particles grouped by brick
+// (brick_start[b] .. brick_start[b+1] hold the particles that were in brick
+// b when the chain sorted its state; a particle that has since drifted out
+// of the brick goes straight to the global sums).  One CTA per brick: its
+// particles add their corner weights into the brick's (BRICK+1)^3 vertex
+// tile in shared memory, then the tile's non-zero sums go to the global
+// field with one atomic each: 4913 global atomics per brick instead of 8 per
+// particle.  The fixed-point tile keeps a low word whose carry goes to a high
+// word (the order of the additions does not change the sums); the FP32 tile
+// adds floats, so its roundings depend on the order, as the global atomics'
+// do.
+__device__ __forceinline__ bool in_brick(int x, int y, int z, int x0, int y0, int z0)
+{
+  return (unsigned)(x - x0) < (unsigned)BRICK && (unsigned)(y - y0) < (unsigned)BRICK &&
+         (unsigned)(z - z0) < (unsigned)BRICK;
+}
+
+// The group's range of brick b, clamped to the particle arrays.
+__device__ __forceinline__ void group_range(const int64_t* brick_start, int64_t b, int64_t np,
+                                            int64_t& p0, int64_t& p1)
+{
+  p0 = min(max(brick_start[b], (int64_t)0), np);
+  p1 = min(max(brick_start[b + 1], p0), np);
+}
+
+// Vertex (x0 + i, y0 + j, z0 + k) of a brick tile, wrapped periodically.
+__device__ __forceinline__ int64_t tile_site(const Geom& g, int t, int x0, int y0, int z0)
+{
+  int x = x0 + t % TILE, y = y0 + (t / TILE) % TILE, z = z0 + t / (TILE * TILE);
+  x -= x >= g.n[0] ? g.n[0] : 0;
+  y -= y >= g.n[1] ? g.n[1] : 0;
+  z -= z >= g.n[2] ? g.n[2] : 0;
+  return site_index(g, x, y, z);
+}
+
+__global__ void __launch_bounds__(256)
+    k_pm_deposit_fixed_tile(Geom g, int64_t np, const int64_t* __restrict__ brick_start,
+                            const int32_t* __restrict__ cell, const float* __restrict__ off3,
+                            const float* __restrict__ mass, const uint32_t* __restrict__ mmax,
+                            unsigned long long* __restrict__ acc)
+{
+  __shared__ uint32_t lo[TILE3], hi[TILE3];
+  for (int t = threadIdx.x; t < TILE3; t += blockDim.x) lo[t] = hi[t] = 0u;
+  __syncthreads();
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+  const float inv_m = mass ? 1.0f / __uint_as_float(*mmax) : 0.0f;
+  int64_t p0, p1;
+  group_range(brick_start, b, np, p0, p1);
+  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    const int32_t c = cell[p];
+    const int x = c % g.n[0], y = (c / g.n[0]) % g.n[1], z = c / (g.n[0] * g.n[1]);
+    const uint32_t ux = weight_q(off3[3 * p]), uy = weight_q(off3[3 * p + 1]), uz = weight_q(off3[3 * p + 2]);
+    const uint32_t qx[2] = {(1u << 31) - ux, ux}, qy[2] = {(1u << 31) - uy, uy}, qz[2] = {(1u << 31) - uz, uz};
+    const uint64_t mq = mass ? (uint64_t)__float2uint_rn(fminf(__fmul_rn(mass[p], inv_m), 1.0f) * 16777216.0f) : 0;
+    if (in_brick(x, y, z, x0, y0, z0)) {
+      const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int cx = (q >> 2) & 1, cy = (q >> 1) & 1, cz = q & 1;
+        uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+        if (mass) w = (w * mq + (1ull << 23)) >> 24;
+        const int t = t0 + cx + TILE * (cy + TILE * cz);
+        const uint32_t wl = (uint32_t)w;
+        const uint32_t old = atomicAdd(&lo[t], wl);
+        const uint32_t up = (uint32_t)(w >> 32) + ((uint32_t)(old + wl) < old ? 1u : 0u);
+        if (up) atomicAdd(&hi[t], up);
+      }
+    } else {  // drifted out of the brick since the sort
+      const int xs[2] = {x, x + 1 < g.n[0] ? x + 1 : 0};
+      const int ys[2] = {y, y + 1 < g.n[1] ? y + 1 : 0};
+      const int zs[2] = {z, z + 1 < g.n[2] ? z + 1 : 0};
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int cx = (q >> 2) & 1, cy = (q >> 1) & 1, cz = q & 1;
+        uint64_t w = fixed_corner(qx[cx], qy[cy], qz[cz]);
+        if (mass) w = (w * mq + (1ull << 23)) >> 24;
+        atomicAdd(&acc[site_index(g, xs[cx], ys[cy], zs[cz])], (unsigned long long)w);
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
+    const unsigned long long v = ((unsigned long long)hi[t] << 32) | lo[t];
+    if (v) atomicAdd(&acc[tile_site(g, t, x0, y0, z0)], v);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_pm_deposit_tile(Geom g, int64_t np, const int64_t* __restrict__ brick_start,
+                      const int32_t* __restrict__ cell, const float* __restrict__ off3,
+                      const float* __restrict__ mass, float gmass, float inv_vol,
+                      float* __restrict__ rho)
+{
+  __shared__ float tile[TILE3];
+  for (int t = threadIdx.x; t < TILE3; t += blockDim.x) tile[t] = 0.0f;
+  __syncthreads();
+  const int64_t b = blockIdx.x;
+  int bx, by, bz;
+  brick_coords(g, b, bx, by, bz);
+  const int x0 = bx * BRICK, y0 = by * BRICK, z0 = bz * BRICK;
+  int64_t p0, p1;
+  group_range(brick_start, b, np, p0, p1);
+  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    const int32_t c = cell[p];
+    const int x = c % g.n[0], y = (c / g.n[0]) % g.n[1], z = c / (g.n[0] * g.n[1]);
+    const float m = (mass ? mass[p] : gmass) * inv_vol;
+    if (in_brick(x, y, z, x0, y0, z0)) {
+      const float f[3] = {off3[3 * p], off3[3 * p + 1], off3[3 * p + 2]};
+      const float h[3] = {1.0f - f[0], 1.0f - f[1], 1.0f - f[2]};
+      const int t0 = (x - x0) + TILE * ((y - y0) + TILE * (z - z0));
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int cx = (q >> 2) & 1, cy = (q >> 1) & 1, cz = q & 1;
+        const float w = (cx ? f[0] : h[0]) * (cy ? f[1] : h[1]) * (cz ? f[2] : h[2]);
+        atomicAdd(&tile[t0 + cx + TILE * (cy + TILE * cz)], w * m);
+      }
+    } else {  // drifted out of the brick since the sort
+      Corners k;
+      corners(g, c, off3, p, k);
+#pragma unroll
+      for (int q = 0; q < 8; q++) atomicAdd(&rho[k.site[q]], k.w[q] * m);
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < TILE3; t += blockDim.x) {
+    const float v = tile[t];
+    if (v != 0.0f) atomicAdd(&rho[tile_site(g, t, x0, y0, z0)], v);
+  }
+}
+
 __global__ void k_pm_fixed_to_rho(int64_t ns, unsigned long long* __restrict__ acc, const float* mass,
                                   const uint32_t* __restrict__ mmax, float gmass, float inv_vol,
                                   float* __restrict__ rho, uint32_t* flags)
@@ -385,6 +518,135 @@ __global__ void k_stencil_adj_S_sum(int ntiles, const float* __restrict__ partia
                                            (red[2][threadIdx.x] + red[3][threadIdx.x]);
 }
 
+// ------------------------------------------------------ chain state
+// Cell and FP32 in-cell offset of a box-unit FP64 position: u = pos * inv_res
+// (the product by the reciprocal, as a division by a scalar runs on the GPU
+// in torch), floor, the offset u - floor(u) rounded to FP32 with the carry of
+// an offset that rounds up to 1, then the periodic wrap.
+__device__ __forceinline__ int32_t pos_state(const Geom& g, const double* p, double inv_res,
+                                             float o[3])
+{
+  long long ci[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const double u = __dmul_rn(p[d], inv_res);
+    double fl = floor(u);
+    float od = __double2float_rn(__dsub_rn(u, fl));
+    if (od >= 1.0f) {
+      od = 0.0f;
+      fl = __dadd_rn(fl, 1.0);
+    }
+    long long c = (long long)fl % (long long)g.n[d];
+    if (c < 0) c += g.n[d];
+    ci[d] = c;
+    o[d] = od;
+  }
+  return (int32_t)(ci[0] + (long long)g.n[0] * (ci[1] + (long long)g.n[1] * ci[2]));
+}
+
+// Sort key of a cell: its brick, then its place in the brick (x fastest),
+// so that sorted particles come grouped by brick and by cell inside it.
+__device__ __forceinline__ int32_t brick_key(const Geom& g, int32_t c)
+{
+  const int x = c % g.n[0], y = (c / g.n[0]) % g.n[1], z = c / (g.n[0] * g.n[1]);
+  const int64_t b = brick_of(g, x, y, z);
+  return (int32_t)(b * (BRICK * BRICK * BRICK) + (x % BRICK) + BRICK * ((y % BRICK) + BRICK * (z % BRICK)));
+}
+
+// Caller order, coalesced: the sort key of every particle (brick_key) and
+// its 32-byte record (cell, offsets, FP32 velocity, FP32 mass), so that the
+// permutation reads one full sector per particle.
+__global__ void k_pm_pack(Geom g, int64_t np, const double* __restrict__ pos,
+                          const double* __restrict__ vel, const double* __restrict__ mass,
+                          double inv_res, int32_t* __restrict__ key, uint4* __restrict__ rec)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float o[3];
+    const int32_t c = pos_state(g, pos + 3 * i, inv_res, o);
+    key[i] = brick_key(g, c);
+    const float m = mass ? __double2float_rn(mass[i]) : 0.0f;
+    rec[2 * i] = make_uint4((uint32_t)c, __float_as_uint(o[0]), __float_as_uint(o[1]),
+                            __float_as_uint(o[2]));
+    rec[2 * i + 1] = make_uint4(__float_as_uint(__double2float_rn(vel[3 * i])),
+                                __float_as_uint(__double2float_rn(vel[3 * i + 1])),
+                                __float_as_uint(__double2float_rn(vel[3 * i + 2])), __float_as_uint(m));
+  }
+}
+
+// Slot i takes the record of particle order[i].
+__global__ void k_pm_unpack(int64_t np, const int64_t* __restrict__ order, const uint4* __restrict__ rec,
+                            int32_t* __restrict__ cell, float* __restrict__ off3,
+                            float* __restrict__ vel3, float* __restrict__ m)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = order[i];
+    const uint4 a = rec[2 * s], b = rec[2 * s + 1];
+    cell[i] = (int32_t)a.x;
+    off3[3 * i] = __uint_as_float(a.y), off3[3 * i + 1] = __uint_as_float(a.z);
+    off3[3 * i + 2] = __uint_as_float(a.w);
+    vel3[3 * i] = __uint_as_float(b.x), vel3[3 * i + 1] = __uint_as_float(b.y);
+    vel3[3 * i + 2] = __uint_as_float(b.z);
+    if (m) m[i] = __uint_as_float(b.w);
+  }
+}
+
+// First slot of every brick among cells sorted by brick_key (bricks without
+// particles start where the next one does; brick_start[nb] = np): one thread
+// per brick, a binary search over the sorted slots.
+__global__ void k_pm_brick_start(Geom g, int64_t np, const int32_t* __restrict__ cell,
+                                 int64_t* __restrict__ brick_start)
+{
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= g.nbricks;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = np;  // first slot whose brick is b or later
+    while (lo < hi) {
+      const int64_t mid = lo + ((hi - lo) >> 1);
+      const int32_t c = cell[mid];
+      const int x = c % g.n[0], y = (c / g.n[0]) % g.n[1], z = c / (g.n[0] * g.n[1]);
+      if (brick_of(g, x, y, z) < b) lo = mid + 1;
+      else hi = mid;
+    }
+    brick_start[b] = lo;
+  }
+}
+
+// The gradients of slot i as the 32-byte record of particle order[i] (one
+// full sector written per particle; no partial-sector writes).
+__global__ void k_pm_grads_scatter(int64_t np, const int64_t* __restrict__ order,
+                                   const float* __restrict__ g_off3, const float* __restrict__ g_vel3,
+                                   const float* __restrict__ g_m, uint4* __restrict__ rec)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = order[i];
+    rec[2 * s] = make_uint4(__float_as_uint(g_off3[3 * i]), __float_as_uint(g_off3[3 * i + 1]),
+                            __float_as_uint(g_off3[3 * i + 2]), __float_as_uint(g_m[i]));
+    rec[2 * s + 1] = make_uint4(__float_as_uint(g_vel3[3 * i]), __float_as_uint(g_vel3[3 * i + 1]),
+                                __float_as_uint(g_vel3[3 * i + 2]), 0u);
+  }
+}
+
+// Caller order, coalesced: the records into FP64 gradients (the offset
+// gradient times inv_res: per box unit).
+__global__ void k_pm_grads_unpack(int64_t np, const uint4* __restrict__ rec, double inv_res,
+                                  double* __restrict__ g_pos, double* __restrict__ g_vel,
+                                  double* __restrict__ g_mass)
+{
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 a = rec[2 * i], b = rec[2 * i + 1];
+    g_pos[3 * i] = __dmul_rn((double)__uint_as_float(a.x), inv_res);
+    g_pos[3 * i + 1] = __dmul_rn((double)__uint_as_float(a.y), inv_res);
+    g_pos[3 * i + 2] = __dmul_rn((double)__uint_as_float(a.z), inv_res);
+    g_mass[i] = (double)__uint_as_float(a.w);
+    g_vel[3 * i] = (double)__uint_as_float(b.x);
+    g_vel[3 * i + 1] = (double)__uint_as_float(b.y);
+    g_vel[3 * i + 2] = (double)__uint_as_float(b.z);
+  }
+}
+
 }  // namespace
 
 inline dim3 stencil_grid(const Geom& g)
@@ -398,6 +660,51 @@ inline int64_t stencil_tiles(const Geom& g)
   return (int64_t)d.x * d.y * d.z;
 }
 
+// The chain's deposit into rho (+=): per particle, or brick-tiled when
+// brick_start is given (particles grouped by brick, nbricks + 1 entries).
+cudaError_t launch_pm_deposit(lf2_ctx* c, int64_t np, const int64_t* brick_start, const int32_t* cell,
+                              const float* off3, const float* mass, float gmass, float* rho)
+{
+  const double vol = c->res * c->res * c->res;
+  const float inv_vol = (float)(1.0 / vol);
+  const Geom g = c->g;
+  const unsigned nb = (unsigned)g.nbricks;
+  if (c->mode == LF2_DEPOSIT_FIXED64) {
+    // integer sums in the context's scratch (zero between calls)
+    if (!c->pm_acc) {
+      cudaError_t e = cudaMalloc(&c->pm_acc, sizeof(unsigned long long) * (size_t)g.nsites + 256);
+      if (e != cudaSuccess) return e;
+      e = cudaMemsetAsync(c->pm_acc, 0, sizeof(unsigned long long) * (size_t)g.nsites + 256, c->stream);
+      if (e != cudaSuccess) return e;
+    }
+    uint32_t* mmax = reinterpret_cast<uint32_t*>(c->pm_acc + g.nsites);
+    if (mass) {
+      cudaError_t e = cudaMemsetAsync(mmax, 0, sizeof(uint32_t), c->stream);
+      if (e != cudaSuccess) return e;
+      c->launches += 1;
+      k_pm_mass_max<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(np, mass, mmax);
+    }
+    c->launches += 2;
+    if (brick_start)
+      k_pm_deposit_fixed_tile<<<nb, 256, 0, c->stream>>>(g, np, brick_start, cell, off3, mass, mmax,
+                                                          c->pm_acc);
+    else
+      k_pm_deposit_fixed<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3,
+                                                                                mass, mmax, c->pm_acc);
+    k_pm_fixed_to_rho<<<grid_for(g.nsites, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+        g.nsites, c->pm_acc, mass, mmax, gmass, inv_vol, rho, c->flags);
+    return cudaGetLastError();
+  }
+  c->launches += 1;
+  if (brick_start)
+    k_pm_deposit_tile<<<nb, 256, 0, c->stream>>>(g, np, brick_start, cell, off3, mass, gmass, inv_vol,
+                                                 rho);
+  else
+    k_pm_deposit<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3, mass,
+                                                                          gmass, inv_vol, rho);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const float* off3,
                       const float* mass, float gmass, const float* in_a, const float* in_b,
                       float* out_a, float* out_b, float dta, float dtb, int32_t* cell_rw,
@@ -408,32 +715,7 @@ cudaError_t launch_pm(lf2_ctx* c, int op, int64_t np, const int32_t* cell, const
   const Geom g = c->g;
   switch (op) {
     case 0:  // deposit into out_a
-      if (c->mode == LF2_DEPOSIT_FIXED64) {
-        // integer sums in the context's scratch (zero between calls)
-        if (!c->pm_acc) {
-          cudaError_t e = cudaMalloc(&c->pm_acc, sizeof(unsigned long long) * (size_t)g.nsites + 256);
-          if (e != cudaSuccess) return e;
-          e = cudaMemsetAsync(c->pm_acc, 0, sizeof(unsigned long long) * (size_t)g.nsites + 256, c->stream);
-          if (e != cudaSuccess) return e;
-        }
-        uint32_t* mmax = reinterpret_cast<uint32_t*>(c->pm_acc + g.nsites);
-        if (mass) {
-          cudaError_t e = cudaMemsetAsync(mmax, 0, sizeof(uint32_t), c->stream);
-          if (e != cudaSuccess) return e;
-          c->launches += 1;
-          k_pm_mass_max<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(np, mass, mmax);
-        }
-        c->launches += 2;
-        k_pm_deposit_fixed<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3,
-                                                                                  mass, mmax, c->pm_acc);
-        k_pm_fixed_to_rho<<<grid_for(g.nsites, PM_THREADS), PM_THREADS, 0, c->stream>>>(
-            g.nsites, c->pm_acc, mass, mmax, gmass, inv_vol, out_a, c->flags);
-        break;
-      }
-      c->launches += 1;
-      k_pm_deposit<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(g, np, cell, off3, mass,
-                                                                            gmass, inv_vol, out_a);
-      break;
+      return launch_pm_deposit(c, np, nullptr, cell, off3, mass, gmass, out_a);
     case 1:  // gather in_a (F4) -> out_a (np x 3)
       c->launches += 1;
       k_pm_gather<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
@@ -483,5 +765,46 @@ cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, f
 }
 
 size_t stencil_partial_floats(const lf2_ctx* c) { return (size_t)stencil_tiles(c->g) * 81; }
+
+cudaError_t launch_pm_pack(lf2_ctx* c, int64_t np, const double* pos, const double* vel,
+                           const double* mass, double inv_res, int32_t* key, void* rec)
+{
+  if (np == 0) return cudaSuccess;
+  c->launches += 1;
+  k_pm_pack<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      c->g, np, pos, vel, mass, inv_res, key, reinterpret_cast<uint4*>(rec));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pm_unpack(lf2_ctx* c, int64_t np, const int64_t* order, const void* rec,
+                             int32_t* cell, float* off3, float* vel3, float* m)
+{
+  if (np == 0) return cudaSuccess;
+  c->launches += 1;
+  k_pm_unpack<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      np, order, reinterpret_cast<const uint4*>(rec), cell, off3, vel3, m);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pm_brick_start(lf2_ctx* c, int64_t np, const int32_t* cell, int64_t* brick_start)
+{
+  c->launches += 1;
+  k_pm_brick_start<<<grid_for(c->g.nbricks + 1, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      c->g, np, cell, brick_start);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pm_grads_back(lf2_ctx* c, int64_t np, const int64_t* order, const float* g_off3,
+                                 const float* g_vel3, const float* g_m, double inv_res, void* rec,
+                                 double* g_pos, double* g_vel, double* g_mass)
+{
+  if (np == 0) return cudaSuccess;
+  c->launches += 2;
+  k_pm_grads_scatter<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      np, order, g_off3, g_vel3, g_m, reinterpret_cast<uint4*>(rec));
+  k_pm_grads_unpack<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      np, reinterpret_cast<const uint4*>(rec), inv_res, g_pos, g_vel, g_mass);
+  return cudaGetLastError();
+}
 
 }  // namespace lf2

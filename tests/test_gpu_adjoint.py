@@ -287,3 +287,100 @@ def test_fixed_point_chain_deposit(cuda, masses):
 def ops_ptr(t):
     import ctypes
     return ctypes.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("n", [48, 64])
+def test_chain_state_kernels_match_the_torch_restatement(cuda, n):
+    """lf2_pm_state_pack / lf2_pm_state_unpack / lf2_pm_grads_unorder (the
+    chain's particle state and its gradients' way back) bit for bit against
+    the torch expressions they replace: positions_to_state, the permutation
+    by order, and the scatter of the FP64 gradients; the sort key (brick,
+    then cell in the brick).  Positions include cell faces, the box's faces
+    and periodic images outside [0, 1)."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops
+    npart = 20000
+    g = torch.Generator(device="cpu").manual_seed(5)
+    pos = torch.rand(npart, 3, generator=g, dtype=torch.float64) * 3.0 - 1.0
+    pos[:500] = torch.randint(-n, 2 * n, (500, 3), generator=g).double() / n  # cell faces
+    pos[500:600] = torch.nextafter(pos[500:600], torch.full_like(pos[500:600], -10.0))
+    vel = torch.randn(npart, 3, generator=g, dtype=torch.float64)
+    m = torch.rand(npart, generator=g, dtype=torch.float64) + 0.5
+    pos, vel, m = pos.cuda(), vel.cuda(), m.cuda()
+    res = 1.0 / n
+    ctx = L.Context((n, n, n), box=1.0)
+    ops = _Ops(ctx)
+    cell_t, off_t = _state(pos, n)
+    key, rec = ops.state_pack(pos, vel, m, 1.0 / res)
+    c = cell_t.long()
+    x, y, z = c % n, (c // n) % n, c // (n * n)
+    nb = -(-n // 16)
+    want_key = (((x // 16) + nb * ((y // 16) + nb * (z // 16))) * 4096 + x % 16
+                + 16 * (y % 16 + 16 * (z % 16)))
+    assert torch.equal(key.long(), want_key)
+    order = torch.argsort(key)
+    cell, off, vel32, m32 = ops.state_unpack(order, rec)
+    assert torch.equal(cell, cell_t[order])
+    assert torch.equal(off, off_t[order])
+    assert torch.equal(vel32, vel.float()[order])
+    assert torch.equal(m32, m.float()[order])
+    g_off = torch.randn(npart, 3, generator=g).cuda()
+    g_v = torch.randn(npart, 3, generator=g).cuda()
+    g_m = torch.randn(npart, generator=g).cuda()
+    g_pos, g_vel, g_mass = ops.grads_unorder(order, g_off, g_v, g_m, 1.0 / res)
+    want = torch.empty(npart, 3, dtype=torch.float64, device="cuda")
+    want[order] = g_off.to(torch.float64) / res
+    assert torch.equal(g_pos, want)
+    want = torch.empty(npart, 3, dtype=torch.float64, device="cuda")
+    want[order] = g_v.to(torch.float64)
+    assert torch.equal(g_vel, want)
+    want = torch.empty(npart, dtype=torch.float64, device="cuda")
+    want[order] = g_m.to(torch.float64)
+    assert torch.equal(g_mass, want)
+
+
+@pytest.mark.parametrize("mode", ["fixed", "fp32"])
+def test_brick_tiled_chain_deposit_matches_the_per_particle_one(cuda, mode):
+    """lf2_pm_deposit_bricks (particles grouped by brick, brick_start from
+    lf2_pm_brick_start) against lf2_pm_deposit on the same particles: the
+    same sums in the fixed-point mode, within 1e-5 of the maximum in the FP32
+    mode (FP32 atomics in two orders); again after a drift has moved
+    particles out of their groups' bricks."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops
+    n, npart = 40, 300000
+    g = torch.Generator(device="cpu").manual_seed(9)
+    pos = (0.5 + 0.15 * torch.randn(npart, 3, generator=g, dtype=torch.float64)) % 1.0
+    vel = torch.randn(npart, 3, generator=g, dtype=torch.float64)
+    m = (torch.rand(npart, generator=g, dtype=torch.float64) + 0.5) / npart
+    pos, vel, m = pos.cuda(), vel.cuda(), m.cuda()
+    ctx = L.Context((n, n, n), box=1.0, mode=L.DEPOSIT_FIXED64 if mode == "fixed" else L.DEPOSIT_FP32)
+    ops = _Ops(ctx)
+    key, rec = ops.state_pack(pos, vel, m, float(n))
+    order = torch.argsort(key)
+    cell, off, vel32, m32 = ops.state_unpack(order, rec)
+    bs = ops.brick_start(cell)
+    c = cell.long()
+    nb = -(-n // 16)
+    brick = (c % n) // 16 + nb * (((c // n) % n) // 16 + nb * ((c // (n * n)) // 16))
+    assert torch.equal(bs, torch.searchsorted(brick, torch.arange(nb ** 3 + 1, device="cuda")))
+    for drift in (0.0, 0.4 / n):
+        if drift:
+            ops.kick_drift(cell, off, vel32, None, drift)
+            c = cell.long()
+            now = (c % n) // 16 + nb * (((c // n) % n) // 16 + nb * ((c // (n * n)) // 16))
+            assert int((now != brick).sum()) > 1000  # strays
+        a = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+        b = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+        ops.bricks = None
+        ops.deposit(cell, off, m32, a)
+        ops.bricks = bs
+        ops.deposit(cell, off, m32, b)
+        if mode == "fixed":
+            assert torch.equal(a, b)
+        else:
+            assert float((a - b).abs().max()) <= 1e-5 * float(a.abs().max())
+        total = float(m32.double().sum())
+        assert abs(float(b.double().sum()) / n ** 3 - total) <= 1e-5 * total
