@@ -1,8 +1,10 @@
 // lf2_pm.cu -- kernels of the differentiable particle-mesh chain: CIC deposit
-// and gather on particles kept in the caller's order (no rebinning, so that
-// gradients stay attached to their particles), the kick-drift update, a
-// periodic 27-point stencil as the grid operator, and the hand-written
-// adjoints of all of them.
+// and gather on particles kept in one order for a whole call (sorted by
+// brick and cell when the call starts, no rebinning, so that gradients stay
+// attached to their slots), the kick-drift update, a periodic 27-point
+// stencil as the grid operator, the hand-written adjoints of all of them,
+// and the permutations of the particle state into that order and of the
+// gradients back.
 //
 //   deposit   rho(v)   += m_p / res^3 * W(v - x_p)            (scalarProjectionCIC)
 //   gather    G_p       = sum_k W_k(x_p) F(corner_k)           (updateVel CIC kick)
