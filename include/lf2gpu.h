@@ -465,6 +465,11 @@ lf2_status lf2_pm_gather(lf2_ctx* ctx, int64_t np, const int32_t* cell,
 lf2_status lf2_pm_kick_drift(lf2_ctx* ctx, int64_t np, int32_t* cell,
                              float* off3, float* vel3, const float* G3,
                              double dt_kick, double dt_drift);
+/* gather + kick_drift in one pass, the same results bit for bit:
+ * vel += dt_kick * sum_k W_k F4(corner_k), then the drift. */
+lf2_status lf2_pm_step(lf2_ctx* ctx, int64_t np, int32_t* cell, float* off3,
+                       float* vel3, const float* F4, double dt_kick,
+                       double dt_drift);
 lf2_status lf2_pm_deposit_adjoint(lf2_ctx* ctx, int64_t np,
                                   const int32_t* cell, const float* off3,
                                   const float* mass, double gmass,

@@ -105,6 +105,7 @@ SIGNATURES = {
                              c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_pm_deposit_bricks": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p,
                               c_void_p],
+    "lf2_pm_step": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double, c_double],
     "lf2_pm_deposit": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_double, c_void_p],
     "lf2_pm_gather": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p],
     "lf2_pm_kick_drift": [c_void_p, c_i64, c_void_p, c_void_p, c_void_p, c_void_p, c_double,

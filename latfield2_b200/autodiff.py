@@ -7,6 +7,7 @@ rebinning; the gradients come back in the caller's order):
     F_k     = pm_force(rho_k)                    lf2_pm_force4       (the FFT Poisson force)
     G_k     = gather(x_k, F_k)                   lf2_pm_gather       (CIC gather of updateVel)
     v_{k+1} = v_k + dt G_k ;  x_{k+1} = x_k + dt v_{k+1}             lf2_pm_kick_drift
+(the last two in one pass, lf2_pm_step)
 and finally rho_K = deposit(x_K, m), loss = sum_g w_g rho_K(g).
 
 `PMChain` is a torch.autograd.Function whose backward runs the hand-written
@@ -160,9 +161,9 @@ class _Ops:
         return rho, F
 
     def step(self, cell, off, vel, F, dt):
-        G = torch.empty_like(vel)
-        self.gather(cell, off, F, G)
-        self.kick_drift(cell, off, vel, G, dt)
+        """gather, kick and drift in one pass (lf2_pm_step)."""
+        _check(self.ctx, self.lib.lf2_pm_step(self.ctx.h, cell.numel(), _p(cell), _p(off), _p(vel),
+                                              _p(F), dt, dt), "pm_step")
 
 
 class PMChain(torch.autograd.Function):

@@ -1215,6 +1215,16 @@ lf2_status lf2_pm_kick_drift(lf2_ctx* c, int64_t np, int32_t* cell, float* off3,
                  dt_drift / c->res, cell, off3, vel3);
 }
 
+lf2_status lf2_pm_step(lf2_ctx* c, int64_t np, int32_t* cell, float* off3, float* vel3,
+                       const float* F4, double dt_kick, double dt_drift)
+{
+  if (!c || np < 0 || !F4 || !f4_ok(F4) || (np > 0 && (!cell || !off3 || !vel3))) return LF2_ERR_ARG;
+  if (np == 0) return LF2_OK;
+  PhaseScope ps(c, PH_OTHER);
+  LF2_CUDA(c, launch_pm_step(c, np, cell, off3, vel3, F4, (float)dt_kick, (float)(dt_drift / c->res)));
+  return LF2_OK;
+}
+
 lf2_status lf2_pm_deposit_adjoint(lf2_ctx* c, int64_t np, const int32_t* cell, const float* off3,
                                   const float* mass, double gmass, const float* g_rho,
                                   float* g_off3, float* g_mass)

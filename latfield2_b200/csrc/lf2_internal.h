@@ -222,6 +222,8 @@ cudaError_t launch_pm_deposit(lf2_ctx* c, int64_t np, const int64_t* brick_start
 // the chain's particle state: sort keys and 32-byte records in the caller's
 // order, the state in a given order, the bricks' first slots; gradients back
 // to the caller's order through the same records
+cudaError_t launch_pm_step(lf2_ctx* c, int64_t np, int32_t* cell, float* off3, float* vel3,
+                           const float* F4, float dtk, float dtn);
 cudaError_t launch_pm_pack(lf2_ctx* c, int64_t np, const double* pos, const double* vel,
                            const double* mass, double inv_res, int32_t* key, void* rec);
 cudaError_t launch_pm_unpack(lf2_ctx* c, int64_t np, const int64_t* order, const void* rec,

@@ -324,6 +324,50 @@ __global__ void k_pm_kick_drift(Geom g, int64_t np, int32_t* __restrict__ cell, 
   }
 }
 
+// The gather, the kick and the drift of one chain step in one pass, with
+// the arithmetic of k_pm_gather and k_pm_kick_drift (the same results bit
+// for bit) and no gathered field written in between.
+__global__ void k_pm_gather_kick_drift(Geom g, int64_t np, int32_t* __restrict__ cell,
+                                       float* __restrict__ off3, float* __restrict__ vel3,
+                                       const float4* __restrict__ F4, float dtk, float dtn,
+                                       uint32_t* flags)
+{
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = cell[p];
+    Corners k;
+    corners(g, c, off3, p, k);
+    float a[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const float4 f = __ldg(F4 + k.site[q]);
+      a[0] = fmaf(k.w[q], f.x, a[0]);
+      a[1] = fmaf(k.w[q], f.y, a[1]);
+      a[2] = fmaf(k.w[q], f.z, a[2]);
+    }
+    int xyz[3] = {c % g.n[0], (c / g.n[0]) % g.n[1], c / (g.n[0] * g.n[1])};
+    for (int d = 0; d < 3; d++) {
+      float v = __fmaf_rn(dtk, a[d], vel3[3 * p + d]);
+      vel3[3 * p + d] = v;
+      float o = __fmaf_rn(dtn, v, off3[3 * p + d]);
+      if (!isfinite(o)) {
+        set_flag(flags, ERR_NONFINITE);
+        continue;
+      }
+      const float fl = floorf(o);
+      o = __fsub_rn(o, fl);
+      int carry = (int)fl;
+      if (o >= 1.0f) {
+        o = 0.0f;
+        carry += 1;
+      }
+      off3[3 * p + d] = o;
+      xyz[d] = wrap_add(xyz[d], carry, g.n[d]);
+    }
+    cell[p] = (int32_t)site_index(g, xyz[0], xyz[1], xyz[2]);
+  }
+}
+
 __global__ void k_pm_deposit_adj(Geom g, int64_t np, const int32_t* __restrict__ cell,
                                  const float* __restrict__ off3, const float* __restrict__ mass,
                                  float gmass, float inv_vol, const float* __restrict__ g_rho,
@@ -767,6 +811,16 @@ cudaError_t launch_stencil(lf2_ctx* c, int op, const float* a, const float* S, f
 }
 
 size_t stencil_partial_floats(const lf2_ctx* c) { return (size_t)stencil_tiles(c->g) * 81; }
+
+cudaError_t launch_pm_step(lf2_ctx* c, int64_t np, int32_t* cell, float* off3, float* vel3,
+                           const float* F4, float dtk, float dtn)
+{
+  if (np == 0) return cudaSuccess;
+  c->launches += 1;
+  k_pm_gather_kick_drift<<<grid_for(np, PM_THREADS), PM_THREADS, 0, c->stream>>>(
+      c->g, np, cell, off3, vel3, reinterpret_cast<const float4*>(F4), dtk, dtn, c->flags);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_pm_pack(lf2_ctx* c, int64_t np, const double* pos, const double* vel,
                            const double* mass, double inv_res, int32_t* key, void* rec)

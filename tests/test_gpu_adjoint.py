@@ -384,3 +384,28 @@ def test_brick_tiled_chain_deposit_matches_the_per_particle_one(cuda, mode):
             assert float((a - b).abs().max()) <= 1e-5 * float(a.abs().max())
         total = float(m32.double().sum())
         assert abs(float(b.double().sum()) / n ** 3 - total) <= 1e-5 * total
+
+
+def test_fused_chain_step_equals_gather_then_kick_drift(cuda):
+    """lf2_pm_step (gather, kick and drift in one pass) gives the cells,
+    offsets and velocities of lf2_pm_gather followed by lf2_pm_kick_drift
+    bit for bit, face crossings and the periodic wrap included."""
+    import torch
+    import latfield2_b200 as L
+    from latfield2_b200.autodiff import _Ops
+    n, npart = 24, 50000
+    pos, vel, m, S, w = _case(n, npart, 21, "cuda")
+    ctx = L.Context((n, n, n), box=1.0)
+    ops = _Ops(ctx)
+    cell, off = _state(pos, n)
+    v = (vel * 20).float().contiguous()
+    F4 = torch.randn(4 * n ** 3, generator=torch.Generator(device="cpu").manual_seed(3)).cuda()
+    a = (cell.clone(), off.clone(), v.clone())
+    b = (cell.clone(), off.clone(), v.clone())
+    G = torch.empty_like(v)
+    ops.gather(a[0], a[1], F4, G)
+    ops.kick_drift(a[0], a[1], a[2], G, 0.05)
+    ops.step(b[0], b[1], b[2], F4, 0.05)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    assert int((a[0] != cell).sum()) > 1000
