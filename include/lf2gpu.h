@@ -174,7 +174,8 @@ lf2_status lf2_particles_add(lf2_ctx* ctx, int64_t n, const int32_t* cell,
  *     the mover path.  A record with a cell index or offset out of range is
  *     dropped and raises LF2_FLAG_BAD_CELL (the store is then not valid).
  *     When the store lacks room the records go through lf2_particles_add,
- *     which waits.
+ *     which waits and refuses the whole set (LF2_ERR_ARG, nothing added)
+ *     when a record is out of range.
  * Raised flags fail the context's next waiting call (lf2_synchronize) with
  * LF2_ERR_STATE. */
 lf2_status lf2_slab_record_words(lf2_ctx* ctx, int* words);
