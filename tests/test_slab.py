@@ -395,3 +395,37 @@ def test_slab_potential_emulated_in_one_process(ranks):
     phi = slab_potential_emulated(OracleEngine, torch.from_numpy(rho), ranks, COUPLING).numpy()
     want = FO.pm_force(rho, 1.0 / NPM, COUPLING)[0]
     assert np.abs(phi - want).max() <= 1e-5 * np.abs(want).max()
+
+
+def _run_still(dist_initialised):
+    """Particles at rest: the migration finds nobody to send, every message is
+    empty, and the particles stay as they were."""
+    from latfield2_b200.distributed import SlabDomain
+    from tests.slab_oracle_engine import OracleEngine
+    cell, off, vel, F, ids = _case()
+    vel = np.zeros_like(vel)
+    d = SlabDomain(N, box=1.0, mode=_lib.DEPOSIT_FIXED64, engine=OracleEngine)
+    d.set_particles(cell, off, vel, 1.0 / cell.shape[0], ids=ids)
+    Ff = d.field(3)
+    d.set_own_planes(Ff, np.zeros_like(F))
+    before = d.engine.particles()
+    for _ in range(2):
+        d.step(Ff, DTK, DTD)
+    after = d.engine.particles()
+    return d.rank, {k: np.array_equal(before[k], after[k]) for k in before}
+
+
+def test_a_step_without_migrants_sends_nothing_and_keeps_the_particles():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q, "_run_still")) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for _, same in res:
+        assert all(same.values()), same
